@@ -1,0 +1,126 @@
+/*
+ * Single-rank MPI stand-in used only to build the reference solver as a CPU
+ * oracle (test infrastructure; never linked into the GPU library).
+ *
+ * The reference is an MPI-3 code (shared-memory windows inside a node,
+ * point-to-point between nodes).  With one rank and SHN=1 every
+ * communicator has size 1, shared windows are plain heap blocks, collectives
+ * are copies and point-to-point messages only ever go to self.  This header
+ * declares exactly the subset of MPI the reference calls (see
+ * mpiparams.cpp, DataArray.H, AMRmpi.H, Nodedata.H, Mesh.cpp); the semantics
+ * are those of the MPI-3.1 standard restricted to a world of one process.
+ */
+#ifndef IB_ORACLE_MPI_SHIM_H
+#define IB_ORACLE_MPI_SHIM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int MPI_Comm;
+typedef int MPI_Datatype;
+typedef int MPI_Op;
+typedef int MPI_Win;
+typedef int MPI_Info;
+typedef int MPI_Request;
+typedef ptrdiff_t MPI_Aint;
+
+typedef struct MPI_Status {
+  int MPI_SOURCE;
+  int MPI_TAG;
+  int MPI_ERROR;
+  int count_bytes;
+} MPI_Status;
+
+#define MPI_COMM_WORLD 1
+#define MPI_COMM_SELF 2
+#define MPI_COMM_NULL 0
+
+#define MPI_DATATYPE_NULL 0
+#define MPI_INT 1
+#define MPI_DOUBLE 2
+#define MPI_CHAR 3
+#define MPI_BYTE 4
+#define MPI_LONG 5
+#define MPI_FLOAT 6
+
+#define MPI_SUM 1
+#define MPI_MAX 2
+#define MPI_MIN 3
+
+#define MPI_INFO_NULL 0
+#define MPI_COMM_TYPE_SHARED 1
+#define MPI_SUCCESS 0
+#define MPI_STATUS_IGNORE ((MPI_Status *)0)
+#define MPI_STATUSES_IGNORE ((MPI_Status *)0)
+#define MPI_REQUEST_NULL 0
+#define MPI_ANY_SOURCE (-1)
+#define MPI_ANY_TAG (-1)
+#define MPI_UNDEFINED (-32766)
+
+#define MPI_IN_PLACE ((void *)1)
+
+int MPI_Init(int *argc, char ***argv);
+int MPI_Finalize(void);
+int MPI_Abort(MPI_Comm comm, int errorcode);
+double MPI_Wtime(void);
+
+int MPI_Comm_size(MPI_Comm comm, int *size);
+int MPI_Comm_rank(MPI_Comm comm, int *rank);
+int MPI_Comm_split(MPI_Comm comm, int color, int key, MPI_Comm *newcomm);
+int MPI_Comm_split_type(MPI_Comm comm, int split_type, int key, MPI_Info info,
+                        MPI_Comm *newcomm);
+
+int MPI_Barrier(MPI_Comm comm);
+int MPI_Bcast(void *buffer, int count, MPI_Datatype datatype, int root, MPI_Comm comm);
+int MPI_Allreduce(const void *sendbuf, void *recvbuf, int count, MPI_Datatype datatype,
+                  MPI_Op op, MPI_Comm comm);
+int MPI_Reduce(const void *sendbuf, void *recvbuf, int count, MPI_Datatype datatype,
+               MPI_Op op, int root, MPI_Comm comm);
+int MPI_Allgather(const void *sendbuf, int sendcount, MPI_Datatype sendtype, void *recvbuf,
+                  int recvcount, MPI_Datatype recvtype, MPI_Comm comm);
+int MPI_Allgatherv(const void *sendbuf, int sendcount, MPI_Datatype sendtype, void *recvbuf,
+                   const int recvcounts[], const int displs[], MPI_Datatype recvtype,
+                   MPI_Comm comm);
+int MPI_Scatter(const void *sendbuf, int sendcount, MPI_Datatype sendtype, void *recvbuf,
+                int recvcount, MPI_Datatype recvtype, int root, MPI_Comm comm);
+
+int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest, int tag,
+             MPI_Comm comm);
+int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest, int tag,
+              MPI_Comm comm, MPI_Request *request);
+int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
+              MPI_Comm comm, MPI_Request *request);
+int MPI_Wait(MPI_Request *request, MPI_Status *status);
+int MPI_Waitany(int count, MPI_Request array_of_requests[], int *index, MPI_Status *status);
+
+int MPI_Type_contiguous(int count, MPI_Datatype oldtype, MPI_Datatype *newtype);
+int MPI_Type_commit(MPI_Datatype *datatype);
+int MPI_Type_free(MPI_Datatype *datatype);
+
+int MPI_Info_create(MPI_Info *info);
+int MPI_Info_set(MPI_Info info, const char *key, const char *value);
+int MPI_Info_free(MPI_Info *info);
+
+int MPI_Win_allocate_shared(MPI_Aint size, int disp_unit, MPI_Info info, MPI_Comm comm,
+                            void *baseptr, MPI_Win *win);
+int MPI_Win_shared_query(MPI_Win win, int rank, MPI_Aint *size, int *disp_unit,
+                         void *baseptr);
+int MPI_Win_create(void *base, MPI_Aint size, int disp_unit, MPI_Info info, MPI_Comm comm,
+                   MPI_Win *win);
+int MPI_Win_free(MPI_Win *win);
+int MPI_Win_fence(int assert_, MPI_Win win);
+int MPI_Win_lock_all(int assert_, MPI_Win win);
+int MPI_Win_unlock_all(MPI_Win win);
+int MPI_Win_flush_all(MPI_Win win);
+int MPI_Get(void *origin_addr, int origin_count, MPI_Datatype origin_datatype,
+            int target_rank, MPI_Aint target_disp, int target_count,
+            MPI_Datatype target_datatype, MPI_Win win);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
