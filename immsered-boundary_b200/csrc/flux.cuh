@@ -1,0 +1,148 @@
+// Face-flux arithmetic of the explicit step, shared by the FP64, exact-FP64
+// and mixed-precision kernel builds (the real type R is double or float).
+//
+// Each function restates one reference macro or member function for an
+// axis-aligned face of the reference's Cartesian cells, in the reference's
+// evaluation order.  With a unit-axis face normal the reference's dot
+// products (n . u, k_x alpha_4, ...) reduce exactly to picking the normal
+// (n) or tangential (t) velocity component, and every z term it evaluates in
+// its one-cell-thick slab is an exact zero, so dropping them changes no
+// result.  The frame velocity is zero (static reference frame).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace ibgpu {
+
+template <typename R>
+struct Gas {
+  R gama, Rg, Cv, Ma;
+  R gm1;      // gama - 1.0
+  R gamaRg;   // gama * Rg   (the reference's left-to-right "gama*Rg*T")
+};
+
+enum { LIM_VANLEER = 0, LIM_MINMOD = 1 };
+
+// Slopelimiter.H:14-20 (VanLeer, the reference's ALimiter) and :84-87 (minmod)
+template <int LIM, typename R>
+__device__ __forceinline__ R limiter_phi(R qr) {
+  if (LIM == LIM_MINMOD) return qr < R(1) ? qr : R(1);
+  return R(2) * qr / (R(1) + qr);
+}
+
+// comptqleft / SlopeCorrection_Left (NS_Solver.H:26-28, Slopelimiter.H:22-39)
+template <int LIM, typename R>
+__device__ __forceinline__ R muscl_left(R q_i, R qi, R qi1) {
+  R dqi = qi - q_i;
+  R dqii = qi1 - qi;
+  R qr = dqii / dqi;
+  if (fabs(qr) > R(1.0e10) || isnan(qr)) qr = (dqii > R(0)) ? R(1000000.0) : R(-1.0);
+  if (qr <= R(0)) qr = R(0);
+  R lv = limiter_phi<LIM>(qr);
+  return qi + R(0.5) * dqi * lv;
+}
+
+// comptqright / SlopeCorrection_Right (NS_Solver.H:22-24, Slopelimiter.H:41-58)
+template <int LIM, typename R>
+__device__ __forceinline__ R muscl_right(R q_i, R qi, R qi1) {
+  R dqi = qi - q_i;
+  R dqii = qi1 - qi;
+  R qr = dqi / dqii;
+  if (fabs(qr) > R(1.0e10) || isnan(qr)) qr = (dqi > R(0)) ? R(1000000.0) : R(-1.0);
+  if (qr <= R(0)) qr = R(0);
+  R lv = limiter_phi<LIM>(qr);
+  return qi - R(0.5) * dqii * lv;
+}
+
+// std::min / std::max as the reference calls them
+template <typename R>
+__device__ __forceinline__ R smin(R a, R b) { return (b < a) ? b : a; }
+template <typename R>
+__device__ __forceinline__ R smax(R a, R b) { return (a < b) ? b : a; }
+
+// Inviscid all-speed Roe flux of one face from the 4-cell stencil
+// [L2, L1 | R1, R2], each cell given as (rho, u_n, u_t, p):
+// FaceLeftRight + Get_T/Get_E (NS_Solver.H:30-44), Get_inv_flux
+// (FlowVariables.H:59-64), Roeaverage (NS_Solver.H:50-62), roe0c_coef with
+// ROE_ALLSPEED (:66-75) and ComptFaceFlux (:87-113).
+// Output (mass, momentum_n, momentum_t, energy), already multiplied by area.
+template <int LIM, typename R>
+__device__ __forceinline__ void roe_face_flux(const Gas<R> &g, R area,
+                                              R r0, R n0, R t0, R p0,
+                                              R r1, R n1, R t1, R p1,
+                                              R r2, R n2, R t2, R p2,
+                                              R r3, R n3, R t3, R p3,
+                                              R &f_mass, R &f_n, R &f_t, R &f_e) {
+  const R lroe = muscl_left<LIM>(r0, r1, r2);
+  const R rroe = muscl_right<LIM>(r1, r2, r3);
+  const R lun = muscl_left<LIM>(n0, n1, n2);
+  const R run = muscl_right<LIM>(n1, n2, n3);
+  const R lut = muscl_left<LIM>(t0, t1, t2);
+  const R rut = muscl_right<LIM>(t1, t2, t3);
+  const R lp = muscl_left<LIM>(p0, p1, p2);
+  const R rp = muscl_right<LIM>(p1, p2, p3);
+
+  const R lT = lp / (lroe * g.Rg);
+  const R le = g.Cv * lT + R(0.5) * (lun * lun + lut * lut);
+  const R rT = rp / (rroe * g.Rg);
+  const R re = g.Cv * rT + R(0.5) * (run * run + rut * rut);
+  const R lv = lun, rv = run;
+
+  const R droe = rroe - lroe;
+  const R dp = rp - lp;
+  const R dut = rut - lut;
+  const R dubar = rv - lv;
+
+  // Roeaverage
+  const R r2lroe = sqrt(rroe / lroe);
+  const R r2l0 = R(1) / (R(1) + r2lroe);
+  const R h_left = le + lp / lroe;
+  const R h_right = re + rp / rroe;
+  const R a_roe = sqrt(lroe * rroe);
+  const R a_un = (lun + run * r2lroe) * r2l0;
+  const R a_ut = (lut + rut * r2lroe) * r2l0;
+  const R a_h = (h_left + h_right * r2lroe) * r2l0;
+  const R a_c = sqrt(g.gm1 * (a_h - (a_un * a_un + a_ut * a_ut) / R(2)));
+  const R ubar = a_un;
+
+  // ComptFaceFlux
+  const R csquare = a_c * a_c;
+  const R namda3 = fabs(ubar);
+  const R coef12 = R(1) / (R(2) * csquare) * area;
+  const R roe0cxdubar = a_roe * a_c * dubar;
+  const R faceareaxabsubar = area * namda3;
+  const R halffacearea = R(0.5) * area;
+  const R alpha0 = faceareaxabsubar * (droe - dp / csquare);
+  // roe0c_coef (all-speed dissipation scaling)
+  const R T_a = (lT + rT) * R(0.5);
+  const R V_a = (lv + rv) * R(0.5);
+  const R Ma_a = fabs(V_a / sqrt(g.gamaRg * T_a));
+  const R f_Ma = smin(smax(Ma_a, g.Ma), R(1));
+  const R s0 = (R(1) - f_Ma) * (R(1) - f_Ma);
+  const R namda0 = sqrt(R(4) * a_c * a_c * f_Ma + s0 * ubar * ubar);
+  const R namda1 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar + namda0));
+  const R namda2 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar - namda0));
+  const R alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
+  const R alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
+  const R alpha3 = alpha0 + alpha1 + alpha2;
+  const R alpha4 = a_c * (alpha1 - alpha2);
+  const R alphat = faceareaxabsubar * (a_roe * dut);
+
+  // Get_inv_flux of both states
+  const R pl0 = lroe * lv, pl1 = lroe * lun * lv + lp, pl2 = lroe * lut * lv;
+  const R pl4 = (lp + le * lroe) * lv;
+  const R pr0 = rroe * rv, pr1 = rroe * run * rv + rp, pr2 = rroe * rut * rv;
+  const R pr4 = (rp + re * rroe) * rv;
+
+  f_mass = -alpha3;
+  f_n = -(a_un * alpha3 + alpha4);
+  f_t = -(a_ut * alpha3 + alphat);
+  f_e = -(a_h * alpha3 + ubar * alpha4 + a_ut * alphat - (csquare / g.gm1) * alpha0);
+  f_mass += (pl0 + pr0) * halffacearea;
+  f_n += (pl1 + pr1) * halffacearea;
+  f_t += (pl2 + pr2) * halffacearea;
+  f_e += (pl4 + pr4) * halffacearea;
+}
+
+}  // namespace ibgpu

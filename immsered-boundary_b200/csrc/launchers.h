@@ -1,0 +1,28 @@
+// Launchers of the kernels in kernels.cuh, one set per arithmetic build:
+// ibgpu::fast (kernels_fp64.cu: FP64 with contracted multiply-adds, and the
+// mixed FP32-flux path) and ibgpu::exact (kernels_exact.cu, -fmad=false).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.h"
+
+namespace ibgpu {
+
+#define IBGPU_DECLARE_LAUNCHERS(NS)                                                           \
+  namespace NS {                                                                              \
+  void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limiter,         \
+                    bool visc, bool final_stage, bool mixed, cudaStream_t st);                \
+  void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st);           \
+  void launch_scatter(const double *rows, const int32_t *cell_slot, const uint8_t *alias,     \
+                      int64_t n, double *const s0[kStateFields], int nsm, cudaStream_t st);   \
+  void launch_gather(double *rows, const int32_t *cell_slot, int64_t n,                       \
+                     double *const s0[kStateFields], int nsm, cudaStream_t st);               \
+  }
+
+IBGPU_DECLARE_LAUNCHERS(fast)
+IBGPU_DECLARE_LAUNCHERS(exact)
+
+#undef IBGPU_DECLARE_LAUNCHERS
+
+}  // namespace ibgpu

@@ -1,0 +1,90 @@
+// Device data layout shared by the host tile builder and the kernels.
+//
+// Each AMR level is stored as Morton-ordered 16 x 16 tiles of cell slots;
+// every field is a structure-of-arrays over slots, slot = tile * 256 +
+// ly * 16 + lx, so one tile of one field is 2 KB of contiguous FP64.  A slot
+// holds a leaf cell or a 2-D ghost cell of the reference mesh (domain ghost,
+// coarse/fine ghost); periodic/block ghosts are not stored, the tile
+// neighbour table wraps around instead.  Absent slots have flags == 0.
+#pragma once
+
+#include <stdint.h>
+
+namespace ibgpu {
+
+constexpr int kTile = 16;
+constexpr int kTileCells = kTile * kTile;
+constexpr int kMaxLevels = 16;
+
+// state field indices of the step-state buffer (FP64 SoA)
+enum { F_RHO = 0, F_U = 1, F_V = 2, F_P = 3, F_E = 4, F_T = 5, kStateFields = 6 };
+
+// slot flags (identical bit values to IBGPU_CELL_*)
+enum : uint8_t {
+  CF_PRESENT = 1,
+  CF_NORMAL = 2,
+  CF_UPDATE = 4,
+  CF_PRIM = 8,
+  CF_RESET = 16,
+  CF_RESNORM = 32,
+};
+
+struct LevelConst {
+  double dx, dy, dz;
+  double vol;      // dh0*dh1*dh2 (m_geom.v)
+  double area_x;   // dh1*dh2 (x-face area)
+  double area_y;   // dh2*dh0 (y-face area)
+  double area_z;   // dh0*dh1 (z-face area; enters the CFL sum)
+  double inv_dx, inv_dy;  // 1.0/dh (m_geom.keisa)
+  double step_num;
+  double cfl_vol;  // CFL * vol
+};
+
+struct CaseConst {
+  double gama, Rg, Cv, Ma, Re, qk, s_over_t, dt_ratio;
+  double gm1, gamaRg;
+  double initvar[7];
+  LevelConst lev[kMaxLevels];
+};
+
+// Device-side abort record.  The reference aborts at the first failing
+// check in its sequential order: the CFL pass (NS_Solver.cpp:253), then per
+// stage all density checks (UpdateConsVars) before all temperature checks
+// (ComptNewPrimVar).  err_key = (phase << 40) | (check << 32) | slot with
+// phase 0 for the CFL pass and 1 + k for stage k; the smallest key is the
+// reference's abort.
+enum : int { ERR_CFL_NEG_DT = 0, ERR_NEG_RHO = 1, ERR_NEG_T = 2 };
+
+struct DevDiag {
+  double dt;
+  unsigned long long cfl_bits;
+  unsigned long long res_bits[5];
+  unsigned long long err_key;  // ~0ull: no error
+};
+
+constexpr int kHaloStage = 2;
+
+struct StageArgs {
+  const int32_t *tile_nb;  // 9 neighbour tiles per tile, (oy+1)*3+(ox+1); -1 absent
+  const int32_t *tile_level;
+  const uint8_t *flags;
+  int tile_begin;
+  double *s0[kStateFields];  // step state rho u v p e T
+  const double *sin[4];      // stage input of varying cells (rho u v p)
+  double *sout[4];           // stage output (non-final stages)
+  const double *vsd;         // frozen viscous residual parts [8][nslots] or null
+  int64_t nslots;
+  double tp;                 // stage coefficient tp[k]
+  int stage;                 // k
+  DevDiag *diag;
+};
+
+struct CflArgs {
+  const int32_t *tile_level;
+  const uint8_t *flags;
+  const double *s0[kStateFields];
+  int64_t nslots;
+  DevDiag *diag;
+};
+
+}  // namespace ibgpu

@@ -1,0 +1,280 @@
+"""ctypes binding of the ibgpu C ABI (include/ibgpu.h) and a host-side
+driver that mirrors the reference solver's step interface.
+
+The reference (C++) drives one time step as
+``AMR::InterfaceExchange -> Body::IBConditions_Image -> NS_Solver::TimeMarching``
+(main.cpp:87-97); :class:`FlowSolver` offers the same step as
+``time_marching()`` over a device-resident state.  All numerics run in the
+CUDA library; this module only moves descriptors and host buffers.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libibgpu.so")
+
+ABI_VERSION = 1
+MAX_LEVELS = 16
+
+OK, E_ARG, E_CUDA, E_STATE, E_ABORT, E_NOMEM, E_TOPOLOGY = 0, -1, -2, -3, -4, -5, -6
+LIM_VANLEER, LIM_MINMOD = 0, 1
+FP64, FP64_EXACT, MIXED = 0, 1, 2
+CELL_PRESENT, CELL_NORMAL, CELL_UPDATE, CELL_PRIM, CELL_RESET, CELL_RESNORM, CELL_ALIAS = (
+    1, 2, 4, 8, 16, 32, 64)
+
+# every symbol include/ibgpu.h declares
+EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_layout_info",
+           "ibgpu_upload_state", "ibgpu_download_state", "ibgpu_step",
+           "ibgpu_set_kernel_timing", "ibgpu_kernel_times", "ibgpu_destroy", "ibgpu_errstr",
+           "ibgpu_last_error")
+
+
+class Case(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("gama", ctypes.c_double), ("Rg", ctypes.c_double), ("Cv", ctypes.c_double),
+        ("Cp", ctypes.c_double), ("Ma", ctypes.c_double), ("Re", ctypes.c_double),
+        ("Pr", ctypes.c_double), ("qk", ctypes.c_double), ("s_over_t", ctypes.c_double),
+        ("cfl", ctypes.c_double), ("dt_ratio", ctypes.c_double), ("dt_var_step", ctypes.c_int),
+        ("nstages", ctypes.c_int), ("tp", ctypes.c_double * 4),
+        ("limiter", ctypes.c_int), ("viscous", ctypes.c_int), ("precision", ctypes.c_int),
+        ("initvar", ctypes.c_double * 7),
+        ("nlevels", ctypes.c_int),
+        ("dh", (ctypes.c_double * 3) * MAX_LEVELS),
+        ("march_step", ctypes.c_int * MAX_LEVELS), ("march_left", ctypes.c_int * MAX_LEVELS),
+        ("step_num", ctypes.c_double * MAX_LEVELS),
+        ("domain_nx", ctypes.c_int), ("domain_ny", ctypes.c_int),
+        ("periodic_x", ctypes.c_int), ("periodic_y", ctypes.c_int),
+    ]
+
+
+class Cells(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("level", ctypes.POINTER(ctypes.c_int32)),
+                ("ix", ctypes.POINTER(ctypes.c_int32)), ("iy", ctypes.POINTER(ctypes.c_int32)),
+                ("flags", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("cfl_dt", ctypes.c_double),
+                ("res_max", ctypes.c_double * 5), ("abort_code", ctypes.c_int),
+                ("abort_level", ctypes.c_int), ("abort_ix", ctypes.c_int),
+                ("abort_iy", ctypes.c_int), ("cells_marched", ctypes.c_int64)]
+
+
+class IbgpuError(RuntimeError):
+    def __init__(self, code: int, what: str, detail: str = "", diag: Diag | None = None):
+        self.code = code
+        self.diag = diag
+        self.abort_code = diag.abort_code if diag is not None else 0
+        msg = f"{what}: {lib().ibgpu_errstr(code).decode()} ({code})"
+        if detail:
+            msg += f" [{detail}]"
+        if diag is not None and diag.abort_code:
+            msg += (f" abort code {diag.abort_code} at level {diag.abort_level} "
+                    f"cell ({diag.abort_ix},{diag.abort_iy})")
+        super().__init__(msg)
+
+
+_lib = None
+
+
+def lib(path: str | None = None):
+    """Load libibgpu.so (fails loudly when the CUDA library is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"ibgpu CUDA library not built: {p} is missing "
+                          "(run immsered-boundary_b200/build_lib.py)")
+    L = ctypes.CDLL(p)
+    vp = ctypes.c_void_p
+    L.ibgpu_create.argtypes = [ctypes.POINTER(Case), ctypes.POINTER(vp)]
+    L.ibgpu_set_stream.argtypes = [vp, vp]
+    L.ibgpu_upload_topology.argtypes = [vp, ctypes.POINTER(Cells)]
+    L.ibgpu_layout_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_upload_state.argtypes = [vp, vp]
+    L.ibgpu_download_state.argtypes = [vp, vp]
+    L.ibgpu_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Diag)]
+    L.ibgpu_set_kernel_timing.argtypes = [vp, ctypes.c_int]
+    L.ibgpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_destroy.argtypes = [vp]
+    L.ibgpu_destroy.restype = None
+    L.ibgpu_errstr.argtypes = [ctypes.c_int]
+    L.ibgpu_errstr.restype = ctypes.c_char_p
+    L.ibgpu_last_error.argtypes = []
+    L.ibgpu_last_error.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("ibgpu_destroy", "ibgpu_errstr", "ibgpu_last_error"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str, diag: Diag | None = None):
+    if rc != OK:
+        raise IbgpuError(rc, what, lib().ibgpu_last_error().decode(), diag)
+
+
+def make_case(params: dict) -> Case:
+    """Fill an ibgpu_case from a parameter dict (same keys as the fields)."""
+    c = Case()
+    c.abi_version = ABI_VERSION
+    for k in ("gama", "Rg", "Cv", "Cp", "Ma", "Re", "Pr", "qk", "s_over_t", "cfl", "dt_ratio"):
+        setattr(c, k, float(params.get(k, 0.0)))
+    c.dt_var_step = int(params.get("dt_var_step", 1))
+    c.nstages = int(params["nstages"])
+    for i, v in enumerate(params["tp"]):
+        c.tp[i] = float(v)
+    c.limiter = int(params.get("limiter", LIM_VANLEER))
+    c.viscous = int(params.get("viscous", 0))
+    c.precision = int(params.get("precision", FP64))
+    for i, v in enumerate(params["initvar"]):
+        c.initvar[i] = float(v)
+    nl = int(params["nlevels"])
+    c.nlevels = nl
+    for l in range(nl):
+        for k in range(3):
+            c.dh[l][k] = float(params["dh"][l][k])
+        c.march_step[l] = int(params["march_step"][l])
+        c.march_left[l] = int(params["march_left"][l])
+        c.step_num[l] = float(params["step_num"][l])
+    c.domain_nx = int(params["domain_nx"])
+    c.domain_ny = int(params["domain_ny"])
+    c.periodic_x = int(params.get("periodic_x", 0))
+    c.periodic_y = int(params.get("periodic_y", 0))
+    return c
+
+
+class FlowSolver:
+    """GPU time step behind the reference's NS_Solver step interface.
+
+    ``upload_topology`` takes the canonical cell list (level, ix, iy, flags),
+    ``init_flow``/``download`` move FlowVariables rows (roe,u,v,w,p,T,e), and
+    ``time_marching(ts)`` runs one full step (NS_Solver::TimeMarching plus the
+    ghost fills the reference runs before it).
+    """
+
+    def __init__(self, params: dict):
+        self._case = make_case(params)
+        self._ctx = ctypes.c_void_p()
+        _check(lib().ibgpu_create(ctypes.byref(self._case), ctypes.byref(self._ctx)), "ibgpu_create")
+        self.params = dict(params)
+        self.dt = float(params.get("dt0", 1.0))
+        self.ncells = 0
+        self._keep = []
+        self.init_res = None
+
+    def close(self):
+        if self._ctx:
+            lib().ibgpu_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        _check(lib().ibgpu_set_stream(self._ctx, ctypes.c_void_p(stream_handle or 0)), "ibgpu_set_stream")
+
+    def upload_topology(self, level, ix, iy, flags):
+        lv = np.ascontiguousarray(level, np.int32)
+        x = np.ascontiguousarray(ix, np.int32)
+        y = np.ascontiguousarray(iy, np.int32)
+        f = np.ascontiguousarray(flags, np.uint8)
+        cells = Cells(len(lv), lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                      x.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                      y.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                      f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        _check(lib().ibgpu_upload_topology(self._ctx, ctypes.byref(cells)), "ibgpu_upload_topology")
+        self.ncells = len(lv)
+
+    def layout_info(self):
+        ns, nt = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().ibgpu_layout_info(self._ctx, ctypes.byref(ns), ctypes.byref(nt)), "ibgpu_layout_info")
+        return ns.value, nt.value
+
+    def init_flow(self, prim_rows):
+        """Upload FlowVariables rows (n, 7); also accepts a host pointer (int)."""
+        if isinstance(prim_rows, int):
+            _check(lib().ibgpu_upload_state(self._ctx, ctypes.c_void_p(prim_rows)), "ibgpu_upload_state")
+            return
+        a = np.ascontiguousarray(prim_rows, np.float64)
+        assert a.shape == (self.ncells, 7)
+        _check(lib().ibgpu_upload_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p)), "ibgpu_upload_state")
+
+    def download(self, out=None):
+        if isinstance(out, int):
+            _check(lib().ibgpu_download_state(self._ctx, ctypes.c_void_p(out)), "ibgpu_download_state")
+            return None
+        a = np.empty((self.ncells, 7), np.float64) if out is None else out
+        _check(lib().ibgpu_download_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p)), "ibgpu_download_state")
+        return a
+
+    def time_marching(self, ts: int) -> Diag:
+        d = Diag()
+        dt = ctypes.c_double(self.dt)
+        rc = lib().ibgpu_step(self._ctx, int(ts), ctypes.byref(dt), ctypes.byref(d))
+        if rc != OK:
+            raise IbgpuError(rc, "ibgpu_step", lib().ibgpu_last_error().decode(), d)
+        self.dt = dt.value
+        return d
+
+    def set_kernel_timing(self, on: bool):
+        _check(lib().ibgpu_set_kernel_timing(self._ctx, int(bool(on))), "ibgpu_set_kernel_timing")
+
+    def kernel_times(self):
+        ms = (ctypes.c_double * 3)()
+        n = (ctypes.c_int64 * 3)()
+        _check(lib().ibgpu_kernel_times(self._ctx, ms, n), "ibgpu_kernel_times")
+        return list(ms), list(n)
+
+    def res_normalised(self, diag: Diag, ts: int):
+        """ResinDomain's printed residual (NS_Solver.H:331-345): max-norm
+        divided by the step-0 value, z component zero in 2-D."""
+        r = list(diag.res_max)
+        if ts == 0 or self.init_res is None:
+            self.init_res = r
+        out = [r[i] / self.init_res[i] if self.init_res[i] else float("nan") for i in range(5)]
+        out[3] = 0.0
+        return out
+
+
+# box kinds of the reference mesh as the adapters report them
+BOX_NORMAL, BOX_DOMAIN_GHOST, BOX_BLOCK_GHOST, BOX_OTHER_GHOST = 0, 1, 2, 3
+
+
+def cell_flags_from_boxes(kind, solid, infect, signdis, body_level: bool) -> np.ndarray:
+    """Per-cell IBGPU_CELL_* flags from the reference's box attributes.
+
+    Encodes which branch of UpdateConsVars / ComptNewPrimVar / ResinDomain
+    (NS_Solver.cpp:3-194, 844-985; NS_Solver.H:264-378) a box takes: on the
+    finest level of a run with bodies only non-solid, non-immersed-boundary
+    boxes are updated, elsewhere every leaf box is; a leaf box inside a body
+    (signed distance <= 0) is reset to the free stream instead of recovering
+    its primitives.  Block (periodic) ghosts become aliases.
+    """
+    kind = np.asarray(kind)
+    fl = np.full(kind.shape, CELL_PRESENT, np.uint8)
+    normal = kind == BOX_NORMAL
+    fl[normal] |= CELL_NORMAL
+    pos = np.asarray(signdis) > 0.0
+    if body_level:
+        free = np.asarray(infect) == -1
+        upd = normal & free & (np.asarray(solid) == 0)
+        fl[upd] |= CELL_UPDATE
+        fl[upd & pos] |= CELL_PRIM
+        fl[normal & free & ~pos] |= CELL_RESET
+        fl[normal & free & pos] |= CELL_RESNORM
+    else:
+        fl[normal] |= CELL_UPDATE | CELL_RESNORM
+        fl[normal & pos] |= CELL_PRIM
+        fl[normal & ~pos] |= CELL_RESET
+    fl[kind == BOX_BLOCK_GHOST] |= CELL_ALIAS
+    return fl

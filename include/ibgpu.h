@@ -1,0 +1,164 @@
+/*
+ * ibgpu — C ABI of the B200 explicit time step for the cell-based AMR
+ * compressible Navier-Stokes solver (2-D, immersed bodies).
+ *
+ * The GPU step replaces, for one time step of the reference solver:
+ *   NS_Solver::TimeMarching       (NS_Solver.H:657-702)
+ *   AMR::InterfaceExchange         (AMRInterface.cpp:3-35)
+ *   the per-cell part of Body::IBConditions_Image (Body.cpp:1361-1496)
+ * called from the reference main loop (main.cpp:87, 89, 97).  The host keeps
+ * the mesh (topology is built and regridded by the reference's Mesh/AMR
+ * classes on the host); the device owns the flow state between regrids.
+ *
+ * Conventions
+ *   - Plain C types only; every pointer is host memory unless a name says
+ *     otherwise; sizes are element counts.
+ *   - Every call returns IBGPU_OK (0) or a negative IBGPU_E* code; the
+ *     solver's own abort conditions are reported as the reference's abort
+ *     code (e.g. 523 for negative density) through ibgpu_diag.abort_code and
+ *     the return value IBGPU_E_ABORT.  The library never exits the process.
+ *   - One context = one CUDA stream; a context is not re-entrant.
+ *   - Primitive state rows are the reference's FlowVariables layout
+ *     (FlowVariables.H:235-334): roe, u, v, w, p, T, e  (7 doubles per cell).
+ */
+#ifndef IBGPU_H
+#define IBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IBGPU_ABI_VERSION 1
+#define IBGPU_MAX_LEVELS 16
+
+/* return codes */
+#define IBGPU_OK 0
+#define IBGPU_E_ARG (-1)       /* invalid argument / inconsistent input        */
+#define IBGPU_E_CUDA (-2)      /* CUDA runtime error (see ibgpu_last_error)     */
+#define IBGPU_E_STATE (-3)     /* call order (e.g. step before upload)         */
+#define IBGPU_E_ABORT (-4)     /* solver abort condition, see ibgpu_diag        */
+#define IBGPU_E_NOMEM (-5)     /* device allocation failed                     */
+#define IBGPU_E_TOPOLOGY (-6)  /* cell list cannot be laid out (e.g. periodic
+                                  extent not a multiple of the tile edge)      */
+
+/* limiter (Slopelimiter.H): VanLeer is the reference's active ALimiter */
+#define IBGPU_LIM_VANLEER 0
+#define IBGPU_LIM_MINMOD 1
+
+/* arithmetic of the flux/limiter/viscous kernels */
+#define IBGPU_FP64 0        /* FP64 throughout (contracted multiply-adds)       */
+#define IBGPU_FP64_EXACT 1  /* FP64, no contraction: reproduces the reference
+                               operation by operation                            */
+#define IBGPU_MIXED 2       /* FP32 flux/limiter/viscous; FP64 accumulation of
+                               conserved variables, pressure recovery, dt,
+                               residual and forces                               */
+
+/* per-cell flags of the canonical cell list (same meaning as the reference
+ * code paths they select; see ibgpu_cells) */
+#define IBGPU_CELL_PRESENT 1  /* a box of the level exists at (ix, iy)          */
+#define IBGPU_CELL_NORMAL 2   /* leaf cell (the level's normal range [0,size))  */
+#define IBGPU_CELL_UPDATE 4   /* UpdateConsVars computes cv_new (rho<0 check)   */
+#define IBGPU_CELL_PRIM 8     /* ComptNewPrimVar: prim <- Get_Prim_Vars(cv_new)*/
+#define IBGPU_CELL_RESET 16   /* ComptNewPrimVar: prim <- initvar              */
+#define IBGPU_CELL_RESNORM 32 /* counted by ResinDomain                         */
+#define IBGPU_CELL_ALIAS 64   /* periodic/block ghost: a copy of the cell at the
+                                 wrapped position (Mesh::DataExchange); it gets
+                                 no storage of its own                         */
+
+typedef struct ibgpu_case {
+  int abi_version; /* IBGPU_ABI_VERSION */
+  /* non-dimensional gas constants (FlowConstants.cpp:5-44) */
+  double gama, Rg, Cv, Cp, Ma, Re, Pr, qk, s_over_t;
+  /* time step control (NS_Solver.cpp:196-280; case globals) */
+  double cfl, dt_ratio;
+  int dt_var_step;
+  /* multistage scheme U^(k) = U^n + tp[k] dt R(U^(k-1)) (NS_Solver.H:200-231) */
+  int nstages;
+  double tp[4];
+  int limiter;   /* IBGPU_LIM_* */
+  int viscous;   /* 1: ComptViscousStress terms (frozen per step)      */
+  int precision; /* IBGPU_FP64 / IBGPU_FP64_EXACT / IBGPU_MIXED        */
+  double initvar[7];
+  /* levels (AMRSpaceTime.H, mpiparams.cpp:134-212) */
+  int nlevels;
+  double dh[IBGPU_MAX_LEVELS][3];
+  int march_step[IBGPU_MAX_LEVELS], march_left[IBGPU_MAX_LEVELS];
+  double step_num[IBGPU_MAX_LEVELS];
+  /* domain: level-0 cell counts and periodicity; level l spans n*2^l */
+  int domain_nx, domain_ny;
+  int periodic_x, periodic_y;
+} ibgpu_case;
+
+/* Canonical cell list: one row per box of the z = 0 plane of each level
+ * (normal cells and 2-D ghosts), keyed by (level, ix, iy).  Replaces the
+ * reference's per-level AoS arrays Meshlevel::m_box / m_data
+ * (Meshlevel.H:688-872, Box.H:113-300) as the device's input. */
+typedef struct ibgpu_cells {
+  int64_t n;
+  const int32_t *level;
+  const int32_t *ix;
+  const int32_t *iy;
+  const uint8_t *flags; /* IBGPU_CELL_* */
+} ibgpu_cells;
+
+typedef struct ibgpu_diag {
+  double dt;          /* dt used by this step                                */
+  double cfl_dt;      /* CFL time step (NS_Solver.cpp:262), when evaluated   */
+  double res_max[5];  /* ResinDomain max-norm of the residual (unnormalised) */
+  int abort_code;     /* reference abort code, 0 if none                     */
+  int abort_level, abort_ix, abort_iy;
+  int64_t cells_marched; /* leaf cells of the levels that marched           */
+} ibgpu_diag;
+
+typedef struct ibgpu_ctx ibgpu_ctx;
+
+/* Create a context on the current CUDA device.  Replaces the NS_Solver
+ * constructor (NS_Solver.H:192-236) plus the case globals it reads. */
+int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out);
+
+/* Run the context's work on an existing CUDA stream (cudaStream_t passed as
+ * a pointer); NULL restores the context's own stream. */
+int ibgpu_set_stream(ibgpu_ctx *ctx, void *stream);
+
+/* Upload the mesh as a cell list; lays the levels out as Morton-ordered
+ * 16x16 tiles.  Call again after every regrid (AMR::PerformAdaptive). */
+int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells);
+
+/* Number of device cell slots and tiles after the last topology upload. */
+int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);
+
+/* State in cell-list order, 7 doubles per cell (FlowVariables layout).
+ * Upload replaces NS_Solver::InitFlow (NS_Solver.H:432-446) / a restart;
+ * alias rows are ignored on upload and filled from their source on
+ * download. */
+int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim);
+int ibgpu_download_state(ibgpu_ctx *ctx, double *prim);
+
+/* One full time step at step index ts (main.cpp:87-97): C/F ghost fill,
+ * immersed-body ghost fill, CFL dt every dt_var_step steps, U^n, domain
+ * ghosts, frozen viscous flux, nstages stages, residual max-norm.
+ * *dt is the current dt on entry and the dt used on return (dt =
+ * min(CFL_dt, dt*dt_ratio), NS_Solver.cpp:263).  diag may be NULL. */
+int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag);
+
+/* Event timing of the dominant kernels, accumulated while enabled:
+ * kernel 0 = stage update (flux + residual + update + prim recovery),
+ * 1 = viscous flux, 2 = CFL dt.  ms_out[k] total milliseconds,
+ * launches_out[k] launch count. */
+int ibgpu_set_kernel_timing(ibgpu_ctx *ctx, int enable);
+int ibgpu_kernel_times(const ibgpu_ctx *ctx, double ms_out[3], int64_t launches_out[3]);
+
+void ibgpu_destroy(ibgpu_ctx *ctx);
+
+const char *ibgpu_errstr(int code);
+/* Last CUDA error string seen by this thread's most recent failing call. */
+const char *ibgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -284,6 +284,7 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
   double **vx = (double **)calloc((size_t)nlev, sizeof(double *));
   double **vy = (double **)calloc((size_t)nlev, sizeof(double *));
   double **src = (double **)calloc((size_t)nlev, sizeof(double *));
+  double **cvn = (double **)calloc((size_t)nlev, sizeof(double *));
   for (int l = 0; l < nlev; ++l) {
     size_t n = (size_t)lev[l].nx * (size_t)lev[l].ny;
     un[l] = (double *)calloc(4 * n, sizeof(double));
@@ -292,6 +293,7 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
     vx[l] = (double *)calloc(4 * n, sizeof(double));
     vy[l] = (double *)calloc(4 * n, sizeof(double));
     src[l] = (double *)calloc(4 * n, sizeof(double));
+    cvn[l] = (double *)calloc(4 * n, sizeof(double));
   }
 
   /* ComptOldConsVar (NS_Solver.H:392-424) */
@@ -364,7 +366,8 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
         }
       }
     }
-    /* UpdateConsVars (NS_Solver.cpp:844-985) + ComptNewPrimVar (:3-194) */
+    /* UpdateConsVars (NS_Solver.cpp:844-985): every level's cv_new and its
+     * density check first (abort 523, or 611 on the body level) ... */
     double dt0 = P->tp[k] * *dt;
     for (int l = 0; l < nlev && !rc; ++l) {
       ibo_level *L = &lev[l];
@@ -373,13 +376,20 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
       double v = L->dx * L->dy * L->dz;
       for (int s = 0; s < L->nx * L->ny; ++s) {
         uint8_t fl = L->flags[s];
+        if (!(fl & IBO_NORMAL) || !(fl & IBO_UPDATE)) continue;
+        for (int c = 0; c < 4; ++c) cvn[l][4 * s + c] = un[l][4 * s + c] + src[l][4 * s + c] * level_ts / v;
+        if (cvn[l][4 * s] < 0.0) { rc = (l == P->body_level) ? 611 : 523; break; }
+      }
+    }
+    /* ... then ComptNewPrimVar (NS_Solver.cpp:3-194) and its T check (37) */
+    for (int l = 0; l < nlev && !rc; ++l) {
+      ibo_level *L = &lev[l];
+      if (!marches(L, ts)) continue;
+      for (int s = 0; s < L->nx * L->ny; ++s) {
+        uint8_t fl = L->flags[s];
         if (!(fl & IBO_NORMAL)) continue;
-        double cv[4];
-        if (fl & IBO_UPDATE) {
-          for (int c = 0; c < 4; ++c) cv[c] = un[l][4 * s + c] + src[l][4 * s + c] * level_ts / v;
-          if (cv[0] < 0.0) { rc = 523; break; }
-        }
         if ((fl & IBO_PRIM) && (fl & IBO_UPDATE)) {
+          const double *cv = &cvn[l][4 * s];
           double r = cv[0];
           double u = cv[1] / cv[0];
           double vv = cv[2] / cv[0];
@@ -395,6 +405,8 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
           L->q[Q_T][s] = T;
         } else if (fl & IBO_RESET) {
           for (int c = 0; c < 7; ++c) L->q[c][s] = P->initvar[c];
+        } else {
+          continue;
         }
         if (L->q[Q_T][s] < 0.0) { rc = 37; break; }
       }
@@ -424,8 +436,8 @@ int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
   }
 
   for (int l = 0; l < nlev; ++l) {
-    free(un[l]); free(fx[l]); free(fy[l]); free(vx[l]); free(vy[l]); free(src[l]);
+    free(un[l]); free(fx[l]); free(fy[l]); free(vx[l]); free(vy[l]); free(src[l]); free(cvn[l]);
   }
-  free(un); free(fx); free(fy); free(vx); free(vy); free(src);
+  free(un); free(fx); free(fy); free(vx); free(vy); free(src); free(cvn);
   return rc;
 }

@@ -40,6 +40,7 @@ typedef struct ibo_params {
   int limiter;
   int viscous;
   int dt_var_step;
+  int body_level;    /* finest level of a run with bodies, or -1 */
 } ibo_params;
 
 typedef struct ibo_level {
@@ -59,7 +60,8 @@ typedef struct ibo_level {
  * (every dt_var_step steps), U^n, viscous flux (frozen), S stages of
  * flux -> residual -> update -> prim recovery with an exchange between
  * stages, residual max-norm.  Returns 0, or the reference's abort code
- * (523 rho < 0, 37 T < 0, 424 dt < 0, 268 NaN residual). */
+ * (523 rho < 0, 611 rho < 0 on the body level, 37 T < 0, 424 dt < 0,
+ * 268 NaN residual), checked in the reference's order. */
 int ibo_step(const ibo_params *P, ibo_level *lev, int nlev, int ts, double *dt,
              double *cfl_dt, double res_max[5]);
 

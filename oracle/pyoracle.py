@@ -46,7 +46,7 @@ class _Params(ctypes.Structure):
                 ("dt_ratio", ctypes.c_double), ("tp", ctypes.c_double * 4),
                 ("initvar", ctypes.c_double * 7), ("nstages", ctypes.c_int),
                 ("limiter", ctypes.c_int), ("viscous", ctypes.c_int),
-                ("dt_var_step", ctypes.c_int)]
+                ("dt_var_step", ctypes.c_int), ("body_level", ctypes.c_int)]
 
 
 class _Level(ctypes.Structure):
@@ -187,6 +187,7 @@ def step(P: dict, lv: OracleLevels, ts: int, dt: float):
     cp.limiter = int(P["limiter"])
     cp.viscous = int(P["viscous"])
     cp.dt_var_step = int(P["dt_var_step"])
+    cp.body_level = int(P.get("body_level", -1))
     arr = (_Level * len(lv.levels))()
     keep = []
     for i, L in enumerate(lv.levels):

@@ -199,6 +199,7 @@ int main(int argc, char **argv) {
   else flowsolver.InitFlow();
 
   const int nsteps = env_int("IB_STEPS", 5);
+  const int timed_from = env_int("IB_TIMED_FROM", 0);  // steps before this are warm-up
   const int every = env_int("IB_DUMP_EVERY", 1);
   const bool forces_on = env_int("IB_FORCES", 0) != 0;
   const char *prefix = std::getenv("IB_DUMP");
@@ -225,8 +226,10 @@ int main(int argc, char **argv) {
     ++ts;
     t += dt;
     double t1 = MPI_Wtime();
-    loop_time += t1 - t0;
-    cell_updates += marching_cells;
+    if (s >= timed_from) {
+      loop_time += t1 - t0;
+      cell_updates += marching_cells;
+    }
     forces.clear();
     if (forces_on) {
       for (size_t b = 0; b < sphere.size(); ++b) {
@@ -242,7 +245,7 @@ int main(int argc, char **argv) {
   }
   std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
               "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g}\n",
-              nsteps, loop_time, cell_updates,
+              nsteps - timed_from, loop_time, cell_updates,
               loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt);
   MPI_Finalize();
   return 0;

@@ -1,0 +1,86 @@
+"""Regenerate the golden fixtures from the reference solver itself.
+
+Runs the reference-solver oracle binaries (built from the reference's own
+sources by ``make -C oracle``) on small cases and packs their state dumps
+into compressed .npz files next to this script.  The fixtures pin both the
+C restatement of the step (oracle/ib_oracle.c) and the GPU path.
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture holds the box list of the z = 0 plane (level, ix, iy, kind,
+ptype, solid, infect, signdis), the case constants, and the primitive state
+(roe, u, v, w, p, T, e) plus scalars (t, dt, CFL_dt, ts, ...) of every dumped
+step.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+# name -> (binary, environment, number of steps)
+CASES = {
+    "vortex_vanleer_s4_n32": ("ref_vortex_vanleer", {"IB_NX": "32", "IB_STAGES": "4"}, 4),
+    "vortex_minmod_s3_n32": ("ref_vortex_minmod", {"IB_NX": "32", "IB_STAGES": "3"}, 3),
+}
+
+STATIC = ("level", "ix", "iy", "kind", "ptype", "solid", "infect", "signdis")
+
+
+def run_case(name: str, binary: str, env: dict, steps: int) -> str:
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        e = dict(os.environ)
+        e.update(env)
+        e["IB_STEPS"] = str(steps)
+        e["IB_DUMP"] = os.path.join(work, "d")
+        subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
+                       stdout=subprocess.DEVNULL)
+        snaps = [pyoracle.read_dump(os.path.join(work, f"d_{k:06d}.bin")) for k in range(steps + 1)]
+        out = {k: snaps[0][k] for k in STATIC}
+        for k in ("dh", "schedule", "initvar", "domain"):
+            out[k] = snaps[0][k]
+        for s in snaps[1:]:
+            for k in STATIC:
+                if not np.array_equal(s[k], snaps[0][k]):
+                    raise RuntimeError(f"{name}: topology changed between dumps ({k})")
+        out["prim"] = np.stack([s["prim"].reshape(-1, 7) for s in snaps])
+        out["scalars"] = np.stack([s["scalars"] for s in snaps])
+        forces = [s["forces"] for s in snaps]
+        out["forces"] = np.stack(forces) if all(len(f) == len(forces[0]) for f in forces) else np.zeros((0,))
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        return path
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def load(name: str) -> dict:
+    with np.load(os.path.join(HERE, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def snapshot(g: dict, k: int) -> dict:
+    """Dump-shaped dict of snapshot k (what pyoracle.OracleLevels expects)."""
+    d = {key: g[key] for key in STATIC + ("dh", "schedule", "initvar", "domain")}
+    d["prim"] = g["prim"][k].ravel()
+    d["scalars"] = g["scalars"][k]
+    return d
+
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        b, env, steps = CASES[n]
+        print(run_case(n, b, env, steps))
