@@ -164,6 +164,7 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
   k.dt_ratio = cs->dt_ratio;
   k.gm1 = cs->gama - 1.0;
   k.gamaRg = cs->gama * cs->Rg;
+  k.inv_Rg = 1.0 / cs->Rg;
   for (int i = 0; i < 7; ++i) k.initvar[i] = cs->initvar[i];
   for (int l = 0; l < cs->nlevels; ++l) {
     LevelConst &L = k.lev[l];
@@ -171,6 +172,7 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
     L.dy = cs->dh[l][1];
     L.dz = cs->dh[l][2];
     L.vol = cs->dh[l][0] * cs->dh[l][1] * cs->dh[l][2];
+    L.inv_vol = 1.0 / L.vol;
     L.area_x = cs->dh[l][1] * cs->dh[l][2];
     L.area_y = cs->dh[l][2] * cs->dh[l][0];
     L.area_z = cs->dh[l][0] * cs->dh[l][1];

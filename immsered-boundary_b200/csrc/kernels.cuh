@@ -232,6 +232,227 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
   }
 }
 
+// Fast build of the stage (FP64 with FastMath divisions/roots, or FP32 flux
+// arithmetic for the mixed mode): per-cell limited slopes computed once and
+// shared by the cell's two faces in each direction, divisions replaced by
+// reciprocals.  Faces whose outer stencil cell is missing use the
+// reference's one-sided reconstruction (NS_Solver.H:743-750).  The residual,
+// update and primitive recovery run in FP64 in every mode.
+template <typename R, int LIM, bool VISC, bool FINAL>
+__global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
+  constexpr int kSlopeX = kTile * (kTile + 2);  // x-slopes: rows 0..15, cols -1..16
+  constexpr int kSlopeY = (kTile + 2) * kTile;  // y-slopes: rows -1..16, cols 0..15
+  __shared__ R sq[4][kReg * kReg];
+  __shared__ uint8_t sfl[kReg * kReg];
+  __shared__ R slx[4][kSlopeX];
+  __shared__ R sly[4][kSlopeY];
+  __shared__ R fx[4][kXFaces];
+  __shared__ R fy[4][kYFaces];
+
+  const int tid = threadIdx.x;
+  const int tile = a.tile_begin + blockIdx.x;
+  const int lvl = a.tile_level[tile];
+  const LevelConst &L = cc.lev[lvl];
+
+  for (int r = tid; r < kReg * kReg; r += kTileCells) {
+    int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
+    int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
+    int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
+    uint8_t f = 0;
+    R q0 = R(0), q1 = R(0), q2 = R(0), q3 = R(0);
+    if (!(ox && oy)) {
+      int nb = a.tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
+      if (nb >= 0) {
+        int64_t s = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
+        f = a.flags[s];
+        if (f & CF_PRESENT) {
+          const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
+          q0 = (R)(varying ? a.sin[0] : a.s0[F_RHO])[s];
+          q1 = (R)(varying ? a.sin[1] : a.s0[F_U])[s];
+          q2 = (R)(varying ? a.sin[2] : a.s0[F_V])[s];
+          q3 = (R)(varying ? a.sin[3] : a.s0[F_P])[s];
+        }
+      }
+    }
+    sfl[r] = f;
+    sq[0][r] = q0;
+    sq[1][r] = q1;
+    sq[2][r] = q2;
+    sq[3][r] = q3;
+  }
+  __syncthreads();
+
+  // ---- per-cell limited slopes (valid where both neighbours exist)
+  for (int w = tid; w < kSlopeX + kSlopeY; w += kTileCells) {
+    int rc, step;
+    if (w < kSlopeX) {
+      int row = w / (kTile + 2), col = w % (kTile + 2) - 1;
+      rc = (row + kHalo) * kReg + (col + kHalo);
+      step = 1;
+    } else {
+      int v = w - kSlopeX;
+      int row = v / kTile - 1, col = v % kTile;
+      rc = (row + kHalo) * kReg + (col + kHalo);
+      step = kReg;
+    }
+    R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
+    if ((sfl[rc - step] & CF_PRESENT) && (sfl[rc + step] & CF_PRESENT)) {
+      s0 = limited_slope<LIM>(sq[0][rc] - sq[0][rc - step], sq[0][rc + step] - sq[0][rc]);
+      s1 = limited_slope<LIM>(sq[1][rc] - sq[1][rc - step], sq[1][rc + step] - sq[1][rc]);
+      s2 = limited_slope<LIM>(sq[2][rc] - sq[2][rc - step], sq[2][rc + step] - sq[2][rc]);
+      s3 = limited_slope<LIM>(sq[3][rc] - sq[3][rc - step], sq[3][rc + step] - sq[3][rc]);
+    }
+    if (w < kSlopeX) {
+      slx[0][w] = s0; slx[1][w] = s1; slx[2][w] = s2; slx[3][w] = s3;
+    } else {
+      int v = w - kSlopeX;
+      sly[0][v] = s0; sly[1][v] = s1; sly[2][v] = s2; sly[3][v] = s3;
+    }
+  }
+  __syncthreads();
+
+  Gas<R> g;
+  g.gama = (R)cc.gama;
+  g.Rg = (R)cc.Rg;
+  g.Cv = (R)cc.Cv;
+  g.Ma = (R)cc.Ma;
+  g.gm1 = (R)cc.gm1;
+  g.gamaRg = (R)cc.gamaRg;
+  g.inv_Rg = (R)(1.0 / cc.Rg);
+  g.inv_gm1 = (R)(1.0 / cc.gm1);
+
+  // ---- face fluxes
+  for (int w = tid; w < kXFaces + kYFaces; w += kTileCells) {
+    const bool xdir = w < kXFaces;
+    int rL1, rR1, step, sL, sR;  // sL, sR: slope slots of L1 and R1
+    const R(*sl)[kSlopeX];
+    if (xdir) {
+      int j = w / (kTile + 1), i = w % (kTile + 1);
+      rR1 = (j + kHalo) * kReg + (i + kHalo);
+      rL1 = rR1 - 1;
+      step = 1;
+      sR = j * (kTile + 2) + (i + 1);
+      sL = sR - 1;
+      sl = slx;
+    } else {
+      int v = w - kXFaces;
+      int j = v / kTile, i = v % kTile;
+      rR1 = (j + kHalo) * kReg + (i + kHalo);
+      rL1 = rR1 - kReg;
+      step = kReg;
+      sR = (j + 1) * kTile + i;
+      sL = sR - kTile;
+      sl = sly;
+    }
+    const uint8_t fL = sfl[rL1], fR = sfl[rR1];
+    R fm = R(0), fn = R(0), ft = R(0), fe = R(0);
+    if ((fL & CF_PRESENT) && (fR & CF_PRESENT) && ((fL | fR) & CF_NORMAL)) {
+      const int rL2 = rL1 - step, rR2 = rR1 + step;
+      const bool hasL2 = (sfl[rL2] & CF_PRESENT) != 0;
+      const bool hasR2 = (sfl[rR2] & CF_PRESENT) != 0;
+      R ls[4], rs[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        ls[c] = hasL2 ? sq[c][rL1] + sl[c][sL]
+                      : muscl_left_fast<LIM>(sq[c][rR2], sq[c][rL1], sq[c][rR1]);
+        rs[c] = hasR2 ? sq[c][rR1] - sl[c][sR]
+                      : muscl_right_fast<LIM>(sq[c][rL1], sq[c][rR1], sq[c][rL2]);
+      }
+      const int cn = xdir ? 1 : 2, ct = xdir ? 2 : 1;
+      const R area = (R)(xdir ? L.area_x : L.area_y);
+      roe_flux_states<R>(g, area, ls[0], ls[cn], ls[ct], ls[3], rs[0], rs[cn], rs[ct], rs[3],
+                         fm, fn, ft, fe);
+    }
+    if (xdir) {
+      fx[0][w] = fm; fx[1][w] = fn; fx[2][w] = ft; fx[3][w] = fe;
+    } else {
+      int v = w - kXFaces;
+      fy[0][v] = fm; fy[1][v] = ft; fy[2][v] = fn; fy[3][v] = fe;
+    }
+  }
+  __syncthreads();
+
+  // ---- residual, update, primitive recovery (FP64)
+  const int lx = tid % kTile, ly = tid / kTile;
+  const int64_t slot = (int64_t)tile * kTileCells + tid;
+  const uint8_t fl = sfl[(ly + kHalo) * kReg + (lx + kHalo)];
+  unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
+  if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
+    const int xlo = ly * (kTile + 1) + lx, xhi = xlo + 1;
+    const int ylo = ly * kTile + lx, yhi = ylo + kTile;
+    double res[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double sx = (double)fx[c][xlo] - (double)fx[c][xhi];
+      double sy = (double)fy[c][ylo] - (double)fy[c][yhi];
+      if (VISC) {
+        sx += a.vsd[(int64_t)c * a.nslots + slot];
+        sy += a.vsd[(int64_t)(4 + c) * a.nslots + slot];
+      }
+      res[c] = sx + sy;
+    }
+    const double dt = a.diag->dt;
+    const double scale = (a.tp * dt) * L.step_num * L.inv_vol;
+    double nrho, nu, nv, np, ne, nT;
+    bool wrote = false;
+    if (fl & CF_UPDATE) {
+      const double orho = a.s0[F_RHO][slot], ou = a.s0[F_U][slot], ov = a.s0[F_V][slot],
+                   oe = a.s0[F_E][slot];
+      const double cv0 = orho + res[0] * scale;
+      const double cv1 = orho * ou + res[1] * scale;
+      const double cv2 = orho * ov + res[2] * scale;
+      const double cv3 = orho * oe + res[3] * scale;
+      if (cv0 < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_RHO, (int)slot);
+      if (fl & CF_PRIM) {
+        const double ir = FastMath<double>::rcp(cv0);
+        nrho = cv0;
+        nu = cv1 * ir;
+        nv = cv2 * ir;
+        ne = cv3 * ir;
+        np = (ne - 0.5 * (nu * nu + nv * nv)) * cc.gm1 * nrho;
+        nT = np * ir * cc.inv_Rg;
+        wrote = true;
+      }
+    }
+    if (!wrote && (fl & CF_RESET)) {
+      nrho = cc.initvar[0];
+      nu = cc.initvar[1];
+      nv = cc.initvar[2];
+      np = cc.initvar[4];
+      nT = cc.initvar[5];
+      ne = cc.initvar[6];
+      wrote = true;
+    }
+    if (wrote) {
+      if (nT < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_T, (int)slot);
+      if (FINAL) {
+        a.s0[F_RHO][slot] = nrho;
+        a.s0[F_U][slot] = nu;
+        a.s0[F_V][slot] = nv;
+        a.s0[F_P][slot] = np;
+        a.s0[F_E][slot] = ne;
+        a.s0[F_T][slot] = nT;
+      } else {
+        a.sout[0][slot] = nrho;
+        a.sout[1][slot] = nu;
+        a.sout[2][slot] = nv;
+        a.sout[3][slot] = np;
+      }
+    }
+    if (FINAL && (fl & CF_RESNORM)) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
+    }
+  }
+  if (FINAL) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      unsigned long long m = warp_max_u64(rb[c]);
+      if ((tid & 31) == 0 && m) atomicMax(&a.diag->res_bits[c == 3 ? 4 : c], m);
+    }
+  }
+}
+
 // CFL time step over the normal cells of every level, NS_Solver::Comptdt
 // (NS_Solver.cpp:196-280): a per-cell bound, a warp-shuffle min and one
 // atomic per warp (positive doubles order like their bit patterns).
@@ -305,22 +526,31 @@ __global__ void gather_state_kernel(double *rows, const int32_t *cell_slot, int6
 }
 
 // ---- launchers (one set per arithmetic build)
+#ifdef IBGPU_FAST_BUILD
+#define IBGPU_STAGE_KERNEL stage_kernel_fast
+#else
+#define IBGPU_STAGE_KERNEL stage_kernel
+#endif
+
 template <typename R, int LIM>
 static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
                            bool final_stage, cudaStream_t st) {
   dim3 grid(ntiles), block(kTileCells);
   if (visc) {
-    if (final_stage) stage_kernel<R, LIM, true, true><<<grid, block, 0, st>>>(a, cc);
-    else stage_kernel<R, LIM, true, false><<<grid, block, 0, st>>>(a, cc);
+    if (final_stage) IBGPU_STAGE_KERNEL<R, LIM, true, true><<<grid, block, 0, st>>>(a, cc);
+    else IBGPU_STAGE_KERNEL<R, LIM, true, false><<<grid, block, 0, st>>>(a, cc);
   } else {
-    if (final_stage) stage_kernel<R, LIM, false, true><<<grid, block, 0, st>>>(a, cc);
-    else stage_kernel<R, LIM, false, false><<<grid, block, 0, st>>>(a, cc);
+    if (final_stage) IBGPU_STAGE_KERNEL<R, LIM, false, true><<<grid, block, 0, st>>>(a, cc);
+    else IBGPU_STAGE_KERNEL<R, LIM, false, false><<<grid, block, 0, st>>>(a, cc);
   }
 }
 
 void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limiter, bool visc,
                   bool final_stage, bool mixed, cudaStream_t st) {
   if (ntiles <= 0) return;
+#ifndef IBGPU_FAST_BUILD
+  mixed = false;  // the exact build is FP64 only
+#endif
   if (mixed) {
     if (limiter == LIM_MINMOD) launch_stage_t<float, LIM_MINMOD>(a, cc, ntiles, visc, final_stage, st);
     else launch_stage_t<float, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, st);

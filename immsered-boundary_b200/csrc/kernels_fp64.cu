@@ -1,4 +1,5 @@
 // FP64 (contracted multiply-adds) and mixed-precision builds of the step kernels.
 #define IBGPU_KNS fast
+#define IBGPU_FAST_BUILD 1
 #include "kernels.cuh"
 #include "launchers.h"

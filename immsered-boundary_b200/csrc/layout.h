@@ -32,6 +32,7 @@ enum : uint8_t {
 struct LevelConst {
   double dx, dy, dz;
   double vol;      // dh0*dh1*dh2 (m_geom.v)
+  double inv_vol;  // 1 / vol (fast builds)
   double area_x;   // dh1*dh2 (x-face area)
   double area_y;   // dh2*dh0 (y-face area)
   double area_z;   // dh0*dh1 (z-face area; enters the CFL sum)
@@ -42,7 +43,7 @@ struct LevelConst {
 
 struct CaseConst {
   double gama, Rg, Cv, Ma, Re, qk, s_over_t, dt_ratio;
-  double gm1, gamaRg;
+  double gm1, gamaRg, inv_Rg;
   double initvar[7];
   LevelConst lev[kMaxLevels];
 };

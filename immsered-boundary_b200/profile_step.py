@@ -1,0 +1,57 @@
+"""Run a few time steps of a workload through the C ABI, for profilers.
+
+    python immsered-boundary_b200/profile_step.py --n 2048 --steps 4 --precision fp64
+
+Builds the periodic isentropic-vortex case of the given size and runs
+``--steps`` full time steps (4 stages each) on cuda:0; prints the mean step
+time.  Used as the command under ``ncu`` (the kernel of interest is
+``stage_kernel``).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _pkg():
+    name = "immsered_boundary_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, "__init__.py"),
+                                                  submodule_search_locations=[HERE])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"])
+    ap.add_argument("--limiter", default="vanleer", choices=["vanleer", "minmod"])
+    a = ap.parse_args()
+    pkg = _pkg()
+    ib, wl = pkg.ibgpu, pkg.workloads
+    prec = {"fp64": ib.FP64, "exact": ib.FP64_EXACT, "mixed": ib.MIXED}[a.precision]
+    lim = ib.LIM_VANLEER if a.limiter == "vanleer" else ib.LIM_MINMOD
+    P, cells, prim = wl.vortex_case(a.n, limiter=lim, precision=prec)
+    sol = ib.FlowSolver(P)
+    sol.upload_topology(**cells)
+    sol.init_flow(prim)
+    t0 = time.perf_counter()
+    for ts in range(a.steps):
+        sol.time_marching(ts)
+    dt = (time.perf_counter() - t0) / max(a.steps, 1)
+    print(f"{a.n}x{a.n} {a.precision}: {dt * 1e3:.3f} ms/step (wall, incl. first-step overheads)")
+    sol.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -263,7 +263,11 @@ def test_blown_out_cell_aborts_on_temperature(cuda_lib, pkg, oracle):
 
 
 def test_nan_state_reports_nan_residual(cuda_lib, pkg, oracle):
-    """A NaN in the state ends as the reference's NaN-residual abort (268)."""
+    """A NaN in the state propagates identically, and the GPU reports it as
+    the NaN-residual abort (268).  Deliberately stricter than the reference:
+    its max-norm fold std::max(|s|, acc) (NS_Solver.H:302-307) drops a NaN
+    unless it sits in the last cell of the loop, so the reference (and the
+    oracle that restates it) usually carries on with the NaN state."""
     ib, wl = pkg.ibgpu, pkg.workloads
     n = 32
     P, cells, prim = wl.vortex_case(n, precision=ib.FP64_EXACT)
@@ -271,12 +275,18 @@ def test_nan_state_reports_nan_residual(cuda_lib, pkg, oracle):
     bad[5 * n + 7, 4] = np.nan
     d, lv = oracle_levels_for(oracle, cells["ix"], cells["iy"], bad, n, P)
     rc, *_ = oracle.step(P, lv, 0, 1.0)
+    ref = lv.state_like_dump(d)[: n * n]
+    assert rc == 0 and np.isnan(ref).any()
     sol = ib.FlowSolver(P)
     sol.upload_topology(**cells)
     sol.init_flow(bad)
     with pytest.raises(ib.IbgpuError) as ei:
         sol.time_marching(0)
-    assert ei.value.abort_code == rc == 268
+    assert ei.value.abort_code == 268
+    got = sol.download()
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    ok = ~np.isnan(ref)
+    assert np.array_equal(got[ok], ref[ok])
     sol.close()
 
 
