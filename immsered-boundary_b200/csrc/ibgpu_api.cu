@@ -3,6 +3,7 @@
 // reference main loop and NS_Solver::TimeMarching (main.cpp:84-116,
 // NS_Solver.H:657-702).
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -91,12 +92,73 @@ struct ibgpu_ctx {
   DevDiag *d_diag = nullptr;
   DevDiag *h_diag = nullptr;  // pinned
 
+  // slot lookup: per level, tile (tx,ty) -> tile index
+  std::vector<std::unordered_map<uint64_t, int>> tilemap;
+
+  // coarse/fine pairs per coarse level
+  struct DevPairs {
+    int32_t *coarse = nullptr, *fine = nullptr, *nb = nullptr;
+    int n = 0;
+  };
+  std::vector<DevPairs> res, pro;
+
+  // domain ghosts: level-sorted, dependency waves [begin, end)
+  int32_t *d_bc_ghost = nullptr, *d_bc_ref = nullptr, *d_bc_type = nullptr, *d_bc_face = nullptr;
+  double *d_bc_nmv = nullptr, *d_facevar = nullptr;
+  std::vector<std::vector<std::pair<int, int>>> bc_waves;  // per level
+  double backpressure = 0.0, cos_in = 1.0, sin_in = 0.0;
+
+  // immersed boundary
+  int32_t *d_ib_cell = nullptr, *d_ib_intp = nullptr;
+  double *d_ib_f = nullptr, *d_ib_out = nullptr;
+  int n_ib = 0;
+  int32_t *d_pat_body = nullptr, *d_pat_intp = nullptr, *d_body_begin = nullptr;
+  double *d_pat_f = nullptr, *d_pat_out = nullptr, *d_body_center = nullptr, *d_force = nullptr;
+  int n_pat = 0, nbodies = 0;
+
   // kernel timing
   bool timing = false;
   double kms[3] = {0, 0, 0};
   int64_t klaunch[3] = {0, 0, 0};
 
+  void free_aux() {
+    for (auto *v : {&res, &pro})
+      for (auto &p : *v) {
+        cudaFree(p.coarse);
+        cudaFree(p.fine);
+        cudaFree(p.nb);
+      }
+    res.clear();
+    pro.clear();
+    for (int32_t **p : {&d_bc_ghost, &d_bc_ref, &d_bc_type, &d_bc_face, &d_ib_cell, &d_ib_intp,
+                        &d_pat_body, &d_pat_intp, &d_body_begin}) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+    for (double **p : {&d_bc_nmv, &d_facevar, &d_ib_f, &d_ib_out, &d_pat_f, &d_pat_out,
+                       &d_body_center, &d_force}) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+    bc_waves.clear();
+    n_ib = n_pat = nbodies = 0;
+  }
+
+  // slot of (level, x, y) with periodic wrap, -1 if absent
+  int64_t slot_at(int l, int ix, int iy) const {
+    if (l < 0 || l >= (int)tilemap.size()) return -1;
+    if (cs.periodic_x) { int e = cs.domain_nx << l; ix = ((ix % e) + e) % e; }
+    if (cs.periodic_y) { int e = cs.domain_ny << l; iy = ((iy % e) + e) % e; }
+    int tx = floordiv(ix, kTile), ty = floordiv(iy, kTile);
+    auto it = tilemap[l].find(key2(tx, ty));
+    if (it == tilemap[l].end() || it->second < 0) return -1;
+    int64_t s = (int64_t)it->second * kTileCells + (iy - ty * kTile) * kTile + (ix - tx * kTile);
+    return h_flags_present[s] ? s : -1;
+  }
+  std::vector<uint8_t> h_flags_present;
+
   void free_layout() {
+    free_aux();
     cudaFree(d_tile_nb);
     cudaFree(d_tile_level);
     cudaFree(d_cell_slot);
@@ -165,6 +227,12 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
   k.gm1 = cs->gama - 1.0;
   k.gamaRg = cs->gama * cs->Rg;
   k.inv_Rg = 1.0 / cs->Rg;
+  k.Cp = cs->Cp;
+  k.p_ref = cs->p_ref;
+  k.area_ref = cs->area_ref;
+  k.shear_ref = cs->shear_ref;
+  k.L_ref = cs->L_ref;
+  k.mu = cs->mu;
   for (int i = 0; i < 7; ++i) k.initvar[i] = cs->initvar[i];
   for (int l = 0; l < cs->nlevels; ++l) {
     LevelConst &L = k.lev[l];
@@ -192,6 +260,7 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
     return rc;
   }
   c->stream = c->own_stream;
+  c->body_level = cs->body_level;
   *out = c;
   return IBGPU_OK;
 }
@@ -381,6 +450,9 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
     for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(ctx->d_buf[b][f], 0, nslots * 8, st));
   if (ctx->d_vsd) CK(cudaMemsetAsync(ctx->d_vsd, 0, nslots * 8 * 8, st));
   CK(cudaStreamSynchronize(st));
+  ctx->tilemap = std::move(tilemap);
+  ctx->h_flags_present.assign(nslots, 0);
+  for (int64_t s = 0; s < nslots; ++s) ctx->h_flags_present[s] = (h_flags[s] & CF_PRESENT) ? 1 : 0;
   ctx->ncells = n;
   ctx->ntiles = ntiles;
   ctx->nslots = nslots;
@@ -474,6 +546,47 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     if (b) cudaEventRecord(b, st);
   };
 
+  // AMR::InterfaceExchange (AMRInterface.cpp:3-35): restriction of every
+  // scheduled pair (coarse level ascending), then prolongation
+  for (int l = 0; l + 1 < cs.nlevels && l < (int)ctx->res.size(); ++l) {
+    if (ts % cs.average_step[l + 1] != cs.average_left[l + 1] || ctx->res[l].n == 0) continue;
+    PairArgs pa;
+    pa.coarse = ctx->res[l].coarse;
+    pa.fine = ctx->res[l].fine;
+    pa.nb = nullptr;
+    pa.n = ctx->res[l].n;
+    for (int f = 0; f < kStateFields; ++f) pa.s0[f] = ctx->d_s0[f];
+    if (exact) exact::launch_restrict(pa, ctx->cc, st);
+    else fast::launch_restrict(pa, ctx->cc, st);
+    CK(cudaGetLastError());
+  }
+  for (int l = 0; l + 1 < cs.nlevels && l < (int)ctx->pro.size(); ++l) {
+    if (ts % cs.prolong_step[l + 1] != cs.prolong_left[l + 1] || ctx->pro[l].n == 0) continue;
+    PairArgs pa;
+    pa.coarse = ctx->pro[l].coarse;
+    pa.fine = ctx->pro[l].fine;
+    pa.nb = ctx->pro[l].nb;
+    pa.n = ctx->pro[l].n;
+    for (int f = 0; f < kStateFields; ++f) pa.s0[f] = ctx->d_s0[f];
+    if (exact) exact::launch_prolong(pa, ctx->cc, st);
+    else fast::launch_prolong(pa, ctx->cc, st);
+    CK(cudaGetLastError());
+  }
+  // Body::IBConditions_Image (static bodies): IB ghost cells of the finest level
+  if (ctx->n_ib > 0) {
+    IbArgs ia;
+    ia.cell = ctx->d_ib_cell;
+    ia.intp = ctx->d_ib_intp;
+    ia.cellf = ctx->d_ib_f;
+    ia.out = ctx->d_ib_out;
+    ia.n = ctx->n_ib;
+    for (int f = 0; f < kStateFields; ++f) ia.s0[f] = ctx->d_s0[f];
+    ia.diag = ctx->d_diag;
+    if (exact) exact::launch_ib(ia, ctx->cc, st);
+    else fast::launch_ib(ia, ctx->cc, st);
+    CK(cudaGetLastError());
+  }
+
   // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0)
   const bool do_cfl = (ts % cs.dt_var_step) == 0;
   if (do_cfl) {
@@ -488,6 +601,48 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     else fast::launch_cfl(ca, ctx->cc, ctx->nsm, st);
     done(e);
     CK(cudaGetLastError());
+  }
+
+  // BCValues::BCBoxTreat over the levels that march at ts, by dependency wave
+  for (int l = 0; l < cs.nlevels && l < (int)ctx->bc_waves.size(); ++l) {
+    if (ts % cs.march_step[l] != cs.march_left[l]) continue;
+    for (auto &w : ctx->bc_waves[l]) {
+      BcArgs ba;
+      ba.ghost = ctx->d_bc_ghost;
+      ba.ref = ctx->d_bc_ref;
+      ba.type = ctx->d_bc_type;
+      ba.face = ctx->d_bc_face;
+      ba.nmv = ctx->d_bc_nmv;
+      ba.facevar = ctx->d_facevar;
+      ba.begin = w.first;
+      ba.end = w.second;
+      ba.backpressure = ctx->backpressure;
+      ba.cos_in = ctx->cos_in;
+      ba.sin_in = ctx->sin_in;
+      for (int f = 0; f < kStateFields; ++f) ba.s0[f] = ctx->d_s0[f];
+      if (exact) exact::launch_bc(ba, ctx->cc, st);
+      else fast::launch_bc(ba, ctx->cc, st);
+      CK(cudaGetLastError());
+    }
+  }
+  // NS_Solver::ComptViscousStress, frozen for the stages
+  if (cs.viscous) {
+    ViscArgs va;
+    va.tile_nb = ctx->d_tile_nb;
+    va.tile_level = ctx->d_tile_level;
+    va.flags = ctx->d_flags;
+    for (int f = 0; f < kStateFields; ++f) va.s0[f] = ctx->d_s0[f];
+    va.vsd = ctx->d_vsd;
+    va.nslots = ctx->nslots;
+    for (int l = 0; l < cs.nlevels; ++l) {
+      if (ts % cs.march_step[l] != cs.march_left[l]) continue;
+      va.tile_begin = ctx->level_tile_begin[l];
+      cudaEvent_t e = mark(1);
+      if (exact) exact::launch_viscous(va, ctx->cc, ctx->level_tile_count[l], false, st);
+      else fast::launch_viscous(va, ctx->cc, ctx->level_tile_count[l], mixed, st);
+      done(e);
+      CK(cudaGetLastError());
+    }
   }
 
   // stages over the tiles of the levels that march at ts
@@ -538,7 +693,9 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
   if (hd->err_key != ~0ull) {
     int check = (int)((hd->err_key >> 32) & 0xff);
     abort_slot = (int)(hd->err_key & 0xffffffffull);
-    if (check == ERR_CFL_NEG_DT) abort_code = 424;
+    if (check == ERR_IB_NEG_T) abort_code = 1050;
+    else if (check == ERR_IB_NAN) abort_code = 1076;
+    else if (check == ERR_CFL_NEG_DT) abort_code = 424;
     else if (check == ERR_NEG_T) abort_code = 37;
     else {
       // UpdateConsVars: 611 on the finest level of a run with bodies, else 523
@@ -571,6 +728,279 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
   }
   return IBGPU_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int upload_vec(T **dst, const std::vector<T> &v, cudaStream_t st) {
+  int rc = dev_alloc(dst, v.size());
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ibgpu_upload_interfaces(ibgpu_ctx *ctx, const ibgpu_cf_pairs *pp) {
+  if (!ctx || !pp || pp->nres < 0 || pp->npro < 0 || (pp->nres && !pp->res) || (pp->npro && !pp->pro))
+    return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  const int nlev = ctx->cs.nlevels;
+  cudaStream_t st = ctx->stream;
+  CK(cudaStreamSynchronize(st));
+  for (auto *v : {&ctx->res, &ctx->pro})
+    for (auto &p : *v) {
+      cudaFree(p.coarse);
+      cudaFree(p.fine);
+      cudaFree(p.nb);
+    }
+  ctx->res.assign(nlev, {});
+  ctx->pro.assign(nlev, {});
+  // restriction: per coarse level, in list order
+  std::vector<std::vector<int32_t>> rc_(nlev), rf(nlev);
+  for (int64_t i = 0; i < pp->nres; ++i) {
+    const int32_t *r = pp->res + 11 * i;
+    int l = r[0];
+    if (l < 0 || l + 1 >= nlev) { g_last_error = "restriction pair level out of range"; return IBGPU_E_ARG; }
+    int64_t c = ctx->slot_at(l, r[1], r[2]);
+    if (c < 0) { g_last_error = "restriction coarse cell absent"; return IBGPU_E_TOPOLOGY; }
+    rc_[l].push_back((int32_t)c);
+    for (int k = 0; k < 4; ++k) {
+      int64_t f = ctx->slot_at(l + 1, r[3 + 2 * k], r[4 + 2 * k]);
+      if (f < 0) { g_last_error = "restriction son absent"; return IBGPU_E_TOPOLOGY; }
+      rf[l].push_back((int32_t)f);
+    }
+  }
+  // prolongation: duplicates of a coarse cell write identical sons; keep one
+  std::vector<std::vector<int32_t>> pc(nlev), pf(nlev), pn(nlev);
+  std::vector<std::unordered_map<int64_t, int64_t>> fine_owner(nlev);
+  std::vector<std::unordered_map<int64_t, int>> seen(nlev);
+  for (int64_t i = 0; i < pp->npro; ++i) {
+    const int32_t *r = pp->pro + 11 * i;
+    int l = r[0];
+    if (l < 0 || l + 1 >= nlev) { g_last_error = "prolongation pair level out of range"; return IBGPU_E_ARG; }
+    int64_t c = ctx->slot_at(l, r[1], r[2]);
+    if (c < 0) { g_last_error = "prolongation coarse cell absent"; return IBGPU_E_TOPOLOGY; }
+    int64_t sons[4];
+    for (int k = 0; k < 4; ++k) {
+      sons[k] = ctx->slot_at(l + 1, r[3 + 2 * k], r[4 + 2 * k]);
+      if (sons[k] < 0) { g_last_error = "prolongation son absent"; return IBGPU_E_TOPOLOGY; }
+      auto it = fine_owner[l].find(sons[k]);
+      if (it != fine_owner[l].end() && it->second != c) {
+        g_last_error = "fine ghost claimed by two coarse cells";
+        return IBGPU_E_TOPOLOGY;
+      }
+      fine_owner[l][sons[k]] = c;
+    }
+    if (seen[l].count(c)) continue;
+    seen[l][c] = 1;
+    const int off[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    for (int k = 0; k < 4; ++k) {
+      int64_t nb = ctx->slot_at(l, r[1] + off[k][0], r[2] + off[k][1]);
+      if (nb < 0) { g_last_error = "prolongation stencil cell absent"; return IBGPU_E_TOPOLOGY; }
+      pn[l].push_back((int32_t)nb);
+    }
+    pc[l].push_back((int32_t)c);
+    for (int k = 0; k < 4; ++k) pf[l].push_back((int32_t)sons[k]);
+  }
+  int e;
+  for (int l = 0; l < nlev; ++l) {
+    if ((e = upload_vec(&ctx->res[l].coarse, rc_[l], st)) || (e = upload_vec(&ctx->res[l].fine, rf[l], st)) ||
+        (e = upload_vec(&ctx->pro[l].coarse, pc[l], st)) || (e = upload_vec(&ctx->pro[l].fine, pf[l], st)) ||
+        (e = upload_vec(&ctx->pro[l].nb, pn[l], st)))
+      return e;
+    ctx->res[l].n = (int)rc_[l].size();
+    ctx->pro[l].n = (int)pc[l].size();
+  }
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_upload_boundaries(ibgpu_ctx *ctx, const ibgpu_bc *bc) {
+  if (!ctx || !bc || bc->n < 0 || (bc->n && !bc->ghost) || bc->nfaces < 0 || (bc->nfaces && !bc->facevar))
+    return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  const int nlev = ctx->cs.nlevels;
+  cudaStream_t st = ctx->stream;
+  CK(cudaStreamSynchronize(st));
+  for (int32_t **p : {&ctx->d_bc_ghost, &ctx->d_bc_ref, &ctx->d_bc_type, &ctx->d_bc_face}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  for (double **p : {&ctx->d_bc_nmv, &ctx->d_facevar}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  // entries per level in list order (periodic faces need no work)
+  struct Ent { int64_t g, r; int type, face; double n[3]; int wave; };
+  std::vector<std::vector<Ent>> per(nlev);
+  for (int64_t i = 0; i < bc->n; ++i) {
+    const int32_t *g = bc->ghost + 7 * i;
+    int l = g[0], type = g[6], face = g[5];
+    if (l < 0 || l >= nlev) { g_last_error = "boundary ghost level out of range"; return IBGPU_E_ARG; }
+    if (type == -99 || type == -125) continue;
+    if (type != -50 && type != -12 && type != -13 && type != -49 && type != -46 && type != -42 &&
+        type != -51 && type != -10 && type != -45) {
+      g_last_error = "unknown boundary type";
+      return IBGPU_E_ARG;
+    }
+    if (face < 0 || face >= bc->nfaces) { g_last_error = "boundary face out of range"; return IBGPU_E_ARG; }
+    if (type == -51 && !bc->nmv) { g_last_error = "slip wall without normals"; return IBGPU_E_ARG; }
+    Ent en;
+    en.g = ctx->slot_at(l, g[1], g[2]);
+    en.r = ctx->slot_at(l, g[3], g[4]);
+    if (en.g < 0 || en.r < 0) { g_last_error = "boundary ghost or reference cell absent"; return IBGPU_E_TOPOLOGY; }
+    en.type = type;
+    en.face = face;
+    for (int k = 0; k < 3; ++k) en.n[k] = bc->nmv ? bc->nmv[3 * i + k] : 0.0;
+    per[l].push_back(en);
+  }
+  // dependency waves: a ghost whose reference is written earlier in the list
+  // runs after that write; one written later must read it before the write;
+  // a cell written twice keeps the later value (BCBoxTreat is sequential)
+  ctx->bc_waves.assign(nlev, {});
+  std::vector<int32_t> hg, hr, ht, hf;
+  std::vector<double> hn;
+  for (int l = 0; l < nlev; ++l) {
+    auto &E = per[l];
+    std::unordered_map<int64_t, int> last_writer, max_reader_wave;
+    for (size_t i = 0; i < E.size(); ++i) {
+      int w = 0;
+      auto it = last_writer.find(E[i].r);
+      if (it != last_writer.end()) w = std::max(w, E[it->second].wave + 1);
+      auto rd = max_reader_wave.find(E[i].g);
+      if (rd != max_reader_wave.end()) w = std::max(w, rd->second + 1);
+      auto pw = last_writer.find(E[i].g);
+      if (pw != last_writer.end()) w = std::max(w, E[pw->second].wave + 1);
+      E[i].wave = w;
+      last_writer[E[i].g] = (int)i;
+      int &mr = max_reader_wave[E[i].r];
+      mr = std::max(mr, w);
+    }
+    std::stable_sort(E.begin(), E.end(), [](const Ent &x, const Ent &y) { return x.wave < y.wave; });
+    size_t i = 0;
+    while (i < E.size()) {
+      size_t j = i;
+      while (j < E.size() && E[j].wave == E[i].wave) ++j;
+      ctx->bc_waves[l].push_back({(int)(hg.size() + i), (int)(hg.size() + j)});
+      i = j;
+    }
+    for (auto &en : E) {
+      hg.push_back((int32_t)en.g);
+      hr.push_back((int32_t)en.r);
+      ht.push_back(en.type);
+      hf.push_back(en.face);
+      hn.insert(hn.end(), en.n, en.n + 3);
+    }
+  }
+  std::vector<double> fv(bc->facevar, bc->facevar + 7 * (size_t)bc->nfaces);
+  int e;
+  if ((e = upload_vec(&ctx->d_bc_ghost, hg, st)) || (e = upload_vec(&ctx->d_bc_ref, hr, st)) ||
+      (e = upload_vec(&ctx->d_bc_type, ht, st)) || (e = upload_vec(&ctx->d_bc_face, hf, st)) ||
+      (e = upload_vec(&ctx->d_bc_nmv, hn, st)) || (e = upload_vec(&ctx->d_facevar, fv, st)))
+    return e;
+  ctx->backpressure = bc->backpressure;
+  ctx->cos_in = std::cos(bc->inlet_flow_angle);
+  ctx->sin_in = std::sin(bc->inlet_flow_angle);
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib) {
+  if (!ctx || !ib || ib->ncells < 0 || ib->npatches < 0 || ib->nbodies < 0 ||
+      (ib->ncells && (!ib->cell || !ib->cellf)) || (ib->npatches && (!ib->patch || !ib->patchf)) ||
+      (ib->nbodies && !ib->body_center))
+    return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  const int bl = ctx->body_level;
+  if ((ib->ncells || ib->npatches) && (bl < 0 || bl >= ctx->cs.nlevels)) {
+    g_last_error = "immersed-boundary records without a body level";
+    return IBGPU_E_ARG;
+  }
+  cudaStream_t st = ctx->stream;
+  CK(cudaStreamSynchronize(st));
+  for (int32_t **p : {&ctx->d_ib_cell, &ctx->d_ib_intp, &ctx->d_pat_body, &ctx->d_pat_intp, &ctx->d_body_begin}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  for (double **p : {&ctx->d_ib_f, &ctx->d_ib_out, &ctx->d_pat_f, &ctx->d_pat_out, &ctx->d_body_center, &ctx->d_force}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  std::vector<int32_t> cell, intp, pbody, pintp, begin(ib->nbodies + 1, 0);
+  for (int64_t i = 0; i < ib->ncells; ++i) {
+    const int32_t *c = ib->cell + 18 * i;
+    int64_t s = ctx->slot_at(bl, c[0], c[1]);
+    if (s < 0) { g_last_error = "IB cell absent"; return IBGPU_E_TOPOLOGY; }
+    cell.push_back((int32_t)s);
+    for (int k = 0; k < 8; ++k) {
+      int64_t t = ctx->slot_at(bl, c[2 + 2 * k], c[3 + 2 * k]);
+      if (t < 0) { g_last_error = "IB interpolation cell absent"; return IBGPU_E_TOPOLOGY; }
+      intp.push_back((int32_t)t);
+    }
+  }
+  int prev = 0;
+  for (int64_t i = 0; i < ib->npatches; ++i) {
+    const int32_t *p = ib->patch + 17 * i;
+    if (p[0] < prev || p[0] >= ib->nbodies) { g_last_error = "patches must be grouped by body"; return IBGPU_E_ARG; }
+    prev = p[0];
+    pbody.push_back(p[0]);
+    begin[p[0] + 1]++;
+    for (int k = 0; k < 8; ++k) {
+      int64_t t = ctx->slot_at(bl, p[1 + 2 * k], p[2 + 2 * k]);
+      if (t < 0) { g_last_error = "patch interpolation cell absent"; return IBGPU_E_TOPOLOGY; }
+      pintp.push_back((int32_t)t);
+    }
+  }
+  for (int b = 0; b < ib->nbodies; ++b) begin[b + 1] += begin[b];
+  std::vector<double> cf(ib->cellf, ib->cellf + 16 * (size_t)ib->ncells);
+  std::vector<double> pf(ib->patchf, ib->patchf + 19 * (size_t)ib->npatches);
+  std::vector<double> bc(ib->body_center, ib->body_center + 3 * (size_t)ib->nbodies);
+  int e;
+  if ((e = upload_vec(&ctx->d_ib_cell, cell, st)) || (e = upload_vec(&ctx->d_ib_intp, intp, st)) ||
+      (e = upload_vec(&ctx->d_ib_f, cf, st)) || (e = dev_alloc(&ctx->d_ib_out, 6 * cell.size())) ||
+      (e = upload_vec(&ctx->d_pat_body, pbody, st)) || (e = upload_vec(&ctx->d_pat_intp, pintp, st)) ||
+      (e = upload_vec(&ctx->d_pat_f, pf, st)) || (e = dev_alloc(&ctx->d_pat_out, 12 * pbody.size())) ||
+      (e = upload_vec(&ctx->d_body_center, bc, st)) || (e = upload_vec(&ctx->d_body_begin, begin, st)) ||
+      (e = dev_alloc(&ctx->d_force, 6 * (size_t)std::max(ib->nbodies, 1))))
+    return e;
+  ctx->n_ib = (int)cell.size();
+  ctx->n_pat = (int)pbody.size();
+  ctx->nbodies = ib->nbodies;
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_wall_forces(ibgpu_ctx *ctx, double *out) {
+  if (!ctx || (!out && ctx->nbodies > 0)) return IBGPU_E_ARG;
+  if (!ctx->has_state) return IBGPU_E_STATE;
+  if (ctx->nbodies == 0) return IBGPU_OK;
+  cudaStream_t st = ctx->stream;
+  ForceArgs fa;
+  fa.body = ctx->d_pat_body;
+  fa.intp = ctx->d_pat_intp;
+  fa.patchf = ctx->d_pat_f;
+  fa.body_center = ctx->d_body_center;
+  fa.body_begin = ctx->d_body_begin;
+  fa.n = ctx->n_pat;
+  fa.nbodies = ctx->nbodies;
+  fa.out = ctx->d_pat_out;
+  fa.result = ctx->d_force;
+  for (int f = 0; f < kStateFields; ++f) fa.s0[f] = ctx->d_s0[f];
+  fast::launch_forces(fa, ctx->cc, st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, ctx->d_force, 6 * sizeof(double) * ctx->nbodies, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
 
 void ibgpu_destroy(ibgpu_ctx *ctx) {
   if (!ctx) return;

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
       const double cv1 = un1 + res[1] * level_ts / L.vol;
       const double cv2 = un2 + res[2] * level_ts / L.vol;
       const double cv3 = un3 + res[3] * level_ts / L.vol;
-      if (cv0 < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_RHO, (int)slot);
+      if (cv0 < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_RHO, (int)slot);
       if (fl & CF_PRIM) {
         // Get_Prim_Vars (FlowVariables.H:50-57), FP64
         nrho = cv0;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
       wrote = true;
     }
     if (wrote) {
-      if (nT < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_T, (int)slot);
+      if (nT < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_T, (int)slot);
       if (FINAL) {
         a.s0[F_RHO][slot] = nrho;
         a.s0[F_U][slot] = nu;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       const double cv1 = orho * ou + res[1] * scale;
       const double cv2 = orho * ov + res[2] * scale;
       const double cv3 = orho * oe + res[3] * scale;
-      if (cv0 < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_RHO, (int)slot);
+      if (cv0 < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_RHO, (int)slot);
       if (fl & CF_PRIM) {
         const double ir = FastMath<double>::rcp(cv0);
         nrho = cv0;
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       wrote = true;
     }
     if (wrote) {
-      if (nT < 0.0) raise_error(a.diag, 1 + a.stage, ERR_NEG_T, (int)slot);
+      if (nT < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_T, (int)slot);
       if (FINAL) {
         a.s0[F_RHO][slot] = nrho;
         a.s0[F_U][slot] = nu;
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
     double c1 = (fabs(a.s0[F_V][s]) + c) * L.area_y;
     double c2 = (0.0 + c) * L.area_z;
     double d0 = L.cfl_vol / (c0 + c1 + c2);
-    if (d0 < 0.0) raise_error(a.diag, 0, ERR_CFL_NEG_DT, (int)s);
+    if (d0 < 0.0) raise_error(a.diag, 1, ERR_CFL_NEG_DT, (int)s);
     best = (d0 < best) ? d0 : best;  // std::min(CFL_dt, CFL_dt0) ignores NaN
   }
   unsigned long long b = (unsigned long long)__double_as_longlong(best);

@@ -3,4 +3,5 @@
 // reference operation for operation (the parity build).
 #define IBGPU_KNS exact
 #include "kernels.cuh"
+#include "amr_kernels.cuh"
 #include "launchers.h"

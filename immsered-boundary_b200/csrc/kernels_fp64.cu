@@ -2,4 +2,5 @@
 #define IBGPU_KNS fast
 #define IBGPU_FAST_BUILD 1
 #include "kernels.cuh"
+#include "amr_kernels.cuh"
 #include "launchers.h"

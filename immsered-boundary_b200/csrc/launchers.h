@@ -18,6 +18,13 @@ namespace ibgpu {
                       int64_t n, double *const s0[kStateFields], int nsm, cudaStream_t st);   \
   void launch_gather(double *rows, const int32_t *cell_slot, int64_t n,                       \
                      double *const s0[kStateFields], int nsm, cudaStream_t st);               \
+  void launch_restrict(const PairArgs &a, const CaseConst &cc, cudaStream_t st);               \
+  void launch_prolong(const PairArgs &a, const CaseConst &cc, cudaStream_t st);                \
+  void launch_bc(const BcArgs &a, const CaseConst &cc, cudaStream_t st);                       \
+  void launch_ib(const IbArgs &a, const CaseConst &cc, cudaStream_t st);                       \
+  void launch_forces(const ForceArgs &a, const CaseConst &cc, cudaStream_t st);                \
+  void launch_viscous(const ViscArgs &a, const CaseConst &cc, int ntiles, bool mixed,          \
+                      cudaStream_t st);                                                        \
   }
 
 IBGPU_DECLARE_LAUNCHERS(fast)

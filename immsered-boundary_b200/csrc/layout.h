@@ -43,7 +43,8 @@ struct LevelConst {
 
 struct CaseConst {
   double gama, Rg, Cv, Ma, Re, qk, s_over_t, dt_ratio;
-  double gm1, gamaRg, inv_Rg;
+  double gm1, gamaRg, inv_Rg, Cp;
+  double p_ref, area_ref, shear_ref, L_ref, mu;
   double initvar[7];
   LevelConst lev[kMaxLevels];
 };
@@ -54,7 +55,13 @@ struct CaseConst {
 // (ComptNewPrimVar).  err_key = (phase << 40) | (check << 32) | slot with
 // phase 0 for the CFL pass and 1 + k for stage k; the smallest key is the
 // reference's abort.
-enum : int { ERR_CFL_NEG_DT = 0, ERR_NEG_RHO = 1, ERR_NEG_T = 2 };
+enum : int {
+  ERR_IB_NEG_T = 0,    // phase 0: Body::IBConditions_Image, image point T < 0 (1050)
+  ERR_IB_NAN = 1,      //          IB cell state NaN (1076)
+  ERR_CFL_NEG_DT = 2,  // phase 1: Comptdt (424)
+  ERR_NEG_RHO = 3,     // phase 2+k: UpdateConsVars (523 / 611)
+  ERR_NEG_T = 4        //            ComptNewPrimVar (37)
+};
 
 struct DevDiag {
   double dt;
@@ -86,6 +93,58 @@ struct CflArgs {
   const double *s0[kStateFields];
   int64_t nslots;
   DevDiag *diag;
+};
+
+// Coarse/fine pairs of one level: coarse slot, four son slots and (for
+// prolongation) the coarse cell's -x, +x, -y, +y neighbour slots.
+struct PairArgs {
+  const int32_t *coarse;
+  const int32_t *fine;  // 4 per pair
+  const int32_t *nb;    // 4 per pair (prolongation only)
+  int n;
+  double *s0[kStateFields];
+};
+
+// One dependency wave [begin, end) of the domain-ghost list.
+struct BcArgs {
+  const int32_t *ghost, *ref, *type, *face;
+  const double *nmv;      // 3 per ghost
+  const double *facevar;  // 7 per face
+  int begin, end;
+  double backpressure, cos_in, sin_in;
+  double *s0[kStateFields];
+};
+
+struct IbArgs {
+  const int32_t *cell;   // slot per IB cell
+  const int32_t *intp;   // 8 slots per IB cell
+  const double *cellf;   // 16 per IB cell
+  double *out;           // 6 per IB cell (rho u v p e T)
+  int n;
+  double *s0[kStateFields];
+  DevDiag *diag;
+};
+
+struct ForceArgs {
+  const int32_t *body;   // per patch
+  const int32_t *intp;   // 8 slots per patch
+  const double *patchf;  // 19 per patch
+  const double *body_center;
+  const int32_t *body_begin;  // nbodies + 1 (patches sorted by body, reference order)
+  int n, nbodies;
+  double *out;     // 12 per patch
+  double *result;  // 6 per body
+  double *s0[kStateFields];
+};
+
+struct ViscArgs {
+  const int32_t *tile_nb;
+  const int32_t *tile_level;
+  const uint8_t *flags;
+  int tile_begin;
+  const double *s0[kStateFields];
+  double *vsd;
+  int64_t nslots;
 };
 
 }  // namespace ibgpu

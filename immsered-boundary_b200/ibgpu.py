@@ -28,7 +28,8 @@ CELL_PRESENT, CELL_NORMAL, CELL_UPDATE, CELL_PRIM, CELL_RESET, CELL_RESNORM, CEL
 
 # every symbol include/ibgpu.h declares
 EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_layout_info",
-           "ibgpu_upload_state", "ibgpu_download_state", "ibgpu_step",
+           "ibgpu_upload_interfaces", "ibgpu_upload_boundaries", "ibgpu_upload_ib",
+           "ibgpu_wall_forces", "ibgpu_upload_state", "ibgpu_download_state", "ibgpu_step",
            "ibgpu_set_kernel_timing", "ibgpu_kernel_times", "ibgpu_destroy", "ibgpu_errstr",
            "ibgpu_last_error")
 
@@ -49,7 +50,31 @@ class Case(ctypes.Structure):
         ("step_num", ctypes.c_double * MAX_LEVELS),
         ("domain_nx", ctypes.c_int), ("domain_ny", ctypes.c_int),
         ("periodic_x", ctypes.c_int), ("periodic_y", ctypes.c_int),
+        ("average_step", ctypes.c_int * MAX_LEVELS), ("average_left", ctypes.c_int * MAX_LEVELS),
+        ("prolong_step", ctypes.c_int * MAX_LEVELS), ("prolong_left", ctypes.c_int * MAX_LEVELS),
+        ("body_level", ctypes.c_int),
+        ("p_ref", ctypes.c_double), ("area_ref", ctypes.c_double), ("shear_ref", ctypes.c_double),
+        ("L_ref", ctypes.c_double), ("mu", ctypes.c_double),
     ]
+
+
+class CfPairs(ctypes.Structure):
+    _fields_ = [("nres", ctypes.c_int64), ("res", ctypes.POINTER(ctypes.c_int32)),
+                ("npro", ctypes.c_int64), ("pro", ctypes.POINTER(ctypes.c_int32))]
+
+
+class Bc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("ghost", ctypes.POINTER(ctypes.c_int32)),
+                ("nmv", ctypes.POINTER(ctypes.c_double)), ("nfaces", ctypes.c_int),
+                ("facevar", ctypes.POINTER(ctypes.c_double)), ("backpressure", ctypes.c_double),
+                ("inlet_flow_angle", ctypes.c_double)]
+
+
+class Ib(ctypes.Structure):
+    _fields_ = [("ncells", ctypes.c_int64), ("cell", ctypes.POINTER(ctypes.c_int32)),
+                ("cellf", ctypes.POINTER(ctypes.c_double)), ("npatches", ctypes.c_int64),
+                ("patch", ctypes.POINTER(ctypes.c_int32)), ("patchf", ctypes.POINTER(ctypes.c_double)),
+                ("nbodies", ctypes.c_int), ("body_center", ctypes.POINTER(ctypes.c_double))]
 
 
 class Cells(ctypes.Structure):
@@ -97,6 +122,10 @@ def lib(path: str | None = None):
     L.ibgpu_set_stream.argtypes = [vp, vp]
     L.ibgpu_upload_topology.argtypes = [vp, ctypes.POINTER(Cells)]
     L.ibgpu_layout_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_upload_interfaces.argtypes = [vp, ctypes.POINTER(CfPairs)]
+    L.ibgpu_upload_boundaries.argtypes = [vp, ctypes.POINTER(Bc)]
+    L.ibgpu_upload_ib.argtypes = [vp, ctypes.POINTER(Ib)]
+    L.ibgpu_wall_forces.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ibgpu_upload_state.argtypes = [vp, vp]
     L.ibgpu_download_state.argtypes = [vp, vp]
     L.ibgpu_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Diag)]
@@ -147,7 +176,25 @@ def make_case(params: dict) -> Case:
     c.domain_ny = int(params["domain_ny"])
     c.periodic_x = int(params.get("periodic_x", 0))
     c.periodic_y = int(params.get("periodic_y", 0))
+    for l in range(nl):
+        c.average_step[l] = int(params.get("average_step", [2] * nl)[l])
+        c.average_left[l] = int(params.get("average_left", [1] * nl)[l])
+        c.prolong_step[l] = int(params.get("prolong_step", [2] * nl)[l])
+        c.prolong_left[l] = int(params.get("prolong_left", [1] * nl)[l])
+    c.body_level = int(params.get("body_level", -1))
+    for k in ("p_ref", "area_ref", "shear_ref", "L_ref", "mu"):
+        setattr(c, k, float(params.get(k, 1.0)))
     return c
+
+
+def _i32(a):
+    a = np.ascontiguousarray(a, np.int32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, np.float64)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
 class FlowSolver:
@@ -194,6 +241,40 @@ class FlowSolver:
                       f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
         _check(lib().ibgpu_upload_topology(self._ctx, ctypes.byref(cells)), "ibgpu_upload_topology")
         self.ncells = len(lv)
+
+    def upload_interfaces(self, res, pro):
+        """Coarse/fine pairs as (n, 11) int arrays: level, cx, cy, 4 x (fx, fy)."""
+        r, rp = _i32(np.asarray(res, np.int32).reshape(-1, 11))
+        p, pp = _i32(np.asarray(pro, np.int32).reshape(-1, 11))
+        c = CfPairs(len(r), rp, len(p), pp)
+        _check(lib().ibgpu_upload_interfaces(self._ctx, ctypes.byref(c)), "ibgpu_upload_interfaces")
+
+    def upload_boundaries(self, ghost, nmv, facevar, backpressure=0.0, inlet_flow_angle=0.0):
+        """Domain ghosts (n, 7): level, x, y, ref_x, ref_y, face, type, in the
+        reference's processing order; nmv (n, 3); facevar (nfaces, 7)."""
+        g, gp = _i32(np.asarray(ghost, np.int32).reshape(-1, 7))
+        n, np_ = _f64(np.asarray(nmv, np.float64).reshape(-1, 3))
+        f, fp = _f64(np.asarray(facevar, np.float64).reshape(-1, 7))
+        b = Bc(len(g), gp, np_, len(f), fp, float(backpressure), float(inlet_flow_angle))
+        _check(lib().ibgpu_upload_boundaries(self._ctx, ctypes.byref(b)), "ibgpu_upload_boundaries")
+
+    def upload_ib(self, cell, cellf, patch, patchf, body_center):
+        c, cp = _i32(np.asarray(cell, np.int32).reshape(-1, 18))
+        cf, cfp = _f64(np.asarray(cellf, np.float64).reshape(-1, 16))
+        p, pp = _i32(np.asarray(patch, np.int32).reshape(-1, 17))
+        pf, pfp = _f64(np.asarray(patchf, np.float64).reshape(-1, 19))
+        bc, bcp = _f64(np.asarray(body_center, np.float64).reshape(-1, 3))
+        ib = Ib(len(c), cp, cfp, len(p), pp, pfp, len(bc), bcp)
+        _check(lib().ibgpu_upload_ib(self._ctx, ctypes.byref(ib)), "ibgpu_upload_ib")
+        self.nbodies = len(bc)
+
+    def wall_forces(self):
+        """(nbodies, 6): force(3), moment(3) in the reference's scaling."""
+        nb = getattr(self, "nbodies", 0)
+        out = np.zeros((max(nb, 1), 6))
+        _check(lib().ibgpu_wall_forces(self._ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+               "ibgpu_wall_forces")
+        return out[:nb]
 
     def layout_info(self):
         ns, nt = ctypes.c_int64(), ctypes.c_int64()

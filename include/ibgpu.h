@@ -90,6 +90,17 @@ typedef struct ibgpu_case {
   /* domain: level-0 cell counts and periodicity; level l spans n*2^l */
   int domain_nx, domain_ny;
   int periodic_x, periodic_y;
+  /* coarse/fine schedule of the pair (l-1, l), indexed by the fine level l
+   * (AMRInterface.cpp:8-30, mpiparams.cpp:186-212): restriction when
+   * ts % average_step[l] == average_left[l], prolongation likewise */
+  int average_step[IBGPU_MAX_LEVELS], average_left[IBGPU_MAX_LEVELS];
+  int prolong_step[IBGPU_MAX_LEVELS], prolong_left[IBGPU_MAX_LEVELS];
+  /* finest level of a run with immersed bodies (its leaf-cell branches and
+   * abort code 611 differ, NS_Solver.cpp:146-190, 946-984), -1 without */
+  int body_level;
+  /* reference scales of the wall-force output (Body.cpp:546-552) and the
+   * viscosity mu of the wall shear (FlowConstants.cpp) */
+  double p_ref, area_ref, shear_ref, L_ref, mu;
 } ibgpu_case;
 
 /* Canonical cell list: one row per box of the z = 0 plane of each level
@@ -103,6 +114,53 @@ typedef struct ibgpu_cells {
   const int32_t *iy;
   const uint8_t *flags; /* IBGPU_CELL_* */
 } ibgpu_cells;
+
+/* Coarse/fine pairs.  Restriction pair (AMRLevel::f_res_ghost): the coarse
+ * ghost at (cx, cy) on level `level` takes the density-weighted average of
+ * its four sons on level+1 (TwoLevelOp.H:67-87, 225-231).  Prolongation pair
+ * (AMRLevel::f_pro_ghost, g_pro): the four sons of the coarse leaf cell are
+ * fine ghosts reconstructed from its conserved variables and central
+ * gradients (TwoLevelOp.H:16-22, 35-43, 200-215).  Sons are given explicitly,
+ * in the order (0,0), (0,1), (1,0), (1,1) of (x, y) offsets. */
+typedef struct ibgpu_cf_pairs {
+  int64_t nres;
+  const int32_t *res; /* nres x 11: level, cx, cy, then 4 x (fx, fy) */
+  int64_t npro;
+  const int32_t *pro; /* npro x 11: same layout */
+} ibgpu_cf_pairs;
+
+/* Domain ghosts in the reference's processing order per level
+ * (BCValues::BCBoxTreat, BCValues.H:51-188).  type is the face's boundary
+ * type (-99 periodic, -50 outflow copy, -51 slip wall, -49/-46/-42 no-slip,
+ * -45 fixed velocity, -13 pressure inlet, -12 pressure outlet, -10 fixed). */
+typedef struct ibgpu_bc {
+  int64_t n;
+  const int32_t *ghost; /* n x 7: level, x, y, ref_x, ref_y, face, type */
+  const double *nmv;    /* n x 3: wall normal of type -51 ghosts (or NULL) */
+  int nfaces;
+  const double *facevar; /* nfaces x 7: BCValues::facevar rows */
+  double backpressure;
+  double inlet_flow_angle;
+} ibgpu_bc;
+
+/* Immersed-boundary ghost cells of the finest level (IBCell,
+ * Body::IBConditions_Image, Body.cpp:1361-1496) and wall patches
+ * (Surfpatch, Body::ComptWallForce, Body.cpp:439-558).  The eight
+ * interpolation cells and weights are the reference's [2][2][2] image-point
+ * stencil in its order; in the one-cell-thick slab the z neighbours are the
+ * same 2-D cells. */
+typedef struct ibgpu_ib {
+  int64_t ncells;
+  const int32_t *cell;  /* ncells x 18: x, y, then 8 x (x, y) of the stencil */
+  const double *cellf;  /* ncells x 16: signdis, hgdis, 8 weights, normal(3),
+                           wall velocity(3) */
+  int64_t npatches;
+  const int32_t *patch; /* npatches x 17: body, then 8 x (x, y) */
+  const double *patchf; /* npatches x 19: centre(3), normal(3), area, hgdis,
+                           8 weights, wall velocity(3) */
+  int nbodies;
+  const double *body_center; /* nbodies x 3 */
+} ibgpu_ib;
 
 typedef struct ibgpu_diag {
   double dt;          /* dt used by this step                                */
@@ -126,6 +184,17 @@ int ibgpu_set_stream(ibgpu_ctx *ctx, void *stream);
 /* Upload the mesh as a cell list; lays the levels out as Morton-ordered
  * 16x16 tiles.  Call again after every regrid (AMR::PerformAdaptive). */
 int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells);
+
+/* Coarse/fine pairs, domain ghosts and immersed-boundary records; call after
+ * ibgpu_upload_topology (each replaces the previous upload of its kind). */
+int ibgpu_upload_interfaces(ibgpu_ctx *ctx, const ibgpu_cf_pairs *pairs);
+int ibgpu_upload_boundaries(ibgpu_ctx *ctx, const ibgpu_bc *bc);
+int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib);
+
+/* Wall force and moment of every body from the current state
+ * (Body::ComptWallForce): out[6*b + 0..2] force, out[6*b + 3..5] moment,
+ * in the reference's dimensional scaling. */
+int ibgpu_wall_forces(ibgpu_ctx *ctx, double *out);
 
 /* Number of device cell slots and tiles after the last topology upload. */
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);

@@ -1,0 +1,276 @@
+// Oracle case: viscous flow past a static NACA0012 on the AMR mesh (the
+// plain-method airfoil workload: [0,20]^2 domain, i.e. [-10,10]^2 shifted by
+// the reference's non-negative index origin, Mach 0.5, 2 degrees angle of
+// attack, Re 5000, uniform free-stream start, CFL 0.5).
+//
+// Test infrastructure only: this file plays the role of the reference's
+// per-case user file (Userfunction_cy_naca15.cpp) — it defines the globals
+// and hooks the reference solver expects — for this workload.  The airfoil
+// is the analytic 4-digit thickness distribution (closed trailing edge),
+// written at start-up as two one-cell-thick surface meshes (upper and lower
+// surface, the reference's two-body NACA layout) in the reference's .ugrid
+// format, then read by Body::ReadShapeFile.
+//
+// Environment: IB_NX (base cells per side, default 128), IB_LEVELS (mesh
+// levels, default 4), IB_NPTS (surface points per side, default 200).
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "AMR.H"
+#include "AMRSpaceTime.H"
+#include "BCValues.H"
+#include "Body.H"
+#include "Domain.H"
+#include "FlowVariables.H"
+#include "InputFunc.H"
+#include "Pltoutput.H"
+#include "case_env.h"
+
+using namespace std;
+
+// ---- time-step control -----------------------------------------------------
+double dt = 1.0;  // large: the first CFL evaluation sets dt
+double t_sum = 1.0e30;
+const int ts_sum = 1 << 30;
+const double CFL = case_env_double("IB_CFL", 0.5);
+const double dt_ratio = 1.0;
+int dt_var_step = 1;  // rounded up to the coarsest level's step by the reference
+const int dts_plt = 1 << 30;
+const int dts_time_var = 1 << 30;
+const int dts_space_var = 1 << 30;
+
+// ---- mesh ------------------------------------------------------------------
+const int max_mesh_level = case_env_int("IB_LEVELS", 4);
+const int init_level_num = case_env_int("IB_LEVELS", 4);
+const Point lowpt = Point(0, 0, 0);
+const Point highpt = Point(case_env_int("IB_NX", 128), case_env_int("IB_NX", 128), 1);
+static const double kDomainLength = 20.0;
+
+string meshfile = "none";
+Pointxyz meshscale(1.0, 1.0, 1.0);
+Pointxyz frame_rotate_vel = Pointxyz(0.0, 0.0, 0.0);
+Pointxyz frame_rotate_origin = Pointxyz(0.0, 0.0, 0.0);
+Pointxyz frame_trans_vel = Pointxyz(0.0, 0.0, 0.0);
+const bool moveflag = false;
+
+// ---- reference scales (constant-initialised) ------------------------------
+double roe_ref = 1.0;
+double L_ref = 1.0;
+double mu_ref = 1.0 / 5000.0;                      // Re = 5000
+double u_ref = 1.0;
+double T_ref = 1.0 / (0.5 * 0.5 * 287.4 * 1.4);   // Mach 0.5
+
+bool additional_output = false;
+const int init_jump = 0;
+const int filenodenum = 1;
+const int filelevelnum = 1;
+const int filebodynum = 2;
+const char soln_file_name[30] = "none";
+
+// ---- airfoil placement -----------------------------------------------------
+static const double kAoA = 2.0 / 180.0 * 3.14159265358979323846;
+static const double kLeX = 9.5, kLeY = 10.0;      // leading edge; chord 1 along +x
+static const double kPitchX = 0.25;               // moment / body centre at quarter chord
+
+// NACA 4-digit symmetric thickness, closed trailing edge
+static double naca_half_thickness(double x, double t) {
+  return 5.0 * t * (0.2969 * sqrt(x) - 0.1260 * x - 0.3516 * x * x + 0.2843 * x * x * x -
+                    0.1036 * x * x * x * x);
+}
+
+// One surface as a one-cell-thick quad strip (z = 0 and 0.1), points from
+// the trailing edge to the leading edge, in the reference's .ugrid layout:
+// "npts nelem", npts lines of xyz, nelem lines of four 1-based indices.
+static void write_surface(const string &path, int n, double sign) {
+  FILE *f = fopen(path.c_str(), "w");
+  fprintf(f, "%d %d\n", 2 * n, n - 1);
+  for (int layer = 0; layer < 2; ++layer)
+    for (int i = 0; i < n; ++i) {
+      double x = 0.5 * (1.0 + cos(3.14159265358979323846 * i / (n - 1)));  // 1 -> 0
+      double y = sign * naca_half_thickness(x, 0.12);
+      fprintf(f, "%.17g %.17g %.17g\n", x, y, layer ? 0.1 : 0.0);
+    }
+  for (int i = 1; i < n; ++i) fprintf(f, "%d %d %d %d\n", i, i + 1, n + i + 1, n + i);
+  fclose(f);
+}
+
+void AMR::ADPRule(vector<Body> &) {
+  adpflag = false;
+  for (int i = 0; i < max_mesh_level; ++i) {
+    m_level[i].torefine = false;
+    m_level[i].toderefine = false;
+  }
+}
+
+void AMR::SetRefineFlag() {
+  if (ts == 0) {
+    m_level.back().torefine = true;
+    init_adjust_level = 0;
+  }
+}
+
+// Plain geometric criterion in the reference's style
+// (Userfunction_cy_naca15.cpp:533-650): boxes around the airfoil on the
+// coarse levels, a signed-distance band on the last refined level.
+void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
+  m_level[ilevel].Inittag();
+  if (!m_level[ilevel].torefine) return;
+  int bs = m_level[ilevel].m_box.ps();
+  int be = m_level[ilevel].m_box.pe();
+  int tagnum = 0;
+  if (ilevel < max_mesh_level - 2) {
+    double s = pow(0.5, ilevel);
+    double up = 4.0 * s, down = 8.0 * s, half_h = 4.0 * s;
+    for (int i = bs; i < be; ++i) {
+      double x = m_mesh.bc(ilevel, i)[0], y = m_mesh.bc(ilevel, i)[1];
+      if (x - kLeX > -up && x - (kLeX + 1.0) < down && fabs(y - kLeY) < half_h) {
+        m_level[ilevel].m_tag[i].givetag();
+        ++tagnum;
+        m_level[ilevel].taggedbox.push_back(i);
+      }
+    }
+  } else {
+    double rs = -3.0 * dh[ilevel][0];
+    double re = max(0.25, 16.0 * dh[max_mesh_level - 1][0]);
+    for (int i = bs; i < be; ++i) {
+      double celldis = m_level[ilevel].m_box[i].pair.signdis;
+      double x = m_mesh.bc(ilevel, i)[0], y = m_mesh.bc(ilevel, i)[1];
+      // the signed distance is measured along the nearest patch normal, so
+      // bound the band to the airfoil's neighbourhood
+      bool near = x > kLeX - re && x < kLeX + 1.0 + re && fabs(y - kLeY) < 0.5 + re;
+      if (near && celldis > rs && celldis < re) {
+        m_level[ilevel].m_tag[i].tag = 0;
+        ++tagnum;
+        m_level[ilevel].taggedbox.push_back(i);
+      }
+    }
+  }
+  MPI_Barrier(share_comm);
+  CheckDetagLocation(ilevel);
+  if (morelevel && ilevel == m_mesh.MyCurNum() - 2) {
+    int l0 = m_mesh.MyCurNum() - 2;
+    for (size_t i = 0; i < abody.size(); ++i) abody[i].CheckAttachBoxTag(m_level[l0].m_tag, l0, m_mesh);
+  }
+  MPI_Barrier(share_comm);
+}
+
+void Body::Motion_Rule(Mesh &, double &) {}
+
+void SetTwodFlag() {
+  level_twod_flag.resize(max_mesh_level);
+  level_twod_flag[0] = false;
+  for (int i = 1; i < max_mesh_level; ++i) level_twod_flag[i] = true;
+}
+
+void InitSpaceParams() {
+  double h = kDomainLength / double(highpt.xy[0]);
+  double dh0[3] = {h, h, 0.1};
+  periodic[0] = false;
+  periodic[1] = false;
+  periodic[2] = true;
+  ComptLevelgridsize(dh0);
+}
+
+void Body::SetBodyParams(vector<Body> &abody, Mesh &amesh, vector<Body> &) {
+  const int npts = case_env_int("IB_NPTS", 200);
+  write_surface("naca0012_upper.ugrid", npts, 1.0);
+  write_surface("naca0012_lower.ugrid", npts, -1.0);
+  bodynum = 2;
+  const char *files[2] = {"naca0012_upper.ugrid", "naca0012_lower.ugrid"};
+  for (int i = 0; i < bodynum; ++i) {
+    abody.push_back(Body(i));
+    abody.back().FindNearBody();
+    abody.back().SetBodyCenter(kLeX + kPitchX, kLeY, 0.05);
+    abody.back().SetBodyOffset(kLeX, kLeY, 0.0);
+    abody.back().SetBodyScale(1.0, 1.0, 1.0);
+    abody.back().InitVelZero();
+    abody[i].ReadShapeFile(files[i]);
+    abody[i].ComptSurfptOff();
+    abody[i].ComptPatchParams();
+    abody[i].Attachbox_Init(amesh);
+  }
+  for (int i = 0; i < bodynum; ++i) abody[i].CheckBodyPatchCenter();
+  MPI_Barrier(MPI_COMM_WORLD);
+  Body::ComptDisFromBoxtoBody_Init(amesh, abody);
+}
+
+void Domain::SetBlockNum() { blocknum = Point(1, 1, 1); }
+
+// Far field: pressure inlet (x-), pressure outlet (x+), zero-gradient top
+// and bottom, periodic z (the reference case's face types).
+void Domain::SetFaceProperty(DataArray<Box> &, DataArray<BoxCellGeom> &) {
+  facenum = 6;
+  faceup.resize(facenum);
+  facedown.resize(facenum);
+  facetype.resize(facenum);
+  facedir.resize(facenum);
+  refboxface.resize(facenum);
+  faceup[0] = Point(0, 99999, 99999);
+  facedown[0] = Point(-10, -99999, -99999);
+  facetype[0] = -13;
+  facedir[0] = Point(1, 0, 0);
+  faceup[1] = Point(boxnum.ix() + 10, 99999, 99999);
+  facedown[1] = Point(boxnum.ix() - 1, -99999, -99999);
+  facetype[1] = -12;
+  facedir[1] = Point(-1, 0, 0);
+  faceup[2] = Point(99999, 0, 99999);
+  facedown[2] = Point(-99999, -10, -99999);
+  facetype[2] = -50;
+  facedir[2] = Point(0, 1, 0);
+  faceup[3] = Point(99999, boxnum.iy() + 10, 99999);
+  facedown[3] = Point(-99999, boxnum.iy() - 1, -99999);
+  facetype[3] = -50;
+  facedir[3] = Point(0, -1, 0);
+  faceup[4] = Point(99999, 99999, 0);
+  facedown[4] = Point(-99999, -99999, -10);
+  facetype[4] = -99;
+  facedir[4] = Point(0, 0, 1);
+  faceup[5] = Point(99999, 99999, boxnum.iz() + 10);
+  facedown[5] = Point(-99999, -99999, boxnum.iz() - 1);
+  facetype[5] = -99;
+  facedir[5] = Point(0, 0, -1);
+  CheckPeriodicFaceType();
+}
+
+void BCValues::SetBCType_125_Inputinletbdlayer(FlowVariables &, FlowVariables &, const int &,
+                                               double &, int &, Mesh &) {}
+
+void BCValues::SetInitValues() {
+  inlet_flow_angle = kAoA;
+  initvar.u = cos(kAoA);
+  initvar.v = sin(kAoA);
+  initvar.w = 0.0;
+  double speed = pow(pow(initvar.u, 2) + pow(initvar.v, 2) + pow(initvar.w, 2), 0.5);
+  initvar.T = pow(speed / Ma, 2) / (gama * Rg);
+  initvar.roe = 1.0;
+  Get_p_ideal_gas(initvar);
+  Get_E(initvar);
+}
+
+void BCValues::UserInit(Mesh &amesh, const int &ilevel, const int &bn) {
+  amesh.LevelBoxData(ilevel, bn) = initvar;
+}
+
+// Total conditions at the inlet, free-stream static pressure at the outlet
+// (as the reference case file sets them).
+void BCValues::SetBDFaceVars() {
+  for (size_t i = 0; i < facevar.size(); ++i) facevar[i] = initvar;
+  facevar[0].T = kineticenergy(initvar) * initvar.roe / Cp + initvar.T;
+  facevar[0].p = initvar.p * pow(1.0 + 0.2 * pow(Ma, 2), 1.4 / 0.4);
+  facevar[1].p = initvar.p;
+}
+
+void BCValues::SetBackPressure(Mesh &) { backpressure = 0.0; }
+
+void Pltoutput::Design_User_File() { userfilenum = 0; }
+
+void Pltoutput::Print_Var_as_Func_of_Time(vector<Body> &, NS_Solver &) {}
+
+void Pltoutput::Print_Var_as_Func_of_Space(vector<Body> &) {}
+
+void Mesh::ComptSectionAvePre(const int &, double &p0, double &T0, int) {
+  p0 = 0.0;
+  T0 = 0.0;
+}

@@ -27,6 +27,17 @@
 #include <string>
 #include <vector>
 
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <unistd.h>
+
+// Test-infrastructure access: the dump below reads the reference's private
+// AMR pair lists, boundary values and immersed-boundary records.  Standard
+// headers are included above so only the reference's own classes see this.
+#define private public
+#define protected public
+
 #include "Check.H"
 using namespace std;  // the reference headers assume it (min/max/abs in macros)
 #include "Slopelimiter.H"
@@ -45,6 +56,7 @@ using namespace std;  // the reference headers assume it (min/max/abs in macros)
 #include "TwoLevelOp.H"
 
 extern const double Ma;
+extern double p_ref, area_ref, shear_ref;
 
 namespace {
 
@@ -93,6 +105,155 @@ struct Dump {
   }
 };
 
+AMR *g_amr = nullptr;
+std::vector<Body> *g_bodies = nullptr;
+
+inline void put_pos(std::vector<int32_t> &v, Mesh &mesh, int l, int b) {
+  if (b < 0) {
+    v.push_back(INT32_MIN);
+    v.push_back(INT32_MIN);
+    return;
+  }
+  Box &bx = mesh.ShowLevelBox(l)[b];
+  v.push_back(bx.ix());
+  v.push_back(bx.iy());
+}
+
+// Coarse/fine pairs (AMRLevel::f_res_ghost, f_pro_ghost, g_pro), positions
+// of the coarse box and its four z = 0 sons in Point_iterator_2d order.
+void dump_interfaces(Dump &d, Mesh &mesh, AMR &amr) {
+  std::vector<int32_t> res, pro;
+  int nlev = mesh.MyCurNum();
+  for (int l = 0; l + 1 < nlev; ++l) {
+    AMRLevel &al = amr.m_level[l];
+    for (int ig = 0; ig < ighost; ++ig) {
+      DataArray<CtoFPair> &lst = al.f_res_ghost[ig];
+      for (int i = 0; i < lst.size(); ++i) {
+        res.push_back(l);
+        res.push_back(ig);
+        put_pos(res, mesh, l, lst[i].ci);
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) put_pos(res, mesh, l + 1, lst[i].fi.son[a][b][0]);
+      }
+    }
+    for (int i = 0; i < al.f_pro_ghost.size(); ++i) {
+      pro.push_back(l);
+      pro.push_back(0);
+      put_pos(pro, mesh, l, al.f_pro_ghost[i].ci);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) put_pos(pro, mesh, l + 1, al.f_pro_ghost[i].fi.son[a][b][0]);
+    }
+    for (int i = 0; i < al.g_pro.size(); ++i) {
+      CtoFPair &cfp = al.level_pro_ghost[al.g_pro[i]];
+      pro.push_back(l);
+      pro.push_back(1);
+      put_pos(pro, mesh, l, cfp.ci);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) put_pos(pro, mesh, l + 1, cfp.fi.son[a][b][0]);
+    }
+  }
+  d.i32("cf_res", res);
+  d.i32("cf_pro", pro);
+}
+
+// Domain ghosts in BCBoxTreat order (BCValues.H:51-188) and the face values.
+void dump_boundaries(Dump &d, Mesh &mesh, OracleSolver &solver) {
+  std::vector<int32_t> bc;
+  std::vector<double> nmv;
+  int nlev = mesh.MyCurNum();
+  for (int l = 0; l < nlev; ++l) {
+    DataArray<Domainghost> &dmg = mesh.MeshGhostArray(l);
+    for (int i = 0; i < dmg.size(); ++i) {
+      int f0 = dmg[i].nbface;
+      bc.push_back(l);
+      put_pos(bc, mesh, l, dmg[i].cell);
+      put_pos(bc, mesh, l, dmg[i].refcell);
+      bc.push_back(f0);
+      bc.push_back(mesh.m_dm.facetype[f0]);
+      bc.push_back(mesh.m_dm.facedir[f0][2] != 0 ? 1 : 0);
+      bc.push_back(mesh.ShowLevelBox(l)[dmg[i].cell].iz());
+      nmv.push_back(dmg[i].nmv[0]);
+      nmv.push_back(dmg[i].nmv[1]);
+      nmv.push_back(dmg[i].nmv[2]);
+    }
+  }
+  d.i32("bc", bc);
+  d.f64("bc_nmv", nmv);
+  BCValues &B = solver.meshbc;
+  std::vector<double> fv;
+  for (size_t f = 0; f < B.facevar.size(); ++f) {
+    FlowVariables &v = B.facevar[f];
+    double r[7] = {v.roe, v.u, v.v, v.w, v.p, v.T, v.e};
+    fv.insert(fv.end(), r, r + 7);
+  }
+  d.f64("facevar", fv);
+  std::vector<double> bs = {B.backpressure, inlet_flow_angle};
+  d.f64("bc_scalars", bs);
+}
+
+// Immersed-boundary cells processed by Body::IBConditions_Image
+// (Body.cpp:1361-1496) and the surface patches of Body::ComptWallForce
+// (Body.cpp:439-558).
+void dump_body(Dump &d, Mesh &mesh, std::vector<Body> &bodies) {
+  std::vector<int32_t> ib, pat;
+  std::vector<double> ibf, patf, bodyf;
+  int last = mesh.MyCurNum() - 1;
+  DataArray<IBCell> &mdis = mesh.ibarray();
+  for (int i = 0; i < mdis.size(); ++i) {
+    IBCell &c = mdis[i];
+    if (!(mesh.m_level[last].m_box.isnormal(c.ci) && c.mynode == node)) continue;
+    BoxtoWall &w = mesh.m_level[last].m_box[c.ci].pair;
+    put_pos(ib, mesh, last, c.ci);
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 2; ++k) put_pos(ib, mesh, last, c.hgc.intpcell[a][b][k]);
+    ib.push_back(w.body);
+    ib.push_back(w.patch);
+    Pointxyz patv;
+    bodies[w.body].Surface_Point_Velocity(c.hgc.attach_pt, patv);
+    Pointxyz &nv = bodies[w.body].patch[w.patch].nv;
+    ibf.push_back(w.signdis);
+    ibf.push_back(c.hgc.hgdis);
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 2; ++k) ibf.push_back(c.hgc.intpcoef[a][b][k]);
+    for (int k = 0; k < 3; ++k) ibf.push_back(nv[k]);
+    for (int k = 0; k < 3; ++k) ibf.push_back(patv[k]);
+  }
+  for (size_t bi = 0; bi < bodies.size(); ++bi) {
+    Body &B = bodies[bi];
+    for (int k = 0; k < 3; ++k) bodyf.push_back(B.bodycenter[k]);
+    for (int i = 0; i < B.patch.size(); ++i) {
+      Surfpatch &P = B.patch[i];
+      if (P.node != node) continue;
+      pat.push_back((int32_t)bi);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int k = 0; k < 2; ++k) put_pos(pat, mesh, last, P.hgc.intpcell[a][b][k]);
+      for (int k = 0; k < 3; ++k) patf.push_back(P.pc[k]);
+      for (int k = 0; k < 3; ++k) patf.push_back(P.nv[k]);
+      patf.push_back(P.area);
+      patf.push_back(P.hgc.hgdis);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int k = 0; k < 2; ++k) patf.push_back(P.hgc.intpcoef[a][b][k]);
+      Pointxyz patv;
+      B.Surface_Point_Velocity(P.pc, patv);
+      for (int k = 0; k < 3; ++k) patf.push_back(patv[k]);
+    }
+  }
+  d.i32("ib", ib);
+  d.f64("ib_f", ibf);
+  d.i32("patch", pat);
+  d.f64("patch_f", patf);
+  bodyf.push_back(p_ref);
+  bodyf.push_back(area_ref);
+  bodyf.push_back(shear_ref);
+  bodyf.push_back(L_ref);
+  bodyf.push_back(mu);
+  d.f64("body_f", bodyf);
+}
+
 // Every box of the z = 0 plane of every level (normal cells and 2-D ghosts),
 // keyed by (level, ix, iy) so the comparison never depends on the
 // reference's internal array order.
@@ -139,6 +300,7 @@ void dump_state(const std::string &path, Mesh &mesh, OracleSolver &solver,
   std::vector<double> scal = {t, dt, CFL_dt, (double)ts, gama, Rg, Cv, Cp, Ma, Re, Pr, qk,
                               S_over_T_ref, CFL, (double)solver.stages()};
   for (int k = 0; k < solver.stages(); ++k) scal.push_back(solver.coef(k));
+  scal.push_back((double)dt_var_step);
   d.f64("scalars", scal);
   std::vector<double> dhv;
   for (int l = 0; l < nlev; ++l) {
@@ -173,6 +335,9 @@ void dump_state(const std::string &path, Mesh &mesh, OracleSolver &solver,
   d.f64("signdis", signdis);
   d.f64("prim", prim);
   d.f64("forces", forces);
+  dump_interfaces(d, mesh, *g_amr);
+  dump_boundaries(d, mesh, solver);
+  dump_body(d, mesh, *g_bodies);
 }
 
 }  // namespace
@@ -191,6 +356,8 @@ int main(int argc, char **argv) {
   pltfile.Design_User_File();
   amr.SetupNewAMR(sphere);
   Body::ImmerseWallBoundary(mesh, sphere);
+  g_amr = &amr;
+  g_bodies = &sphere;
 
   const int stages = env_int("IB_STAGES", 4);
   OracleSolver flowsolver(mesh, p_domain, (int)sphere.size(), stages);

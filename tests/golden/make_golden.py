@@ -33,7 +33,16 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 CASES = {
     "vortex_vanleer_s4_n32": ("ref_vortex_vanleer", {"IB_NX": "32", "IB_STAGES": "4"}, 4),
     "vortex_minmod_s3_n32": ("ref_vortex_minmod", {"IB_NX": "32", "IB_STAGES": "3"}, 3),
+    # static NACA0012, 3 levels, immersed body, far-field boundaries, Re 5000:
+    # covers restriction/prolongation schedules, boundary ghosts, IB cells,
+    # viscous fluxes, subcycling and the wall forces
+    "naca_minmod_s4_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
+                                                  "IB_STAGES": "4", "IB_USER_INIT": "0",
+                                                  "IB_FORCES": "1", "IB_NPTS": "120"}, 4),
 }
+# per-case records that do not change between dumps of a static mesh
+AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
+       "patch_f", "body_f")
 
 STATIC = ("level", "ix", "iy", "kind", "ptype", "solid", "infect", "signdis")
 
@@ -49,16 +58,19 @@ def run_case(name: str, binary: str, env: dict, steps: int) -> str:
                        stdout=subprocess.DEVNULL)
         snaps = [pyoracle.read_dump(os.path.join(work, f"d_{k:06d}.bin")) for k in range(steps + 1)]
         out = {k: snaps[0][k] for k in STATIC}
-        for k in ("dh", "schedule", "initvar", "domain"):
-            out[k] = snaps[0][k]
+        for k in ("dh", "schedule", "initvar", "domain") + AUX:
+            if k in snaps[0]:
+                out[k] = snaps[0][k]
         for s in snaps[1:]:
             for k in STATIC:
                 if not np.array_equal(s[k], snaps[0][k]):
                     raise RuntimeError(f"{name}: topology changed between dumps ({k})")
         out["prim"] = np.stack([s["prim"].reshape(-1, 7) for s in snaps])
         out["scalars"] = np.stack([s["scalars"] for s in snaps])
-        forces = [s["forces"] for s in snaps]
-        out["forces"] = np.stack(forces) if all(len(f) == len(forces[0]) for f in forces) else np.zeros((0,))
+        # wall forces exist after each step (none for the initial state)
+        nf = max(len(s["forces"]) for s in snaps)
+        out["forces"] = np.stack([s["forces"] if len(s["forces"]) == nf else np.full(nf, np.nan)
+                                  for s in snaps])
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)
         return path
@@ -73,7 +85,7 @@ def load(name: str) -> dict:
 
 def snapshot(g: dict, k: int) -> dict:
     """Dump-shaped dict of snapshot k (what pyoracle.OracleLevels expects)."""
-    d = {key: g[key] for key in STATIC + ("dh", "schedule", "initvar", "domain")}
+    d = {key: g[key] for key in STATIC + ("dh", "schedule", "initvar", "domain") + AUX if key in g}
     d["prim"] = g["prim"][k].ravel()
     d["scalars"] = g["scalars"][k]
     return d
