@@ -23,6 +23,7 @@ UNITS = {
     "ibgpu_api.cu": [],
     "kernels_fp64.cu": [],
     "kernels_exact.cu": ["-fmad=false"],
+    "noalloc.cu": [],
 }
 
 

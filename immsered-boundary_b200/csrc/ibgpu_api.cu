@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ibgpu.h"
+#include "host_internal.h"
 #include "launchers.h"
 #include "layout.h"
 
@@ -176,26 +177,10 @@ struct ibgpu_ctx {
   }
 };
 
-extern "C" {
+namespace ibgpu {
+void set_last_error(const std::string &msg) { g_last_error = msg; }
 
-const char *ibgpu_errstr(int code) {
-  switch (code) {
-    case IBGPU_OK: return "ok";
-    case IBGPU_E_ARG: return "invalid argument";
-    case IBGPU_E_CUDA: return "CUDA runtime error";
-    case IBGPU_E_STATE: return "call out of order (topology/state not uploaded)";
-    case IBGPU_E_ABORT: return "solver abort condition (see ibgpu_diag.abort_code)";
-    case IBGPU_E_NOMEM: return "device allocation failed";
-    case IBGPU_E_TOPOLOGY: return "cell list cannot be laid out on the tiled mesh";
-    default: return "unknown error";
-  }
-}
-
-const char *ibgpu_last_error(void) { return g_last_error.c_str(); }
-
-int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
-  if (!cs || !out) return IBGPU_E_ARG;
-  *out = nullptr;
+int validate_case(const ibgpu_case *cs) {
   if (cs->abi_version != IBGPU_ABI_VERSION) {
     g_last_error = "ABI version mismatch";
     return IBGPU_E_ARG;
@@ -211,10 +196,13 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
       g_last_error = "invalid level parameters";
       return IBGPU_E_ARG;
     }
-  ibgpu_ctx *c = new (std::nothrow) ibgpu_ctx();
-  if (!c) return IBGPU_E_NOMEM;
-  c->cs = *cs;
-  CaseConst &k = c->cc;
+  return IBGPU_OK;
+}
+}  // namespace ibgpu
+
+namespace ibgpu {
+// CaseConst of a validated case (shared with the allocation-free entry point)
+void fill_case_const(const ibgpu_case *cs, CaseConst &k) {
   std::memset(&k, 0, sizeof(k));
   k.gama = cs->gama;
   k.Rg = cs->Rg;
@@ -249,6 +237,35 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
     L.step_num = cs->step_num[l];
     L.cfl_vol = cs->cfl * L.vol;
   }
+}
+}  // namespace ibgpu
+
+extern "C" {
+
+const char *ibgpu_errstr(int code) {
+  switch (code) {
+    case IBGPU_OK: return "ok";
+    case IBGPU_E_ARG: return "invalid argument";
+    case IBGPU_E_CUDA: return "CUDA runtime error";
+    case IBGPU_E_STATE: return "call out of order (topology/state not uploaded)";
+    case IBGPU_E_ABORT: return "solver abort condition (see ibgpu_diag.abort_code)";
+    case IBGPU_E_NOMEM: return "device allocation failed";
+    case IBGPU_E_TOPOLOGY: return "cell list cannot be laid out on the tiled mesh";
+    default: return "unknown error";
+  }
+}
+
+const char *ibgpu_last_error(void) { return g_last_error.c_str(); }
+
+int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
+  if (!cs || !out) return IBGPU_E_ARG;
+  *out = nullptr;
+  int vrc = validate_case(cs);
+  if (vrc) return vrc;
+  ibgpu_ctx *c = new (std::nothrow) ibgpu_ctx();
+  if (!c) return IBGPU_E_NOMEM;
+  c->cs = *cs;
+  fill_case_const(cs, c->cc);
   cudaError_t e = cudaGetDevice(&c->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);

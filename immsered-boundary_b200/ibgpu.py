@@ -31,7 +31,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_upload_interfaces", "ibgpu_upload_boundaries", "ibgpu_upload_ib",
            "ibgpu_wall_forces", "ibgpu_upload_state", "ibgpu_download_state", "ibgpu_step",
            "ibgpu_set_kernel_timing", "ibgpu_kernel_times", "ibgpu_destroy", "ibgpu_errstr",
-           "ibgpu_last_error")
+           "ibgpu_last_error", "ibgpu_step_periodic_noalloc")
+NOALLOC_MAX_CELLS = 65536
 
 
 class Case(ctypes.Structure):
@@ -131,6 +132,9 @@ def lib(path: str | None = None):
     L.ibgpu_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Diag)]
     L.ibgpu_set_kernel_timing.argtypes = [vp, ctypes.c_int]
     L.ibgpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_step_periodic_noalloc.argtypes = [ctypes.POINTER(Case), ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, vp, vp, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(Diag), vp]
     L.ibgpu_destroy.argtypes = [vp]
     L.ibgpu_destroy.restype = None
     L.ibgpu_errstr.argtypes = [ctypes.c_int]
@@ -195,6 +199,22 @@ def _i32(a):
 def _f64(a):
     a = np.ascontiguousarray(a, np.float64)
     return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def step_periodic_noalloc(params: dict, ts: int, nx: int, ny: int, d_rows_in: int,
+                          d_rows_out: int, dt: float, stream: int = 0):
+    """One step of a periodic single-level grid through the allocation-free
+    entry point; d_rows_in/out are device addresses of (nx*ny, 7) float64
+    rows in row-major cell order.  Returns (dt, Diag)."""
+    case = make_case(params)
+    d = Diag()
+    dtv = ctypes.c_double(dt)
+    rc = lib().ibgpu_step_periodic_noalloc(ctypes.byref(case), int(ts), int(nx), int(ny),
+                                           ctypes.c_void_p(d_rows_in), ctypes.c_void_p(d_rows_out),
+                                           ctypes.byref(dtv), ctypes.byref(d), ctypes.c_void_p(stream))
+    if rc != OK:
+        raise IbgpuError(rc, "ibgpu_step_periodic_noalloc", lib().ibgpu_last_error().decode(), d)
+    return dtv.value, d
 
 
 class FlowSolver:

@@ -222,6 +222,29 @@ int ibgpu_kernel_times(const ibgpu_ctx *ctx, double ms_out[3], int64_t launches_
 
 void ibgpu_destroy(ibgpu_ctx *ctx);
 
+/* Allocation-free variant of ibgpu_step for one periodic, inviscid,
+ * single-level grid of nx x ny cells (this entry point has no counterpart in
+ * the reference).  For callers that must not allocate device memory while
+ * they run, e.g. a coupler whose device memory belongs to another
+ * framework's pool, or a time loop that cannot afford cudaMalloc/cudaFree's
+ * device-wide synchronisation.  The caller passes device buffers of
+ * FlowVariables rows in row-major cell order (iy * nx + ix), 7 doubles per
+ * cell; d_rows_in may equal d_rows_out.  Every intermediate lives in one
+ * fixed file-scope device array sized for IBGPU_NOALLOC_MAX_CELLS cells
+ * (about 7.4 MB, held by each GPU that loads the library until exit); no
+ * cudaMalloc, cudaFree or allocating library routine is called.  nx and ny
+ * must be multiples of 16 with nx * ny <= IBGPU_NOALLOC_MAX_CELLS, else
+ * IBGPU_E_ARG.  The first call on a device looks up that array's address
+ * (once per device, with the device current): make it before any stream
+ * capture.  All calls share the array, which keeps the last call's contents;
+ * calls that overlap on the GPU race, so the caller serialises them.  The
+ * call synchronises `stream` (a cudaStream_t, NULL for the legacy stream)
+ * to return dt and diag. */
+#define IBGPU_NOALLOC_MAX_CELLS 65536
+int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx, int ny,
+                                const double *d_rows_in, double *d_rows_out, double *dt,
+                                ibgpu_diag *diag, void *stream);
+
 const char *ibgpu_errstr(int code);
 /* Last CUDA error string seen by this thread's most recent failing call. */
 const char *ibgpu_last_error(void);
