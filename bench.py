@@ -259,8 +259,7 @@ def our_arm(args):
         if sampler:
             sampler.start()
         ev0.record(stream)
-        for s in range(k):
-            sol.time_marching(first_ts + s)
+        sol.run(first_ts, k)  # k steps back to back, dt kept on the device
         ev1.record(stream)
         ev1.synchronize()
         clocks = sampler.stop() if sampler else None
@@ -269,8 +268,7 @@ def our_arm(args):
 
     # ---- FP64 plain path (headline)
     sol, prim = make(ib.FP64)
-    for ts in range(args.warmup):
-        sol.time_marching(ts)
+    sol.run(0, args.warmup)
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     ms, clocks = timed_steps(sol, args.warmup, args.steps, sampler)
     ms = max_over_ranks(ms)
@@ -279,8 +277,7 @@ def our_arm(args):
     # stage-kernel duration (CUDA events on the launching stream)
     sol.set_kernel_timing(True)
     kt_steps = min(args.steps, 10)
-    for s in range(kt_steps):
-        sol.time_marching(args.warmup + args.steps + s)
+    sol.run(args.warmup + args.steps, kt_steps)
     kms, kn = sol.kernel_times()
     sol.set_kernel_timing(False)
     stage_ms = kms[0] / max(kn[0], 1)
@@ -311,14 +308,12 @@ def our_arm(args):
 
     # ---- mixed precision (FP32 flux/limiter, FP64 accumulation)
     msol, _ = make(ib.MIXED)
-    for ts in range(args.warmup):
-        msol.time_marching(ts)
+    msol.run(0, args.warmup)
     mms, _ = timed_steps(msol, args.warmup, args.steps)
     mms = max_over_ranks(mms)
     mixed_value = ncell * args.steps * ws / (mms / 1e3)
     msol.set_kernel_timing(True)
-    for s in range(kt_steps):
-        msol.time_marching(args.warmup + args.steps + s)
+    msol.run(args.warmup + args.steps, kt_steps)
     mk, mkn = msol.kernel_times()
     msol.close()
 

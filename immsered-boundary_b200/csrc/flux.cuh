@@ -164,9 +164,17 @@ __device__ __forceinline__ void roe_face_flux(const Gas<R> &g, R area,
 template <int LIM, typename R>
 __device__ __forceinline__ R limited_slope(R a, R b) {
   const R ab = a * b;
+  if (LIM == LIM_MINMOD) return (ab > R(0)) ? R(0.5) * (fabs(b) < fabs(a) ? b : a) : R(0);
+  if (sizeof(R) == 4) {
+    // FP32: one MUFU reciprocal, cheaper than a branch; the select discards
+    // the cases where a + b may vanish
+    const R s = ab * FastMath<R>::rcp(a + b);
+    return (ab > R(0)) ? s : R(0);
+  }
+  // FP64: the Newton-refined reciprocal is long, and uniform regions
+  // (a = b = 0) skip it warp-wide
   if (!(ab > R(0))) return R(0);
-  if (LIM == LIM_MINMOD) return R(0.5) * (fabs(b) < fabs(a) ? b : a);
-  return FastMath<R>::div(ab, a + b);
+  return ab * FastMath<R>::rcp(a + b);
 }
 
 // The reference's explicit one-sided reconstructions, used for faces whose
@@ -191,29 +199,33 @@ __device__ __forceinline__ R muscl_right_fast(R q_i, R qi, R qi1) {
 }
 
 // All-speed Roe flux from reconstructed left/right states (rho, u_n, u_t, p).
+// One inverse square root per side gives both 1/rho (a^2) and sqrt(rho)
+// (rho a); the Roe weights are sqrt(rho_L,R) / (sqrt(rho_L) + sqrt(rho_R)),
+// and one inverse root of c^2 gives c and 1/c^2.
 template <typename R>
 __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe, R lun, R lut,
                                                 R lp, R rroe, R run, R rut, R rp, R &f_mass,
                                                 R &f_n, R &f_t, R &f_e) {
   typedef FastMath<R> M;
-  const R ilroe = M::rcp(lroe), irroe = M::rcp(rroe);
-  const R lpr = lp * ilroe, rpr = rp * irroe;          // p / rho
-  const R inv_Rg = g.inv_Rg;
-  const R lT = lpr * inv_Rg, rT = rpr * inv_Rg;
-  const R lke = R(0.5) * (lun * lun + lut * lut), rke = R(0.5) * (run * run + rut * rut);
-  const R le = g.Cv * lT + lke, re = g.Cv * rT + rke;
+  const R aL = M::rsqrt(lroe), aR = M::rsqrt(rroe);
+  const R ilroe = aL * aL, irroe = aR * aR;
+  const R sL = lroe * aL, sR = rroe * aR;  // sqrt(rho)
+  const R lpr = lp * ilroe, rpr = rp * irroe;  // p / rho
+  const R lT = lpr * g.inv_Rg, rT = rpr * g.inv_Rg;
+  const R le = g.Cv * lT + R(0.5) * (lun * lun + lut * lut);
+  const R re = g.Cv * rT + R(0.5) * (run * run + rut * rut);
   const R lv = lun, rv = run;
   const R droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = rv - lv;
-  const R r2lroe = M::sqrt(rroe * ilroe);
-  const R r2l0 = M::rcp(R(1) + r2lroe);
-  const R h_left = le + lpr, h_right = re + rpr;
-  const R a_roe = M::sqrt(lroe * rroe);
-  const R a_un = (lun + run * r2lroe) * r2l0;
-  const R a_ut = (lut + rut * r2lroe) * r2l0;
-  const R a_h = (h_left + h_right * r2lroe) * r2l0;
+  const R isum = M::rcp(sL + sR);
+  const R wL = sL * isum, wR = sR * isum;
+  const R a_roe = sL * sR;
+  const R a_un = lun * wL + run * wR;
+  const R a_ut = lut * wL + rut * wR;
+  const R a_h = (le + lpr) * wL + (re + rpr) * wR;
   const R csquare = g.gm1 * (a_h - R(0.5) * (a_un * a_un + a_ut * a_ut));
-  const R a_c = M::sqrt(csquare);
-  const R icsq = M::rcp(csquare);
+  const R rc = M::rsqrt(csquare);
+  const R a_c = csquare * rc;
+  const R icsq = rc * rc;
   const R ubar = a_un;
   const R namda3 = fabs(ubar);
   const R coef12 = R(0.5) * icsq * area;
@@ -226,7 +238,8 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
   const R Ma_a = fabs(V_a) * M::rsqrt(g.gamaRg * T_a);
   const R f_Ma = smin(smax(Ma_a, g.Ma), R(1));
   const R s0 = (R(1) - f_Ma) * (R(1) - f_Ma);
-  const R namda0 = M::sqrt(R(4) * csquare * f_Ma + s0 * ubar * ubar);
+  const R n0sq = R(4) * csquare * f_Ma + s0 * ubar * ubar;
+  const R namda0 = n0sq * M::rsqrt(n0sq);
   const R namda1 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar + namda0));
   const R namda2 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar - namda0));
   const R alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
@@ -234,14 +247,11 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
   const R alpha3 = alpha0 + alpha1 + alpha2;
   const R alpha4 = a_c * (alpha1 - alpha2);
   const R alphat = faceareaxabsubar * (a_roe * dut);
-  const R pl0 = lroe * lv, pl1 = lroe * lun * lv + lp, pl2 = lroe * lut * lv;
-  const R pl4 = (lp + le * lroe) * lv;
-  const R pr0 = rroe * rv, pr1 = rroe * run * rv + rp, pr2 = rroe * rut * rv;
-  const R pr4 = (rp + re * rroe) * rv;
-  f_mass = (pl0 + pr0) * halffacearea - alpha3;
-  f_n = (pl1 + pr1) * halffacearea - (a_un * alpha3 + alpha4);
-  f_t = (pl2 + pr2) * halffacearea - (a_ut * alpha3 + alphat);
-  f_e = (pl4 + pr4) * halffacearea -
+  const R ml = lroe * lv, mr = rroe * rv;  // mass fluxes of both states
+  f_mass = (ml + mr) * halffacearea - alpha3;
+  f_n = (ml * lun + lp + mr * run + rp) * halffacearea - (a_un * alpha3 + alpha4);
+  f_t = (ml * lut + mr * rut) * halffacearea - (a_ut * alpha3 + alphat);
+  f_e = ((lp + le * lroe) * lv + (rp + re * rroe) * rv) * halffacearea -
         (a_h * alpha3 + ubar * alpha4 + a_ut * alphat - (csquare * g.inv_gm1) * alpha0);
 }
 

@@ -83,7 +83,7 @@ struct ibgpu_ctx {
   std::vector<int64_t> level_normal_cells;
   std::vector<int32_t> h_slot_level, h_slot_ix, h_slot_iy;  // slot -> position (abort reports)
   int32_t *d_tile_nb = nullptr, *d_tile_level = nullptr, *d_cell_slot = nullptr;
-  uint8_t *d_flags = nullptr, *d_cell_alias = nullptr;
+  uint8_t *d_flags = nullptr, *d_cell_alias = nullptr, *d_tile_uniform = nullptr;
 
   // state: step state (6 fields) + two stage buffers (4 fields each)
   double *d_s0[kStateFields] = {};
@@ -165,6 +165,8 @@ struct ibgpu_ctx {
     cudaFree(d_cell_slot);
     cudaFree(d_flags);
     cudaFree(d_cell_alias);
+    cudaFree(d_tile_uniform);
+    d_tile_uniform = nullptr;
     for (auto &p : d_s0) { cudaFree(p); p = nullptr; }
     for (auto &b : d_buf)
       for (auto &p : b) { cudaFree(p); p = nullptr; }
@@ -438,11 +440,30 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       }
     }
   }
-  // 6. device arrays
+  // 6. uniform tiles: the tile and its four side neighbours hold only leaf
+  //    cells that update and recover their primitives (the stage kernel then
+  //    needs no presence flags and no one-sided stencils)
+  const uint8_t kFull = CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM;
+  std::vector<uint8_t> tile_full(ntiles, 0), h_uniform(ntiles, 0);
+  for (int64_t t = 0; t < ntiles; ++t) {
+    bool full = true;
+    for (int i = 0; i < kTileCells && full; ++i) full = h_flags[t * kTileCells + i] == kFull;
+    tile_full[t] = full;
+  }
+  for (int64_t t = 0; t < ntiles; ++t) {
+    bool u = tile_full[t];
+    for (int k : {1, 3, 5, 7}) {
+      int nb = h_nb[t * 9 + k];
+      u = u && nb >= 0 && tile_full[nb];
+    }
+    h_uniform[t] = u;
+  }
+  // 7. device arrays
   int rc;
   if ((rc = dev_alloc(&ctx->d_tile_nb, h_nb.size())) ||
       (rc = dev_alloc(&ctx->d_tile_level, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_flags, (size_t)nslots)) ||
+      (rc = dev_alloc(&ctx->d_tile_uniform, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_cell_slot, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_cell_alias, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)))
@@ -457,6 +478,8 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   CK(cudaMemcpyAsync(ctx->d_tile_nb, h_nb.data(), h_nb.size() * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_tile_level, h_tile_level.data(), ntiles * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_flags, h_flags.data(), nslots, cudaMemcpyHostToDevice, st));
+  if (ntiles > 0)
+    CK(cudaMemcpyAsync(ctx->d_tile_uniform, h_uniform.data(), ntiles, cudaMemcpyHostToDevice, st));
   if (n > 0) {
     CK(cudaMemcpyAsync(ctx->d_cell_slot, cell_slot.data(), n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cell_alias, alias.data(), n, cudaMemcpyHostToDevice, st));
@@ -531,8 +554,8 @@ int ibgpu_kernel_times(const ibgpu_ctx *ctx, double ms_out[3], int64_t launches_
   return IBGPU_OK;
 }
 
-int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
-  if (!ctx || !dt || ts < 0) return IBGPU_E_ARG;
+static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
+  if (!ctx || !dt || ts0 < 0 || nsteps < 1) return IBGPU_E_ARG;
   if (!ctx->has_state) return IBGPU_E_STATE;
   const ibgpu_case &cs = ctx->cs;
   cudaStream_t st = ctx->stream;
@@ -563,6 +586,15 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     if (b) cudaEventRecord(b, st);
   };
 
+  int64_t marched = 0;
+  for (int step = 0; step < nsteps; ++step) {
+  const int ts = ts0 + step;
+  const int pbase = 8 * step;  // abort-order phases of this step
+  if (step > 0) {
+    if (exact) exact::launch_step_begin(ctx->d_diag, st);
+    else fast::launch_step_begin(ctx->d_diag, st);
+  }
+  marched = 0;
   // AMR::InterfaceExchange (AMRInterface.cpp:3-35): restriction of every
   // scheduled pair (coarse level ascending), then prolongation
   for (int l = 0; l + 1 < cs.nlevels && l < (int)ctx->res.size(); ++l) {
@@ -598,6 +630,7 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     ia.out = ctx->d_ib_out;
     ia.n = ctx->n_ib;
     for (int f = 0; f < kStateFields; ++f) ia.s0[f] = ctx->d_s0[f];
+    ia.phase = pbase + 0;
     ia.diag = ctx->d_diag;
     if (exact) exact::launch_ib(ia, ctx->cc, st);
     else fast::launch_ib(ia, ctx->cc, st);
@@ -612,6 +645,7 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     ca.flags = ctx->d_flags;
     for (int f = 0; f < kStateFields; ++f) ca.s0[f] = ctx->d_s0[f];
     ca.nslots = ctx->nslots;
+    ca.phase = pbase + 1;
     ca.diag = ctx->d_diag;
     cudaEvent_t e = mark(2);
     if (exact) exact::launch_cfl(ca, ctx->cc, ctx->nsm, st);
@@ -663,11 +697,11 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
   }
 
   // stages over the tiles of the levels that march at ts
-  int64_t marched = 0;
   StageArgs sa;
   std::memset(&sa, 0, sizeof(sa));
   sa.tile_nb = ctx->d_tile_nb;
   sa.tile_level = ctx->d_tile_level;
+  sa.tile_uniform = ctx->d_tile_uniform;
   sa.flags = ctx->d_flags;
   for (int f = 0; f < kStateFields; ++f) sa.s0[f] = ctx->d_s0[f];
   sa.vsd = ctx->d_vsd;
@@ -682,7 +716,7 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
       sa.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
     }
     sa.tp = cs.tp[k];
-    sa.stage = k;
+    sa.phase = pbase + 2 + k;
     for (int l = 0; l < cs.nlevels; ++l) {
       if (ts % cs.march_step[l] != cs.march_left[l]) continue;
       if (k == 0) marched += ctx->level_normal_cells[l];
@@ -694,6 +728,7 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
       CK(cudaGetLastError());
     }
   }
+  }  // steps
   CK(cudaMemcpyAsync(hd, ctx->d_diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   for (size_t i = 0; i < evs.size(); ++i) {
@@ -706,9 +741,10 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
   }
 
   // decode the first abort in the reference's order
-  int abort_code = 0, abort_slot = -1;
+  int abort_code = 0, abort_slot = -1, abort_step = 0;
   if (hd->err_key != ~0ull) {
     int check = (int)((hd->err_key >> 32) & 0xff);
+    abort_step = (int)((hd->err_key >> 40) / 8);
     abort_slot = (int)(hd->err_key & 0xffffffffull);
     if (check == ERR_IB_NEG_T) abort_code = 1050;
     else if (check == ERR_IB_NAN) abort_code = 1076;
@@ -728,6 +764,7 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     for (int c = 0; c < 5; ++c) std::memcpy(&diag->res_max[c], &hd->res_bits[c], sizeof(double));
     diag->cells_marched = marched;
     diag->abort_code = abort_code;
+    diag->abort_step = abort_step;
     if (abort_code && abort_slot >= 0 && abort_slot < ctx->nslots) {
       diag->abort_level = ctx->h_slot_level[abort_slot];
       diag->abort_ix = ctx->h_slot_ix[abort_slot];
@@ -744,6 +781,14 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
     }
   }
   return IBGPU_OK;
+}
+
+int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
+  return run_steps(ctx, ts, 1, dt, diag);
+}
+
+int ibgpu_run(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
+  return run_steps(ctx, ts0, nsteps, dt, diag);
 }
 
 }  // extern "C"

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
       const double cv1 = un1 + res[1] * level_ts / L.vol;
       const double cv2 = un2 + res[2] * level_ts / L.vol;
       const double cv3 = un3 + res[3] * level_ts / L.vol;
-      if (cv0 < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_RHO, (int)slot);
+      if (cv0 < 0.0) raise_error(a.diag, a.phase, ERR_NEG_RHO, (int)slot);
       if (fl & CF_PRIM) {
         // Get_Prim_Vars (FlowVariables.H:50-57), FP64
         nrho = cv0;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
       wrote = true;
     }
     if (wrote) {
-      if (nT < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_T, (int)slot);
+      if (nT < 0.0) raise_error(a.diag, a.phase, ERR_NEG_T, (int)slot);
       if (FINAL) {
         a.s0[F_RHO][slot] = nrho;
         a.s0[F_U][slot] = nu;
@@ -238,75 +238,206 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
 // reciprocals.  Faces whose outer stencil cell is missing use the
 // reference's one-sided reconstruction (NS_Solver.H:743-750).  The residual,
 // update and primitive recovery run in FP64 in every mode.
+// Four values of one cell (rho, u, v, p), one limited slope set, or one
+// face flux (mass, x-momentum, y-momentum, energy), stored as one 16- or
+// 32-byte shared-memory record so a face reads each operand with one (FP32)
+// or two (FP64) 128-bit loads.
+template <typename R>
+struct __align__(4 * sizeof(R)) Q4 {
+  R x, y, z, w;
+};
+
+template <typename R>
+__device__ __forceinline__ Q4<R> lds4(const Q4<R> *p) {
+  if (sizeof(R) == 4) {
+    float4 t = *reinterpret_cast<const float4 *>(p);
+    return Q4<R>{(R)t.x, (R)t.y, (R)t.z, (R)t.w};
+  } else {
+    double2 a = reinterpret_cast<const double2 *>(p)[0];
+    double2 b = reinterpret_cast<const double2 *>(p)[1];
+    return Q4<R>{(R)a.x, (R)a.y, (R)b.x, (R)b.y};
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void sts4(Q4<R> *p, R x, R y, R z, R w) {
+  if (sizeof(R) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4((float)x, (float)y, (float)z, (float)w);
+  } else {
+    reinterpret_cast<double2 *>(p)[0] = make_double2((double)x, (double)y);
+    reinterpret_cast<double2 *>(p)[1] = make_double2((double)z, (double)w);
+  }
+}
+
+// One face of the stencil region: cells rL1 | rR1 (rL2, rR2 one further
+// out), slope records sL, sR; dir 0 = x (normal u), 1 = y (normal v).
+template <typename R, int LIM>
+__device__ __forceinline__ Q4<R> fast_face(const Q4<R> *sq, const uint8_t *sfl, const Q4<R> *sl,
+                                           int rL1, int rR1, int step, int sL, int sR, bool xdir,
+                                           bool uni, const Gas<R> &g, R area) {
+  bool active = true, hasL2 = true, hasR2 = true;
+  if (!uni) {
+    const uint8_t fL = sfl[rL1], fR = sfl[rR1];
+    active = (fL & CF_PRESENT) && (fR & CF_PRESENT) && ((fL | fR) & CF_NORMAL);
+    hasL2 = (sfl[rL1 - step] & CF_PRESENT) != 0;
+    hasR2 = (sfl[rR1 + step] & CF_PRESENT) != 0;
+  }
+  Q4<R> out = {R(0), R(0), R(0), R(0)};
+  if (!active) return out;
+  const Q4<R> cL = lds4(sq + rL1), cR = lds4(sq + rR1);
+  R ls[4], rs[4];
+  if (hasL2) {
+    const Q4<R> s = lds4(sl + sL);
+    ls[0] = cL.x + s.x; ls[1] = cL.y + s.y; ls[2] = cL.z + s.z; ls[3] = cL.w + s.w;
+  } else {
+    const Q4<R> o = lds4(sq + rR1 + step);
+    ls[0] = muscl_left_fast<LIM>(o.x, cL.x, cR.x);
+    ls[1] = muscl_left_fast<LIM>(o.y, cL.y, cR.y);
+    ls[2] = muscl_left_fast<LIM>(o.z, cL.z, cR.z);
+    ls[3] = muscl_left_fast<LIM>(o.w, cL.w, cR.w);
+  }
+  if (hasR2) {
+    const Q4<R> s = lds4(sl + sR);
+    rs[0] = cR.x - s.x; rs[1] = cR.y - s.y; rs[2] = cR.z - s.z; rs[3] = cR.w - s.w;
+  } else {
+    const Q4<R> o = lds4(sq + rL1 - step);
+    rs[0] = muscl_right_fast<LIM>(cL.x, cR.x, o.x);
+    rs[1] = muscl_right_fast<LIM>(cL.y, cR.y, o.y);
+    rs[2] = muscl_right_fast<LIM>(cL.z, cR.z, o.z);
+    rs[3] = muscl_right_fast<LIM>(cL.w, cR.w, o.w);
+  }
+  R fm, fn, ft, fe;
+  if (xdir) {
+    roe_flux_states<R>(g, area, ls[0], ls[1], ls[2], ls[3], rs[0], rs[1], rs[2], rs[3], fm, fn, ft, fe);
+    out = Q4<R>{fm, fn, ft, fe};
+  } else {
+    roe_flux_states<R>(g, area, ls[0], ls[2], ls[1], ls[3], rs[0], rs[2], rs[1], rs[3], fm, fn, ft, fe);
+    out = Q4<R>{fm, ft, fn, fe};
+  }
+  return out;
+}
+
+// Limited slopes of one cell in one direction (zero where a neighbour is
+// missing; such faces take the one-sided reconstruction instead).
+template <typename R, int LIM>
+__device__ __forceinline__ void fast_slope(const Q4<R> *sq, const uint8_t *sfl, Q4<R> *dst, int rc,
+                                           int step, bool uni) {
+  R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
+  if (uni || ((sfl[rc - step] & CF_PRESENT) && (sfl[rc + step] & CF_PRESENT))) {
+    const Q4<R> m = lds4(sq + rc - step), c = lds4(sq + rc), p = lds4(sq + rc + step);
+    s0 = limited_slope<LIM>(c.x - m.x, p.x - c.x);
+    s1 = limited_slope<LIM>(c.y - m.y, p.y - c.y);
+    s2 = limited_slope<LIM>(c.z - m.z, p.z - c.z);
+    s3 = limited_slope<LIM>(c.w - m.w, p.w - c.w);
+  }
+  sts4(dst, s0, s1, s2, s3);
+}
+
+// Fast build of the stage (FP64 with FastMath divisions/roots, or FP32 flux
+// arithmetic for the mixed mode): per-cell limited slopes computed once and
+// shared by the cell's two faces in each direction, divisions replaced by
+// reciprocals, cell and face records in shared memory as 128-bit vectors,
+// fixed thread-to-cell/face mapping (thread (tx, ty) owns the slopes and the
+// west/south faces of cell (tx, ty); one warp adds the east/north edge).
+// Faces whose outer stencil cell is missing use the reference's one-sided
+// reconstruction (NS_Solver.H:743-750).  The residual, update and primitive
+// recovery run in FP64 in every mode.
 template <typename R, int LIM, bool VISC, bool FINAL>
 __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
-  constexpr int kSlopeX = kTile * (kTile + 2);  // x-slopes: rows 0..15, cols -1..16
-  constexpr int kSlopeY = (kTile + 2) * kTile;  // y-slopes: rows -1..16, cols 0..15
-  __shared__ R sq[4][kReg * kReg];
+  constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
+  __shared__ Q4<R> sq[kReg * kReg];
   __shared__ uint8_t sfl[kReg * kReg];
-  __shared__ R slx[4][kSlopeX];
-  __shared__ R sly[4][kSlopeY];
-  __shared__ R fx[4][kXFaces];
-  __shared__ R fy[4][kYFaces];
+  __shared__ Q4<R> slx[kTile * kSX];      // rows 0..15, cols -1..16
+  __shared__ Q4<R> sly[kSX * kTile];      // rows -1..16, cols 0..15
+  __shared__ Q4<R> fx[kTile * (kTile + 1)];  // x-face (i, j) at j*17 + i
+  __shared__ Q4<R> fy[(kTile + 1) * kTile];  // y-face (i, j) at j*16 + i
 
   const int tid = threadIdx.x;
+  const int tx = tid & (kTile - 1), ty = tid >> 4;
   const int tile = a.tile_begin + blockIdx.x;
   const int lvl = a.tile_level[tile];
   const LevelConst &L = cc.lev[lvl];
+  // uniform tile: it and its four side neighbours hold only leaf cells that
+  // recover their primitives, so no presence flags or one-sided stencils
+  const bool uni = a.tile_uniform != nullptr && a.tile_uniform[tile] != 0;
 
-  for (int r = tid; r < kReg * kReg; r += kTileCells) {
-    int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
-    int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
-    int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
-    uint8_t f = 0;
-    R q0 = R(0), q1 = R(0), q2 = R(0), q3 = R(0);
-    if (!(ox && oy)) {
-      int nb = a.tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
-      if (nb >= 0) {
-        int64_t s = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
-        f = a.flags[s];
-        if (f & CF_PRESENT) {
-          const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
-          q0 = (R)(varying ? a.sin[0] : a.s0[F_RHO])[s];
-          q1 = (R)(varying ? a.sin[1] : a.s0[F_U])[s];
-          q2 = (R)(varying ? a.sin[2] : a.s0[F_V])[s];
-          q3 = (R)(varying ? a.sin[3] : a.s0[F_P])[s];
+  if (uni) {
+    // 768 16-byte loads: the tile's 4 fields (512), the west/east 2-column
+    // strips (128) and the south/north 2-row strips (128)
+#pragma unroll
+    for (int it = 0; it < 3; ++it) {
+      const int w = tid + it * kTileCells;
+      int f, dst;
+      const double *src;
+      if (w < 512) {
+        f = w >> 7;
+        int p = w & 127, row = p >> 3, cp = (p & 7) * 2;
+        src = a.sin[f] + (int64_t)tile * kTileCells + row * kTile + cp;
+        dst = (row + kHalo) * kReg + cp + kHalo;
+      } else if (w < 640) {
+        int v = w - 512;
+        f = v >> 5;
+        int east = (v >> 4) & 1, row = v & 15;
+        int nb = a.tile_nb[tile * 9 + (east ? 5 : 3)];
+        src = a.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
+        dst = (row + kHalo) * kReg + (east ? kTile + kHalo : 0);
+      } else {
+        int v = w - 640;
+        f = v >> 5;
+        int north = (v >> 4) & 1, rr = (v >> 3) & 1, cp = (v & 7) * 2;
+        int nb = a.tile_nb[tile * 9 + (north ? 7 : 1)];
+        int srow = north ? rr : kTile - 2 + rr;
+        src = a.sin[f] + (int64_t)nb * kTileCells + srow * kTile + cp;
+        dst = (north ? kTile + kHalo + rr : rr) * kReg + cp + kHalo;
+      }
+      const double2 val = __ldg(reinterpret_cast<const double2 *>(src));
+      R *c0 = &sq[dst].x, *c1 = &sq[dst + 1].x;
+      c0[f] = (R)val.x;
+      c1[f] = (R)val.y;
+    }
+  } else {
+    for (int r = tid; r < kReg * kReg; r += kTileCells) {
+      int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
+      int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
+      int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
+      uint8_t f = 0;
+      R q0 = R(0), q1 = R(0), q2 = R(0), q3 = R(0);
+      if (!(ox && oy)) {
+        int nb = a.tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
+        if (nb >= 0) {
+          int64_t s = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
+          f = a.flags[s];
+          if (f & CF_PRESENT) {
+            const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
+            q0 = (R)(varying ? a.sin[0] : a.s0[F_RHO])[s];
+            q1 = (R)(varying ? a.sin[1] : a.s0[F_U])[s];
+            q2 = (R)(varying ? a.sin[2] : a.s0[F_V])[s];
+            q3 = (R)(varying ? a.sin[3] : a.s0[F_P])[s];
+          }
         }
       }
+      sfl[r] = f;
+      sts4(&sq[r], q0, q1, q2, q3);
     }
-    sfl[r] = f;
-    sq[0][r] = q0;
-    sq[1][r] = q1;
-    sq[2][r] = q2;
-    sq[3][r] = q3;
   }
   __syncthreads();
 
-  // ---- per-cell limited slopes (valid where both neighbours exist)
-  for (int w = tid; w < kSlopeX + kSlopeY; w += kTileCells) {
-    int rc, step;
-    if (w < kSlopeX) {
-      int row = w / (kTile + 2), col = w % (kTile + 2) - 1;
-      rc = (row + kHalo) * kReg + (col + kHalo);
-      step = 1;
-    } else {
-      int v = w - kSlopeX;
-      int row = v / kTile - 1, col = v % kTile;
-      rc = (row + kHalo) * kReg + (col + kHalo);
-      step = kReg;
-    }
-    R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
-    if ((sfl[rc - step] & CF_PRESENT) && (sfl[rc + step] & CF_PRESENT)) {
-      s0 = limited_slope<LIM>(sq[0][rc] - sq[0][rc - step], sq[0][rc + step] - sq[0][rc]);
-      s1 = limited_slope<LIM>(sq[1][rc] - sq[1][rc - step], sq[1][rc + step] - sq[1][rc]);
-      s2 = limited_slope<LIM>(sq[2][rc] - sq[2][rc - step], sq[2][rc + step] - sq[2][rc]);
-      s3 = limited_slope<LIM>(sq[3][rc] - sq[3][rc - step], sq[3][rc + step] - sq[3][rc]);
-    }
-    if (w < kSlopeX) {
-      slx[0][w] = s0; slx[1][w] = s1; slx[2][w] = s2; slx[3][w] = s3;
-    } else {
-      int v = w - kSlopeX;
-      sly[0][v] = s0; sly[1][v] = s1; sly[2][v] = s2; sly[3][v] = s3;
+  // ---- per-cell limited slopes: (tx, ty) in both directions, then the
+  //      two outer columns (x) and rows (y) of the face stencils
+  {
+    const int rc = (ty + kHalo) * kReg + (tx + kHalo);
+    fast_slope<R, LIM>(sq, sfl, &slx[ty * kSX + tx + 1], rc, 1, uni);
+    fast_slope<R, LIM>(sq, sfl, &sly[(ty + 1) * kTile + tx], rc, kReg, uni);
+    if (tid < 64) {
+      const int e = tid & 15;
+      if (tid < 32) {
+        const int col = (tid < 16) ? -1 : kTile;
+        fast_slope<R, LIM>(sq, sfl, &slx[e * kSX + col + 1], (e + kHalo) * kReg + col + kHalo, 1, uni);
+      } else {
+        const int row = (tid < 48) ? -1 : kTile;
+        fast_slope<R, LIM>(sq, sfl, &sly[(row + 1) * kTile + e], (row + kHalo) * kReg + e + kHalo,
+                           kReg, uni);
+      }
     }
   }
   __syncthreads();
@@ -320,71 +451,46 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
   g.gamaRg = (R)cc.gamaRg;
   g.inv_Rg = (R)(1.0 / cc.Rg);
   g.inv_gm1 = (R)(1.0 / cc.gm1);
+  const R ax = (R)L.area_x, ay = (R)L.area_y;
 
-  // ---- face fluxes
-  for (int w = tid; w < kXFaces + kYFaces; w += kTileCells) {
-    const bool xdir = w < kXFaces;
-    int rL1, rR1, step, sL, sR;  // sL, sR: slope slots of L1 and R1
-    const R(*sl)[kSlopeX];
-    if (xdir) {
-      int j = w / (kTile + 1), i = w % (kTile + 1);
-      rR1 = (j + kHalo) * kReg + (i + kHalo);
-      rL1 = rR1 - 1;
-      step = 1;
-      sR = j * (kTile + 2) + (i + 1);
-      sL = sR - 1;
-      sl = slx;
-    } else {
-      int v = w - kXFaces;
-      int j = v / kTile, i = v % kTile;
-      rR1 = (j + kHalo) * kReg + (i + kHalo);
-      rL1 = rR1 - kReg;
-      step = kReg;
-      sR = (j + 1) * kTile + i;
-      sL = sR - kTile;
-      sl = sly;
-    }
-    const uint8_t fL = sfl[rL1], fR = sfl[rR1];
-    R fm = R(0), fn = R(0), ft = R(0), fe = R(0);
-    if ((fL & CF_PRESENT) && (fR & CF_PRESENT) && ((fL | fR) & CF_NORMAL)) {
-      const int rL2 = rL1 - step, rR2 = rR1 + step;
-      const bool hasL2 = (sfl[rL2] & CF_PRESENT) != 0;
-      const bool hasR2 = (sfl[rR2] & CF_PRESENT) != 0;
-      R ls[4], rs[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        ls[c] = hasL2 ? sq[c][rL1] + sl[c][sL]
-                      : muscl_left_fast<LIM>(sq[c][rR2], sq[c][rL1], sq[c][rR1]);
-        rs[c] = hasR2 ? sq[c][rR1] - sl[c][sR]
-                      : muscl_right_fast<LIM>(sq[c][rL1], sq[c][rR1], sq[c][rL2]);
+  // ---- face fluxes: west x-face and south y-face of cell (tx, ty), plus the
+  //      east column (threads 0..15) and north row (threads 16..31)
+  {
+    const int rR1 = (ty + kHalo) * kReg + (tx + kHalo);
+    fx[ty * (kTile + 1) + tx] =
+        fast_face<R, LIM>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx, ty * kSX + tx + 1, true, uni, g, ax);
+    fy[ty * kTile + tx] = fast_face<R, LIM>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
+                                            (ty + 1) * kTile + tx, false, uni, g, ay);
+    if (tid < 32) {
+      const int e = tid & 15;
+      if (tid < 16) {
+        const int r = (e + kHalo) * kReg + kTile + kHalo;
+        fx[e * (kTile + 1) + kTile] = fast_face<R, LIM>(sq, sfl, slx, r - 1, r, 1, e * kSX + kTile,
+                                                        e * kSX + kTile + 1, true, uni, g, ax);
+      } else {
+        const int r = (kTile + kHalo) * kReg + e + kHalo;
+        fy[kTile * kTile + e] = fast_face<R, LIM>(sq, sfl, sly, r - kReg, r, kReg, kTile * kTile + e,
+                                                  (kTile + 1) * kTile + e, false, uni, g, ay);
       }
-      const int cn = xdir ? 1 : 2, ct = xdir ? 2 : 1;
-      const R area = (R)(xdir ? L.area_x : L.area_y);
-      roe_flux_states<R>(g, area, ls[0], ls[cn], ls[ct], ls[3], rs[0], rs[cn], rs[ct], rs[3],
-                         fm, fn, ft, fe);
-    }
-    if (xdir) {
-      fx[0][w] = fm; fx[1][w] = fn; fx[2][w] = ft; fx[3][w] = fe;
-    } else {
-      int v = w - kXFaces;
-      fy[0][v] = fm; fy[1][v] = ft; fy[2][v] = fn; fy[3][v] = fe;
     }
   }
   __syncthreads();
 
   // ---- residual, update, primitive recovery (FP64)
-  const int lx = tid % kTile, ly = tid / kTile;
   const int64_t slot = (int64_t)tile * kTileCells + tid;
-  const uint8_t fl = sfl[(ly + kHalo) * kReg + (lx + kHalo)];
+  const uint8_t fl = uni ? (uint8_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM)
+                         : sfl[(ty + kHalo) * kReg + (tx + kHalo)];
   unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
   if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
-    const int xlo = ly * (kTile + 1) + lx, xhi = xlo + 1;
-    const int ylo = ly * kTile + lx, yhi = ylo + kTile;
+    const Q4<R> fxl = lds4(&fx[ty * (kTile + 1) + tx]), fxh = lds4(&fx[ty * (kTile + 1) + tx + 1]);
+    const Q4<R> fyl = lds4(&fy[ty * kTile + tx]), fyh = lds4(&fy[(ty + 1) * kTile + tx]);
     double res[4];
+    const R sxl[4] = {fxl.x, fxl.y, fxl.z, fxl.w}, sxh[4] = {fxh.x, fxh.y, fxh.z, fxh.w};
+    const R syl[4] = {fyl.x, fyl.y, fyl.z, fyl.w}, syh[4] = {fyh.x, fyh.y, fyh.z, fyh.w};
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      double sx = (double)fx[c][xlo] - (double)fx[c][xhi];
-      double sy = (double)fy[c][ylo] - (double)fy[c][yhi];
+      double sx = (double)sxl[c] - (double)sxh[c];
+      double sy = (double)syl[c] - (double)syh[c];
       if (VISC) {
         sx += a.vsd[(int64_t)c * a.nslots + slot];
         sy += a.vsd[(int64_t)(4 + c) * a.nslots + slot];
@@ -402,7 +508,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       const double cv1 = orho * ou + res[1] * scale;
       const double cv2 = orho * ov + res[2] * scale;
       const double cv3 = orho * oe + res[3] * scale;
-      if (cv0 < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_RHO, (int)slot);
+      if (cv0 < 0.0) raise_error(a.diag, a.phase, ERR_NEG_RHO, (int)slot);
       if (fl & CF_PRIM) {
         const double ir = FastMath<double>::rcp(cv0);
         nrho = cv0;
@@ -424,7 +530,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       wrote = true;
     }
     if (wrote) {
-      if (nT < 0.0) raise_error(a.diag, 2 + a.stage, ERR_NEG_T, (int)slot);
+      if (nT < 0.0) raise_error(a.diag, a.phase, ERR_NEG_T, (int)slot);
       if (FINAL) {
         a.s0[F_RHO][slot] = nrho;
         a.s0[F_U][slot] = nu;
@@ -467,7 +573,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
     double c1 = (fabs(a.s0[F_V][s]) + c) * L.area_y;
     double c2 = (0.0 + c) * L.area_z;
     double d0 = L.cfl_vol / (c0 + c1 + c2);
-    if (d0 < 0.0) raise_error(a.diag, 1, ERR_CFL_NEG_DT, (int)s);
+    if (d0 < 0.0) raise_error(a.diag, a.phase, ERR_CFL_NEG_DT, (int)s);
     best = (d0 < best) ? d0 : best;  // std::min(CFL_dt, CFL_dt0) ignores NaN
   }
   unsigned long long b = (unsigned long long)__double_as_longlong(best);
@@ -477,6 +583,13 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
     b = w < b ? w : b;
   }
   if ((threadIdx.x & 31) == 0) atomicMin(&a.diag->cfl_bits, b);
+}
+
+// Per-step reset of the step's reductions (the dt and any earlier abort
+// carry over between the steps of one run).
+__global__ void step_begin_kernel(DevDiag *d) {
+  d->cfl_bits = (unsigned long long)__double_as_longlong(10000.0);
+  for (int c = 0; c < 5; ++c) d->res_bits[c] = 0ull;
 }
 
 // dt = min(CFL_dt, dt*dt_ratio) (NS_Solver.cpp:263)
@@ -568,6 +681,8 @@ void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st)
   cfl_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, cc);
   finalize_dt_kernel<<<1, 1, 0, st>>>(a.diag, cc);
 }
+
+void launch_step_begin(DevDiag *d, cudaStream_t st) { step_begin_kernel<<<1, 1, 0, st>>>(d); }
 
 void launch_scatter(const double *rows, const int32_t *cell_slot, const uint8_t *alias, int64_t n,
                     double *const s0[kStateFields], int nsm, cudaStream_t st) {

@@ -50,11 +50,12 @@ struct CaseConst {
 };
 
 // Device-side abort record.  The reference aborts at the first failing
-// check in its sequential order: the CFL pass (NS_Solver.cpp:253), then per
-// stage all density checks (UpdateConsVars) before all temperature checks
-// (ComptNewPrimVar).  err_key = (phase << 40) | (check << 32) | slot with
-// phase 0 for the CFL pass and 1 + k for stage k; the smallest key is the
-// reference's abort.
+// check in its sequential order: the immersed-boundary fill (Body.cpp:1428,
+// 1476), the CFL pass (NS_Solver.cpp:253), then per stage all density checks
+// (UpdateConsVars) before all temperature checks (ComptNewPrimVar).
+// err_key = (phase << 40) | (check << 32) | slot, phase = 8 * step + p with
+// p = 0 for the IB fill, 1 for the CFL pass and 2 + k for stage k; the
+// smallest key is the reference's abort.
 enum : int {
   ERR_IB_NEG_T = 0,    // phase 0: Body::IBConditions_Image, image point T < 0 (1050)
   ERR_IB_NAN = 1,      //          IB cell state NaN (1076)
@@ -75,6 +76,7 @@ constexpr int kHaloStage = 2;
 struct StageArgs {
   const int32_t *tile_nb;  // 9 neighbour tiles per tile, (oy+1)*3+(ox+1); -1 absent
   const int32_t *tile_level;
+  const uint8_t *tile_uniform;  // 1: tile and side neighbours all recovering leaf cells
   const uint8_t *flags;
   int tile_begin;
   double *s0[kStateFields];  // step state rho u v p e T
@@ -83,7 +85,7 @@ struct StageArgs {
   const double *vsd;         // frozen viscous residual parts [8][nslots] or null
   int64_t nslots;
   double tp;                 // stage coefficient tp[k]
-  int stage;                 // k
+  int phase;                 // abort-order phase of this stage (see DevDiag)
   DevDiag *diag;
 };
 
@@ -92,6 +94,7 @@ struct CflArgs {
   const uint8_t *flags;
   const double *s0[kStateFields];
   int64_t nslots;
+  int phase;
   DevDiag *diag;
 };
 
@@ -122,6 +125,7 @@ struct IbArgs {
   double *out;           // 6 per IB cell (rho u v p e T)
   int n;
   double *s0[kStateFields];
+  int phase;
   DevDiag *diag;
 };
 

@@ -188,6 +188,7 @@ extern "C" int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx,
     ca.flags = d_flags;
     for (int f = 0; f < kStateFields; ++f) ca.s0[f] = d_s0 + (int64_t)f * kMaxCells;
     ca.nslots = nslots;
+    ca.phase = 1;
     ca.diag = d_diag;
     if (exact) exact::launch_cfl(ca, cc, nsm, st);
     else fast::launch_cfl(ca, cc, nsm, st);
@@ -210,7 +211,7 @@ extern "C" int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx,
       sa.sout[f] = fin ? nullptr : d_buf + ((int64_t)((k & 1) * 4 + f)) * kMaxCells;
     }
     sa.tp = cs->tp[k];
-    sa.stage = k;
+    sa.phase = 2 + k;
     if (exact) exact::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, false, st);
     else fast::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, mixed, st);
   }
@@ -222,7 +223,7 @@ extern "C" int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx,
   NA_CK(cudaStreamSynchronize(st));
   int abort_code = 0;
   if (hd.err_key != ~0ull) {
-    int check = (int)((hd.err_key >> 32) & 0xff);
+    int check = (int)((hd.err_key >> 32) & 0xff);  // one step: phases 1 (CFL), 2+k
     abort_code = check == ERR_CFL_NEG_DT ? 424 : check == ERR_NEG_T ? 37 : 523;
   }
   for (int c = 0; c < 5; ++c) {

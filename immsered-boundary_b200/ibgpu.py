@@ -88,7 +88,8 @@ class Diag(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("cfl_dt", ctypes.c_double),
                 ("res_max", ctypes.c_double * 5), ("abort_code", ctypes.c_int),
                 ("abort_level", ctypes.c_int), ("abort_ix", ctypes.c_int),
-                ("abort_iy", ctypes.c_int), ("cells_marched", ctypes.c_int64)]
+                ("abort_iy", ctypes.c_int), ("abort_step", ctypes.c_int),
+                ("cells_marched", ctypes.c_int64)]
 
 
 class IbgpuError(RuntimeError):
@@ -130,6 +131,8 @@ def lib(path: str | None = None):
     L.ibgpu_upload_state.argtypes = [vp, vp]
     L.ibgpu_download_state.argtypes = [vp, vp]
     L.ibgpu_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Diag)]
+    L.ibgpu_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(Diag)]
     L.ibgpu_set_kernel_timing.argtypes = [vp, ctypes.c_int]
     L.ibgpu_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_step_periodic_noalloc.argtypes = [ctypes.POINTER(Case), ctypes.c_int, ctypes.c_int,
@@ -324,6 +327,16 @@ class FlowSolver:
         rc = lib().ibgpu_step(self._ctx, int(ts), ctypes.byref(dt), ctypes.byref(d))
         if rc != OK:
             raise IbgpuError(rc, "ibgpu_step", lib().ibgpu_last_error().decode(), d)
+        self.dt = dt.value
+        return d
+
+    def run(self, ts0: int, nsteps: int) -> Diag:
+        """nsteps steps back to back, one host synchronisation at the end."""
+        d = Diag()
+        dt = ctypes.c_double(self.dt)
+        rc = lib().ibgpu_run(self._ctx, int(ts0), int(nsteps), ctypes.byref(dt), ctypes.byref(d))
+        if rc != OK:
+            raise IbgpuError(rc, "ibgpu_run", lib().ibgpu_last_error().decode(), d)
         self.dt = dt.value
         return d
 

@@ -168,6 +168,7 @@ typedef struct ibgpu_diag {
   double res_max[5];  /* ResinDomain max-norm of the residual (unnormalised) */
   int abort_code;     /* reference abort code, 0 if none                     */
   int abort_level, abort_ix, abort_iy;
+  int abort_step;     /* index of the aborting step within an ibgpu_run      */
   int64_t cells_marched; /* leaf cells of the levels that marched           */
 } ibgpu_diag;
 
@@ -212,6 +213,12 @@ int ibgpu_download_state(ibgpu_ctx *ctx, double *prim);
  * *dt is the current dt on entry and the dt used on return (dt =
  * min(CFL_dt, dt*dt_ratio), NS_Solver.cpp:263).  diag may be NULL. */
 int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag);
+
+/* nsteps consecutive steps ts0, ts0+1, ... enqueued back to back with one
+ * host synchronisation at the end: dt stays on the device between steps,
+ * diag reports the last step's reductions and the first abort (with its
+ * step index; the steps after an abort run on but their state is invalid). */
+int ibgpu_run(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag);
 
 /* Event timing of the dominant kernels, accumulated while enabled:
  * kernel 0 = stage update (flux + residual + update + prim recovery),

@@ -323,3 +323,34 @@ def test_topology_errors(cuda_lib, pkg):
     sol.init_flow(np.zeros((0, 7)))
     d = sol.time_marching(0)
     assert d.cells_marched == 0
+
+
+def test_run_equals_single_steps_and_reports_abort_step(cuda_lib, pkg):
+    """ibgpu_run (steps back to back, dt kept on the device) gives exactly the
+    state of the same number of single ibgpu_step calls, and reports an
+    abort with the index of the step that hit it."""
+    ib, wl = pkg.ibgpu, pkg.workloads
+    n = 64
+    P, cells, prim = wl.vortex_case(n, precision=ib.FP64)
+    a = ib.FlowSolver(P)
+    a.upload_topology(**cells)
+    a.init_flow(prim)
+    for ts in range(5):
+        a.time_marching(ts)
+    b = ib.FlowSolver(P)
+    b.upload_topology(**cells)
+    b.init_flow(prim)
+    d = b.run(0, 5)
+    assert d.abort_code == 0 and b.dt == a.dt
+    assert np.array_equal(a.download(), b.download())
+    # over-large dt from step 1 on (CFL evaluated only every 4 steps): the
+    # first step is fine, a later one aborts
+    P2 = dict(P, dt_var_step=4)
+    c = ib.FlowSolver(P2)
+    c.upload_topology(**cells)
+    c.init_flow(prim)
+    c.dt = 1.0
+    with pytest.raises(ib.IbgpuError) as ei:
+        c.run(1, 3)
+    assert ei.value.abort_code in (523, 37)
+    assert ei.value.diag.abort_step == 0
