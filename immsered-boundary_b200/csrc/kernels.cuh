@@ -239,42 +239,61 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
 // reference's one-sided reconstruction (NS_Solver.H:743-750).  The residual,
 // update and primitive recovery run in FP64 in every mode.
 // Four values of one cell (rho, u, v, p), one limited slope set, or one
-// face flux (mass, x-momentum, y-momentum, energy), stored as one 16- or
-// 32-byte shared-memory record so a face reads each operand with one (FP32)
-// or two (FP64) 128-bit loads.
+// face flux (mass, x-momentum, y-momentum, energy).  In shared memory an FP32
+// record is one float4; an FP64 record is split over two double2 planes
+// (components 0-1 at [i], 2-3 at [i + n] for an array of n records), so a
+// warp reading consecutive records moves 16-byte words at a 16-byte stride
+// and every 128-bit access is conflict-free.
 template <typename R>
-struct __align__(4 * sizeof(R)) Q4 {
+struct Q4 {
   R x, y, z, w;
 };
 
 template <typename R>
-__device__ __forceinline__ Q4<R> lds4(const Q4<R> *p) {
-  if (sizeof(R) == 4) {
-    float4 t = *reinterpret_cast<const float4 *>(p);
-    return Q4<R>{(R)t.x, (R)t.y, (R)t.z, (R)t.w};
-  } else {
-    double2 a = reinterpret_cast<const double2 *>(p)[0];
-    double2 b = reinterpret_cast<const double2 *>(p)[1];
-    return Q4<R>{(R)a.x, (R)a.y, (R)b.x, (R)b.y};
-  }
-}
+struct SRec;
 
-template <typename R>
-__device__ __forceinline__ void sts4(Q4<R> *p, R x, R y, R z, R w) {
-  if (sizeof(R) == 4) {
-    *reinterpret_cast<float4 *>(p) = make_float4((float)x, (float)y, (float)z, (float)w);
-  } else {
-    reinterpret_cast<double2 *>(p)[0] = make_double2((double)x, (double)y);
-    reinterpret_cast<double2 *>(p)[1] = make_double2((double)z, (double)w);
+template <>
+struct SRec<float> {
+  using V = float4;
+  static constexpr int kPlanes = 1;
+  static __device__ __forceinline__ Q4<float> ld(const V *a, int i, int) {
+    const float4 t = a[i];
+    return Q4<float>{t.x, t.y, t.z, t.w};
   }
-}
+  static __device__ __forceinline__ void st(V *a, int i, int, float x, float y, float z, float w) {
+    a[i] = make_float4(x, y, z, w);
+  }
+  static __device__ __forceinline__ float *comp(V *a, int i, int, int c) {
+    return reinterpret_cast<float *>(a + i) + c;
+  }
+};
+
+template <>
+struct SRec<double> {
+  using V = double2;
+  static constexpr int kPlanes = 2;
+  static __device__ __forceinline__ Q4<double> ld(const V *a, int i, int n) {
+    const double2 lo = a[i], hi = a[i + n];
+    return Q4<double>{lo.x, lo.y, hi.x, hi.y};
+  }
+  static __device__ __forceinline__ void st(V *a, int i, int n, double x, double y, double z,
+                                            double w) {
+    a[i] = make_double2(x, y);
+    a[i + n] = make_double2(z, w);
+  }
+  static __device__ __forceinline__ double *comp(V *a, int i, int n, int c) {
+    return reinterpret_cast<double *>(a + i + (c >> 1) * n) + (c & 1);
+  }
+};
 
 // One face of the stencil region: cells rL1 | rR1 (rL2, rR2 one further
 // out), slope records sL, sR; dir 0 = x (normal u), 1 = y (normal v).
-template <typename R, int LIM>
-__device__ __forceinline__ Q4<R> fast_face(const Q4<R> *sq, const uint8_t *sfl, const Q4<R> *sl,
-                                           int rL1, int rR1, int step, int sL, int sR, bool xdir,
-                                           bool uni, const Gas<R> &g, R area) {
+template <typename R, int LIM, int NQ, int NS>
+__device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const uint8_t *sfl,
+                                           const typename SRec<R>::V *sl, int rL1, int rR1, int step,
+                                           int sL, int sR, bool xdir, bool uni, const Gas<R> &g,
+                                           R area) {
+  using S = SRec<R>;
   bool active = true, hasL2 = true, hasR2 = true;
   if (!uni) {
     const uint8_t fL = sfl[rL1], fR = sfl[rR1];
@@ -284,23 +303,23 @@ __device__ __forceinline__ Q4<R> fast_face(const Q4<R> *sq, const uint8_t *sfl, 
   }
   Q4<R> out = {R(0), R(0), R(0), R(0)};
   if (!active) return out;
-  const Q4<R> cL = lds4(sq + rL1), cR = lds4(sq + rR1);
+  const Q4<R> cL = S::ld(sq, rL1, NQ), cR = S::ld(sq, rR1, NQ);
   R ls[4], rs[4];
   if (hasL2) {
-    const Q4<R> s = lds4(sl + sL);
+    const Q4<R> s = S::ld(sl, sL, NS);
     ls[0] = cL.x + s.x; ls[1] = cL.y + s.y; ls[2] = cL.z + s.z; ls[3] = cL.w + s.w;
   } else {
-    const Q4<R> o = lds4(sq + rR1 + step);
+    const Q4<R> o = S::ld(sq, rR1 + step, NQ);
     ls[0] = muscl_left_fast<LIM>(o.x, cL.x, cR.x);
     ls[1] = muscl_left_fast<LIM>(o.y, cL.y, cR.y);
     ls[2] = muscl_left_fast<LIM>(o.z, cL.z, cR.z);
     ls[3] = muscl_left_fast<LIM>(o.w, cL.w, cR.w);
   }
   if (hasR2) {
-    const Q4<R> s = lds4(sl + sR);
+    const Q4<R> s = S::ld(sl, sR, NS);
     rs[0] = cR.x - s.x; rs[1] = cR.y - s.y; rs[2] = cR.z - s.z; rs[3] = cR.w - s.w;
   } else {
-    const Q4<R> o = lds4(sq + rL1 - step);
+    const Q4<R> o = S::ld(sq, rL1 - step, NQ);
     rs[0] = muscl_right_fast<LIM>(cL.x, cR.x, o.x);
     rs[1] = muscl_right_fast<LIM>(cL.y, cR.y, o.y);
     rs[2] = muscl_right_fast<LIM>(cL.z, cR.z, o.z);
@@ -319,18 +338,20 @@ __device__ __forceinline__ Q4<R> fast_face(const Q4<R> *sq, const uint8_t *sfl, 
 
 // Limited slopes of one cell in one direction (zero where a neighbour is
 // missing; such faces take the one-sided reconstruction instead).
-template <typename R, int LIM>
-__device__ __forceinline__ void fast_slope(const Q4<R> *sq, const uint8_t *sfl, Q4<R> *dst, int rc,
-                                           int step, bool uni) {
+template <typename R, int LIM, int NQ, int NS>
+__device__ __forceinline__ void fast_slope(const typename SRec<R>::V *sq, const uint8_t *sfl,
+                                           typename SRec<R>::V *sl, int di, int rc, int step,
+                                           bool uni) {
+  using S = SRec<R>;
   R s0 = R(0), s1 = R(0), s2 = R(0), s3 = R(0);
   if (uni || ((sfl[rc - step] & CF_PRESENT) && (sfl[rc + step] & CF_PRESENT))) {
-    const Q4<R> m = lds4(sq + rc - step), c = lds4(sq + rc), p = lds4(sq + rc + step);
+    const Q4<R> m = S::ld(sq, rc - step, NQ), c = S::ld(sq, rc, NQ), p = S::ld(sq, rc + step, NQ);
     s0 = limited_slope<LIM>(c.x - m.x, p.x - c.x);
     s1 = limited_slope<LIM>(c.y - m.y, p.y - c.y);
     s2 = limited_slope<LIM>(c.z - m.z, p.z - c.z);
     s3 = limited_slope<LIM>(c.w - m.w, p.w - c.w);
   }
-  sts4(dst, s0, s1, s2, s3);
+  S::st(sl, di, NS, s0, s1, s2, s3);
 }
 
 // Fast build of the stage (FP64 with FastMath divisions/roots, or FP32 flux
@@ -345,12 +366,15 @@ __device__ __forceinline__ void fast_slope(const Q4<R> *sq, const uint8_t *sfl, 
 template <typename R, int LIM, bool VISC, bool FINAL>
 __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
   constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
-  __shared__ Q4<R> sq[kReg * kReg];
-  __shared__ uint8_t sfl[kReg * kReg];
-  __shared__ Q4<R> slx[kTile * kSX];      // rows 0..15, cols -1..16
-  __shared__ Q4<R> sly[kSX * kTile];      // rows -1..16, cols 0..15
-  __shared__ Q4<R> fx[kTile * (kTile + 1)];  // x-face (i, j) at j*17 + i
-  __shared__ Q4<R> fy[(kTile + 1) * kTile];  // y-face (i, j) at j*16 + i
+  using S = SRec<R>;
+  using V = typename S::V;
+  constexpr int NQ = kReg * kReg, NS = kTile * kSX, NF = kTile * (kTile + 1);
+  __shared__ V sq[S::kPlanes * NQ];
+  __shared__ uint8_t sfl[NQ];
+  __shared__ V slx[S::kPlanes * NS];  // rows 0..15, cols -1..16
+  __shared__ V sly[S::kPlanes * NS];  // rows -1..16, cols 0..15
+  __shared__ V fx[S::kPlanes * NF];   // x-face (i, j) at j*17 + i
+  __shared__ V fy[S::kPlanes * NF];   // y-face (i, j) at j*16 + i
 
   const int tid = threadIdx.x;
   const int tx = tid & (kTile - 1), ty = tid >> 4;
@@ -391,9 +415,8 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
         dst = (north ? kTile + kHalo + rr : rr) * kReg + cp + kHalo;
       }
       const double2 val = __ldg(reinterpret_cast<const double2 *>(src));
-      R *c0 = &sq[dst].x, *c1 = &sq[dst + 1].x;
-      c0[f] = (R)val.x;
-      c1[f] = (R)val.y;
+      *S::comp(sq, dst, NQ, f) = (R)val.x;
+      *S::comp(sq, dst + 1, NQ, f) = (R)val.y;
     }
   } else {
     for (int r = tid; r < kReg * kReg; r += kTileCells) {
@@ -417,7 +440,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
         }
       }
       sfl[r] = f;
-      sts4(&sq[r], q0, q1, q2, q3);
+      S::st(sq, r, NQ, q0, q1, q2, q3);
     }
   }
   __syncthreads();
@@ -426,17 +449,18 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
   //      two outer columns (x) and rows (y) of the face stencils
   {
     const int rc = (ty + kHalo) * kReg + (tx + kHalo);
-    fast_slope<R, LIM>(sq, sfl, &slx[ty * kSX + tx + 1], rc, 1, uni);
-    fast_slope<R, LIM>(sq, sfl, &sly[(ty + 1) * kTile + tx], rc, kReg, uni);
+    fast_slope<R, LIM, NQ, NS>(sq, sfl, slx, ty * kSX + tx + 1, rc, 1, uni);
+    fast_slope<R, LIM, NQ, NS>(sq, sfl, sly, (ty + 1) * kTile + tx, rc, kReg, uni);
     if (tid < 64) {
       const int e = tid & 15;
       if (tid < 32) {
         const int col = (tid < 16) ? -1 : kTile;
-        fast_slope<R, LIM>(sq, sfl, &slx[e * kSX + col + 1], (e + kHalo) * kReg + col + kHalo, 1, uni);
+        fast_slope<R, LIM, NQ, NS>(sq, sfl, slx, e * kSX + col + 1, (e + kHalo) * kReg + col + kHalo,
+                                   1, uni);
       } else {
         const int row = (tid < 48) ? -1 : kTile;
-        fast_slope<R, LIM>(sq, sfl, &sly[(row + 1) * kTile + e], (row + kHalo) * kReg + e + kHalo,
-                           kReg, uni);
+        fast_slope<R, LIM, NQ, NS>(sq, sfl, sly, (row + 1) * kTile + e,
+                                   (row + kHalo) * kReg + e + kHalo, kReg, uni);
       }
     }
   }
@@ -457,20 +481,24 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
   //      east column (threads 0..15) and north row (threads 16..31)
   {
     const int rR1 = (ty + kHalo) * kReg + (tx + kHalo);
-    fx[ty * (kTile + 1) + tx] =
-        fast_face<R, LIM>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx, ty * kSX + tx + 1, true, uni, g, ax);
-    fy[ty * kTile + tx] = fast_face<R, LIM>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
-                                            (ty + 1) * kTile + tx, false, uni, g, ay);
+    Q4<R> o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
+                                        ty * kSX + tx + 1, true, uni, g, ax);
+    S::st(fx, ty * (kTile + 1) + tx, NF, o.x, o.y, o.z, o.w);
+    o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
+                                  (ty + 1) * kTile + tx, false, uni, g, ay);
+    S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
     if (tid < 32) {
       const int e = tid & 15;
       if (tid < 16) {
         const int r = (e + kHalo) * kReg + kTile + kHalo;
-        fx[e * (kTile + 1) + kTile] = fast_face<R, LIM>(sq, sfl, slx, r - 1, r, 1, e * kSX + kTile,
-                                                        e * kSX + kTile + 1, true, uni, g, ax);
+        o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, r - 1, r, 1, e * kSX + kTile,
+                                      e * kSX + kTile + 1, true, uni, g, ax);
+        S::st(fx, e * (kTile + 1) + kTile, NF, o.x, o.y, o.z, o.w);
       } else {
         const int r = (kTile + kHalo) * kReg + e + kHalo;
-        fy[kTile * kTile + e] = fast_face<R, LIM>(sq, sfl, sly, r - kReg, r, kReg, kTile * kTile + e,
-                                                  (kTile + 1) * kTile + e, false, uni, g, ay);
+        o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, r - kReg, r, kReg, kTile * kTile + e,
+                                      (kTile + 1) * kTile + e, false, uni, g, ay);
+        S::st(fy, kTile * kTile + e, NF, o.x, o.y, o.z, o.w);
       }
     }
   }
@@ -482,8 +510,8 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
                          : sfl[(ty + kHalo) * kReg + (tx + kHalo)];
   unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
   if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
-    const Q4<R> fxl = lds4(&fx[ty * (kTile + 1) + tx]), fxh = lds4(&fx[ty * (kTile + 1) + tx + 1]);
-    const Q4<R> fyl = lds4(&fy[ty * kTile + tx]), fyh = lds4(&fy[(ty + 1) * kTile + tx]);
+    const Q4<R> fxl = S::ld(fx, ty * (kTile + 1) + tx, NF), fxh = S::ld(fx, ty * (kTile + 1) + tx + 1, NF);
+    const Q4<R> fyl = S::ld(fy, ty * kTile + tx, NF), fyh = S::ld(fy, (ty + 1) * kTile + tx, NF);
     double res[4];
     const R sxl[4] = {fxl.x, fxl.y, fxl.z, fxl.w}, sxh[4] = {fxh.x, fxh.y, fxh.z, fxh.w};
     const R syl[4] = {fyl.x, fyl.y, fyl.z, fyl.w}, syh[4] = {fyh.x, fyh.y, fyh.z, fyh.w};
