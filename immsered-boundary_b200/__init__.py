@@ -6,6 +6,6 @@ The directory name is not a Python identifier; load it with
 ``importlib`` under the module name ``immsered_boundary_b200`` (tests/,
 bench.py and __graft_entry__.py do so).
 """
-from . import ibgpu, workloads  # noqa: F401
+from . import ibgpu, indicator, workloads  # noqa: F401
 
-__all__ = ["ibgpu", "workloads"]
+__all__ = ["ibgpu", "indicator", "workloads"]

@@ -24,6 +24,7 @@ UNITS = {
     "kernels_fp64.cu": [],
     "kernels_exact.cu": ["-fmad=false"],
     "noalloc.cu": [],
+    "indicator.cu": [],
 }
 
 

@@ -6,7 +6,24 @@
 #include "../../include/ibgpu.h"
 #include "layout.h"
 
+#include <cuda_runtime.h>
+
 namespace ibgpu {
+// Read-only view of a context's device state for the indicator entry points.
+struct CtxView {
+  cudaStream_t stream;
+  int device, nsm;
+  bool has_topology, has_state;
+  const double *s0[kStateFields];
+  const uint8_t *flags;
+  const int32_t *tile_nb;
+  int *aux_err;  // device word: set by a kernel whose wait ran out of time
+  CaseConst cc;
+};
+int ctx_view(const ibgpu_ctx *ctx, CtxView *v);
+// slot of box (l, ix, iy) of the uploaded topology (periodic wrap), -1 if absent
+int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy);
+
 int validate_case(const ibgpu_case *cs);
 void fill_case_const(const ibgpu_case *cs, CaseConst &k);
 void set_last_error(const std::string &msg);

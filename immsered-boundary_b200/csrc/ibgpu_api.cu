@@ -92,6 +92,7 @@ struct ibgpu_ctx {
   double *d_rows = nullptr;  // staging for AoS state transfers
   DevDiag *d_diag = nullptr;
   DevDiag *h_diag = nullptr;  // pinned
+  int *d_aux_err = nullptr;   // time-out flag of the indicator kernels
 
   // slot lookup: per level, tile (tx,ty) -> tile index
   std::vector<std::unordered_map<uint64_t, int>> tilemap;
@@ -242,6 +243,26 @@ void fill_case_const(const ibgpu_case *cs, CaseConst &k) {
 }
 }  // namespace ibgpu
 
+namespace ibgpu {
+int ctx_view(const ibgpu_ctx *ctx, CtxView *v) {
+  if (!ctx || !v) return IBGPU_E_ARG;
+  v->stream = ctx->stream;
+  v->device = ctx->device;
+  v->nsm = ctx->nsm;
+  v->has_topology = ctx->has_topology;
+  v->has_state = ctx->has_state;
+  for (int k = 0; k < kStateFields; ++k) v->s0[k] = ctx->d_s0[k];
+  v->flags = ctx->d_flags;
+  v->tile_nb = ctx->d_tile_nb;
+  v->aux_err = ctx->d_aux_err;
+  v->cc = ctx->cc;
+  return IBGPU_OK;
+}
+int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy) {
+  return ctx ? ctx->slot_at(l, ix, iy) : -1;
+}
+}  // namespace ibgpu
+
 extern "C" {
 
 const char *ibgpu_errstr(int code) {
@@ -253,6 +274,7 @@ const char *ibgpu_errstr(int code) {
     case IBGPU_E_ABORT: return "solver abort condition (see ibgpu_diag.abort_code)";
     case IBGPU_E_NOMEM: return "device allocation failed";
     case IBGPU_E_TOPOLOGY: return "cell list cannot be laid out on the tiled mesh";
+    case IBGPU_E_TIMEOUT: return "device-side wait ran out of its time limit";
     default: return "unknown error";
   }
 }
@@ -273,6 +295,8 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_diag, sizeof(DevDiag));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_diag, sizeof(DevDiag));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_aux_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_aux_err, 0, sizeof(int));
   if (e != cudaSuccess) {
     int rc = cuda_fail(e, "ibgpu_create");
     ibgpu_destroy(c);
@@ -499,6 +523,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   ctx->has_topology = true;
   return IBGPU_OK;
 }
+
 
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles) {
   if (!ctx) return IBGPU_E_ARG;
@@ -1069,6 +1094,7 @@ void ibgpu_destroy(ibgpu_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->free_layout();
   cudaFree(ctx->d_diag);
+  cudaFree(ctx->d_aux_err);
   cudaFreeHost(ctx->h_diag);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;

@@ -1,0 +1,934 @@
+// AMR refinement indicator on the GPU: the plain geometric tag criterion of
+// the case hook AMR::TagtheBox (Userfunction_cy_naca15.cpp:533-650, rftag in
+// Box.H:11-61) and a learned replacement for its per-box decision, a small
+// MLP whose forward and backward passes run on the sm_100a tensor cores
+// (tcgen05.mma, BF16 operands staged in shared memory, FP32 accumulators in
+// Tensor Memory).
+//
+// MLP shapes: X[rows x 112] -> 64 -> 64 -> 3 (padded to 16 output columns).
+// One CTA of 128 threads works on tiles of 128 rows; thread t owns row t of
+// the tile, which is Tensor Memory lane t of every M = 128 accumulator.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/ibgpu.h"
+#include "host_internal.h"
+#include "layout.h"
+#include "tcgen05.cuh"
+
+namespace ibgpu {
+namespace ind {
+
+constexpr int kIn = IBGPU_MLP_IN;         // 112 inputs
+constexpr int kHid = IBGPU_MLP_HIDDEN;    // 64
+constexpr int kOut = IBGPU_MLP_CLASSES;   // 3
+constexpr int kOutPad = 16;               // N of the last layer's MMA
+constexpr int kRows = 128;                // rows per tile = M of every MMA
+constexpr int kThreads = 128;
+constexpr int kOnesRow = kIn;             // row of X^T held at 1 (bias gradients)
+constexpr int kCatN = kHid + kOutPad;     // [dz2 | dz3] columns
+
+// parameter array offsets (floats)
+constexpr int P_W1 = 0;
+constexpr int P_B1 = P_W1 + kHid * kIn;
+constexpr int P_W2 = P_B1 + kHid;
+constexpr int P_B2 = P_W2 + kHid * kHid;
+constexpr int P_W3 = P_B2 + kHid;
+constexpr int P_B3 = P_W3 + kOut * kHid;
+constexpr int P_COUNT = P_B3 + kOut;
+static_assert(P_COUNT == IBGPU_MLP_PARAMS, "parameter layout");
+
+// Tensor Memory columns (f32, one per column, lanes = tile rows)
+constexpr uint32_t T_D1 = 0;      // layer-1 pre-activation   (64)
+constexpr uint32_t T_D2 = 64;     // layer-2 pre-activation   (64)
+constexpr uint32_t T_D3 = 128;    // logits                   (16)
+constexpr uint32_t T_DH2 = 144;   // dL/dh2                   (64)
+constexpr uint32_t T_DH1 = 208;   // dL/dh1                   (64)
+constexpr uint32_t T_GCAT = 272;  // [h1|h2]^T [dz2|dz3]      (80), accumulated
+constexpr uint32_t T_GB = 352;    // X^T [dz2|dz3] (ones row)  (80), accumulated
+constexpr uint32_t T_G1 = 432;    // X^T dz1                  (64), accumulated
+constexpr uint32_t T_COLS_TRAIN = 512;
+constexpr uint32_t T_COLS_FWD = 256;
+static_assert(T_G1 + kHid <= T_COLS_TRAIN, "tensor memory budget");
+
+constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at the boost clock
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+}
+
+// GELU, tanh form (Hendrycks & Gimpel): 0.5 z (1 + tanh(sqrt(2/pi)(z + 0.044715 z^3)))
+constexpr float kGeluA = 0.7978845608028654f;
+constexpr float kGeluB = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float u = kGeluA * (z + kGeluB * z * z * z);
+  return 0.5f * z * (1.0f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float u = kGeluA * (z + kGeluB * z * z * z);
+  const float th = tanhf(u);
+  return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * kGeluA * (1.0f + 3.0f * kGeluB * z * z);
+}
+
+__device__ __forceinline__ void st_bf16(uint8_t *base, int off, float v) {
+  *reinterpret_cast<uint16_t *>(base + off) = bf16_bits(v);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory plan of the training kernel (bytes, 1024-aligned pieces)
+struct TrainSmem {
+  static constexpr int X = 0;                          // [128 x 112] A of layer 1
+  static constexpr int XT = X + kRows * kIn * 2;       // [128 feat x 128 rows] A of dW1, dB
+  static constexpr int H1 = XT + 128 * kRows * 2;      // [128 x 64] A of layer 2; later dz1^T
+  static constexpr int H2 = H1 + kRows * kHid * 2;     // [128 x 64] A of layer 3
+  static constexpr int HT = H2 + kRows * kHid * 2;     // [(h1|h2) 128 x 128 rows] A of dW2|dW3
+  static constexpr int DZ3 = HT + 128 * kRows * 2;     // [128 x 16] A of dh2
+  static constexpr int DZ2 = DZ3 + kRows * kOutPad * 2;  // [128 x 64] A of dh1
+  static constexpr int BCAT = DZ2 + kRows * kHid * 2;  // [80 x 128 rows] B of dW2|dW3, dB
+  static constexpr int W1 = BCAT + kCatN * kRows * 2;  // [64 x 112] B of layer 1
+  static constexpr int W2 = W1 + kHid * kIn * 2;       // [64 x 64]  B of layer 2
+  static constexpr int W2T = W2 + kHid * kHid * 2;     // [64 x 64]  B of dh1
+  static constexpr int W3 = W2T + kHid * kHid * 2;     // [16 x 64]  B of layer 3
+  static constexpr int W3T = W3 + kOutPad * kHid * 2;  // [64 x 16]  B of dh2
+  static constexpr int BIAS = W3T + kHid * kOutPad * 2;  // b1, b2, b3 (f32)
+  // unused tail: keeps every descriptor's reach inside the allocation even
+  // if a tile's stride fields were read the other way round
+  static constexpr int BYTES = BIAS + 1024 + 16384;
+};
+static_assert(TrainSmem::BYTES <= 227 * 1024, "shared memory budget");
+
+struct FwdSmem {
+  static constexpr int X = 0;
+  static constexpr int H1 = X + kRows * kIn * 2;
+  static constexpr int H2 = H1 + kRows * kHid * 2;
+  static constexpr int W1 = H2 + kRows * kHid * 2;
+  static constexpr int W2 = W1 + kHid * kIn * 2;
+  static constexpr int W3 = W2 + kHid * kHid * 2;
+  static constexpr int BIAS = W3 + kOutPad * kHid * 2;
+  static constexpr int BYTES = BIAS + 1024 + 16384;
+};
+
+// Weights (rounded to bf16) into their B-operand tiles; biases as f32.
+__device__ void load_weights(const float *__restrict__ P, uint8_t *sW1, uint8_t *sW2,
+                             uint8_t *sW2T, uint8_t *sW3, uint8_t *sW3T, float *sB) {
+  using tc::kmajor_off;
+  for (int i = threadIdx.x; i < kHid * kIn; i += blockDim.x) {
+    const int o = i / kIn, k = i % kIn;
+    st_bf16(sW1, kmajor_off(kHid, o, k), P[P_W1 + i]);
+  }
+  for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
+    const int o = i / kHid, k = i % kHid;
+    const float w = P[P_W2 + i];
+    st_bf16(sW2, kmajor_off(kHid, o, k), w);
+    if (sW2T) st_bf16(sW2T, kmajor_off(kHid, k, o), w);
+  }
+  for (int i = threadIdx.x; i < kOutPad * kHid; i += blockDim.x) {
+    const int o = i / kHid, j = i % kHid;
+    const float w = (o < kOut) ? P[P_W3 + o * kHid + j] : 0.0f;
+    st_bf16(sW3, kmajor_off(kOutPad, o, j), w);
+    if (sW3T) st_bf16(sW3T, kmajor_off(kHid, j, o), w);
+  }
+  for (int i = threadIdx.x; i < 2 * kHid + 4; i += blockDim.x) {
+    float b = 0.0f;
+    if (i < kHid) b = P[P_B1 + i];
+    else if (i < 2 * kHid) b = P[P_B2 + i - kHid];
+    else if (i - 2 * kHid < kOut) b = P[P_B3 + i - 2 * kHid];
+    sB[i] = b;
+  }
+}
+
+// Issue `ksteps` MMAs of K = 16 over tiles whose K-slab strides are a_lbo /
+// b_lbo bytes (two slabs per step), into Tensor Memory column `col`.
+__device__ __forceinline__ void mma_chain(uint32_t tmem, uint32_t col, const uint8_t *A,
+                                          uint32_t a_lbo, const uint8_t *B, uint32_t b_lbo,
+                                          int ksteps, uint32_t idesc, bool accumulate) {
+  for (int s = 0; s < ksteps; ++s) {
+    const uint64_t ad = tc::smem_desc(A + 2 * s * a_lbo, a_lbo, 128);
+    const uint64_t bd = tc::smem_desc(B + 2 * s * b_lbo, b_lbo, 128);
+    tc::mma_bf16(tmem + col, ad, bd, idesc, (accumulate || s > 0) ? 1u : 0u);
+  }
+}
+
+// Block-wide barrier that also orders tensor-core work across it.
+__device__ __forceinline__ void tc_sync() {
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+}
+
+// Commit the issuing thread's MMAs to the mbarrier and wait for them from
+// every thread; false (uniformly) when the wait ran out of time.
+__device__ __forceinline__ bool commit_and_wait(uint64_t *bar, uint32_t &phase, int *abort_flag) {
+  if (threadIdx.x == 0) tc::mma_commit(bar);
+  const bool ok = tc::mbar_wait_bounded(bar, phase, kWaitCycles);
+  phase ^= 1u;
+  if (!ok) atomicExch(abort_flag, 1);
+  tc_sync();
+  return *(volatile int *)abort_flag == 0;
+}
+
+// 64 f32 columns of this thread's lane starting at `col`, plus bias.
+__device__ __forceinline__ void tmem_row64(uint32_t taddr, const float *bias, float (&v)[64]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t r[16];
+    tc::tmem_ld16(taddr + 16 * q, r);
+    tc::tmem_wait_ld16(r);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[16 * q + e] = __uint_as_float(r[e]) + (bias ? bias[16 * q + e] : 0.0f);
+  }
+}
+
+// Row-major [rows x 64] bf16 A tile: this thread's row from 64 values.
+__device__ __forceinline__ void store_row64(uint8_t *tile, int t, const float (&v)[64]) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint4 w;
+    w.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    w.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    w.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    w.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4 *>(tile + c * (kRows * 16) + t * 16) = w;
+  }
+}
+
+// Feature row -> X (row-major A tile) and optionally X^T (column t).
+__device__ __forceinline__ void load_x_row(const uint16_t *__restrict__ feat, int64_t row, bool valid,
+                                           int t, uint8_t *sX, uint8_t *sXT) {
+  const uint4 *src = reinterpret_cast<const uint4 *>(feat + row * kIn);
+#pragma unroll 2
+  for (int c = 0; c < kIn / 8; ++c) {
+    uint4 w = make_uint4(0u, 0u, 0u, 0u);
+    if (valid) w = __ldg(src + c);
+    *reinterpret_cast<uint4 *>(sX + c * (kRows * 16) + t * 16) = w;
+    if (sXT) {
+      const uint32_t q[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        *reinterpret_cast<uint16_t *>(sXT + tc::kmajor_off(128, 8 * c + e, t)) =
+            (uint16_t)(q[e >> 1] >> (16 * (e & 1)));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient of the class-weighted cross entropy, accumulated over the tiles
+// this CTA processes and added to grad once at the end.
+__global__ void __launch_bounds__(kThreads, 1)
+    mlp_grad_kernel(const float *__restrict__ P, const uint16_t *__restrict__ feat,
+                    const uint8_t *__restrict__ label, int64_t n, float cw0, float cw1, float cw2,
+                    float inv_n, float *__restrict__ grad, float *__restrict__ stats,
+                    int *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int abort_flag;
+  using S = TrainSmem;
+  using tc::kmajor_off;
+  uint8_t *sX = smem + S::X, *sXT = smem + S::XT, *sH1 = smem + S::H1, *sH2 = smem + S::H2,
+          *sHT = smem + S::HT, *sDZ3 = smem + S::DZ3, *sDZ2 = smem + S::DZ2,
+          *sBC = smem + S::BCAT, *sW1 = smem + S::W1, *sW2 = smem + S::W2, *sW2T = smem + S::W2T,
+          *sW3 = smem + S::W3, *sW3T = smem + S::W3T;
+  float *sB = reinterpret_cast<float *>(smem + S::BIAS);
+  uint8_t *sDZ1T = sH1;  // dz1^T [64 x 128 rows] reuses the h1 tile
+  const int t = threadIdx.x;
+
+  load_weights(P, sW1, sW2, sW2T, sW3, sW3T, sB);
+  // constant parts: X^T row 112 = 1 (bias gradients), rows 113..127 = 0;
+  // [dz2|dz3] rows 67..79 = 0; dz3 columns 3..15 = 0
+  for (int f = kIn; f < 128; ++f)
+    *reinterpret_cast<uint16_t *>(sXT + kmajor_off(128, f, t)) = (f == kOnesRow) ? 0x3F80u : 0u;
+  for (int o = kHid + kOut; o < kCatN; ++o)
+    *reinterpret_cast<uint16_t *>(sBC + kmajor_off(kCatN, o, t)) = 0u;
+  *reinterpret_cast<uint4 *>(sDZ3 + 1 * (kRows * 16) + t * 16) = make_uint4(0u, 0u, 0u, 0u);
+  if (t == 0) {
+    tc::mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((t >> 5) == 0) {
+    tc::tmem_alloc(&tbase, T_COLS_TRAIN);
+    tc::tmem_relinquish();
+  }
+  tc::fence_async_smem();
+  tc_sync();
+  const uint32_t tm = tbase;
+  const uint32_t lane_off = (uint32_t)((t & ~31) << 16);  // this warp's lane quarter
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad),
+                 id80 = tc::idesc_bf16_f32(128, kCatN);
+  uint32_t phase = 0;
+  bool first = true, ok = true;
+  float loss = 0.0f, correct = 0.0f;
+  const float cw[3] = {cw0, cw1, cw2};
+
+  for (int64_t tile = blockIdx.x; ok && tile * kRows < n; tile += gridDim.x) {
+    const int64_t row = tile * kRows + t;
+    const bool valid = row < n;
+    load_x_row(feat, row, valid, t, sX, sXT);
+    const int y = valid ? (int)label[row] : -1;
+    const float wy = (y >= 0 && y < kOut) ? cw[y] * inv_n : 0.0f;
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- layer 1: D1 = X W1^T
+    if (t == 0) mma_chain(tm, T_D1, sX, kRows * 16, sW1, kHid * 16, kIn / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float v[64];
+      tmem_row64(tm + lane_off + T_D1, sB, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
+      store_row64(sH1, t, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) st_bf16(sHT, kmajor_off(128, j, t), v[j]);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- layer 2: D2 = H1 W2^T
+    if (t == 0) mma_chain(tm, T_D2, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float v[64];
+      tmem_row64(tm + lane_off + T_D2, sB + kHid, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
+      store_row64(sH2, t, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) st_bf16(sHT, kmajor_off(128, kHid + j, t), v[j]);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- layer 3: logits = H2 W3^T
+    if (t == 0) mma_chain(tm, T_D3, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      uint32_t r[16];
+      tc::tmem_ld16(tm + lane_off + T_D3, r);
+      tc::tmem_wait_ld16(r);
+      float z[3];
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
+      const float m = fmaxf(z[0], fmaxf(z[1], z[2]));
+      float e[3], se = 0.0f;
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) { e[o] = expf(z[o] - m); se += e[o]; }
+      const float inv = 1.0f / se;
+      int am = 0;
+      if (z[1] > z[am]) am = 1;
+      if (z[2] > z[am]) am = 2;
+      float dz[3] = {0.0f, 0.0f, 0.0f};
+      if (wy != 0.0f) {
+        loss += wy * (logf(se) + m - z[y]);
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) dz[o] = wy * (e[o] * inv - (o == y ? 1.0f : 0.0f));
+      }
+      if (valid && y >= 0 && y < kOut && am == y) correct += 1.0f;
+      uint4 w;
+      w.x = pack_bf16(dz[0], dz[1]);
+      w.y = pack_bf16(dz[2], 0.0f);
+      w.z = 0u;
+      w.w = 0u;
+      *reinterpret_cast<uint4 *>(sDZ3 + t * 16) = w;
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) st_bf16(sBC, kmajor_off(kCatN, kHid + o, t), dz[o]);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- dh2 = dz3 W3 (B = W3^T tile)
+    if (t == 0) mma_chain(tm, T_DH2, sDZ3, kRows * 16, sW3T, kHid * 16, 1, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float dh[64], z[64];
+      tmem_row64(tm + lane_off + T_DH2, nullptr, dh);
+      tmem_row64(tm + lane_off + T_D2, sB + kHid, z);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) dh[j] *= gelu_grad(z[j]);
+      store_row64(sDZ2, t, dh);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) st_bf16(sBC, kmajor_off(kCatN, j, t), dh[j]);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- dh1 = dz2 W2; [dW2|dW3]^T += [h1|h2]^T [dz2|dz3]; bias rows
+    if (t == 0) {
+      mma_chain(tm, T_DH1, sDZ2, kRows * 16, sW2T, kHid * 16, kHid / 16, id64, false);
+      mma_chain(tm, T_GCAT, sHT, 128 * 16, sBC, kCatN * 16, kRows / 16, id80, !first);
+      mma_chain(tm, T_GB, sXT, 128 * 16, sBC, kCatN * 16, kRows / 16, id80, !first);
+    }
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float dh[64], z[64];
+      tmem_row64(tm + lane_off + T_DH1, nullptr, dh);
+      tmem_row64(tm + lane_off + T_D1, sB, z);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) st_bf16(sDZ1T, kmajor_off(kHid, j, t), dh[j] * gelu_grad(z[j]));
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    // ---- dW1^T += X^T dz1 (row 112 of X^T gives db1)
+    if (t == 0) mma_chain(tm, T_G1, sXT, 128 * 16, sDZ1T, kHid * 16, kRows / 16, id64, !first);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    first = false;
+  }
+
+  if (ok && !first) {
+    // lane t of the accumulators is input feature t (X^T rows) or hidden
+    // unit t (h1 for t < 64, h2 for t >= 64)
+    float g[64];
+    tmem_row64(tm + lane_off + T_G1, nullptr, g);
+    if (t < kIn) {
+      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_W1 + o * kIn + t], g[o]);
+    } else if (t == kOnesRow) {
+      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_B1 + o], g[o]);
+    }
+    float c[80];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      uint32_t r[16];
+      tc::tmem_ld16(tm + lane_off + T_GCAT + 16 * q, r);
+      tc::tmem_wait_ld16(r);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) c[16 * q + e] = __uint_as_float(r[e]);
+    }
+    if (t < kHid) {
+      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_W2 + o * kHid + t], c[o]);
+    } else {
+      for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_W3 + o * kHid + (t - kHid)], c[kHid + o]);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      uint32_t r[16];
+      tc::tmem_ld16(tm + lane_off + T_GB + 16 * q, r);
+      tc::tmem_wait_ld16(r);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) c[16 * q + e] = __uint_as_float(r[e]);
+    }
+    if (t == kOnesRow) {
+      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_B2 + o], c[o]);
+      for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_B3 + o], c[kHid + o]);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    loss += __shfl_xor_sync(0xffffffffu, loss, off);
+    correct += __shfl_xor_sync(0xffffffffu, correct, off);
+  }
+  if ((t & 31) == 0) {
+    atomicAdd(&stats[0], loss);
+    atomicAdd(&stats[1], correct);
+  }
+  if (!ok) {
+    if (t == 0) atomicExch(err, 1);
+    // let the MMAs already issued finish (bounded) before freeing their memory
+    tc::mbar_wait_bounded(&bar, phase, kWaitCycles);
+  }
+  tc_sync();
+  if ((t >> 5) == 0) tc::tmem_dealloc(tm, T_COLS_TRAIN);
+}
+
+// ---------------------------------------------------------------------------
+// Inference: logits and argmax class per row.
+__global__ void __launch_bounds__(kThreads)
+    mlp_forward_kernel(const float *__restrict__ P, const uint16_t *__restrict__ feat, int64_t n,
+                       uint8_t *__restrict__ cls, float *__restrict__ logits, int *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int abort_flag;
+  using S = FwdSmem;
+  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sH2 = smem + S::H2, *sW1 = smem + S::W1,
+          *sW2 = smem + S::W2, *sW3 = smem + S::W3;
+  float *sB = reinterpret_cast<float *>(smem + S::BIAS);
+  const int t = threadIdx.x;
+  load_weights(P, sW1, sW2, nullptr, sW3, nullptr, sB);
+  if (t == 0) {
+    tc::mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((t >> 5) == 0) {
+    tc::tmem_alloc(&tbase, T_COLS_FWD);
+    tc::tmem_relinquish();
+  }
+  tc::fence_async_smem();
+  tc_sync();
+  const uint32_t tm = tbase;
+  const uint32_t lane_off = (uint32_t)((t & ~31) << 16);
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int64_t tile = blockIdx.x; ok && tile * kRows < n; tile += gridDim.x) {
+    const int64_t row = tile * kRows + t;
+    const bool valid = row < n;
+    load_x_row(feat, row, valid, t, sX, nullptr);
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, T_D1, sX, kRows * 16, sW1, kHid * 16, kIn / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float v[64];
+      tmem_row64(tm + lane_off + T_D1, sB, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
+      store_row64(sH1, t, v);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, T_D2, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float v[64];
+      tmem_row64(tm + lane_off + T_D2, sB + kHid, v);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
+      store_row64(sH2, t, v);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, T_D3, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      uint32_t r[16];
+      tc::tmem_ld16(tm + lane_off + T_D3, r);
+      tc::tmem_wait_ld16(r);
+      float z[3];
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
+      int am = 0;
+      if (z[1] > z[am]) am = 1;
+      if (z[2] > z[am]) am = 2;
+      if (valid) {
+        cls[row] = (uint8_t)am;
+        if (logits) {
+          logits[row * 3 + 0] = z[0];
+          logits[row * 3 + 1] = z[1];
+          logits[row * 3 + 2] = z[2];
+        }
+      }
+    }
+    // the next tile's layer-1 MMA overwrites D1..D3 only after every
+    // thread's loads above (tc_sync at the top of the loop)
+  }
+  if (!ok) {
+    if (t == 0) atomicExch(err, 1);
+    tc::mbar_wait_bounded(&bar, phase, kWaitCycles);
+  }
+  tc_sync();
+  if ((t >> 5) == 0) tc::tmem_dealloc(tm, T_COLS_FWD);
+}
+
+__global__ void adam_kernel(float *__restrict__ P, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, int n, float lr, float c1, float c2) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    P[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain criterion and features.
+
+struct RuleDev {
+  double left, right, yc, half_h;
+  int n_rect, n_rect_c;
+  int torefine[IBGPU_TAG_MAX_LEVELS], toderefine[IBGPU_TAG_MAX_LEVELS];
+  double ru[IBGPU_TAG_MAX_LEVELS], rd[IBGPU_TAG_MAX_LEVELS], rh[IBGPU_TAG_MAX_LEVELS];
+  double bl[IBGPU_TAG_MAX_LEVELS], bh[IBGPU_TAG_MAX_LEVELS], nm[IBGPU_TAG_MAX_LEVELS];
+  double dru[IBGPU_TAG_MAX_LEVELS], drd[IBGPU_TAG_MAX_LEVELS], drh[IBGPU_TAG_MAX_LEVELS];
+  double dbl[IBGPU_TAG_MAX_LEVELS], dbh[IBGPU_TAG_MAX_LEVELS], dnm[IBGPU_TAG_MAX_LEVELS];
+};
+
+__device__ __forceinline__ bool in_region(double x, double y, double sd, int k, int nrect,
+                                          const RuleDev &R, const double *ru, const double *rd,
+                                          const double *rh, const double *bl, const double *bh,
+                                          const double *nm) {
+  if (k < nrect) return x - R.left > -ru[k] && x - R.right < rd[k] && fabs(y - R.yc) < rh[k];
+  bool near = true;
+  if (nm[k] > 0.0) {
+    const double m = nm[k];
+    near = x > R.left - m && x < R.right + m && fabs(y - R.yc) < R.half_h + m;
+  }
+  return near && sd > bl[k] && sd < bh[k];
+}
+
+__global__ void tag_plain_kernel(RuleDev R, int64_t n, const int32_t *__restrict__ lvl,
+                                 const double *__restrict__ xc, const double *__restrict__ yc,
+                                 const double *__restrict__ sd, uint8_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int l = lvl[i];
+    const double x = xc[i], y = yc[i], s = sd[i];
+    uint8_t b = 0;
+    if (R.torefine[l] && in_region(x, y, s, l, R.n_rect, R, R.ru, R.rd, R.rh, R.bl, R.bh, R.nm))
+      b |= IBGPU_TAG_REFINE;
+    if (l >= 1 && R.toderefine[l] &&
+        !in_region(x, y, s, l - 1, R.n_rect_c, R, R.dru, R.drd, R.drh, R.dbl, R.dbh, R.dnm))
+      b |= IBGPU_TAG_COARSEN;
+    out[i] = b;
+  }
+}
+
+struct FeatConst {
+  double inv_rho, inv_c, inv_p;  // freestream scales
+  double left, yc, inv_chord;
+  double dh[IBGPU_TAG_MAX_LEVELS];
+};
+
+__global__ void features_kernel(FeatConst F, int64_t n, const int64_t *__restrict__ slot,
+                                const int32_t *__restrict__ lvl, const double *__restrict__ xc,
+                                const double *__restrict__ yc, const double *__restrict__ sd,
+                                const int32_t *__restrict__ tile_nb,
+                                const uint8_t *__restrict__ flags, const double *__restrict__ rho,
+                                const double *__restrict__ u, const double *__restrict__ v,
+                                const double *__restrict__ p, uint16_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s0 = slot[i];
+    const int tile = (int)(s0 >> 8), lx = (int)(s0 & 15), ly = (int)((s0 >> 4) & 15);
+    uint16_t *o = out + i * kIn;
+    const double cr = rho[s0], cu = u[s0], cv = v[s0], cp = p[s0];
+    for (int dy = -2; dy <= 2; ++dy) {
+      for (int dx = -2; dx <= 2; ++dx) {
+        const int nx = lx + dx, ny = ly + dy;
+        const int ox = nx < 0 ? -1 : (nx >= kTile ? 1 : 0);
+        const int oy = ny < 0 ? -1 : (ny >= kTile ? 1 : 0);
+        const int nb = tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
+        double qr = cr, qu = cu, qv = cv, qp = cp;
+        if (nb >= 0) {
+          const int64_t s = (int64_t)nb * kTileCells + (ny - oy * kTile) * kTile + (nx - ox * kTile);
+          if (flags[s] & CF_PRESENT) {
+            qr = rho[s];
+            qu = u[s];
+            qv = v[s];
+            qp = p[s];
+          }
+        }
+        // separately rounded products and sums (no contraction), so the
+        // features are reproducible on the host
+        const int k = (dy + 2) * 5 + (dx + 2);
+        o[k] = bf16_bits((float)__dadd_rn(__dmul_rn(qr, F.inv_rho), -1.0));
+        o[25 + k] = bf16_bits((float)__dmul_rn(qu, F.inv_c));
+        o[50 + k] = bf16_bits((float)__dmul_rn(qv, F.inv_c));
+        o[75 + k] = bf16_bits((float)__dadd_rn(__dmul_rn(qp, F.inv_p), -1.0));
+      }
+    }
+    const int l = lvl[i];
+    const double s = sd[i];
+    const double a = fmin(fmax(s / F.dh[l], -8.0), 8.0) * 0.125;
+    const double b = fmin(fmax(__dmul_rn(s, F.inv_chord), -4.0), 4.0) * 0.25;
+    const double rx = __dmul_rn(__dmul_rn(__dsub_rn(xc[i], F.left), F.inv_chord), 0.125);
+    const double ry = __dmul_rn(__dmul_rn(__dsub_rn(yc[i], F.yc), F.inv_chord), 0.125);
+    o[100] = bf16_bits((float)a);
+    o[101] = bf16_bits((float)b);
+    o[102] = bf16_bits((float)rx);
+    o[103] = bf16_bits((float)ry);
+    o[104] = bf16_bits((float)fabs(ry));
+    const int lc = l < 6 ? l : 6;
+    for (int e = 0; e < 7; ++e) o[105 + e] = (e == lc) ? (uint16_t)0x3F80u : (uint16_t)0u;
+  }
+}
+
+__global__ void class_to_tag_kernel(const uint8_t *__restrict__ cls, int64_t n,
+                                    uint8_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t c = cls[i];
+    out[i] = c == 0 ? (uint8_t)IBGPU_TAG_REFINE : (c == 1 ? (uint8_t)IBGPU_TAG_COARSEN : (uint8_t)0);
+  }
+}
+
+}  // namespace ind
+}  // namespace ibgpu
+
+// ===========================================================================
+// C ABI
+using namespace ibgpu;
+using namespace ibgpu::ind;
+
+namespace {
+
+int cuda_err(cudaError_t e, const char *what) {
+  set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return IBGPU_E_CUDA;
+}
+#define CKI(call)                                      \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_err(e_, #call); \
+  } while (0)
+
+// Device scratch freed at scope exit.
+struct DevBuf {
+  void *p = nullptr;
+  ~DevBuf() { cudaFree(p); }
+  template <typename T>
+  T *as() { return static_cast<T *>(p); }
+};
+
+int grid_for(int64_t n, int nsm, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)nsm * 8;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+RuleDev to_dev(const ibgpu_tag_rule *r) {
+  RuleDev R;
+  R.left = r->body_left_x;
+  R.right = r->body_right_x;
+  R.yc = r->body_center_y;
+  R.half_h = r->body_half_height;
+  R.n_rect = r->n_rect;
+  R.n_rect_c = r->n_rect_coarsen;
+  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) {
+    R.torefine[k] = r->torefine[k];
+    R.toderefine[k] = r->toderefine[k];
+    R.ru[k] = r->rect_up[k];
+    R.rd[k] = r->rect_down[k];
+    R.rh[k] = r->rect_half[k];
+    R.bl[k] = r->band_lo[k];
+    R.bh[k] = r->band_hi[k];
+    R.nm[k] = r->near_margin[k];
+    R.dru[k] = r->derect_up[k];
+    R.drd[k] = r->derect_down[k];
+    R.drh[k] = r->derect_half[k];
+    R.dbl[k] = r->deband_lo[k];
+    R.dbh[k] = r->deband_hi[k];
+    R.dnm[k] = r->denear_margin[k];
+  }
+  return R;
+}
+
+int check_cells(const ibgpu_tag_cells *c) {
+  if (!c || c->n < 0) return IBGPU_E_ARG;
+  if (c->n == 0) return IBGPU_OK;
+  if (!c->level || !c->xc || !c->yc || !c->signdis) return IBGPU_E_ARG;
+  for (int64_t i = 0; i < c->n; ++i)
+    if (c->level[i] < 0 || c->level[i] >= IBGPU_TAG_MAX_LEVELS) return IBGPU_E_ARG;
+  return IBGPU_OK;
+}
+
+template <typename T>
+int upload(DevBuf &b, const T *h, int64_t n, cudaStream_t st) {
+  CKI(cudaMalloc(&b.p, (size_t)(n > 0 ? n : 1) * sizeof(T)));
+  if (n > 0) CKI(cudaMemcpyAsync(b.p, h, (size_t)n * sizeof(T), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+
+int kernel_error_check(int *d_err, cudaStream_t st) {
+  int h = 0;
+  CKI(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKI(cudaStreamSynchronize(st));
+  if (h) {
+    CKI(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    CKI(cudaStreamSynchronize(st));
+    set_last_error("tensor-core wait ran out of its time limit");
+    return IBGPU_E_TIMEOUT;
+  }
+  return IBGPU_OK;
+}
+
+// opt in to the large dynamic shared-memory carve-out (per device, cheap)
+int configure_smem() {
+  CKI(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           TrainSmem::BYTES));
+  CKI(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           FwdSmem::BYTES));
+  return IBGPU_OK;
+}
+
+int features_impl(const CtxView &V, const ibgpu_ctx *ctx, const ibgpu_tag_rule *rule,
+                  const ibgpu_tag_cells *cells, uint16_t *d_feat) {
+  const int64_t n = cells->n;
+  if (n == 0) return IBGPU_OK;
+  if (!cells->ix || !cells->iy || !d_feat) return IBGPU_E_ARG;
+  if (!V.has_topology || !V.has_state) return IBGPU_E_STATE;
+  std::vector<int64_t> slots((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    slots[i] = ctx_slot_at(ctx, cells->level[i], cells->ix[i], cells->iy[i]);
+    if (slots[i] < 0) {
+      set_last_error("indicator box is not a cell of the uploaded topology");
+      return IBGPU_E_ARG;
+    }
+  }
+  FeatConst F;
+  const double rho_inf = V.cc.initvar[0], p_inf = V.cc.initvar[4];
+  F.inv_rho = 1.0 / rho_inf;
+  F.inv_p = 1.0 / p_inf;
+  F.inv_c = 1.0 / std::sqrt(V.cc.gama * p_inf / rho_inf);
+  F.left = rule->body_left_x;
+  F.yc = rule->body_center_y;
+  F.inv_chord = 1.0 / (rule->body_right_x - rule->body_left_x);
+  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) F.dh[k] = V.cc.lev[k].dx > 0 ? V.cc.lev[k].dx : 1.0;
+  cudaStream_t st = V.stream;
+  DevBuf ds, dl, dx, dy, dsd;
+  int rc;
+  if ((rc = upload(ds, slots.data(), n, st)) || (rc = upload(dl, cells->level, n, st)) ||
+      (rc = upload(dx, cells->xc, n, st)) || (rc = upload(dy, cells->yc, n, st)) ||
+      (rc = upload(dsd, cells->signdis, n, st)))
+    return rc;
+  features_kernel<<<grid_for(n, V.nsm, 128), 128, 0, st>>>(
+      F, n, ds.as<int64_t>(), dl.as<int32_t>(), dx.as<double>(), dy.as<double>(), dsd.as<double>(),
+      V.tile_nb, V.flags, V.s0[F_RHO], V.s0[F_U], V.s0[F_V], V.s0[F_P], d_feat);
+  CKI(cudaGetLastError());
+  CKI(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int launch_grad(const CtxView &V, const float *d_params, int64_t n, const uint16_t *d_feat,
+                const uint8_t *d_label, const float class_weight[3], float *d_grad,
+                float *d_stats) {
+  const int64_t tiles = (n + kRows - 1) / kRows;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)V.nsm);
+  mlp_grad_kernel<<<grid, kThreads, TrainSmem::BYTES, V.stream>>>(
+      d_params, d_feat, d_label, n, class_weight[0], class_weight[1], class_weight[2],
+      (float)(1.0 / (double)n), d_grad, d_stats, V.aux_err);
+  CKI(cudaGetLastError());
+  return IBGPU_OK;
+}
+
+int launch_adam(const CtxView &V, float *d_params, const float *d_grad, float *d_m, float *d_v,
+                int step, float lr) {
+  const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, step)));
+  const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, step)));
+  adam_kernel<<<grid_for(P_COUNT, V.nsm, 256), 256, 0, V.stream>>>(d_params, d_grad, d_m, d_v,
+                                                                   P_COUNT, lr, c1, c2);
+  CKI(cudaGetLastError());
+  return IBGPU_OK;
+}
+
+int forward_impl(const CtxView &V, const float *d_params, int64_t n, const uint16_t *d_feat,
+                 uint8_t *d_class, float *d_logits) {
+  int rc = configure_smem();
+  if (rc) return rc;
+  const int64_t tiles = (n + kRows - 1) / kRows;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)V.nsm * 2);
+  mlp_forward_kernel<<<grid, kThreads, FwdSmem::BYTES, V.stream>>>(d_params, d_feat, n, d_class,
+                                                                   d_logits, V.aux_err);
+  CKI(cudaGetLastError());
+  return kernel_error_check(V.aux_err, V.stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ibgpu_tag_plain(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
+                    uint8_t *out) {
+  CtxView V;
+  if (!rule || ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  int rc = check_cells(cells);
+  if (rc) return rc;
+  const int64_t n = cells->n;
+  if (n == 0) return IBGPU_OK;
+  if (!out) return IBGPU_E_ARG;
+  cudaStream_t st = V.stream;
+  DevBuf dl, dx, dy, dsd, dout;
+  if ((rc = upload(dl, cells->level, n, st)) || (rc = upload(dx, cells->xc, n, st)) ||
+      (rc = upload(dy, cells->yc, n, st)) || (rc = upload(dsd, cells->signdis, n, st)))
+    return rc;
+  CKI(cudaMalloc(&dout.p, (size_t)n));
+  tag_plain_kernel<<<grid_for(n, V.nsm, 256), 256, 0, st>>>(to_dev(rule), n, dl.as<int32_t>(),
+                                                            dx.as<double>(), dy.as<double>(),
+                                                            dsd.as<double>(), dout.as<uint8_t>());
+  CKI(cudaGetLastError());
+  CKI(cudaMemcpyAsync(out, dout.p, (size_t)n, cudaMemcpyDeviceToHost, st));
+  CKI(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_indicator_features(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule,
+                             const ibgpu_tag_cells *cells, uint16_t *d_feat) {
+  CtxView V;
+  if (!rule || ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  int rc = check_cells(cells);
+  if (rc) return rc;
+  return features_impl(V, ctx, rule, cells, d_feat);
+}
+
+int ibgpu_mlp_forward(ibgpu_ctx *ctx, const float *d_params, int64_t n, const uint16_t *d_feat,
+                      uint8_t *d_class, float *d_logits) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK || n < 0) return IBGPU_E_ARG;
+  if (n == 0) return IBGPU_OK;
+  if (!d_params || !d_feat || !d_class) return IBGPU_E_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_feat) & 15u) != 0) return IBGPU_E_ARG;
+  return forward_impl(V, d_params, n, d_feat, d_class, d_logits);
+}
+
+int ibgpu_mlp_grad(ibgpu_ctx *ctx, const float *d_params, int64_t n, const uint16_t *d_feat,
+                   const uint8_t *d_label, const float class_weight[3], float *d_grad,
+                   float *d_stats) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK || n < 0) return IBGPU_E_ARG;
+  if (n == 0) return IBGPU_OK;
+  if (!d_params || !d_feat || !d_label || !class_weight || !d_grad || !d_stats) return IBGPU_E_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_feat) & 15u) != 0) return IBGPU_E_ARG;
+  int rc = configure_smem();
+  if (rc) return rc;
+  rc = launch_grad(V, d_params, n, d_feat, d_label, class_weight, d_grad, d_stats);
+  if (rc) return rc;
+  return kernel_error_check(V.aux_err, V.stream);
+}
+
+int ibgpu_mlp_train_step(ibgpu_ctx *ctx, float *d_params, float *d_m, float *d_v, float *d_grad,
+                         int step, float lr, int64_t n, const uint16_t *d_feat,
+                         const uint8_t *d_label, const float class_weight[3], float *d_stats) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK || n <= 0 || step < 1) return IBGPU_E_ARG;
+  if (!d_params || !d_m || !d_v || !d_grad || !d_feat || !d_label || !class_weight || !d_stats)
+    return IBGPU_E_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_feat) & 15u) != 0) return IBGPU_E_ARG;
+  int rc = configure_smem();
+  if (rc) return rc;
+  CKI(cudaMemsetAsync(d_grad, 0, (size_t)P_COUNT * sizeof(float), V.stream));
+  rc = launch_grad(V, d_params, n, d_feat, d_label, class_weight, d_grad, d_stats);
+  if (rc) return rc;
+  rc = launch_adam(V, d_params, d_grad, d_m, d_v, step, lr);
+  if (rc) return rc;
+  return kernel_error_check(V.aux_err, V.stream);
+}
+
+int ibgpu_mlp_adam(ibgpu_ctx *ctx, float *d_params, const float *d_grad, float *d_m, float *d_v,
+                   int step, float lr) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK || step < 1 || !d_params || !d_grad || !d_m || !d_v)
+    return IBGPU_E_ARG;
+  return launch_adam(V, d_params, d_grad, d_m, d_v, step, lr);
+}
+
+int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
+                      const float *d_params, uint8_t *out) {
+  CtxView V;
+  if (!rule || ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  int rc = check_cells(cells);
+  if (rc) return rc;
+  const int64_t n = cells->n;
+  if (n == 0) return IBGPU_OK;
+  if (!out || !d_params) return IBGPU_E_ARG;
+  DevBuf feat, cls, tags;
+  CKI(cudaMalloc(&feat.p, (size_t)n * kIn * sizeof(uint16_t)));
+  CKI(cudaMalloc(&cls.p, (size_t)n));
+  CKI(cudaMalloc(&tags.p, (size_t)n));
+  if ((rc = features_impl(V, ctx, rule, cells, feat.as<uint16_t>()))) return rc;
+  if ((rc = forward_impl(V, d_params, n, feat.as<uint16_t>(), cls.as<uint8_t>(), nullptr))) return rc;
+  class_to_tag_kernel<<<grid_for(n, V.nsm, 256), 256, 0, V.stream>>>(cls.as<uint8_t>(), n,
+                                                                      tags.as<uint8_t>());
+  CKI(cudaGetLastError());
+  CKI(cudaMemcpyAsync(out, tags.p, (size_t)n, cudaMemcpyDeviceToHost, V.stream));
+  CKI(cudaStreamSynchronize(V.stream));
+  return IBGPU_OK;
+}
+
+}  // extern "C"

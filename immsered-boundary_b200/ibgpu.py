@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libibgpu.so")
 ABI_VERSION = 1
 MAX_LEVELS = 16
 
-OK, E_ARG, E_CUDA, E_STATE, E_ABORT, E_NOMEM, E_TOPOLOGY = 0, -1, -2, -3, -4, -5, -6
+OK, E_ARG, E_CUDA, E_STATE, E_ABORT, E_NOMEM, E_TOPOLOGY, E_TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 LIM_VANLEER, LIM_MINMOD = 0, 1
 FP64, FP64_EXACT, MIXED = 0, 1, 2
 CELL_PRESENT, CELL_NORMAL, CELL_UPDATE, CELL_PRIM, CELL_RESET, CELL_RESNORM, CELL_ALIAS = (
@@ -31,8 +31,13 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_upload_interfaces", "ibgpu_upload_boundaries", "ibgpu_upload_ib",
            "ibgpu_wall_forces", "ibgpu_upload_state", "ibgpu_download_state", "ibgpu_step",
            "ibgpu_set_kernel_timing", "ibgpu_kernel_times", "ibgpu_destroy", "ibgpu_errstr",
-           "ibgpu_last_error", "ibgpu_step_periodic_noalloc")
+           "ibgpu_last_error", "ibgpu_step_periodic_noalloc", "ibgpu_tag_plain",
+           "ibgpu_indicator_features", "ibgpu_mlp_forward", "ibgpu_mlp_grad", "ibgpu_mlp_adam",
+           "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step")
 NOALLOC_MAX_CELLS = 65536
+TAG_MAX_LEVELS = 16
+TAG_REFINE, TAG_COARSEN = 1, 2
+MLP_IN, MLP_STENCIL, MLP_HIDDEN, MLP_CLASSES, MLP_PARAMS = 112, 100, 64, 3, 11587
 
 
 class Case(ctypes.Structure):
@@ -92,6 +97,64 @@ class Diag(ctypes.Structure):
                 ("cells_marched", ctypes.c_int64)]
 
 
+_TL = TAG_MAX_LEVELS
+
+
+class TagRule(ctypes.Structure):
+    """ibgpu_tag_rule: the case hook AMR::TagtheBox as data."""
+    _fields_ = [("body_left_x", ctypes.c_double), ("body_right_x", ctypes.c_double),
+                ("body_center_y", ctypes.c_double), ("body_half_height", ctypes.c_double),
+                ("n_rect", ctypes.c_int), ("n_rect_coarsen", ctypes.c_int),
+                ("torefine", ctypes.c_int * _TL), ("toderefine", ctypes.c_int * _TL),
+                ("rect_up", ctypes.c_double * _TL), ("rect_down", ctypes.c_double * _TL),
+                ("rect_half", ctypes.c_double * _TL), ("band_lo", ctypes.c_double * _TL),
+                ("band_hi", ctypes.c_double * _TL), ("near_margin", ctypes.c_double * _TL),
+                ("derect_up", ctypes.c_double * _TL), ("derect_down", ctypes.c_double * _TL),
+                ("derect_half", ctypes.c_double * _TL), ("deband_lo", ctypes.c_double * _TL),
+                ("deband_hi", ctypes.c_double * _TL), ("denear_margin", ctypes.c_double * _TL)]
+
+
+class TagCells(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("level", ctypes.POINTER(ctypes.c_int32)),
+                ("ix", ctypes.POINTER(ctypes.c_int32)), ("iy", ctypes.POINTER(ctypes.c_int32)),
+                ("xc", ctypes.POINTER(ctypes.c_double)), ("yc", ctypes.POINTER(ctypes.c_double)),
+                ("signdis", ctypes.POINTER(ctypes.c_double))]
+
+
+def make_tag_rule(rule: dict) -> TagRule:
+    """ibgpu_tag_rule from a dict with the same keys (arrays of up to 16)."""
+    r = TagRule()
+    for name, ctype in TagRule._fields_:
+        if name not in rule:
+            continue
+        v = rule[name]
+        if hasattr(ctype, "_length_"):
+            arr = getattr(r, name)
+            vals = np.asarray(v).ravel()
+            for k in range(min(len(vals), ctype._length_)):
+                arr[k] = vals[k].item()
+        else:
+            setattr(r, name, v.item() if hasattr(v, "item") else v)
+    return r
+
+
+class _TagCellsHolder:
+    """Keeps the numpy arrays of a TagCells alive."""
+
+    def __init__(self, level, ix, iy, xc, yc, signdis):
+        self.arrays = [np.ascontiguousarray(level, np.int32), np.ascontiguousarray(ix, np.int32),
+                       np.ascontiguousarray(iy, np.int32), np.ascontiguousarray(xc, np.float64),
+                       np.ascontiguousarray(yc, np.float64),
+                       np.ascontiguousarray(signdis, np.float64)]
+        lv, x, y, a, b, s = self.arrays
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        f64 = ctypes.POINTER(ctypes.c_double)
+        self.s = TagCells(len(lv), lv.ctypes.data_as(i32), x.ctypes.data_as(i32),
+                          y.ctypes.data_as(i32), a.ctypes.data_as(f64), b.ctypes.data_as(f64),
+                          s.ctypes.data_as(f64))
+        self.n = len(lv)
+
+
 class IbgpuError(RuntimeError):
     def __init__(self, code: int, what: str, detail: str = "", diag: Diag | None = None):
         self.code = code
@@ -138,6 +201,15 @@ def lib(path: str | None = None):
     L.ibgpu_step_periodic_noalloc.argtypes = [ctypes.POINTER(Case), ctypes.c_int, ctypes.c_int,
                                               ctypes.c_int, vp, vp, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(Diag), vp]
+    L.ibgpu_tag_plain.argtypes = [vp, ctypes.POINTER(TagRule), ctypes.POINTER(TagCells), vp]
+    L.ibgpu_indicator_features.argtypes = [vp, ctypes.POINTER(TagRule), ctypes.POINTER(TagCells), vp]
+    L.ibgpu_mlp_forward.argtypes = [vp, vp, ctypes.c_int64, vp, vp, vp]
+    L.ibgpu_mlp_grad.argtypes = [vp, vp, ctypes.c_int64, vp, vp, ctypes.POINTER(ctypes.c_float),
+                                 vp, vp]
+    L.ibgpu_mlp_adam.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_float]
+    L.ibgpu_tag_learned.argtypes = [vp, ctypes.POINTER(TagRule), ctypes.POINTER(TagCells), vp, vp]
+    L.ibgpu_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_float,
+                                       ctypes.c_int64, vp, vp, ctypes.POINTER(ctypes.c_float), vp]
     L.ibgpu_destroy.argtypes = [vp]
     L.ibgpu_destroy.restype = None
     L.ibgpu_errstr.argtypes = [ctypes.c_int]
@@ -290,6 +362,60 @@ class FlowSolver:
         ib = Ib(len(c), cp, cfp, len(p), pp, pfp, len(bc), bcp)
         _check(lib().ibgpu_upload_ib(self._ctx, ctypes.byref(ib)), "ibgpu_upload_ib")
         self.nbodies = len(bc)
+
+    # ---- refinement indicator (AMR::TagtheBox and its learned replacement)
+    def tag_plain(self, rule: dict, level, xc, yc, signdis, ix=None, iy=None) -> np.ndarray:
+        """IBGPU_TAG_REFINE | IBGPU_TAG_COARSEN bits per box, computed on the GPU."""
+        z = np.zeros(len(level), np.int32)
+        h = _TagCellsHolder(level, z if ix is None else ix, z if iy is None else iy, xc, yc, signdis)
+        r = make_tag_rule(rule)
+        out = np.zeros(max(h.n, 1), np.uint8)
+        _check(lib().ibgpu_tag_plain(self._ctx, ctypes.byref(r), ctypes.byref(h.s),
+                                     out.ctypes.data_as(ctypes.c_void_p)), "ibgpu_tag_plain")
+        return out[:h.n]
+
+    def indicator_features(self, rule: dict, level, ix, iy, xc, yc, signdis, d_feat: int):
+        """Write the boxes' feature rows (BF16 bits, n x 112) to device address d_feat."""
+        h = _TagCellsHolder(level, ix, iy, xc, yc, signdis)
+        r = make_tag_rule(rule)
+        _check(lib().ibgpu_indicator_features(self._ctx, ctypes.byref(r), ctypes.byref(h.s),
+                                              ctypes.c_void_p(d_feat)), "ibgpu_indicator_features")
+
+    def tag_learned(self, rule: dict, level, ix, iy, xc, yc, signdis, d_params: int) -> np.ndarray:
+        h = _TagCellsHolder(level, ix, iy, xc, yc, signdis)
+        r = make_tag_rule(rule)
+        out = np.zeros(max(h.n, 1), np.uint8)
+        _check(lib().ibgpu_tag_learned(self._ctx, ctypes.byref(r), ctypes.byref(h.s),
+                                       ctypes.c_void_p(d_params), out.ctypes.data_as(ctypes.c_void_p)),
+               "ibgpu_tag_learned")
+        return out[:h.n]
+
+    def mlp_forward(self, d_params: int, n: int, d_feat: int, d_class: int, d_logits: int = 0):
+        _check(lib().ibgpu_mlp_forward(self._ctx, ctypes.c_void_p(d_params), int(n),
+                                       ctypes.c_void_p(d_feat), ctypes.c_void_p(d_class),
+                                       ctypes.c_void_p(d_logits or None)), "ibgpu_mlp_forward")
+
+    def mlp_grad(self, d_params: int, n: int, d_feat: int, d_label: int, class_weight,
+                 d_grad: int, d_stats: int):
+        cw = (ctypes.c_float * 3)(*[float(c) for c in class_weight])
+        _check(lib().ibgpu_mlp_grad(self._ctx, ctypes.c_void_p(d_params), int(n),
+                                    ctypes.c_void_p(d_feat), ctypes.c_void_p(d_label), cw,
+                                    ctypes.c_void_p(d_grad), ctypes.c_void_p(d_stats)),
+               "ibgpu_mlp_grad")
+
+    def mlp_train_step(self, d_params: int, d_m: int, d_v: int, d_grad: int, step: int, lr: float,
+                       n: int, d_feat: int, d_label: int, class_weight, d_stats: int):
+        cw = (ctypes.c_float * 3)(*[float(c) for c in class_weight])
+        _check(lib().ibgpu_mlp_train_step(self._ctx, ctypes.c_void_p(d_params), ctypes.c_void_p(d_m),
+                                          ctypes.c_void_p(d_v), ctypes.c_void_p(d_grad), int(step),
+                                          float(lr), int(n), ctypes.c_void_p(d_feat),
+                                          ctypes.c_void_p(d_label), cw, ctypes.c_void_p(d_stats)),
+               "ibgpu_mlp_train_step")
+
+    def mlp_adam(self, d_params: int, d_grad: int, d_m: int, d_v: int, step: int, lr: float):
+        _check(lib().ibgpu_mlp_adam(self._ctx, ctypes.c_void_p(d_params), ctypes.c_void_p(d_grad),
+                                    ctypes.c_void_p(d_m), ctypes.c_void_p(d_v), int(step),
+                                    float(lr)), "ibgpu_mlp_adam")
 
     def wall_forces(self):
         """(nbodies, 6): force(3), moment(3) in the reference's scaling."""

@@ -112,3 +112,93 @@ def vortex_exact_density(n: int, t: float, beta: float = 5.0, length: float = 10
     gama = g["gama"]
     dT = -(gama - 1.0) * beta * beta / (8.0 * gama * math.pi * math.pi) * np.exp(1.0 - r2)
     return init[0] * np.power(1.0 + dT, 1.0 / (gama - 1.0))
+
+
+def naca_params(g: dict, k: int, precision: int) -> dict:
+    """Case parameters of a NACA0012 AMR run from a mesh/state record of the
+    reference solver (the dict of tests/golden/make_golden.load): gas
+    constants, stage coefficients, level sizes and schedules, domain,
+    body-force scales, and the dt of snapshot k."""
+    s = g["scalars"][k]
+    nst = int(s[14])
+    dom = g["domain"]
+    nlev = int(dom[5])
+    sched = g["schedule"].reshape(-1, 6)
+    dh = g["dh"].reshape(-1, 3)
+    bf = g["body_f"]
+    nb = int(dom[4])
+    return dict(gama=s[4], Rg=s[5], Cv=s[6], Cp=s[7], Ma=s[8], Re=s[9], Pr=s[10], qk=s[11],
+                s_over_t=s[12], cfl=s[13], nstages=nst, tp=list(s[15:15 + nst]),
+                dt_var_step=int(s[15 + nst]), dt_ratio=1.0, limiter=1, viscous=1,
+                precision=precision, initvar=list(g["initvar"]), nlevels=nlev,
+                dh=[tuple(dh[l]) for l in range(nlev)],
+                march_step=[int(sched[l, 0]) for l in range(nlev)],
+                march_left=[int(sched[l, 3]) for l in range(nlev)],
+                step_num=[float(sched[l, 0]) for l in range(nlev)],
+                average_step=[int(sched[l, 1]) for l in range(nlev)],
+                average_left=[int(sched[l, 4]) for l in range(nlev)],
+                prolong_step=[int(sched[l, 2]) for l in range(nlev)],
+                prolong_left=[int(sched[l, 5]) for l in range(nlev)],
+                domain_nx=int(dom[0]), domain_ny=int(dom[1]), periodic_x=int(dom[2]),
+                periodic_y=int(dom[3]), body_level=nlev - 1 if nb > 0 else -1,
+                p_ref=bf[3 * nb], area_ref=bf[3 * nb + 1], shear_ref=bf[3 * nb + 2],
+                L_ref=bf[3 * nb + 3], mu=bf[3 * nb + 4], dt0=float(s[1]))
+
+
+def naca_solver(g: dict, k: int, precision: int):
+    """FlowSolver holding the record's mesh (cell list, coarse/fine pairs,
+    domain ghosts, immersed-boundary cells and wall patches) and snapshot
+    k's state."""
+    ib = ibgpu
+    P = naca_params(g, k, precision)
+    sol = ib.FlowSolver(P)
+    nlev = P["nlevels"]
+    flags = np.zeros(len(g["level"]), np.uint8)
+    for l in range(nlev):
+        m = g["level"] == l
+        flags[m] = ib.cell_flags_from_boxes(g["kind"][m], g["solid"][m], g["infect"][m],
+                                            g["signdis"][m], l == P["body_level"])
+    sol.upload_topology(g["level"], g["ix"], g["iy"], flags)
+    res = g["cf_res"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
+    pro = g["cf_pro"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
+    sol.upload_interfaces(res, pro)
+    bc = g["bc"].reshape(-1, 9)
+    keep = (bc[:, 7] == 0) & (bc[:, 8] == 0)  # x/y faces, z = 0 plane
+    sol.upload_boundaries(bc[keep][:, :7], g["bc_nmv"].reshape(-1, 3)[keep],
+                          g["facevar"].reshape(-1, 7), g["bc_scalars"][0], g["bc_scalars"][1])
+    nb = int(g["domain"][4])
+    sol.upload_ib(g["ib"].reshape(-1, 20)[:, :18], g["ib_f"].reshape(-1, 16),
+                  g["patch"].reshape(-1, 17), g["patch_f"].reshape(-1, 19),
+                  g["body_f"][:3 * nb].reshape(-1, 3))
+    sol.init_flow(g["prim"][k])
+    return sol
+
+
+def naca_tag_rule(nlevels: int, dh, le_x: float = 9.5, le_y: float = 10.0,
+                  chord: float = 1.0) -> dict:
+    """ibgpu_tag_rule of the NACA0012 case's TagtheBox: rectangles (up 4s,
+    down 8s, half-height 4s with s = 0.5^k) around the airfoil on levels
+    k < nlevels-2, then the signed-distance band -3 dh_k < signdis <
+    max(0.25, 16 dh_finest) inside the airfoil box grown by the band's upper
+    limit; coarsening of level l judges against level l-1's region."""
+    L = ibgpu.TAG_MAX_LEVELS
+    z = lambda: np.zeros(L)  # noqa: E731
+    r = dict(body_left_x=le_x, body_right_x=le_x + chord, body_center_y=le_y,
+             body_half_height=0.5 * chord, n_rect=nlevels - 2, n_rect_coarsen=nlevels - 2,
+             torefine=np.zeros(L, np.int32), toderefine=np.zeros(L, np.int32))
+    for pre in ("", "de"):
+        for key in ("rect_up", "rect_down", "rect_half", "band_lo", "band_hi", "near_margin"):
+            r[pre + key] = z()
+    re = max(0.25, 16.0 * float(dh[nlevels - 1]))
+    for k in range(nlevels):
+        s = 0.5 ** k
+        for pre in ("", "de"):
+            r[pre + "rect_up"][k] = 4.0 * s
+            r[pre + "rect_down"][k] = 8.0 * s
+            r[pre + "rect_half"][k] = 4.0 * s
+            r[pre + "band_lo"][k] = -3.0 * float(dh[k])
+            r[pre + "band_hi"][k] = re
+            r[pre + "near_margin"][k] = re
+    r["torefine"][:nlevels] = 1
+    r["toderefine"][1:nlevels] = 1
+    return r

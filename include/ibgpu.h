@@ -43,6 +43,9 @@ extern "C" {
 #define IBGPU_E_NOMEM (-5)     /* device allocation failed                     */
 #define IBGPU_E_TOPOLOGY (-6)  /* cell list cannot be laid out (e.g. periodic
                                   extent not a multiple of the tile edge)      */
+#define IBGPU_E_TIMEOUT (-7)   /* a device-side wait ran out of its time limit;
+                                  the kernel released its resources and the
+                                  context stays usable                         */
 
 /* limiter (Slopelimiter.H): VanLeer is the reference's active ALimiter */
 #define IBGPU_LIM_VANLEER 0
@@ -251,6 +254,114 @@ void ibgpu_destroy(ibgpu_ctx *ctx);
 int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx, int ny,
                                 const double *d_rows_in, double *d_rows_out, double *dt,
                                 ibgpu_diag *diag, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * AMR refinement indicator: the plain (geometric) tag criterion and a learned
+ * replacement for its per-box refine / coarsen / keep decision.
+ * ------------------------------------------------------------------------- */
+
+#define IBGPU_TAG_MAX_LEVELS 16
+#define IBGPU_TAG_REFINE 1  /* rftag::tag   == 0 (AMR::TagtheBox givetag)   */
+#define IBGPU_TAG_COARSEN 2 /* rftag::detag == 0 (AMR::TagtheBox givedetag) */
+
+/* The case hook AMR::TagtheBox (Userfunction_cy_naca15.cpp:533-650) as data.
+ * A box of level l is tagged for refinement when torefine[l] and it lies in
+ * region(l); it is tagged for coarsening when toderefine[l], l >= 1 and it
+ * lies outside the coarsening region of level l-1.  region(k) is, for
+ * k < n_rect, the rectangle
+ *     x - body_left_x > -rect_up[k] && x - body_right_x < rect_down[k] &&
+ *     |y - body_center_y| < rect_half[k]
+ * and otherwise the signed-distance band band_lo[k] < signdis < band_hi[k]
+ * (the shipped case, :560-611), optionally also requiring the centre inside
+ * the body box grown by near_margin[k] when near_margin[k] > 0.  The
+ * coarsening regions use the de* arrays with n_rect_coarsen (:612-635). */
+typedef struct ibgpu_tag_rule {
+  double body_left_x, body_right_x, body_center_y, body_half_height;
+  int n_rect, n_rect_coarsen;
+  int torefine[IBGPU_TAG_MAX_LEVELS], toderefine[IBGPU_TAG_MAX_LEVELS];
+  double rect_up[IBGPU_TAG_MAX_LEVELS], rect_down[IBGPU_TAG_MAX_LEVELS],
+      rect_half[IBGPU_TAG_MAX_LEVELS];
+  double band_lo[IBGPU_TAG_MAX_LEVELS], band_hi[IBGPU_TAG_MAX_LEVELS],
+      near_margin[IBGPU_TAG_MAX_LEVELS];
+  double derect_up[IBGPU_TAG_MAX_LEVELS], derect_down[IBGPU_TAG_MAX_LEVELS],
+      derect_half[IBGPU_TAG_MAX_LEVELS];
+  double deband_lo[IBGPU_TAG_MAX_LEVELS], deband_hi[IBGPU_TAG_MAX_LEVELS],
+      denear_margin[IBGPU_TAG_MAX_LEVELS];
+} ibgpu_tag_rule;
+
+/* Boxes to judge: level and integer position (the learned indicator reads
+ * the 5x5 same-level stencil around (ix, iy) from the context's state), the
+ * box centre as the host mesh holds it (Mesh::bc) and the signed wall
+ * distance (Box::pair.signdis). */
+typedef struct ibgpu_tag_cells {
+  int64_t n;
+  const int32_t *level, *ix, *iy;
+  const double *xc, *yc, *signdis;
+} ibgpu_tag_cells;
+
+/* Plain criterion on the GPU: out[i] = IBGPU_TAG_REFINE | IBGPU_TAG_COARSEN
+ * bits of box i, the (tag, detag) pair AMR::TagtheBox's loops leave in
+ * m_tag.  Host arrays in and out; ctx supplies the stream (may be any
+ * context, no topology needed). */
+int ibgpu_tag_plain(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
+                    uint8_t *out);
+
+/* Learned indicator: an MLP with IBGPU_MLP_IN inputs, two hidden layers of
+ * IBGPU_MLP_HIDDEN with GELU (tanh form) and IBGPU_MLP_CLASSES logits
+ * (0 refine, 1 coarsen, 2 keep), BF16 operands on the tensor cores with FP32
+ * accumulation.  Inputs per box: the 5x5 same-level stencil of (rho, u, v,
+ * p) normalised by the freestream (rho/rho_inf - 1, u/c_inf, v/c_inf,
+ * p/p_inf - 1; an absent stencil cell takes the centre's value), then
+ * signdis/dh clipped to [-8, 8] / 8, signdis/chord clipped to [-4, 4] / 4,
+ * (x - body_left_x)/chord/8, (y - body_center_y)/chord/8, |y -
+ * body_center_y|/chord/8 and a one-hot level (0..6, deeper levels as 6).
+ * Parameters: one FP32 device array of IBGPU_MLP_PARAMS floats, W1[64][112],
+ * b1[64], W2[64][64], b2[64], W3[3][64], b3[3]; weights are rounded to BF16
+ * (nearest even) when a kernel loads them. */
+#define IBGPU_MLP_IN 112
+#define IBGPU_MLP_STENCIL 100
+#define IBGPU_MLP_HIDDEN 64
+#define IBGPU_MLP_CLASSES 3
+#define IBGPU_MLP_PARAMS 11587
+
+/* Feature rows of the boxes (device output, n x IBGPU_MLP_IN BF16 bit
+ * patterns, row-major) from the context's current state; every box must be
+ * a cell of the uploaded topology (else IBGPU_E_ARG). */
+int ibgpu_indicator_features(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule,
+                             const ibgpu_tag_cells *cells, uint16_t *d_feat);
+
+/* Inference on device feature rows: d_class[i] = argmax logit (0 refine,
+ * 1 coarsen, 2 keep); d_logits (n x 3 FP32) may be NULL. */
+int ibgpu_mlp_forward(ibgpu_ctx *ctx, const float *d_params, int64_t n, const uint16_t *d_feat,
+                      uint8_t *d_class, float *d_logits);
+
+/* Gradient of the class-weighted cross entropy
+ *     L = (1/n) * sum_i w[y_i] * -log softmax(z_i)[y_i]
+ * over the n device rows (labels 0..2; a label outside 0..2 contributes
+ * nothing), ADDED to d_grad (IBGPU_MLP_PARAMS floats); d_stats[0] += L,
+ * d_stats[1] += number of rows whose argmax equals the label.  The backward
+ * pass rounds each layer's output gradient to BF16 before its products. */
+int ibgpu_mlp_grad(ibgpu_ctx *ctx, const float *d_params, int64_t n, const uint16_t *d_feat,
+                   const uint8_t *d_label, const float class_weight[3], float *d_grad,
+                   float *d_stats);
+
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) of the
+ * FP32 parameters with moments d_m, d_v, step >= 1. */
+int ibgpu_mlp_adam(ibgpu_ctx *ctx, float *d_params, const float *d_grad, float *d_m, float *d_v,
+                   int step, float lr);
+
+/* One training step: d_grad (IBGPU_MLP_PARAMS floats of scratch) is zeroed,
+ * filled with the minibatch gradient (as ibgpu_mlp_grad) and applied by
+ * ibgpu_mlp_adam at the given step; d_stats as in ibgpu_mlp_grad. */
+int ibgpu_mlp_train_step(ibgpu_ctx *ctx, float *d_params, float *d_m, float *d_v, float *d_grad,
+                         int step, float lr, int64_t n, const uint16_t *d_feat,
+                         const uint8_t *d_label, const float class_weight[3], float *d_stats);
+
+/* Learned tags: the features of the boxes, the MLP and the class mapped to
+ * the plain criterion's bits (refine -> IBGPU_TAG_REFINE, coarsen ->
+ * IBGPU_TAG_COARSEN, keep -> 0); host output. */
+int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
+                      const float *d_params, uint8_t *out);
 
 const char *ibgpu_errstr(int code);
 /* Last CUDA error string seen by this thread's most recent failing call. */

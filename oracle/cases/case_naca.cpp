@@ -113,43 +113,70 @@ void AMR::SetRefineFlag() {
 
 // Plain geometric criterion in the reference's style
 // (Userfunction_cy_naca15.cpp:533-650): boxes around the airfoil on the
-// coarse levels, a signed-distance band on the last refined level.
+// coarse levels, a signed-distance band on the last refined levels; a box of
+// level l >= 1 is marked for coarsening when it lies outside level l-1's
+// refinement region (the shipped case's second loop, :612-635, with this
+// case's regions).  With g_oracle_tag_dump set, the (tag, detag) pair of
+// every normal box is written right after the two loops, before the
+// ghost-consistency clean-up of CheckDetagLocation.
+FILE *g_oracle_tag_dump = nullptr;
+int g_oracle_tag_pass = 0;
+
+static bool naca_region(int k, double x, double y, double celldis) {
+  if (k < max_mesh_level - 2) {
+    double s = pow(0.5, k);
+    double up = 4.0 * s, down = 8.0 * s, half_h = 4.0 * s;
+    return x - kLeX > -up && x - (kLeX + 1.0) < down && fabs(y - kLeY) < half_h;
+  }
+  double rs = -3.0 * dh[k][0];
+  double re = max(0.25, 16.0 * dh[max_mesh_level - 1][0]);
+  // the signed distance is measured along the nearest patch normal, so
+  // bound the band to the airfoil's neighbourhood
+  bool near = x > kLeX - re && x < kLeX + 1.0 + re && fabs(y - kLeY) < 0.5 + re;
+  return near && celldis > rs && celldis < re;
+}
+
 void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
   m_level[ilevel].Inittag();
-  if (!m_level[ilevel].torefine) return;
+  const bool refine = m_level[ilevel].torefine;
+  const bool coarsen = m_level[ilevel].toderefine && ilevel >= 1;
+  if (!refine && !coarsen) return;
   int bs = m_level[ilevel].m_box.ps();
   int be = m_level[ilevel].m_box.pe();
-  int tagnum = 0;
-  if (ilevel < max_mesh_level - 2) {
-    double s = pow(0.5, ilevel);
-    double up = 4.0 * s, down = 8.0 * s, half_h = 4.0 * s;
+  if (refine) {
     for (int i = bs; i < be; ++i) {
       double x = m_mesh.bc(ilevel, i)[0], y = m_mesh.bc(ilevel, i)[1];
-      if (x - kLeX > -up && x - (kLeX + 1.0) < down && fabs(y - kLeY) < half_h) {
+      if (naca_region(ilevel, x, y, m_level[ilevel].m_box[i].pair.signdis)) {
         m_level[ilevel].m_tag[i].givetag();
-        ++tagnum;
-        m_level[ilevel].taggedbox.push_back(i);
-      }
-    }
-  } else {
-    double rs = -3.0 * dh[ilevel][0];
-    double re = max(0.25, 16.0 * dh[max_mesh_level - 1][0]);
-    for (int i = bs; i < be; ++i) {
-      double celldis = m_level[ilevel].m_box[i].pair.signdis;
-      double x = m_mesh.bc(ilevel, i)[0], y = m_mesh.bc(ilevel, i)[1];
-      // the signed distance is measured along the nearest patch normal, so
-      // bound the band to the airfoil's neighbourhood
-      bool near = x > kLeX - re && x < kLeX + 1.0 + re && fabs(y - kLeY) < 0.5 + re;
-      if (near && celldis > rs && celldis < re) {
-        m_level[ilevel].m_tag[i].tag = 0;
-        ++tagnum;
         m_level[ilevel].taggedbox.push_back(i);
       }
     }
   }
+  if (coarsen) {
+    for (int i = bs; i < be; ++i) {
+      double x = m_mesh.bc(ilevel, i)[0], y = m_mesh.bc(ilevel, i)[1];
+      if (!naca_region(ilevel - 1, x, y, m_level[ilevel].m_box[i].pair.signdis))
+        m_level[ilevel].m_tag[i].givedetag();
+    }
+  }
+  if (g_oracle_tag_dump) {
+    for (int i = bs; i < be; ++i) {
+      const Box &b = m_level[ilevel].m_box[i];
+      if (b.iz() != 0) continue;
+      double row[9] = {(double)ilevel, (double)b.ix(), (double)b.iy(), m_mesh.bc(ilevel, i)[0],
+                       m_mesh.bc(ilevel, i)[1], b.pair.signdis,
+                       (double)m_level[ilevel].m_tag[i].tag, (double)m_level[ilevel].m_tag[i].detag,
+                       (double)g_oracle_tag_pass};
+      fwrite(row, sizeof(double), 9, g_oracle_tag_dump);
+    }
+  }
   MPI_Barrier(share_comm);
   CheckDetagLocation(ilevel);
-  if (morelevel && ilevel == m_mesh.MyCurNum() - 2) {
+  // the attach-box consistency check belongs to mesh generation; the tag
+  // dump's pass 1 re-judges a finished mesh, whose attach boxes live one
+  // level up
+  if (!(g_oracle_tag_dump && g_oracle_tag_pass == 1) && refine && morelevel &&
+      ilevel == m_mesh.MyCurNum() - 2) {
     int l0 = m_mesh.MyCurNum() - 2;
     for (size_t i = 0; i < abody.size(); ++i) abody[i].CheckAttachBoxTag(m_level[l0].m_tag, l0, m_mesh);
   }

@@ -83,6 +83,10 @@ void AMR::ADPRule(vector<Body> &) {
 
 void AMR::SetRefineFlag() {}
 
+// single-level case: nothing to tag, nothing to dump
+FILE *g_oracle_tag_dump = nullptr;
+int g_oracle_tag_pass = 0;
+
 void AMR::TagtheBox(const int &ilevel, vector<Body> &) { m_level[ilevel].Inittag(); }
 
 void Body::Motion_Rule(Mesh &, double &) {}

@@ -57,6 +57,8 @@ using namespace std;  // the reference headers assume it (min/max/abs in macros)
 
 extern const double Ma;
 extern double p_ref, area_ref, shear_ref;
+extern FILE *g_oracle_tag_dump;  // defined by the case file (tag dump hook)
+extern int g_oracle_tag_pass;
 
 namespace {
 
@@ -354,6 +356,16 @@ int main(int argc, char **argv) {
   AMR amr(mesh);
   Pltoutput pltfile(mesh);
   pltfile.Design_User_File();
+  // IB_TAG_DUMP=<file>: record the case's TagtheBox decisions, 9 doubles per
+  // normal box (level, ix, iy, centre x, centre y, signdis, tag, detag,
+  // pass): pass 0 while the initial mesh is built (refinement requested
+  // level by level, every box of the level being judged is a leaf), pass 1
+  // re-judging the finished mesh with refinement and coarsening requested
+  const char *tagpath = std::getenv("IB_TAG_DUMP");
+  if (tagpath) {
+    g_oracle_tag_dump = std::fopen(tagpath, "wb");
+    g_oracle_tag_pass = 0;
+  }
   amr.SetupNewAMR(sphere);
   Body::ImmerseWallBoundary(mesh, sphere);
   g_amr = &amr;
@@ -364,6 +376,20 @@ int main(int argc, char **argv) {
   amr.AllocateDataMem();
   if (env_int("IB_USER_INIT", 1)) flowsolver.InitFlow_User();
   else flowsolver.InitFlow();
+
+  if (tagpath) {
+    g_oracle_tag_pass = 1;
+    for (int l = 0; l < mesh.MyCurNum(); ++l) {
+      amr.m_level[l].torefine = true;
+      amr.m_level[l].toderefine = l >= 1;
+      amr.TagtheBox(l, sphere);
+      amr.m_level[l].torefine = false;
+      amr.m_level[l].toderefine = false;
+      amr.m_level[l].Inittag();
+    }
+    std::fclose(g_oracle_tag_dump);
+    g_oracle_tag_dump = nullptr;
+  }
 
   const int nsteps = env_int("IB_STEPS", 5);
   const int timed_from = env_int("IB_TIMED_FROM", 0);  // steps before this are warm-up

@@ -40,6 +40,12 @@ CASES = {
                                                   "IB_STAGES": "4", "IB_USER_INIT": "0",
                                                   "IB_FORCES": "1", "IB_NPTS": "120"}, 4),
 }
+# plain tag criterion only (TagtheBox on the initial mesh, refine and coarsen
+# requested on every level): name -> (binary, environment)
+TAG_CASES = {
+    "naca_tags_n64_l4": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "4", "IB_USER_INIT": "0",
+                                             "IB_NPTS": "200"}),
+}
 # per-case records that do not change between dumps of a static mesh
 AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
        "patch_f", "body_f")
@@ -54,6 +60,7 @@ def run_case(name: str, binary: str, env: dict, steps: int) -> str:
         e.update(env)
         e["IB_STEPS"] = str(steps)
         e["IB_DUMP"] = os.path.join(work, "d")
+        e["IB_TAG_DUMP"] = os.path.join(work, "tags.bin")
         subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
                        stdout=subprocess.DEVNULL)
         snaps = [pyoracle.read_dump(os.path.join(work, f"d_{k:06d}.bin")) for k in range(steps + 1)]
@@ -71,8 +78,33 @@ def run_case(name: str, binary: str, env: dict, steps: int) -> str:
         nf = max(len(s["forces"]) for s in snaps)
         out["forces"] = np.stack([s["forces"] if len(s["forces"]) == nf else np.full(nf, np.nan)
                                   for s in snaps])
+        tags = np.fromfile(os.path.join(work, "tags.bin"), dtype=np.float64).reshape(-1, 9)
+        if len(tags):
+            out["tags"] = tags
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)
+        return path
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_tag_case(name: str, binary: str, env: dict) -> str:
+    """(level, ix, iy, centre x, centre y, signdis, tag, detag, pass) of every
+    normal box, as the case's AMR::TagtheBox leaves them after its loops:
+    pass 0 while the mesh is built, pass 1 re-judging the finished mesh."""
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        e = dict(os.environ)
+        e.update(env)
+        e["IB_STEPS"] = "0"
+        e["IB_DUMP"] = os.path.join(work, "d")
+        e["IB_TAG_DUMP"] = os.path.join(work, "tags.bin")
+        subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
+                       stdout=subprocess.DEVNULL)
+        tags = np.fromfile(os.path.join(work, "tags.bin"), dtype=np.float64).reshape(-1, 9)
+        dh = pyoracle.read_dump(os.path.join(work, "d_000000.bin"))["dh"]
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, tags=tags, dh=dh)
         return path
     finally:
         shutil.rmtree(work, ignore_errors=True)
@@ -92,7 +124,10 @@ def snapshot(g: dict, k: int) -> dict:
 
 
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + list(TAG_CASES)
     for n in names:
-        b, env, steps = CASES[n]
-        print(run_case(n, b, env, steps))
+        if n in TAG_CASES:
+            print(run_tag_case(n, *TAG_CASES[n]))
+        else:
+            b, env, steps = CASES[n]
+            print(run_case(n, b, env, steps))

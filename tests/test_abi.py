@@ -55,6 +55,10 @@ def test_ctypes_layouts_match_c(pkg, tmp_path):
         "ibgpu_cells": (ib.Cells, ["n", "level", "flags"]),
         "ibgpu_diag": (ib.Diag, ["dt", "cfl_dt", "res_max", "abort_code", "abort_iy",
                                  "cells_marched"]),
+        "ibgpu_tag_rule": (ib.TagRule, ["body_half_height", "n_rect", "n_rect_coarsen",
+                                        "torefine", "toderefine", "rect_up", "near_margin",
+                                        "derect_up", "denear_margin"]),
+        "ibgpu_tag_cells": (ib.TagCells, ["n", "level", "iy", "xc", "signdis"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ibgpu.h"', "int main(void){"]
     for cname, (_, fields) in checks.items():

@@ -1,0 +1,196 @@
+"""Refinement indicator on the GPU: the plain criterion against the
+reference's own tags, the learned indicator's features, tensor-core MLP
+forward pass, gradient and Adam step against the CPU oracle, and training
+on the plain criterion's tags."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, ORACLE_DIR, load_pkg
+
+sys.path.insert(0, ORACLE_DIR)
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import indicator_oracle as io  # noqa: E402
+import make_golden  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+pkg = load_pkg()
+ib, wl, ind = pkg.ibgpu, pkg.workloads, pkg.indicator
+NAME = "naca_minmod_s4_n64_l3"
+# logits: FP32 accumulation of BF16 products vs the FP64 oracle, plus the
+# rare BF16 rounding flip of a hidden activation (2^-8 relative)
+LOGIT_TOL = 2e-3
+GRAD_REL_TOL = 1e-2
+
+
+def tag_rows(name):
+    with np.load(os.path.join(GOLDEN_DIR, name + ".npz")) as z:
+        return z["tags"], z["dh"].reshape(-1, 3)[:, 0]
+
+
+def boxes_of(t):
+    return dict(level=t[:, 0].astype(np.int32), ix=t[:, 1].astype(np.int32),
+                iy=t[:, 2].astype(np.int32), xc=t[:, 3], yc=t[:, 4], signdis=t[:, 5])
+
+
+@pytest.fixture(scope="module")
+def naca():
+    g = make_golden.load(NAME)
+    sol = wl.naca_solver(g, 0, ib.FP64)
+    yield g, sol
+    sol.close()
+
+
+@pytest.mark.parametrize("name,nlev", [("naca_minmod_s4_n64_l3", 3), ("naca_tags_n64_l4", 4)])
+def test_tag_plain_gpu_matches_reference(cuda_lib, naca, name, nlev):
+    _, sol = naca
+    t, dh = tag_rows(name)
+    rule = wl.naca_tag_rule(nlev, dh)
+    for p in (0, 1):
+        m = t[:, 8] == p
+        r = dict(rule)
+        if p == 0:  # the mesh build requests refinement only
+            r["toderefine"] = np.zeros(ib.TAG_MAX_LEVELS, np.int32)
+        got = sol.tag_plain(r, t[m, 0].astype(np.int32), t[m, 3], t[m, 4], t[m, 5])
+        ref = io.tags_from_rftag(t[m, 6], t[m, 7])
+        assert np.array_equal(got, ref), f"pass {p}: {np.sum(got != ref)} boxes differ"
+
+
+def oracle_state(g, prim):
+    return {(int(l), int(x), int(y)): (r[0], r[1], r[2], r[4])
+            for l, x, y, r in zip(g["level"], g["ix"], g["iy"], prim)}
+
+
+def test_features_match_oracle(cuda_lib, naca):
+    import torch
+    g, sol = naca
+    t, dh = tag_rows(NAME)
+    t = t[t[:, 8] == 1][::7]
+    rule = wl.naca_tag_rule(3, dh)
+    B = boxes_of(t)
+    feat = torch.empty((len(t), ib.MLP_IN), dtype=torch.int16, device="cuda")
+    sol.indicator_features(rule, B["level"], B["ix"], B["iy"], B["xc"], B["yc"], B["signdis"],
+                           feat.data_ptr())
+    got = feat.cpu().numpy().view(np.uint16)
+    prim = sol.download()
+    ref = io.features(oracle_state(g, prim), B, io.naca_rule(3, dh), g["initvar"],
+                      float(g["scalars"][0][4]), dh)
+    assert np.array_equal(got, ref), f"{np.sum(np.any(got != ref, axis=1))} rows differ"
+
+
+def random_problem(n, seed):
+    rng = np.random.default_rng(seed)
+    P = ind.init_params(seed)
+    P[io.P_B1:io.P_W2] = rng.normal(0, 0.1, io.N_HID)
+    P[io.P_B2:io.P_W3] = rng.normal(0, 0.1, io.N_HID)
+    P[io.P_B3:io.P_COUNT] = rng.normal(0, 0.1, io.N_OUT)
+    X = io.bf16_bits(rng.normal(0, 1, (n, io.N_IN)))
+    y = rng.integers(0, 3, n).astype(np.uint8)
+    return P, X, y
+
+
+def to_dev(a, dtype):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda") if dtype is None else \
+        torch.from_numpy(np.ascontiguousarray(a).view(dtype)).to("cuda")
+
+
+@pytest.mark.parametrize("n", [1, 128, 1000])
+def test_mlp_forward_matches_oracle(cuda_lib, naca, n):
+    _, sol = naca
+    P, X, _ = random_problem(n, 11 + n)
+    li = ind.LearnedIndicator(sol, params=P)
+    Xd = to_dev(X, np.int16)
+    cls, logits = li.predict(Xd, logits=True)
+    ref, _ = io.mlp_forward(P, X_bits=X)
+    assert np.abs(logits - ref).max() <= LOGIT_TOL * max(1.0, np.abs(ref).max())
+    srt = np.sort(ref, axis=1)
+    clear = (srt[:, 2] - srt[:, 1]) > 1e-2
+    assert np.array_equal(cls[clear], np.argmax(ref, axis=1)[clear])
+
+
+@pytest.mark.parametrize("n", [200, 3000])
+def test_mlp_gradient_matches_oracle(cuda_lib, naca, n):
+    _, sol = naca
+    P, X, y = random_problem(n, 5 + n)
+    y[::17] = 255  # unlabelled rows contribute nothing
+    cw = np.array([1.0, 3.0, 0.7], np.float32)
+    li = ind.LearnedIndicator(sol, params=P)
+    loss, g, correct = li.gradient(to_dev(X, np.int16), y, cw)
+    rloss, rg, rcorrect = io.mlp_loss_grad(P, y, cw.astype(np.float64), X_bits=X)
+    assert abs(loss - rloss) <= 1e-4 * abs(rloss)
+    assert abs(correct - rcorrect) <= max(2, n // 500)
+    blocks = [("W1", io.P_W1, io.P_B1), ("b1", io.P_B1, io.P_W2), ("W2", io.P_W2, io.P_B2),
+              ("b2", io.P_B2, io.P_W3), ("W3", io.P_W3, io.P_B3), ("b3", io.P_B3, io.P_COUNT)]
+    for name, a, b in blocks:
+        err = np.linalg.norm(g[a:b] - rg[a:b]) / max(np.linalg.norm(rg[a:b]), 1e-30)
+        assert err <= GRAD_REL_TOL, f"{name}: relative error {err:.3e}"
+
+
+def test_adam_step_matches_oracle(cuda_lib, naca):
+    import torch
+    _, sol = naca
+    P, X, y = random_problem(600, 2)
+    cw = np.array([1.0, 1.0, 1.0], np.float32)
+    li = ind.LearnedIndicator(sol, params=P)
+    _, g, _ = li.gradient(to_dev(X, np.int16), y, cw)
+    gd = torch.from_numpy(g.astype(np.float32)).cuda()
+    sol.mlp_adam(li.params.data_ptr(), gd.data_ptr(), li.m.data_ptr(), li.v.data_ptr(), 1, 1e-3)
+    ref, _, _ = io.adam(P.astype(np.float64), g.astype(np.float32).astype(np.float64),
+                        np.zeros(io.P_COUNT), np.zeros(io.P_COUNT), 1, 1e-3)
+    assert np.allclose(li.params.cpu().numpy(), ref, rtol=0, atol=2e-6)
+
+
+def training_set(g, sol, dh, snapshots, every):
+    """Boxes of both tag passes (deduplicated) with the plain criterion's
+    full decision as labels, features from several states of a GPU run."""
+    t, _ = tag_rows(NAME)
+    key = t[:, 0] * 1e8 + t[:, 1] * 1e4 + t[:, 2]
+    _, first = np.unique(key, return_index=True)
+    t = t[np.sort(first)]
+    # boxes judged while the mesh was built that the finished mesh no longer
+    # holds (neither leaf nor ghost) have no state
+    mesh = set(zip(g["level"].tolist(), g["ix"].tolist(), g["iy"].tolist()))
+    t = t[[(int(a), int(b), int(c)) in mesh for a, b, c in t[:, :3]]]
+    B = boxes_of(t)
+    rule = wl.naca_tag_rule(3, dh)
+    labels = ind.classes_from_tags(sol.tag_plain(rule, B["level"], B["xc"], B["yc"], B["signdis"]))
+    li = ind.LearnedIndicator(sol, seed=0)
+    feats = []
+    for s in range(snapshots):
+        feats.append(li.features(rule, B))
+        sol.run(s * every, every)
+    return li, rule, B, labels, feats
+
+
+def test_training_beats_untrained_and_majority(cuda_lib, naca):
+    import torch
+    g, sol = naca
+    _, dh = tag_rows(NAME)
+    li, rule, B, labels, feats = training_set(g, sol, dh, snapshots=4, every=2)
+    n = len(labels)
+    rng = np.random.default_rng(0)
+    hold = rng.random(n) < 0.2
+    Xtr = torch.cat([f[torch.from_numpy(~hold).cuda()] for f in feats[:-1]]).contiguous()
+    ytr = np.concatenate([labels[~hold]] * (len(feats) - 1))
+    Xte = feats[-1][torch.from_numpy(hold).cuda()].contiguous()
+    yte = labels[hold]
+    untrained = np.mean(li.predict(Xte) != yte)
+    majority = np.mean(yte != np.bincount(ytr, minlength=3).argmax())
+    hist = li.train(Xtr, ytr, steps=600, batch=4096, lr=3e-3)
+    assert hist[-1][0] < hist[0][0]
+    trained = np.mean(li.predict(Xte) != yte)
+    print(f"\nheld-out tag mismatch: trained {trained:.4f}, untrained {untrained:.4f}, "
+          f"majority class {majority:.4f}")
+    assert trained < 0.5 * majority
+    assert trained < untrained
+    # deployment policy: learned tags on ordinary regrids, the plain
+    # criterion on every 10th (and its mismatch recorded)
+    rg = ind.Regridder(li, rule, judge_every=10)
+    for _ in range(11):
+        tags = rg.tags(B)
+    assert len(rg.mismatch) == 2 and tags.shape == (n,)
+    assert rg.mismatch[0][1] < 0.5

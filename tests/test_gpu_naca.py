@@ -15,6 +15,9 @@ import pytest
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 import make_golden  # noqa: E402
+from conftest import load_pkg  # noqa: E402
+
+workloads = load_pkg().workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -24,56 +27,8 @@ REL_MIXED = 5e-5
 FORCE_TOL = 1e-3  # |dCl|, |dCd| bar of the airfoil workloads
 
 
-def naca_params(g, k, precision):
-    s = g["scalars"][k]
-    nst = int(s[14])
-    dom = g["domain"]
-    nlev = int(dom[5])
-    sched = g["schedule"].reshape(-1, 6)
-    dh = g["dh"].reshape(-1, 3)
-    bf = g["body_f"]
-    nb = int(dom[4])
-    return dict(gama=s[4], Rg=s[5], Cv=s[6], Cp=s[7], Ma=s[8], Re=s[9], Pr=s[10], qk=s[11],
-                s_over_t=s[12], cfl=s[13], nstages=nst, tp=list(s[15:15 + nst]),
-                dt_var_step=int(s[15 + nst]), dt_ratio=1.0, limiter=1, viscous=1,
-                precision=precision, initvar=list(g["initvar"]), nlevels=nlev,
-                dh=[tuple(dh[l]) for l in range(nlev)],
-                march_step=[int(sched[l, 0]) for l in range(nlev)],
-                march_left=[int(sched[l, 3]) for l in range(nlev)],
-                step_num=[float(sched[l, 0]) for l in range(nlev)],
-                average_step=[int(sched[l, 1]) for l in range(nlev)],
-                average_left=[int(sched[l, 4]) for l in range(nlev)],
-                prolong_step=[int(sched[l, 2]) for l in range(nlev)],
-                prolong_left=[int(sched[l, 5]) for l in range(nlev)],
-                domain_nx=int(dom[0]), domain_ny=int(dom[1]), periodic_x=int(dom[2]),
-                periodic_y=int(dom[3]), body_level=nlev - 1 if nb > 0 else -1,
-                p_ref=bf[3 * nb], area_ref=bf[3 * nb + 1], shear_ref=bf[3 * nb + 2],
-                L_ref=bf[3 * nb + 3], mu=bf[3 * nb + 4], dt0=float(s[1]))
-
-
 def naca_solver(ib, g, k, precision):
-    P = naca_params(g, k, precision)
-    sol = ib.FlowSolver(P)
-    nlev = P["nlevels"]
-    flags = np.zeros(len(g["level"]), np.uint8)
-    for l in range(nlev):
-        m = g["level"] == l
-        flags[m] = ib.cell_flags_from_boxes(g["kind"][m], g["solid"][m], g["infect"][m],
-                                            g["signdis"][m], l == P["body_level"])
-    sol.upload_topology(g["level"], g["ix"], g["iy"], flags)
-    res = g["cf_res"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
-    pro = g["cf_pro"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
-    sol.upload_interfaces(res, pro)
-    bc = g["bc"].reshape(-1, 9)
-    keep = (bc[:, 7] == 0) & (bc[:, 8] == 0)  # x/y faces, z = 0 plane
-    sol.upload_boundaries(bc[keep][:, :7], g["bc_nmv"].reshape(-1, 3)[keep],
-                          g["facevar"].reshape(-1, 7), g["bc_scalars"][0], g["bc_scalars"][1])
-    nb = int(g["domain"][4])
-    sol.upload_ib(g["ib"].reshape(-1, 20)[:, :18], g["ib_f"].reshape(-1, 16),
-                  g["patch"].reshape(-1, 17), g["patch_f"].reshape(-1, 19),
-                  g["body_f"][:3 * nb].reshape(-1, 3))
-    sol.init_flow(g["prim"][k])
-    return sol
+    return workloads.naca_solver(g, k, precision)
 
 
 def conserved(prim):
