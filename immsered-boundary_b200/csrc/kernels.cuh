@@ -36,6 +36,32 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
   return v;
 }
 
+// Residual max-norm of a 256-thread block into the step's diag: warp and
+// block maxima, then one atomicMax per component and block, skipped when the
+// global value is already as large (the maximum settles after the first
+// blocks, so later blocks only read it instead of serialising on four
+// addresses).  Components map to res_max[0,1,2,4] (no z momentum in 2-D).
+// Every thread of the block must call it; sred is shared scratch of 32
+// words that no thread reads or writes any more.
+__device__ __forceinline__ void block_resnorm(const unsigned long long (&rb)[4], DevDiag *d,
+                                              unsigned long long *sred) {
+  constexpr int kW = kTileCells / 32;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const unsigned long long m = warp_max_u64(rb[c]);
+    if ((tid & 31) == 0) sred[c * kW + (tid >> 5)] = m;
+  }
+  __syncthreads();
+  if (tid < 4) {
+    unsigned long long m = 0ull;
+#pragma unroll
+    for (int w = 0; w < kW; ++w) m = sred[tid * kW + w] > m ? sred[tid * kW + w] : m;
+    unsigned long long *dst = &d->res_bits[tid == 3 ? 4 : tid];
+    if (m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
+  }
+}
+
 // One stage of the multistage update for one tile per CTA (256 threads):
 // NS_Solver::ComputeFaceFlux (NS_Solver.H:704-832), ComptSource
 // (NS_Solver.cpp:282-363), UpdateConsVars (:844-985) and ComptNewPrimVar
@@ -223,12 +249,8 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
     }
   }
   if (FINAL) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      unsigned long long m = warp_max_u64(rb[c]);
-      // residual components map to res_max[0,1,2,4] (no z momentum in 2-D)
-      if ((tid & 31) == 0 && m) atomicMax(&a.diag->res_bits[c == 3 ? 4 : c], m);
-    }
+    __shared__ unsigned long long sred[4 * kTileCells / 32];
+    block_resnorm(rb, a.diag, sred);
   }
 }
 
@@ -578,13 +600,8 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
     }
   }
-  if (FINAL) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      unsigned long long m = warp_max_u64(rb[c]);
-      if ((tid & 31) == 0 && m) atomicMax(&a.diag->res_bits[c == 3 ? 4 : c], m);
-    }
-  }
+  // the y-slope records are dead after the face phase: reuse them
+  if (FINAL) block_resnorm(rb, a.diag, reinterpret_cast<unsigned long long *>(sly));
 }
 
 // CFL time step over the normal cells of every level, NS_Solver::Comptdt
@@ -610,7 +627,15 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
     unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
     b = w < b ? w : b;
   }
-  if ((threadIdx.x & 31) == 0) atomicMin(&a.diag->cfl_bits, b);
+  // block minimum, then one atomic per block, skipped when the global value
+  // is already as small
+  __shared__ unsigned long long sred[8];
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = sred[w] < b ? sred[w] : b;
+    if (b < *(volatile unsigned long long *)&a.diag->cfl_bits) atomicMin(&a.diag->cfl_bits, b);
+  }
 }
 
 // Per-step reset of the step's reductions (the dt and any earlier abort
