@@ -579,47 +579,67 @@ int ibgpu_kernel_times(const ibgpu_ctx *ctx, double ms_out[3], int64_t launches_
   return IBGPU_OK;
 }
 
-static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
-  if (!ctx || !dt || ts0 < 0 || nsteps < 1) return IBGPU_E_ARG;
-  if (!ctx->has_state) return IBGPU_E_STATE;
-  const ibgpu_case &cs = ctx->cs;
-  cudaStream_t st = ctx->stream;
-  const bool exact = cs.precision == IBGPU_FP64_EXACT;
-  const bool mixed = cs.precision == IBGPU_MIXED;
+namespace {
 
-  DevDiag *hd = ctx->h_diag;
-  std::memset(hd, 0, sizeof(DevDiag));
-  hd->dt = *dt;
-  double cfl_init = 10000.0;
-  std::memcpy(&hd->cfl_bits, &cfl_init, sizeof(double));
-  hd->err_key = ~0ull;
-  CK(cudaMemcpyAsync(ctx->d_diag, hd, sizeof(DevDiag), cudaMemcpyHostToDevice, st));
-
+// Event timing of the dominant kernels of one run (kind 0 stage, 1 viscous,
+// 2 CFL), read back after the run's synchronisation.
+struct RunTimer {
+  ibgpu_ctx *ctx;
+  cudaStream_t st;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
-  std::vector<int> evkind;
-  auto mark = [&](int kind) -> cudaEvent_t {
+  std::vector<int> kind;
+  cudaEvent_t mark(int k) {
     if (!ctx->timing) return nullptr;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
     evs.push_back({a, b});
-    evkind.push_back(kind);
+    kind.push_back(k);
     return b;
-  };
-  auto done = [&](cudaEvent_t b) {
+  }
+  void done(cudaEvent_t b) {
     if (b) cudaEventRecord(b, st);
-  };
+  }
+  void collect() {
+    for (size_t i = 0; i < evs.size(); ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, evs[i].first, evs[i].second);
+      ctx->kms[kind[i]] += ms;
+      ctx->klaunch[kind[i]] += 1;
+      cudaEventDestroy(evs[i].first);
+      cudaEventDestroy(evs[i].second);
+    }
+    evs.clear();
+    kind.clear();
+  }
+};
 
-  int64_t marched = 0;
-  for (int step = 0; step < nsteps; ++step) {
-  const int ts = ts0 + step;
+// Device diag of a run: dt in, CFL/residual reductions reset, no abort.
+int begin_diag(ibgpu_ctx *ctx, double dt, cudaStream_t st) {
+  DevDiag *hd = ctx->h_diag;
+  std::memset(hd, 0, sizeof(DevDiag));
+  hd->dt = dt;
+  double cfl_init = 10000.0;
+  std::memcpy(&hd->cfl_bits, &cfl_init, sizeof(double));
+  hd->err_key = ~0ull;
+  CK(cudaMemcpyAsync(ctx->d_diag, hd, sizeof(DevDiag), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+
+// Everything of step ts before the stages (main.cpp:87-89 and the frozen
+// part of NS_Solver::TimeMarching): reduction reset, restriction and
+// prolongation on their schedules, immersed-body ghosts, CFL dt, domain
+// ghosts and the viscous flux of the levels that march.
+int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer &tm) {
+  const ibgpu_case &cs = ctx->cs;
+  const bool exact = cs.precision == IBGPU_FP64_EXACT;
+  const bool mixed = cs.precision == IBGPU_MIXED;
   const int pbase = 8 * step;  // abort-order phases of this step
   if (step > 0) {
     if (exact) exact::launch_step_begin(ctx->d_diag, st);
     else fast::launch_step_begin(ctx->d_diag, st);
   }
-  marched = 0;
   // AMR::InterfaceExchange (AMRInterface.cpp:3-35): restriction of every
   // scheduled pair (coarse level ascending), then prolongation
   for (int l = 0; l + 1 < cs.nlevels && l < (int)ctx->res.size(); ++l) {
@@ -663,8 +683,7 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
   }
 
   // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0)
-  const bool do_cfl = (ts % cs.dt_var_step) == 0;
-  if (do_cfl) {
+  if ((ts % cs.dt_var_step) == 0) {
     CflArgs ca;
     ca.tile_level = ctx->d_tile_level;
     ca.flags = ctx->d_flags;
@@ -672,10 +691,10 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
     ca.nslots = ctx->nslots;
     ca.phase = pbase + 1;
     ca.diag = ctx->d_diag;
-    cudaEvent_t e = mark(2);
+    cudaEvent_t e = tm.mark(2);
     if (exact) exact::launch_cfl(ca, ctx->cc, ctx->nsm, st);
     else fast::launch_cfl(ca, ctx->cc, ctx->nsm, st);
-    done(e);
+    tm.done(e);
     CK(cudaGetLastError());
   }
 
@@ -713,16 +732,20 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
     for (int l = 0; l < cs.nlevels; ++l) {
       if (ts % cs.march_step[l] != cs.march_left[l]) continue;
       va.tile_begin = ctx->level_tile_begin[l];
-      cudaEvent_t e = mark(1);
+      cudaEvent_t e = tm.mark(1);
       if (exact) exact::launch_viscous(va, ctx->cc, ctx->level_tile_count[l], false, st);
       else fast::launch_viscous(va, ctx->cc, ctx->level_tile_count[l], mixed, st);
-      done(e);
+      tm.done(e);
       CK(cudaGetLastError());
     }
   }
+  return IBGPU_OK;
+}
 
-  // stages over the tiles of the levels that march at ts
-  StageArgs sa;
+// Stage arguments of stage k (ping-pong stage buffers; the final stage
+// writes the step state).
+void stage_args(const ibgpu_ctx *ctx, int k, StageArgs &sa) {
+  const ibgpu_case &cs = ctx->cs;
   std::memset(&sa, 0, sizeof(sa));
   sa.tile_nb = ctx->d_tile_nb;
   sa.tile_level = ctx->d_tile_level;
@@ -732,40 +755,27 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
   sa.vsd = ctx->d_vsd;
   sa.nslots = ctx->nslots;
   sa.diag = ctx->d_diag;
-  const int S = cs.nstages;
-  for (int k = 0; k < S; ++k) {
-    const bool fin = (k == S - 1);
-    for (int f = 0; f < 4; ++f) {
-      static const int map[4] = {F_RHO, F_U, F_V, F_P};
-      sa.sin[f] = (k == 0) ? ctx->d_s0[map[f]] : ctx->d_buf[(k - 1) & 1][f];
-      sa.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
-    }
-    sa.tp = cs.tp[k];
-    sa.phase = pbase + 2 + k;
-    for (int l = 0; l < cs.nlevels; ++l) {
-      if (ts % cs.march_step[l] != cs.march_left[l]) continue;
-      if (k == 0) marched += ctx->level_normal_cells[l];
-      sa.tile_begin = ctx->level_tile_begin[l];
-      cudaEvent_t e = mark(0);
-      if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, st);
-      else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, st);
-      done(e);
-      CK(cudaGetLastError());
-    }
+  const bool fin = (k == cs.nstages - 1);
+  static const int map[4] = {F_RHO, F_U, F_V, F_P};
+  for (int f = 0; f < 4; ++f) {
+    sa.sin[f] = (k == 0) ? ctx->d_s0[map[f]] : ctx->d_buf[(k - 1) & 1][f];
+    sa.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
   }
-  }  // steps
-  CK(cudaMemcpyAsync(hd, ctx->d_diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  for (size_t i = 0; i < evs.size(); ++i) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, evs[i].first, evs[i].second);
-    ctx->kms[evkind[i]] += ms;
-    ctx->klaunch[evkind[i]] += 1;
-    cudaEventDestroy(evs[i].first);
-    cudaEventDestroy(evs[i].second);
-  }
+  sa.tp = cs.tp[k];
+}
 
-  // decode the first abort in the reference's order
+int64_t marched_cells(const ibgpu_ctx *ctx, int ts) {
+  int64_t m = 0;
+  for (int l = 0; l < ctx->cs.nlevels; ++l)
+    if (ts % ctx->cs.march_step[l] == ctx->cs.march_left[l]) m += ctx->level_normal_cells[l];
+  return m;
+}
+
+// The first abort of the run in the reference's order, dt and the
+// reductions of the last step, from the device diag already copied to
+// ctx->h_diag.
+int decode_diag(ibgpu_ctx *ctx, int64_t marched, double *dt, ibgpu_diag *diag) {
+  DevDiag *hd = ctx->h_diag;
   int abort_code = 0, abort_slot = -1, abort_step = 0;
   if (hd->err_key != ~0ull) {
     int check = (int)((hd->err_key >> 32) & 0xff);
@@ -808,12 +818,366 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
   return IBGPU_OK;
 }
 
+}  // namespace
+
+static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
+  if (!ctx || !dt || ts0 < 0 || nsteps < 1) return IBGPU_E_ARG;
+  if (!ctx->has_state) return IBGPU_E_STATE;
+  const ibgpu_case &cs = ctx->cs;
+  cudaStream_t st = ctx->stream;
+  const bool exact = cs.precision == IBGPU_FP64_EXACT;
+  const bool mixed = cs.precision == IBGPU_MIXED;
+  int rc = begin_diag(ctx, *dt, st);
+  if (rc) return rc;
+  RunTimer tm{ctx, st, {}, {}};
+  int64_t marched = 0;
+  for (int step = 0; step < nsteps; ++step) {
+    const int ts = ts0 + step;
+    if ((rc = enqueue_prestage(ctx, ts, step, st, tm))) return rc;
+    marched = marched_cells(ctx, ts);
+    // stages over the tiles of the levels that march at ts
+    for (int k = 0; k < cs.nstages; ++k) {
+      StageArgs sa;
+      stage_args(ctx, k, sa);
+      sa.phase = 8 * step + 2 + k;
+      const bool fin = (k == cs.nstages - 1);
+      for (int l = 0; l < cs.nlevels; ++l) {
+        if (ts % cs.march_step[l] != cs.march_left[l]) continue;
+        sa.tile_begin = ctx->level_tile_begin[l];
+        cudaEvent_t e = tm.mark(0);
+        if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, st);
+        else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, st);
+        tm.done(e);
+        CK(cudaGetLastError());
+      }
+    }
+  }
+  CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  tm.collect();
+  return decode_diag(ctx, marched, dt, diag);
+}
+
 int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
   return run_steps(ctx, ts, 1, dt, diag);
 }
 
 int ibgpu_run(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
   return run_steps(ctx, ts0, nsteps, dt, diag);
+}
+
+// ---------------------------------------------------------------------------
+// Batched cases: the stage launches of every case merged into one persistent
+// launch over a (case, tile) work list, replayed from a CUDA graph.
+struct ibgpu_batch {
+  std::vector<ibgpu_ctx *> cases;
+  cudaStream_t stream = nullptr;
+  int nsm = 148, nstages = 0, limiter = 0, period = 1;
+  bool visc = false, mixed = false;
+  StageArgs *d_args = nullptr;     // [case * nstages + k]
+  CaseConst *d_ccs = nullptr;      // [case]
+  int *d_phase_base = nullptr;
+  std::vector<int2 *> d_work;      // per schedule phase r = ts % period
+  std::vector<int> nwork;
+  std::vector<cudaGraphExec_t> graphs;  // per phase: the nstages merged launches
+  int grid = 0;                    // CTAs of the persistent launch (0 = one per item)
+  bool tuned = false;
+  bool timing = false;
+  double stage_ms = 0.0;
+  int64_t stage_launches = 0;
+  std::vector<int> tune_grid;
+  std::vector<float> tune_ms;
+
+  void release() {
+    for (auto g : graphs)
+      if (g) cudaGraphExecDestroy(g);
+    graphs.clear();
+    for (auto w : d_work) cudaFree(w);
+    d_work.clear();
+    cudaFree(d_args);
+    cudaFree(d_ccs);
+    cudaFree(d_phase_base);
+    d_args = nullptr;
+    d_ccs = nullptr;
+    d_phase_base = nullptr;
+  }
+};
+
+namespace {
+
+int enqueue_batch_stages(ibgpu_batch *b, int r, cudaStream_t st) {
+  for (int k = 0; k < b->nstages; ++k) {
+    fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], k, b->nstages,
+                             b->d_phase_base, b->limiter, b->visc, k == b->nstages - 1, b->mixed,
+                             b->grid, st);
+    CK(cudaGetLastError());
+  }
+  return IBGPU_OK;
+}
+
+// Autotuner: time the first stage of the largest phase's work list at each
+// candidate CTA count (one CTA per item, or 1..6 resident CTAs per SM) and
+// keep the fastest.  Runs before the run's diag is initialised; it writes
+// only the first stage buffer, which stage 0 of every step rewrites.
+int autotune(ibgpu_batch *b) {
+  int r = 0;
+  for (int i = 1; i < b->period; ++i)
+    if (b->nwork[i] > b->nwork[r]) r = i;
+  if (b->nwork[r] == 0) {
+    b->tuned = true;
+    return IBGPU_OK;
+  }
+  std::vector<int> cand = {0};
+  for (int m = 1; m <= (b->mixed ? 6 : 4); ++m)
+    if (m * b->nsm < b->nwork[r]) cand.push_back(m * b->nsm);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_grid = 0;
+  b->tune_grid.clear();
+  b->tune_ms.clear();
+  for (int g : cand) {
+    float tbest = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      CK(cudaEventRecord(e0, b->stream));
+      fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], 0, b->nstages,
+                               b->d_phase_base, b->limiter, b->visc, b->nstages == 1, b->mixed, g,
+                               b->stream);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(e1, b->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0 && ms < tbest) tbest = ms;  // the first launch warms up
+    }
+    b->tune_grid.push_back(g);
+    b->tune_ms.push_back(tbest);
+    if (tbest < best) {
+      best = tbest;
+      best_grid = g;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->grid = best_grid;
+  b->tuned = true;
+  return IBGPU_OK;
+}
+
+// One graph per schedule phase holding the nstages merged stage launches;
+// without a capturable stream the launches are issued directly.
+int build_graphs(ibgpu_batch *b) {
+  b->graphs.assign(b->period, nullptr);
+  if (b->stream == nullptr) return IBGPU_OK;  // legacy stream: not capturable
+  for (int r = 0; r < b->period; ++r) {
+    if (b->nwork[r] == 0) continue;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_batch_stages(b, r, b->stream);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&b->graphs[r], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  return IBGPU_OK;
+}
+
+}  // namespace
+
+int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
+  if (!cases || ncases < 1 || !out) return IBGPU_E_ARG;
+  *out = nullptr;
+  const ibgpu_case &c0 = cases[0]->cs;
+  if (c0.precision == IBGPU_FP64_EXACT) {
+    g_last_error = "batched cases run the FP64 or mixed builds";
+    return IBGPU_E_ARG;
+  }
+  for (int i = 0; i < ncases; ++i) {
+    const ibgpu_ctx *c = cases[i];
+    if (!c) return IBGPU_E_ARG;
+    if (!c->has_state) return IBGPU_E_STATE;
+    const ibgpu_case &cs = c->cs;
+    bool same = cs.precision == c0.precision && cs.limiter == c0.limiter &&
+                (cs.viscous != 0) == (c0.viscous != 0) && cs.nstages == c0.nstages &&
+                c->device == cases[0]->device;
+    for (int k = 0; same && k < cs.nstages; ++k) same = cs.tp[k] == c0.tp[k];
+    if (!same) {
+      g_last_error = "batched cases differ in precision, limiter, viscosity, stages or device";
+      return IBGPU_E_ARG;
+    }
+  }
+  ibgpu_batch *b = new (std::nothrow) ibgpu_batch;
+  if (!b) return IBGPU_E_NOMEM;
+  b->cases.assign(cases, cases + ncases);
+  b->stream = cases[0]->stream;
+  b->nsm = cases[0]->nsm;
+  b->nstages = c0.nstages;
+  b->limiter = c0.limiter;
+  b->visc = c0.viscous != 0;
+  b->mixed = c0.precision == IBGPU_MIXED;
+  // schedule period: every level's marching step divides the largest
+  for (auto *c : b->cases)
+    for (int l = 0; l < c->cs.nlevels; ++l) b->period = std::max(b->period, c->cs.march_step[l]);
+  for (auto *c : b->cases)
+    for (int l = 0; l < c->cs.nlevels; ++l)
+      if (b->period % c->cs.march_step[l] != 0) {
+        delete b;
+        g_last_error = "marching steps of the batched cases have no common period";
+        return IBGPU_E_ARG;
+      }
+  const int S = b->nstages;
+  std::vector<StageArgs> args((size_t)ncases * S);
+  std::vector<CaseConst> ccs(ncases);
+  for (int i = 0; i < ncases; ++i) {
+    for (int k = 0; k < S; ++k) stage_args(b->cases[i], k, args[(size_t)i * S + k]);
+    ccs[i] = b->cases[i]->cc;
+  }
+  auto fail = [&](int rc) {
+    b->release();
+    delete b;
+    return rc;
+  };
+  int rc;
+  if ((rc = dev_alloc(&b->d_args, args.size())) || (rc = dev_alloc(&b->d_ccs, ccs.size())) ||
+      (rc = dev_alloc(&b->d_phase_base, 1)))
+    return fail(rc);
+  cudaError_t e = cudaMemcpy(b->d_args, args.data(), args.size() * sizeof(StageArgs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_ccs, ccs.data(), ccs.size() * sizeof(CaseConst), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->d_phase_base, 0, sizeof(int));
+  if (e != cudaSuccess) return fail(cuda_fail(e, "batch upload"));
+  // work lists: case-interleaved so the persistent CTAs mix the cases
+  b->d_work.assign(b->period, nullptr);
+  b->nwork.assign(b->period, 0);
+  for (int r = 0; r < b->period; ++r) {
+    std::vector<std::vector<int2>> per(ncases);
+    size_t total = 0;
+    for (int i = 0; i < ncases; ++i) {
+      const ibgpu_ctx *c = b->cases[i];
+      for (int l = 0; l < c->cs.nlevels; ++l) {
+        if (r % c->cs.march_step[l] != c->cs.march_left[l]) continue;
+        for (int t = 0; t < c->level_tile_count[l]; ++t)
+          per[i].push_back(make_int2(i, c->level_tile_begin[l] + t));
+      }
+      total += per[i].size();
+    }
+    std::vector<int2> w;
+    w.reserve(total);
+    std::vector<double> pos(ncases, 0.0);
+    // proportional interleave: case i's j-th item at key (j + 0.5) / n_i
+    std::vector<std::pair<double, int2>> keyed;
+    keyed.reserve(total);
+    for (int i = 0; i < ncases; ++i)
+      for (size_t j = 0; j < per[i].size(); ++j)
+        keyed.push_back({(j + 0.5) / (double)per[i].size(), per[i][j]});
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const std::pair<double, int2> &a, const std::pair<double, int2> &b2) {
+                       return a.first < b2.first;
+                     });
+    for (auto &kv : keyed) w.push_back(kv.second);
+    if (w.size() > (size_t)INT32_MAX) return fail(IBGPU_E_ARG);
+    b->nwork[r] = (int)w.size();
+    if ((rc = dev_alloc(&b->d_work[r], w.size()))) return fail(rc);
+    e = cudaMemcpy(b->d_work[r], w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "batch work list"));
+  }
+  *out = b;
+  return IBGPU_OK;
+}
+
+int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
+  if (!b || !dt || ts0 < 0 || nsteps < 1) return IBGPU_E_ARG;
+  const int n = (int)b->cases.size();
+  cudaStream_t st = b->stream;
+  int rc;
+  if (!b->tuned) {
+    if ((rc = autotune(b))) return rc;
+    if ((rc = build_graphs(b))) return rc;
+  }
+  for (int i = 0; i < n; ++i)
+    if ((rc = begin_diag(b->cases[i], dt[i], st))) return rc;
+  std::vector<RunTimer> tms;
+  for (int i = 0; i < n; ++i) tms.push_back(RunTimer{b->cases[i], st, {}, {}});
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sev;
+  std::vector<int64_t> marched(n, 0);
+  for (int step = 0; step < nsteps; ++step) {
+    const int ts = ts0 + step;
+    const int r = ts % b->period;
+    for (int i = 0; i < n; ++i) {
+      if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i]))) return rc;
+      marched[i] = marched_cells(b->cases[i], ts);
+    }
+    if (b->nwork[r] == 0) continue;
+    fast::launch_set_phase_base(b->d_phase_base, 8 * step, st);
+    if (b->timing) {
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      CK(cudaEventRecord(e0, st));
+    }
+    if (b->graphs[r]) CK(cudaGraphLaunch(b->graphs[r], st));
+    else if ((rc = enqueue_batch_stages(b, r, st))) return rc;
+    if (b->timing) {
+      CK(cudaEventRecord(e1, st));
+      sev.push_back({e0, e1});
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    CK(cudaMemcpyAsync(b->cases[i]->h_diag, b->cases[i]->d_diag, sizeof(DevDiag),
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (auto &p : sev) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.first, p.second);
+    b->stage_ms += ms;
+    b->stage_launches += b->nstages;
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  int result = IBGPU_OK;
+  for (int i = 0; i < n; ++i) {
+    tms[i].collect();
+    int ri = decode_diag(b->cases[i], marched[i], &dt[i], diag ? &diag[i] : nullptr);
+    if (ri != IBGPU_OK && result == IBGPU_OK) result = ri;
+  }
+  return result;
+}
+
+int ibgpu_batch_set_timing(ibgpu_batch *b, int enable) {
+  if (!b) return IBGPU_E_ARG;
+  b->timing = enable != 0;
+  b->stage_ms = 0.0;
+  b->stage_launches = 0;
+  return IBGPU_OK;
+}
+
+int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage_ms,
+                     int64_t *stage_launches) {
+  if (!b) return IBGPU_E_ARG;
+  if (grid) *grid = b->grid;
+  if (period) *period = b->period;
+  if (stage_ms) *stage_ms = b->stage_ms;
+  if (stage_launches) *stage_launches = b->stage_launches;
+  return IBGPU_OK;
+}
+
+int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms) {
+  if (!b || max < 0) return IBGPU_E_ARG;
+  const int n = std::min<int>(max, (int)b->tune_grid.size());
+  for (int i = 0; i < n; ++i) {
+    if (grids) grids[i] = b->tune_grid[i];
+    if (ms) ms[i] = b->tune_ms[i];
+  }
+  return (int)b->tune_grid.size();
+}
+
+void ibgpu_batch_destroy(ibgpu_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  b->release();
+  delete b;
 }
 
 }  // extern "C"

@@ -386,7 +386,8 @@ __device__ __forceinline__ void fast_slope(const typename SRec<R>::V *sq, const 
 // reconstruction (NS_Solver.H:743-750).  The residual, update and primitive
 // recovery run in FP64 in every mode.
 template <typename R, int LIM, bool VISC, bool FINAL>
-__global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
+__device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseConst &cc,
+                                                const int tile, const int phase) {
   constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
   using S = SRec<R>;
   using V = typename S::V;
@@ -400,7 +401,6 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
 
   const int tid = threadIdx.x;
   const int tx = tid & (kTile - 1), ty = tid >> 4;
-  const int tile = a.tile_begin + blockIdx.x;
   const int lvl = a.tile_level[tile];
   const LevelConst &L = cc.lev[lvl];
   // uniform tile: it and its four side neighbours hold only leaf cells that
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       const double cv1 = orho * ou + res[1] * scale;
       const double cv2 = orho * ov + res[2] * scale;
       const double cv3 = orho * oe + res[3] * scale;
-      if (cv0 < 0.0) raise_error(a.diag, a.phase, ERR_NEG_RHO, (int)slot);
+      if (cv0 < 0.0) raise_error(a.diag, phase, ERR_NEG_RHO, (int)slot);
       if (fl & CF_PRIM) {
         const double ir = FastMath<double>::rcp(cv0);
         nrho = cv0;
@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
       wrote = true;
     }
     if (wrote) {
-      if (nT < 0.0) raise_error(a.diag, a.phase, ERR_NEG_T, (int)slot);
+      if (nT < 0.0) raise_error(a.diag, phase, ERR_NEG_T, (int)slot);
       if (FINAL) {
         a.s0[F_RHO][slot] = nrho;
         a.s0[F_U][slot] = nu;
@@ -602,6 +602,31 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, Cas
   }
   // the y-slope records are dead after the face phase: reuse them
   if (FINAL) block_resnorm(rb, a.diag, reinterpret_cast<unsigned long long *>(sly));
+}
+
+template <typename R, int LIM, bool VISC, bool FINAL>
+__global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
+  stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase);
+}
+
+// Batched stage: persistent CTAs over a work list of (case, tile) pairs of
+// several independent cases (each its own mesh, state and constants); the
+// stage's arguments of case c are args[c * nstages + stage] and its
+// constants ccs[c].  phase_base holds 8 x the step's index within the run
+// (abort ordering), written on the device so a captured graph can replay
+// the launch for every step.
+template <typename R, int LIM, bool VISC, bool FINAL>
+__global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
+    stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
+                       const int2 *__restrict__ work, int nwork, int stage, int nstages,
+                       const int *__restrict__ phase_base) {
+  const int pb = *phase_base;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int2 it = work[w];
+    stage_tile_fast<R, LIM, VISC, FINAL>(args[it.x * nstages + stage], ccs[it.x], it.y,
+                                         pb + 2 + stage);
+    __syncthreads();  // shared-memory reuse by the next work item
+  }
 }
 
 // CFL time step over the normal cells of every level, NS_Solver::Comptdt
@@ -725,6 +750,46 @@ void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limit
     else launch_stage_t<double, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, st);
   }
 }
+
+#ifdef IBGPU_FAST_BUILD
+template <typename R, int LIM>
+static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                           int stage, int nstages, const int *phase_base, bool visc,
+                           bool final_stage, int grid, cudaStream_t st) {
+  dim3 g(grid), block(kTileCells);
+  if (visc) {
+    if (final_stage)
+      stage_kernel_batch<R, LIM, true, true><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+    else
+      stage_kernel_batch<R, LIM, true, false><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+  } else {
+    if (final_stage)
+      stage_kernel_batch<R, LIM, false, true><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+    else
+      stage_kernel_batch<R, LIM, false, false><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+  }
+}
+
+void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                        int stage, int nstages, const int *phase_base, int limiter, bool visc,
+                        bool final_stage, bool mixed, int grid, cudaStream_t st) {
+  if (nwork <= 0) return;
+  if (grid < 1 || grid > nwork) grid = nwork;
+  if (mixed) {
+    if (limiter == LIM_MINMOD) launch_batch_t<float, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+    else launch_batch_t<float, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+  } else {
+    if (limiter == LIM_MINMOD) launch_batch_t<double, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+    else launch_batch_t<double, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+  }
+}
+
+// set the abort-order phase base of the current step (8 x step index)
+__global__ void set_phase_base_kernel(int *phase_base, int value) { *phase_base = value; }
+void launch_set_phase_base(int *phase_base, int value, cudaStream_t st) {
+  set_phase_base_kernel<<<1, 1, 0, st>>>(phase_base, value);
+}
+#endif
 
 void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st) {
   int64_t blocks = (a.nslots + 255) / 256;

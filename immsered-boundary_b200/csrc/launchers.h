@@ -31,6 +31,15 @@ namespace ibgpu {
 IBGPU_DECLARE_LAUNCHERS(fast)
 IBGPU_DECLARE_LAUNCHERS(exact)
 
+// batched stage over several cases (fast builds only): work = (case, tile)
+// pairs, args[case * nstages + stage], ccs[case]; grid 0 = one CTA per item
+namespace fast {
+void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                        int stage, int nstages, const int *phase_base, int limiter, bool visc,
+                        bool final_stage, bool mixed, int grid, cudaStream_t st);
+void launch_set_phase_base(int *phase_base, int value, cudaStream_t st);
+}  // namespace fast
+
 #undef IBGPU_DECLARE_LAUNCHERS
 
 }  // namespace ibgpu

@@ -33,7 +33,9 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_set_kernel_timing", "ibgpu_kernel_times", "ibgpu_destroy", "ibgpu_errstr",
            "ibgpu_last_error", "ibgpu_step_periodic_noalloc", "ibgpu_tag_plain",
            "ibgpu_indicator_features", "ibgpu_mlp_forward", "ibgpu_mlp_grad", "ibgpu_mlp_adam",
-           "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step")
+           "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step", "ibgpu_batch_create",
+           "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
+           "ibgpu_batch_destroy")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -210,6 +212,16 @@ def lib(path: str | None = None):
     L.ibgpu_tag_learned.argtypes = [vp, ctypes.POINTER(TagRule), ctypes.POINTER(TagCells), vp, vp]
     L.ibgpu_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_int64, vp, vp, ctypes.POINTER(ctypes.c_float), vp]
+    L.ibgpu_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    L.ibgpu_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(Diag)]
+    L.ibgpu_batch_set_timing.argtypes = [vp, ctypes.c_int]
+    L.ibgpu_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_float)]
+    L.ibgpu_batch_destroy.argtypes = [vp]
+    L.ibgpu_batch_destroy.restype = None
     L.ibgpu_destroy.argtypes = [vp]
     L.ibgpu_destroy.restype = None
     L.ibgpu_errstr.argtypes = [ctypes.c_int]
@@ -217,7 +229,7 @@ def lib(path: str | None = None):
     L.ibgpu_last_error.argtypes = []
     L.ibgpu_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:
-        if name not in ("ibgpu_destroy", "ibgpu_errstr", "ibgpu_last_error"):
+        if name not in ("ibgpu_destroy", "ibgpu_errstr", "ibgpu_last_error", "ibgpu_batch_destroy"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -518,3 +530,53 @@ def cell_flags_from_boxes(kind, solid, infect, signdis, body_level: bool) -> np.
         fl[normal & ~pos] |= CELL_RESET
     fl[kind == BOX_BLOCK_GHOST] |= CELL_ALIAS
     return fl
+
+
+class Batch:
+    """Several FlowSolver cases advanced together (ibgpu_batch_*): one
+    persistent, graph-replayed launch per stage covers every case's tiles."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s._ctx.value for s in self.solvers])
+        self._b = ctypes.c_void_p()
+        _check(lib().ibgpu_batch_create(arr, len(self.solvers), ctypes.byref(self._b)),
+               "ibgpu_batch_create")
+
+    def run(self, ts0: int, nsteps: int):
+        """nsteps steps of every case; returns the per-case Diag list."""
+        n = len(self.solvers)
+        dt = (ctypes.c_double * n)(*[s.dt for s in self.solvers])
+        diags = (Diag * n)()
+        rc = lib().ibgpu_batch_run(self._b, int(ts0), int(nsteps), dt, diags)
+        for i, s in enumerate(self.solvers):
+            s.dt = dt[i]
+        if rc != OK:
+            bad = next((d for d in diags if d.abort_code), None)
+            raise IbgpuError(rc, "ibgpu_batch_run", lib().ibgpu_last_error().decode(), bad)
+        return list(diags)
+
+    def set_timing(self, on: bool):
+        _check(lib().ibgpu_batch_set_timing(self._b, int(bool(on))), "ibgpu_batch_set_timing")
+
+    def info(self) -> dict:
+        g, p = ctypes.c_int(), ctypes.c_int()
+        ms, nl = ctypes.c_double(), ctypes.c_int64()
+        _check(lib().ibgpu_batch_info(self._b, ctypes.byref(g), ctypes.byref(p), ctypes.byref(ms),
+                                      ctypes.byref(nl)), "ibgpu_batch_info")
+        grids = (ctypes.c_int * 16)()
+        tms = (ctypes.c_float * 16)()
+        k = lib().ibgpu_batch_tuning(self._b, 16, grids, tms)
+        return dict(grid=g.value, period=p.value, stage_ms=ms.value, stage_launches=nl.value,
+                    tuning=[(grids[i], tms[i]) for i in range(max(0, min(k, 16)))])
+
+    def close(self):
+        if self._b:
+            lib().ibgpu_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

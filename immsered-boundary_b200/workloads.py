@@ -51,10 +51,13 @@ def freestream(g: dict, angle: float) -> list:
 
 def vortex_case(n: int, nstages: int = 4, limiter: int = ibgpu.LIM_VANLEER,
                 precision: int = ibgpu.FP64, cfl: float = 0.5, beta: float = 5.0,
-                length: float = 10.0) -> tuple[dict, dict, np.ndarray]:
-    """Returns (params, cells, prim_rows) for the periodic isentropic vortex."""
-    angle = 45.0 / 180.0 * math.pi
-    g = gas_constants(0.5, 0.0)
+                length: float = 10.0, mach: float = 0.5,
+                angle_deg: float = 45.0) -> tuple[dict, dict, np.ndarray]:
+    """Returns (params, cells, prim_rows) for the periodic isentropic vortex
+    (advection Mach number and direction selectable; 0.5 and 45 degrees are
+    the bandwidth workload)."""
+    angle = angle_deg / 180.0 * math.pi
+    g = gas_constants(mach, 0.0)
     init = freestream(g, angle)
     h = length / float(n)
     params = dict(g)
@@ -202,3 +205,21 @@ def naca_tag_rule(nlevels: int, dh, le_x: float = 9.5, le_y: float = 10.0,
     r["torefine"][:nlevels] = 1
     r["toderefine"][1:nlevels] = 1
     return r
+
+
+def batch_vortex_cases(ncases: int, seed: int = 0, min_cells: int = 50_000,
+                       max_cells: int = 800_000, precision: int = ibgpu.FP64):
+    """Independent periodic vortex cases with uneven sizes for the batched
+    solver: side n (a multiple of 16) with n^2 log-uniform in [min_cells,
+    max_cells], advection Mach uniform in [0.1, 0.8] and direction uniform in
+    [-5, 10] degrees from a seeded generator.  Returns a list of
+    (params, cells, prim_rows)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(ncases):
+        cells = math.exp(rng.uniform(math.log(min_cells), math.log(max_cells)))
+        n = max(16, int(round(math.sqrt(cells) / 16.0)) * 16)
+        mach = float(rng.uniform(0.1, 0.8))
+        ang = float(rng.uniform(-5.0, 10.0))
+        out.append(vortex_case(n, precision=precision, mach=mach, angle_deg=ang))
+    return out

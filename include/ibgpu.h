@@ -232,6 +232,36 @@ int ibgpu_kernel_times(const ibgpu_ctx *ctx, double ms_out[3], int64_t launches_
 
 void ibgpu_destroy(ibgpu_ctx *ctx);
 
+/* ---------------------------------------------------------------------------
+ * Batched independent cases (no counterpart in the reference, which runs one
+ * case per process): several contexts, each with its own mesh, state and
+ * case constants, advance together.  Every step runs each case's ghost
+ * fills, CFL and viscous pass, then ONE persistent launch per stage covers
+ * the marching tiles of all cases (a work list of (case, tile) pairs per
+ * subcycling phase, cases interleaved); the stage launches of each phase are
+ * captured once in a CUDA graph and replayed.  On the first run an
+ * autotuner times the candidate CTA counts of the persistent launch and
+ * keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
+ * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; the batch
+ * runs on the first context's stream.  Uploads to a context (topology,
+ * lists) invalidate a batch that holds it: destroy and recreate it.
+ * ------------------------------------------------------------------------- */
+typedef struct ibgpu_batch ibgpu_batch;
+int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out);
+/* nsteps steps of every case from step index ts0; dt[i] and diag[i] (diag
+ * may be NULL) as in ibgpu_run for case i.  Returns the first case's
+ * non-OK code, IBGPU_OK when every case ran clean. */
+int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag *diag);
+/* Event timing of the merged stage launches (total ms, launch count). */
+int ibgpu_batch_set_timing(ibgpu_batch *b, int enable);
+/* Chosen CTA count (0 = one CTA per work item), subcycling period, timing. */
+int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage_ms,
+                     int64_t *stage_launches);
+/* Autotuner record: up to max (CTA count, ms) pairs; returns the number of
+ * candidates timed. */
+int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms);
+void ibgpu_batch_destroy(ibgpu_batch *b);
+
 /* Allocation-free variant of ibgpu_step for one periodic, inviscid,
  * single-level grid of nx x ny cells (this entry point has no counterpart in
  * the reference).  For callers that must not allocate device memory while
