@@ -17,10 +17,18 @@ struct CtxView {
   const double *s0[kStateFields];
   const uint8_t *flags;
   const int32_t *tile_nb;
+  const int32_t *tile_level;
+  const int2 *tile_org;
+  const int32_t *cell_slot;
+  int64_t ncells, nslots, ntiles;
   int *aux_err;  // device word: set by a kernel whose wait ran out of time
   CaseConst cc;
 };
 int ctx_view(const ibgpu_ctx *ctx, CtxView *v);
+// per-slot signed wall distance (created on demand); tag buffer of nslots
+// per-slot bytes followed by ncells per-row bytes
+int ctx_signdis_buffer(ibgpu_ctx *ctx, double **dev, bool create);
+int ctx_tags_buffer(ibgpu_ctx *ctx, uint8_t **dev);
 // slot of box (l, ix, iy) of the uploaded topology (periodic wrap), -1 if absent
 int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy);
 

@@ -83,6 +83,9 @@ struct ibgpu_ctx {
   std::vector<int64_t> level_normal_cells;
   std::vector<int32_t> h_slot_level, h_slot_ix, h_slot_iy;  // slot -> position (abort reports)
   int32_t *d_tile_nb = nullptr, *d_tile_level = nullptr, *d_cell_slot = nullptr;
+  int2 *d_tile_org = nullptr;      // (ix, iy) of each tile's first cell
+  double *d_signdis = nullptr;     // per slot, after ibgpu_upload_signdis
+  uint8_t *d_tags = nullptr;       // indicator output: per slot, then per cell row
   uint8_t *d_flags = nullptr, *d_cell_alias = nullptr, *d_tile_uniform = nullptr;
 
   // state: step state (6 fields) + two stage buffers (4 fields each)
@@ -168,6 +171,12 @@ struct ibgpu_ctx {
     cudaFree(d_cell_alias);
     cudaFree(d_tile_uniform);
     d_tile_uniform = nullptr;
+    cudaFree(d_tile_org);
+    cudaFree(d_signdis);
+    cudaFree(d_tags);
+    d_tile_org = nullptr;
+    d_signdis = nullptr;
+    d_tags = nullptr;
     for (auto &p : d_s0) { cudaFree(p); p = nullptr; }
     for (auto &b : d_buf)
       for (auto &p : b) { cudaFree(p); p = nullptr; }
@@ -254,8 +263,31 @@ int ctx_view(const ibgpu_ctx *ctx, CtxView *v) {
   for (int k = 0; k < kStateFields; ++k) v->s0[k] = ctx->d_s0[k];
   v->flags = ctx->d_flags;
   v->tile_nb = ctx->d_tile_nb;
+  v->tile_level = ctx->d_tile_level;
+  v->tile_org = ctx->d_tile_org;
+  v->cell_slot = ctx->d_cell_slot;
+  v->ncells = ctx->ncells;
+  v->nslots = ctx->nslots;
+  v->ntiles = ctx->ntiles;
   v->aux_err = ctx->d_aux_err;
   v->cc = ctx->cc;
+  return IBGPU_OK;
+}
+int ctx_signdis_buffer(ibgpu_ctx *ctx, double **dev, bool create) {
+  if (!ctx->d_signdis && create) {
+    int rc = dev_alloc(&ctx->d_signdis, (size_t)std::max<int64_t>(ctx->nslots, 1));
+    if (rc) return rc;
+  }
+  *dev = ctx->d_signdis;
+  return IBGPU_OK;
+}
+int ctx_tags_buffer(ibgpu_ctx *ctx, uint8_t **dev) {
+  if (!ctx->d_tags) {
+    // per slot, then per cell row
+    int rc = dev_alloc(&ctx->d_tags, (size_t)std::max<int64_t>(ctx->nslots + ctx->ncells, 1));
+    if (rc) return rc;
+  }
+  *dev = ctx->d_tags;
   return IBGPU_OK;
 }
 int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy) {
@@ -488,6 +520,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       (rc = dev_alloc(&ctx->d_tile_level, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_flags, (size_t)nslots)) ||
       (rc = dev_alloc(&ctx->d_tile_uniform, (size_t)ntiles)) ||
+      (rc = dev_alloc(&ctx->d_tile_org, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_cell_slot, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_cell_alias, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)))
@@ -502,8 +535,13 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   CK(cudaMemcpyAsync(ctx->d_tile_nb, h_nb.data(), h_nb.size() * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_tile_level, h_tile_level.data(), ntiles * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_flags, h_flags.data(), nslots, cudaMemcpyHostToDevice, st));
-  if (ntiles > 0)
+  std::vector<int2> h_org(ntiles);
+  for (int64_t t = 0; t < ntiles; ++t)
+    h_org[t] = make_int2(tile_pos[t].first * kTile, tile_pos[t].second * kTile);
+  if (ntiles > 0) {
     CK(cudaMemcpyAsync(ctx->d_tile_uniform, h_uniform.data(), ntiles, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_tile_org, h_org.data(), ntiles * sizeof(int2), cudaMemcpyHostToDevice, st));
+  }
   if (n > 0) {
     CK(cudaMemcpyAsync(ctx->d_cell_slot, cell_slot.data(), n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cell_alias, alias.data(), n, cudaMemcpyHostToDevice, st));
@@ -631,12 +669,16 @@ int begin_diag(ibgpu_ctx *ctx, double dt, cudaStream_t st) {
 // part of NS_Solver::TimeMarching): reduction reset, restriction and
 // prolongation on their schedules, immersed-body ghosts, CFL dt, domain
 // ghosts and the viscous flux of the levels that march.
-int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer &tm) {
+int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer &tm,
+                     bool batched = false) {
   const ibgpu_case &cs = ctx->cs;
   const bool exact = cs.precision == IBGPU_FP64_EXACT;
   const bool mixed = cs.precision == IBGPU_MIXED;
   const int pbase = 8 * step;  // abort-order phases of this step
-  if (step > 0) {
+  // a batch resets the reductions and runs the CFL pass of all its cases in
+  // merged launches (the CFL pass reads normal cells only, which the domain
+  // ghosts and the viscous pass below do not write, so it may follow them)
+  if (step > 0 && !batched) {
     if (exact) exact::launch_step_begin(ctx->d_diag, st);
     else fast::launch_step_begin(ctx->d_diag, st);
   }
@@ -683,7 +725,7 @@ int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer
   }
 
   // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0)
-  if ((ts % cs.dt_var_step) == 0) {
+  if (!batched && (ts % cs.dt_var_step) == 0) {
     CflArgs ca;
     ca.tile_level = ctx->d_tile_level;
     ca.flags = ctx->d_flags;
@@ -879,7 +921,9 @@ struct ibgpu_batch {
   int *d_phase_base = nullptr;
   std::vector<int2 *> d_work;      // per schedule phase r = ts % period
   std::vector<int> nwork;
-  std::vector<cudaGraphExec_t> graphs;  // per phase: the nstages merged launches
+  std::vector<cudaGraphExec_t> graphs;  // per phase r (+ period with the CFL pass)
+  int2 *d_cfl_work = nullptr;      // every tile of every case
+  int ncfl = 0, dt_var_step = 1;
   int grid = 0;                    // CTAs of the persistent launch (0 = one per item)
   bool tuned = false;
   bool timing = false;
@@ -894,6 +938,8 @@ struct ibgpu_batch {
     graphs.clear();
     for (auto w : d_work) cudaFree(w);
     d_work.clear();
+    cudaFree(d_cfl_work);
+    d_cfl_work = nullptr;
     cudaFree(d_args);
     cudaFree(d_ccs);
     cudaFree(d_phase_base);
@@ -905,7 +951,12 @@ struct ibgpu_batch {
 
 namespace {
 
-int enqueue_batch_stages(ibgpu_batch *b, int r, cudaStream_t st) {
+int enqueue_batch_stages(ibgpu_batch *b, int r, bool cfl, cudaStream_t st) {
+  if (cfl) {
+    fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work, b->ncfl, b->nstages,
+                           b->d_phase_base, (int)b->cases.size(), 0, st);
+    CK(cudaGetLastError());
+  }
   for (int k = 0; k < b->nstages; ++k) {
     fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], k, b->nstages,
                              b->d_phase_base, b->limiter, b->visc, k == b->nstages - 1, b->mixed,
@@ -968,17 +1019,18 @@ int autotune(ibgpu_batch *b) {
 // One graph per schedule phase holding the nstages merged stage launches;
 // without a capturable stream the launches are issued directly.
 int build_graphs(ibgpu_batch *b) {
-  b->graphs.assign(b->period, nullptr);
+  b->graphs.assign(2 * b->period, nullptr);
   if (b->stream == nullptr) return IBGPU_OK;  // legacy stream: not capturable
-  for (int r = 0; r < b->period; ++r) {
-    if (b->nwork[r] == 0) continue;
+  for (int v = 0; v < 2 * b->period; ++v) {
+    const int r = v % b->period;
+    const bool cfl = v >= b->period;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_batch_stages(b, r, b->stream);
+    int rc = enqueue_batch_stages(b, r, cfl, b->stream);
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&b->graphs[r], g, 0);
+    e = cudaGraphInstantiate(&b->graphs[v], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
   }
@@ -1004,8 +1056,10 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
                 (cs.viscous != 0) == (c0.viscous != 0) && cs.nstages == c0.nstages &&
                 c->device == cases[0]->device;
     for (int k = 0; same && k < cs.nstages; ++k) same = cs.tp[k] == c0.tp[k];
+    same = same && cs.dt_var_step == c0.dt_var_step;
     if (!same) {
-      g_last_error = "batched cases differ in precision, limiter, viscosity, stages or device";
+      g_last_error = "batched cases differ in precision, limiter, viscosity, stages, dt_var_step "
+                     "or device";
       return IBGPU_E_ARG;
     }
   }
@@ -1018,6 +1072,7 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   b->limiter = c0.limiter;
   b->visc = c0.viscous != 0;
   b->mixed = c0.precision == IBGPU_MIXED;
+  b->dt_var_step = c0.dt_var_step;
   // schedule period: every level's marching step divides the largest
   for (auto *c : b->cases)
     for (int l = 0; l < c->cs.nlevels; ++l) b->period = std::max(b->period, c->cs.march_step[l]);
@@ -1083,6 +1138,15 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
     e = cudaMemcpy(b->d_work[r], w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_fail(e, "batch work list"));
   }
+  {
+    std::vector<int2> w;
+    for (int i = 0; i < ncases; ++i)
+      for (int t = 0; t < (int)b->cases[i]->ntiles; ++t) w.push_back(make_int2(i, t));
+    b->ncfl = (int)w.size();
+    if ((rc = dev_alloc(&b->d_cfl_work, w.size()))) return fail(rc);
+    e = cudaMemcpy(b->d_cfl_work, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "batch CFL work list"));
+  }
   *out = b;
   return IBGPU_OK;
 }
@@ -1106,19 +1170,21 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
   for (int step = 0; step < nsteps; ++step) {
     const int ts = ts0 + step;
     const int r = ts % b->period;
+    if (step > 0) fast::launch_step_begin_batch(b->d_args, n, b->nstages, st);
     for (int i = 0; i < n; ++i) {
-      if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i]))) return rc;
+      if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i], true))) return rc;
       marched[i] = marched_cells(b->cases[i], ts);
     }
-    if (b->nwork[r] == 0) continue;
+    const bool cfl = (ts % b->dt_var_step) == 0;
     fast::launch_set_phase_base(b->d_phase_base, 8 * step, st);
     if (b->timing) {
       CK(cudaEventCreate(&e0));
       CK(cudaEventCreate(&e1));
       CK(cudaEventRecord(e0, st));
     }
-    if (b->graphs[r]) CK(cudaGraphLaunch(b->graphs[r], st));
-    else if ((rc = enqueue_batch_stages(b, r, st))) return rc;
+    const int v = r + (cfl ? b->period : 0);
+    if (b->graphs[v]) CK(cudaGraphLaunch(b->graphs[v], st));
+    else if ((rc = enqueue_batch_stages(b, r, cfl, st))) return rc;
     if (b->timing) {
       CK(cudaEventRecord(e1, st));
       sev.push_back({e0, e1});

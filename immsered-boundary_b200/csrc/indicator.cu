@@ -649,6 +649,222 @@ __global__ void class_to_tag_kernel(const uint8_t *__restrict__ cls, int64_t n,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Deployment on the mesh: every normal cell of the context, features
+// gathered straight from the state into the A tile (no feature matrix in
+// HBM), the three layers, the argmax mapped to tag bits.  Shared memory:
+// X (reused for h2), h1, weights; Tensor Memory: 128 columns (D1 0..63,
+// D2 64..127, logits reuse D1) so several CTAs share an SM.
+struct MeshSmem {
+  static constexpr int X = 0;  // also h2
+  static constexpr int H1 = X + kRows * kIn * 2;
+  static constexpr int W1 = H1 + kRows * kHid * 2;
+  static constexpr int W2 = W1 + kHid * kIn * 2;
+  static constexpr int W3 = W2 + kHid * kHid * 2;
+  static constexpr int BIAS = W3 + kOutPad * kHid * 2;
+  static constexpr int BYTES = BIAS + 1024;
+};
+constexpr uint32_t T_COLS_MESH = 128;
+
+struct MeshArgs {
+  const int32_t *tile_nb, *tile_level;
+  const int2 *tile_org;
+  const uint8_t *flags;
+  const double *rho, *u, *v, *p;
+  const double *signdis;  // per slot or null (far from any wall)
+  uint8_t *tags;          // per slot
+  int64_t nslots;
+};
+
+struct FeatScale {
+  double inv_rho, inv_c, inv_p, left, yc, inv_chord;
+  double dx[IBGPU_TAG_MAX_LEVELS], dy[IBGPU_TAG_MAX_LEVELS];
+};
+
+__global__ void __launch_bounds__(kThreads)
+    mlp_tag_mesh_kernel(const float *__restrict__ P, MeshArgs m, FeatScale F, int *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int abort_flag;
+  constexpr int kSW = kTile + 4, kSH = 8 + 4;  // staged region of a half tile
+  __shared__ float4 sn[kSH * kSW];
+  __shared__ uint8_t sp[kSH * kSW];
+  using S = MeshSmem;
+  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sW1 = smem + S::W1, *sW2 = smem + S::W2,
+          *sW3 = smem + S::W3;
+  uint8_t *sH2 = sX;
+  float *sB = reinterpret_cast<float *>(smem + S::BIAS);
+  const int t = threadIdx.x;
+  load_weights(P, sW1, sW2, nullptr, sW3, nullptr, sB);
+  if (t == 0) {
+    tc::mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if ((t >> 5) == 0) {
+    tc::tmem_alloc(&tbase, T_COLS_MESH);
+    tc::tmem_relinquish();
+  }
+  tc::fence_async_smem();
+  tc_sync();
+  const uint32_t tm = tbase;
+  const uint32_t lane_off = (uint32_t)((t & ~31) << 16);
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int64_t nitems = m.nslots / kRows;  // half tiles
+  for (int64_t item = blockIdx.x; ok && item < nitems; item += gridDim.x) {
+    const int64_t slot = item * kRows + t;
+    const bool normal = (m.flags[slot] & CF_NORMAL) != 0;
+    // stage the freestream-normalised (rho, u, v, p) of the 12 x 20 region
+    // around this half tile (rows -2..9 of the half, columns -2..17)
+    const int half = (int)(item & 1);
+    {
+      const int tile = (int)(item >> 1);
+      for (int r = t; r < kSH * kSW; r += kThreads) {
+        const int rx = r % kSW - 2, ry = r / kSW - 2 + 8 * half;
+        const int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
+        const int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
+        const int nb = m.tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
+        uint8_t pres = 0;
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (nb >= 0) {
+          const int64_t s = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
+          if (m.flags[s] & CF_PRESENT) {
+            pres = 1;
+            q = make_float4((float)(m.rho[s] * F.inv_rho - 1.0), (float)(m.u[s] * F.inv_c),
+                            (float)(m.v[s] * F.inv_c), (float)(m.p[s] * F.inv_p - 1.0));
+          }
+        }
+        sn[r] = q;
+        sp[r] = pres;
+      }
+    }
+    __syncthreads();
+    {
+      // feature row of this thread's cell (zeros for other slots)
+      auto put = [&](int k, float val) {
+        *reinterpret_cast<uint16_t *>(sX + tc::kmajor_off(kRows, t, k)) = bf16_bits(val);
+      };
+      if (normal) {
+        const int tile = (int)(slot >> 8), lx = (int)(slot & 15), ly = (int)((slot >> 4) & 15);
+        const int rc = ((ly - 8 * half) + 2) * kSW + (lx + 2);  // centre in the staged region
+        const float4 c = sn[rc];
+        for (int dy = -2; dy <= 2; ++dy) {
+          for (int dx = -2; dx <= 2; ++dx) {
+            const int r = rc + dy * kSW + dx;
+            const float4 q = sp[r] ? sn[r] : c;
+            const int k = (dy + 2) * 5 + (dx + 2);
+            put(k, q.x);
+            put(25 + k, q.y);
+            put(50 + k, q.z);
+            put(75 + k, q.w);
+          }
+        }
+        const int l = m.tile_level[tile];
+        const int2 org = m.tile_org[tile];
+        const double xc = (org.x + lx + 0.5) * F.dx[l], yc = (org.y + ly + 0.5) * F.dy[l];
+        const double sd = m.signdis ? m.signdis[slot] : 1e30;
+        put(100, (float)(fmin(fmax(sd / F.dx[l], -8.0), 8.0) * 0.125));
+        put(101, (float)(fmin(fmax(sd * F.inv_chord, -4.0), 4.0) * 0.25));
+        const double ry = (yc - F.yc) * F.inv_chord * 0.125;
+        put(102, (float)((xc - F.left) * F.inv_chord * 0.125));
+        put(103, (float)ry);
+        put(104, (float)fabs(ry));
+        const int lc = l < 6 ? l : 6;
+        for (int e = 0; e < 7; ++e) put(105 + e, e == lc ? 1.0f : 0.0f);
+      } else {
+        for (int c = 0; c < kIn / 8; ++c)
+          *reinterpret_cast<uint4 *>(sX + c * (kRows * 16) + t * 16) = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, 0, sX, kRows * 16, sW1, kHid * 16, kIn / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float h[64];
+      tmem_row64(tm + lane_off + 0, sB, h);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) h[j] = gelu(h[j]);
+      store_row64(sH1, t, h);
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, 64, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      float h[64];
+      tmem_row64(tm + lane_off + 64, sB + kHid, h);
+#pragma unroll
+      for (int j = 0; j < kHid; ++j) h[j] = gelu(h[j]);
+      store_row64(sH2, t, h);  // X is free: the layer-1 MMA has completed
+    }
+    tc::fence_async_smem();
+    tc_sync();
+    if (t == 0) mma_chain(tm, 0, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
+    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    {
+      uint32_t r[16];
+      tc::tmem_ld16(tm + lane_off + 0, r);
+      tc::tmem_wait_ld16(r);
+      float z[3];
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
+      int am = 0;
+      if (z[1] > z[am]) am = 1;
+      if (z[2] > z[am]) am = 2;
+      uint8_t tag = 0;
+      if (normal) tag = am == 0 ? (uint8_t)IBGPU_TAG_REFINE : (am == 1 ? (uint8_t)IBGPU_TAG_COARSEN : 0);
+      m.tags[slot] = tag;
+    }
+    tc_sync();  // every lane read before the next item's MMAs overwrite them
+  }
+  if (!ok) {
+    if (t == 0) atomicExch(err, 1);
+    tc::mbar_wait_bounded(&bar, phase, kWaitCycles);
+  }
+  tc_sync();
+  if ((t >> 5) == 0) tc::tmem_dealloc(tm, T_COLS_MESH);
+}
+
+// Plain criterion over every normal cell of the context (centres from the
+// tile origins, signed distance per slot or far from any wall).
+__global__ void tag_plain_mesh_kernel(RuleDev R, MeshArgs m, FeatScale F) {
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < m.nslots;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    uint8_t b = 0;
+    if (m.flags[s] & CF_NORMAL) {
+      const int tile = (int)(s >> 8), lx = (int)(s & 15), ly = (int)((s >> 4) & 15);
+      const int l = m.tile_level[tile];
+      const int2 org = m.tile_org[tile];
+      const double x = (org.x + lx + 0.5) * F.dx[l], y = (org.y + ly + 0.5) * F.dy[l];
+      const double sd = m.signdis ? m.signdis[s] : 1e30;
+      if (R.torefine[l] && in_region(x, y, sd, l, R.n_rect, R, R.ru, R.rd, R.rh, R.bl, R.bh, R.nm))
+        b |= IBGPU_TAG_REFINE;
+      if (l >= 1 && R.toderefine[l] &&
+          !in_region(x, y, sd, l - 1, R.n_rect_c, R, R.dru, R.drd, R.drh, R.dbl, R.dbh, R.dnm))
+        b |= IBGPU_TAG_COARSEN;
+    }
+    m.tags[s] = b;
+  }
+}
+
+__global__ void gather_rows_u8(const uint8_t *__restrict__ per_slot, const int32_t *__restrict__ cell_slot,
+                               int64_t n, uint8_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = per_slot[cell_slot[i]];
+}
+
+__global__ void scatter_rows_f64(const double *__restrict__ rows, const int32_t *__restrict__ cell_slot,
+                                 int64_t n, double *__restrict__ per_slot) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    per_slot[cell_slot[i]] = rows[i];
+}
+
 }  // namespace ind
 }  // namespace ibgpu
 
@@ -741,6 +957,8 @@ int kernel_error_check(int *d_err, cudaStream_t st) {
 
 // opt in to the large dynamic shared-memory carve-out (per device, cheap)
 int configure_smem() {
+  CKI(cudaFuncSetAttribute(mlp_tag_mesh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           MeshSmem::BYTES));
   CKI(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            TrainSmem::BYTES));
   CKI(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -927,6 +1145,81 @@ int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_ta
                                                                       tags.as<uint8_t>());
   CKI(cudaGetLastError());
   CKI(cudaMemcpyAsync(out, tags.p, (size_t)n, cudaMemcpyDeviceToHost, V.stream));
+  CKI(cudaStreamSynchronize(V.stream));
+  return IBGPU_OK;
+}
+
+int ibgpu_upload_signdis(ibgpu_ctx *ctx, const double *signdis) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  if (!V.has_topology) return IBGPU_E_STATE;
+  if (V.ncells == 0) return IBGPU_OK;
+  if (!signdis) return IBGPU_E_ARG;
+  double *dsd = nullptr;
+  int rc = ctx_signdis_buffer(ctx, &dsd, true);
+  if (rc) return rc;
+  DevBuf rows;
+  if ((rc = upload(rows, signdis, V.ncells, V.stream))) return rc;
+  // slots that no row names (absent cells) are far from any wall
+  std::vector<double> far((size_t)V.nslots, 1e30);
+  CKI(cudaMemcpyAsync(dsd, far.data(), far.size() * sizeof(double), cudaMemcpyHostToDevice, V.stream));
+  scatter_rows_f64<<<grid_for(V.ncells, V.nsm, 256), 256, 0, V.stream>>>(rows.as<double>(), V.cell_slot,
+                                                                         V.ncells, dsd);
+  CKI(cudaGetLastError());
+  CKI(cudaStreamSynchronize(V.stream));
+  return IBGPU_OK;
+}
+
+int ibgpu_tag_mesh(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
+                   uint8_t *tags) {
+  CtxView V;
+  if (!rule || ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  if (!V.has_topology || (d_params && !V.has_state)) return IBGPU_E_STATE;
+  if (V.ncells == 0) return IBGPU_OK;
+  if (!tags) return IBGPU_E_ARG;
+  uint8_t *dtags = nullptr;
+  double *dsd = nullptr;
+  int rc;
+  if ((rc = ctx_tags_buffer(ctx, &dtags)) || (rc = ctx_signdis_buffer(ctx, &dsd, false))) return rc;
+  MeshArgs m;
+  m.tile_nb = V.tile_nb;
+  m.tile_level = V.tile_level;
+  m.tile_org = V.tile_org;
+  m.flags = V.flags;
+  m.rho = V.s0[F_RHO];
+  m.u = V.s0[F_U];
+  m.v = V.s0[F_V];
+  m.p = V.s0[F_P];
+  m.signdis = dsd;
+  m.tags = dtags;
+  m.nslots = V.nslots;
+  FeatScale F;
+  const double rho_inf = V.cc.initvar[0], p_inf = V.cc.initvar[4];
+  F.inv_rho = 1.0 / rho_inf;
+  F.inv_p = 1.0 / p_inf;
+  F.inv_c = 1.0 / std::sqrt(V.cc.gama * p_inf / rho_inf);
+  F.left = rule->body_left_x;
+  F.yc = rule->body_center_y;
+  F.inv_chord = 1.0 / (rule->body_right_x - rule->body_left_x);
+  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) {
+    F.dx[k] = V.cc.lev[k].dx > 0 ? V.cc.lev[k].dx : 1.0;
+    F.dy[k] = V.cc.lev[k].dy > 0 ? V.cc.lev[k].dy : 1.0;
+  }
+  if (d_params) {
+    if ((rc = configure_smem())) return rc;
+    const int64_t items = V.nslots / kRows;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)V.nsm * 3));
+    mlp_tag_mesh_kernel<<<grid, kThreads, MeshSmem::BYTES, V.stream>>>(d_params, m, F, V.aux_err);
+  } else {
+    tag_plain_mesh_kernel<<<grid_for(V.nslots, V.nsm, 256), 256, 0, V.stream>>>(to_dev(rule), m, F);
+  }
+  CKI(cudaGetLastError());
+  uint8_t *rows = dtags + V.nslots;
+  gather_rows_u8<<<grid_for(V.ncells, V.nsm, 256), 256, 0, V.stream>>>(dtags, V.cell_slot, V.ncells,
+                                                                      rows);
+  CKI(cudaGetLastError());
+  CKI(cudaMemcpyAsync(tags, rows, (size_t)V.ncells, cudaMemcpyDeviceToHost, V.stream));
+  if (d_params) return kernel_error_check(V.aux_err, V.stream);
   CKI(cudaStreamSynchronize(V.stream));
   return IBGPU_OK;
 }

@@ -784,6 +784,80 @@ void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 
   }
 }
 
+// CFL pass of every batched case in one launch: one CTA per (case, tile)
+// item of all tiles, the same per-cell bound as cfl_kernel, block minimum and
+// one guarded atomic into the case's diag.
+__global__ void __launch_bounds__(kTileCells)
+    cfl_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
+                     const int2 *__restrict__ work, int nwork, int nstages,
+                     const int *__restrict__ phase_base) {
+  __shared__ unsigned long long sred[kTileCells / 32];
+  const int pb = *phase_base;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int2 it = work[w];
+    const StageArgs &a = args[it.x * nstages];
+    const CaseConst &cc = ccs[it.x];
+    const int64_t s = (int64_t)it.y * kTileCells + threadIdx.x;
+    double best = 10000.0;
+    if (a.flags[s] & CF_NORMAL) {
+      const LevelConst &L = cc.lev[a.tile_level[it.y]];
+      double c = sqrt(cc.gamaRg * a.s0[F_T][s]);
+      double c0 = (fabs(a.s0[F_U][s]) + c) * L.area_x;
+      double c1 = (fabs(a.s0[F_V][s]) + c) * L.area_y;
+      double c2 = (0.0 + c) * L.area_z;
+      double d0 = L.cfl_vol / (c0 + c1 + c2);
+      if (d0 < 0.0) raise_error(a.diag, pb + 1, ERR_CFL_NEG_DT, (int)s);
+      best = (d0 < best) ? d0 : best;
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong(best);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long v = __shfl_xor_sync(0xffffffffu, b, o);
+      b = v < b ? v : b;
+    }
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 1; k < kTileCells / 32; ++k) b = sred[k] < b ? sred[k] : b;
+      if (b < *(volatile unsigned long long *)&a.diag->cfl_bits) atomicMin(&a.diag->cfl_bits, b);
+    }
+    __syncthreads();
+  }
+}
+
+// dt = min(CFL_dt, dt*dt_ratio) of every batched case (one thread each)
+__global__ void finalize_dt_batch(const StageArgs *__restrict__ args,
+                                  const CaseConst *__restrict__ ccs, int ncases, int nstages) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases) return;
+  DevDiag *d = args[c * nstages].diag;
+  double cdt = __longlong_as_double((long long)d->cfl_bits);
+  double cand = d->dt * ccs[c].dt_ratio;
+  d->dt = (cand < cdt) ? cand : cdt;
+}
+
+// per-step reset of the reductions of every batched case
+__global__ void step_begin_batch(const StageArgs *__restrict__ args, int ncases, int nstages) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases) return;
+  DevDiag *d = args[c * nstages].diag;
+  d->cfl_bits = (unsigned long long)__double_as_longlong(10000.0);
+  for (int k = 0; k < 5; ++k) d->res_bits[k] = 0ull;
+}
+
+void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st) {
+  if (nwork > 0) {
+    if (grid < 1 || grid > nwork) grid = nwork;
+    cfl_kernel_batch<<<grid, kTileCells, 0, st>>>(args, ccs, work, nwork, nstages, phase_base);
+  }
+  finalize_dt_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, ncases, nstages);
+}
+
+void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cudaStream_t st) {
+  step_begin_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ncases, nstages);
+}
+
 // set the abort-order phase base of the current step (8 x step index)
 __global__ void set_phase_base_kernel(int *phase_base, int value) { *phase_base = value; }
 void launch_set_phase_base(int *phase_base, int value, cudaStream_t st) {

@@ -38,6 +38,9 @@ void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 
                         int stage, int nstages, const int *phase_base, int limiter, bool visc,
                         bool final_stage, bool mixed, int grid, cudaStream_t st);
 void launch_set_phase_base(int *phase_base, int value, cudaStream_t st);
+void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st);
+void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cudaStream_t st);
 }  // namespace fast
 
 #undef IBGPU_DECLARE_LAUNCHERS

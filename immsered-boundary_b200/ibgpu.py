@@ -35,7 +35,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_indicator_features", "ibgpu_mlp_forward", "ibgpu_mlp_grad", "ibgpu_mlp_adam",
            "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step", "ibgpu_batch_create",
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
-           "ibgpu_batch_destroy")
+           "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -220,6 +220,8 @@ def lib(path: str | None = None):
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_float)]
+    L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ibgpu_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
     L.ibgpu_batch_destroy.argtypes = [vp]
     L.ibgpu_batch_destroy.restype = None
     L.ibgpu_destroy.argtypes = [vp]
@@ -401,6 +403,18 @@ class FlowSolver:
                                        ctypes.c_void_p(d_params), out.ctypes.data_as(ctypes.c_void_p)),
                "ibgpu_tag_learned")
         return out[:h.n]
+
+    def upload_signdis(self, signdis):
+        s, sp = _f64(signdis)
+        _check(lib().ibgpu_upload_signdis(self._ctx, sp), "ibgpu_upload_signdis")
+
+    def tag_mesh(self, rule: dict, d_params: int = 0) -> np.ndarray:
+        """Tag bits of every uploaded cell row: learned (d_params) or plain."""
+        r = make_tag_rule(rule)
+        out = np.zeros(max(self.ncells, 1), np.uint8)
+        _check(lib().ibgpu_tag_mesh(self._ctx, ctypes.byref(r), ctypes.c_void_p(d_params or None),
+                                    out.ctypes.data_as(ctypes.c_void_p)), "ibgpu_tag_mesh")
+        return out[:self.ncells]
 
     def mlp_forward(self, d_params: int, n: int, d_feat: int, d_class: int, d_logits: int = 0):
         _check(lib().ibgpu_mlp_forward(self._ctx, ctypes.c_void_p(d_params), int(n),

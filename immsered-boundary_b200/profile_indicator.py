@@ -35,7 +35,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--rows", type=int, default=262144)
     ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--mesh", type=int, default=0,
+                    help="instead: learned tagging of every cell of an N x N vortex case")
     a = ap.parse_args()
+    if a.mesh:
+        return mesh_tagging(a.mesh, a.steps)
     import torch
     pkg = _pkg()
     ib, ind, wl = pkg.ibgpu, pkg.indicator, pkg.workloads
@@ -54,6 +58,29 @@ def main():
     torch.cuda.synchronize()
     dt = (time.perf_counter() - t0) / a.steps
     print(f"{a.rows} rows: {dt * 1e3:.3f} ms per training step (wall, incl. host sync)")
+    sol.close()
+
+
+def mesh_tagging(n: int, reps: int):
+    """ibgpu_tag_mesh (learned) on every cell of an n x n case; the kernel
+    of interest is ``mlp_tag_mesh_kernel``."""
+    import torch
+    pkg = _pkg()
+    ib, ind, wl = pkg.ibgpu, pkg.indicator, pkg.workloads
+    P, cells, prim = wl.vortex_case(n)
+    sol = ib.FlowSolver(P)
+    sol.upload_topology(**cells)
+    sol.init_flow(prim)
+    li = ind.LearnedIndicator(sol, seed=0)
+    rule = wl.naca_tag_rule(1, [10.0 / n])
+    sol.tag_mesh(rule, li.params.data_ptr())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        tags = sol.tag_mesh(rule, li.params.data_ptr())
+    dt = (time.perf_counter() - t0) / reps
+    print(f"{n}x{n}: {dt * 1e3:.3f} ms per ibgpu_tag_mesh call ({n * n / dt / 1e9:.3f} G cells/s), "
+          f"tag counts {np.bincount(tags, minlength=4).tolist()}")
     sol.close()
 
 

@@ -393,6 +393,18 @@ int ibgpu_mlp_train_step(ibgpu_ctx *ctx, float *d_params, float *d_m, float *d_v
 int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
                       const float *d_params, uint8_t *out);
 
+/* Signed wall distance of every uploaded cell row (Box::pair.signdis), kept
+ * on the device per cell until the next topology upload; cells without it
+ * count as far from any wall. */
+int ibgpu_upload_signdis(ibgpu_ctx *ctx, const double *signdis);
+
+/* Tags of every row of the uploaded cell list (0 for rows that are not
+ * normal cells): the learned indicator when d_params is non-NULL (features
+ * gathered from the device state inside the tensor-core kernel, no feature
+ * matrix; centres from the cell positions), else the plain criterion. */
+int ibgpu_tag_mesh(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
+                   uint8_t *tags);
+
 const char *ibgpu_errstr(int code);
 /* Last CUDA error string seen by this thread's most recent failing call. */
 const char *ibgpu_last_error(void);

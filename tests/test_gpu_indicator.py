@@ -194,3 +194,39 @@ def test_training_beats_untrained_and_majority(cuda_lib, naca):
         tags = rg.tags(B)
     assert len(rg.mismatch) == 2 and tags.shape == (n,)
     assert rg.mismatch[0][1] < 0.5
+
+
+def test_tag_mesh_plain_and_learned(cuda_lib):
+    """Whole-mesh tagging from the device state: the plain criterion per
+    normal cell equals the oracle's, and the fused learned kernel (features
+    gathered inside the tensor-core kernel) agrees with the learned decision
+    of the explicit-box path."""
+    g = make_golden.load(NAME)
+    sol = wl.naca_solver(g, 0, ib.FP64)
+    _, dh = tag_rows(NAME)
+    rule = wl.naca_tag_rule(3, dh)
+    sol.upload_signdis(g["signdis"])
+    got = sol.tag_mesh(rule)
+    normal = (g["kind"] == ib.BOX_NORMAL)
+    lv = g["level"].astype(np.int64)
+    xc = (g["ix"] + 0.5) * dh[lv]
+    yc = (g["iy"] + 0.5) * dh[lv]
+    ref = io.tag_plain(io.naca_rule(3, dh), lv, xc, yc, g["signdis"])
+    assert np.array_equal(got[normal], ref[normal])
+    assert np.all(got[~normal] == 0)
+    # learned: train briefly, then compare the two deployment paths
+    t, _ = tag_rows(NAME)
+    t = t[t[:, 8] == 1]
+    B = boxes_of(t)
+    li = ind.LearnedIndicator(sol, seed=1)
+    X = li.features(rule, B)
+    y = ind.classes_from_tags(sol.tag_plain(rule, B["level"], B["xc"], B["yc"], B["signdis"]))
+    li.train(X, y, steps=200, batch=2048, lr=3e-3)
+    mesh_tags = sol.tag_mesh(rule, li.params.data_ptr())
+    box_tags = li.tags(rule, B)
+    row = {(int(l), int(x), int(yy)): i for i, (l, x, yy) in
+           enumerate(zip(g["level"], g["ix"], g["iy"]))}
+    idx = np.array([row[(int(a), int(b), int(c))] for a, b, c in t[:, :3]])
+    agree = np.mean(mesh_tags[idx] == box_tags)
+    assert agree >= 0.999, agree
+    sol.close()
