@@ -347,14 +347,13 @@ __device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const 
     rs[2] = muscl_right_fast<LIM>(cL.z, cR.z, o.z);
     rs[3] = muscl_right_fast<LIM>(cL.w, cR.w, o.w);
   }
+  // normal / tangential velocity by selection (one flux evaluation even
+  // when the lanes of a warp mix x- and y-faces)
   R fm, fn, ft, fe;
-  if (xdir) {
-    roe_flux_states<R>(g, area, ls[0], ls[1], ls[2], ls[3], rs[0], rs[1], rs[2], rs[3], fm, fn, ft, fe);
-    out = Q4<R>{fm, fn, ft, fe};
-  } else {
-    roe_flux_states<R>(g, area, ls[0], ls[2], ls[1], ls[3], rs[0], rs[2], rs[1], rs[3], fm, fn, ft, fe);
-    out = Q4<R>{fm, ft, fn, fe};
-  }
+  const R lun = xdir ? ls[1] : ls[2], lut = xdir ? ls[2] : ls[1];
+  const R run = xdir ? rs[1] : rs[2], rut = xdir ? rs[2] : rs[1];
+  roe_flux_states<R>(g, area, ls[0], lun, lut, ls[3], rs[0], run, rut, rs[3], fm, fn, ft, fe);
+  out = Q4<R>{fm, xdir ? fn : ft, xdir ? ft : fn, fe};
   return out;
 }
 
@@ -510,18 +509,17 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
                                   (ty + 1) * kTile + tx, false, uni, g, ay);
     S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
     if (tid < 32) {
+      // east column (lanes 0..15) and north row (lanes 16..31) through one
+      // call site, so the warp evaluates the flux once
       const int e = tid & 15;
-      if (tid < 16) {
-        const int r = (e + kHalo) * kReg + kTile + kHalo;
-        o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, r - 1, r, 1, e * kSX + kTile,
-                                      e * kSX + kTile + 1, true, uni, g, ax);
-        S::st(fx, e * (kTile + 1) + kTile, NF, o.x, o.y, o.z, o.w);
-      } else {
-        const int r = (kTile + kHalo) * kReg + e + kHalo;
-        o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, r - kReg, r, kReg, kTile * kTile + e,
-                                      (kTile + 1) * kTile + e, false, uni, g, ay);
-        S::st(fy, kTile * kTile + e, NF, o.x, o.y, o.z, o.w);
-      }
+      const bool xd = tid < 16;
+      const int r = xd ? (e + kHalo) * kReg + kTile + kHalo : (kTile + kHalo) * kReg + e + kHalo;
+      const int step = xd ? 1 : kReg;
+      const int sL = xd ? e * kSX + kTile : kTile * kTile + e;
+      const int sR = xd ? e * kSX + kTile + 1 : (kTile + 1) * kTile + e;
+      o = fast_face<R, LIM, NQ, NS>(sq, sfl, xd ? slx : sly, r - step, r, step, sL, sR, xd, uni,
+                                    g, xd ? ax : ay);
+      S::st(xd ? fx : fy, xd ? e * (kTile + 1) + kTile : kTile * kTile + e, NF, o.x, o.y, o.z, o.w);
     }
   }
   __syncthreads();
@@ -605,7 +603,8 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
-__global__ void __launch_bounds__(kTileCells) stage_kernel_fast(StageArgs a, CaseConst cc) {
+__global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
+    stage_kernel_fast(StageArgs a, CaseConst cc) {
   stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase);
 }
 

@@ -36,10 +36,31 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"])
     ap.add_argument("--limiter", default="vanleer", choices=["vanleer", "minmod"])
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead: this many batched vortex cases (50k..800k cells, seed 0)")
     a = ap.parse_args()
     pkg = _pkg()
     ib, wl = pkg.ibgpu, pkg.workloads
     prec = {"fp64": ib.FP64, "exact": ib.FP64_EXACT, "mixed": ib.MIXED}[a.precision]
+    if a.batch:
+        sols = []
+        for P, cells, prim in wl.batch_vortex_cases(a.batch, seed=0, precision=prec):
+            s = ib.FlowSolver(P)
+            s.upload_topology(**cells)
+            s.init_flow(prim)
+            sols.append(s)
+        b = ib.Batch(sols)
+        b.run(0, 1)
+        t0 = time.perf_counter()
+        b.run(1, a.steps)
+        dt = (time.perf_counter() - t0) / max(a.steps, 1)
+        ncell = sum(s.ncells for s in sols)
+        print(f"batch of {a.batch} cases ({ncell} cells) {a.precision}: {dt * 1e3:.3f} ms/step "
+              f"({ncell / dt / 1e9:.2f} G cell-updates/s, wall), {b.info()}")
+        b.close()
+        for s in sols:
+            s.close()
+        return
     lim = ib.LIM_VANLEER if a.limiter == "vanleer" else ib.LIM_MINMOD
     P, cells, prim = wl.vortex_case(a.n, limiter=lim, precision=prec)
     sol = ib.FlowSolver(P)
