@@ -10,6 +10,10 @@
 // of units in the last place of the correctly rounded value for the normal,
 // positive operands the flux uses (densities, sound speeds, 1 + r); they are
 // not IEEE-exact, which is why the exact build does not use them.
+// Inside the flux and the limiter a single Newton step suffices (rcp1,
+// rsqrt1: relative error of order 1e-14, far inside the FP64 build's
+// per-step tolerance, and these quantities only scale dissipation terms and
+// slopes); primitive recovery keeps the two-step versions.
 // FP32 (mixed precision): the PTX single-precision approximations directly.
 #pragma once
 
@@ -30,6 +34,16 @@ struct FastMath<double> {
     e = fma(-x, y, 1.0);
     y = fma(y, e, y);
     return y;
+  }
+  static __device__ __forceinline__ double rcp1(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return fma(y, fma(-x, y, 1.0), y);
+  }
+  static __device__ __forceinline__ double rsqrt1(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return fma(y, fma(-0.5 * x * y, y, 0.5), y);
   }
   static __device__ __forceinline__ double div(double a, double b) {
     double r = rcp(b);
@@ -58,12 +72,14 @@ struct FastMath<float> {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
   }
+  static __device__ __forceinline__ float rcp1(float x) { return rcp(x); }
   static __device__ __forceinline__ float div(float a, float b) { return a * rcp(b); }
   static __device__ __forceinline__ float rsqrt(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
   }
+  static __device__ __forceinline__ float rsqrt1(float x) { return rsqrt(x); }
   static __device__ __forceinline__ float sqrt(float x) {
     float y;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));

@@ -174,7 +174,7 @@ __device__ __forceinline__ R limited_slope(R a, R b) {
   // FP64: the Newton-refined reciprocal is long, and uniform regions
   // (a = b = 0) skip it warp-wide
   if (!(ab > R(0))) return R(0);
-  return ab * FastMath<R>::rcp(a + b);
+  return ab * FastMath<R>::rcp1(a + b);
 }
 
 // The reference's explicit one-sided reconstructions, used for faces whose
@@ -207,7 +207,7 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
                                                 R lp, R rroe, R run, R rut, R rp, R &f_mass,
                                                 R &f_n, R &f_t, R &f_e) {
   typedef FastMath<R> M;
-  const R aL = M::rsqrt(lroe), aR = M::rsqrt(rroe);
+  const R aL = M::rsqrt1(lroe), aR = M::rsqrt1(rroe);
   const R ilroe = aL * aL, irroe = aR * aR;
   const R sL = lroe * aL, sR = rroe * aR;  // sqrt(rho)
   const R lpr = lp * ilroe, rpr = rp * irroe;  // p / rho
@@ -216,14 +216,14 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
   const R re = g.Cv * rT + R(0.5) * (run * run + rut * rut);
   const R lv = lun, rv = run;
   const R droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = rv - lv;
-  const R isum = M::rcp(sL + sR);
+  const R isum = M::rcp1(sL + sR);
   const R wL = sL * isum, wR = sR * isum;
   const R a_roe = sL * sR;
   const R a_un = lun * wL + run * wR;
   const R a_ut = lut * wL + rut * wR;
   const R a_h = (le + lpr) * wL + (re + rpr) * wR;
   const R csquare = g.gm1 * (a_h - R(0.5) * (a_un * a_un + a_ut * a_ut));
-  const R rc = M::rsqrt(csquare);
+  const R rc = M::rsqrt1(csquare);
   const R a_c = csquare * rc;
   const R icsq = rc * rc;
   const R ubar = a_un;
@@ -235,11 +235,11 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
   const R alpha0 = faceareaxabsubar * (droe - dp * icsq);
   const R T_a = (lT + rT) * R(0.5);
   const R V_a = (lv + rv) * R(0.5);
-  const R Ma_a = fabs(V_a) * M::rsqrt(g.gamaRg * T_a);
+  const R Ma_a = fabs(V_a) * M::rsqrt1(g.gamaRg * T_a);
   const R f_Ma = smin(smax(Ma_a, g.Ma), R(1));
   const R s0 = (R(1) - f_Ma) * (R(1) - f_Ma);
   const R n0sq = R(4) * csquare * f_Ma + s0 * ubar * ubar;
-  const R namda0 = n0sq * M::rsqrt(n0sq);
+  const R namda0 = n0sq * M::rsqrt1(n0sq);
   const R namda1 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar + namda0));
   const R namda2 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar - namda0));
   const R alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
