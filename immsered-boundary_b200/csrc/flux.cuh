@@ -255,4 +255,84 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
         (a_h * alpha3 + ubar * alpha4 + a_ut * alphat - (csquare * g.inv_gm1) * alpha0);
 }
 
+// ---- paired FP32 flux (mixed build) ----------------------------------------
+// Two faces per thread as the lanes of a float2, evaluated with the sm_100
+// paired FP32 instructions (add/mul/fma .f32x2: one instruction per two
+// operations); roots and reciprocals stay per lane.
+struct F2 {
+  float2 v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ F2 f2(float a) { return F2{make_float2(a, a)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  return F2{__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))};
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ F2 abs2(F2 a) { return f2(fabsf(a.v.x), fabsf(a.v.y)); }
+__device__ __forceinline__ F2 rsqrt2(F2 a) {
+  return f2(FastMath<float>::rsqrt(a.v.x), FastMath<float>::rsqrt(a.v.y));
+}
+__device__ __forceinline__ F2 rcp2(F2 a) {
+  return f2(FastMath<float>::rcp(a.v.x), FastMath<float>::rcp(a.v.y));
+}
+__device__ __forceinline__ F2 clamp2(F2 a, float lo, float hi) {
+  return f2(fminf(fmaxf(a.v.x, lo), hi), fminf(fmaxf(a.v.y, lo), hi));
+}
+
+// roe_flux_states for two faces at once (same arithmetic, paired).
+__device__ __forceinline__ void roe_flux_pair(const Gas<float> &g, F2 area, F2 lroe, F2 lun,
+                                              F2 lut, F2 lp, F2 rroe, F2 run, F2 rut, F2 rp,
+                                              F2 &f_mass, F2 &f_n, F2 &f_t, F2 &f_e) {
+  const F2 half = f2(0.5f);
+  const F2 aL = rsqrt2(lroe), aR = rsqrt2(rroe);
+  const F2 ilroe = aL * aL, irroe = aR * aR;
+  const F2 sL = lroe * aL, sR = rroe * aR;
+  const F2 lpr = lp * ilroe, rpr = rp * irroe;
+  const F2 lT = lpr * f2(g.inv_Rg), rT = rpr * f2(g.inv_Rg);
+  const F2 le = fma2(f2(g.Cv), lT, half * fma2(lun, lun, lut * lut));
+  const F2 re = fma2(f2(g.Cv), rT, half * fma2(run, run, rut * rut));
+  const F2 droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = run - lun;
+  const F2 isum = rcp2(sL + sR);
+  const F2 wL = sL * isum, wR = sR * isum;
+  const F2 a_roe = sL * sR;
+  const F2 a_un = fma2(lun, wL, run * wR);
+  const F2 a_ut = fma2(lut, wL, rut * wR);
+  const F2 a_h = fma2(le + lpr, wL, (re + rpr) * wR);
+  const F2 csquare = f2(g.gm1) * (a_h - half * fma2(a_un, a_un, a_ut * a_ut));
+  const F2 rc = rsqrt2(csquare);
+  const F2 a_c = csquare * rc;
+  const F2 icsq = rc * rc;
+  const F2 ubar = a_un;
+  const F2 namda3 = abs2(ubar);
+  const F2 coef12 = half * icsq * area;
+  const F2 roe0cxdubar = a_roe * a_c * dubar;
+  const F2 faceareaxabsubar = area * namda3;
+  const F2 halffacearea = half * area;
+  const F2 alpha0 = faceareaxabsubar * (droe - dp * icsq);
+  const F2 T_a = (lT + rT) * half;
+  const F2 V_a = (lun + run) * half;
+  const F2 Ma_a = abs2(V_a) * rsqrt2(f2(g.gamaRg) * T_a);
+  const F2 f_Ma = clamp2(Ma_a, g.Ma, 1.0f);
+  const F2 om = f2(1.0f) - f_Ma;
+  const F2 s0 = om * om;
+  const F2 n0sq = fma2(f2(4.0f) * csquare, f_Ma, s0 * ubar * ubar);
+  const F2 namda0 = n0sq * rsqrt2(n0sq);
+  const F2 opf = (f2(1.0f) + f_Ma) * ubar;
+  const F2 namda1 = abs2(half * (opf + namda0));
+  const F2 namda2 = abs2(half * (opf - namda0));
+  const F2 alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
+  const F2 alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
+  const F2 alpha3 = alpha0 + alpha1 + alpha2;
+  const F2 alpha4 = a_c * (alpha1 - alpha2);
+  const F2 alphat = faceareaxabsubar * (a_roe * dut);
+  const F2 ml = lroe * lun, mr = rroe * run;
+  f_mass = (ml + mr) * halffacearea - alpha3;
+  f_n = (fma2(ml, lun, lp) + fma2(mr, run, rp)) * halffacearea - fma2(a_un, alpha3, alpha4);
+  f_t = fma2(ml, lut, mr * rut) * halffacearea - fma2(a_ut, alpha3, alphat);
+  f_e = fma2(fma2(le, lroe, lp), lun, fma2(re, rroe, rp) * run) * halffacearea -
+        (fma2(a_h, alpha3, fma2(ubar, alpha4, a_ut * alphat)) - (csquare * f2(g.inv_gm1)) * alpha0);
+}
+
 }  // namespace ibgpu

@@ -310,11 +310,13 @@ struct SRec<double> {
 
 // One face of the stencil region: cells rL1 | rR1 (rL2, rR2 one further
 // out), slope records sL, sR; dir 0 = x (normal u), 1 = y (normal v).
+// Reconstructed left/right states of one face; false (states set to a
+// benign 1) when the face carries no flux.
 template <typename R, int LIM, int NQ, int NS>
-__device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const uint8_t *sfl,
-                                           const typename SRec<R>::V *sl, int rL1, int rR1, int step,
-                                           int sL, int sR, bool xdir, bool uni, const Gas<R> &g,
-                                           R area) {
+__device__ __forceinline__ bool face_recon(const typename SRec<R>::V *sq, const uint8_t *sfl,
+                                           const typename SRec<R>::V *sl, int rL1, int rR1,
+                                           int step, int sL, int sR, bool uni, R (&ls)[4],
+                                           R (&rs)[4]) {
   using S = SRec<R>;
   bool active = true, hasL2 = true, hasR2 = true;
   if (!uni) {
@@ -323,10 +325,12 @@ __device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const 
     hasL2 = (sfl[rL1 - step] & CF_PRESENT) != 0;
     hasR2 = (sfl[rR1 + step] & CF_PRESENT) != 0;
   }
-  Q4<R> out = {R(0), R(0), R(0), R(0)};
-  if (!active) return out;
+  if (!active) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ls[c] = rs[c] = R(1);
+    return false;
+  }
   const Q4<R> cL = S::ld(sq, rL1, NQ), cR = S::ld(sq, rR1, NQ);
-  R ls[4], rs[4];
   if (hasL2) {
     const Q4<R> s = S::ld(sl, sL, NS);
     ls[0] = cL.x + s.x; ls[1] = cL.y + s.y; ls[2] = cL.z + s.z; ls[3] = cL.w + s.w;
@@ -347,6 +351,17 @@ __device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const 
     rs[2] = muscl_right_fast<LIM>(cL.z, cR.z, o.z);
     rs[3] = muscl_right_fast<LIM>(cL.w, cR.w, o.w);
   }
+  return true;
+}
+
+template <typename R, int LIM, int NQ, int NS>
+__device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const uint8_t *sfl,
+                                           const typename SRec<R>::V *sl, int rL1, int rR1, int step,
+                                           int sL, int sR, bool xdir, bool uni, const Gas<R> &g,
+                                           R area) {
+  R ls[4], rs[4];
+  Q4<R> out = {R(0), R(0), R(0), R(0)};
+  if (!face_recon<R, LIM, NQ, NS>(sq, sfl, sl, rL1, rR1, step, sL, sR, uni, ls, rs)) return out;
   // normal / tangential velocity by selection (one flux evaluation even
   // when the lanes of a warp mix x- and y-faces)
   R fm, fn, ft, fe;
@@ -384,6 +399,48 @@ __device__ __forceinline__ void fast_slope(const typename SRec<R>::V *sq, const 
 // Faces whose outer stencil cell is missing use the reference's one-sided
 // reconstruction (NS_Solver.H:743-750).  The residual, update and primitive
 // recovery run in FP64 in every mode.
+// The 768 16-byte pieces of a uniform tile's stencil region: the tile's 4
+// fields (w < 512), the west/east 2-column strips (w < 640) and the
+// south/north 2-row strips; piece w is two adjacent cells of field f whose
+// first cell lands on region record dst.
+__device__ __forceinline__ void uniform_piece_dst(int w, int &f, int &dst) {
+  if (w < 512) {
+    f = w >> 7;
+    const int p = w & 127;
+    dst = ((p >> 3) + kHalo) * kReg + (p & 7) * 2 + kHalo;
+  } else if (w < 640) {
+    const int v = w - 512;
+    f = v >> 5;
+    dst = ((v & 15) + kHalo) * kReg + (((v >> 4) & 1) ? kTile + kHalo : 0);
+  } else {
+    const int v = w - 640;
+    f = v >> 5;
+    const int north = (v >> 4) & 1, rr = (v >> 3) & 1;
+    dst = (north ? kTile + kHalo + rr : rr) * kReg + (v & 7) * 2 + kHalo;
+  }
+}
+
+// Global address of piece w of tile `tile`.
+__device__ __forceinline__ const double *uniform_piece(const StageArgs &a, int tile, int w, int &f,
+                                                       int &dst) {
+  uniform_piece_dst(w, f, dst);
+  if (w < 512) {
+    const int p = w & 127;
+    return a.sin[f] + (int64_t)tile * kTileCells + (p >> 3) * kTile + (p & 7) * 2;
+  }
+  if (w < 640) {
+    const int v = w - 512;
+    const int east = (v >> 4) & 1, row = v & 15;
+    const int nb = a.tile_nb[tile * 9 + (east ? 5 : 3)];
+    return a.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
+  }
+  const int v = w - 640;
+  const int north = (v >> 4) & 1, rr = (v >> 3) & 1;
+  const int nb = a.tile_nb[tile * 9 + (north ? 7 : 1)];
+  const int srow = north ? rr : kTile - 2 + rr;
+  return a.sin[f] + (int64_t)nb * kTileCells + srow * kTile + (v & 7) * 2;
+}
+
 template <typename R, int LIM, bool VISC, bool FINAL>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseConst &cc,
                                                 const int tile, const int phase) {
@@ -407,35 +464,12 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
   const bool uni = a.tile_uniform != nullptr && a.tile_uniform[tile] != 0;
 
   if (uni) {
-    // 768 16-byte loads: the tile's 4 fields (512), the west/east 2-column
-    // strips (128) and the south/north 2-row strips (128)
+    // 768 16-byte pieces straight from global memory
 #pragma unroll
     for (int it = 0; it < 3; ++it) {
       const int w = tid + it * kTileCells;
       int f, dst;
-      const double *src;
-      if (w < 512) {
-        f = w >> 7;
-        int p = w & 127, row = p >> 3, cp = (p & 7) * 2;
-        src = a.sin[f] + (int64_t)tile * kTileCells + row * kTile + cp;
-        dst = (row + kHalo) * kReg + cp + kHalo;
-      } else if (w < 640) {
-        int v = w - 512;
-        f = v >> 5;
-        int east = (v >> 4) & 1, row = v & 15;
-        int nb = a.tile_nb[tile * 9 + (east ? 5 : 3)];
-        src = a.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
-        dst = (row + kHalo) * kReg + (east ? kTile + kHalo : 0);
-      } else {
-        int v = w - 640;
-        f = v >> 5;
-        int north = (v >> 4) & 1, rr = (v >> 3) & 1, cp = (v & 7) * 2;
-        int nb = a.tile_nb[tile * 9 + (north ? 7 : 1)];
-        int srow = north ? rr : kTile - 2 + rr;
-        src = a.sin[f] + (int64_t)nb * kTileCells + srow * kTile + cp;
-        dst = (north ? kTile + kHalo + rr : rr) * kReg + cp + kHalo;
-      }
-      const double2 val = __ldg(reinterpret_cast<const double2 *>(src));
+      const double2 val = __ldg(reinterpret_cast<const double2 *>(uniform_piece(a, tile, w, f, dst)));
       *S::comp(sq, dst, NQ, f) = (R)val.x;
       *S::comp(sq, dst + 1, NQ, f) = (R)val.y;
     }
@@ -502,12 +536,32 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
   //      east column (threads 0..15) and north row (threads 16..31)
   {
     const int rR1 = (ty + kHalo) * kReg + (tx + kHalo);
-    Q4<R> o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
-                                        ty * kSX + tx + 1, true, uni, g, ax);
-    S::st(fx, ty * (kTile + 1) + tx, NF, o.x, o.y, o.z, o.w);
-    o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
-                                  (ty + 1) * kTile + tx, false, uni, g, ay);
-    S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
+    Q4<R> o;
+    if constexpr (sizeof(R) == 4) {
+      // mixed build: the cell's west and south faces as the two lanes of
+      // one paired-FP32 flux evaluation
+      R lx[4], rx[4], ly[4], ry[4];
+      const bool ax_ok = face_recon<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
+                                                   ty * kSX + tx + 1, uni, lx, rx);
+      const bool ay_ok = face_recon<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg,
+                                                   ty * kTile + tx, (ty + 1) * kTile + tx, uni, ly,
+                                                   ry);
+      F2 fm, fn, ft, fe;
+      roe_flux_pair(g, f2(ax, ay), f2(lx[0], ly[0]), f2(lx[1], ly[2]), f2(lx[2], ly[1]),
+                    f2(lx[3], ly[3]), f2(rx[0], ry[0]), f2(rx[1], ry[2]), f2(rx[2], ry[1]),
+                    f2(rx[3], ry[3]), fm, fn, ft, fe);
+      if (ax_ok) S::st(fx, ty * (kTile + 1) + tx, NF, fm.v.x, fn.v.x, ft.v.x, fe.v.x);
+      else S::st(fx, ty * (kTile + 1) + tx, NF, R(0), R(0), R(0), R(0));
+      if (ay_ok) S::st(fy, ty * kTile + tx, NF, fm.v.y, ft.v.y, fn.v.y, fe.v.y);
+      else S::st(fy, ty * kTile + tx, NF, R(0), R(0), R(0), R(0));
+    } else {
+      o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
+                                    ty * kSX + tx + 1, true, uni, g, ax);
+      S::st(fx, ty * (kTile + 1) + tx, NF, o.x, o.y, o.z, o.w);
+      o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
+                                    (ty + 1) * kTile + tx, false, uni, g, ay);
+      S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
+    }
     if (tid < 32) {
       // east column (lanes 0..15) and north row (lanes 16..31) through one
       // call site, so the warp evaluates the flux once
@@ -537,13 +591,19 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
     const R syl[4] = {fyl.x, fyl.y, fyl.z, fyl.w}, syh[4] = {fyh.x, fyh.y, fyh.z, fyh.w};
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      double sx = (double)sxl[c] - (double)sxh[c];
-      double sy = (double)syl[c] - (double)syh[c];
-      if (VISC) {
-        sx += a.vsd[(int64_t)c * a.nslots + slot];
-        sy += a.vsd[(int64_t)(4 + c) * a.nslots + slot];
+      if (sizeof(R) == 4 && !VISC) {
+        // mixed build: face differences in FP32 (the fluxes are FP32), one
+        // conversion per component
+        res[c] = (double)((sxl[c] - sxh[c]) + (syl[c] - syh[c]));
+      } else {
+        double sx = (sizeof(R) == 4) ? (double)(sxl[c] - sxh[c]) : (double)sxl[c] - (double)sxh[c];
+        double sy = (sizeof(R) == 4) ? (double)(syl[c] - syh[c]) : (double)syl[c] - (double)syh[c];
+        if (VISC) {
+          sx += a.vsd[(int64_t)c * a.nslots + slot];
+          sy += a.vsd[(int64_t)(4 + c) * a.nslots + slot];
+        }
+        res[c] = sx + sy;
       }
-      res[c] = sx + sy;
     }
     const double dt = a.diag->dt;
     const double scale = (a.tp * dt) * L.step_num * L.inv_vol;
@@ -607,6 +667,7 @@ __global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
   stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase);
 }
+
 
 // Batched stage: persistent CTAs over a work list of (case, tile) pairs of
 // several independent cases (each its own mesh, state and constants); the
@@ -721,6 +782,7 @@ __global__ void gather_state_kernel(double *rows, const int32_t *cell_slot, int6
 #else
 #define IBGPU_STAGE_KERNEL stage_kernel
 #endif
+
 
 template <typename R, int LIM>
 static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
