@@ -36,16 +36,25 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
   return v;
 }
 
-// Residual max-norm of a 256-thread block into the step's diag: warp and
+// Threads of a fast-build stage CTA: FP64 adds a ninth warp that owns the
+// tile's east/north edge faces and outer slopes, so every warp computes two
+// faces; FP32 keeps 8 warps (its face work is cheap enough).
+template <typename R>
+struct StageThreads {
+  static constexpr int value = sizeof(R) == 8 ? 288 : kTileCells;
+};
+
+// Residual max-norm of a block of up to 9 warps into the step's diag: warp and
 // block maxima, then one atomicMax per component and block, skipped when the
 // global value is already as large (the maximum settles after the first
 // blocks, so later blocks only read it instead of serialising on four
 // addresses).  Components map to res_max[0,1,2,4] (no z momentum in 2-D).
 // Every thread of the block must call it; sred is shared scratch of 32
 // words that no thread reads or writes any more.
+template <int NT = kTileCells>
 __device__ __forceinline__ void block_resnorm(const unsigned long long (&rb)[4], DevDiag *d,
                                               unsigned long long *sred) {
-  constexpr int kW = kTileCells / 32;
+  constexpr int kW = NT / 32;
   const int tid = threadIdx.x;
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
@@ -455,8 +464,11 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
   __shared__ V fx[S::kPlanes * NF];   // x-face (i, j) at j*17 + i
   __shared__ V fy[S::kPlanes * NF];   // y-face (i, j) at j*16 + i
 
+  constexpr int NT = StageThreads<R>::value;
   const int tid = threadIdx.x;
-  const int tx = tid & (kTile - 1), ty = tid >> 4;
+  const int tx = tid & (kTile - 1), ty = (NT > kTileCells) ? ((tid >> 4) & (kTile - 1)) : (tid >> 4);
+  // a cell of the tile (the ninth warp owns none)
+  const bool own = (NT > kTileCells) ? tid < kTileCells : true;
   const int lvl = a.tile_level[tile];
   const LevelConst &L = cc.lev[lvl];
   // uniform tile: it and its four side neighbours hold only leaf cells that
@@ -466,15 +478,16 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
   if (uni) {
     // 768 16-byte pieces straight from global memory
 #pragma unroll
-    for (int it = 0; it < 3; ++it) {
-      const int w = tid + it * kTileCells;
+    for (int it = 0; it < (768 + NT - 1) / NT; ++it) {
+      const int w = tid + it * NT;
+      if (w >= 768) break;
       int f, dst;
       const double2 val = __ldg(reinterpret_cast<const double2 *>(uniform_piece(a, tile, w, f, dst)));
       *S::comp(sq, dst, NQ, f) = (R)val.x;
       *S::comp(sq, dst + 1, NQ, f) = (R)val.y;
     }
   } else {
-    for (int r = tid; r < kReg * kReg; r += kTileCells) {
+    for (int r = tid; r < kReg * kReg; r += NT) {
       int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
       int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
       int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
@@ -502,7 +515,23 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 
   // ---- per-cell limited slopes: (tx, ty) in both directions, then the
   //      two outer columns (x) and rows (y) of the face stencils
-  {
+  if (NT > kTileCells) {
+    if (own) {
+      const int rc = (ty + kHalo) * kReg + (tx + kHalo);
+      fast_slope<R, LIM, NQ, NS>(sq, sfl, slx, ty * kSX + tx + 1, rc, 1, uni);
+      fast_slope<R, LIM, NQ, NS>(sq, sfl, sly, (ty + 1) * kTile + tx, rc, kReg, uni);
+    } else {
+      // ninth warp: one outer x-slope (columns -1, 16) and one outer
+      // y-slope (rows -1, 16) per lane
+      const int e = (tid - kTileCells) & 15, hi = (tid - kTileCells) >= 16;
+      const int col = hi ? kTile : -1;
+      fast_slope<R, LIM, NQ, NS>(sq, sfl, slx, e * kSX + col + 1, (e + kHalo) * kReg + col + kHalo,
+                                 1, uni);
+      const int row = hi ? kTile : -1;
+      fast_slope<R, LIM, NQ, NS>(sq, sfl, sly, (row + 1) * kTile + e,
+                                 (row + kHalo) * kReg + e + kHalo, kReg, uni);
+    }
+  } else {
     const int rc = (ty + kHalo) * kReg + (tx + kHalo);
     fast_slope<R, LIM, NQ, NS>(sq, sfl, slx, ty * kSX + tx + 1, rc, 1, uni);
     fast_slope<R, LIM, NQ, NS>(sq, sfl, sly, (ty + 1) * kTile + tx, rc, kReg, uni);
@@ -537,7 +566,9 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
   {
     const int rR1 = (ty + kHalo) * kReg + (tx + kHalo);
     Q4<R> o;
-    if constexpr (sizeof(R) == 4) {
+    if (!own) {
+      // ninth warp: edge faces only (below)
+    } else if constexpr (sizeof(R) == 4) {
       // mixed build: the cell's west and south faces as the two lanes of
       // one paired-FP32 flux evaluation
       R lx[4], rx[4], ly[4], ry[4];
@@ -562,11 +593,12 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
                                     (ty + 1) * kTile + tx, false, uni, g, ay);
       S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
     }
-    if (tid < 32) {
+    const int et = tid - (NT > kTileCells ? kTileCells : 0);
+    if (et >= 0 && et < 32) {
       // east column (lanes 0..15) and north row (lanes 16..31) through one
       // call site, so the warp evaluates the flux once
-      const int e = tid & 15;
-      const bool xd = tid < 16;
+      const int e = et & 15;
+      const bool xd = et < 16;
       const int r = xd ? (e + kHalo) * kReg + kTile + kHalo : (kTile + kHalo) * kReg + e + kHalo;
       const int step = xd ? 1 : kReg;
       const int sL = xd ? e * kSX + kTile : kTile * kTile + e;
@@ -580,8 +612,9 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 
   // ---- residual, update, primitive recovery (FP64)
   const int64_t slot = (int64_t)tile * kTileCells + tid;
-  const uint8_t fl = uni ? (uint8_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM)
-                         : sfl[(ty + kHalo) * kReg + (tx + kHalo)];
+  const uint8_t fl = !own ? (uint8_t)0
+                         : uni ? (uint8_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM)
+                               : sfl[(ty + kHalo) * kReg + (tx + kHalo)];
   unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
   if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
     const Q4<R> fxl = S::ld(fx, ty * (kTile + 1) + tx, NF), fxh = S::ld(fx, ty * (kTile + 1) + tx + 1, NF);
@@ -659,11 +692,11 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
     }
   }
   // the y-slope records are dead after the face phase: reuse them
-  if (FINAL) block_resnorm(rb, a.diag, reinterpret_cast<unsigned long long *>(sly));
+  if (FINAL) block_resnorm<NT>(rb, a.diag, reinterpret_cast<unsigned long long *>(sly));
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
-__global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
+__global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
   stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase);
 }
@@ -676,7 +709,7 @@ __global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
 // (abort ordering), written on the device so a captured graph can replay
 // the launch for every step.
 template <typename R, int LIM, bool VISC, bool FINAL>
-__global__ void __launch_bounds__(kTileCells, sizeof(R) == 8 ? 4 : 6)
+__global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                        const int2 *__restrict__ work, int nwork, int stage, int nstages,
                        const int *__restrict__ phase_base) {
@@ -787,7 +820,11 @@ __global__ void gather_state_kernel(double *rows, const int32_t *cell_slot, int6
 template <typename R, int LIM>
 static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
                            bool final_stage, cudaStream_t st) {
+#ifdef IBGPU_FAST_BUILD
+  dim3 grid(ntiles), block(StageThreads<R>::value);
+#else
   dim3 grid(ntiles), block(kTileCells);
+#endif
   if (visc) {
     if (final_stage) IBGPU_STAGE_KERNEL<R, LIM, true, true><<<grid, block, 0, st>>>(a, cc);
     else IBGPU_STAGE_KERNEL<R, LIM, true, false><<<grid, block, 0, st>>>(a, cc);
@@ -817,7 +854,7 @@ template <typename R, int LIM>
 static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
                            bool final_stage, int grid, cudaStream_t st) {
-  dim3 g(grid), block(kTileCells);
+  dim3 g(grid), block(StageThreads<R>::value);
   if (visc) {
     if (final_stage)
       stage_kernel_batch<R, LIM, true, true><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
