@@ -255,84 +255,108 @@ __device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe,
         (a_h * alpha3 + ubar * alpha4 + a_ut * alphat - (csquare * g.inv_gm1) * alpha0);
 }
 
-// ---- paired FP32 flux (mixed build) ----------------------------------------
-// Two faces per thread as the lanes of a float2, evaluated with the sm_100
-// paired FP32 instructions (add/mul/fma .f32x2: one instruction per two
-// operations); roots and reciprocals stay per lane.
+// ---- paired flux: two faces per thread -----------------------------------
+// The west and south faces of a cell evaluated together.  FP32 (mixed
+// build): the lanes of a float2 through the sm_100 paired instructions
+// (add/mul/fma .f32x2, one instruction per two operations).  FP64: two
+// interleaved scalar chains, which doubles the independent work each warp
+// has in flight.  Roots and reciprocals stay per lane.
 struct F2 {
   float2 v;
 };
-__device__ __forceinline__ F2 f2(float a, float b) { return F2{make_float2(a, b)}; }
-__device__ __forceinline__ F2 f2(float a) { return F2{make_float2(a, a)}; }
+struct D2 {
+  double x, y;
+};
+__device__ __forceinline__ F2 pair(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ D2 pair(double a, double b) { return D2{a, b}; }
+__device__ __forceinline__ float lane0(F2 a) { return a.v.x; }
+__device__ __forceinline__ float lane1(F2 a) { return a.v.y; }
+__device__ __forceinline__ double lane0(D2 a) { return a.x; }
+__device__ __forceinline__ double lane1(D2 a) { return a.y; }
 __device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
 __device__ __forceinline__ F2 operator-(F2 a, F2 b) {
   return F2{__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))};
 }
 __device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
-__device__ __forceinline__ F2 abs2(F2 a) { return f2(fabsf(a.v.x), fabsf(a.v.y)); }
-__device__ __forceinline__ F2 rsqrt2(F2 a) {
-  return f2(FastMath<float>::rsqrt(a.v.x), FastMath<float>::rsqrt(a.v.y));
+__device__ __forceinline__ D2 operator+(D2 a, D2 b) { return D2{a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ D2 operator-(D2 a, D2 b) { return D2{a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ D2 operator*(D2 a, D2 b) { return D2{a.x * b.x, a.y * b.y}; }
+__device__ __forceinline__ D2 fma2(D2 a, D2 b, D2 c) { return D2{fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)}; }
+template <typename P>
+__device__ __forceinline__ P abs2(P a) {
+  return pair(fabs(lane0(a)), fabs(lane1(a)));
 }
-__device__ __forceinline__ F2 rcp2(F2 a) {
-  return f2(FastMath<float>::rcp(a.v.x), FastMath<float>::rcp(a.v.y));
+template <typename P>
+__device__ __forceinline__ P rsqrt2(P a) {
+  typedef decltype(lane0(a)) S;
+  return pair(FastMath<S>::rsqrt1(lane0(a)), FastMath<S>::rsqrt1(lane1(a)));
 }
-__device__ __forceinline__ F2 clamp2(F2 a, float lo, float hi) {
-  return f2(fminf(fmaxf(a.v.x, lo), hi), fminf(fmaxf(a.v.y, lo), hi));
+template <typename P>
+__device__ __forceinline__ P rcp2(P a) {
+  typedef decltype(lane0(a)) S;
+  return pair(FastMath<S>::rcp1(lane0(a)), FastMath<S>::rcp1(lane1(a)));
+}
+template <typename P, typename S>
+__device__ __forceinline__ P clamp2(P a, S lo, S hi) {
+  return pair(smin(smax(lane0(a), lo), hi), smin(smax(lane1(a), lo), hi));
 }
 
 // roe_flux_states for two faces at once (same arithmetic, paired).
-__device__ __forceinline__ void roe_flux_pair(const Gas<float> &g, F2 area, F2 lroe, F2 lun,
-                                              F2 lut, F2 lp, F2 rroe, F2 run, F2 rut, F2 rp,
-                                              F2 &f_mass, F2 &f_n, F2 &f_t, F2 &f_e) {
-  const F2 half = f2(0.5f);
-  const F2 aL = rsqrt2(lroe), aR = rsqrt2(rroe);
-  const F2 ilroe = aL * aL, irroe = aR * aR;
-  const F2 sL = lroe * aL, sR = rroe * aR;
-  const F2 lpr = lp * ilroe, rpr = rp * irroe;
-  const F2 lT = lpr * f2(g.inv_Rg), rT = rpr * f2(g.inv_Rg);
-  const F2 le = fma2(f2(g.Cv), lT, half * fma2(lun, lun, lut * lut));
-  const F2 re = fma2(f2(g.Cv), rT, half * fma2(run, run, rut * rut));
-  const F2 droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = run - lun;
-  const F2 isum = rcp2(sL + sR);
-  const F2 wL = sL * isum, wR = sR * isum;
-  const F2 a_roe = sL * sR;
-  const F2 a_un = fma2(lun, wL, run * wR);
-  const F2 a_ut = fma2(lut, wL, rut * wR);
-  const F2 a_h = fma2(le + lpr, wL, (re + rpr) * wR);
-  const F2 csquare = f2(g.gm1) * (a_h - half * fma2(a_un, a_un, a_ut * a_ut));
-  const F2 rc = rsqrt2(csquare);
-  const F2 a_c = csquare * rc;
-  const F2 icsq = rc * rc;
-  const F2 ubar = a_un;
-  const F2 namda3 = abs2(ubar);
-  const F2 coef12 = half * icsq * area;
-  const F2 roe0cxdubar = a_roe * a_c * dubar;
-  const F2 faceareaxabsubar = area * namda3;
-  const F2 halffacearea = half * area;
-  const F2 alpha0 = faceareaxabsubar * (droe - dp * icsq);
-  const F2 T_a = (lT + rT) * half;
-  const F2 V_a = (lun + run) * half;
-  const F2 Ma_a = abs2(V_a) * rsqrt2(f2(g.gamaRg) * T_a);
-  const F2 f_Ma = clamp2(Ma_a, g.Ma, 1.0f);
-  const F2 om = f2(1.0f) - f_Ma;
-  const F2 s0 = om * om;
-  const F2 n0sq = fma2(f2(4.0f) * csquare, f_Ma, s0 * ubar * ubar);
-  const F2 namda0 = n0sq * rsqrt2(n0sq);
-  const F2 opf = (f2(1.0f) + f_Ma) * ubar;
-  const F2 namda1 = abs2(half * (opf + namda0));
-  const F2 namda2 = abs2(half * (opf - namda0));
-  const F2 alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
-  const F2 alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
-  const F2 alpha3 = alpha0 + alpha1 + alpha2;
-  const F2 alpha4 = a_c * (alpha1 - alpha2);
-  const F2 alphat = faceareaxabsubar * (a_roe * dut);
-  const F2 ml = lroe * lun, mr = rroe * run;
+template <typename P, typename S>
+__device__ __forceinline__ void roe_flux_pair(const Gas<S> &g, P area, P lroe, P lun, P lut, P lp,
+                                              P rroe, P run, P rut, P rp, P &f_mass, P &f_n,
+                                              P &f_t, P &f_e) {
+  const P half = pair(S(0.5), S(0.5)), one = pair(S(1), S(1));
+  const P inv_Rg = pair(g.inv_Rg, g.inv_Rg), Cv = pair(g.Cv, g.Cv);
+  const P aL = rsqrt2(lroe), aR = rsqrt2(rroe);
+  const P ilroe = aL * aL, irroe = aR * aR;
+  const P sL = lroe * aL, sR = rroe * aR;
+  const P lpr = lp * ilroe, rpr = rp * irroe;
+  const P lT = lpr * inv_Rg, rT = rpr * inv_Rg;
+  const P le = fma2(Cv, lT, half * fma2(lun, lun, lut * lut));
+  const P re = fma2(Cv, rT, half * fma2(run, run, rut * rut));
+  const P droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = run - lun;
+  const P isum = rcp2(sL + sR);
+  const P wL = sL * isum, wR = sR * isum;
+  const P a_roe = sL * sR;
+  const P a_un = fma2(lun, wL, run * wR);
+  const P a_ut = fma2(lut, wL, rut * wR);
+  const P a_h = fma2(le + lpr, wL, (re + rpr) * wR);
+  const P csquare = pair(g.gm1, g.gm1) * (a_h - half * fma2(a_un, a_un, a_ut * a_ut));
+  const P rc = rsqrt2(csquare);
+  const P a_c = csquare * rc;
+  const P icsq = rc * rc;
+  const P ubar = a_un;
+  const P namda3 = abs2(ubar);
+  const P coef12 = half * icsq * area;
+  const P roe0cxdubar = a_roe * a_c * dubar;
+  const P faceareaxabsubar = area * namda3;
+  const P halffacearea = half * area;
+  const P alpha0 = faceareaxabsubar * (droe - dp * icsq);
+  const P T_a = (lT + rT) * half;
+  const P V_a = (lun + run) * half;
+  const P Ma_a = abs2(V_a) * rsqrt2(pair(g.gamaRg, g.gamaRg) * T_a);
+  const P f_Ma = clamp2(Ma_a, g.Ma, S(1));
+  const P om = one - f_Ma;
+  const P s0 = om * om;
+  const P n0sq = fma2(pair(S(4), S(4)) * csquare, f_Ma, s0 * ubar * ubar);
+  const P namda0 = n0sq * rsqrt2(n0sq);
+  const P opf = (one + f_Ma) * ubar;
+  const P namda1 = abs2(half * (opf + namda0));
+  const P namda2 = abs2(half * (opf - namda0));
+  const P alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
+  const P alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
+  const P alpha3 = alpha0 + alpha1 + alpha2;
+  const P alpha4 = a_c * (alpha1 - alpha2);
+  const P alphat = faceareaxabsubar * (a_roe * dut);
+  const P ml = lroe * lun, mr = rroe * run;
   f_mass = (ml + mr) * halffacearea - alpha3;
   f_n = (fma2(ml, lun, lp) + fma2(mr, run, rp)) * halffacearea - fma2(a_un, alpha3, alpha4);
   f_t = fma2(ml, lut, mr * rut) * halffacearea - fma2(a_ut, alpha3, alphat);
   f_e = fma2(fma2(le, lroe, lp), lun, fma2(re, rroe, rp) * run) * halffacearea -
-        (fma2(a_h, alpha3, fma2(ubar, alpha4, a_ut * alphat)) - (csquare * f2(g.inv_gm1)) * alpha0);
+        (fma2(a_h, alpha3, fma2(ubar, alpha4, a_ut * alphat)) -
+         (csquare * pair(g.inv_gm1, g.inv_gm1)) * alpha0);
 }
 
 }  // namespace ibgpu

@@ -39,6 +39,12 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
 // Threads of a fast-build stage CTA: FP64 adds a ninth warp that owns the
 // tile's east/north edge faces and outer slopes, so every warp computes two
 // faces; FP32 keeps 8 warps (its face work is cheap enough).
+// Whether a thread evaluates its two faces as one paired flux: FP32 yes
+// (f32x2 instructions); FP64 no (interleaving two scalar chains needs
+// registers that cost more occupancy than the extra independence returns).
+template <typename R>
+constexpr bool kPairFaces = sizeof(R) == 4;
+
 template <typename R>
 struct StageThreads {
   static constexpr int value = sizeof(R) == 8 ? 288 : kTileCells;
@@ -568,22 +574,24 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
     Q4<R> o;
     if (!own) {
       // ninth warp: edge faces only (below)
-    } else if constexpr (sizeof(R) == 4) {
-      // mixed build: the cell's west and south faces as the two lanes of
-      // one paired-FP32 flux evaluation
+    } else if constexpr (kPairFaces<R>) {
+      // the cell's west and south faces as the two lanes of one paired flux
+      // evaluation (f32x2 instructions in the mixed build)
       R lx[4], rx[4], ly[4], ry[4];
       const bool ax_ok = face_recon<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
                                                    ty * kSX + tx + 1, uni, lx, rx);
       const bool ay_ok = face_recon<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg,
                                                    ty * kTile + tx, (ty + 1) * kTile + tx, uni, ly,
                                                    ry);
-      F2 fm, fn, ft, fe;
-      roe_flux_pair(g, f2(ax, ay), f2(lx[0], ly[0]), f2(lx[1], ly[2]), f2(lx[2], ly[1]),
-                    f2(lx[3], ly[3]), f2(rx[0], ry[0]), f2(rx[1], ry[2]), f2(rx[2], ry[1]),
-                    f2(rx[3], ry[3]), fm, fn, ft, fe);
-      if (ax_ok) S::st(fx, ty * (kTile + 1) + tx, NF, fm.v.x, fn.v.x, ft.v.x, fe.v.x);
+      using P = decltype(pair(R(0), R(0)));
+      P fm, fn, ft, fe;
+      roe_flux_pair<P, R>(g, pair(ax, ay), pair(lx[0], ly[0]), pair(lx[1], ly[2]),
+                          pair(lx[2], ly[1]), pair(lx[3], ly[3]), pair(rx[0], ry[0]),
+                          pair(rx[1], ry[2]), pair(rx[2], ry[1]), pair(rx[3], ry[3]), fm, fn, ft,
+                          fe);
+      if (ax_ok) S::st(fx, ty * (kTile + 1) + tx, NF, lane0(fm), lane0(fn), lane0(ft), lane0(fe));
       else S::st(fx, ty * (kTile + 1) + tx, NF, R(0), R(0), R(0), R(0));
-      if (ay_ok) S::st(fy, ty * kTile + tx, NF, fm.v.y, ft.v.y, fn.v.y, fe.v.y);
+      if (ay_ok) S::st(fy, ty * kTile + tx, NF, lane1(fm), lane1(ft), lane1(fn), lane1(fe));
       else S::st(fy, ty * kTile + tx, NF, R(0), R(0), R(0), R(0));
     } else {
       o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
