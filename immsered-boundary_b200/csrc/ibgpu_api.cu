@@ -73,6 +73,10 @@ struct ibgpu_ctx {
   int nsm = 148;
   int body_level = -1;  // finest level of a run with immersed bodies
   cudaStream_t own_stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // asynchronous state downloads
+  cudaEvent_t ev_ready = nullptr, ev_copied = nullptr;
+  bool download_pending = false;       // an asynchronous download may still read s0
+  double *d_rows_out = nullptr;        // staging of asynchronous downloads
   cudaStream_t stream = nullptr;
 
   // layout
@@ -182,6 +186,8 @@ struct ibgpu_ctx {
       for (auto &p : b) { cudaFree(p); p = nullptr; }
     cudaFree(d_vsd);
     cudaFree(d_rows);
+    cudaFree(d_rows_out);
+    d_rows_out = nullptr;
     d_tile_nb = d_tile_level = d_cell_slot = nullptr;
     d_flags = d_cell_alias = nullptr;
     d_vsd = d_rows = nullptr;
@@ -325,6 +331,9 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
   cudaError_t e = cudaGetDevice(&c->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_diag, sizeof(DevDiag));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_diag, sizeof(DevDiag));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_aux_err, sizeof(int));
@@ -354,6 +363,8 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   const int nlev = cs.nlevels;
   const int64_t n = cells->n;
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // pending downloads
+  ctx->download_pending = false;
   ctx->free_layout();
 
   // 1. owners vs aliases; tiles per level
@@ -570,12 +581,26 @@ int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles) {
   return IBGPU_OK;
 }
 
+// Work on the context's stream that writes the state waits for an
+// asynchronous download still reading it.
+static int order_after_download(ibgpu_ctx *ctx, cudaStream_t st) {
+  if (ctx->download_pending) {
+    CK(cudaStreamWaitEvent(st, ctx->ev_copied, 0));
+    ctx->download_pending = false;
+  }
+  return IBGPU_OK;
+}
+
 int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim) {
   if (!ctx || (!prim && ctx->ncells > 0)) return IBGPU_E_ARG;
   if (!ctx->has_topology) return IBGPU_E_STATE;
   cudaStream_t st = ctx->stream;
   if (ctx->ncells > 0) {
+    // the host-to-device copy may overlap a pending download (other buffer,
+    // other copy direction); the scatter into the state waits for it
     CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * 7 * sizeof(double), cudaMemcpyHostToDevice, st));
+    int rc = order_after_download(ctx, st);
+    if (rc) return rc;
     fast::launch_scatter(ctx->d_rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->d_s0,
                          ctx->nsm, st);
     CK(cudaGetLastError());
@@ -595,6 +620,34 @@ int ibgpu_download_state(ibgpu_ctx *ctx, double *prim) {
     CK(cudaMemcpyAsync(prim, ctx->d_rows, ctx->ncells * 7 * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_download_state_async(ibgpu_ctx *ctx, double *prim) {
+  if (!ctx || (!prim && ctx->ncells > 0)) return IBGPU_E_ARG;
+  if (!ctx->has_state) return IBGPU_E_STATE;
+  if (ctx->ncells == 0) return IBGPU_OK;
+  if (!ctx->d_rows_out) {
+    int rc = dev_alloc(&ctx->d_rows_out, (size_t)ctx->ncells * 7);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(ctx->ev_ready, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
+  fast::launch_gather(ctx->d_rows_out, ctx->d_cell_slot, ctx->ncells, ctx->d_s0, ctx->nsm,
+                      ctx->copy_stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev_copied, ctx->copy_stream));
+  ctx->download_pending = true;
+  CK(cudaMemcpyAsync(prim, ctx->d_rows_out, ctx->ncells * 7 * sizeof(double),
+                     cudaMemcpyDeviceToHost, ctx->copy_stream));
+  return IBGPU_OK;
+}
+
+int ibgpu_synchronize(ibgpu_ctx *ctx) {
+  if (!ctx) return IBGPU_E_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->copy_stream));
+  ctx->download_pending = false;
   return IBGPU_OK;
 }
 
@@ -869,8 +922,9 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
   cudaStream_t st = ctx->stream;
   const bool exact = cs.precision == IBGPU_FP64_EXACT;
   const bool mixed = cs.precision == IBGPU_MIXED;
-  int rc = begin_diag(ctx, *dt, st);
+  int rc = order_after_download(ctx, st);
   if (rc) return rc;
+  if ((rc = begin_diag(ctx, *dt, st))) return rc;
   RunTimer tm{ctx, st, {}, {}};
   int64_t marched = 0;
   for (int step = 0; step < nsteps; ++step) {
@@ -1160,8 +1214,13 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
     if ((rc = autotune(b))) return rc;
     if ((rc = build_graphs(b))) return rc;
   }
-  for (int i = 0; i < n; ++i)
+  for (int i = 0; i < n; ++i) {
+    if (b->cases[i]->download_pending) {
+      CK(cudaStreamWaitEvent(st, b->cases[i]->ev_copied, 0));
+      b->cases[i]->download_pending = false;
+    }
     if ((rc = begin_diag(b->cases[i], dt[i], st))) return rc;
+  }
   std::vector<RunTimer> tms;
   for (int i = 0; i < n; ++i) tms.push_back(RunTimer{b->cases[i], st, {}, {}});
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1526,6 +1585,12 @@ void ibgpu_destroy(ibgpu_ctx *ctx) {
   cudaFree(ctx->d_diag);
   cudaFree(ctx->d_aux_err);
   cudaFreeHost(ctx->h_diag);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  if (ctx->ev_ready) cudaEventDestroy(ctx->ev_ready);
+  if (ctx->ev_copied) cudaEventDestroy(ctx->ev_copied);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }

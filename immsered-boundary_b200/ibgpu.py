@@ -35,7 +35,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_indicator_features", "ibgpu_mlp_forward", "ibgpu_mlp_grad", "ibgpu_mlp_adam",
            "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step", "ibgpu_batch_create",
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
-           "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh")
+           "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
+           "ibgpu_download_state_async", "ibgpu_synchronize")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -221,6 +222,8 @@ def lib(path: str | None = None):
     L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_float)]
     L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ibgpu_download_state_async.argtypes = [vp, vp]
+    L.ibgpu_synchronize.argtypes = [vp]
     L.ibgpu_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
     L.ibgpu_batch_destroy.argtypes = [vp]
     L.ibgpu_batch_destroy.restype = None
@@ -472,6 +475,15 @@ class FlowSolver:
         a = np.empty((self.ncells, 7), np.float64) if out is None else out
         _check(lib().ibgpu_download_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p)), "ibgpu_download_state")
         return a
+
+    def download_async(self, out_ptr: int):
+        """Enqueue a download into host memory at out_ptr (pinned for
+        overlap); valid after synchronize()."""
+        _check(lib().ibgpu_download_state_async(self._ctx, ctypes.c_void_p(out_ptr)),
+               "ibgpu_download_state_async")
+
+    def synchronize(self):
+        _check(lib().ibgpu_synchronize(self._ctx), "ibgpu_synchronize")
 
     def time_marching(self, ts: int) -> Diag:
         d = Diag()

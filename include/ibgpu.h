@@ -210,6 +210,14 @@ int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);
 int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim);
 int ibgpu_download_state(ibgpu_ctx *ctx, double *prim);
 
+/* Download without waiting: the copy runs on the context's copy stream after
+ * the work enqueued so far, so it overlaps later uploads and steps (work
+ * that writes the state waits for it on the device).  prim (pinned host
+ * memory for real overlap) holds the state once ibgpu_synchronize returns. */
+int ibgpu_download_state_async(ibgpu_ctx *ctx, double *prim);
+/* Wait for all work and copies of the context. */
+int ibgpu_synchronize(ibgpu_ctx *ctx);
+
 /* One full time step at step index ts (main.cpp:87-97): C/F ghost fill,
  * immersed-body ghost fill, CFL dt every dt_var_step steps, U^n, domain
  * ghosts, frozen viscous flux, nstages stages, residual max-norm.

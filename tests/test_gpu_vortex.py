@@ -354,3 +354,30 @@ def test_run_equals_single_steps_and_reports_abort_step(cuda_lib, pkg):
         c.run(1, 3)
     assert ei.value.abort_code in (523, 37)
     assert ei.value.diag.abort_step == 0
+
+
+def test_async_download_is_ordered_with_later_uploads(cuda_lib, pkg):
+    """ibgpu_download_state_async returns before the copy ends; an upload and
+    a step issued right after must not disturb the state it copies."""
+    import torch
+    ib, wl = pkg.ibgpu, pkg.workloads
+    P, cells, prim = wl.vortex_case(64)
+    ref = ib.FlowSolver(P)
+    ref.upload_topology(**cells)
+    ref.init_flow(prim)
+    ref.time_marching(0)
+    want = ref.download()
+    ref.close()
+    sol = ib.FlowSolver(P)
+    sol.upload_topology(**cells)
+    sol.init_flow(prim)
+    sol.time_marching(0)
+    out = torch.empty((len(prim), 7), dtype=torch.float64).pin_memory()
+    sol.download_async(out.data_ptr())
+    other = prim.copy()
+    other[:, 4] *= 1.01  # a different state uploaded while the copy may run
+    sol.init_flow(other)
+    sol.time_marching(1)
+    sol.synchronize()
+    assert np.array_equal(out.numpy(), want)
+    sol.close()
