@@ -1270,6 +1270,26 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
   return result;
 }
 
+int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float *d_params,
+                         uint8_t *tags) {
+  if (!b || !rule || !tags) return IBGPU_E_ARG;
+  cudaStream_t st = b->stream;
+  int rc = tag_mesh_prepare(d_params != nullptr);
+  if (rc) return rc;
+  int64_t off = 0;
+  for (auto *c : b->cases) {
+    if (c->ncells == 0) continue;
+    uint8_t *rows = nullptr;
+    if ((rc = tag_mesh_enqueue(c, rule, d_params, st, &rows))) return rc;
+    CK(cudaMemcpyAsync(tags + off, rows, (size_t)c->ncells, cudaMemcpyDeviceToHost, st));
+    off += c->ncells;
+  }
+  for (auto *c : b->cases)
+    if (d_params && (rc = tag_mesh_error(c, st))) return rc;
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
 int ibgpu_batch_set_timing(ibgpu_batch *b, int enable) {
   if (!b) return IBGPU_E_ARG;
   b->timing = enable != 0;

@@ -1040,6 +1040,66 @@ int forward_impl(const CtxView &V, const float *d_params, int64_t n, const uint1
 
 }  // namespace
 
+namespace ibgpu {
+// Tags of every row of ctx's cell list enqueued on st (no synchronisation):
+// the learned decision with d_params, else the plain criterion; *rows_out
+// is the device array of the row tags (valid once st reaches it).
+int tag_mesh_enqueue(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
+                     cudaStream_t st, uint8_t **rows_out) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  uint8_t *dtags = nullptr;
+  double *dsd = nullptr;
+  int rc;
+  if ((rc = ctx_tags_buffer(ctx, &dtags)) || (rc = ctx_signdis_buffer(ctx, &dsd, false))) return rc;
+  MeshArgs m;
+  m.tile_nb = V.tile_nb;
+  m.tile_level = V.tile_level;
+  m.tile_org = V.tile_org;
+  m.flags = V.flags;
+  m.rho = V.s0[F_RHO];
+  m.u = V.s0[F_U];
+  m.v = V.s0[F_V];
+  m.p = V.s0[F_P];
+  m.signdis = dsd;
+  m.tags = dtags;
+  m.nslots = V.nslots;
+  FeatScale F;
+  const double rho_inf = V.cc.initvar[0], p_inf = V.cc.initvar[4];
+  F.inv_rho = 1.0 / rho_inf;
+  F.inv_p = 1.0 / p_inf;
+  F.inv_c = 1.0 / std::sqrt(V.cc.gama * p_inf / rho_inf);
+  F.left = rule->body_left_x;
+  F.yc = rule->body_center_y;
+  F.inv_chord = 1.0 / (rule->body_right_x - rule->body_left_x);
+  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) {
+    F.dx[k] = V.cc.lev[k].dx > 0 ? V.cc.lev[k].dx : 1.0;
+    F.dy[k] = V.cc.lev[k].dy > 0 ? V.cc.lev[k].dy : 1.0;
+  }
+  if (d_params) {
+    const int64_t items = V.nslots / kRows;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)V.nsm * 3));
+    mlp_tag_mesh_kernel<<<grid, kThreads, MeshSmem::BYTES, st>>>(d_params, m, F, V.aux_err);
+  } else {
+    tag_plain_mesh_kernel<<<grid_for(V.nslots, V.nsm, 256), 256, 0, st>>>(to_dev(rule), m, F);
+  }
+  CKI(cudaGetLastError());
+  uint8_t *rows = dtags + V.nslots;
+  gather_rows_u8<<<grid_for(V.ncells, V.nsm, 256), 256, 0, st>>>(dtags, V.cell_slot, V.ncells, rows);
+  CKI(cudaGetLastError());
+  *rows_out = rows;
+  return IBGPU_OK;
+}
+
+int tag_mesh_prepare(bool learned) { return learned ? configure_smem() : IBGPU_OK; }
+
+int tag_mesh_error(ibgpu_ctx *ctx, cudaStream_t st) {
+  CtxView V;
+  if (ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
+  return kernel_error_check(V.aux_err, st);
+}
+}  // namespace ibgpu
+
 extern "C" {
 
 int ibgpu_tag_plain(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
@@ -1177,47 +1237,10 @@ int ibgpu_tag_mesh(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_pa
   if (!V.has_topology || (d_params && !V.has_state)) return IBGPU_E_STATE;
   if (V.ncells == 0) return IBGPU_OK;
   if (!tags) return IBGPU_E_ARG;
-  uint8_t *dtags = nullptr;
-  double *dsd = nullptr;
   int rc;
-  if ((rc = ctx_tags_buffer(ctx, &dtags)) || (rc = ctx_signdis_buffer(ctx, &dsd, false))) return rc;
-  MeshArgs m;
-  m.tile_nb = V.tile_nb;
-  m.tile_level = V.tile_level;
-  m.tile_org = V.tile_org;
-  m.flags = V.flags;
-  m.rho = V.s0[F_RHO];
-  m.u = V.s0[F_U];
-  m.v = V.s0[F_V];
-  m.p = V.s0[F_P];
-  m.signdis = dsd;
-  m.tags = dtags;
-  m.nslots = V.nslots;
-  FeatScale F;
-  const double rho_inf = V.cc.initvar[0], p_inf = V.cc.initvar[4];
-  F.inv_rho = 1.0 / rho_inf;
-  F.inv_p = 1.0 / p_inf;
-  F.inv_c = 1.0 / std::sqrt(V.cc.gama * p_inf / rho_inf);
-  F.left = rule->body_left_x;
-  F.yc = rule->body_center_y;
-  F.inv_chord = 1.0 / (rule->body_right_x - rule->body_left_x);
-  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) {
-    F.dx[k] = V.cc.lev[k].dx > 0 ? V.cc.lev[k].dx : 1.0;
-    F.dy[k] = V.cc.lev[k].dy > 0 ? V.cc.lev[k].dy : 1.0;
-  }
-  if (d_params) {
-    if ((rc = configure_smem())) return rc;
-    const int64_t items = V.nslots / kRows;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)V.nsm * 3));
-    mlp_tag_mesh_kernel<<<grid, kThreads, MeshSmem::BYTES, V.stream>>>(d_params, m, F, V.aux_err);
-  } else {
-    tag_plain_mesh_kernel<<<grid_for(V.nslots, V.nsm, 256), 256, 0, V.stream>>>(to_dev(rule), m, F);
-  }
-  CKI(cudaGetLastError());
-  uint8_t *rows = dtags + V.nslots;
-  gather_rows_u8<<<grid_for(V.ncells, V.nsm, 256), 256, 0, V.stream>>>(dtags, V.cell_slot, V.ncells,
-                                                                      rows);
-  CKI(cudaGetLastError());
+  if (d_params && (rc = configure_smem())) return rc;
+  uint8_t *rows = nullptr;
+  if ((rc = tag_mesh_enqueue(ctx, rule, d_params, V.stream, &rows))) return rc;
   CKI(cudaMemcpyAsync(tags, rows, (size_t)V.ncells, cudaMemcpyDeviceToHost, V.stream));
   if (d_params) return kernel_error_check(V.aux_err, V.stream);
   CKI(cudaStreamSynchronize(V.stream));

@@ -36,7 +36,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step", "ibgpu_batch_create",
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
-           "ibgpu_download_state_async", "ibgpu_synchronize")
+           "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -223,6 +223,7 @@ def lib(path: str | None = None):
                                      ctypes.POINTER(ctypes.c_float)]
     L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ibgpu_download_state_async.argtypes = [vp, vp]
+    L.ibgpu_batch_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
     L.ibgpu_synchronize.argtypes = [vp]
     L.ibgpu_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
     L.ibgpu_batch_destroy.argtypes = [vp]
@@ -581,6 +582,21 @@ class Batch:
             bad = next((d for d in diags if d.abort_code), None)
             raise IbgpuError(rc, "ibgpu_batch_run", lib().ibgpu_last_error().decode(), bad)
         return list(diags)
+
+    def tag_mesh(self, rule: dict, d_params: int = 0, out=None) -> list:
+        """Row tags of every case (learned with d_params, else plain); out
+        may be a preallocated uint8 array (e.g. pinned) of all cases' rows."""
+        r = make_tag_rule(rule)
+        n = sum(s.ncells for s in self.solvers)
+        if out is None:
+            out = np.zeros(max(n, 1), np.uint8)
+        _check(lib().ibgpu_batch_tag_mesh(self._b, ctypes.byref(r), ctypes.c_void_p(d_params or None),
+                                          out.ctypes.data_as(ctypes.c_void_p)), "ibgpu_batch_tag_mesh")
+        res, off = [], 0
+        for s in self.solvers:
+            res.append(out[off:off + s.ncells])
+            off += s.ncells
+        return res
 
     def set_timing(self, on: bool):
         _check(lib().ibgpu_batch_set_timing(self._b, int(bool(on))), "ibgpu_batch_set_timing")

@@ -413,6 +413,12 @@ int ibgpu_upload_signdis(ibgpu_ctx *ctx, const double *signdis);
 int ibgpu_tag_mesh(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
                    uint8_t *tags);
 
+/* ibgpu_tag_mesh of every case of a batch, enqueued back to back with one
+ * synchronisation: tags holds the cases' row tags one after another (case
+ * order, each case's cell-list order). */
+int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float *d_params,
+                         uint8_t *tags);
+
 const char *ibgpu_errstr(int code);
 /* Last CUDA error string seen by this thread's most recent failing call. */
 const char *ibgpu_last_error(void);

@@ -75,3 +75,19 @@ def test_batched_amr_cases_follow_their_own_schedules(cuda_lib):
     batch.close()
     for s in (a, bcase, ra, rb):
         s.close()
+
+
+def test_batch_tag_mesh_equals_per_case_tagging(cuda_lib):
+    import torch
+    cases = [wl.vortex_case(n, mach=m) for n, m in [(64, 0.5), (48, 0.3)]]
+    sols = [make_solver(c) for c in cases]
+    rule = wl.naca_tag_rule(1, [10.0 / 64])
+    params = torch.from_numpy(pkg.indicator.init_params(3)).cuda()
+    b = ib.Batch(sols)
+    for dp in (0, params.data_ptr()):
+        got = b.tag_mesh(rule, dp)
+        for s, g in zip(sols, got):
+            assert np.array_equal(g, s.tag_mesh(rule, dp))
+    b.close()
+    for s in sols:
+        s.close()
