@@ -714,8 +714,18 @@ int begin_diag(ibgpu_ctx *ctx, double dt, cudaStream_t st) {
   double cfl_init = 10000.0;
   std::memcpy(&hd->cfl_bits, &cfl_init, sizeof(double));
   hd->err_key = ~0ull;
+  std::memcpy(&hd->cfl_next_bits, &cfl_init, sizeof(double));
   CK(cudaMemcpyAsync(ctx->d_diag, hd, sizeof(DevDiag), cudaMemcpyHostToDevice, st));
   return IBGPU_OK;
+}
+
+// Whether the final stage folds in the next step's CFL pass: one level (all
+// cells march every step), no immersed body (the immersed-boundary fill
+// rewrites normal cells between the stages and the CFL pass) and a CFL pass
+// every step.
+bool folds_cfl(const ibgpu_ctx *ctx) {
+  return ctx->cs.nlevels == 1 && ctx->body_level < 0 && ctx->n_ib == 0 &&
+         ctx->cs.dt_var_step == 1;
 }
 
 // Everything of step ts before the stages (main.cpp:87-89 and the frozen
@@ -777,8 +787,16 @@ int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer
     CK(cudaGetLastError());
   }
 
-  // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0)
-  if (!batched && (ts % cs.dt_var_step) == 0) {
+  // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0); from
+  // the second step of a run that folds it into the final stage, the
+  // previous step already accumulated the bound
+  if (!batched && (ts % cs.dt_var_step) == 0 && step > 0 && folds_cfl(ctx)) {
+    cudaEvent_t e = tm.mark(2);
+    if (exact) exact::launch_take_folded_cfl(ctx->d_diag, ctx->cc, st);
+    else fast::launch_take_folded_cfl(ctx->d_diag, ctx->cc, st);
+    tm.done(e);
+    CK(cudaGetLastError());
+  } else if (!batched && (ts % cs.dt_var_step) == 0) {
     CflArgs ca;
     ca.tile_level = ctx->d_tile_level;
     ca.flags = ctx->d_flags;
@@ -937,6 +955,7 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
       stage_args(ctx, k, sa);
       sa.phase = 8 * step + 2 + k;
       const bool fin = (k == cs.nstages - 1);
+      if (fin && folds_cfl(ctx) && step + 1 < nsteps) sa.cfl_next = 1 + 8 * (step + 1) + 1;
       for (int l = 0; l < cs.nlevels; ++l) {
         if (ts % cs.march_step[l] != cs.march_left[l]) continue;
         sa.tile_begin = ctx->level_tile_begin[l];

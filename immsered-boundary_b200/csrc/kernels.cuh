@@ -77,6 +77,58 @@ __device__ __forceinline__ void block_resnorm(const unsigned long long (&rb)[4],
   }
 }
 
+// CFL bound of one normal cell, NS_Solver::Comptdt (NS_Solver.cpp:196-280),
+// with every operation separately rounded so the CFL pass and the final
+// stages that fold it in produce the same bits in every build.
+__device__ __forceinline__ double cfl_cell_bound(double T, double u, double v, const LevelConst &L,
+                                                 const CaseConst &cc) {
+  const double c = __dsqrt_rn(__dmul_rn(cc.gamaRg, T));
+  const double c0 = __dmul_rn(__dadd_rn(fabs(u), c), L.area_x);
+  const double c1 = __dmul_rn(__dadd_rn(fabs(v), c), L.area_y);
+  const double c2 = __dmul_rn(__dadd_rn(0.0, c), L.area_z);
+  return __ddiv_rn(L.cfl_vol, __dadd_rn(__dadd_rn(c0, c1), c2));
+}
+
+// Block minimum of one positive double per thread (as bits) into *dst, one
+// guarded atomic per block; every thread of the block calls it; sred is
+// shared scratch of NT/32 words nobody else uses meanwhile.
+template <int NT>
+__device__ __forceinline__ void block_min_bits(unsigned long long b, unsigned long long *dst,
+                                               unsigned long long *sred) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
+    b = w < b ? w : b;
+  }
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NT / 32; ++k) b = sred[k] < b ? sred[k] : b;
+    if (b < *(volatile unsigned long long *)dst) atomicMin(dst, b);
+  }
+}
+
+// The next step's CFL pass folded into a final stage: the bound of each
+// normal cell from the state this stage wrote (cb >= 0) or, for a normal
+// cell it did not write, from the step state; block minimum into
+// diag->cfl_next_bits.  All threads call it (own = the thread owns a cell).
+template <int NT>
+__device__ __forceinline__ void fold_next_cfl(const StageArgs &a, const LevelConst &L,
+                                              const CaseConst &cc, uint8_t fl, int64_t slot,
+                                              double cb, unsigned long long *sred,
+                                              bool own = true) {
+  double best = 10000.0;
+  if (own && (fl & CF_NORMAL)) {
+    const double d0 =
+        cb >= 0.0 ? cb : cfl_cell_bound(a.s0[F_T][slot], a.s0[F_U][slot], a.s0[F_V][slot], L, cc);
+    if (d0 < 0.0) raise_error(a.diag, a.cfl_next - 1, ERR_CFL_NEG_DT, (int)slot);
+    best = (d0 < best) ? d0 : best;
+  }
+  __syncthreads();  // sred is free again (block_resnorm read it)
+  block_min_bits<NT>((unsigned long long)__double_as_longlong(best), &a.diag->cfl_next_bits,
+                     sred + 64);
+}
+
 // One stage of the multistage update for one tile per CTA (256 threads):
 // NS_Solver::ComputeFaceFlux (NS_Solver.H:704-832), ComptSource
 // (NS_Solver.cpp:282-363), UpdateConsVars (:844-985) and ComptNewPrimVar
@@ -194,6 +246,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
   const int64_t slot = (int64_t)tile * kTileCells + tid;
   const uint8_t fl = sfl[(ly + kHalo) * kReg + (lx + kHalo)];
   unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
+  double cb = -1.0;  // next step's CFL bound of this cell, when this stage writes it
   if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
     const int xlo = ly * (kTile + 1) + lx, xhi = xlo + 1;
     const int ylo = ly * kTile + lx, yhi = ylo + kTile;
@@ -262,10 +315,12 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
 #pragma unroll
       for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
     }
+    if (FINAL && a.cfl_next && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
   }
   if (FINAL) {
-    __shared__ unsigned long long sred[4 * kTileCells / 32];
+    __shared__ unsigned long long sred[64 + kTileCells / 32];
     block_resnorm(rb, a.diag, sred);
+    if (a.cfl_next) fold_next_cfl<kTileCells>(a, L, cc, fl, slot, cb, sred);
   }
 }
 
@@ -624,6 +679,7 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
                          : uni ? (uint8_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM)
                                : sfl[(ty + kHalo) * kReg + (tx + kHalo)];
   unsigned long long rb[4] = {0ull, 0ull, 0ull, 0ull};
+  double cb = -1.0;  // next step's CFL bound of this cell, when this stage writes it
   if ((fl & CF_NORMAL) && (fl & (CF_UPDATE | CF_RESET))) {
     const Q4<R> fxl = S::ld(fx, ty * (kTile + 1) + tx, NF), fxh = S::ld(fx, ty * (kTile + 1) + tx + 1, NF);
     const Q4<R> fyl = S::ld(fy, ty * kTile + tx, NF), fyh = S::ld(fy, (ty + 1) * kTile + tx, NF);
@@ -698,9 +754,14 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 #pragma unroll
       for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
     }
+    if (FINAL && a.cfl_next && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
   }
   // the y-slope records are dead after the face phase: reuse them
-  if (FINAL) block_resnorm<NT>(rb, a.diag, reinterpret_cast<unsigned long long *>(sly));
+  if (FINAL) {
+    unsigned long long *sred = reinterpret_cast<unsigned long long *>(sly);
+    block_resnorm<NT>(rb, a.diag, sred);
+    if (a.cfl_next) fold_next_cfl<NT>(a, L, cc, fl, slot, cb, sred, own);
+  }
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
@@ -739,11 +800,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
        s += (int64_t)gridDim.x * blockDim.x) {
     if (!(a.flags[s] & CF_NORMAL)) continue;
     const LevelConst &L = cc.lev[a.tile_level[s / kTileCells]];
-    double c = sqrt(cc.gamaRg * a.s0[F_T][s]);
-    double c0 = (fabs(a.s0[F_U][s]) + c) * L.area_x;
-    double c1 = (fabs(a.s0[F_V][s]) + c) * L.area_y;
-    double c2 = (0.0 + c) * L.area_z;
-    double d0 = L.cfl_vol / (c0 + c1 + c2);
+    const double d0 = cfl_cell_bound(a.s0[F_T][s], a.s0[F_U][s], a.s0[F_V][s], L, cc);
     if (d0 < 0.0) raise_error(a.diag, a.phase, ERR_CFL_NEG_DT, (int)s);
     best = (d0 < best) ? d0 : best;  // std::min(CFL_dt, CFL_dt0) ignores NaN
   }
@@ -773,6 +830,17 @@ __global__ void step_begin_kernel(DevDiag *d) {
 
 // dt = min(CFL_dt, dt*dt_ratio) (NS_Solver.cpp:263)
 __global__ void finalize_dt_kernel(DevDiag *d, CaseConst cc) {
+  double cdt = __longlong_as_double((long long)d->cfl_bits);
+  double cand = d->dt * cc.dt_ratio;
+  d->dt = (cand < cdt) ? cand : cdt;
+}
+
+// The CFL pass of a step whose bound the previous step's final stage
+// accumulated (cfl_next_bits): take it, reset the accumulator for this
+// step's final stage, and finalise dt.
+__global__ void take_folded_cfl_kernel(DevDiag *d, CaseConst cc) {
+  d->cfl_bits = d->cfl_next_bits;
+  d->cfl_next_bits = (unsigned long long)__double_as_longlong(10000.0);
   double cdt = __longlong_as_double((long long)d->cfl_bits);
   double cand = d->dt * cc.dt_ratio;
   d->dt = (cand < cdt) ? cand : cdt;
@@ -907,11 +975,7 @@ __global__ void __launch_bounds__(kTileCells)
     double best = 10000.0;
     if (a.flags[s] & CF_NORMAL) {
       const LevelConst &L = cc.lev[a.tile_level[it.y]];
-      double c = sqrt(cc.gamaRg * a.s0[F_T][s]);
-      double c0 = (fabs(a.s0[F_U][s]) + c) * L.area_x;
-      double c1 = (fabs(a.s0[F_V][s]) + c) * L.area_y;
-      double c2 = (0.0 + c) * L.area_z;
-      double d0 = L.cfl_vol / (c0 + c1 + c2);
+      const double d0 = cfl_cell_bound(a.s0[F_T][s], a.s0[F_U][s], a.s0[F_V][s], L, cc);
       if (d0 < 0.0) raise_error(a.diag, pb + 1, ERR_CFL_NEG_DT, (int)s);
       best = (d0 < best) ? d0 : best;
     }
@@ -981,6 +1045,10 @@ void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st)
 }
 
 void launch_step_begin(DevDiag *d, cudaStream_t st) { step_begin_kernel<<<1, 1, 0, st>>>(d); }
+
+void launch_take_folded_cfl(DevDiag *d, const CaseConst &cc, cudaStream_t st) {
+  take_folded_cfl_kernel<<<1, 1, 0, st>>>(d, cc);
+}
 
 void launch_scatter(const double *rows, const int32_t *cell_slot, const uint8_t *alias, int64_t n,
                     double *const s0[kStateFields], int nsm, cudaStream_t st) {

@@ -15,6 +15,7 @@ namespace ibgpu {
                     bool visc, bool final_stage, bool mixed, cudaStream_t st);                \
   void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st);           \
   void launch_step_begin(DevDiag *d, cudaStream_t st);                                         \
+  void launch_take_folded_cfl(DevDiag *d, const CaseConst &cc, cudaStream_t st);              \
   void launch_scatter(const double *rows, const int32_t *cell_slot, const uint8_t *alias,     \
                       int64_t n, double *const s0[kStateFields], int nsm, cudaStream_t st);   \
   void launch_gather(double *rows, const int32_t *cell_slot, int64_t n,                       \

@@ -69,6 +69,9 @@ struct DevDiag {
   unsigned long long cfl_bits;
   unsigned long long res_bits[5];
   unsigned long long err_key;  // ~0ull: no error
+  // CFL bound of the next step, accumulated by a final stage that computes
+  // it (StageArgs::cfl_next) for single-level runs without bodies
+  unsigned long long cfl_next_bits;
 };
 
 constexpr int kHaloStage = 2;
@@ -87,6 +90,11 @@ struct StageArgs {
   double tp;                 // stage coefficient tp[k]
   int phase;                 // abort-order phase of this stage (see DevDiag)
   DevDiag *diag;
+  // final stage only: 1 + the abort-order phase of the next step's CFL pass
+  // to fold that pass into this stage (0: off).  The next step's CFL reads
+  // the normal cells this stage writes, and nothing else writes them in
+  // between when the run has one level and no immersed body.
+  int cfl_next;
 };
 
 struct CflArgs {
