@@ -997,6 +997,7 @@ struct ibgpu_batch {
   std::vector<cudaGraphExec_t> graphs;  // per phase r (+ period with the CFL pass)
   int2 *d_cfl_work = nullptr;      // every tile of every case
   int ncfl = 0, dt_var_step = 1;
+  bool folds = false;  // every case single-level without bodies: CFL folded into final stages
   int grid = 0;                    // CTAs of the persistent launch (0 = one per item)
   bool tuned = false;
   bool timing = false;
@@ -1024,10 +1025,14 @@ struct ibgpu_batch {
 
 namespace {
 
-int enqueue_batch_stages(ibgpu_batch *b, int r, bool cfl, cudaStream_t st) {
-  if (cfl) {
+// cfl: 0 none, 1 the CFL pass, 2 the bound folded into the previous step
+int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
+  if (cfl == 1) {
     fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work, b->ncfl, b->nstages,
                            b->d_phase_base, (int)b->cases.size(), 0, st);
+    CK(cudaGetLastError());
+  } else if (cfl == 2) {
+    fast::launch_take_folded_batch(b->d_args, b->d_ccs, (int)b->cases.size(), b->nstages, st);
     CK(cudaGetLastError());
   }
   for (int k = 0; k < b->nstages; ++k) {
@@ -1092,11 +1097,11 @@ int autotune(ibgpu_batch *b) {
 // One graph per schedule phase holding the nstages merged stage launches;
 // without a capturable stream the launches are issued directly.
 int build_graphs(ibgpu_batch *b) {
-  b->graphs.assign(2 * b->period, nullptr);
+  b->graphs.assign(3 * b->period, nullptr);
   if (b->stream == nullptr) return IBGPU_OK;  // legacy stream: not capturable
-  for (int v = 0; v < 2 * b->period; ++v) {
+  for (int v = 0; v < 3 * b->period; ++v) {
     const int r = v % b->period;
-    const bool cfl = v >= b->period;
+    const int cfl = v / b->period;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_batch_stages(b, r, cfl, b->stream);
@@ -1146,6 +1151,7 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   b->visc = c0.viscous != 0;
   b->mixed = c0.precision == IBGPU_MIXED;
   b->dt_var_step = c0.dt_var_step;
+  b->folds = true;
   // schedule period: every level's marching step divides the largest
   for (auto *c : b->cases)
     for (int l = 0; l < c->cs.nlevels; ++l) b->period = std::max(b->period, c->cs.march_step[l]);
@@ -1162,7 +1168,10 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   for (int i = 0; i < ncases; ++i) {
     for (int k = 0; k < S; ++k) stage_args(b->cases[i], k, args[(size_t)i * S + k]);
     ccs[i] = b->cases[i]->cc;
+    b->folds = b->folds && folds_cfl(b->cases[i]);
   }
+  if (b->folds)
+    for (int i = 0; i < ncases; ++i) args[(size_t)i * S + S - 1].cfl_next = 1;  // enabled marker
   auto fail = [&](int rc) {
     b->release();
     delete b;
@@ -1170,11 +1179,11 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   };
   int rc;
   if ((rc = dev_alloc(&b->d_args, args.size())) || (rc = dev_alloc(&b->d_ccs, ccs.size())) ||
-      (rc = dev_alloc(&b->d_phase_base, 1)))
+      (rc = dev_alloc(&b->d_phase_base, 2)))
     return fail(rc);
   cudaError_t e = cudaMemcpy(b->d_args, args.data(), args.size() * sizeof(StageArgs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_ccs, ccs.data(), ccs.size() * sizeof(CaseConst), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(b->d_phase_base, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_phase_base, 0, 2 * sizeof(int));
   if (e != cudaSuccess) return fail(cuda_fail(e, "batch upload"));
   // work lists: case-interleaved so the persistent CTAs mix the cases
   b->d_work.assign(b->period, nullptr);
@@ -1253,14 +1262,14 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
       if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i], true))) return rc;
       marched[i] = marched_cells(b->cases[i], ts);
     }
-    const bool cfl = (ts % b->dt_var_step) == 0;
-    fast::launch_set_phase_base(b->d_phase_base, 8 * step, st);
+    const int cfl = (ts % b->dt_var_step) != 0 ? 0 : (b->folds && step > 0 ? 2 : 1);
+    fast::launch_set_phase_base(b->d_phase_base, 8 * step, b->folds && step + 1 < nsteps, st);
     if (b->timing) {
       CK(cudaEventCreate(&e0));
       CK(cudaEventCreate(&e1));
       CK(cudaEventRecord(e0, st));
     }
-    const int v = r + (cfl ? b->period : 0);
+    const int v = r + cfl * b->period;
     if (b->graphs[v]) CK(cudaGraphLaunch(b->graphs[v], st));
     else if ((rc = enqueue_batch_stages(b, r, cfl, st))) return rc;
     if (b->timing) {

@@ -115,13 +115,13 @@ __device__ __forceinline__ void block_min_bits(unsigned long long b, unsigned lo
 template <int NT>
 __device__ __forceinline__ void fold_next_cfl(const StageArgs &a, const LevelConst &L,
                                               const CaseConst &cc, uint8_t fl, int64_t slot,
-                                              double cb, unsigned long long *sred,
+                                              double cb, unsigned long long *sred, int phase,
                                               bool own = true) {
   double best = 10000.0;
   if (own && (fl & CF_NORMAL)) {
     const double d0 =
         cb >= 0.0 ? cb : cfl_cell_bound(a.s0[F_T][slot], a.s0[F_U][slot], a.s0[F_V][slot], L, cc);
-    if (d0 < 0.0) raise_error(a.diag, a.cfl_next - 1, ERR_CFL_NEG_DT, (int)slot);
+    if (d0 < 0.0) raise_error(a.diag, phase, ERR_CFL_NEG_DT, (int)slot);
     best = (d0 < best) ? d0 : best;
   }
   __syncthreads();  // sred is free again (block_resnorm read it)
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
   if (FINAL) {
     __shared__ unsigned long long sred[64 + kTileCells / 32];
     block_resnorm(rb, a.diag, sred);
-    if (a.cfl_next) fold_next_cfl<kTileCells>(a, L, cc, fl, slot, cb, sred);
+    if (a.cfl_next) fold_next_cfl<kTileCells>(a, L, cc, fl, slot, cb, sred, a.cfl_next - 1);
   }
 }
 
@@ -513,7 +513,8 @@ __device__ __forceinline__ const double *uniform_piece(const StageArgs &a, int t
 
 template <typename R, int LIM, bool VISC, bool FINAL>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseConst &cc,
-                                                const int tile, const int phase) {
+                                                const int tile, const int phase,
+                                                const int fold) {
   constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
   using S = SRec<R>;
   using V = typename S::V;
@@ -754,20 +755,20 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 #pragma unroll
       for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
     }
-    if (FINAL && a.cfl_next && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
+    if (FINAL && fold && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
   }
   // the y-slope records are dead after the face phase: reuse them
   if (FINAL) {
     unsigned long long *sred = reinterpret_cast<unsigned long long *>(sly);
     block_resnorm<NT>(rb, a.diag, sred);
-    if (a.cfl_next) fold_next_cfl<NT>(a, L, cc, fl, slot, cb, sred, own);
+    if (fold) fold_next_cfl<NT>(a, L, cc, fl, slot, cb, sred, fold - 1, own);
   }
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
-  stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase);
+  stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase, a.cfl_next);
 }
 
 
@@ -782,11 +783,14 @@ __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6
     stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                        const int2 *__restrict__ work, int nwork, int stage, int nstages,
                        const int *__restrict__ phase_base) {
-  const int pb = *phase_base;
+  // phase_base[0]: 8 x the step index; phase_base[1]: 1 when this step's
+  // final stage folds in the next step's CFL pass of the cases that allow it
+  const int pb = phase_base[0], fold_step = phase_base[1];
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const int2 it = work[w];
-    stage_tile_fast<R, LIM, VISC, FINAL>(args[it.x * nstages + stage], ccs[it.x], it.y,
-                                         pb + 2 + stage);
+    const StageArgs &a = args[it.x * nstages + stage];
+    const int fold = (FINAL && fold_step && a.cfl_next) ? 1 + pb + 8 + 1 : 0;
+    stage_tile_fast<R, LIM, VISC, FINAL>(a, ccs[it.x], it.y, pb + 2 + stage, fold);
     __syncthreads();  // shared-memory reuse by the next work item
   }
 }
@@ -1006,6 +1010,23 @@ __global__ void finalize_dt_batch(const StageArgs *__restrict__ args,
   d->dt = (cand < cdt) ? cand : cdt;
 }
 
+// the CFL bound each batched case's previous final stage accumulated
+__global__ void take_folded_batch(const StageArgs *__restrict__ args,
+                                  const CaseConst *__restrict__ ccs, int ncases, int nstages) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases) return;
+  DevDiag *d = args[c * nstages].diag;
+  d->cfl_bits = d->cfl_next_bits;
+  d->cfl_next_bits = (unsigned long long)__double_as_longlong(10000.0);
+  double cdt = __longlong_as_double((long long)d->cfl_bits);
+  double cand = d->dt * ccs[c].dt_ratio;
+  d->dt = (cand < cdt) ? cand : cdt;
+}
+void launch_take_folded_batch(const StageArgs *args, const CaseConst *ccs, int ncases, int nstages,
+                              cudaStream_t st) {
+  take_folded_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, ncases, nstages);
+}
+
 // per-step reset of the reductions of every batched case
 __global__ void step_begin_batch(const StageArgs *__restrict__ args, int ncases, int nstages) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1029,9 +1050,12 @@ void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cud
 }
 
 // set the abort-order phase base of the current step (8 x step index)
-__global__ void set_phase_base_kernel(int *phase_base, int value) { *phase_base = value; }
-void launch_set_phase_base(int *phase_base, int value, cudaStream_t st) {
-  set_phase_base_kernel<<<1, 1, 0, st>>>(phase_base, value);
+__global__ void set_phase_base_kernel(int *phase_base, int value, int fold) {
+  phase_base[0] = value;
+  phase_base[1] = fold;
+}
+void launch_set_phase_base(int *phase_base, int value, int fold, cudaStream_t st) {
+  set_phase_base_kernel<<<1, 1, 0, st>>>(phase_base, value, fold);
 }
 #endif
 

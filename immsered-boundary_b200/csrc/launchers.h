@@ -38,7 +38,9 @@ namespace fast {
 void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                         int stage, int nstages, const int *phase_base, int limiter, bool visc,
                         bool final_stage, bool mixed, int grid, cudaStream_t st);
-void launch_set_phase_base(int *phase_base, int value, cudaStream_t st);
+void launch_set_phase_base(int *phase_base, int value, int fold, cudaStream_t st);
+void launch_take_folded_batch(const StageArgs *args, const CaseConst *ccs, int ncases, int nstages,
+                              cudaStream_t st);
 void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                       int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st);
 void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cudaStream_t st);
