@@ -568,9 +568,11 @@ def our_arm(args):
                        "leaf_cells": ncell, "precision": "fp64",
                        "l2": "state (~470 MB incl. stage buffers) larger than L2; no flush",
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
-            # per step: reduction reset (not on a run's first step), CFL +
-            # dt finalisation, one launch per stage
-            "gpu_launches": (3 + STAGES) * args.steps - 1,
+            # one timed run of K steps: the first step launches the CFL pass
+            # and dt finalisation, later steps the reduction reset and the
+            # take-over of the CFL bound folded into the previous final
+            # stage; every step one launch per stage
+            "gpu_launches": (2 + STAGES) * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "stage_kernel (flux + residual + update + prim recovery)",
