@@ -17,7 +17,8 @@
 // Environment: IB_STEPS (default 5), IB_STAGES (3 or 4, default 4),
 // IB_DUMP=<prefix> (write <prefix>_<step>.bin for the initial state and after
 // each step listed by IB_DUMP_EVERY, default every step), IB_FORCES=1 (static
-// body: compute wall forces each step, Body::ComptWallForce).
+// body: compute wall forces each step, Body::ComptWallForce), IB_FORCE_LOG=<file>
+// (the per-step force history).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -396,6 +397,10 @@ int main(int argc, char **argv) {
   const int every = env_int("IB_DUMP_EVERY", 1);
   const bool forces_on = env_int("IB_FORCES", 0) != 0;
   const char *prefix = std::getenv("IB_DUMP");
+  // IB_FORCE_LOG=<file>: per step ts, t, dt and the forces/moments of every
+  // body (6 doubles each) as raw doubles, the Cl/Cd history of a run
+  const char *force_log = std::getenv("IB_FORCE_LOG");
+  FILE *flog = force_log ? std::fopen(force_log, "wb") : nullptr;
   std::vector<double> forces;
   auto do_dump = [&](int step) {
     if (!prefix) return;
@@ -431,11 +436,17 @@ int main(int argc, char **argv) {
         for (int k = 0; k < 3; ++k) forces.push_back(sphere[b].bodymoment(k));
       }
     }
+    if (flog) {
+      const double head[3] = {(double)ts, t, dt};
+      std::fwrite(head, sizeof(double), 3, flog);
+      if (!forces.empty()) std::fwrite(forces.data(), sizeof(double), forces.size(), flog);
+    }
     amr.ADPRule(sphere);
     if (adpflag) amr.PerformAdaptive(sphere);
     adpflag = false;
     if (prefix && (ts % every == 0 || s == nsteps - 1)) do_dump(ts);
   }
+  if (flog) std::fclose(flog);
   std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
               "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g}\n",
               nsteps - timed_from, loop_time, cell_updates,

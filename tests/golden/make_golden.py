@@ -46,6 +46,13 @@ TAG_CASES = {
     "naca_tags_n64_l4": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "4", "IB_USER_INIT": "0",
                                              "IB_NPTS": "200"}),
 }
+# force histories (Cl/Cd time series) of longer runs of a case above, started
+# from that case's initial state: name -> (binary, environment, steps)
+FORCE_CASES = {
+    "naca_forces_s400_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
+                                                   "IB_STAGES": "4", "IB_USER_INIT": "0",
+                                                   "IB_FORCES": "1", "IB_NPTS": "120"}, 400),
+}
 # per-case records that do not change between dumps of a static mesh
 AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
        "patch_f", "body_f")
@@ -123,11 +130,31 @@ def snapshot(g: dict, k: int) -> dict:
     return d
 
 
+def run_force_case(name: str, binary: str, env: dict, steps: int) -> str:
+    """ts, t, dt and each body's force and moment after every step."""
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        e = dict(os.environ)
+        e.update(env)
+        e["IB_STEPS"] = str(steps)
+        e["IB_FORCE_LOG"] = os.path.join(work, "forces.bin")
+        subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
+                       stdout=subprocess.DEVNULL)
+        hist = np.fromfile(os.path.join(work, "forces.bin"), dtype=np.float64).reshape(steps, -1)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, history=hist)
+        return path
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(TAG_CASES)
+    names = sys.argv[1:] or list(CASES) + list(TAG_CASES) + list(FORCE_CASES)
     for n in names:
         if n in TAG_CASES:
             print(run_tag_case(n, *TAG_CASES[n]))
+        elif n in FORCE_CASES:
+            print(run_force_case(n, *FORCE_CASES[n]))
         else:
             b, env, steps = CASES[n]
             print(run_case(n, b, env, steps))

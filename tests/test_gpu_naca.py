@@ -114,3 +114,34 @@ def test_four_steps_in_a_row_match_reference(cuda_lib, pkg):
     f = sol.wall_forces().ravel()
     assert np.allclose(f, g["forces"][-1], rtol=1e-10, atol=1e-13)
     sol.close()
+
+
+def force_history():
+    with np.load(os.path.join(os.path.dirname(__file__), "golden",
+                              "naca_forces_s400_n64_l3.npz")) as z:
+        return z["history"]
+
+
+@pytest.mark.parametrize("precision,tol_coef,dt_rtol", [
+    ("exact", 1e-12, 1e-12), ("fp64", 1e-10, 1e-10), ("mixed", FORCE_TOL, 1e-4)])
+def test_cl_cd_history_matches_reference(cuda_lib, pkg, precision, tol_coef, dt_rtol):
+    """400 steps from the reference's initial state: the drag/lift history
+    (force_foil.dat columns Fx/F_ref, Fy/F_ref) and the dt history against
+    the reference's own run, step by step."""
+    ib = pkg.ibgpu
+    prec = {"exact": ib.FP64_EXACT, "fp64": ib.FP64, "mixed": ib.MIXED}[precision]
+    g = make_golden.load(NAME)
+    hist = force_history()
+    F_ref = 0.5 * 1.0 * 0.1
+    sol = naca_solver(ib, g, 0, prec)
+    worst = np.zeros(2)
+    for k in range(len(hist)):
+        d = sol.time_marching(k)
+        assert d.abort_code == 0
+        assert abs(sol.dt - hist[k, 2]) <= dt_rtol * hist[k, 2]
+        f = sol.wall_forces()[0]
+        coef = np.abs(f[:2] - hist[k, 3:5]) / F_ref
+        worst = np.maximum(worst, coef)
+    print(f"\n{precision}: max |dCd| {worst[0]:.2e}, max |dCl| {worst[1]:.2e} over {len(hist)} steps")
+    assert worst.max() <= tol_coef
+    sol.close()
