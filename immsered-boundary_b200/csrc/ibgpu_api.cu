@@ -871,10 +871,10 @@ void stage_args(const ibgpu_ctx *ctx, int k, StageArgs &sa) {
   const bool fin = (k == cs.nstages - 1);
   static const int map[4] = {F_RHO, F_U, F_V, F_P};
   for (int f = 0; f < 4; ++f) {
-    sa.sin[f] = (k == 0) ? ctx->d_s0[map[f]] : ctx->d_buf[(k - 1) & 1][f];
-    sa.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
+    sa.v.sin[f] = (k == 0) ? ctx->d_s0[map[f]] : ctx->d_buf[(k - 1) & 1][f];
+    sa.v.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
   }
-  sa.tp = cs.tp[k];
+  sa.v.tp = cs.tp[k];
 }
 
 int64_t marched_cells(const ibgpu_ctx *ctx, int ts) {
@@ -955,7 +955,7 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
       stage_args(ctx, k, sa);
       sa.phase = 8 * step + 2 + k;
       const bool fin = (k == cs.nstages - 1);
-      if (fin && folds_cfl(ctx) && step + 1 < nsteps) sa.cfl_next = 1 + 8 * (step + 1) + 1;
+      if (fin && folds_cfl(ctx) && step + 1 < nsteps) sa.v.cfl_next = 1 + 8 * (step + 1) + 1;
       for (int l = 0; l < cs.nlevels; ++l) {
         if (ts % cs.march_step[l] != cs.march_left[l]) continue;
         sa.tile_begin = ctx->level_tile_begin[l];
@@ -999,6 +999,9 @@ struct ibgpu_batch {
   int ncfl = 0, dt_var_step = 1;
   bool folds = false;  // every case single-level without bodies: CFL folded into final stages
   int grid = 0;                    // CTAs of the persistent launch (0 = one per item)
+  int device = 0;
+  int table = -1;       // byte offset of the arguments in the constant-memory table (-1: global)
+  int table_bytes = 0;  // bytes reserved there
   bool tuned = false;
   bool timing = false;
   double stage_ms = 0.0;
@@ -1020,6 +1023,9 @@ struct ibgpu_batch {
     d_args = nullptr;
     d_ccs = nullptr;
     d_phase_base = nullptr;
+    fast::batch_table_release(device, table);
+    table = -1;
+    table_bytes = 0;
   }
 };
 
@@ -1038,7 +1044,7 @@ int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
   for (int k = 0; k < b->nstages; ++k) {
     fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], k, b->nstages,
                              b->d_phase_base, b->limiter, b->visc, k == b->nstages - 1, b->mixed,
-                             b->grid, st);
+                             b->grid, b->table, st);
     CK(cudaGetLastError());
   }
   return IBGPU_OK;
@@ -1072,7 +1078,7 @@ int autotune(ibgpu_batch *b) {
       CK(cudaEventRecord(e0, b->stream));
       fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], 0, b->nstages,
                                b->d_phase_base, b->limiter, b->visc, b->nstages == 1, b->mixed, g,
-                               b->stream);
+                               b->table, b->stream);
       CK(cudaGetLastError());
       CK(cudaEventRecord(e1, b->stream));
       CK(cudaEventSynchronize(e1));
@@ -1091,6 +1097,48 @@ int autotune(ibgpu_batch *b) {
   cudaEventDestroy(e1);
   b->grid = best_grid;
   b->tuned = true;
+  return IBGPU_OK;
+}
+
+// The batch's stage arguments in the constant-memory table when they fit:
+// a header of one int4 per case (byte offsets of the case's StageArgs up to
+// its stage-dependent part, of its StageVar records, of its CaseConst), then
+// per case those three, the CaseConst cut after its finest level (the stage
+// kernel reads only the levels the case's tiles have).  A batch that does
+// not fit keeps reading its arguments from global memory.
+int write_batch_table(ibgpu_batch *b, const std::vector<StageArgs> &args,
+                      const std::vector<CaseConst> &ccs) {
+  const int n = (int)b->cases.size(), S = b->nstages;
+  auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  std::vector<size_t> rec(n);
+  size_t total = up16((size_t)n * sizeof(int4));
+  for (int i = 0; i < n; ++i) {
+    rec[i] = total;
+    const size_t cc_bytes = offsetof(CaseConst, lev) + b->cases[i]->cs.nlevels * sizeof(LevelConst);
+    total += up16(kStageCommonBytes) + up16((size_t)S * sizeof(StageVar)) + up16(cc_bytes);
+  }
+  if (total > (size_t)INT32_MAX) return IBGPU_OK;
+  const int off = fast::batch_table_reserve(b->device, (int)total);
+  if (off < 0) return IBGPU_OK;  // does not fit: global-memory arguments
+  std::vector<unsigned char> img(total, 0);
+  for (int i = 0; i < n; ++i) {
+    const size_t a_at = rec[i], v_at = a_at + up16(kStageCommonBytes),
+                 c_at = v_at + up16((size_t)S * sizeof(StageVar));
+    const int4 h = make_int4(off + (int)a_at, off + (int)v_at, off + (int)c_at, 0);
+    std::memcpy(&img[(size_t)i * sizeof(int4)], &h, sizeof(int4));
+    std::memcpy(&img[a_at], &args[(size_t)i * S], kStageCommonBytes);
+    for (int k = 0; k < S; ++k)
+      std::memcpy(&img[v_at + k * sizeof(StageVar)], &args[(size_t)i * S + k].v, sizeof(StageVar));
+    std::memcpy(&img[c_at], &ccs[i],
+                offsetof(CaseConst, lev) + b->cases[i]->cs.nlevels * sizeof(LevelConst));
+  }
+  cudaError_t e = fast::batch_table_write(off, img.data(), (int)total);
+  if (e != cudaSuccess) {
+    fast::batch_table_release(b->device, off);
+    return cuda_fail(e, "batch constant table");
+  }
+  b->table = off;
+  b->table_bytes = (int)total;
   return IBGPU_OK;
 }
 
@@ -1146,6 +1194,7 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   b->cases.assign(cases, cases + ncases);
   b->stream = cases[0]->stream;
   b->nsm = cases[0]->nsm;
+  b->device = cases[0]->device;
   b->nstages = c0.nstages;
   b->limiter = c0.limiter;
   b->visc = c0.viscous != 0;
@@ -1171,7 +1220,7 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
     b->folds = b->folds && folds_cfl(b->cases[i]);
   }
   if (b->folds)
-    for (int i = 0; i < ncases; ++i) args[(size_t)i * S + S - 1].cfl_next = 1;  // enabled marker
+    for (int i = 0; i < ncases; ++i) args[(size_t)i * S + S - 1].v.cfl_next = 1;  // enabled marker
   auto fail = [&](int rc) {
     b->release();
     delete b;
@@ -1185,6 +1234,7 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
   if (e == cudaSuccess) e = cudaMemcpy(b->d_ccs, ccs.data(), ccs.size() * sizeof(CaseConst), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(b->d_phase_base, 0, 2 * sizeof(int));
   if (e != cudaSuccess) return fail(cuda_fail(e, "batch upload"));
+  if ((rc = write_batch_table(b, args, ccs))) return fail(rc);
   // work lists: case-interleaved so the persistent CTAs mix the cases
   b->d_work.assign(b->period, nullptr);
   b->nwork.assign(b->period, 0);
@@ -1345,6 +1395,8 @@ int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms) {
   }
   return (int)b->tune_grid.size();
 }
+
+int ibgpu_batch_table_bytes(const ibgpu_batch *b) { return b ? b->table_bytes : 0; }
 
 void ibgpu_batch_destroy(ibgpu_batch *b) {
   if (!b) return;

@@ -8,6 +8,9 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
 #include <stdint.h>
 
 #include "flux.cuh"
@@ -162,10 +165,10 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
         f = a.flags[s];
         if (f & CF_PRESENT) {
           const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
-          const double *p0 = varying ? a.sin[0] : a.s0[F_RHO];
-          const double *p1 = varying ? a.sin[1] : a.s0[F_U];
-          const double *p2 = varying ? a.sin[2] : a.s0[F_V];
-          const double *p3 = varying ? a.sin[3] : a.s0[F_P];
+          const double *p0 = varying ? a.v.sin[0] : a.s0[F_RHO];
+          const double *p1 = varying ? a.v.sin[1] : a.s0[F_U];
+          const double *p2 = varying ? a.v.sin[2] : a.s0[F_V];
+          const double *p3 = varying ? a.v.sin[3] : a.s0[F_P];
           q0 = (R)p0[s];
           q1 = (R)p1[s];
           q2 = (R)p2[s];
@@ -262,7 +265,7 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
       res[c] = sx + sy;
     }
     const double dt = a.diag->dt;
-    const double level_ts = (a.tp * dt) * L.step_num;
+    const double level_ts = (a.v.tp * dt) * L.step_num;
     double orho = a.s0[F_RHO][slot], ou = a.s0[F_U][slot], ov = a.s0[F_V][slot],
            oe = a.s0[F_E][slot];
     double nrho, nu, nv, np, ne, nT;
@@ -305,22 +308,22 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
         a.s0[F_E][slot] = ne;
         a.s0[F_T][slot] = nT;
       } else {
-        a.sout[0][slot] = nrho;
-        a.sout[1][slot] = nu;
-        a.sout[2][slot] = nv;
-        a.sout[3][slot] = np;
+        a.v.sout[0][slot] = nrho;
+        a.v.sout[1][slot] = nu;
+        a.v.sout[2][slot] = nv;
+        a.v.sout[3][slot] = np;
       }
     }
     if (FINAL && (fl & CF_RESNORM)) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) rb[c] = (unsigned long long)__double_as_longlong(fabs(res[c]));
     }
-    if (FINAL && a.cfl_next && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
+    if (FINAL && a.v.cfl_next && wrote) cb = cfl_cell_bound(nT, nu, nv, L, cc);
   }
   if (FINAL) {
     __shared__ unsigned long long sred[64 + kTileCells / 32];
     block_resnorm(rb, a.diag, sred);
-    if (a.cfl_next) fold_next_cfl<kTileCells>(a, L, cc, fl, slot, cb, sred, a.cfl_next - 1);
+    if (a.v.cfl_next) fold_next_cfl<kTileCells>(a, L, cc, fl, slot, cb, sred, a.v.cfl_next - 1);
   }
 }
 
@@ -491,28 +494,29 @@ __device__ __forceinline__ void uniform_piece_dst(int w, int &f, int &dst) {
 }
 
 // Global address of piece w of tile `tile`.
-__device__ __forceinline__ const double *uniform_piece(const StageArgs &a, int tile, int w, int &f,
-                                                       int &dst) {
+__device__ __forceinline__ const double *uniform_piece(const StageArgs &a, const StageVar &v, int tile,
+                                                       int w, int &f, int &dst) {
   uniform_piece_dst(w, f, dst);
   if (w < 512) {
     const int p = w & 127;
-    return a.sin[f] + (int64_t)tile * kTileCells + (p >> 3) * kTile + (p & 7) * 2;
+    return v.sin[f] + (int64_t)tile * kTileCells + (p >> 3) * kTile + (p & 7) * 2;
   }
   if (w < 640) {
-    const int v = w - 512;
-    const int east = (v >> 4) & 1, row = v & 15;
+    const int q = w - 512;
+    const int east = (q >> 4) & 1, row = q & 15;
     const int nb = a.tile_nb[tile * 9 + (east ? 5 : 3)];
-    return a.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
+    return v.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
   }
-  const int v = w - 640;
-  const int north = (v >> 4) & 1, rr = (v >> 3) & 1;
+  const int q = w - 640;
+  const int north = (q >> 4) & 1, rr = (q >> 3) & 1;
   const int nb = a.tile_nb[tile * 9 + (north ? 7 : 1)];
   const int srow = north ? rr : kTile - 2 + rr;
-  return a.sin[f] + (int64_t)nb * kTileCells + srow * kTile + (v & 7) * 2;
+  return v.sin[f] + (int64_t)nb * kTileCells + srow * kTile + (q & 7) * 2;
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
-__device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseConst &cc,
+__device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageVar &v,
+                                                const CaseConst &cc,
                                                 const int tile, const int phase,
                                                 const int fold) {
   constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
@@ -544,7 +548,7 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
       const int w = tid + it * NT;
       if (w >= 768) break;
       int f, dst;
-      const double2 val = __ldg(reinterpret_cast<const double2 *>(uniform_piece(a, tile, w, f, dst)));
+      const double2 val = __ldg(reinterpret_cast<const double2 *>(uniform_piece(a, v, tile, w, f, dst)));
       *S::comp(sq, dst, NQ, f) = (R)val.x;
       *S::comp(sq, dst + 1, NQ, f) = (R)val.y;
     }
@@ -562,10 +566,10 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
           f = a.flags[s];
           if (f & CF_PRESENT) {
             const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
-            q0 = (R)(varying ? a.sin[0] : a.s0[F_RHO])[s];
-            q1 = (R)(varying ? a.sin[1] : a.s0[F_U])[s];
-            q2 = (R)(varying ? a.sin[2] : a.s0[F_V])[s];
-            q3 = (R)(varying ? a.sin[3] : a.s0[F_P])[s];
+            q0 = (R)(varying ? v.sin[0] : a.s0[F_RHO])[s];
+            q1 = (R)(varying ? v.sin[1] : a.s0[F_U])[s];
+            q2 = (R)(varying ? v.sin[2] : a.s0[F_V])[s];
+            q3 = (R)(varying ? v.sin[3] : a.s0[F_P])[s];
           }
         }
       }
@@ -704,7 +708,7 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
       }
     }
     const double dt = a.diag->dt;
-    const double scale = (a.tp * dt) * L.step_num * L.inv_vol;
+    const double scale = (v.tp * dt) * L.step_num * L.inv_vol;
     double nrho, nu, nv, np, ne, nT;
     bool wrote = false;
     if (fl & CF_UPDATE) {
@@ -745,10 +749,10 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
         a.s0[F_E][slot] = ne;
         a.s0[F_T][slot] = nT;
       } else {
-        a.sout[0][slot] = nrho;
-        a.sout[1][slot] = nu;
-        a.sout[2][slot] = nv;
-        a.sout[3][slot] = np;
+        v.sout[0][slot] = nrho;
+        v.sout[1][slot] = nu;
+        v.sout[2][slot] = nv;
+        v.sout[3][slot] = np;
       }
     }
     if (FINAL && (fl & CF_RESNORM)) {
@@ -768,29 +772,60 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const CaseCo
 template <typename R, int LIM, bool VISC, bool FINAL>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
-  stage_tile_fast<R, LIM, VISC, FINAL>(a, cc, a.tile_begin + blockIdx.x, a.phase, a.cfl_next);
+  stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, cc, a.tile_begin + blockIdx.x, a.phase,
+                                       a.v.cfl_next);
 }
 
 
-// Batched stage: persistent CTAs over a work list of (case, tile) pairs of
-// several independent cases (each its own mesh, state and constants); the
-// stage's arguments of case c are args[c * nstages + stage] and its
-// constants ccs[c].  phase_base holds 8 x the step's index within the run
-// (abort ordering), written on the device so a captured graph can replay
-// the launch for every step.
-template <typename R, int LIM, bool VISC, bool FINAL>
+#ifdef IBGPU_FAST_BUILD
+// Constant-memory table of batched stage arguments.  A batch that fits keeps
+// here, per case, its stage arguments up to the stage-dependent part
+// (kStageCommonBytes), one StageVar per stage and its CaseConst up to its
+// finest level, found through a per-batch header of one int4 per case
+// (byte offsets of the three; w unused).  Read with a CTA-uniform index,
+// these are constant-bank operands like a single-case launch's parameters,
+// which keeps the batched tile body's registers, spills and argument loads
+// at the single-case kernel's level.
+constexpr int kBatchTableBytes = 60 * 1024;
+__constant__ __align__(16) unsigned char c_batch_table[kBatchTableBytes];
+#endif
+
+// Batched stage over a work list of (case, tile) pairs of several
+// independent cases (each its own mesh, state and constants).  TABLE: the
+// case's arguments come from the constant-memory table, header at byte
+// offset `table` (fast builds only); otherwise the stage's arguments of case
+// c are args[c * nstages + stage] and its constants ccs[c] in global memory.
+// phase_base holds 8 x the step's index within the run (abort ordering),
+// written on the device so a captured graph can replay the launch for every
+// step.  LOOP: persistent CTAs striding over the list; otherwise one CTA per
+// item (no loop state, which keeps the tile body's register spills at the
+// single-case kernel's level).
+template <typename R, int LIM, bool VISC, bool FINAL, bool LOOP, bool TABLE>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                        const int2 *__restrict__ work, int nwork, int stage, int nstages,
-                       const int *__restrict__ phase_base) {
+                       const int *__restrict__ phase_base, int table) {
   // phase_base[0]: 8 x the step index; phase_base[1]: 1 when this step's
   // final stage folds in the next step's CFL pass of the cases that allow it
   const int pb = phase_base[0], fold_step = phase_base[1];
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const int2 it = work[w];
-    const StageArgs &a = args[it.x * nstages + stage];
-    const int fold = (FINAL && fold_step && a.cfl_next) ? 1 + pb + 8 + 1 : 0;
-    stage_tile_fast<R, LIM, VISC, FINAL>(a, ccs[it.x], it.y, pb + 2 + stage, fold);
+#ifdef IBGPU_FAST_BUILD
+    if (TABLE) {
+      const int4 h = reinterpret_cast<const int4 *>(c_batch_table + table)[it.x];
+      const StageArgs &a = *reinterpret_cast<const StageArgs *>(c_batch_table + h.x);
+      const StageVar &v = reinterpret_cast<const StageVar *>(c_batch_table + h.y)[stage];
+      const CaseConst &cc = *reinterpret_cast<const CaseConst *>(c_batch_table + h.z);
+      const int fold = (FINAL && fold_step && v.cfl_next) ? 1 + pb + 8 + 1 : 0;
+      stage_tile_fast<R, LIM, VISC, FINAL>(a, v, cc, it.y, pb + 2 + stage, fold);
+    } else
+#endif
+    {
+      const StageArgs &a = args[it.x * nstages + stage];
+      const int fold = (FINAL && fold_step && a.v.cfl_next) ? 1 + pb + 8 + 1 : 0;
+      stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold);
+    }
+    if (!LOOP) break;
     __syncthreads();  // shared-memory reuse by the next work item
   }
 }
@@ -930,36 +965,88 @@ void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limit
 }
 
 #ifdef IBGPU_FAST_BUILD
-template <typename R, int LIM>
-static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+template <typename R, int LIM, bool LOOP, bool TABLE>
+static void launch_batch_l(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
-                           bool final_stage, int grid, cudaStream_t st) {
+                           bool final_stage, int grid, int table, cudaStream_t st) {
   dim3 g(grid), block(StageThreads<R>::value);
   if (visc) {
     if (final_stage)
-      stage_kernel_batch<R, LIM, true, true><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+      stage_kernel_batch<R, LIM, true, true, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
     else
-      stage_kernel_batch<R, LIM, true, false><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+      stage_kernel_batch<R, LIM, true, false, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
   } else {
     if (final_stage)
-      stage_kernel_batch<R, LIM, false, true><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+      stage_kernel_batch<R, LIM, false, true, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
     else
-      stage_kernel_batch<R, LIM, false, false><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base);
+      stage_kernel_batch<R, LIM, false, false, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+  }
+}
+
+// grid == nwork: one CTA per work item; fewer: persistent CTAs.  table >= 0:
+// the arguments come from the constant-memory table.
+template <typename R, int LIM>
+static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                           int stage, int nstages, const int *phase_base, bool visc,
+                           bool final_stage, int grid, int table, cudaStream_t st) {
+  const bool loop = grid < nwork;
+  if (!loop) grid = nwork;
+  if (table >= 0) {
+    if (loop) launch_batch_l<R, LIM, true, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    else launch_batch_l<R, LIM, false, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+  } else {
+    if (loop) launch_batch_l<R, LIM, true, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
+    else launch_batch_l<R, LIM, false, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
   }
 }
 
 void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                         int stage, int nstages, const int *phase_base, int limiter, bool visc,
-                        bool final_stage, bool mixed, int grid, cudaStream_t st) {
+                        bool final_stage, bool mixed, int grid, int table, cudaStream_t st) {
   if (nwork <= 0) return;
   if (grid < 1 || grid > nwork) grid = nwork;
+  if (table >= kBatchTableBytes) table = -1;
   if (mixed) {
-    if (limiter == LIM_MINMOD) launch_batch_t<float, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
-    else launch_batch_t<float, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+    if (limiter == LIM_MINMOD) launch_batch_t<float, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    else launch_batch_t<float, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
   } else {
-    if (limiter == LIM_MINMOD) launch_batch_t<double, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
-    else launch_batch_t<double, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, st);
+    if (limiter == LIM_MINMOD) launch_batch_t<double, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    else launch_batch_t<double, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
   }
+}
+
+// ---- constant-memory table: first-fit byte ranges per device
+namespace {
+std::mutex g_table_mu;
+std::map<int, std::map<int, int>> g_table_used;  // device -> (offset -> bytes)
+}  // namespace
+
+int batch_table_reserve(int device, int bytes) {
+  if (bytes <= 0 || bytes > kBatchTableBytes) return -1;
+  bytes = (bytes + 15) & ~15;
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  std::map<int, int> &used = g_table_used[device];
+  int at = 0;
+  for (const auto &r : used) {
+    if (r.first - at >= bytes) break;
+    at = r.first + r.second;
+  }
+  if (at + bytes > kBatchTableBytes) return -1;
+  used[at] = bytes;
+  return at;
+}
+
+void batch_table_release(int device, int offset) {
+  if (offset < 0) return;
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  auto d = g_table_used.find(device);
+  if (d != g_table_used.end()) d->second.erase(offset);
+}
+
+cudaError_t batch_table_write(int offset, const void *src, int bytes) {
+  if (offset < 0 || bytes < 0 || offset + bytes > kBatchTableBytes) return cudaErrorInvalidValue;
+  return cudaMemcpyToSymbol(c_batch_table, src, (size_t)bytes, (size_t)offset,
+                            cudaMemcpyHostToDevice);
 }
 
 // CFL pass of every batched case in one launch: one CTA per (case, tile)

@@ -8,6 +8,7 @@
 // neighbour table wraps around instead.  Absent slots have flags == 0.
 #pragma once
 
+#include <stddef.h>
 #include <stdint.h>
 
 namespace ibgpu {
@@ -76,26 +77,39 @@ struct DevDiag {
 
 constexpr int kHaloStage = 2;
 
-struct StageArgs {
-  const int32_t *tile_nb;  // 9 neighbour tiles per tile, (oy+1)*3+(ox+1); -1 absent
-  const int32_t *tile_level;
-  const uint8_t *tile_uniform;  // 1: tile and side neighbours all recovering leaf cells
-  const uint8_t *flags;
-  int tile_begin;
-  double *s0[kStateFields];  // step state rho u v p e T
-  const double *sin[4];      // stage input of varying cells (rho u v p)
-  double *sout[4];           // stage output (non-final stages)
-  const double *vsd;         // frozen viscous residual parts [8][nslots] or null
-  int64_t nslots;
-  double tp;                 // stage coefficient tp[k]
-  int phase;                 // abort-order phase of this stage (see DevDiag)
-  DevDiag *diag;
+// Stage-dependent part of the stage arguments.
+struct StageVar {
+  const double *sin[4];  // stage input of varying cells (rho u v p)
+  double *sout[4];       // stage output (non-final stages)
+  double tp;             // stage coefficient tp[k]
   // final stage only: 1 + the abort-order phase of the next step's CFL pass
   // to fold that pass into this stage (0: off).  The next step's CFL reads
   // the normal cells this stage writes, and nothing else writes them in
   // between when the run has one level and no immersed body.
   int cfl_next;
+  int pad_;
 };
+
+struct StageArgs {
+  const int32_t *tile_nb;  // 9 neighbour tiles per tile, (oy+1)*3+(ox+1); -1 absent
+  const int32_t *tile_level;
+  const uint8_t *tile_uniform;  // 1: tile and side neighbours all recovering leaf cells
+  const uint8_t *flags;
+  double *s0[kStateFields];  // step state rho u v p e T
+  const double *vsd;         // frozen viscous residual parts [8][nslots] or null
+  int64_t nslots;
+  DevDiag *diag;
+  int tile_begin;
+  int phase;  // abort-order phase of this stage (see DevDiag)
+  // last member: the batched stage's constant-memory table keeps each case's
+  // arguments up to here once and its StageVar records per stage
+  StageVar v;
+};
+
+// bytes of StageArgs before the stage-dependent part
+constexpr int kStageCommonBytes = (int)offsetof(StageArgs, v);
+static_assert(kStageCommonBytes % 8 == 0, "StageVar starts 8-byte aligned");
+static_assert(sizeof(StageVar) % 8 == 0, "StageVar keeps 8-byte alignment");
 
 struct CflArgs {
   const int32_t *tile_level;

@@ -207,10 +207,10 @@ extern "C" int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx,
   for (int k = 0; k < cs->nstages; ++k) {
     const bool fin = k == cs->nstages - 1;
     for (int f = 0; f < 4; ++f) {
-      sa.sin[f] = (k == 0) ? sa.s0[map[f]] : d_buf + ((int64_t)(((k - 1) & 1) * 4 + f)) * kMaxCells;
-      sa.sout[f] = fin ? nullptr : d_buf + ((int64_t)((k & 1) * 4 + f)) * kMaxCells;
+      sa.v.sin[f] = (k == 0) ? sa.s0[map[f]] : d_buf + ((int64_t)(((k - 1) & 1) * 4 + f)) * kMaxCells;
+      sa.v.sout[f] = fin ? nullptr : d_buf + ((int64_t)((k & 1) * 4 + f)) * kMaxCells;
     }
-    sa.tp = cs->tp[k];
+    sa.v.tp = cs->tp[k];
     sa.phase = 2 + k;
     if (exact) exact::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, false, st);
     else fast::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, mixed, st);

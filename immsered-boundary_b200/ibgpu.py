@@ -36,7 +36,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_tag_learned", "ibgpu_run", "ibgpu_mlp_train_step", "ibgpu_batch_create",
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
-           "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh")
+           "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
+           "ibgpu_batch_table_bytes")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -221,6 +222,7 @@ def lib(path: str | None = None):
                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_float)]
+    L.ibgpu_batch_table_bytes.argtypes = [vp]
     L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ibgpu_download_state_async.argtypes = [vp, vp]
     L.ibgpu_batch_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
@@ -610,7 +612,8 @@ class Batch:
         tms = (ctypes.c_float * 16)()
         k = lib().ibgpu_batch_tuning(self._b, 16, grids, tms)
         return dict(grid=g.value, period=p.value, stage_ms=ms.value, stage_launches=nl.value,
-                    tuning=[(grids[i], tms[i]) for i in range(max(0, min(k, 16)))])
+                    tuning=[(grids[i], tms[i]) for i in range(max(0, min(k, 16)))],
+                    table_bytes=lib().ibgpu_batch_table_bytes(self._b))
 
     def close(self):
         if self._b:

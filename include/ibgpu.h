@@ -268,6 +268,13 @@ int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage
 /* Autotuner record: up to max (CTA count, ms) pairs; returns the number of
  * candidates timed. */
 int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms);
+/* Bytes of the device's constant-memory argument table this batch holds
+ * (its stage kernels read their arguments from there); 0 when the batch did
+ * not fit and its stage kernels read the arguments from global memory.  The
+ * table (60 KiB per device) is shared by the live batches of the device;
+ * destroying a batch returns its part.  Creation assumes the cases' device
+ * is the current one. */
+int ibgpu_batch_table_bytes(const ibgpu_batch *b);
 void ibgpu_batch_destroy(ibgpu_batch *b);
 
 /* Allocation-free variant of ibgpu_step for one periodic, inviscid,

@@ -43,8 +43,39 @@ def test_batched_vortex_cases_equal_single_runs(cuda_lib, precision):
         assert di.abort_code == 0 and di.cells_marched > 0
     info = b.info()
     assert info["period"] == 1 and len(info["tuning"]) >= 1
+    assert info["table_bytes"] > 0  # arguments read from the constant-memory table
     b.close()
     for s in single + batched:
+        s.close()
+
+
+@pytest.mark.parametrize("precision", [ib.FP64, ib.MIXED])
+def test_batch_beyond_constant_table_reads_global_arguments(cuda_lib, precision):
+    """88 small cases need more than the 60 KiB constant-memory argument
+    table: the batch falls back to arguments in global memory and still
+    equals the cases stepped alone; a small batch created beside it gets
+    table space and agrees too."""
+    cases = [wl.vortex_case(16 * (1 + i % 3), precision=precision, mach=0.2 + 0.007 * i,
+                            angle_deg=float(i % 11)) for i in range(90)]
+    ref = []
+    for c in cases:
+        s = make_solver(c)
+        s.run(0, 3)
+        ref.append((s.dt, s.download()))
+        s.close()
+    sols = [make_solver(c) for c in cases]
+    big = ib.Batch(sols[:88])  # about 736 bytes of table per case
+    small = ib.Batch(sols[88:])
+    assert big.info()["table_bytes"] == 0
+    assert small.info()["table_bytes"] > 0
+    big.run(0, 3)
+    small.run(0, 3)
+    for s, (dt, prim) in zip(sols, ref):
+        assert s.dt == dt
+        assert np.array_equal(s.download(), prim)
+    big.close()
+    small.close()
+    for s in sols:
         s.close()
 
 
