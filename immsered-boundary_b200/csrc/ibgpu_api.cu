@@ -1003,6 +1003,7 @@ struct ibgpu_batch {
   int table = -1;       // byte offset of the arguments in the constant-memory table (-1: global)
   int table_bytes = 0;  // bytes reserved there
   bool tuned = false;
+  int fixed_grid = -1;  // >= 0: CTA count set by the caller (no autotuning)
   bool timing = false;
   double stage_ms = 0.0;
   int64_t stage_launches = 0;
@@ -1289,7 +1290,14 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
   cudaStream_t st = b->stream;
   int rc;
   if (!b->tuned) {
-    if ((rc = autotune(b))) return rc;
+    if (b->fixed_grid >= 0) {
+      b->grid = b->fixed_grid;
+      b->tune_grid.clear();
+      b->tune_ms.clear();
+      b->tuned = true;
+    } else if ((rc = autotune(b))) {
+      return rc;
+    }
     if ((rc = build_graphs(b))) return rc;
   }
   for (int i = 0; i < n; ++i) {
@@ -1365,6 +1373,17 @@ int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float
   for (auto *c : b->cases)
     if (d_params && (rc = tag_mesh_error(c, st))) return rc;
   CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_batch_set_grid(ibgpu_batch *b, int grid) {
+  if (!b || grid < -1) return IBGPU_E_ARG;
+  if (b->stream) CK(cudaStreamSynchronize(b->stream));  // captured graphs may be in flight
+  for (auto g : b->graphs)
+    if (g) cudaGraphExecDestroy(g);
+  b->graphs.clear();
+  b->fixed_grid = grid;
+  b->tuned = false;  // the next run tunes (grid -1) or takes the count, and recaptures
   return IBGPU_OK;
 }
 

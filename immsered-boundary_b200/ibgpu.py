@@ -37,7 +37,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
-           "ibgpu_batch_table_bytes")
+           "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -223,6 +223,7 @@ def lib(path: str | None = None):
     L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_float)]
     L.ibgpu_batch_table_bytes.argtypes = [vp]
+    L.ibgpu_batch_set_grid.argtypes = [vp, ctypes.c_int]
     L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ibgpu_download_state_async.argtypes = [vp, vp]
     L.ibgpu_batch_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
@@ -602,6 +603,11 @@ class Batch:
 
     def set_timing(self, on: bool):
         _check(lib().ibgpu_batch_set_timing(self._b, int(bool(on))), "ibgpu_batch_set_timing")
+
+    def set_grid(self, grid: int):
+        """CTA count of the merged stage launches: 0 one per work item, > 0
+        persistent CTAs, -1 autotuned at the next run (default)."""
+        _check(lib().ibgpu_batch_set_grid(self._b, int(grid)), "ibgpu_batch_set_grid")
 
     def info(self) -> dict:
         g, p = ctypes.c_int(), ctypes.c_int()

@@ -38,6 +38,9 @@ def main():
     ap.add_argument("--limiter", default="vanleer", choices=["vanleer", "minmod"])
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: this many batched vortex cases (50k..800k cells, seed 0)")
+    ap.add_argument("--grid", type=int, default=-1,
+                    help="batched: CTA count of the merged launches (0 one per item, "
+                         "-1 autotuned)")
     a = ap.parse_args()
     pkg = _pkg()
     ib, wl = pkg.ibgpu, pkg.workloads
@@ -50,6 +53,7 @@ def main():
             s.init_flow(prim)
             sols.append(s)
         b = ib.Batch(sols)
+        b.set_grid(a.grid)
         b.run(0, 1)
         t0 = time.perf_counter()
         b.run(1, a.steps)

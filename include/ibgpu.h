@@ -260,6 +260,10 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out);
  * may be NULL) as in ibgpu_run for case i.  Returns the first case's
  * non-OK code, IBGPU_OK when every case ran clean. */
 int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag *diag);
+/* CTA count of the merged stage launches from the next run on: 0 = one CTA
+ * per work item, > 0 = that many persistent CTAs, -1 = chosen by the
+ * autotuner at the next run (the default). */
+int ibgpu_batch_set_grid(ibgpu_batch *b, int grid);
 /* Event timing of the merged stage launches (total ms, launch count). */
 int ibgpu_batch_set_timing(ibgpu_batch *b, int enable);
 /* Chosen CTA count (0 = one CTA per work item), subcycling period, timing. */

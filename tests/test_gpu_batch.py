@@ -49,6 +49,30 @@ def test_batched_vortex_cases_equal_single_runs(cuda_lib, precision):
         s.close()
 
 
+@pytest.mark.parametrize("grid", [0, 3])
+def test_batch_fixed_cta_counts_equal_single_runs(cuda_lib, grid):
+    """One CTA per work item and a persistent grid of 3 CTAs (each strides
+    over many items) set by the caller instead of the autotuner."""
+    cases = [wl.vortex_case(n, precision=ib.MIXED, mach=m) for n, m in [(64, 0.4), (32, 0.7)]]
+    single = [make_solver(c) for c in cases]
+    for s in single:
+        s.run(0, 3)
+    batched = [make_solver(c) for c in cases]
+    b = ib.Batch(batched)
+    b.set_grid(grid)
+    b.run(0, 3)
+    info = b.info()
+    assert info["grid"] == grid and info["tuning"] == []
+    for s, t in zip(single, batched):
+        assert t.dt == s.dt
+        assert np.array_equal(t.download(), s.download())
+    with pytest.raises(ib.IbgpuError):
+        b.set_grid(-2)
+    b.close()
+    for s in single + batched:
+        s.close()
+
+
 @pytest.mark.parametrize("precision", [ib.FP64, ib.MIXED])
 def test_batch_beyond_constant_table_reads_global_arguments(cuda_lib, precision):
     """88 small cases need more than the 60 KiB constant-memory argument
