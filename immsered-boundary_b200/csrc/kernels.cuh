@@ -493,25 +493,28 @@ __device__ __forceinline__ void uniform_piece_dst(int w, int &f, int &dst) {
   }
 }
 
-// Global address of piece w of tile `tile`.
-__device__ __forceinline__ const double *uniform_piece(const StageArgs &a, const StageVar &v, int tile,
-                                                       int w, int &f, int &dst) {
+// Global address of piece w of tile `tile` (side neighbours west, east,
+// south, north already loaded).
+__device__ __forceinline__ const double2 *uniform_src(const StageVar &v, int tile, int nbw, int nbe,
+                                                      int nbs, int nbn, int w) {
+  int f, dst;
   uniform_piece_dst(w, f, dst);
   if (w < 512) {
     const int p = w & 127;
-    return v.sin[f] + (int64_t)tile * kTileCells + (p >> 3) * kTile + (p & 7) * 2;
+    return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)tile * kTileCells +
+                                             (p >> 3) * kTile + (p & 7) * 2);
   }
   if (w < 640) {
     const int q = w - 512;
     const int east = (q >> 4) & 1, row = q & 15;
-    const int nb = a.tile_nb[tile * 9 + (east ? 5 : 3)];
-    return v.sin[f] + (int64_t)nb * kTileCells + row * kTile + (east ? 0 : kTile - 2);
+    return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)(east ? nbe : nbw) * kTileCells +
+                                             row * kTile + (east ? 0 : kTile - 2));
   }
   const int q = w - 640;
   const int north = (q >> 4) & 1, rr = (q >> 3) & 1;
-  const int nb = a.tile_nb[tile * 9 + (north ? 7 : 1)];
   const int srow = north ? rr : kTile - 2 + rr;
-  return v.sin[f] + (int64_t)nb * kTileCells + srow * kTile + (q & 7) * 2;
+  return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)(north ? nbn : nbs) * kTileCells +
+                                           srow * kTile + (q & 7) * 2);
 }
 
 template <typename R, int LIM, bool VISC, bool FINAL>
@@ -541,40 +544,71 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   // recover their primitives, so no presence flags or one-sided stencils
   const bool uni = a.tile_uniform != nullptr && a.tile_uniform[tile] != 0;
 
+  // side neighbours (the centre entry of the table is the tile itself),
+  // loaded beside the tile's level and uniform flag so the region's loads
+  // below wait for one round trip, not one per neighbour lookup
+  const int32_t *nbrow = a.tile_nb + (int64_t)tile * 9;
+  const int nbs = __ldg(nbrow + 1), nbw = __ldg(nbrow + 3), nbe = __ldg(nbrow + 5),
+            nbn = __ldg(nbrow + 7);
+
   if (uni) {
-    // 768 16-byte pieces straight from global memory
+    // 768 16-byte pieces straight from global memory: every load issued
+    // before the first shared-memory store
+    constexpr int NIT = (768 + NT - 1) / NT;
+    double2 val[NIT];
 #pragma unroll
-    for (int it = 0; it < (768 + NT - 1) / NT; ++it) {
+    for (int it = 0; it < NIT; ++it) {
       const int w = tid + it * NT;
-      if (w >= 768) break;
-      int f, dst;
-      const double2 val = __ldg(reinterpret_cast<const double2 *>(uniform_piece(a, v, tile, w, f, dst)));
-      *S::comp(sq, dst, NQ, f) = (R)val.x;
-      *S::comp(sq, dst + 1, NQ, f) = (R)val.y;
+      if (w < 768) val[it] = __ldg(uniform_src(v, tile, nbw, nbe, nbs, nbn, w));
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int w = tid + it * NT;
+      if (w < 768) {
+        int f, dst;
+        uniform_piece_dst(w, f, dst);
+        *S::comp(sq, dst, NQ, f) = (R)val[it].x;
+        *S::comp(sq, dst + 1, NQ, f) = (R)val[it].y;
+      }
     }
   } else {
-    for (int r = tid; r < kReg * kReg; r += NT) {
-      int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
-      int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
-      int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
-      uint8_t f = 0;
-      R q0 = R(0), q1 = R(0), q2 = R(0), q3 = R(0);
-      if (!(ox && oy)) {
-        int nb = a.tile_nb[tile * 9 + (oy + 1) * 3 + (ox + 1)];
-        if (nb >= 0) {
-          int64_t s = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
-          f = a.flags[s];
-          if (f & CF_PRESENT) {
-            const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
-            q0 = (R)(varying ? v.sin[0] : a.s0[F_RHO])[s];
-            q1 = (R)(varying ? v.sin[1] : a.s0[F_U])[s];
-            q2 = (R)(varying ? v.sin[2] : a.s0[F_V])[s];
-            q3 = (R)(varying ? v.sin[3] : a.s0[F_P])[s];
-          }
+    // region records: slot, then presence flags, then the state, each
+    // step's loads of both records issued together
+    constexpr int NIT = (kReg * kReg + NT - 1) / NT;
+    int64_t sl[NIT];
+    uint8_t fl[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int r = tid + it * NT;
+      sl[it] = -1;
+      if (r < kReg * kReg) {
+        const int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
+        const int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
+        const int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
+        if (!(ox && oy)) {
+          const int nb = ox < 0 ? nbw : (ox > 0 ? nbe : (oy < 0 ? nbs : (oy > 0 ? nbn : tile)));
+          if (nb >= 0) sl[it] = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
         }
       }
-      sfl[r] = f;
-      S::st(sq, r, NQ, q0, q1, q2, q3);
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) fl[it] = sl[it] >= 0 ? a.flags[sl[it]] : uint8_t(0);
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int r = tid + it * NT;
+      if (r < kReg * kReg) {
+        R q0 = R(0), q1 = R(0), q2 = R(0), q3 = R(0);
+        if (fl[it] & CF_PRESENT) {
+          const int64_t s = sl[it];
+          const bool varying = (fl[it] & (CF_PRIM | CF_RESET)) != 0;
+          q0 = (R)(varying ? v.sin[0] : a.s0[F_RHO])[s];
+          q1 = (R)(varying ? v.sin[1] : a.s0[F_U])[s];
+          q2 = (R)(varying ? v.sin[2] : a.s0[F_V])[s];
+          q3 = (R)(varying ? v.sin[3] : a.s0[F_P])[s];
+        }
+        sfl[r] = fl[it];
+        S::st(sq, r, NQ, q0, q1, q2, q3);
+      }
     }
   }
   __syncthreads();
