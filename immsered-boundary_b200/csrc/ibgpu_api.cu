@@ -875,6 +875,8 @@ void stage_args(const ibgpu_ctx *ctx, int k, StageArgs &sa) {
     sa.v.sout[f] = fin ? nullptr : ctx->d_buf[k & 1][f];
   }
   sa.v.tp = cs.tp[k];
+  // one wave of resident stage CTAs (4 per SM FP64, 6 mixed)
+  sa.prefetch = ctx->nsm * (cs.precision == IBGPU_MIXED ? 6 : 4);
 }
 
 int64_t marched_cells(const ibgpu_ctx *ctx, int ts) {

@@ -521,7 +521,7 @@ template <typename R, int LIM, bool VISC, bool FINAL>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageVar &v,
                                                 const CaseConst &cc,
                                                 const int tile, const int phase,
-                                                const int fold) {
+                                                const int fold, const int prefetch) {
   constexpr int kSX = kTile + 2;  // x-slope row length (cols -1..16)
   using S = SRec<R>;
   using V = typename S::V;
@@ -550,6 +550,13 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   const int32_t *nbrow = a.tile_nb + (int64_t)tile * 9;
   const int nbs = __ldg(nbrow + 1), nbw = __ldg(nbrow + 3), nbe = __ldg(nbrow + 5),
             nbn = __ldg(nbrow + 7);
+
+  if (prefetch > 0) {
+    // the CTA that starts when this one ends reads this tile's input from L2
+    const int64_t pt = (int64_t)(tile + prefetch) * kTileCells;
+    if (tid < 64 && pt < a.nslots)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(v.sin[tid >> 4] + pt + (tid & 15) * 16));
+  }
 
   if (uni) {
     // 768 16-byte pieces straight from global memory: every load issued
@@ -807,7 +814,7 @@ template <typename R, int LIM, bool VISC, bool FINAL>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
   stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, cc, a.tile_begin + blockIdx.x, a.phase,
-                                       a.v.cfl_next);
+                                       a.v.cfl_next, a.prefetch);
 }
 
 
@@ -851,13 +858,13 @@ __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6
       const StageVar &v = reinterpret_cast<const StageVar *>(c_batch_table + h.y)[stage];
       const CaseConst &cc = *reinterpret_cast<const CaseConst *>(c_batch_table + h.z);
       const int fold = (FINAL && fold_step && v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL>(a, v, cc, it.y, pb + 2 + stage, fold);
+      stage_tile_fast<R, LIM, VISC, FINAL>(a, v, cc, it.y, pb + 2 + stage, fold, 0);
     } else
 #endif
     {
       const StageArgs &a = args[it.x * nstages + stage];
       const int fold = (FINAL && fold_step && a.v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold);
+      stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold, 0);
     }
     if (!LOOP) break;
     __syncthreads();  // shared-memory reuse by the next work item

@@ -101,6 +101,9 @@ struct StageArgs {
   DevDiag *diag;
   int tile_begin;
   int phase;  // abort-order phase of this stage (see DevDiag)
+  // single-case fast stage: warm L2 with the stage input of tile + prefetch,
+  // about one wave of resident CTAs ahead (0: off)
+  int prefetch;
   // last member: the batched stage's constant-memory table keeps each case's
   // arguments up to here once and its StageVar records per stage
   StageVar v;
