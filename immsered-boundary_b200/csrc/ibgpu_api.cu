@@ -94,7 +94,7 @@ struct ibgpu_ctx {
 
   // state: step state (6 fields) + two stage buffers (4 fields each)
   double *d_s0[kStateFields] = {};
-  double *d_buf[2][4] = {};
+  void *d_buf[2][4] = {};  // stage buffers: FP64, FP32 in the mixed build
   double *d_vsd = nullptr;
   double *d_rows = nullptr;  // staging for AoS state transfers
   DevDiag *d_diag = nullptr;
@@ -538,9 +538,10 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
     return rc;
   for (int f = 0; f < kStateFields; ++f)
     if ((rc = dev_alloc(&ctx->d_s0[f], (size_t)nslots))) return rc;
+  const size_t buf_elem = cs.precision == IBGPU_MIXED ? sizeof(float) : sizeof(double);
   for (int b = 0; b < 2; ++b)
     for (int f = 0; f < 4; ++f)
-      if ((rc = dev_alloc(&ctx->d_buf[b][f], (size_t)nslots))) return rc;
+      if ((rc = dev_alloc((unsigned char **)&ctx->d_buf[b][f], (size_t)nslots * buf_elem))) return rc;
   if (cs.viscous && (rc = dev_alloc(&ctx->d_vsd, (size_t)nslots * 8))) return rc;
   cudaStream_t st = ctx->stream;
   CK(cudaMemcpyAsync(ctx->d_tile_nb, h_nb.data(), h_nb.size() * 4, cudaMemcpyHostToDevice, st));
@@ -560,7 +561,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   // absent slots hold zeros in every field (never read as a stencil value)
   for (int f = 0; f < kStateFields; ++f) CK(cudaMemsetAsync(ctx->d_s0[f], 0, nslots * 8, st));
   for (int b = 0; b < 2; ++b)
-    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(ctx->d_buf[b][f], 0, nslots * 8, st));
+    for (int f = 0; f < 4; ++f) CK(cudaMemsetAsync(ctx->d_buf[b][f], 0, nslots * buf_elem, st));
   if (ctx->d_vsd) CK(cudaMemsetAsync(ctx->d_vsd, 0, nslots * 8 * 8, st));
   CK(cudaStreamSynchronize(st));
   ctx->tilemap = std::move(tilemap);
@@ -962,8 +963,8 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
         if (ts % cs.march_step[l] != cs.march_left[l]) continue;
         sa.tile_begin = ctx->level_tile_begin[l];
         cudaEvent_t e = tm.mark(0);
-        if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, st);
-        else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, st);
+        if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, k, st);
+        else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, k, st);
         tm.done(e);
         CK(cudaGetLastError());
       }

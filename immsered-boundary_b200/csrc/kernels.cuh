@@ -165,10 +165,10 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
         f = a.flags[s];
         if (f & CF_PRESENT) {
           const bool varying = (f & (CF_PRIM | CF_RESET)) != 0;
-          const double *p0 = varying ? a.v.sin[0] : a.s0[F_RHO];
-          const double *p1 = varying ? a.v.sin[1] : a.s0[F_U];
-          const double *p2 = varying ? a.v.sin[2] : a.s0[F_V];
-          const double *p3 = varying ? a.v.sin[3] : a.s0[F_P];
+          const double *p0 = varying ? static_cast<const double *>(a.v.sin[0]) : a.s0[F_RHO];
+          const double *p1 = varying ? static_cast<const double *>(a.v.sin[1]) : a.s0[F_U];
+          const double *p2 = varying ? static_cast<const double *>(a.v.sin[2]) : a.s0[F_V];
+          const double *p3 = varying ? static_cast<const double *>(a.v.sin[3]) : a.s0[F_P];
           q0 = (R)p0[s];
           q1 = (R)p1[s];
           q2 = (R)p2[s];
@@ -308,10 +308,10 @@ __global__ void __launch_bounds__(kTileCells) stage_kernel(StageArgs a, CaseCons
         a.s0[F_E][slot] = ne;
         a.s0[F_T][slot] = nT;
       } else {
-        a.v.sout[0][slot] = nrho;
-        a.v.sout[1][slot] = nu;
-        a.v.sout[2][slot] = nv;
-        a.v.sout[3][slot] = np;
+        static_cast<double *>(a.v.sout[0])[slot] = nrho;
+        static_cast<double *>(a.v.sout[1])[slot] = nu;
+        static_cast<double *>(a.v.sout[2])[slot] = nv;
+        static_cast<double *>(a.v.sout[3])[slot] = np;
       }
     }
     if (FINAL && (fl & CF_RESNORM)) {
@@ -494,30 +494,69 @@ __device__ __forceinline__ void uniform_piece_dst(int w, int &f, int &dst) {
 }
 
 // Global address of piece w of tile `tile` (side neighbours west, east,
-// south, north already loaded).
+// south, north already loaded), FP64 stage input.
 __device__ __forceinline__ const double2 *uniform_src(const StageVar &v, int tile, int nbw, int nbe,
                                                       int nbs, int nbn, int w) {
   int f, dst;
   uniform_piece_dst(w, f, dst);
+  const double *in = static_cast<const double *>(v.sin[f]);
   if (w < 512) {
     const int p = w & 127;
-    return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)tile * kTileCells +
-                                             (p >> 3) * kTile + (p & 7) * 2);
+    return reinterpret_cast<const double2 *>(in + (int64_t)tile * kTileCells + (p >> 3) * kTile +
+                                             (p & 7) * 2);
   }
   if (w < 640) {
     const int q = w - 512;
     const int east = (q >> 4) & 1, row = q & 15;
-    return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)(east ? nbe : nbw) * kTileCells +
+    return reinterpret_cast<const double2 *>(in + (int64_t)(east ? nbe : nbw) * kTileCells +
                                              row * kTile + (east ? 0 : kTile - 2));
   }
   const int q = w - 640;
   const int north = (q >> 4) & 1, rr = (q >> 3) & 1;
   const int srow = north ? rr : kTile - 2 + rr;
-  return reinterpret_cast<const double2 *>(v.sin[f] + (int64_t)(north ? nbn : nbs) * kTileCells +
+  return reinterpret_cast<const double2 *>(in + (int64_t)(north ? nbn : nbs) * kTileCells +
                                            srow * kTile + (q & 7) * 2);
 }
 
-template <typename R, int LIM, bool VISC, bool FINAL>
+// FP32 stage input of a uniform tile: 448 16-byte pieces of four adjacent
+// cells of one field row: the tile (w < 256), the west/east neighbours'
+// last/first four columns (w < 384; the strip keeps two of them) and the
+// south/north neighbours' two rows (w < 448).  Piece w of field f lands on
+// region records dst + c for its cells c in [c0, c0 + n).
+__device__ __forceinline__ const float4 *uniform_src32(const StageVar &v, int tile, int nbw, int nbe,
+                                                       int nbs, int nbn, int w, int &f, int &dst,
+                                                       int &c0) {
+  c0 = 0;
+  if (w < 256) {
+    f = w >> 6;
+    const int p = w & 63, row = p >> 2, col = (p & 3) * 4;
+    dst = (row + kHalo) * kReg + col + kHalo;
+    return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
+                                            (int64_t)tile * kTileCells + row * kTile + col);
+  }
+  if (w < 384) {
+    const int q = w - 256;
+    f = q >> 5;
+    const int east = (q >> 4) & 1, row = q & 15;
+    // east strip = neighbour columns 0, 1 (cells 0, 1 of the piece) at region
+    // columns 18, 19; west strip = neighbour columns 14, 15 (cells 2, 3) at 0, 1
+    c0 = east ? 0 : 2;
+    dst = (row + kHalo) * kReg + (east ? kTile + kHalo : 0) - c0;
+    return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
+                                            (int64_t)(east ? nbe : nbw) * kTileCells + row * kTile +
+                                            (east ? 0 : kTile - 4));
+  }
+  const int q = w - 384;
+  f = q >> 4;
+  const int north = (q >> 3) & 1, rr = (q >> 2) & 1, col = (q & 3) * 4;
+  const int srow = north ? rr : kTile - 2 + rr;
+  dst = (north ? kTile + kHalo + rr : rr) * kReg + col + kHalo;
+  return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
+                                          (int64_t)(north ? nbn : nbs) * kTileCells + srow * kTile +
+                                          col);
+}
+
+template <typename R, int LIM, bool VISC, bool FINAL, typename TI>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageVar &v,
                                                 const CaseConst &cc,
                                                 const int tile, const int phase,
@@ -553,12 +592,38 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
 
   if (prefetch > 0) {
     // the CTA that starts when this one ends reads this tile's input from L2
+    constexpr int kLines = kTileCells * (int)sizeof(TI) / 128;  // 128-byte lines per field
     const int64_t pt = (int64_t)(tile + prefetch) * kTileCells;
-    if (tid < 64 && pt < a.nslots)
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(v.sin[tid >> 4] + pt + (tid & 15) * 16));
+    if (tid < 4 * kLines && pt < a.nslots)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const TI *>(v.sin[tid / kLines]) + pt +
+                                                    (tid % kLines) * (128 / (int)sizeof(TI))));
   }
 
-  if (uni) {
+  if (uni && sizeof(TI) == 4) {
+    // FP32 input: 448 16-byte pieces, every load issued before the first
+    // shared-memory store
+    constexpr int NIT = (448 + NT - 1) / NT;
+    float4 val[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int w = tid + it * NT;
+      int f, dst, c0;
+      if (w < 448) val[it] = __ldg(uniform_src32(v, tile, nbw, nbe, nbs, nbn, w, f, dst, c0));
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int w = tid + it * NT;
+      if (w < 448) {
+        int f, dst, c0;
+        uniform_src32(v, tile, nbw, nbe, nbs, nbn, w, f, dst, c0);
+        const float c[4] = {val[it].x, val[it].y, val[it].z, val[it].w};
+        const bool strip = w >= 256 && w < 384;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (!strip || (i >= c0 && i < c0 + 2)) *S::comp(sq, dst + i, NQ, f) = (R)c[i];
+      }
+    }
+  } else if (uni) {
     // 768 16-byte pieces straight from global memory: every load issued
     // before the first shared-memory store
     constexpr int NIT = (768 + NT - 1) / NT;
@@ -608,10 +673,17 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
         if (fl[it] & CF_PRESENT) {
           const int64_t s = sl[it];
           const bool varying = (fl[it] & (CF_PRIM | CF_RESET)) != 0;
-          q0 = (R)(varying ? v.sin[0] : a.s0[F_RHO])[s];
-          q1 = (R)(varying ? v.sin[1] : a.s0[F_U])[s];
-          q2 = (R)(varying ? v.sin[2] : a.s0[F_V])[s];
-          q3 = (R)(varying ? v.sin[3] : a.s0[F_P])[s];
+          if (varying) {
+            q0 = (R) static_cast<const TI *>(v.sin[0])[s];
+            q1 = (R) static_cast<const TI *>(v.sin[1])[s];
+            q2 = (R) static_cast<const TI *>(v.sin[2])[s];
+            q3 = (R) static_cast<const TI *>(v.sin[3])[s];
+          } else {
+            q0 = (R)a.s0[F_RHO][s];
+            q1 = (R)a.s0[F_U][s];
+            q2 = (R)a.s0[F_V][s];
+            q3 = (R)a.s0[F_P][s];
+          }
         }
         sfl[r] = fl[it];
         S::st(sq, r, NQ, q0, q1, q2, q3);
@@ -790,10 +862,12 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
         a.s0[F_E][slot] = ne;
         a.s0[F_T][slot] = nT;
       } else {
-        v.sout[0][slot] = nrho;
-        v.sout[1][slot] = nu;
-        v.sout[2][slot] = nv;
-        v.sout[3][slot] = np;
+        // stage buffers in the arithmetic's precision (FP32 in the mixed build)
+        typedef R TO;
+        static_cast<TO *>(v.sout[0])[slot] = (TO)nrho;
+        static_cast<TO *>(v.sout[1])[slot] = (TO)nu;
+        static_cast<TO *>(v.sout[2])[slot] = (TO)nv;
+        static_cast<TO *>(v.sout[3])[slot] = (TO)np;
       }
     }
     if (FINAL && (fl & CF_RESNORM)) {
@@ -810,11 +884,13 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   }
 }
 
-template <typename R, int LIM, bool VISC, bool FINAL>
+// TI: element type of the stage input (the FP64 step state for the first
+// stage; the stage buffers, R, after it)
+template <typename R, int LIM, bool VISC, bool FINAL, typename TI>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_fast(StageArgs a, CaseConst cc) {
-  stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, cc, a.tile_begin + blockIdx.x, a.phase,
-                                       a.v.cfl_next, a.prefetch);
+  stage_tile_fast<R, LIM, VISC, FINAL, TI>(a, a.v, cc, a.tile_begin + blockIdx.x, a.phase,
+                                           a.v.cfl_next, a.prefetch);
 }
 
 
@@ -841,7 +917,7 @@ __constant__ __align__(16) unsigned char c_batch_table[kBatchTableBytes];
 // step.  LOOP: persistent CTAs striding over the list; otherwise one CTA per
 // item (no loop state, which keeps the tile body's register spills at the
 // single-case kernel's level).
-template <typename R, int LIM, bool VISC, bool FINAL, bool LOOP, bool TABLE>
+template <typename R, int LIM, bool VISC, bool FINAL, bool LOOP, bool TABLE, typename TI>
 __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
     stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                        const int2 *__restrict__ work, int nwork, int stage, int nstages,
@@ -858,13 +934,13 @@ __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6
       const StageVar &v = reinterpret_cast<const StageVar *>(c_batch_table + h.y)[stage];
       const CaseConst &cc = *reinterpret_cast<const CaseConst *>(c_batch_table + h.z);
       const int fold = (FINAL && fold_step && v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL>(a, v, cc, it.y, pb + 2 + stage, fold, 0);
+      stage_tile_fast<R, LIM, VISC, FINAL, TI>(a, v, cc, it.y, pb + 2 + stage, fold, 0);
     } else
 #endif
     {
       const StageArgs &a = args[it.x * nstages + stage];
       const int fold = (FINAL && fold_step && a.v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold, 0);
+      stage_tile_fast<R, LIM, VISC, FINAL, TI>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold, 0);
     }
     if (!LOOP) break;
     __syncthreads();  // shared-memory reuse by the next work item
@@ -966,62 +1042,97 @@ __global__ void gather_state_kernel(double *rows, const int32_t *cell_slot, int6
 }
 
 // ---- launchers (one set per arithmetic build)
-#ifdef IBGPU_FAST_BUILD
-#define IBGPU_STAGE_KERNEL stage_kernel_fast
-#else
-#define IBGPU_STAGE_KERNEL stage_kernel
-#endif
 
 
-template <typename R, int LIM>
-static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
-                           bool final_stage, cudaStream_t st) {
 #ifdef IBGPU_FAST_BUILD
+template <typename R, int LIM, typename TI>
+static void launch_stage_ti(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
+                            bool final_stage, cudaStream_t st) {
   dim3 grid(ntiles), block(StageThreads<R>::value);
-#else
-  dim3 grid(ntiles), block(kTileCells);
-#endif
   if (visc) {
-    if (final_stage) IBGPU_STAGE_KERNEL<R, LIM, true, true><<<grid, block, 0, st>>>(a, cc);
-    else IBGPU_STAGE_KERNEL<R, LIM, true, false><<<grid, block, 0, st>>>(a, cc);
+    if (final_stage) stage_kernel_fast<R, LIM, true, true, TI><<<grid, block, 0, st>>>(a, cc);
+    else stage_kernel_fast<R, LIM, true, false, TI><<<grid, block, 0, st>>>(a, cc);
   } else {
-    if (final_stage) IBGPU_STAGE_KERNEL<R, LIM, false, true><<<grid, block, 0, st>>>(a, cc);
-    else IBGPU_STAGE_KERNEL<R, LIM, false, false><<<grid, block, 0, st>>>(a, cc);
+    if (final_stage) stage_kernel_fast<R, LIM, false, true, TI><<<grid, block, 0, st>>>(a, cc);
+    else stage_kernel_fast<R, LIM, false, false, TI><<<grid, block, 0, st>>>(a, cc);
   }
 }
 
+// in32: the stage input is the mixed build's FP32 stage buffer
+template <typename R, int LIM>
+static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
+                           bool final_stage, bool in32, cudaStream_t st) {
+  if constexpr (sizeof(R) == 4) {
+    if (in32) {
+      launch_stage_ti<R, LIM, float>(a, cc, ntiles, visc, final_stage, st);
+      return;
+    }
+  }
+  launch_stage_ti<R, LIM, double>(a, cc, ntiles, visc, final_stage, st);
+}
+#else
+template <typename R, int LIM>
+static void launch_stage_t(const StageArgs &a, const CaseConst &cc, int ntiles, bool visc,
+                           bool final_stage, bool, cudaStream_t st) {
+  dim3 grid(ntiles), block(kTileCells);
+  if (visc) {
+    if (final_stage) stage_kernel<R, LIM, true, true><<<grid, block, 0, st>>>(a, cc);
+    else stage_kernel<R, LIM, true, false><<<grid, block, 0, st>>>(a, cc);
+  } else {
+    if (final_stage) stage_kernel<R, LIM, false, true><<<grid, block, 0, st>>>(a, cc);
+    else stage_kernel<R, LIM, false, false><<<grid, block, 0, st>>>(a, cc);
+  }
+}
+#endif
+
 void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limiter, bool visc,
-                  bool final_stage, bool mixed, cudaStream_t st) {
+                  bool final_stage, bool mixed, int stage, cudaStream_t st) {
   if (ntiles <= 0) return;
 #ifndef IBGPU_FAST_BUILD
   mixed = false;  // the exact build is FP64 only
 #endif
+  const bool in32 = mixed && stage > 0;
   if (mixed) {
-    if (limiter == LIM_MINMOD) launch_stage_t<float, LIM_MINMOD>(a, cc, ntiles, visc, final_stage, st);
-    else launch_stage_t<float, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, st);
+    if (limiter == LIM_MINMOD) launch_stage_t<float, LIM_MINMOD>(a, cc, ntiles, visc, final_stage, in32, st);
+    else launch_stage_t<float, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, in32, st);
   } else {
-    if (limiter == LIM_MINMOD) launch_stage_t<double, LIM_MINMOD>(a, cc, ntiles, visc, final_stage, st);
-    else launch_stage_t<double, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, st);
+    if (limiter == LIM_MINMOD) launch_stage_t<double, LIM_MINMOD>(a, cc, ntiles, visc, final_stage, false, st);
+    else launch_stage_t<double, LIM_VANLEER>(a, cc, ntiles, visc, final_stage, false, st);
   }
 }
 
 #ifdef IBGPU_FAST_BUILD
-template <typename R, int LIM, bool LOOP, bool TABLE>
+template <typename R, int LIM, bool LOOP, bool TABLE, typename TI>
 static void launch_batch_l(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
                            bool final_stage, int grid, int table, cudaStream_t st) {
   dim3 g(grid), block(StageThreads<R>::value);
   if (visc) {
     if (final_stage)
-      stage_kernel_batch<R, LIM, true, true, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+      stage_kernel_batch<R, LIM, true, true, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
     else
-      stage_kernel_batch<R, LIM, true, false, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+      stage_kernel_batch<R, LIM, true, false, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
   } else {
     if (final_stage)
-      stage_kernel_batch<R, LIM, false, true, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+      stage_kernel_batch<R, LIM, false, true, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
     else
-      stage_kernel_batch<R, LIM, false, false, LOOP, TABLE><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+      stage_kernel_batch<R, LIM, false, false, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
   }
+}
+
+// stage input element type: the FP64 step state for the first stage, the
+// stage buffers (R) after it
+template <typename R, int LIM, bool LOOP, bool TABLE>
+static void launch_batch_i(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                           int stage, int nstages, const int *phase_base, bool visc,
+                           bool final_stage, int grid, int table, cudaStream_t st) {
+  if constexpr (sizeof(R) == 4) {
+    if (stage > 0) {
+      launch_batch_l<R, LIM, LOOP, TABLE, float>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+      return;
+    }
+  }
+  launch_batch_l<R, LIM, LOOP, TABLE, double>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
 }
 
 // grid == nwork: one CTA per work item; fewer: persistent CTAs.  table >= 0:
@@ -1033,11 +1144,11 @@ static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const in
   const bool loop = grid < nwork;
   if (!loop) grid = nwork;
   if (table >= 0) {
-    if (loop) launch_batch_l<R, LIM, true, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
-    else launch_batch_l<R, LIM, false, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    if (loop) launch_batch_i<R, LIM, true, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    else launch_batch_i<R, LIM, false, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
   } else {
-    if (loop) launch_batch_l<R, LIM, true, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
-    else launch_batch_l<R, LIM, false, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
+    if (loop) launch_batch_i<R, LIM, true, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
+    else launch_batch_i<R, LIM, false, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
   }
 }
 

@@ -12,7 +12,7 @@ namespace ibgpu {
 #define IBGPU_DECLARE_LAUNCHERS(NS)                                                           \
   namespace NS {                                                                              \
   void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limiter,         \
-                    bool visc, bool final_stage, bool mixed, cudaStream_t st);                \
+                    bool visc, bool final_stage, bool mixed, int stage, cudaStream_t st);     \
   void launch_cfl(const CflArgs &a, const CaseConst &cc, int nsm, cudaStream_t st);           \
   void launch_step_begin(DevDiag *d, cudaStream_t st);                                         \
   void launch_take_folded_cfl(DevDiag *d, const CaseConst &cc, cudaStream_t st);              \

@@ -77,10 +77,14 @@ struct DevDiag {
 
 constexpr int kHaloStage = 2;
 
-// Stage-dependent part of the stage arguments.
+// Stage-dependent part of the stage arguments.  Stage input and output of
+// the varying cells (rho u v p): the first stage reads the FP64 step state;
+// the stage buffers between stages hold FP64 values in the FP64 builds and
+// FP32 values in the mixed build, whose flux reads its inputs as FP32 (the
+// rounding happens at the store instead of the load: same values).
 struct StageVar {
-  const double *sin[4];  // stage input of varying cells (rho u v p)
-  double *sout[4];       // stage output (non-final stages)
+  const void *sin[4];  // stage input of varying cells
+  void *sout[4];       // stage output (non-final stages)
   double tp;             // stage coefficient tp[k]
   // final stage only: 1 + the abort-order phase of the next step's CFL pass
   // to fold that pass into this stage (0: off).  The next step's CFL reads

@@ -207,13 +207,15 @@ extern "C" int ibgpu_step_periodic_noalloc(const ibgpu_case *cs, int ts, int nx,
   for (int k = 0; k < cs->nstages; ++k) {
     const bool fin = k == cs->nstages - 1;
     for (int f = 0; f < 4; ++f) {
-      sa.v.sin[f] = (k == 0) ? sa.s0[map[f]] : d_buf + ((int64_t)(((k - 1) & 1) * 4 + f)) * kMaxCells;
-      sa.v.sout[f] = fin ? nullptr : d_buf + ((int64_t)((k & 1) * 4 + f)) * kMaxCells;
+      // stage buffers (FP32 values in the mixed build, in the same regions)
+      sa.v.sin[f] = (k == 0) ? (const void *)sa.s0[map[f]]
+                             : (const void *)(d_buf + ((int64_t)(((k - 1) & 1) * 4 + f)) * kMaxCells);
+      sa.v.sout[f] = fin ? nullptr : (void *)(d_buf + ((int64_t)((k & 1) * 4 + f)) * kMaxCells);
     }
     sa.v.tp = cs->tp[k];
     sa.phase = 2 + k;
-    if (exact) exact::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, false, st);
-    else fast::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, mixed, st);
+    if (exact) exact::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, false, k, st);
+    else fast::launch_stage(sa, cc, ntiles, cs->limiter, false, fin, mixed, k, st);
   }
   noalloc_rows_out_kernel<<<(nx * ny + 255) / 256, 256, 0, st>>>(d_s0, nx, ny, d_rows_out);
   NA_CK(cudaGetLastError());
