@@ -640,14 +640,7 @@ __global__ void features_kernel(FeatConst F, int64_t n, const int64_t *__restric
   }
 }
 
-__global__ void class_to_tag_kernel(const uint8_t *__restrict__ cls, int64_t n,
-                                    uint8_t *__restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const uint8_t c = cls[i];
-    out[i] = c == 0 ? (uint8_t)IBGPU_TAG_REFINE : (c == 1 ? (uint8_t)IBGPU_TAG_COARSEN : (uint8_t)0);
-  }
-}
+
 
 // ---------------------------------------------------------------------------
 // Deployment on the mesh: every normal cell of the context, features
@@ -679,7 +672,35 @@ struct MeshArgs {
 struct FeatScale {
   double inv_rho, inv_c, inv_p, left, yc, inv_chord;
   double dx[IBGPU_TAG_MAX_LEVELS], dy[IBGPU_TAG_MAX_LEVELS];
+  // levels on which the rule requests refinement / coarsening (bit l); the
+  // learned decision, like the plain one, only acts where requested
+  unsigned refine_levels, coarsen_levels;
 };
+
+// The rule's request masks over the levels (coarsening never on level 0).
+inline void request_masks(const ibgpu_tag_rule *rule, unsigned &refine, unsigned &coarsen) {
+  refine = coarsen = 0u;
+  for (int k = 0; k < IBGPU_TAG_MAX_LEVELS; ++k) {
+    if (rule->torefine[k]) refine |= 1u << k;
+    if (k >= 1 && rule->toderefine[k]) coarsen |= 1u << k;
+  }
+}
+
+// Class (0 refine, 1 coarsen, 2 keep) -> tag bits on level l under the masks.
+__host__ __device__ __forceinline__ uint8_t masked_tag(int c, int l, unsigned refine,
+                                                       unsigned coarsen) {
+  if (c == 0 && ((refine >> l) & 1u)) return (uint8_t)IBGPU_TAG_REFINE;
+  if (c == 1 && ((coarsen >> l) & 1u)) return (uint8_t)IBGPU_TAG_COARSEN;
+  return 0;
+}
+
+__global__ void class_to_tag_kernel(const uint8_t *__restrict__ cls, int64_t n,
+                                    const int32_t *__restrict__ lvl, unsigned refine,
+                                    unsigned coarsen, uint8_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = masked_tag(cls[i], lvl[i], refine, coarsen);
+}
 
 __global__ void __launch_bounds__(kThreads)
     mlp_tag_mesh_kernel(const float *__restrict__ P, MeshArgs m, FeatScale F, int *__restrict__ err) {
@@ -815,9 +836,9 @@ __global__ void __launch_bounds__(kThreads)
       int am = 0;
       if (z[1] > z[am]) am = 1;
       if (z[2] > z[am]) am = 2;
-      uint8_t tag = 0;
-      if (normal) tag = am == 0 ? (uint8_t)IBGPU_TAG_REFINE : (am == 1 ? (uint8_t)IBGPU_TAG_COARSEN : 0);
-      m.tags[slot] = tag;
+      m.tags[slot] = normal ? masked_tag(am, m.tile_level[slot >> 8], F.refine_levels,
+                                         F.coarsen_levels)
+                            : (uint8_t)0;
     }
     tc_sync();  // every lane read before the next item's MMAs overwrite them
   }
@@ -1076,6 +1097,7 @@ int tag_mesh_enqueue(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_
     F.dx[k] = V.cc.lev[k].dx > 0 ? V.cc.lev[k].dx : 1.0;
     F.dy[k] = V.cc.lev[k].dy > 0 ? V.cc.lev[k].dy : 1.0;
   }
+  request_masks(rule, F.refine_levels, F.coarsen_levels);
   if (d_params) {
     const int64_t items = V.nslots / kRows;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)V.nsm * 3));
@@ -1195,14 +1217,17 @@ int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_ta
   const int64_t n = cells->n;
   if (n == 0) return IBGPU_OK;
   if (!out || !d_params) return IBGPU_E_ARG;
-  DevBuf feat, cls, tags;
+  DevBuf feat, cls, tags, lvl;
   CKI(cudaMalloc(&feat.p, (size_t)n * kIn * sizeof(uint16_t)));
   CKI(cudaMalloc(&cls.p, (size_t)n));
   CKI(cudaMalloc(&tags.p, (size_t)n));
+  if ((rc = upload(lvl, cells->level, n, V.stream))) return rc;
   if ((rc = features_impl(V, ctx, rule, cells, feat.as<uint16_t>()))) return rc;
   if ((rc = forward_impl(V, d_params, n, feat.as<uint16_t>(), cls.as<uint8_t>(), nullptr))) return rc;
-  class_to_tag_kernel<<<grid_for(n, V.nsm, 256), 256, 0, V.stream>>>(cls.as<uint8_t>(), n,
-                                                                      tags.as<uint8_t>());
+  unsigned refine, coarsen;
+  request_masks(rule, refine, coarsen);
+  class_to_tag_kernel<<<grid_for(n, V.nsm, 256), 256, 0, V.stream>>>(
+      cls.as<uint8_t>(), n, lvl.as<int32_t>(), refine, coarsen, tags.as<uint8_t>());
   CKI(cudaGetLastError());
   CKI(cudaMemcpyAsync(out, tags.p, (size_t)n, cudaMemcpyDeviceToHost, V.stream));
   CKI(cudaStreamSynchronize(V.stream));

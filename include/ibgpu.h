@@ -408,7 +408,10 @@ int ibgpu_mlp_train_step(ibgpu_ctx *ctx, float *d_params, float *d_m, float *d_v
 
 /* Learned tags: the features of the boxes, the MLP and the class mapped to
  * the plain criterion's bits (refine -> IBGPU_TAG_REFINE, coarsen ->
- * IBGPU_TAG_COARSEN, keep -> 0); host output. */
+ * IBGPU_TAG_COARSEN, keep -> 0); host output.  Like the plain criterion it
+ * refines only on levels whose rule->torefine is set and coarsens only on
+ * levels >= 1 whose rule->toderefine is set (AMR::TagtheBox acts only on
+ * the requests of AMRLevel::torefine / toderefine). */
 int ibgpu_tag_learned(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const ibgpu_tag_cells *cells,
                       const float *d_params, uint8_t *out);
 

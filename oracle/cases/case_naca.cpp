@@ -13,7 +13,27 @@
 //
 // Environment: IB_NX (base cells per side, default 128), IB_LEVELS (mesh
 // levels, default 4), IB_NPTS (surface points per side, default 200).
+//
+// Runtime regrids (harness options; off by default).  The shipped case calls
+// AMR::PerformAdaptive every 2 steps but requests neither refinement nor
+// coarsening after the mesh is built (SetRefineFlag's else-branch is
+// commented out, Userfunction_cy_naca15.cpp:515-531), so its regrids never
+// change the mesh.  IB_REGRID_EVERY=n regrids every n steps with both
+// requested on every level (that branch), the plain criterion deciding.
+// IB_TAG_SERVER=<dir> lets another process decide instead: for each level
+// the case writes <dir>/req_<ts>_<level>.bin (7 doubles per normal box:
+// level, ix, iy, centre x, centre y, signdis, plain decision 0 keep /
+// 1 refine / 2 coarsen), waits for <dir>/resp_<ts>_<level>.bin (one int32
+// decision per box) and applies it.  Decisions the reference's regrid
+// rejects with an abort keep the box instead: refinement of a son of the
+// coarse level's restriction ghosts (AMRLevel::CheckRefineTagLocation,
+// AMRLevel.cpp:989-1067, abort 1009) and coarsening next to the level's own
+// restriction pairs (AMR::CheckDetagLocation, AMR.H:715-925, abort 772).
+// One ORACLE_REGRID line per level reports boxes, applied decisions
+// differing from the plain ones and decisions replaced by keep.
 #include <cmath>
+#include <cstdlib>
+#include <unistd.h>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -96,8 +116,10 @@ static void write_surface(const string &path, int n, double sign) {
   fclose(f);
 }
 
+static const int kRegridEvery = case_env_int("IB_REGRID_EVERY", 0);
+
 void AMR::ADPRule(vector<Body> &) {
-  adpflag = false;
+  adpflag = kRegridEvery > 0 && ts > 0 && ts % kRegridEvery == 0;
   for (int i = 0; i < max_mesh_level; ++i) {
     m_level[i].torefine = false;
     m_level[i].toderefine = false;
@@ -108,8 +130,48 @@ void AMR::SetRefineFlag() {
   if (ts == 0) {
     m_level.back().torefine = true;
     init_adjust_level = 0;
+  } else if (kRegridEvery > 0) {
+    init_adjust_level = 0;
+    for (int i = 0; i < m_mesh.MyCurNum(); ++i) {
+      m_level[i].torefine = true;
+      m_level[i].toderefine = i >= 1;
+    }
   }
 }
+
+// Decisions of another process for the normal boxes of a level
+// (IB_TAG_SERVER); false when no server is configured.
+static bool served_decisions(int ilevel, const vector<int> &plain,
+                             const vector<vector<double>> &rows, vector<int> &out) {
+  static const char *dir = getenv("IB_TAG_SERVER");
+  if (!dir || !*dir) return false;
+  char req[512], tmp[520], resp[512];
+  snprintf(req, sizeof req, "%s/req_%d_%d.bin", dir, ts, ilevel);
+  snprintf(tmp, sizeof tmp, "%s.part", req);
+  snprintf(resp, sizeof resp, "%s/resp_%d_%d.bin", dir, ts, ilevel);
+  FILE *f = fopen(tmp, "wb");
+  if (!f) MPI_Abort(MPI_COMM_WORLD, 3301);
+  for (size_t r = 0; r < rows.size(); ++r) {
+    double row[7] = {rows[r][0], rows[r][1], rows[r][2], rows[r][3], rows[r][4], rows[r][5],
+                     (double)plain[r]};
+    fwrite(row, sizeof(double), 7, f);
+  }
+  fclose(f);
+  rename(tmp, req);  // appears complete
+  out.assign(rows.size(), 0);
+  for (int waited = 0;; ++waited) {  // 10 ms polls, at most 10 minutes
+    FILE *g = fopen(resp, "rb");
+    if (g) {
+      size_t got = fread(out.data(), sizeof(int), out.size(), g);
+      fclose(g);
+      if (got != out.size()) MPI_Abort(MPI_COMM_WORLD, 3302);
+      return true;
+    }
+    if (waited > 60000) MPI_Abort(MPI_COMM_WORLD, 3303);
+    usleep(10000);
+  }
+}
+
 
 // Plain geometric criterion in the reference's style
 // (Userfunction_cy_naca15.cpp:533-650): boxes around the airfoil on the
@@ -159,6 +221,85 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
         m_level[ilevel].m_tag[i].givedetag();
     }
   }
+  if (ts > 0 && kRegridEvery > 0) {
+    AMRLevel &lv = m_level[ilevel];
+    vector<int> plain, dec;
+    vector<vector<double>> rows;
+    for (int i = bs; i < be; ++i) {
+      const Box &b = lv.m_box[i];
+      plain.push_back(lv.m_tag[i].istag() ? 1 : (lv.m_tag[i].isdetag() ? 2 : 0));
+      rows.push_back({(double)ilevel, (double)b.ix(), (double)b.iy(), m_mesh.bc(ilevel, i)[0],
+                      m_mesh.bc(ilevel, i)[1], b.pair.signdis});
+    }
+    if (served_decisions(ilevel, plain, rows, dec)) {
+      // Boxes of a level whose refinement (no_refine) or coarsening (no_coarsen)
+      // the reference's regrid rejects: the sons of the coarse level's restriction
+      // ghosts (the boxes CheckRefineTagLocation checks), and the neighbourhood of
+      // the level's own restriction pairs that CheckDetagLocation's 2-D branch
+      // walks (a 2x2 block of neighbours on the pair's side of its parity and
+      // their 2x2 blocks, and the box 4 steps away along each in-plane direction,
+      // 2 along z).
+      auto inadmissible = [&](AMRLevel &lv, vector<char> &no_refine, vector<char> &no_coarsen) {
+        const int n = lv.m_box.realsize();
+        no_refine.assign(n, 0);
+        no_coarsen.assign(n, 0);
+        if (lv.coarselevel)
+          for (int ig = 0; ig < ighost; ++ig)
+            for (int i = lv.coarselevel->f_res_ghost[ig].ps(); i < lv.coarselevel->f_res_ghost[ig].pe(); ++i)
+              for (Point_iterator_2d p(0, 2); p.end(); ++p) {
+                const int fi0 = lv.coarselevel->f_res_ghost[ig][i].fi.son[p.i][p.j][p.k];
+                if (fi0 >= 0 && fi0 < n) no_refine[fi0] = 1;
+              }
+        const int dp[6][3] = {{0, 1, 1}, {2, 1, 1}, {1, 0, 1},
+                              {1, 2, 1}, {1, 1, 0}, {1, 1, 2}};
+        const int steps[6] = {4, 4, 4, 4, 2, 2};
+        for (int i = lv.f_res_ghost[0].ps(); i < lv.f_res_ghost[0].pe(); ++i) {
+          const int ci0 = lv.f_res_ghost[0][i].ci;
+          const int ix0 = lv.m_box[ci0].ix() & 1, iy0 = lv.m_box[ci0].iy() & 1;
+          for (int nx = 1 - ix0; nx < 3 - ix0; ++nx)
+            for (int ny = 1 - iy0; ny < 3 - iy0; ++ny) {
+              const int anb = lv.m_box[ci0].neib[nx][ny][1];
+              if (anb < 0) continue;
+              const int ax = lv.m_box[anb].ix() & 1, ay = lv.m_box[anb].iy() & 1;
+              for (Point_iterator_2d p(0, 2); p.end(); ++p)
+                for (int nz = 0; nz < 3; ++nz) {
+                  const int anb2 = lv.m_box[anb].neib[ax + p.i][ay + p.j][nz];
+                  if (anb2 >= 0 && anb2 < n) no_coarsen[anb2] = 1;
+                }
+            }
+          for (int di = 0; di < 6; ++di) {
+            int an1 = ci0;
+            for (int k = 0; k < steps[di] && an1 > -1; ++k) an1 = lv.m_box[an1].neib[dp[di][0]][dp[di][1]][dp[di][2]];
+            if (an1 >= 0 && an1 < n) no_coarsen[an1] = 1;
+          }
+        }
+      };
+      vector<char> no_refine, no_coarsen;
+      inadmissible(lv, no_refine, no_coarsen);
+      int differ = 0, fallback = 0;
+      lv.taggedbox.clear();
+      for (int i = bs; i < be; ++i) {
+        int d = dec[i - bs];
+        // an inadmissible decision keeps the box (the plain decision itself
+        // can be inadmissible on a mesh that earlier served regrids shaped)
+        if ((d == 1 && (!refine || no_refine[i])) || (d == 2 && (!coarsen || no_coarsen[i])) ||
+            d < 0 || d > 2) {
+          ++fallback;
+          d = 0;
+        }
+        if (d != plain[i - bs]) ++differ;
+        lv.m_tag[i].tag = -1;
+        lv.m_tag[i].detag = -1;
+        if (d == 1) {
+          lv.m_tag[i].givetag();
+          lv.taggedbox.push_back(i);
+        } else if (d == 2) {
+          lv.m_tag[i].givedetag();
+        }
+      }
+      printf("ORACLE_REGRID %d %d %d %d %d\n", ts, ilevel, be - bs, differ, fallback);
+    }
+  }
   if (g_oracle_tag_dump) {
     for (int i = bs; i < be; ++i) {
       const Box &b = m_level[ilevel].m_box[i];
@@ -172,10 +313,10 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
   }
   MPI_Barrier(share_comm);
   CheckDetagLocation(ilevel);
-  // the attach-box consistency check belongs to mesh generation; the tag
-  // dump's pass 1 re-judges a finished mesh, whose attach boxes live one
-  // level up
-  if (!(g_oracle_tag_dump && g_oracle_tag_pass == 1) && refine && morelevel &&
+  // the attach-box consistency check belongs to mesh generation (ts == 0);
+  // the tag dump's pass 1 and runtime regrids re-judge a finished mesh,
+  // whose attach boxes live one level up
+  if (ts == 0 && !(g_oracle_tag_dump && g_oracle_tag_pass == 1) && refine && morelevel &&
       ilevel == m_mesh.MyCurNum() - 2) {
     int l0 = m_mesh.MyCurNum() - 2;
     for (size_t i = 0; i < abody.size(); ++i) abody[i].CheckAttachBoxTag(m_level[l0].m_tag, l0, m_mesh);

@@ -15,6 +15,8 @@
 //     (the only one that instantiates NS_Solver::ComputeFaceFlux).
 //
 // Environment: IB_STEPS (default 5), IB_STAGES (3 or 4, default 4),
+// IB_TAG_SERVER=<dir> (runtime regrids of the case file: write the state the
+// tag server decides from to <dir>/state_<ts>.bin before each regrid),
 // IB_DUMP=<prefix> (write <prefix>_<step>.bin for the initial state and after
 // each step listed by IB_DUMP_EVERY, default every step), IB_FORCES=1 (static
 // body: compute wall forces each step, Body::ComptWallForce), IB_FORCE_LOG=<file>
@@ -442,7 +444,16 @@ int main(int argc, char **argv) {
       if (!forces.empty()) std::fwrite(forces.data(), sizeof(double), forces.size(), flog);
     }
     amr.ADPRule(sphere);
-    if (adpflag) amr.PerformAdaptive(sphere);
+    if (adpflag) {
+      // a tag server decides from the state it sees here (case file)
+      const char *server = std::getenv("IB_TAG_SERVER");
+      if (server && *server) {
+        const std::string path = std::string(server) + "/state_" + std::to_string(ts) + ".bin";
+        dump_state(path + ".part", mesh, flowsolver, forces);
+        std::rename((path + ".part").c_str(), path.c_str());
+      }
+      amr.PerformAdaptive(sphere);
+    }
     adpflag = false;
     if (prefix && (ts % every == 0 || s == nsteps - 1)) do_dump(ts);
   }
