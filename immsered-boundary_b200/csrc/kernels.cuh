@@ -590,6 +590,15 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   const int nbs = __ldg(nbrow + 1), nbw = __ldg(nbrow + 3), nbe = __ldg(nbrow + 5),
             nbn = __ldg(nbrow + 7);
 
+  {
+    // U^n of the tile's own cells, which the update phase reads after the
+    // faces, into L1 now (FP64 step 0.798 -> 0.779 ms)
+    if (tid < 64) {
+      const int fld = tid >> 4;
+      const double *un = a.s0[fld == 0 ? F_RHO : (fld == 1 ? F_U : (fld == 2 ? F_V : F_E))];
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(un + (int64_t)tile * kTileCells + (tid & 15) * 16));
+    }
+  }
   if (prefetch > 0) {
     // the CTA that starts when this one ends reads this tile's input from L2
     constexpr int kLines = kTileCells * (int)sizeof(TI) / 128;  // 128-byte lines per field
