@@ -472,90 +472,6 @@ __device__ __forceinline__ void fast_slope(const typename SRec<R>::V *sq, const 
 // Faces whose outer stencil cell is missing use the reference's one-sided
 // reconstruction (NS_Solver.H:743-750).  The residual, update and primitive
 // recovery run in FP64 in every mode.
-// The 768 16-byte pieces of a uniform tile's stencil region: the tile's 4
-// fields (w < 512), the west/east 2-column strips (w < 640) and the
-// south/north 2-row strips; piece w is two adjacent cells of field f whose
-// first cell lands on region record dst.
-__device__ __forceinline__ void uniform_piece_dst(int w, int &f, int &dst) {
-  if (w < 512) {
-    f = w >> 7;
-    const int p = w & 127;
-    dst = ((p >> 3) + kHalo) * kReg + (p & 7) * 2 + kHalo;
-  } else if (w < 640) {
-    const int v = w - 512;
-    f = v >> 5;
-    dst = ((v & 15) + kHalo) * kReg + (((v >> 4) & 1) ? kTile + kHalo : 0);
-  } else {
-    const int v = w - 640;
-    f = v >> 5;
-    const int north = (v >> 4) & 1, rr = (v >> 3) & 1;
-    dst = (north ? kTile + kHalo + rr : rr) * kReg + (v & 7) * 2 + kHalo;
-  }
-}
-
-// Global address of piece w of tile `tile` (side neighbours west, east,
-// south, north already loaded), FP64 stage input.
-__device__ __forceinline__ const double2 *uniform_src(const StageVar &v, int tile, int nbw, int nbe,
-                                                      int nbs, int nbn, int w) {
-  int f, dst;
-  uniform_piece_dst(w, f, dst);
-  const double *in = static_cast<const double *>(v.sin[f]);
-  if (w < 512) {
-    const int p = w & 127;
-    return reinterpret_cast<const double2 *>(in + (int64_t)tile * kTileCells + (p >> 3) * kTile +
-                                             (p & 7) * 2);
-  }
-  if (w < 640) {
-    const int q = w - 512;
-    const int east = (q >> 4) & 1, row = q & 15;
-    return reinterpret_cast<const double2 *>(in + (int64_t)(east ? nbe : nbw) * kTileCells +
-                                             row * kTile + (east ? 0 : kTile - 2));
-  }
-  const int q = w - 640;
-  const int north = (q >> 4) & 1, rr = (q >> 3) & 1;
-  const int srow = north ? rr : kTile - 2 + rr;
-  return reinterpret_cast<const double2 *>(in + (int64_t)(north ? nbn : nbs) * kTileCells +
-                                           srow * kTile + (q & 7) * 2);
-}
-
-// FP32 stage input of a uniform tile: 448 16-byte pieces of four adjacent
-// cells of one field row: the tile (w < 256), the west/east neighbours'
-// last/first four columns (w < 384; the strip keeps two of them) and the
-// south/north neighbours' two rows (w < 448).  Piece w of field f lands on
-// region records dst + c for its cells c in [c0, c0 + n).
-__device__ __forceinline__ const float4 *uniform_src32(const StageVar &v, int tile, int nbw, int nbe,
-                                                       int nbs, int nbn, int w, int &f, int &dst,
-                                                       int &c0) {
-  c0 = 0;
-  if (w < 256) {
-    f = w >> 6;
-    const int p = w & 63, row = p >> 2, col = (p & 3) * 4;
-    dst = (row + kHalo) * kReg + col + kHalo;
-    return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
-                                            (int64_t)tile * kTileCells + row * kTile + col);
-  }
-  if (w < 384) {
-    const int q = w - 256;
-    f = q >> 5;
-    const int east = (q >> 4) & 1, row = q & 15;
-    // east strip = neighbour columns 0, 1 (cells 0, 1 of the piece) at region
-    // columns 18, 19; west strip = neighbour columns 14, 15 (cells 2, 3) at 0, 1
-    c0 = east ? 0 : 2;
-    dst = (row + kHalo) * kReg + (east ? kTile + kHalo : 0) - c0;
-    return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
-                                            (int64_t)(east ? nbe : nbw) * kTileCells + row * kTile +
-                                            (east ? 0 : kTile - 4));
-  }
-  const int q = w - 384;
-  f = q >> 4;
-  const int north = (q >> 3) & 1, rr = (q >> 2) & 1, col = (q & 3) * 4;
-  const int srow = north ? rr : kTile - 2 + rr;
-  dst = (north ? kTile + kHalo + rr : rr) * kReg + col + kHalo;
-  return reinterpret_cast<const float4 *>(static_cast<const float *>(v.sin[f]) +
-                                          (int64_t)(north ? nbn : nbs) * kTileCells + srow * kTile +
-                                          col);
-}
-
 template <typename R, int LIM, bool VISC, bool FINAL, typename TI>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageVar &v,
                                                 const CaseConst &cc,
@@ -608,50 +524,35 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
                                                     (tid % kLines) * (128 / (int)sizeof(TI))));
   }
 
-  if (uni && sizeof(TI) == 4) {
-    // FP32 input: 448 16-byte pieces, every load issued before the first
-    // shared-memory store
-    constexpr int NIT = (448 + NT - 1) / NT;
-    float4 val[NIT];
+  if (uni) {
+    // one region record per thread and pass: its four fields loaded (all
+    // loads of both passes issued before the first store), then one record
+    // store (no shared-memory bank conflicts); corners stay unset (a
+    // uniform tile's stencils never read them)
+    constexpr int NIT = (kReg * kReg + NT - 1) / NT;
+    const TI *in0 = static_cast<const TI *>(v.sin[0]), *in1 = static_cast<const TI *>(v.sin[1]),
+             *in2 = static_cast<const TI *>(v.sin[2]), *in3 = static_cast<const TI *>(v.sin[3]);
+    R q[NIT][4];
+    bool has[NIT];
 #pragma unroll
     for (int it = 0; it < NIT; ++it) {
-      const int w = tid + it * NT;
-      int f, dst, c0;
-      if (w < 448) val[it] = __ldg(uniform_src32(v, tile, nbw, nbe, nbs, nbn, w, f, dst, c0));
-    }
-#pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int w = tid + it * NT;
-      if (w < 448) {
-        int f, dst, c0;
-        uniform_src32(v, tile, nbw, nbe, nbs, nbn, w, f, dst, c0);
-        const float c[4] = {val[it].x, val[it].y, val[it].z, val[it].w};
-        const bool strip = w >= 256 && w < 384;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (!strip || (i >= c0 && i < c0 + 2)) *S::comp(sq, dst + i, NQ, f) = (R)c[i];
+      const int r = tid + it * NT;
+      const int rx = r % kReg - kHalo, ry = r / kReg - kHalo;
+      const int ox = rx < 0 ? -1 : (rx >= kTile ? 1 : 0);
+      const int oy = ry < 0 ? -1 : (ry >= kTile ? 1 : 0);
+      has[it] = r < kReg * kReg && !(ox && oy);
+      if (has[it]) {
+        const int nb = ox < 0 ? nbw : (ox > 0 ? nbe : (oy < 0 ? nbs : (oy > 0 ? nbn : tile)));
+        const int64_t sl = (int64_t)nb * kTileCells + (ry - oy * kTile) * kTile + (rx - ox * kTile);
+        q[it][0] = (R)__ldg(in0 + sl);
+        q[it][1] = (R)__ldg(in1 + sl);
+        q[it][2] = (R)__ldg(in2 + sl);
+        q[it][3] = (R)__ldg(in3 + sl);
       }
     }
-  } else if (uni) {
-    // 768 16-byte pieces straight from global memory: every load issued
-    // before the first shared-memory store
-    constexpr int NIT = (768 + NT - 1) / NT;
-    double2 val[NIT];
 #pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int w = tid + it * NT;
-      if (w < 768) val[it] = __ldg(uniform_src(v, tile, nbw, nbe, nbs, nbn, w));
-    }
-#pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int w = tid + it * NT;
-      if (w < 768) {
-        int f, dst;
-        uniform_piece_dst(w, f, dst);
-        *S::comp(sq, dst, NQ, f) = (R)val[it].x;
-        *S::comp(sq, dst + 1, NQ, f) = (R)val[it].y;
-      }
-    }
+    for (int it = 0; it < NIT; ++it)
+      if (has[it]) S::st(sq, tid + it * NT, NQ, q[it][0], q[it][1], q[it][2], q[it][3]);
   } else {
     // region records: slot, then presence flags, then the state, each
     // step's loads of both records issued together
