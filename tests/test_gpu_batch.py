@@ -88,7 +88,7 @@ def test_batch_beyond_constant_table_reads_global_arguments(cuda_lib, precision)
         ref.append((s.dt, s.download()))
         s.close()
     sols = [make_solver(c) for c in cases]
-    big = ib.Batch(sols[:88])  # about 736 bytes of table per case
+    big = ib.Batch(sols[:88])  # about 752 bytes of table per case
     small = ib.Batch(sols[88:])
     assert big.info()["table_bytes"] == 0
     assert small.info()["table_bytes"] > 0
