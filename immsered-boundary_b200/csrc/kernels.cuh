@@ -30,13 +30,22 @@ __device__ __forceinline__ void raise_error(DevDiag *d, int phase, int check, in
   atomicMin(&d->err_key, key);
 }
 
+// Exact maximum / minimum of a 64-bit word over the full warp with the
+// 32-bit warp reductions (redux.sync): the extreme high word first, then the
+// extreme low word among the lanes that hold it.  Four instructions instead
+// of five rounds of two 32-bit shuffles and a 64-bit compare.
 __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-    v = w > v ? w : v;
-  }
-  return v;
+  const unsigned hi = (unsigned)(v >> 32), lo = (unsigned)v;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+  return ((unsigned long long)mh << 32) | ml;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  const unsigned hi = (unsigned)(v >> 32), lo = (unsigned)v;
+  const unsigned mh = __reduce_min_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_min_sync(0xffffffffu, hi == mh ? lo : 0xffffffffu);
+  return ((unsigned long long)mh << 32) | ml;
 }
 
 // Threads of a fast-build stage CTA: FP64 adds a ninth warp that owns the
@@ -54,10 +63,11 @@ struct StageThreads {
 };
 
 // Residual max-norm of a block of up to 9 warps into the step's diag: warp and
-// block maxima, then one atomicMax per component and block, skipped when the
-// global value is already as large (the maximum settles after the first
-// blocks, so later blocks only read it instead of serialising on four
-// addresses).  Components map to res_max[0,1,2,4] (no z momentum in 2-D).
+// block maxima, then one atomicMax per component and block whose result
+// nobody reads, so it retires as a fire-and-forget reduction (reading the
+// global value first to skip it put a memory round trip on the tail of
+// every CTA: 29 us per FP64 2048^2 final stage).  Components map to
+// res_max[0,1,2,4] (no z momentum in 2-D).
 // Every thread of the block must call it; sred is shared scratch of 32
 // words that no thread reads or writes any more.
 template <int NT = kTileCells>
@@ -76,7 +86,7 @@ __device__ __forceinline__ void block_resnorm(const unsigned long long (&rb)[4],
 #pragma unroll
     for (int w = 0; w < kW; ++w) m = sred[tid * kW + w] > m ? sred[tid * kW + w] : m;
     unsigned long long *dst = &d->res_bits[tid == 3 ? 4 : tid];
-    if (m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
+    atomicMax(dst, m);  // result unused: a reduction the CTA does not wait for
   }
 }
 
@@ -93,21 +103,18 @@ __device__ __forceinline__ double cfl_cell_bound(double T, double u, double v, c
 }
 
 // Block minimum of one positive double per thread (as bits) into *dst, one
-// guarded atomic per block; every thread of the block calls it; sred is
-// shared scratch of NT/32 words nobody else uses meanwhile.
+// atomic per block (result unused: not waited for); every thread of the
+// block calls it; sred is shared scratch of NT/32 words nobody else uses
+// meanwhile.
 template <int NT>
 __device__ __forceinline__ void block_min_bits(unsigned long long b, unsigned long long *dst,
                                                unsigned long long *sred) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
-    b = w < b ? w : b;
-  }
+  b = warp_min_u64(b);
   if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int k = 1; k < NT / 32; ++k) b = sred[k] < b ? sred[k] : b;
-    if (b < *(volatile unsigned long long *)dst) atomicMin(dst, b);
+    atomicMin(dst, b);  // result unused: a reduction the CTA does not wait for
   }
 }
 
@@ -858,8 +865,8 @@ __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6
 }
 
 // CFL time step over the normal cells of every level, NS_Solver::Comptdt
-// (NS_Solver.cpp:196-280): a per-cell bound, a warp-shuffle min and one
-// atomic per warp (positive doubles order like their bit patterns).
+// (NS_Solver.cpp:196-280): a per-cell bound, a warp-shuffle and block min and
+// one atomic per block (positive doubles order like their bit patterns).
 __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
   double best = 10000.0;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < a.nslots;
@@ -870,20 +877,14 @@ __global__ void __launch_bounds__(256) cfl_kernel(CflArgs a, CaseConst cc) {
     if (d0 < 0.0) raise_error(a.diag, a.phase, ERR_CFL_NEG_DT, (int)s);
     best = (d0 < best) ? d0 : best;  // std::min(CFL_dt, CFL_dt0) ignores NaN
   }
-  unsigned long long b = (unsigned long long)__double_as_longlong(best);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
-    b = w < b ? w : b;
-  }
-  // block minimum, then one atomic per block, skipped when the global value
-  // is already as small
+  unsigned long long b = warp_min_u64((unsigned long long)__double_as_longlong(best));
+  // block minimum, then one atomic per block (result unused: not waited for)
   __shared__ unsigned long long sred[8];
   if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = sred[w] < b ? sred[w] : b;
-    if (b < *(volatile unsigned long long *)&a.diag->cfl_bits) atomicMin(&a.diag->cfl_bits, b);
+    atomicMin(&a.diag->cfl_bits, b);
   }
 }
 
@@ -1113,7 +1114,7 @@ cudaError_t batch_table_write(int offset, const void *src, int bytes) {
 
 // CFL pass of every batched case in one launch: one CTA per (case, tile)
 // item of all tiles, the same per-cell bound as cfl_kernel, block minimum and
-// one guarded atomic into the case's diag.
+// one atomic (not waited for) into the case's diag.
 __global__ void __launch_bounds__(kTileCells)
     cfl_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                      const int2 *__restrict__ work, int nwork, int nstages,
@@ -1132,17 +1133,12 @@ __global__ void __launch_bounds__(kTileCells)
       if (d0 < 0.0) raise_error(a.diag, pb + 1, ERR_CFL_NEG_DT, (int)s);
       best = (d0 < best) ? d0 : best;
     }
-    unsigned long long b = (unsigned long long)__double_as_longlong(best);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      unsigned long long v = __shfl_xor_sync(0xffffffffu, b, o);
-      b = v < b ? v : b;
-    }
+    unsigned long long b = warp_min_u64((unsigned long long)__double_as_longlong(best));
     if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = b;
     __syncthreads();
     if (threadIdx.x == 0) {
       for (int k = 1; k < kTileCells / 32; ++k) b = sred[k] < b ? sred[k] : b;
-      if (b < *(volatile unsigned long long *)&a.diag->cfl_bits) atomicMin(&a.diag->cfl_bits, b);
+      atomicMin(&a.diag->cfl_bits, b);
     }
     __syncthreads();
   }
