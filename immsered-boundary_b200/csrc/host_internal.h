@@ -36,7 +36,6 @@ int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy);
 int tag_mesh_enqueue(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
                      cudaStream_t st, uint8_t **rows_out);
 int tag_mesh_prepare(bool learned);
-int tag_mesh_error(ibgpu_ctx *ctx, cudaStream_t st);
 
 int validate_case(const ibgpu_case *cs);
 void fill_case_const(const ibgpu_case *cs, CaseConst &k);

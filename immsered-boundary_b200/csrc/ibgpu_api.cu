@@ -1006,6 +1006,7 @@ struct ibgpu_batch {
   int table = -1;       // byte offset of the arguments in the constant-memory table (-1: global)
   int table_bytes = 0;  // bytes reserved there
   bool tuned = false;
+  int *h_err = nullptr;  // pinned: the cases' time-out flags (batch tagging)
   int fixed_grid = -1;  // >= 0: CTA count set by the caller (no autotuning)
   bool timing = false;
   double stage_ms = 0.0;
@@ -1030,6 +1031,8 @@ struct ibgpu_batch {
     fast::batch_table_release(device, table);
     table = -1;
     table_bytes = 0;
+    if (h_err) cudaFreeHost(h_err);
+    h_err = nullptr;
   }
 };
 
@@ -1365,17 +1368,41 @@ int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float
   cudaStream_t st = b->stream;
   int rc = tag_mesh_prepare(d_params != nullptr);
   if (rc) return rc;
+  // every case's kernels first, then the copies back (a copy between two
+  // cases' kernels would hold the second one back), then all time-out flags
+  // in one synchronisation
+  const size_t n = b->cases.size();
+  std::vector<uint8_t *> rows(n, nullptr);
+  for (size_t i = 0; i < n; ++i)
+    if (b->cases[i]->ncells > 0 &&
+        (rc = tag_mesh_enqueue(b->cases[i], rule, d_params, st, &rows[i])))
+      return rc;
   int64_t off = 0;
-  for (auto *c : b->cases) {
+  for (size_t i = 0; i < n; ++i) {
+    const ibgpu_ctx *c = b->cases[i];
     if (c->ncells == 0) continue;
-    uint8_t *rows = nullptr;
-    if ((rc = tag_mesh_enqueue(c, rule, d_params, st, &rows))) return rc;
-    CK(cudaMemcpyAsync(tags + off, rows, (size_t)c->ncells, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(tags + off, rows[i], (size_t)c->ncells, cudaMemcpyDeviceToHost, st));
     off += c->ncells;
   }
-  for (auto *c : b->cases)
-    if (d_params && (rc = tag_mesh_error(c, st))) return rc;
+  if (d_params) {
+    if (!b->h_err) CK(cudaHostAlloc((void **)&b->h_err, n * sizeof(int), cudaHostAllocDefault));
+    for (size_t i = 0; i < n; ++i)
+      CK(cudaMemcpyAsync(b->h_err + i, b->cases[i]->d_aux_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
   CK(cudaStreamSynchronize(st));
+  if (d_params) {
+    bool timed_out = false;
+    for (size_t i = 0; i < n; ++i)
+      if (b->h_err[i]) {
+        timed_out = true;
+        CK(cudaMemsetAsync(b->cases[i]->d_aux_err, 0, sizeof(int), st));
+      }
+    if (timed_out) {
+      CK(cudaStreamSynchronize(st));
+      g_last_error = "tensor-core wait ran out of its time limit";
+      return IBGPU_E_TIMEOUT;
+    }
+  }
   return IBGPU_OK;
 }
 

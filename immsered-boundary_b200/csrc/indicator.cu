@@ -1115,11 +1115,6 @@ int tag_mesh_enqueue(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_
 
 int tag_mesh_prepare(bool learned) { return learned ? configure_smem() : IBGPU_OK; }
 
-int tag_mesh_error(ibgpu_ctx *ctx, cudaStream_t st) {
-  CtxView V;
-  if (ctx_view(ctx, &V) != IBGPU_OK) return IBGPU_E_ARG;
-  return kernel_error_check(V.aux_err, st);
-}
 }  // namespace ibgpu
 
 extern "C" {
