@@ -1007,6 +1007,7 @@ struct ibgpu_batch {
   int table_bytes = 0;  // bytes reserved there
   bool tuned = false;
   int *h_err = nullptr;  // pinned: the cases' time-out flags (batch tagging)
+  std::vector<cudaEvent_t> ev_tag;  // batch tagging: per case, + the fork
   int fixed_grid = -1;  // >= 0: CTA count set by the caller (no autotuning)
   bool timing = false;
   double stage_ms = 0.0;
@@ -1033,6 +1034,8 @@ struct ibgpu_batch {
     table_bytes = 0;
     if (h_err) cudaFreeHost(h_err);
     h_err = nullptr;
+    for (auto e : ev_tag) cudaEventDestroy(e);
+    ev_tag.clear();
   }
 };
 
@@ -1368,20 +1371,29 @@ int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float
   cudaStream_t st = b->stream;
   int rc = tag_mesh_prepare(d_params != nullptr);
   if (rc) return rc;
-  // every case's kernels first, then the copies back (a copy between two
-  // cases' kernels would hold the second one back), then all time-out flags
-  // in one synchronisation
+  // each case tags on its own stream after the batch's pending work (the
+  // cases' kernels overlap, so one case's last partial wave does not idle the
+  // GPU), its rows copied back behind its kernels; the batch stream then
+  // waits for all of them and reads every time-out flag in one
+  // synchronisation
   const size_t n = b->cases.size();
-  std::vector<uint8_t *> rows(n, nullptr);
-  for (size_t i = 0; i < n; ++i)
-    if (b->cases[i]->ncells > 0 &&
-        (rc = tag_mesh_enqueue(b->cases[i], rule, d_params, st, &rows[i])))
-      return rc;
+  if (b->ev_tag.size() != n + 1) {
+    for (auto e : b->ev_tag) cudaEventDestroy(e);
+    b->ev_tag.assign(n + 1, nullptr);
+    for (auto &e : b->ev_tag) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  CK(cudaEventRecord(b->ev_tag[n], st));
   int64_t off = 0;
   for (size_t i = 0; i < n; ++i) {
-    const ibgpu_ctx *c = b->cases[i];
+    ibgpu_ctx *c = b->cases[i];
     if (c->ncells == 0) continue;
-    CK(cudaMemcpyAsync(tags + off, rows[i], (size_t)c->ncells, cudaMemcpyDeviceToHost, st));
+    cudaStream_t cst = c->stream;
+    CK(cudaStreamWaitEvent(cst, b->ev_tag[n], 0));
+    uint8_t *rows = nullptr;
+    if ((rc = tag_mesh_enqueue(c, rule, d_params, cst, &rows))) return rc;
+    CK(cudaMemcpyAsync(tags + off, rows, (size_t)c->ncells, cudaMemcpyDeviceToHost, cst));
+    CK(cudaEventRecord(b->ev_tag[i], cst));
+    CK(cudaStreamWaitEvent(st, b->ev_tag[i], 0));
     off += c->ncells;
   }
   if (d_params) {
