@@ -427,9 +427,11 @@ int ibgpu_upload_signdis(ibgpu_ctx *ctx, const double *signdis);
 int ibgpu_tag_mesh(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,
                    uint8_t *tags);
 
-/* ibgpu_tag_mesh of every case of a batch, enqueued back to back with one
- * synchronisation: tags holds the cases' row tags one after another (case
- * order, each case's cell-list order). */
+/* ibgpu_tag_mesh of every case of a batch with one synchronisation: each
+ * case tags on its own context stream (ordered after the batch stream's
+ * pending work; the cases' kernels overlap) and the batch stream waits for
+ * all of them; tags holds the cases' row tags one after another (case
+ * order, each case's cell-list order).  Use pinned host memory for tags. */
 int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float *d_params,
                          uint8_t *tags);
 
