@@ -75,6 +75,12 @@ struct ibgpu_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // asynchronous state downloads
   cudaEvent_t ev_ready = nullptr, ev_copied = nullptr;
+  cudaStream_t in_stream = nullptr;  // asynchronous state uploads
+  cudaEvent_t ev_in_free = nullptr, ev_in_done = nullptr;
+  bool in_used = false;     // ev_in_free marks the last upload's scatter
+  bool chain_open = false;  // asynchronous steps since the last ibgpu_step_result
+  int chain_steps = 0;
+  int64_t chain_marched = 0;
   bool download_pending = false;       // an asynchronous download may still read s0
   double *d_rows_out = nullptr;        // staging of asynchronous downloads
   cudaStream_t stream = nullptr;
@@ -334,6 +340,9 @@ int ibgpu_create(const ibgpu_case *cs, ibgpu_ctx **out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->in_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_in_free, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_in_done, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_diag, sizeof(DevDiag));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_diag, sizeof(DevDiag));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_aux_err, sizeof(int));
@@ -364,7 +373,11 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   const int64_t n = cells->n;
   CK(cudaStreamSynchronize(ctx->stream));
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // pending downloads
+  if (ctx->in_stream) cudaStreamSynchronize(ctx->in_stream);      // pending uploads
   ctx->download_pending = false;
+  ctx->in_used = false;
+  ctx->chain_open = false;  // a new mesh ends any chain of asynchronous steps
+  ctx->chain_steps = 0;
   ctx->free_layout();
 
   // 1. owners vs aliases; tiles per level
@@ -647,6 +660,7 @@ int ibgpu_download_state_async(ibgpu_ctx *ctx, double *prim) {
 int ibgpu_synchronize(ibgpu_ctx *ctx) {
   if (!ctx) return IBGPU_E_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->in_stream));
   CK(cudaStreamSynchronize(ctx->copy_stream));
   ctx->download_pending = false;
   return IBGPU_OK;
@@ -680,8 +694,9 @@ struct RunTimer {
   cudaStream_t st;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
   std::vector<int> kind;
+  bool off = false;  // asynchronous steps are not timed
   cudaEvent_t mark(int k) {
-    if (!ctx->timing) return nullptr;
+    if (off || !ctx->timing) return nullptr;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -734,7 +749,7 @@ bool folds_cfl(const ibgpu_ctx *ctx) {
 // prolongation on their schedules, immersed-body ghosts, CFL dt, domain
 // ghosts and the viscous flux of the levels that march.
 int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer &tm,
-                     bool batched = false) {
+                     bool batched = false, bool fresh_cfl = false) {
   const ibgpu_case &cs = ctx->cs;
   const bool exact = cs.precision == IBGPU_FP64_EXACT;
   const bool mixed = cs.precision == IBGPU_MIXED;
@@ -791,7 +806,7 @@ int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer
   // CFL time step (TimeMarching: Comptdt when ts % dt_var_step == 0); from
   // the second step of a run that folds it into the final stage, the
   // previous step already accumulated the bound
-  if (!batched && (ts % cs.dt_var_step) == 0 && step > 0 && folds_cfl(ctx)) {
+  if (!batched && (ts % cs.dt_var_step) == 0 && step > 0 && !fresh_cfl && folds_cfl(ctx)) {
     cudaEvent_t e = tm.mark(2);
     if (exact) exact::launch_take_folded_cfl(ctx->d_diag, ctx->cc, st);
     else fast::launch_take_folded_cfl(ctx->d_diag, ctx->cc, st);
@@ -936,13 +951,45 @@ int decode_diag(ibgpu_ctx *ctx, int64_t marched, double *dt, ibgpu_diag *diag) {
 
 }  // namespace
 
+// asynchronous steps between two ibgpu_step_result calls (abort-order phases
+// 8 * step + p stay below 2^24)
+constexpr int kMaxChainSteps = 1 << 20;
+
+// The stages of step ts (index `step` of its run: abort-order phases) over
+// the tiles of the levels that march at ts; fold_next: the final stage
+// accumulates the next step's CFL bound where the case allows it.
+static int enqueue_stages(ibgpu_ctx *ctx, int ts, int step, bool fold_next, cudaStream_t st,
+                          RunTimer &tm) {
+  const ibgpu_case &cs = ctx->cs;
+  const bool exact = cs.precision == IBGPU_FP64_EXACT;
+  const bool mixed = cs.precision == IBGPU_MIXED;
+  for (int k = 0; k < cs.nstages; ++k) {
+    StageArgs sa;
+    stage_args(ctx, k, sa);
+    sa.phase = 8 * step + 2 + k;
+    const bool fin = (k == cs.nstages - 1);
+    if (fin && fold_next && folds_cfl(ctx)) sa.v.cfl_next = 1 + 8 * (step + 1) + 1;
+    for (int l = 0; l < cs.nlevels; ++l) {
+      if (ts % cs.march_step[l] != cs.march_left[l]) continue;
+      sa.tile_begin = ctx->level_tile_begin[l];
+      cudaEvent_t e = tm.mark(0);
+      if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, k, st);
+      else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, k, st);
+      tm.done(e);
+      CK(cudaGetLastError());
+    }
+  }
+  return IBGPU_OK;
+}
+
 static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
   if (!ctx || !dt || ts0 < 0 || nsteps < 1) return IBGPU_E_ARG;
   if (!ctx->has_state) return IBGPU_E_STATE;
-  const ibgpu_case &cs = ctx->cs;
+  if (ctx->chain_open) {
+    g_last_error = "asynchronous steps pending: call ibgpu_step_result first";
+    return IBGPU_E_STATE;
+  }
   cudaStream_t st = ctx->stream;
-  const bool exact = cs.precision == IBGPU_FP64_EXACT;
-  const bool mixed = cs.precision == IBGPU_MIXED;
   int rc = order_after_download(ctx, st);
   if (rc) return rc;
   if ((rc = begin_diag(ctx, *dt, st))) return rc;
@@ -952,23 +999,7 @@ static int run_steps(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag
     const int ts = ts0 + step;
     if ((rc = enqueue_prestage(ctx, ts, step, st, tm))) return rc;
     marched = marched_cells(ctx, ts);
-    // stages over the tiles of the levels that march at ts
-    for (int k = 0; k < cs.nstages; ++k) {
-      StageArgs sa;
-      stage_args(ctx, k, sa);
-      sa.phase = 8 * step + 2 + k;
-      const bool fin = (k == cs.nstages - 1);
-      if (fin && folds_cfl(ctx) && step + 1 < nsteps) sa.v.cfl_next = 1 + 8 * (step + 1) + 1;
-      for (int l = 0; l < cs.nlevels; ++l) {
-        if (ts % cs.march_step[l] != cs.march_left[l]) continue;
-        sa.tile_begin = ctx->level_tile_begin[l];
-        cudaEvent_t e = tm.mark(0);
-        if (exact) exact::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, false, k, st);
-        else fast::launch_stage(sa, ctx->cc, ctx->level_tile_count[l], cs.limiter, cs.viscous != 0, fin, mixed, k, st);
-        tm.done(e);
-        CK(cudaGetLastError());
-      }
-    }
+    if ((rc = enqueue_stages(ctx, ts, step, step + 1 < nsteps, st, tm))) return rc;
   }
   CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -982,6 +1013,70 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag) {
 
 int ibgpu_run(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag) {
   return run_steps(ctx, ts0, nsteps, dt, diag);
+}
+
+int ibgpu_upload_state_async(ibgpu_ctx *ctx, const double *prim) {
+  if (!ctx || (!prim && ctx->ncells > 0)) return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  if (ctx->ncells > 0) {
+    cudaStream_t st = ctx->stream;
+    // the rows buffer is free once the previous upload's scatter has run
+    if (ctx->in_used) CK(cudaStreamWaitEvent(ctx->in_stream, ctx->ev_in_free, 0));
+    CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * 7 * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->in_stream));
+    CK(cudaEventRecord(ctx->ev_in_done, ctx->in_stream));
+    // the scatter follows the copy and the context's pending work, and
+    // overwrites the state a pending download still reads only after it
+    CK(cudaStreamWaitEvent(st, ctx->ev_in_done, 0));
+    int rc = order_after_download(ctx, st);
+    if (rc) return rc;
+    fast::launch_scatter(ctx->d_rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->d_s0,
+                         ctx->nsm, st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev_in_free, st));
+    ctx->in_used = true;
+  }
+  ctx->has_state = true;
+  return IBGPU_OK;
+}
+
+int ibgpu_step_async(ibgpu_ctx *ctx, int ts, double dt) {
+  if (!ctx || ts < 0) return IBGPU_E_ARG;
+  if (!ctx->has_state) return IBGPU_E_STATE;
+  if (ctx->chain_steps >= kMaxChainSteps) {
+    g_last_error = "too many asynchronous steps: call ibgpu_step_result";
+    return IBGPU_E_ARG;
+  }
+  cudaStream_t st = ctx->stream;
+  int rc = order_after_download(ctx, st);
+  if (rc) return rc;
+  if (!ctx->chain_open) {
+    if (!(dt > 0.0)) return IBGPU_E_ARG;
+    if ((rc = begin_diag(ctx, dt, st))) return rc;
+    ctx->chain_open = true;
+    ctx->chain_steps = 0;
+  }
+  RunTimer tm{ctx, st, {}, {}};
+  tm.off = true;
+  // a fresh CFL pass every step (the state may have been replaced since the
+  // previous one), so no fold into the final stage either
+  const int step = ctx->chain_steps;
+  if ((rc = enqueue_prestage(ctx, ts, step, st, tm, false, true))) return rc;
+  if ((rc = enqueue_stages(ctx, ts, step, false, st, tm))) return rc;
+  ctx->chain_marched = marched_cells(ctx, ts);
+  ctx->chain_steps = step + 1;
+  return IBGPU_OK;
+}
+
+int ibgpu_step_result(ibgpu_ctx *ctx, double *dt, ibgpu_diag *diag) {
+  if (!ctx || !dt) return IBGPU_E_ARG;
+  if (!ctx->chain_open) return IBGPU_E_STATE;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  ctx->chain_open = false;
+  ctx->chain_steps = 0;
+  return decode_diag(ctx, ctx->chain_marched, dt, diag);
 }
 
 // ---------------------------------------------------------------------------
@@ -1741,15 +1836,18 @@ extern "C" {
 
 void ibgpu_destroy(ibgpu_ctx *ctx) {
   if (!ctx) return;
+  // pending uploads, steps and downloads finish before their buffers go
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->in_stream) cudaStreamSynchronize(ctx->in_stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   ctx->free_layout();
   cudaFree(ctx->d_diag);
   cudaFree(ctx->d_aux_err);
   cudaFreeHost(ctx->h_diag);
-  if (ctx->copy_stream) {
-    cudaStreamSynchronize(ctx->copy_stream);
-    cudaStreamDestroy(ctx->copy_stream);
-  }
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->in_stream) cudaStreamDestroy(ctx->in_stream);
+  if (ctx->ev_in_free) cudaEventDestroy(ctx->ev_in_free);
+  if (ctx->ev_in_done) cudaEventDestroy(ctx->ev_in_done);
   if (ctx->ev_ready) cudaEventDestroy(ctx->ev_ready);
   if (ctx->ev_copied) cudaEventDestroy(ctx->ev_copied);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

@@ -37,7 +37,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
-           "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid")
+           "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
+           "ibgpu_step_async", "ibgpu_step_result")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -224,6 +225,9 @@ def lib(path: str | None = None):
                                      ctypes.POINTER(ctypes.c_float)]
     L.ibgpu_batch_table_bytes.argtypes = [vp]
     L.ibgpu_batch_set_grid.argtypes = [vp, ctypes.c_int]
+    L.ibgpu_upload_state_async.argtypes = [vp, vp]
+    L.ibgpu_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.ibgpu_step_result.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(Diag)]
     L.ibgpu_upload_signdis.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.ibgpu_download_state_async.argtypes = [vp, vp]
     L.ibgpu_batch_tag_mesh.argtypes = [vp, ctypes.POINTER(TagRule), vp, vp]
@@ -488,6 +492,28 @@ class FlowSolver:
 
     def synchronize(self):
         _check(lib().ibgpu_synchronize(self._ctx), "ibgpu_synchronize")
+
+    def upload_async(self, in_ptr: int):
+        """Enqueue an upload of the rows at host address in_ptr (pinned for
+        overlap; left unchanged until synchronize() or step_result())."""
+        _check(lib().ibgpu_upload_state_async(self._ctx, ctypes.c_void_p(in_ptr)),
+               "ibgpu_upload_state_async")
+
+    def step_async(self, ts: int):
+        """Enqueue step ts without waiting; the first one after a result
+        starts from self.dt, later ones from the dt the device computed."""
+        _check(lib().ibgpu_step_async(self._ctx, int(ts), ctypes.c_double(self.dt)),
+               "ibgpu_step_async")
+
+    def step_result(self) -> Diag:
+        """Wait and report the last asynchronous step (dt into self.dt)."""
+        d = Diag()
+        dt = ctypes.c_double(self.dt)
+        rc = lib().ibgpu_step_result(self._ctx, ctypes.byref(dt), ctypes.byref(d))
+        if rc != OK:
+            raise IbgpuError(rc, "ibgpu_step_result", lib().ibgpu_last_error().decode(), d)
+        self.dt = dt.value
+        return d
 
     def time_marching(self, ts: int) -> Diag:
         d = Diag()

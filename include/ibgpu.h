@@ -231,6 +231,26 @@ int ibgpu_step(ibgpu_ctx *ctx, int ts, double *dt, ibgpu_diag *diag);
  * step index; the steps after an abort run on but their state is invalid). */
 int ibgpu_run(ibgpu_ctx *ctx, int ts0, int nsteps, double *dt, ibgpu_diag *diag);
 
+/* Pipelined stepping for callers that hand the state over every step (a host
+ * that keeps the authoritative copy, a coupling loop): nothing here waits on
+ * the host, so the copies of one step overlap the compute of its neighbours.
+ *   ibgpu_upload_state_async: ibgpu_upload_state without waiting; the copy
+ *     runs on the context's upload stream, the scatter into the state after
+ *     the work enqueued so far.  prim (pinned for real overlap) must stay
+ *     unchanged until the next ibgpu_synchronize or ibgpu_step_result.
+ *   ibgpu_step_async: one ibgpu_step of step index ts enqueued; the first one
+ *     after a result (or ever) starts from *dt = dt, later ones continue
+ *     from the dt the device computed (CFL pass every step, as ibgpu_step).
+ *   ibgpu_step_result: waits for the context's stream and reports the last
+ *     asynchronous step's dt and diag, with the first abort of the chain (its
+ *     step counted from the chain's first step).
+ * The results equal those of the synchronous calls bit for bit.  ibgpu_step
+ * and ibgpu_run return IBGPU_E_STATE while a chain is open; at most 2^20
+ * asynchronous steps per result. */
+int ibgpu_upload_state_async(ibgpu_ctx *ctx, const double *prim);
+int ibgpu_step_async(ibgpu_ctx *ctx, int ts, double dt);
+int ibgpu_step_result(ibgpu_ctx *ctx, double *dt, ibgpu_diag *diag);
+
 /* Event timing of the dominant kernels, accumulated while enabled:
  * kernel 0 = stage update (flux + residual + update + prim recovery),
  * 1 = viscous flux, 2 = CFL dt.  ms_out[k] total milliseconds,

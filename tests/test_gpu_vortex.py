@@ -381,3 +381,53 @@ def test_async_download_is_ordered_with_later_uploads(cuda_lib, pkg):
     sol.synchronize()
     assert np.array_equal(out.numpy(), want)
     sol.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pipelined_steps_equal_synchronous_steps(cuda_lib, pkg, precision):
+    """ibgpu_upload_state_async + ibgpu_step_async + ibgpu_download_state_async
+    for several steps, each from its own uploaded state, with one host wait at
+    the end: every step's result and the final dt and diag equal the
+    synchronous calls' bit for bit."""
+    import torch
+    ib, wl = pkg.ibgpu, pkg.workloads
+    prec = {"fp64": ib.FP64, "mixed": ib.MIXED}[precision]
+    P, cells, prim = wl.vortex_case(64, precision=prec)
+    K = 4
+    inputs = []
+    for k in range(K):
+        q = prim.copy()
+        q[:, 4] *= 1.0 + 0.01 * k  # every step starts from its own state
+        inputs.append(q)
+    ref = ib.FlowSolver(P)
+    ref.upload_topology(**cells)
+    want, dts = [], []
+    for k in range(K):
+        ref.init_flow(inputs[k])
+        d_ref = ref.time_marching(k)
+        dts.append(ref.dt)
+        want.append(ref.download())
+    ref.close()
+    sol = ib.FlowSolver(P)
+    sol.upload_topology(**cells)
+    host_in = [torch.from_numpy(q).pin_memory() for q in inputs]
+    host_out = [torch.empty_like(h).pin_memory() for h in host_in]
+    for k in range(K):
+        sol.upload_async(host_in[k].data_ptr())
+        sol.step_async(k)
+        sol.download_async(host_out[k].data_ptr())
+    d = sol.step_result()
+    sol.synchronize()
+    for k in range(K):
+        assert np.array_equal(host_out[k].numpy(), want[k]), k
+    assert sol.dt == dts[-1]
+    assert d.abort_code == 0 and d.cells_marched == d_ref.cells_marched
+    assert list(d.res_max) == list(d_ref.res_max)
+    # no result without a chain; no synchronous step while one is open
+    with pytest.raises(ib.IbgpuError):
+        sol.step_result()
+    sol.step_async(K)
+    with pytest.raises(ib.IbgpuError):
+        sol.time_marching(K + 1)
+    sol.step_result()
+    sol.close()
