@@ -627,6 +627,10 @@ def our_arm(args):
                                    "buffers allocated there)") if e2e_cores else "unbound"},
             "mixed": {"value": mixed_value, "unit": UNIT, "ms_per_step": mms / args.steps,
                       "stage_ms_per_launch": mk[0] / max(mkn[0], 1),
+                      # same algorithmic bytes per launch as the FP64 line (U^n
+                      # and U^(k) stay FP64 in the definition)
+                      "roofline_frac": (stage_bytes / (mk[0] / max(mkn[0], 1) / 1e3) / 1e9) / peak
+                      if peak and mk[0] > 0 else None,
                       "dtype": "f32 flux/limiter, f64 accumulation"},
             "cpu_baseline": cpu,
             "clocks": clocks,
