@@ -77,4 +77,33 @@ def test_state_calls_before_upload(cuda_lib):
     with pytest.raises(ib.IbgpuError) as e:
         s.time_marching(0)
     assert e.value.code == ib.E_STATE
+    with pytest.raises(ib.IbgpuError) as e:
+        s.step_async(0)
+    assert e.value.code == ib.E_STATE
+    s.close()
+
+
+def test_pipelined_entry_points_reject_bad_input(cuda_lib):
+    s = vortex_solver()
+    with pytest.raises(ib.IbgpuError) as e:
+        s.step_result()  # no chain open
+    assert e.value.code == ib.E_STATE
+    s.dt = 0.0  # a chain must start from a positive dt
+    with pytest.raises(ib.IbgpuError) as e:
+        s.step_async(0)
+    assert e.value.code == ib.E_ARG
+    s.dt = 1.0
+    with pytest.raises(ib.IbgpuError) as e:
+        s.step_async(-1)
+    assert e.value.code == ib.E_ARG
+    s.step_async(0)
+    # a new mesh ends the chain; the context stays usable
+    P, cells, prim = wl.vortex_case(32)
+    s.upload_topology(**cells)
+    s.init_flow(prim)
+    with pytest.raises(ib.IbgpuError) as e:
+        s.step_result()
+    assert e.value.code == ib.E_STATE
+    d = s.time_marching(0)
+    assert d.abort_code == 0
     s.close()
