@@ -69,9 +69,17 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 // GELU, tanh form (Hendrycks & Gimpel): 0.5 z (1 + tanh(sqrt(2/pi)(z + 0.044715 z^3)))
 constexpr float kGeluA = 0.7978845608028654f;
 constexpr float kGeluB = 0.044715f;
+// The forward passes take tanh from the SFU's tanh.approx.f32 (one
+// instruction; its error stays well below the BF16 rounding that every
+// activation goes through next), the gradient the accurate tanhf.
+__device__ __forceinline__ float tanh_sfu(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu(float z) {
   const float u = kGeluA * (z + kGeluB * z * z * z);
-  return 0.5f * z * (1.0f + tanhf(u));
+  return 0.5f * z * (1.0f + tanh_sfu(u));
 }
 __device__ __forceinline__ float gelu_grad(float z) {
   const float u = kGeluA * (z + kGeluB * z * z * z);
@@ -177,15 +185,18 @@ __device__ __forceinline__ bool commit_and_wait(uint64_t *bar, uint32_t &phase, 
 }
 
 // 64 f32 columns of this thread's lane starting at `col`, plus bias.
+// (the four loads issued back to back, one wait)
 __device__ __forceinline__ void tmem_row64(uint32_t taddr, const float *bias, float (&v)[64]) {
+  uint32_t r[4][16];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    uint32_t r[16];
-    tc::tmem_ld16(taddr + 16 * q, r);
-    tc::tmem_wait_ld16(r);
+  for (int q = 0; q < 4; ++q) tc::tmem_ld16(taddr + 16 * q, r[q]);
+  tc::tmem_wait_ld16(r[0]);
 #pragma unroll
-    for (int e = 0; e < 16; ++e) v[16 * q + e] = __uint_as_float(r[e]) + (bias ? bias[16 * q + e] : 0.0f);
-  }
+  for (int q = 1; q < 4; ++q) tc::tmem_tie16(r[q]);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[16 * q + e] = __uint_as_float(r[q][e]) + (bias ? bias[16 * q + e] : 0.0f);
 }
 
 // Row-major [rows x 64] bf16 A tile: this thread's row from 64 values.

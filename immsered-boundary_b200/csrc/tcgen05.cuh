@@ -143,5 +143,17 @@ __device__ __forceinline__ void tmem_wait_ld16(uint32_t (&r)[16]) {
                : "memory");
 }
 
+// No instruction: ties 16 registers loaded by tcgen05.ld before an earlier
+// tmem_wait_ld16 (which waits for every load the thread issued) so that no
+// use of them is scheduled before that wait.
+__device__ __forceinline__ void tmem_tie16(uint32_t (&r)[16]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+
 }  // namespace tc
 }  // namespace ibgpu
