@@ -44,6 +44,11 @@ def test_null_arguments_are_rejected_without_gpu(pkg):
     assert lib.ibgpu_create(None, None) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_step(None, 0, None, None) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_upload_topology(None, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_upload_state_async(None, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_step_async(None, 0, 1.0) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_step_result(None, None, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_batch_set_grid(None, 0) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_batch_table_bytes(None) == 0
 
 
 def test_ctypes_layouts_match_c(pkg, tmp_path):
