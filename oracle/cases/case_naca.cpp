@@ -28,13 +28,17 @@
 // rejects with an abort keep the box instead: refinement of a son of the
 // coarse level's restriction ghosts (AMRLevel::CheckRefineTagLocation,
 // AMRLevel.cpp:989-1067, abort 1009) and coarsening next to the level's own
-// restriction pairs (AMR::CheckDetagLocation, AMR.H:715-925, abort 772).
-// One ORACLE_REGRID line per level reports boxes, applied decisions
-// differing from the plain ones and decisions replaced by keep.
+// restriction pairs (AMR::CheckDetagLocation, AMR.H:715-925, abort 772),
+// and either within ighost + 1 coarse cells of a coarser box that this regrid
+// refines or coarsens (the coarser level is adjusted first and moves those
+// ghosts and pairs); refinement also not within two boxes of a box that may
+// not be refined (the regrid adds buffer layers around refined boxes).  One ORACLE_REGRID line per level reports boxes, applied
+// decisions differing from the plain ones and decisions replaced by keep.
 #include <cmath>
 #include <cstdlib>
 #include <unistd.h>
 #include <cstdio>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -276,6 +280,44 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
       };
       vector<char> no_refine, no_coarsen;
       inadmissible(lv, no_refine, no_coarsen);
+      // the coarser levels are adjusted first, so the restriction ghosts and
+      // pairs this level is checked against can still move where a coarser
+      // level changes in this regrid: keep every box within ighost + 1
+      // coarse cells of a coarse box that is refined or coarsened
+      static int changed_ts = -1;
+      static vector<std::set<long long>> changed;  // per level: ix * 2^32 + iy
+      if (changed_ts != ts) {
+        changed_ts = ts;
+        changed.assign(max_mesh_level, std::set<long long>());
+      }
+      if (ilevel >= 1 && !changed[ilevel - 1].empty()) {
+        const int R = ighost + 1;
+        for (int i = bs; i < be; ++i) {
+          const int cx = lv.m_box[i].ix() >> 1, cy = lv.m_box[i].iy() >> 1;
+          bool near = false;
+          for (int dy = -R; dy <= R && !near; ++dy)
+            for (int dx = -R; dx <= R && !near; ++dx)
+              near = changed[ilevel - 1].count(((long long)(cx + dx) << 32) + (cy + dy)) > 0;
+          if (near) no_refine[i] = no_coarsen[i] = 1;
+        }
+      }
+      {
+        // the regrid also tags the neighbours of a refined box (buffer
+        // layers): refine nothing within two boxes of a box it may not refine
+        std::set<long long> banned;
+        for (int i = bs; i < be; ++i)
+          if (no_refine[i]) banned.insert(((long long)lv.m_box[i].ix() << 32) + lv.m_box[i].iy());
+        for (int i = lv.m_box.size(); i < (int)no_refine.size(); ++i)
+          if (no_refine[i]) banned.insert(((long long)lv.m_box[i].ix() << 32) + lv.m_box[i].iy());
+        vector<char> grown(no_refine);
+        for (int i = bs; i < be; ++i) {
+          const int x = lv.m_box[i].ix(), y = lv.m_box[i].iy();
+          for (int dy = -2; dy <= 2 && !grown[i]; ++dy)
+            for (int dx = -2; dx <= 2 && !grown[i]; ++dx)
+              if (banned.count(((long long)(x + dx) << 32) + (y + dy))) grown[i] = 1;
+        }
+        no_refine.swap(grown);
+      }
       int differ = 0, fallback = 0;
       lv.taggedbox.clear();
       for (int i = bs; i < be; ++i) {
@@ -296,6 +338,8 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
         } else if (d == 2) {
           lv.m_tag[i].givedetag();
         }
+        if (d != 0)
+          changed[ilevel].insert(((long long)lv.m_box[i].ix() << 32) + lv.m_box[i].iy());
       }
       printf("ORACLE_REGRID %d %d %d %d %d\n", ts, ilevel, be - bs, differ, fallback);
     }
