@@ -1,6 +1,6 @@
 /*
  * CPU restatement of the reference solver's explicit time step.
- * Test infrastructure only (the checker for the GPU path, and the timed CPU
+ * Test infrastructure only (what the GPU path is tested against, and the timed CPU
  * port); nothing in the GPU library links or calls it.
  *
  * Every function cites the reference code it restates.  Evaluation order

@@ -1,6 +1,6 @@
 /*
  * CPU restatement of the reference solver's explicit time step (test
- * infrastructure only: used by tests/ as the checker and by bench.py's
+ * infrastructure only: used by tests/ to test the GPU path and by bench.py's
  * cpu_baseline leg; never linked into the GPU library).
  *
  * Data model: each AMR level is a dense (ix, iy) index box; a slot is present

@@ -1,7 +1,7 @@
 """CPU oracle of the refinement indicator (test infrastructure only).
 
 Nothing in the product imports this file; tests and the benchmark's CPU
-baseline use it as the checker.
+baseline use it to test the GPU kernels against.
 
 * ``tag_plain``: the plain geometric criterion, the two loops of the case
   hook ``AMR::TagtheBox`` (Userfunction_cy_naca15.cpp:560-635, rftag in

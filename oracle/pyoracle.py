@@ -1,6 +1,6 @@
 """ctypes front end of the CPU oracle (test infrastructure only).
 
-Imported by tests/ (as the checker) and by bench.py's cpu_baseline leg; the
+Imported by tests/ (to test the GPU path against) and by bench.py's cpu_baseline leg; the
 GPU library never imports it.  Provides
 
 * ``read_dump``: reader for the state dumps written by the reference-solver

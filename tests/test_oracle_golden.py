@@ -2,7 +2,7 @@
 
 The golden fixtures were produced by running the reference sources
 (tests/golden/make_golden.py); the restatement must reproduce every dumped
-step bit for bit, which pins it before it is used as the GPU path's checker.
+step bit for bit, which pins it before the GPU path is tested against it.
 """
 import os
 import sys
