@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -335,8 +336,13 @@ class FlowSolver:
         self.ncells = 0
         self._keep = []
         self.init_res = None
+        self._batches = weakref.WeakSet()  # batches holding this context
 
     def close(self):
+        # a batch runs on its first case's stream and holds the contexts:
+        # it goes first
+        for b in list(self._batches):
+            b.close()
         if self._ctx:
             lib().ibgpu_destroy(self._ctx)
             self._ctx = ctypes.c_void_p()
@@ -598,6 +604,8 @@ class Batch:
         self._b = ctypes.c_void_p()
         _check(lib().ibgpu_batch_create(arr, len(self.solvers), ctypes.byref(self._b)),
                "ibgpu_batch_create")
+        for s in self.solvers:
+            s._batches.add(self)
 
     def run(self, ts0: int, nsteps: int):
         """nsteps steps of every case; returns the per-case Diag list."""

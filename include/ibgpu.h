@@ -272,7 +272,8 @@ void ibgpu_destroy(ibgpu_ctx *ctx);
  * keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
  * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; the batch
  * runs on the first context's stream.  Uploads to a context (topology,
- * lists) invalidate a batch that holds it: destroy and recreate it.
+ * lists) invalidate a batch that holds it: destroy and recreate it.  A batch
+ * is destroyed before any context it holds.
  * ------------------------------------------------------------------------- */
 typedef struct ibgpu_batch ibgpu_batch;
 int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out);
