@@ -1,0 +1,44 @@
+"""The benchmark's reference arm on the host cores (no GPU): one JSON line in
+the benchmark's format, timed from the reference's own step (oracle/_ref)
+or, without it, from the C restatement of the same step."""
+import io
+import json
+import os
+import sys
+from contextlib import redirect_stdout
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+class Args:
+    gpus, steps, warmup = 1, 1, 3
+
+
+@pytest.mark.skipif(bench.reference_binary() is None,
+                    reason="reference oracle not built (make -C oracle)")
+def test_reference_arm_prints_one_line_of_the_benchmark_format(monkeypatch):
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    out = io.StringIO()
+    with redirect_stdout(out):
+        assert bench.reference_arm(Args()) == 0
+    lines = [l for l in out.getvalue().splitlines() if l.strip()]
+    assert len(lines) == 1
+    r = json.loads(lines[0])
+    assert r["impl"] == "reference" and r["metric"] == bench.METRIC and r["unit"] == bench.UNIT
+    assert r["value"] > 0 and r["higher_is_better"] is True and r["warmup"] >= 3
+    cb = r["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == r["value"]
+    assert r["e2e"] == {"value": r["value"], "unit": r["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert "workload" in r["config"]
+
+
+def test_port_baseline_times_the_c_restatement(monkeypatch):
+    monkeypatch.setattr(bench, "reference_binary", lambda: None)
+    rate, sec, upd, kind = bench.run_reference(32, 4, 3, 1)
+    assert kind == "port" and upd == 32 * 32 and sec > 0 and rate == upd / sec
