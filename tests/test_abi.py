@@ -53,18 +53,11 @@ def test_null_arguments_are_rejected_without_gpu(pkg):
 
 def test_ctypes_layouts_match_c(pkg, tmp_path):
     ib = pkg.ibgpu
-    checks = {
-        "ibgpu_case": (ib.Case, ["gama", "cfl", "dt_var_step", "nstages", "tp", "limiter",
-                                 "precision", "initvar", "nlevels", "dh", "march_step",
-                                 "step_num", "domain_nx", "periodic_y"]),
-        "ibgpu_cells": (ib.Cells, ["n", "level", "flags"]),
-        "ibgpu_diag": (ib.Diag, ["dt", "cfl_dt", "res_max", "abort_code", "abort_iy",
-                                 "cells_marched"]),
-        "ibgpu_tag_rule": (ib.TagRule, ["body_half_height", "n_rect", "n_rect_coarsen",
-                                        "torefine", "toderefine", "rect_up", "near_margin",
-                                        "derect_up", "denear_margin"]),
-        "ibgpu_tag_cells": (ib.TagCells, ["n", "level", "iy", "xc", "signdis"]),
-    }
+    mirrors = {"ibgpu_case": ib.Case, "ibgpu_cells": ib.Cells, "ibgpu_cf_pairs": ib.CfPairs,
+               "ibgpu_bc": ib.Bc, "ibgpu_ib": ib.Ib, "ibgpu_diag": ib.Diag,
+               "ibgpu_tag_rule": ib.TagRule, "ibgpu_tag_cells": ib.TagCells}
+    # every field of every mirrored struct
+    checks = {c: (cls, [f[0] for f in cls._fields_]) for c, cls in mirrors.items()}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ibgpu.h"', "int main(void){"]
     for cname, (_, fields) in checks.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
@@ -85,3 +78,16 @@ def test_ctypes_layouts_match_c(pkg, tmp_path):
             assert ctypes.sizeof(cls) == int(val), f"{cname} size"
         else:
             assert getattr(cls, what).offset == int(val), f"{cname}.{what}"
+
+
+@pytest.mark.parametrize("compiler,flags", [
+    ("gcc", ["-x", "c", "-std=c99", "-pedantic"]),
+    ("g++", ["-x", "c++", "-std=c++11", "-pedantic"])])
+def test_header_compiles_standalone(tmp_path, compiler, flags):
+    """The boundary header stands alone in C (cgo- or FFI-style bindings) and
+    in C++ (the reference's own code), with no warning."""
+    src = tmp_path / "use.c"
+    src.write_text('#include "ibgpu.h"\nint main(void) { ibgpu_ctx *c = 0; '
+                   'return ibgpu_create(0, &c) == IBGPU_OK; }\n')
+    subprocess.check_call([compiler, *flags, "-Wall", "-Wextra", "-Werror", "-I", INCLUDE,
+                           "-c", str(src), "-o", str(tmp_path / "use.o")])
