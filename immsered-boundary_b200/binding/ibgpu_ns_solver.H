@@ -1,0 +1,342 @@
+// Reference-side binding of the B200 time step: the code a maintainer adds to
+// the reference solver so that its main loop steps on the GPU through the C
+// ABI of include/ibgpu.h, keeping the NS_Solver / Mesh / Body interface.
+//
+// Include after the reference's own headers (AMR.H, Body.H, Mesh.H,
+// NS_Solver.H).  The adapter reads the reference's non-public pair lists,
+// boundary values and immersed-boundary records; the reference grants that
+// with one line in each of AMR, AMRLevel, Mesh, Meshlevel, BCValues and Body:
+//     friend struct IbgpuAdapter;
+//
+// What it replaces (main.cpp:84-116): the three calls
+//     amr.InterfaceExchange(); Body::IBConditions_Image(mesh, bodies);
+//     flowsolver.TimeMarching(amr);
+// become the single GpuNS_Solver::TimeMarching(amr), which runs the
+// coarse/fine exchange (AMRInterface.cpp:3-35), the immersed-body ghost
+// cells (Body.cpp:1361-1496), the domain ghosts and the multistage update
+// (NS_Solver.H:657-702) on the device.  Upload() runs after InitFlow and
+// after every AMR::PerformAdaptive; Download() fills m_data before output,
+// host-side force evaluation or a regrid reads it.
+#pragma once
+
+#include <climits>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ibgpu.h"
+
+// case constants the reference defines in its case file (not in a header)
+extern const double Ma;
+extern double p_ref, area_ref, shear_ref;
+
+// The reference's mesh, pair lists, boundary ghosts and immersed-boundary
+// records as the C ABI's canonical lists (positions, never array indices).
+struct IbgpuLists {
+  // one row per box of the z = 0 plane of every level, normal cells and 2-D
+  // ghosts, in level order and each level's array order
+  std::vector<int32_t> level, ix, iy;
+  std::vector<uint8_t> flags;  // IBGPU_CELL_*
+  std::vector<double> prim;    // 7 per row: roe, u, v, w, p, T, e
+  std::vector<int> box;        // the row's index in its level's box array
+  std::vector<int32_t> res, pro;              // 11 per pair (ibgpu_cf_pairs)
+  std::vector<int32_t> bc;                    // 7 per ghost (ibgpu_bc)
+  std::vector<double> bc_nmv, facevar;        // 3 per ghost, 7 per face
+  double backpressure = 0.0, inlet_flow_angle = 0.0;
+  std::vector<int32_t> ib_cell, patch;        // 18 / 17 per row (ibgpu_ib)
+  std::vector<double> ib_cellf, patchf, body_center;  // 16 / 19 / 3 per row
+};
+
+struct IbgpuAdapter {
+  // Case constants (gas constants, stage coefficients, levels, schedules,
+  // domain, force scales) from the reference's globals and the solver's
+  // stage scheme (NS_Solver.H:200-231).  The limiter is the reference's
+  // compile-time ALimiter choice (Slopelimiter.H:20, 84-87).
+  static ibgpu_case MakeCase(const NS_Solver &s, int limiter, int precision) {
+    ibgpu_case c;
+    std::memset(&c, 0, sizeof c);
+    c.abi_version = IBGPU_ABI_VERSION;
+    c.gama = gama;
+    c.Rg = Rg;
+    c.Cv = Cv;
+    c.Cp = Cp;
+    c.Ma = Ma;
+    c.Re = Re;
+    c.Pr = Pr;
+    c.qk = qk;
+    c.s_over_t = S_over_T_ref;
+    c.cfl = CFL;
+    c.dt_ratio = dt_ratio;
+    c.dt_var_step = dt_var_step;
+    c.nstages = s.sub_time_step;
+    for (int k = 0; k < s.sub_time_step && k < 4; ++k) c.tp[k] = s.tp[k];
+    c.limiter = limiter;
+#ifdef VISCOUSITY
+    c.viscous = 1;
+#else
+    c.viscous = 0;
+#endif
+    c.precision = precision;
+    const double iv[7] = {initvar.roe, initvar.u, initvar.v, initvar.w,
+                          initvar.p,   initvar.T, initvar.e};
+    for (int k = 0; k < 7; ++k) c.initvar[k] = iv[k];
+    const int nlev = s.a_mesh.MyCurNum();
+    c.nlevels = nlev;
+    for (int l = 0; l < nlev && l < IBGPU_MAX_LEVELS; ++l) {
+      for (int k = 0; k < 3; ++k) c.dh[l][k] = dh[l][k];
+      c.march_step[l] = marching_step[l];
+      c.march_left[l] = marching_left_step[l];
+      c.step_num[l] = step_num[l];
+      c.average_step[l] = average_step[l];
+      c.average_left[l] = average_left_step[l];
+      c.prolong_step[l] = prolongation_step[l];
+      c.prolong_left[l] = prolongation_left_step[l];
+    }
+    c.domain_nx = highpt.xy[0];
+    c.domain_ny = highpt.xy[1];
+    c.periodic_x = periodic[0] ? 1 : 0;
+    c.periodic_y = periodic[1] ? 1 : 0;
+    c.body_level = Body::Bodynum() > 0 ? nlev - 1 : -1;
+    c.p_ref = p_ref;
+    c.area_ref = area_ref;
+    c.shear_ref = shear_ref;
+    c.L_ref = L_ref;
+    c.mu = mu;
+    return c;
+  }
+
+  // The code path UpdateConsVars / ComptNewPrimVar / ResinDomain take for a
+  // box (NS_Solver.cpp:3-194, 844-985; NS_Solver.H:264-378): on the finest
+  // level of a run with bodies only non-solid boxes outside the immersed
+  // boundary are updated, elsewhere every leaf box; a leaf box inside a body
+  // (signed distance <= 0) is reset to the free stream.  Block (periodic)
+  // ghosts are copies of the wrapped cell (Mesh::DataExchange).
+  static uint8_t CellFlags(bool normal, bool block_ghost, bool solid, bool free_of_ib,
+                           double signdis, bool body_level) {
+    uint8_t f = IBGPU_CELL_PRESENT;
+    if (normal) f |= IBGPU_CELL_NORMAL;
+    const bool pos = signdis > 0.0;
+    if (body_level) {
+      const bool upd = normal && free_of_ib && !solid;
+      if (upd) f |= IBGPU_CELL_UPDATE;
+      if (upd && pos) f |= IBGPU_CELL_PRIM;
+      if (normal && free_of_ib && !pos) f |= IBGPU_CELL_RESET;
+      if (normal && free_of_ib && pos) f |= IBGPU_CELL_RESNORM;
+    } else if (normal) {
+      f |= IBGPU_CELL_UPDATE | IBGPU_CELL_RESNORM;
+      f |= pos ? IBGPU_CELL_PRIM : IBGPU_CELL_RESET;
+    }
+    if (block_ghost) f |= IBGPU_CELL_ALIAS;
+    return f;
+  }
+
+  static void Pos(std::vector<int32_t> &v, Mesh &mesh, int l, int b) {
+    if (b < 0) {
+      v.push_back(INT32_MIN);
+      v.push_back(INT32_MIN);
+      return;
+    }
+    Box &bx = mesh.ShowLevelBox(l)[b];
+    v.push_back(bx.ix());
+    v.push_back(bx.iy());
+  }
+
+  static void Flatten(Mesh &mesh, AMR &amr, std::vector<Body> &bodies, NS_Solver &solver,
+                      IbgpuLists &L) {
+    L = IbgpuLists();
+    const int nlev = mesh.MyCurNum();
+    const bool with_bodies = Body::Bodynum() > 0;
+    // cells: Meshlevel::m_box / m_data (Meshlevel.H:688-872)
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = mesh.ShowLevelBox(l);
+      DataArray<FlowVariables> &data = mesh.LevelDataArray(l);
+      const int nreal = boxes.realsize(), nnorm = boxes.size();
+      for (int b = 0; b < nreal; ++b) {
+        Box &bx = boxes[b];
+        if (bx.iz() != 0) continue;
+        L.level.push_back(l);
+        L.ix.push_back(bx.ix());
+        L.iy.push_back(bx.iy());
+        L.box.push_back(b);
+        int infect = -1;
+        if (l == nlev - 1 && mesh.Infectboxnum() > b) infect = mesh.BoxInfectIndex(b);
+        L.flags.push_back(CellFlags(b < nnorm, b >= nnorm && bx.type == Blockghost, bx.solid,
+                                    infect == -1, bx.pair.signdis,
+                                    with_bodies && l == nlev - 1));
+        FlowVariables &fv = data[b];
+        const double r[7] = {fv.roe, fv.u, fv.v, fv.w, fv.p, fv.T, fv.e};
+        L.prim.insert(L.prim.end(), r, r + 7);
+      }
+    }
+    // coarse/fine pairs: AMRLevel::f_res_ghost, f_pro_ghost, g_pro
+    // (AMRLevel.H:320-329), the four z = 0 sons in Point_iterator_2d order
+    for (int l = 0; l + 1 < nlev; ++l) {
+      AMRLevel &al = amr.m_level[l];
+      auto pair = [&](std::vector<int32_t> &v, CtoFPair &p) {
+        v.push_back(l);
+        Pos(v, mesh, l, p.ci);
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) Pos(v, mesh, l + 1, p.fi.son[a][b][0]);
+      };
+      for (int ig = 0; ig < ighost; ++ig)
+        for (int i = 0; i < al.f_res_ghost[ig].size(); ++i) pair(L.res, al.f_res_ghost[ig][i]);
+      for (int i = 0; i < al.f_pro_ghost.size(); ++i) pair(L.pro, al.f_pro_ghost[i]);
+      for (int i = 0; i < al.g_pro.size(); ++i) pair(L.pro, al.level_pro_ghost[al.g_pro[i]]);
+    }
+    // domain ghosts of the x and y faces in BCBoxTreat order (BCValues.H:51-188)
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Domainghost> &dmg = mesh.MeshGhostArray(l);
+      for (int i = 0; i < dmg.size(); ++i) {
+        const int f0 = dmg[i].nbface;
+        if (mesh.m_dm.facedir[f0][2] != 0 || mesh.ShowLevelBox(l)[dmg[i].cell].iz() != 0) continue;
+        L.bc.push_back(l);
+        Pos(L.bc, mesh, l, dmg[i].cell);
+        Pos(L.bc, mesh, l, dmg[i].refcell);
+        L.bc.push_back(f0);
+        L.bc.push_back(mesh.m_dm.facetype[f0]);
+        for (int k = 0; k < 3; ++k) L.bc_nmv.push_back(dmg[i].nmv[k]);
+      }
+    }
+    BCValues &B = solver.meshbc;
+    for (size_t f = 0; f < B.facevar.size(); ++f) {
+      FlowVariables &v = B.facevar[f];
+      const double r[7] = {v.roe, v.u, v.v, v.w, v.p, v.T, v.e};
+      L.facevar.insert(L.facevar.end(), r, r + 7);
+    }
+    L.backpressure = B.backpressure;
+    L.inlet_flow_angle = inlet_flow_angle;
+    // immersed-boundary cells of the finest level (IBCell, Body.cpp:1361-1496)
+    const int last = nlev - 1;
+    DataArray<IBCell> &mdis = mesh.ibarray();
+    for (int i = 0; i < mdis.size(); ++i) {
+      IBCell &c = mdis[i];
+      if (!(mesh.m_level[last].m_box.isnormal(c.ci) && c.mynode == node)) continue;
+      BoxtoWall &w = mesh.m_level[last].m_box[c.ci].pair;
+      Pos(L.ib_cell, mesh, last, c.ci);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int k = 0; k < 2; ++k) Pos(L.ib_cell, mesh, last, c.hgc.intpcell[a][b][k]);
+      Pointxyz wall_v;
+      bodies[w.body].Surface_Point_Velocity(c.hgc.attach_pt, wall_v);
+      Pointxyz &nv = bodies[w.body].patch[w.patch].nv;
+      L.ib_cellf.push_back(w.signdis);
+      L.ib_cellf.push_back(c.hgc.hgdis);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int k = 0; k < 2; ++k) L.ib_cellf.push_back(c.hgc.intpcoef[a][b][k]);
+      for (int k = 0; k < 3; ++k) L.ib_cellf.push_back(nv[k]);
+      for (int k = 0; k < 3; ++k) L.ib_cellf.push_back(wall_v[k]);
+    }
+    // wall patches of Body::ComptWallForce (Body.cpp:439-558)
+    for (size_t bi = 0; bi < bodies.size(); ++bi) {
+      Body &Bd = bodies[bi];
+      for (int k = 0; k < 3; ++k) L.body_center.push_back(Bd.bodycenter[k]);
+      for (int i = 0; i < Bd.patch.size(); ++i) {
+        Surfpatch &P = Bd.patch[i];
+        if (P.node != node) continue;
+        L.patch.push_back((int32_t)bi);
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 2; ++k) Pos(L.patch, mesh, last, P.hgc.intpcell[a][b][k]);
+        for (int k = 0; k < 3; ++k) L.patchf.push_back(P.pc[k]);
+        for (int k = 0; k < 3; ++k) L.patchf.push_back(P.nv[k]);
+        L.patchf.push_back(P.area);
+        L.patchf.push_back(P.hgc.hgdis);
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 2; ++k) L.patchf.push_back(P.hgc.intpcoef[a][b][k]);
+        Pointxyz wall_v;
+        Bd.Surface_Point_Velocity(P.pc, wall_v);
+        for (int k = 0; k < 3; ++k) L.patchf.push_back(wall_v[k]);
+      }
+    }
+  }
+
+  // The lists and the state into a context (ibgpu_upload_*).
+  static int Upload(ibgpu_ctx *ctx, const IbgpuLists &L) {
+    ibgpu_cells cells = {(int64_t)L.level.size(), L.level.data(), L.ix.data(), L.iy.data(),
+                         L.flags.data()};
+    int rc = ibgpu_upload_topology(ctx, &cells);
+    if (rc) return rc;
+    ibgpu_cf_pairs cf = {(int64_t)L.res.size() / 11, L.res.data(), (int64_t)L.pro.size() / 11,
+                         L.pro.data()};
+    if ((rc = ibgpu_upload_interfaces(ctx, &cf))) return rc;
+    ibgpu_bc bc = {(int64_t)L.bc.size() / 7, L.bc.data(), L.bc_nmv.data(),
+                   (int)(L.facevar.size() / 7), L.facevar.data(), L.backpressure,
+                   L.inlet_flow_angle};
+    if ((rc = ibgpu_upload_boundaries(ctx, &bc))) return rc;
+    ibgpu_ib ib = {(int64_t)L.ib_cell.size() / 18, L.ib_cell.data(), L.ib_cellf.data(),
+                   (int64_t)L.patch.size() / 17, L.patch.data(), L.patchf.data(),
+                   (int)(L.body_center.size() / 3), L.body_center.data()};
+    if ((rc = ibgpu_upload_ib(ctx, &ib))) return rc;
+    return ibgpu_upload_state(ctx, L.prim.data());
+  }
+};
+
+// NS_Solver whose TimeMarching runs on the GPU.  TimeMarching is non-virtual
+// and inline in the reference (NS_Solver.H:657-702), so the main loop holds
+// the solver with this static type.
+class GpuNS_Solver : public NS_Solver {
+ public:
+  GpuNS_Solver(Mesh &m, Domain &d, int nbody) : NS_Solver(m, d, nbody) {}
+  GpuNS_Solver(const GpuNS_Solver &) = delete;
+  GpuNS_Solver &operator=(const GpuNS_Solver &) = delete;
+  ~GpuNS_Solver() {
+    if (ctx_) ibgpu_destroy(ctx_);
+  }
+
+  // Device context for this case (IBGPU_FP64 / IBGPU_FP64_EXACT /
+  // IBGPU_MIXED; the limiter as the reference was compiled with).
+  int Create(int limiter, int precision) {
+    if (ctx_) return IBGPU_E_STATE;
+    const ibgpu_case c = IbgpuAdapter::MakeCase(*this, limiter, precision);
+    return ibgpu_create(&c, &ctx_);
+  }
+
+  // After InitFlow and after every AMR::PerformAdaptive.
+  int Upload(AMR &amr, std::vector<Body> &bodies) {
+    if (!ctx_) return IBGPU_E_STATE;
+    IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
+    return IbgpuAdapter::Upload(ctx_, lists_);
+  }
+
+  // One step: ghost fills, CFL dt every dt_var_step steps, the stages and
+  // the residual, aborting with the reference's code as it would.
+  void TimeMarching(AMR &) {
+    ibgpu_diag diag;
+    const int rc = ibgpu_step(ctx_, ts, &dt, &diag);
+    if (rc == IBGPU_E_ABORT) MPI_Abort(MPI_COMM_WORLD, diag.abort_code);
+    if (rc != IBGPU_OK) {
+      std::fprintf(stderr, "ibgpu_step: %s (%s)\n", ibgpu_errstr(rc), ibgpu_last_error());
+      MPI_Abort(MPI_COMM_WORLD, 1);
+    }
+    if (ts % dt_var_step == 0) CFL_dt = diag.cfl_dt;
+  }
+
+  // m_data <- the device state, for output, host-side forces or a regrid.
+  int Download() {
+    if (!ctx_) return IBGPU_E_STATE;
+    std::vector<double> rows(lists_.prim.size());
+    const int rc = ibgpu_download_state(ctx_, rows.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < lists_.box.size(); ++i) {
+      FlowVariables &fv = a_mesh.LevelDataArray(lists_.level[i])[lists_.box[i]];
+      const double *r = &rows[7 * i];
+      fv.roe = r[0];
+      fv.u = r[1];
+      fv.v = r[2];
+      fv.w = r[3];
+      fv.p = r[4];
+      fv.T = r[5];
+      fv.e = r[6];
+    }
+    return IBGPU_OK;
+  }
+
+  const IbgpuLists &lists() const { return lists_; }
+
+ private:
+  ibgpu_ctx *ctx_ = nullptr;
+  IbgpuLists lists_;
+};

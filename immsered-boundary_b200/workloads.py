@@ -148,32 +148,45 @@ def naca_params(g: dict, k: int, precision: int) -> dict:
                 L_ref=bf[3 * nb + 3], mu=bf[3 * nb + 4], dt0=float(s[1]))
 
 
-def naca_solver(g: dict, k: int, precision: int):
-    """FlowSolver holding the record's mesh (cell list, coarse/fine pairs,
-    domain ghosts, immersed-boundary cells and wall patches) and snapshot
-    k's state."""
+def naca_lists(g: dict, k: int) -> dict:
+    """The C ABI's lists of a mesh/state record of the reference solver:
+    cell list with IBGPU_CELL_* flags, coarse/fine pairs, domain ghosts of
+    the x and y faces, immersed-boundary cells and wall patches, and the
+    state rows of snapshot k (the arguments of the ibgpu_upload_* calls)."""
     ib = ibgpu
-    P = naca_params(g, k, precision)
-    sol = ib.FlowSolver(P)
-    nlev = P["nlevels"]
+    nlev = int(g["domain"][5])
+    nb = int(g["domain"][4])
+    body_level = nlev - 1 if nb > 0 else -1
     flags = np.zeros(len(g["level"]), np.uint8)
     for l in range(nlev):
         m = g["level"] == l
         flags[m] = ib.cell_flags_from_boxes(g["kind"][m], g["solid"][m], g["infect"][m],
-                                            g["signdis"][m], l == P["body_level"])
-    sol.upload_topology(g["level"], g["ix"], g["iy"], flags)
-    res = g["cf_res"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
-    pro = g["cf_pro"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]]
-    sol.upload_interfaces(res, pro)
+                                            g["signdis"][m], l == body_level)
     bc = g["bc"].reshape(-1, 9)
     keep = (bc[:, 7] == 0) & (bc[:, 8] == 0)  # x/y faces, z = 0 plane
-    sol.upload_boundaries(bc[keep][:, :7], g["bc_nmv"].reshape(-1, 3)[keep],
-                          g["facevar"].reshape(-1, 7), g["bc_scalars"][0], g["bc_scalars"][1])
-    nb = int(g["domain"][4])
-    sol.upload_ib(g["ib"].reshape(-1, 20)[:, :18], g["ib_f"].reshape(-1, 16),
-                  g["patch"].reshape(-1, 17), g["patch_f"].reshape(-1, 19),
-                  g["body_f"][:3 * nb].reshape(-1, 3))
-    sol.init_flow(g["prim"][k])
+    return dict(level=g["level"], ix=g["ix"], iy=g["iy"], flags=flags,
+                res=g["cf_res"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]],
+                pro=g["cf_pro"].reshape(-1, 12)[:, [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11]],
+                bc=bc[keep][:, :7], bc_nmv=g["bc_nmv"].reshape(-1, 3)[keep],
+                facevar=g["facevar"].reshape(-1, 7), bc_scalars=g["bc_scalars"][:2],
+                ib=g["ib"].reshape(-1, 20)[:, :18], ib_f=g["ib_f"].reshape(-1, 16),
+                patch=g["patch"].reshape(-1, 17), patch_f=g["patch_f"].reshape(-1, 19),
+                body_center=g["body_f"][:3 * nb].reshape(-1, 3), prim=g["prim"][k])
+
+
+def naca_solver(g: dict, k: int, precision: int):
+    """FlowSolver holding the record's mesh (cell list, coarse/fine pairs,
+    domain ghosts, immersed-boundary cells and wall patches) and snapshot
+    k's state."""
+    P = naca_params(g, k, precision)
+    L = naca_lists(g, k)
+    sol = ibgpu.FlowSolver(P)
+    sol.upload_topology(L["level"], L["ix"], L["iy"], L["flags"])
+    sol.upload_interfaces(L["res"], L["pro"])
+    sol.upload_boundaries(L["bc"], L["bc_nmv"], L["facevar"], L["bc_scalars"][0],
+                          L["bc_scalars"][1])
+    sol.upload_ib(L["ib"], L["ib_f"], L["patch"], L["patch_f"], L["body_center"])
+    sol.init_flow(L["prim"])
     return sol
 
 

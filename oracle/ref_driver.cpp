@@ -57,6 +57,9 @@ using namespace std;  // the reference headers assume it (min/max/abs in macros)
 #include "NS_Solver.H"
 #include "Pltoutput.H"
 #include "TwoLevelOp.H"
+#ifdef ORACLE_BINDING
+#include "ibgpu_ns_solver.H"
+#endif
 
 extern const double Ma;
 extern double p_ref, area_ref, shear_ref;
@@ -393,6 +396,46 @@ int main(int argc, char **argv) {
     std::fclose(g_oracle_tag_dump);
     g_oracle_tag_dump = nullptr;
   }
+
+#ifdef ORACLE_BINDING
+  // IB_BINDING_LISTS=<file>: the lists and case constants the reference-side
+  // binding (ibgpu_ns_solver.H) hands to the C ABI for this mesh and state,
+  // and the status of ibgpu_create with them
+  if (const char *bl = std::getenv("IB_BINDING_LISTS")) {
+    IbgpuLists L;
+    IbgpuAdapter::Flatten(mesh, amr, sphere, flowsolver, L);
+#ifdef ORACLE_MINMOD
+    const int lim = IBGPU_LIM_MINMOD;
+#else
+    const int lim = IBGPU_LIM_VANLEER;
+#endif
+    const ibgpu_case c = IbgpuAdapter::MakeCase(flowsolver, lim, IBGPU_FP64);
+    std::vector<int32_t> cw(sizeof c / 4);
+    std::memcpy(cw.data(), &c, sizeof c);
+    ibgpu_ctx *ctx = nullptr;
+    const int rc = ibgpu_create(&c, &ctx);
+    if (ctx) ibgpu_destroy(ctx);
+    Dump d(bl);
+    d.i32("level", L.level);
+    d.i32("ix", L.ix);
+    d.i32("iy", L.iy);
+    d.i32("flags", std::vector<int32_t>(L.flags.begin(), L.flags.end()));
+    d.f64("prim", L.prim);
+    d.i32("res", L.res);
+    d.i32("pro", L.pro);
+    d.i32("bc", L.bc);
+    d.f64("bc_nmv", L.bc_nmv);
+    d.f64("facevar", L.facevar);
+    d.f64("bc_scalars", std::vector<double>{L.backpressure, L.inlet_flow_angle});
+    d.i32("ib", L.ib_cell);
+    d.f64("ib_f", L.ib_cellf);
+    d.i32("patch", L.patch);
+    d.f64("patch_f", L.patchf);
+    d.f64("body_center", L.body_center);
+    d.i32("case", cw);
+    d.i32("create_rc", std::vector<int32_t>{rc});
+  }
+#endif
 
   const int nsteps = env_int("IB_STEPS", 5);
   const int timed_from = env_int("IB_TIMED_FROM", 0);  // steps before this are warm-up

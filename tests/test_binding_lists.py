@@ -1,0 +1,70 @@
+"""The reference-side C++ binding (immsered-boundary_b200/binding/
+ibgpu_ns_solver.H) compiled into the reference solver (no GPU): from the
+reference's own NACA0012 mesh and state it hands the C ABI exactly the cell
+list, flags, state rows, coarse/fine pairs, domain ghosts, immersed-boundary
+records and case constants that the GPU parity tests upload from the
+reference's dump of the same run (workloads.naca_lists / naca_params)."""
+import ctypes
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ORACLE_DIR, load_pkg
+
+sys.path.insert(0, ORACLE_DIR)
+import pyoracle  # noqa: E402
+
+BINARY = os.path.join(ORACLE_DIR, "_ref", "ref_naca_minmod_binding")
+CASE_ENV = {"IB_NX": "64", "IB_LEVELS": "3", "IB_STAGES": "4", "IB_USER_INIT": "0",
+            "IB_NPTS": "120", "IB_STEPS": "0"}
+
+pytestmark = pytest.mark.skipif(not os.path.exists(BINARY),
+                                reason="binding oracle not built (make -C oracle)")
+
+
+def run_binding():
+    work = tempfile.mkdtemp(prefix="binding_")
+    env = dict(os.environ, **CASE_ENV, IB_DUMP=os.path.join(work, "d"),
+               IB_BINDING_LISTS=os.path.join(work, "lists.bin"))
+    out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    d = pyoracle.read_dump(os.path.join(work, "d_000000.bin"))
+    d["prim"] = d["prim"].reshape(1, -1, 7)
+    d["scalars"] = d["scalars"].reshape(1, -1)
+    return d, pyoracle.read_dump(os.path.join(work, "lists.bin"))
+
+
+def test_binding_hands_the_abi_the_dumped_lists():
+    pkg = load_pkg()
+    ib, wl = pkg.ibgpu, pkg.workloads
+    d, b = run_binding()
+    want = wl.naca_lists(d, 0)
+    for k in ("level", "ix", "iy", "flags"):
+        assert np.array_equal(b[k], want[k]), k
+    assert np.array_equal(b["prim"].reshape(-1, 7), want["prim"])
+    for k, w in (("res", 11), ("pro", 11), ("bc", 7), ("ib", 18), ("patch", 17)):
+        assert np.array_equal(b[k].reshape(-1, w), want[k]), k
+    for k, w in (("bc_nmv", 3), ("facevar", 7), ("ib_f", 16), ("patch_f", 19),
+                 ("body_center", 3)):
+        assert np.array_equal(b[k].reshape(-1, w), want[k]), k
+    assert np.array_equal(b["bc_scalars"], want["bc_scalars"])
+    # the mesh is a real AMR mesh with a body: every list is populated
+    assert all(len(want[k]) for k in ("res", "pro", "bc", "ib", "patch"))
+    # case constants: the same bytes as the parity tests' ibgpu_case
+    case = ib.make_case(wl.naca_params(d, 0, ib.FP64))
+    assert b["case"].tobytes() == bytes(case)
+    assert ctypes.sizeof(case) == 4 * len(b["case"])
+
+
+def test_binding_context_creation_status():
+    import torch
+    _, b = run_binding()
+    rc = int(b["create_rc"][0])
+    if torch.cuda.is_available():
+        assert rc == 0
+    else:
+        assert rc == load_pkg().ibgpu.E_CUDA  # reported, not aborted
