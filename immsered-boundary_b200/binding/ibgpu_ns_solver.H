@@ -334,6 +334,14 @@ class GpuNS_Solver : public NS_Solver {
     return IBGPU_OK;
   }
 
+  // Force and moment of every body from the device state
+  // (Body::ComptWallForce): 6 per body, force then moment.
+  int WallForces(std::vector<double> &out) {
+    if (!ctx_) return IBGPU_E_STATE;
+    out.assign(6 * (size_t)Body::Bodynum(), 0.0);
+    return out.empty() ? IBGPU_OK : ibgpu_wall_forces(ctx_, out.data());
+  }
+
   const IbgpuLists &lists() const { return lists_; }
 
  private:

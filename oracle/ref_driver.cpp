@@ -73,9 +73,22 @@ int env_int(const char *n, int d) {
   return (s && *s) ? std::atoi(s) : d;
 }
 
-class OracleSolver : public NS_Solver {
+#ifdef ORACLE_BINDING
+// the binding build: the same solver with the reference-side GPU binding
+// underneath, stepping on the GPU once on_gpu is set (IB_BINDING_STEP)
+typedef GpuNS_Solver SolverBase;
+#ifdef ORACLE_MINMOD
+const int kLimiter = IBGPU_LIM_MINMOD;
+#else
+const int kLimiter = IBGPU_LIM_VANLEER;
+#endif
+#else
+typedef NS_Solver SolverBase;
+#endif
+
+class OracleSolver : public SolverBase {
  public:
-  OracleSolver(Mesh &m, Domain &d, int nbody, int stages) : NS_Solver(m, d, nbody) {
+  OracleSolver(Mesh &m, Domain &d, int nbody, int stages) : SolverBase(m, d, nbody) {
     sub_time_step = stages;
     tp.resize(stages);
     if (stages == 4) {
@@ -88,6 +101,13 @@ class OracleSolver : public NS_Solver {
   }
   int stages() const { return sub_time_step; }
   double coef(int k) const { return tp[k]; }
+#ifdef ORACLE_BINDING
+  bool on_gpu = false;
+  void TimeMarching(AMR &amr) {
+    if (on_gpu) GpuNS_Solver::TimeMarching(amr);
+    else NS_Solver::TimeMarching(amr);
+  }
+#endif
 };
 
 // Minimal tagged binary record writer: [u32 name_len][name][u32 kind][u64 n][payload]
@@ -404,12 +424,7 @@ int main(int argc, char **argv) {
   if (const char *bl = std::getenv("IB_BINDING_LISTS")) {
     IbgpuLists L;
     IbgpuAdapter::Flatten(mesh, amr, sphere, flowsolver, L);
-#ifdef ORACLE_MINMOD
-    const int lim = IBGPU_LIM_MINMOD;
-#else
-    const int lim = IBGPU_LIM_VANLEER;
-#endif
-    const ibgpu_case c = IbgpuAdapter::MakeCase(flowsolver, lim, IBGPU_FP64);
+    const ibgpu_case c = IbgpuAdapter::MakeCase(flowsolver, kLimiter, IBGPU_FP64);
     std::vector<int32_t> cw(sizeof c / 4);
     std::memcpy(cw.data(), &c, sizeof c);
     ibgpu_ctx *ctx = nullptr;
@@ -437,6 +452,25 @@ int main(int argc, char **argv) {
   }
 #endif
 
+  // IB_BINDING_STEP=1: the loop steps through the binding on the GPU (FP64
+  // build) instead of the reference's own step; state read back for dumps
+  // and regrids, forces from the device
+#ifdef ORACLE_BINDING
+  const bool gpu_step = env_int("IB_BINDING_STEP", 0) != 0;
+  auto gpu_check = [](int rc, const char *what) {
+    if (rc == IBGPU_OK) return;
+    std::fprintf(stderr, "%s: %s (%s)\n", what, ibgpu_errstr(rc), ibgpu_last_error());
+    std::exit(3);
+  };
+  if (gpu_step) {
+    gpu_check(flowsolver.Create(kLimiter, IBGPU_FP64), "ibgpu_create");
+    gpu_check(flowsolver.Upload(amr, sphere), "upload");
+    flowsolver.on_gpu = true;
+  }
+#else
+  const bool gpu_step = false;
+#endif
+
   const int nsteps = env_int("IB_STEPS", 5);
   const int timed_from = env_int("IB_TIMED_FROM", 0);  // steps before this are warm-up
   const int every = env_int("IB_DUMP_EVERY", 1);
@@ -449,6 +483,9 @@ int main(int argc, char **argv) {
   std::vector<double> forces;
   auto do_dump = [&](int step) {
     if (!prefix) return;
+#ifdef ORACLE_BINDING
+    if (gpu_step) gpu_check(flowsolver.Download(), "download");
+#endif
     char buf[64];
     std::snprintf(buf, sizeof buf, "_%06d.bin", step);
     dump_state(std::string(prefix) + buf, mesh, flowsolver, forces);
@@ -463,8 +500,10 @@ int main(int argc, char **argv) {
     for (int l = 0; l < mesh.MyCurNum(); ++l)
       if (ts % marching_step[l] == marching_left_step[l]) marching_cells += mesh.ShowLevelBox(l).size();
     double t0 = MPI_Wtime();
-    amr.InterfaceExchange();
-    Body::IBConditions_Image(mesh, sphere);
+    if (!gpu_step) {  // the GPU step runs both ghost fills itself
+      amr.InterfaceExchange();
+      Body::IBConditions_Image(mesh, sphere);
+    }
     flowsolver.TimeMarching(amr);
     ++ts;
     t += dt;
@@ -474,7 +513,10 @@ int main(int argc, char **argv) {
       cell_updates += marching_cells;
     }
     forces.clear();
-    if (forces_on) {
+#ifdef ORACLE_BINDING
+    if (forces_on && gpu_step) gpu_check(flowsolver.WallForces(forces), "ibgpu_wall_forces");
+#endif
+    if (forces_on && !gpu_step) {
       for (size_t b = 0; b < sphere.size(); ++b) {
         sphere[b].ComptWallForce(mesh);
         for (int k = 0; k < 3; ++k) forces.push_back(sphere[b].draglift(k));
@@ -487,6 +529,9 @@ int main(int argc, char **argv) {
       if (!forces.empty()) std::fwrite(forces.data(), sizeof(double), forces.size(), flog);
     }
     amr.ADPRule(sphere);
+#ifdef ORACLE_BINDING
+    if (adpflag && gpu_step) gpu_check(flowsolver.Download(), "download");
+#endif
     if (adpflag) {
       // a tag server decides from the state it sees here (case file)
       const char *server = std::getenv("IB_TAG_SERVER");
@@ -496,6 +541,9 @@ int main(int argc, char **argv) {
         std::rename((path + ".part").c_str(), path.c_str());
       }
       amr.PerformAdaptive(sphere);
+#ifdef ORACLE_BINDING
+      if (gpu_step) gpu_check(flowsolver.Upload(amr, sphere), "upload");
+#endif
     }
     adpflag = false;
     if (prefix && (ts % every == 0 || s == nsteps - 1)) do_dump(ts);

@@ -68,3 +68,30 @@ def test_binding_context_creation_status():
         assert rc == 0
     else:
         assert rc == load_pkg().ibgpu.E_CUDA  # reported, not aborted
+
+
+def _forces(binary, extra):
+    work = tempfile.mkdtemp(prefix="binding_run_")
+    log = os.path.join(work, "forces.bin")
+    env = dict(os.environ, **{**CASE_ENV, "IB_STEPS": "20", "IB_FORCES": "1",
+                              "IB_FORCE_LOG": log, **extra})
+    out = subprocess.run([binary], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    return out, (np.fromfile(log, np.float64) if os.path.exists(log) else None)
+
+
+def test_binding_build_keeps_the_reference_step():
+    """Without IB_BINDING_STEP the binding build runs the reference's own step:
+    its force history equals the plain reference build's bit for bit."""
+    out, with_binding = _forces(BINARY, {})
+    assert out.returncode == 0, out.stderr[-2000:]
+    out, plain = _forces(os.path.join(ORACLE_DIR, "_ref", "ref_naca_minmod"), {})
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert len(plain) > 0 and np.array_equal(with_binding, plain)
+
+
+def test_binding_step_without_gpu_reports_the_error():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the binding step would run")
+    out, _ = _forces(BINARY, {"IB_BINDING_STEP": "1"})
+    assert out.returncode == 3 and "ibgpu_create" in out.stderr
