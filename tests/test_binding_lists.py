@@ -95,3 +95,26 @@ def test_binding_step_without_gpu_reports_the_error():
         pytest.skip("a GPU is present: the binding step would run")
     out, _ = _forces(BINARY, {"IB_BINDING_STEP": "1"})
     assert out.returncode == 3 and "ibgpu_create" in out.stderr
+
+
+def test_binding_cells_of_the_periodic_vortex():
+    """Single periodic level: block (periodic) ghosts become alias rows, the
+    cell list and flags equal the ones the vortex parity tests upload."""
+    pkg = load_pkg()
+    ib = pkg.ibgpu
+    binary = os.path.join(ORACLE_DIR, "_ref", "ref_vortex_vanleer_binding")
+    work = tempfile.mkdtemp(prefix="binding_vortex_")
+    env = dict(os.environ, IB_NX="32", IB_STAGES="4", IB_STEPS="0",
+               IB_DUMP=os.path.join(work, "d"), IB_BINDING_LISTS=os.path.join(work, "lists.bin"))
+    out = subprocess.run([binary], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    d = pyoracle.read_dump(os.path.join(work, "d_000000.bin"))
+    b = pyoracle.read_dump(os.path.join(work, "lists.bin"))
+    flags = ib.cell_flags_from_boxes(d["kind"], d["solid"], d["infect"], d["signdis"], False)
+    for k in ("level", "ix", "iy"):
+        assert np.array_equal(b[k], d[k]), k
+    assert np.array_equal(b["flags"], flags)
+    assert np.array_equal(b["prim"], d["prim"])
+    alias = (b["flags"] & ib.CELL_ALIAS) != 0
+    assert alias.sum() == (32 + 4) ** 2 - 32 * 32  # the two-cell periodic frame
+    assert len(b["res"]) == len(b["pro"]) == len(b["ib"]) == 0
