@@ -253,6 +253,57 @@ struct IbgpuAdapter {
     }
   }
 
+  // Boxes of the z = 0 plane in a level's range [ps, pe) as AMR::TagtheBox
+  // judges them: position, centre (Mesh::bc) and signed wall distance.
+  struct TagBoxes {
+    std::vector<int32_t> level, ix, iy;
+    std::vector<double> xc, yc, signdis;
+    std::vector<int> box;  // index in the level's box array
+  };
+  static void GatherTagBoxes(Mesh &mesh, AMR &amr, int level, TagBoxes &T) {
+    T = TagBoxes();
+    AMRLevel &al = amr.m_level[level];
+    for (int i = al.m_box.ps(); i < al.m_box.pe(); ++i) {
+      Box &b = al.m_box[i];
+      if (b.iz() != 0) continue;
+      T.level.push_back(level);
+      T.ix.push_back(b.ix());
+      T.iy.push_back(b.iy());
+      T.xc.push_back(mesh.bc(level, i)[0]);
+      T.yc.push_back(mesh.bc(level, i)[1]);
+      T.signdis.push_back(b.pair.signdis);
+      T.box.push_back(i);
+    }
+  }
+
+  // The tagging loops of a case's AMR::TagtheBox (Userfunction_cy_naca15.cpp
+  // :560-635) for one level through the C ABI: the plain criterion
+  // (ibgpu_tag_plain) or, with device MLP parameters, the learned indicator
+  // (ibgpu_tag_learned, reading the context's uploaded state); the decisions
+  // land in m_tag / taggedbox as the loops leave them.  Call after
+  // Inittag(); CheckDetagLocation stays the caller's.
+  static int TagLevel(ibgpu_ctx *ctx, const ibgpu_tag_rule &rule, Mesh &mesh, AMR &amr,
+                      int level, const float *d_params) {
+    TagBoxes T;
+    GatherTagBoxes(mesh, amr, level, T);
+    const ibgpu_tag_cells q = {(int64_t)T.box.size(), T.level.data(), T.ix.data(), T.iy.data(),
+                               T.xc.data(), T.yc.data(), T.signdis.data()};
+    std::vector<uint8_t> bits(T.box.size());
+    const int rc = d_params ? ibgpu_tag_learned(ctx, &rule, &q, d_params, bits.data())
+                            : ibgpu_tag_plain(ctx, &rule, &q, bits.data());
+    if (rc) return rc;
+    AMRLevel &al = amr.m_level[level];
+    for (size_t k = 0; k < bits.size(); ++k) {
+      const int i = T.box[k];
+      if (bits[k] & IBGPU_TAG_REFINE) {
+        al.m_tag[i].givetag();
+        al.taggedbox.push_back(i);
+      }
+      if (bits[k] & IBGPU_TAG_COARSEN) al.m_tag[i].givedetag();
+    }
+    return IBGPU_OK;
+  }
+
   // The lists and the state into a context (ibgpu_upload_*).
   static int Upload(ibgpu_ctx *ctx, const IbgpuLists &L) {
     ibgpu_cells cells = {(int64_t)L.level.size(), L.level.data(), L.ix.data(), L.iy.data(),

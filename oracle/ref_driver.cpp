@@ -449,6 +449,27 @@ int main(int argc, char **argv) {
     d.f64("body_center", L.body_center);
     d.i32("case", cw);
     d.i32("create_rc", std::vector<int32_t>{rc});
+    // the boxes the binding's TagLevel judges, per level
+    std::vector<int32_t> tl, tx, ty, tb;
+    std::vector<double> txc, tyc, tsd;
+    for (int l = 0; l < mesh.MyCurNum(); ++l) {
+      IbgpuAdapter::TagBoxes T;
+      IbgpuAdapter::GatherTagBoxes(mesh, amr, l, T);
+      tl.insert(tl.end(), T.level.begin(), T.level.end());
+      tx.insert(tx.end(), T.ix.begin(), T.ix.end());
+      ty.insert(ty.end(), T.iy.begin(), T.iy.end());
+      tb.insert(tb.end(), T.box.begin(), T.box.end());
+      txc.insert(txc.end(), T.xc.begin(), T.xc.end());
+      tyc.insert(tyc.end(), T.yc.begin(), T.yc.end());
+      tsd.insert(tsd.end(), T.signdis.begin(), T.signdis.end());
+    }
+    d.i32("tag_level", tl);
+    d.i32("tag_ix", tx);
+    d.i32("tag_iy", ty);
+    d.i32("tag_box", tb);
+    d.f64("tag_xc", txc);
+    d.f64("tag_yc", tyc);
+    d.f64("tag_signdis", tsd);
   }
 #endif
 

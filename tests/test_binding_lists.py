@@ -118,3 +118,22 @@ def test_binding_cells_of_the_periodic_vortex():
     alias = (b["flags"] & ib.CELL_ALIAS) != 0
     assert alias.sum() == (32 + 4) ** 2 - 32 * 32  # the two-cell periodic frame
     assert len(b["res"]) == len(b["pro"]) == len(b["ib"]) == 0
+
+
+def test_binding_tag_boxes_are_the_ones_tagthebox_judges():
+    """The boxes the binding's TagLevel hands ibgpu_tag_plain / _learned are
+    those the case's AMR::TagtheBox judges on the finished mesh (its tag
+    dump, pass 1): same order, positions, centres and wall distances."""
+    work = tempfile.mkdtemp(prefix="binding_tags_")
+    env = dict(os.environ, **CASE_ENV, IB_TAG_DUMP=os.path.join(work, "tags.bin"),
+               IB_BINDING_LISTS=os.path.join(work, "lists.bin"))
+    out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    rows = np.fromfile(os.path.join(work, "tags.bin"), np.float64).reshape(-1, 9)
+    rows = rows[rows[:, 8] == 1]
+    b = pyoracle.read_dump(os.path.join(work, "lists.bin"))
+    assert len(rows) == len(b["tag_level"]) > 0
+    for col, k in enumerate(("tag_level", "tag_ix", "tag_iy")):
+        assert np.array_equal(rows[:, col].astype(np.int32), b[k]), k
+    for col, k in ((3, "tag_xc"), (4, "tag_yc"), (5, "tag_signdis")):
+        assert np.array_equal(rows[:, col], b[k]), k
