@@ -91,3 +91,45 @@ def test_header_compiles_standalone(tmp_path, compiler, flags):
                    'return ibgpu_create(0, &c) == IBGPU_OK; }\n')
     subprocess.check_call([compiler, *flags, "-Wall", "-Wextra", "-Werror", "-I", INCLUDE,
                            "-c", str(src), "-o", str(tmp_path / "use.o")])
+
+
+def test_invalid_case_parameters_are_rejected_before_any_device_call(pkg):
+    """ibgpu_create validates the case before it touches CUDA, so bad case
+    parameters come back as IBGPU_E_ARG with a reason on any machine."""
+    ib = pkg.ibgpu
+    lib = ib.lib()
+    base = dict(nstages=4, tp=[0.1084, 0.2602, 0.5052, 1.0],
+                initvar=[1.0, 0.5, 0.0, 0.0, 1 / 1.4, 1.0, 0.0], nlevels=1, dh=[[0.1, 0.1, 0.1]],
+                march_step=[1], march_left=[0], step_num=[1.0], domain_nx=32, domain_ny=32)
+
+    def create(case):
+        ctx = ctypes.c_void_p()
+        rc = lib.ibgpu_create(ctypes.byref(case), ctypes.byref(ctx))
+        if ctx:
+            lib.ibgpu_destroy(ctx)
+        return rc, lib.ibgpu_last_error().decode()
+
+    bad = []
+    c = ib.make_case(base)
+    c.abi_version += 1
+    bad.append((c, "ABI version"))
+    for key, val in (("nstages", 0), ("nstages", 5), ("limiter", 2), ("precision", 3),
+                     ("dt_var_step", 0)):
+        c = ib.make_case(base)
+        setattr(c, key, val)
+        bad.append((c, "invalid case parameters"))
+    for nl in (0, ib.MAX_LEVELS + 1):
+        c = ib.make_case(base)
+        c.nlevels = nl
+        bad.append((c, "invalid case parameters"))
+    for field, val in (("march_step", 0), ("dh", 0.0), ("dh", float("nan"))):
+        c = ib.make_case(base)
+        if field == "march_step":
+            c.march_step[0] = val
+        else:
+            c.dh[0][1] = val
+        bad.append((c, "invalid level parameters"))
+    for c, why in bad:
+        rc, msg = create(c)
+        assert rc == ib.E_ARG and why in msg, (why, rc, msg)
+    assert lib.ibgpu_create(None, None) == ib.E_ARG
