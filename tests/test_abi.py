@@ -133,3 +133,28 @@ def test_invalid_case_parameters_are_rejected_before_any_device_call(pkg):
         rc, msg = create(c)
         assert rc == ib.E_ARG and why in msg, (why, rc, msg)
     assert lib.ibgpu_create(None, None) == ib.E_ARG
+
+
+def test_noalloc_entry_point_rejects_unsupported_grids_before_any_device_call(pkg):
+    """The allocation-free step checks its case and grid before it touches
+    the device: anything but one periodic inviscid level with sides that are
+    multiples of 16 and at most IBGPU_NOALLOC_MAX_CELLS cells is IBGPU_E_ARG.
+    (The row addresses are never dereferenced on these paths.)"""
+    ib = pkg.ibgpu
+    base = dict(nstages=4, tp=[0.1084, 0.2602, 0.5052, 1.0],
+                initvar=[1.0, 0.5, 0.0, 0.0, 1 / 1.4, 1.0, 0.0], nlevels=1,
+                dh=[[0.1, 0.1, 0.1]], march_step=[1], march_left=[0], step_num=[1.0],
+                domain_nx=64, domain_ny=64, periodic_x=1, periodic_y=1)
+    fake = 1 << 20  # stands for a device address; not read on the rejected paths
+    cases = [
+        (dict(base, periodic_x=0), 64, 64, "periodic inviscid"),
+        (dict(base, viscous=1), 64, 64, "periodic inviscid"),
+        (dict(base, domain_nx=48), 64, 64, "periodic inviscid"),
+        (dict(base, domain_nx=40, domain_ny=40), 40, 40, "multiple of 16"),
+        (dict(base, domain_nx=512, domain_ny=256), 512, 256, "IBGPU_NOALLOC_MAX_CELLS"),
+    ]
+    for params, nx, ny, why in cases:
+        with pytest.raises(ib.IbgpuError) as e:
+            ib.step_periodic_noalloc(params, 0, nx, ny, fake, fake, 1.0)
+        assert e.value.code == ib.E_ARG and why in str(e.value), (why, str(e.value))
+    assert 512 * 256 > ib.NOALLOC_MAX_CELLS
