@@ -42,3 +42,27 @@ def test_port_baseline_times_the_c_restatement(monkeypatch):
     monkeypatch.setattr(bench, "reference_binary", lambda: None)
     rate, sec, upd, kind = bench.run_reference(32, 4, 3, 1)
     assert kind == "port" and upd == 32 * 32 and sec > 0 and rate == upd / sec
+
+
+def test_slowed_timing_is_measured_once_more():
+    runs = []
+
+    def timed(reasons):
+        def f():
+            runs.append(1)
+            return 1.0 + len(runs), {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0,
+                                     "reasons": reasons if len(runs) == 1 else []}
+        return f
+
+    ident = lambda x: x  # noqa: E731  (one rank)
+    for reasons, again in ((["hw_slowdown"], True), (["sw_thermal_slowdown"], True),
+                           (["sw_power_cap"], False), ([], False)):
+        runs.clear()
+        ms, clocks, remeasured = bench.timed_with_retry(timed(reasons), ident)
+        assert remeasured is again and len(runs) == 1 + again
+        assert ms == 1.0 + len(runs)
+    # another rank's slowdown makes every rank measure again
+    runs.clear()
+    _, _, remeasured = bench.timed_with_retry(timed([]), lambda x: max(x, 1.0))
+    assert remeasured and len(runs) == 2
+    assert not bench.clock_rejected(None)
