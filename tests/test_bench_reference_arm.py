@@ -5,6 +5,7 @@ import io
 import json
 import os
 import sys
+import time
 from contextlib import redirect_stdout
 
 import pytest
@@ -66,3 +67,32 @@ def test_slowed_timing_is_measured_once_more():
     _, _, remeasured = bench.timed_with_retry(timed([]), lambda x: max(x, 1.0))
     assert remeasured and len(runs) == 2
     assert not bench.clock_rejected(None)
+
+
+def test_clock_sampler_reads_clocks_and_reasons(tmp_path, monkeypatch):
+    """The sampler's reading of nvidia-smi's CSV, with a stand-in nvidia-smi on
+    PATH: median SM clock over the loaded samples, the maximum, and the
+    active slowdown reasons by name."""
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\n"
+                    "echo '0, 1965, 1965, 700.0, 0x4, Not Active, Not Active, Not Active, Active'\n"
+                    "echo '0, 1950, 1965, 710.0, 0x4, Not Active, Not Active, Not Active, Active'\n"
+                    "echo '0, 345, 1965, 90.0, 0x0, Not Active, Not Active, Not Active, Not Active'\n"
+                    "echo '0, 1800, 1965, 900.0, 0x8, Active, Not Active, Not Active, Not Active'\n"
+                    "echo 'garbage line'\n"
+                    "sleep 5\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ['PATH']}")
+    s = bench.ClockSampler(0)
+    s.start()
+    deadline = time.monotonic() + 10
+    while time.monotonic() < deadline:  # the stand-in has written its lines
+        with open(s.path) as f:
+            if f.read().count("\n") >= 5:
+                break
+        time.sleep(0.01)
+    c = s.stop()
+    assert c["samples"] == 4 and c["sm_max_mhz"] == 1965.0
+    assert c["sm_mhz"] == 1950.0  # median of the three loaded samples; idle 345 MHz left out
+    assert c["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert bench.clock_rejected(c)
