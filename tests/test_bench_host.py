@@ -1,6 +1,7 @@
-"""The benchmark's reference arm on the host cores (no GPU): one JSON line in
-the benchmark's format, timed from the reference's own step (oracle/_ref)
-or, without it, from the C restatement of the same step."""
+"""Host-side parts of the benchmark (no GPU): the reference arm's JSON line,
+timed from the reference's own step (oracle/_ref) or, without it, from the
+C restatement of the same step; the clock sampler's reading of nvidia-smi;
+and the rule that re-measures a timing slowed by the hardware."""
 import io
 import json
 import os
