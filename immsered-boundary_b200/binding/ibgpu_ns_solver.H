@@ -385,6 +385,14 @@ class GpuNS_Solver : public NS_Solver {
     return IBGPU_OK;
   }
 
+  // A level's refine/coarsen decision for AMR::TagtheBox (after Inittag):
+  // the plain criterion, or with device MLP parameters the learned
+  // indicator reading the device state, which is current after a step.
+  int TagLevel(const ibgpu_tag_rule &rule, AMR &amr, int level, const float *d_params = nullptr) {
+    if (!ctx_) return IBGPU_E_STATE;
+    return IbgpuAdapter::TagLevel(ctx_, rule, a_mesh, amr, level, d_params);
+  }
+
   // Force and moment of every body from the device state
   // (Body::ComptWallForce): 6 per body, force then moment.
   int WallForces(std::vector<double> &out) {
