@@ -40,6 +40,14 @@ REF_BYTES_PER_WORKER = 1.2e9  # resident size of one reference process at the sa
 BATCH_CASES = 64     # batched workload: independent cases, 50k..800k leaf cells each
 REGRID_EVERY = 20    # steps between regrids of the airfoil workloads (learned tagging cost)
 NACA_RECORD = os.path.join(ROOT, "tests", "golden", "naca_minmod_s4_n64_l3.npz")
+# the plain-method airfoil workload at its stated size (128^2 base + 3 AMR
+# levels, 400-point NACA0012, Mach 0.5, 2 deg, Re 5000, minmod, 4 stages,
+# CFL 0.5): the reference's mesh, initial state and 1000-step force history
+CONFIG1_RECORD = os.path.join(ROOT, "tests", "golden", "naca_minmod_s4_n128_l4.npz")
+CONFIG1_HISTORY = os.path.join(ROOT, "tests", "golden", "naca_forces_s1000_n128_l4.npz")
+CONFIG1_ENV = {"IB_NX": "128", "IB_LEVELS": "4", "IB_STAGES": "4", "IB_USER_INIT": "0",
+               "IB_NPTS": "200"}
+F_REF = 0.5 * 1.0 * 0.1  # 0.5 rho_inf u_inf^2 * chord * slab depth (Cl, Cd scale)
 
 
 def load_pkg():
@@ -101,71 +109,153 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(name="stage_kernel_vortex2048.md"):
-    """dram bytes per stage launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", name)
-    if not os.path.exists(p):
+def profile_traffic(key="stage_kernel_fp64_vortex2048"):
+    """DRAM bytes per stage launch (dram__bytes_read.sum + dram__bytes_write.sum
+    of one ncu capture) from profiles/roofline_traffic.json, if recorded."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)[key]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError, TypeError):
         return None
-    for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
+
+
+def pci_bus_id(device: int):
+    """PCI bus id of a CUDA device (CUDA ordinals follow CUDA_VISIBLE_DEVICES
+    and CUDA_DEVICE_ORDER; NVML and nvidia-smi index GPUs their own way, so
+    the bus id is the key both understand), or None when unknown."""
+    try:
+        import torch
+        pr = torch.cuda.get_device_properties(device)
+        return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        return None
+
+
+REASON_NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons of the benchmark's GPU, sampled
+    during the timed region only.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is polled from a thread about every millisecond between start() and
+    stop(), so that a timed region of a few milliseconds still gets samples;
+    the GPU is found by its PCI bus id.  Without NVML, nvidia-smi is polled
+    every 20 ms (the same bus id as --id) and only its samples stamped
+    inside the region count."""
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
+    def __init__(self, device: int, bus_id: str | None = None, interval_s: float = 0.001):
+        self.bus_id = bus_id if bus_id is not None else pci_bus_id(device)
+        self.interval = interval_s
+        self.rows = []  # (host time, sm MHz, set of reason names)
+        self.max_mhz = None
+        self._thread = None
+        self._stop = None
+        self._proc = None
         self.path = None
+        self.t0 = self.t1 = None
+
+    # ---- NVML
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        if self.bus_id is None:
+            raise RuntimeError("no PCI bus id")
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(self.bus_id)
+
+    def _poll(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self._stop.is_set():
+            t = time.perf_counter()
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                break
+            self.rows.append((t, mhz, {n for n, b in bits.items() if mask & b}))
+            self._stop.wait(self.interval)
 
     def start(self):
+        import threading
+        self.rows = []
+        self._stop = threading.Event()
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
+            self._start_smi()
+        self.t0 = time.perf_counter()
+
+    # ---- nvidia-smi fallback
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def _start_smi(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        ident = [f"--id={self.bus_id}"] if self.bus_id else []
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", *ident, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
-            self.proc = None
+            self._proc = None
 
-    def stop(self):
-        if self.proc is None:
-            return None
-        time.sleep(0.3)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
+    def _read_smi(self):
+        import datetime
+        # nvidia-smi stamps in local wall-clock time: map onto perf_counter
+        off = time.time() - time.perf_counter()
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 7:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                mhz, mx = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-        os.unlink(self.path)
-        if not rows:
+            self.max_mhz = max(self.max_mhz or 0.0, mx)
+            self.rows.append((ts - off, mhz, {n for n, f in zip(REASON_NAMES, parts[3:7])
+                                              if f.lower() == "active"}))
+
+    def stop(self):
+        self.t1 = time.perf_counter()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        elif self._proc is not None:
+            time.sleep(0.05)  # a last sample stamped after the region
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+            self._read_smi()
+            os.unlink(self.path)
+        else:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags)
-                          if f.lower() == "active"})
-        mx = max(r[1] for r in rows)
-        loaded = [r[0] for r in rows if r[0] > 0.5 * mx] or [r[0] for r in rows]
+        return self.summary()
+
+    def summary(self):
+        inside = [r for r in self.rows if self.t0 <= r[0] <= self.t1]
+        if not inside:
+            return None
+        mx = self.max_mhz or max(r[1] for r in inside)
+        loaded = [r[1] for r in inside if r[1] > 0.5 * mx] or [r[1] for r in inside]
+        reasons = sorted(set().union(*(r[2] for r in inside)))
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(inside), "window_ms": (self.t1 - self.t0) * 1e3,
+                "source": "nvml" if self._thread is not None else "nvidia-smi",
+                "gpu": self.bus_id}
 
 
 # clock-event reasons that make a timing invalid (sw_power_cap is kept and noted)
@@ -207,6 +297,32 @@ def host_workers(per_worker_bytes: float) -> int:
     return max(1, cores)
 
 
+def run_reference_binary(binary: str, env_case: dict, steps: int, warmup: int, workers: int):
+    """`workers` concurrent single-rank processes of a reference oracle binary
+    on the same case; (rate, longest timed loop s, timed cell updates)."""
+    env = dict(os.environ, IB_STEPS=str(steps), IB_TIMED_FROM=str(warmup), **env_case)
+    with tempfile.TemporaryDirectory() as wd:
+        procs = []
+        for k in range(workers):
+            d = os.path.join(wd, str(k))
+            os.makedirs(d)
+            procs.append(subprocess.Popen([binary], cwd=d, env=env, stdout=subprocess.PIPE,
+                                          stderr=subprocess.DEVNULL, text=True))
+        outs = [p.communicate()[0] for p in procs]
+        if any(p.returncode != 0 for p in procs):
+            raise RuntimeError("reference run failed")
+    secs, upd = [], 0
+    for out in outs:
+        for line in out.splitlines():
+            if line.startswith("ORACLE_RESULT"):
+                r = json.loads(line.split(" ", 1)[1])
+                secs.append(r["loop_seconds"])
+                upd += r["cell_updates"]
+    if len(secs) != workers:
+        raise RuntimeError("reference run printed no result")
+    return upd / max(secs), max(secs), upd
+
+
 def run_reference(n: int, steps: int, warmup: int = 0, workers: int = 1):
     """The reference solver's own step (compiled from its sources with the
     single-rank MPI shim) on the host: `workers` independent single-rank
@@ -219,28 +335,9 @@ def run_reference(n: int, steps: int, warmup: int = 0, workers: int = 1):
     is absent."""
     binary = reference_binary()
     if binary is not None:
-        env = dict(os.environ, IB_NX=str(n), IB_STEPS=str(steps), IB_STAGES=str(STAGES),
-                   IB_TIMED_FROM=str(warmup))
-        with tempfile.TemporaryDirectory() as wd:
-            procs = []
-            for k in range(workers):
-                d = os.path.join(wd, str(k))
-                os.makedirs(d)
-                procs.append(subprocess.Popen([binary], cwd=d, env=env, stdout=subprocess.PIPE,
-                                              stderr=subprocess.DEVNULL, text=True))
-            outs = [p.communicate()[0] for p in procs]
-            if any(p.returncode != 0 for p in procs):
-                raise RuntimeError("reference run failed")
-        secs, upd = [], 0
-        for out in outs:
-            for line in out.splitlines():
-                if line.startswith("ORACLE_RESULT"):
-                    r = json.loads(line.split(" ", 1)[1])
-                    secs.append(r["loop_seconds"])
-                    upd += r["cell_updates"]
-        if len(secs) != workers:
-            raise RuntimeError("reference run printed no result")
-        return upd / max(secs), max(secs), upd, "reference"
+        rate, sec, upd = run_reference_binary(binary, {"IB_NX": str(n), "IB_STAGES": str(STAGES)},
+                                              steps, warmup, workers)
+        return rate, sec, upd, "reference"
     # C restatement of the same step
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
@@ -439,11 +536,89 @@ def learned_section(ib, wl, ind, sols, sizes, stream, batched_ms_per_step):
                           "steps): max |dCd| 2.1e-4, max |dCl| 5.8e-4 vs the plain criterion"}
 
 
-def accuracy_section(ib, wl, stream, n: int = 2048, steps: int = 500, naca_steps: int = 1000):
-    """Config accuracy reports: the 2048^2 vortex after `steps` steps (L2
-    density error vs the exact solution for FP64 and mixed, and mixed vs
-    FP64), and |dCl|, |dCd| of the mixed build vs FP64 on the NACA0012
-    record after `naca_steps` steps."""
+def load_record(path):
+    import numpy as np
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def marched_cells(g, ts0: int, nsteps: int) -> int:
+    """Leaf-cell updates of steps ts0 .. ts0+nsteps-1 of a record's mesh: the
+    normal cells of the levels that march each step (subcycling schedule)."""
+    import numpy as np
+    sched = g["schedule"].reshape(-1, 6)
+    per_level = np.bincount(g["level"][g["kind"] == 0], minlength=len(sched))
+    return int(sum(per_level[l] for ts in range(ts0, ts0 + nsteps) for l in range(len(sched))
+                   if ts % sched[l, 0] == sched[l, 3]))
+
+
+def config1_section(ib, wl, stream, max_over_ranks, timed_steps: int = 400, rank: int = 0):
+    """The plain-method airfoil workload at its stated size (the reference's
+    mesh and initial state): FP64 and mixed leaf-cell updates/s (levels that
+    march only), |dCl|, |dCd| of both over the 1000 steps against the
+    reference's own history, and the reference's step on the same case on
+    the host cores."""
+    import numpy as np
+    import torch
+    g = load_record(CONFIG1_RECORD)
+    hist = load_record(CONFIG1_HISTORY)["history"]
+    period = int(g["schedule"].reshape(-1, 6)[:, 0].max())  # one coarse-level period
+    out = {"workload": "static NACA0012 (400 surface points) on a 128x128 base grid of "
+                       "[0,20]^2 + 3 AMR levels, Mach 0.5, 2 deg, Re 5000, minmod, 4-stage, "
+                       "CFL 0.5; the reference's own mesh and initial state",
+           "leaf_cells": int((g["kind"] == 0).sum()),
+           "cell_updates_per_step": marched_cells(g, 0, period) / period}
+    cl_cd = lambda f: np.asarray(f).reshape(-1, 6)[:, :2].sum(axis=0) / F_REF  # noqa: E731
+    ends = {}
+    for name, prec in (("fp64", ib.FP64), ("mixed", ib.MIXED)):
+        s = wl.naca_solver(g, 0, prec)
+        s.set_stream(stream.cuda_stream)
+        s.run(0, period)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.run(period, timed_steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        s.close()
+        upd = marched_cells(g, period, timed_steps)
+        # accuracy: the stated 1000 steps from the initial state, forces each step
+        s = wl.naca_solver(g, 0, prec)
+        s.set_stream(stream.cuda_stream)
+        worst = np.zeros(2)
+        for k in range(len(hist)):
+            s.time_marching(k)
+            f = s.wall_forces()
+            worst = np.maximum(worst, np.abs(cl_cd(f) - cl_cd(hist[k, 3:])))
+        ends[name] = cl_cd(s.wall_forces())
+        s.close()
+        out[name] = {"value": upd / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / timed_steps,
+                     "timed_steps": timed_steps,
+                     "max_dcd_vs_reference": float(worst[0]), "max_dcl_vs_reference": float(worst[1])}
+    out["cd_cl_reference_step1000"] = cl_cd(hist[-1, 3:]).tolist()
+    out["mixed_vs_fp64_step1000"] = np.abs(ends["mixed"] - ends["fp64"]).tolist()
+    out["gate_1e-3"] = bool(max(out["mixed"]["max_dcd_vs_reference"],
+                                out["mixed"]["max_dcl_vs_reference"]) < 1e-3)
+    out["cl_cd_note"] = ("Cd, Cl = x, y force of both surfaces over 0.5 rho u^2 c dz; max over "
+                         "every step of the 1000-step run against the reference's own history")
+    binary = os.path.join(ROOT, "oracle", "_ref", "ref_naca_minmod")
+    if rank == 0 and os.path.exists(binary):
+        workers = host_workers(0.3e9)
+        rate, sec, upd = run_reference_binary(binary, CONFIG1_ENV, 3 * period, period, workers)
+        out["reference"] = {"value": rate, "unit": UNIT, "cores": workers,
+                            "sample": f"{workers} concurrent single-rank processes of the "
+                                      f"reference's own step on this case, each {2 * period} "
+                                      f"timed steps after {period}; rate = all timed cell "
+                                      f"updates / the longest loop"}
+    return out
+
+
+def accuracy_section(ib, wl, stream, n: int = 2048, steps: int = 500):
+    """The bandwidth workload's accuracy: the 2048^2 vortex after `steps`
+    steps, L2 density error vs the exact solution for FP64 and mixed, and
+    mixed vs FP64 (the airfoil gate is in the config1 section)."""
     import numpy as np
     out = {}
     dens = {}
@@ -467,20 +642,6 @@ def accuracy_section(ib, wl, stream, n: int = 2048, steps: int = 500, naca_steps
         exact = wl.vortex_exact_density(n, tfin[name])
         out[f"vortex_l2_rho_{name}_vs_exact"] = float(np.sqrt(np.mean((dens[name] - exact) ** 2)))
     out["vortex_l2_rho_mixed_vs_fp64"] = float(np.sqrt(np.mean((rho_mixed - rho_fp64) ** 2)))
-    rec = np.load(NACA_RECORD)
-    g = {k: rec[k] for k in rec.files}
-    F_ref = 0.5 * 1.0 * 0.1  # 0.5 rho u^2 * chord * slab depth
-    forces = {}
-    for name, prec in (("fp64", ib.FP64), ("mixed", ib.MIXED)):
-        s = wl.naca_solver(g, 0, prec)
-        s.set_stream(stream.cuda_stream)
-        s.run(0, naca_steps)
-        forces[name] = s.wall_forces()[:, :2].sum(axis=0) / F_ref
-        s.close()
-    d = np.abs(forces["mixed"] - forces["fp64"])
-    out.update({"naca_steps": naca_steps, "naca_cd_fp64": float(forces["fp64"][0]),
-                "naca_cl_fp64": float(forces["fp64"][1]), "naca_dcd_mixed": float(d[0]),
-                "naca_dcl_mixed": float(d[1]), "naca_gate_1e-3": bool(d.max() < 1e-3)})
     return out
 
 
@@ -607,6 +768,7 @@ def our_arm(args):
                                            bat["ms_per_step"])
         for s in bsols:
             s.close()
+        extra["config1"] = config1_section(ib, wl, stream, max_over_ranks, rank=rank)
         if rank == 0:
             extra["accuracy"] = accuracy_section(ib, wl, stream, n=n)
 
@@ -666,7 +828,120 @@ def our_arm(args):
     return 0
 
 
-def main():
+def profile_run(args):
+    """A short run of one workload on cuda:0, as the command under ncu:
+      stage     --n N --steps K --precision P  the periodic vortex, K full
+                steps after one (kernel of interest: stage_kernel)
+      batch     --cases C --grid G --precision P  C batched vortex cases
+                (50k..800k cells, seed 0)
+      mlp-grad  --rows R --steps K  K learned-indicator training steps on R
+                random BF16 rows (mlp_grad_kernel)
+      mlp-tag   --n N --steps K  learned tagging of every cell of an N x N
+                vortex case (mlp_tag_mesh_kernel)
+    Prints the mean wall time per step; no JSON line."""
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    ib, wl, ind = pkg.ibgpu, pkg.workloads, pkg.indicator
+    prec = {"fp64": ib.FP64, "exact": ib.FP64_EXACT, "mixed": ib.MIXED}[args.precision]
+    k = max(args.steps, 1)
+    if args.profile == "stage":
+        P, cells, prim = wl.vortex_case(args.n, precision=prec)
+        sol = ib.FlowSolver(P)
+        sol.upload_topology(**cells)
+        sol.init_flow(prim)
+        sol.time_marching(0)
+        t0 = time.perf_counter()
+        sol.run(1, k)
+        dt = (time.perf_counter() - t0) / k
+        print(f"{args.n}x{args.n} {args.precision}: {dt * 1e3:.3f} ms/step (wall, {k} steps)")
+        sol.close()
+    elif args.profile == "batch":
+        sols = []
+        for P, cells, prim in wl.batch_vortex_cases(args.cases, seed=0, precision=prec):
+            s = ib.FlowSolver(P)
+            s.upload_topology(**cells)
+            s.init_flow(prim)
+            sols.append(s)
+        b = ib.Batch(sols)
+        b.set_grid(args.grid)
+        b.run(0, 1)
+        t0 = time.perf_counter()
+        b.run(1, k)
+        dt = (time.perf_counter() - t0) / k
+        ncell = sum(s.ncells for s in sols)
+        print(f"batch of {args.cases} cases ({ncell} cells) {args.precision}: {dt * 1e3:.3f} "
+              f"ms/step (wall), {b.info()}")
+        b.close()
+        for s in sols:
+            s.close()
+    elif args.profile == "mlp-grad":
+        P, cells, prim = wl.vortex_case(64)
+        sol = ib.FlowSolver(P)
+        rng = np.random.default_rng(0)
+        X = rng.normal(0, 1, (args.rows, ib.MLP_IN)).astype(np.float32)
+        feat = torch.from_numpy((X.view(np.uint32) >> 16).astype(np.uint16).view(np.int16)).cuda()
+        y = rng.integers(0, 3, args.rows).astype(np.uint8)
+        li = ind.LearnedIndicator(sol, seed=0)
+        li.train(feat, y, steps=2, batch=args.rows)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        li.train(feat, y, steps=k, batch=args.rows)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / k
+        print(f"{args.rows} rows: {dt * 1e3:.3f} ms per training step (wall)")
+        sol.close()
+    else:  # mlp-tag
+        P, cells, prim = wl.vortex_case(args.n)
+        sol = ib.FlowSolver(P)
+        sol.upload_topology(**cells)
+        sol.init_flow(prim)
+        li = ind.LearnedIndicator(sol, seed=0)
+        rule = wl.naca_tag_rule(1, [10.0 / args.n])
+        sol.tag_mesh(rule, li.params.data_ptr())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            tags = sol.tag_mesh(rule, li.params.data_ptr())
+        dt = (time.perf_counter() - t0) / k
+        print(f"{args.n}x{args.n}: {dt * 1e3:.3f} ms per ibgpu_tag_mesh call, tag counts "
+              f"{np.bincount(tags, minlength=4).tolist()}")
+        sol.close()
+    return 0
+
+
+def spawn_ranks(n: int, cmd: list, extra_env: dict | None = None, timeout: float = 3600.0):
+    """Run cmd as n ranks of one job on this node (RANK, LOCAL_RANK,
+    WORLD_SIZE, MASTER_ADDR/PORT set per process, 127.0.0.1 rendezvous);
+    the ranks share this process's stdout.  Returns the exit codes; every
+    rank is stopped when one fails or the time runs out."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n),
+                   LOCAL_WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                   **(extra_env or {}))
+        procs.append(subprocess.Popen(cmd, env=env))
+    deadline = time.monotonic() + timeout
+    codes = [None] * n
+    while any(c is None for c in codes):
+        for i, p in enumerate(procs):
+            if codes[i] is None:
+                codes[i] = p.poll()
+        if any(c not in (None, 0) for c in codes) or time.monotonic() > deadline:
+            for i, p in enumerate(procs):
+                if codes[i] is None:
+                    p.kill()
+                    codes[i] = p.wait()
+            break
+        time.sleep(0.05)
+    return codes
+
+
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -675,10 +950,30 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
-                    help="skip the batched, learned-indicator and accuracy sections")
-    args = ap.parse_args()
+                    help="skip the batched, learned-indicator, airfoil and accuracy sections")
+    ap.add_argument("--profile", choices=["stage", "batch", "mlp-grad", "mlp-tag"],
+                    help="instead of the benchmark: a short run of one workload as the command "
+                         "under a profiler (see profile_run)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "exact", "mixed"])
+    ap.add_argument("--cases", type=int, default=16, help="--profile batch: batched cases")
+    ap.add_argument("--grid", type=int, default=-1,
+                    help="--profile batch: CTA count of the merged launches (0 one per item, "
+                         "-1 autotuned)")
+    ap.add_argument("--rows", type=int, default=262144, help="--profile mlp-grad: rows")
+    args = ap.parse_args(argv)
+    if args.profile:
+        return profile_run(args)
     if args.warmup < 3:
         args.warmup = 3
+    ws_env = os.environ.get("WORLD_SIZE")
+    if ws_env is None and args.gpus > 1:
+        # launched without a launcher: one rank per GPU on this node
+        codes = spawn_ranks(args.gpus, [sys.executable, os.path.abspath(__file__),
+                                        *(argv if argv is not None else sys.argv[1:])])
+        return max(abs(c) for c in codes)
+    if ws_env is not None and int(ws_env) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={ws_env}", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

@@ -276,22 +276,23 @@ struct IbgpuAdapter {
     }
   }
 
-  // The tagging loops of a case's AMR::TagtheBox (Userfunction_cy_naca15.cpp
-  // :560-635) for one level through the C ABI: the plain criterion
-  // (ibgpu_tag_plain) or, with device MLP parameters, the learned indicator
-  // (ibgpu_tag_learned, reading the context's uploaded state); the decisions
-  // land in m_tag / taggedbox as the loops leave them.  Call after
-  // Inittag(); CheckDetagLocation stays the caller's.
-  static int TagLevel(ibgpu_ctx *ctx, const ibgpu_tag_rule &rule, Mesh &mesh, AMR &amr,
-                      int level, const float *d_params) {
-    TagBoxes T;
-    GatherTagBoxes(mesh, amr, level, T);
-    const ibgpu_tag_cells q = {(int64_t)T.box.size(), T.level.data(), T.ix.data(), T.iy.data(),
-                               T.xc.data(), T.yc.data(), T.signdis.data()};
-    std::vector<uint8_t> bits(T.box.size());
-    const int rc = d_params ? ibgpu_tag_learned(ctx, &rule, &q, d_params, bits.data())
-                            : ibgpu_tag_plain(ctx, &rule, &q, bits.data());
-    if (rc) return rc;
+  // The case's regions with the requests of this regrid for `level`: the
+  // reference's AMR::TagtheBox acts only when the level's own
+  // AMRLevel::torefine / toderefine are set (Userfunction_cy_naca15.cpp:557,
+  // 590), and ADPRule / SetRefineFlag set them level by level, so a rule
+  // built once for the case never decides the request itself.
+  static ibgpu_tag_rule LevelRule(const ibgpu_tag_rule &rule, AMR &amr, int level) {
+    ibgpu_tag_rule r = rule;
+    if (level >= 0 && level < IBGPU_TAG_MAX_LEVELS) {
+      r.torefine[level] = amr.m_level[level].torefine ? 1 : 0;
+      r.toderefine[level] = amr.m_level[level].toderefine ? 1 : 0;
+    }
+    return r;
+  }
+
+  // Decisions (IBGPU_TAG_* bits of the boxes T) into m_tag / taggedbox, as
+  // the tagging loops leave them.
+  static void ApplyTags(AMR &amr, int level, const TagBoxes &T, const std::vector<uint8_t> &bits) {
     AMRLevel &al = amr.m_level[level];
     for (size_t k = 0; k < bits.size(); ++k) {
       const int i = T.box[k];
@@ -301,6 +302,27 @@ struct IbgpuAdapter {
       }
       if (bits[k] & IBGPU_TAG_COARSEN) al.m_tag[i].givedetag();
     }
+  }
+
+  // The tagging loops of a case's AMR::TagtheBox (Userfunction_cy_naca15.cpp
+  // :560-635) for one level through the C ABI: the plain criterion
+  // (ibgpu_tag_plain) or, with device MLP parameters, the learned indicator
+  // (ibgpu_tag_learned, reading the context's uploaded state), with the
+  // level's own refine / coarsen requests (LevelRule); the decisions land in
+  // m_tag / taggedbox as the loops leave them.  Call after Inittag();
+  // CheckDetagLocation stays the caller's.
+  static int TagLevel(ibgpu_ctx *ctx, const ibgpu_tag_rule &rule, Mesh &mesh, AMR &amr,
+                      int level, const float *d_params) {
+    TagBoxes T;
+    GatherTagBoxes(mesh, amr, level, T);
+    const ibgpu_tag_rule lr = LevelRule(rule, amr, level);
+    const ibgpu_tag_cells q = {(int64_t)T.box.size(), T.level.data(), T.ix.data(), T.iy.data(),
+                               T.xc.data(), T.yc.data(), T.signdis.data()};
+    std::vector<uint8_t> bits(T.box.size());
+    const int rc = d_params ? ibgpu_tag_learned(ctx, &lr, &q, d_params, bits.data())
+                            : ibgpu_tag_plain(ctx, &lr, &q, bits.data());
+    if (rc) return rc;
+    ApplyTags(amr, level, T, bits);
     return IBGPU_OK;
   }
 

@@ -358,9 +358,9 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
   MPI_Barrier(share_comm);
   CheckDetagLocation(ilevel);
   // the attach-box consistency check belongs to mesh generation (ts == 0);
-  // the tag dump's pass 1 and runtime regrids re-judge a finished mesh,
+  // the tag dump's passes >= 1 and runtime regrids re-judge a finished mesh,
   // whose attach boxes live one level up
-  if (ts == 0 && !(g_oracle_tag_dump && g_oracle_tag_pass == 1) && refine && morelevel &&
+  if (ts == 0 && !(g_oracle_tag_dump && g_oracle_tag_pass >= 1) && refine && morelevel &&
       ilevel == m_mesh.MyCurNum() - 2) {
     int l0 = m_mesh.MyCurNum() - 2;
     for (size_t i = 0; i < abody.size(); ++i) abody[i].CheckAttachBoxTag(m_level[l0].m_tag, l0, m_mesh);

@@ -18,7 +18,8 @@
 // IB_TAG_SERVER=<dir> (runtime regrids of the case file: write the state the
 // tag server decides from to <dir>/state_<ts>.bin before each regrid),
 // IB_DUMP=<prefix> (write <prefix>_<step>.bin for the initial state and after
-// each step listed by IB_DUMP_EVERY, default every step), IB_FORCES=1 (static
+// each step listed by IB_DUMP_EVERY, default every step, or only after the
+// step counts IB_DUMP_AT lists), IB_FORCES=1 (static
 // body: compute wall forces each step, Body::ComptWallForce), IB_FORCE_LOG=<file>
 // (the per-step force history).
 #include <algorithm>
@@ -471,6 +472,47 @@ int main(int argc, char **argv) {
     d.f64("tag_yc", tyc);
     d.f64("tag_signdis", tsd);
   }
+  // IB_BINDING_TAGCHECK=<dir>: for every level and every request the regrid
+  // can make of it (refine only, coarsen only, both), the case's TagtheBox
+  // decisions (tag dump rows, pass 2 + 3 * level + request) and the
+  // refine / coarsen flags of the rule the binding's TagLevel hands the GPU
+  // for that level (IbgpuAdapter::LevelRule of the case rule in
+  // <dir>/rule.bin), one row (pass, level, torefine, toderefine) per request
+  const char *tc = std::getenv("IB_BINDING_TAGCHECK");
+  if (tc && *tc) {
+    const std::string dir(tc);
+    ibgpu_tag_rule base;
+    FILE *rf = std::fopen((dir + "/rule.bin").c_str(), "rb");
+    if (!rf || std::fread(&base, sizeof base, 1, rf) != 1) {
+      std::fprintf(stderr, "IB_BINDING_TAGCHECK: cannot read rule.bin\n");
+      return 4;
+    }
+    std::fclose(rf);
+    g_oracle_tag_dump = std::fopen((dir + "/tags.bin").c_str(), "wb");
+    std::vector<int32_t> flags;
+    const int req[3][2] = {{1, 0}, {0, 1}, {1, 1}};
+    for (int l = 0; l < mesh.MyCurNum(); ++l)
+      for (int c = 0; c < 3; ++c) {
+        for (int k = 0; k < mesh.MyCurNum(); ++k) {
+          amr.m_level[k].torefine = false;
+          amr.m_level[k].toderefine = false;
+        }
+        amr.m_level[l].torefine = req[c][0] != 0;
+        amr.m_level[l].toderefine = req[c][1] != 0;
+        g_oracle_tag_pass = 2 + 3 * l + c;
+        amr.TagtheBox(l, sphere);
+        const ibgpu_tag_rule lr = IbgpuAdapter::LevelRule(base, amr, l);
+        flags.insert(flags.end(), {g_oracle_tag_pass, l, lr.torefine[l], lr.toderefine[l]});
+        amr.m_level[l].torefine = false;
+        amr.m_level[l].toderefine = false;
+        amr.m_level[l].Inittag();
+        amr.m_level[l].taggedbox.clear();
+      }
+    std::fclose(g_oracle_tag_dump);
+    g_oracle_tag_dump = nullptr;
+    Dump d(dir + "/levelrule.bin");
+    d.i32("levelrule", flags);
+  }
 #endif
 
   // IB_BINDING_STEP=1: the loop steps through the binding on the GPU (FP64
@@ -484,7 +526,9 @@ int main(int argc, char **argv) {
     std::exit(3);
   };
   if (gpu_step) {
-    gpu_check(flowsolver.Create(kLimiter, IBGPU_FP64), "ibgpu_create");
+    // IB_BINDING_PRECISION: IBGPU_FP64 (default), IBGPU_FP64_EXACT or IBGPU_MIXED
+    gpu_check(flowsolver.Create(kLimiter, env_int("IB_BINDING_PRECISION", IBGPU_FP64)),
+              "ibgpu_create");
     gpu_check(flowsolver.Upload(amr, sphere), "upload");
     flowsolver.on_gpu = true;
   }
@@ -495,6 +539,18 @@ int main(int argc, char **argv) {
   const int nsteps = env_int("IB_STEPS", 5);
   const int timed_from = env_int("IB_TIMED_FROM", 0);  // steps before this are warm-up
   const int every = env_int("IB_DUMP_EVERY", 1);
+  // IB_DUMP_AT=<a,b,...>: dump only after these step counts (0 = the initial
+  // state) instead of every IB_DUMP_EVERY steps
+  std::vector<int> dump_at;
+  if (const char *at = std::getenv("IB_DUMP_AT")) {
+    std::stringstream ss(at);
+    std::string item;
+    while (std::getline(ss, item, ',')) if (!item.empty()) dump_at.push_back(std::atoi(item.c_str()));
+  }
+  auto dump_now = [&](int step, bool last) {
+    if (!dump_at.empty()) return std::find(dump_at.begin(), dump_at.end(), step) != dump_at.end();
+    return step == 0 || step % every == 0 || last;
+  };
   const bool forces_on = env_int("IB_FORCES", 0) != 0;
   const char *prefix = std::getenv("IB_DUMP");
   // IB_FORCE_LOG=<file>: per step ts, t, dt and the forces/moments of every
@@ -511,7 +567,7 @@ int main(int argc, char **argv) {
     std::snprintf(buf, sizeof buf, "_%06d.bin", step);
     dump_state(std::string(prefix) + buf, mesh, flowsolver, forces);
   };
-  do_dump(0);
+  if (dump_now(0, false)) do_dump(0);
 
   double loop_time = 0.0;
   long long cell_updates = 0;
@@ -567,7 +623,7 @@ int main(int argc, char **argv) {
 #endif
     }
     adpflag = false;
-    if (prefix && (ts % every == 0 || s == nsteps - 1)) do_dump(ts);
+    if (prefix && dump_now(ts, s == nsteps - 1)) do_dump(ts);
   }
   if (flog) std::fclose(flog);
   std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "

@@ -5,7 +5,7 @@ sources by ``make -C oracle``) on small cases and packs their state dumps
 into compressed .npz files next to this script.  The fixtures pin both the
 C restatement of the step (oracle/ib_oracle.c) and the GPU path.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference dir> && python tests/golden/make_golden.py
 
 Each fixture holds the box list of the z = 0 plane (level, ix, iy, kind,
 ptype, solid, infect, signdis), the case constants, and the primitive state
@@ -14,6 +14,7 @@ step.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -29,6 +30,10 @@ import pyoracle  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref")
 
+# the plain-method airfoil workload at its stated size
+CONFIG1_ENV = {"IB_NX": "128", "IB_LEVELS": "4", "IB_STAGES": "4", "IB_USER_INIT": "0",
+               "IB_FORCES": "1", "IB_NPTS": "200"}
+
 # name -> (binary, environment, number of steps)
 CASES = {
     "vortex_vanleer_s4_n32": ("ref_vortex_vanleer", {"IB_NX": "32", "IB_STAGES": "4"}, 4),
@@ -39,6 +44,10 @@ CASES = {
     "naca_minmod_s4_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
                                                   "IB_STAGES": "4", "IB_USER_INIT": "0",
                                                   "IB_FORCES": "1", "IB_NPTS": "120"}, 4),
+    # the plain-method airfoil workload at its stated size: 128^2 base + 3 AMR
+    # levels (~45k leaf cells), 400-point NACA0012, Mach 0.5, 2 deg, Re 5000,
+    # minmod, 4 stages, CFL 0.5: the mesh, the initial state and two steps
+    "naca_minmod_s4_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, 2),
 }
 # plain tag criterion only (TagtheBox on the initial mesh, refine and coarsen
 # requested on every level): name -> (binary, environment)
@@ -52,6 +61,15 @@ FORCE_CASES = {
     "naca_forces_s400_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
                                                    "IB_STAGES": "4", "IB_USER_INIT": "0",
                                                    "IB_FORCES": "1", "IB_NPTS": "120"}, 400),
+    # the stated 1000 steps of the plain-method airfoil workload
+    "naca_forces_s1000_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, 1000),
+}
+# states of a developed flow, too large to commit (about 1 MB each): the
+# fixture records the SHA-256 of each dumped state's bytes and its scalars,
+# and live_states() regenerates them with the same binary and checks the
+# digests: name -> (binary, environment, dumped step counts)
+STATE_DIGEST_CASES = {
+    "naca_states_s600_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, (600, 601, 602, 603, 604)),
 }
 # per-case records that do not change between dumps of a static mesh
 AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
@@ -148,10 +166,68 @@ def run_force_case(name: str, binary: str, env: dict, steps: int) -> str:
         shutil.rmtree(work, ignore_errors=True)
 
 
+def _dump_states(binary: str, env: dict, at, work: str) -> list:
+    e = dict(os.environ)
+    e.update(env)
+    e["IB_STEPS"] = str(max(at))
+    e["IB_DUMP"] = os.path.join(work, "d")
+    e["IB_DUMP_AT"] = ",".join(str(k) for k in (0,) + tuple(at))
+    subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
+                   stdout=subprocess.DEVNULL)
+    return [pyoracle.read_dump(os.path.join(work, f"d_{k:06d}.bin")) for k in (0,) + tuple(at)]
+
+
+def _digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def run_state_digest_case(name: str, binary: str, env: dict, at) -> str:
+    """SHA-256 of the prim rows of every dumped step, and its scalars."""
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        snaps = _dump_states(binary, env, at, work)[1:]
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, steps=np.array(at, np.int64),
+                            digests=np.array([_digest(s["prim"]) for s in snaps]),
+                            scalars=np.stack([s["scalars"] for s in snaps]))
+        return path
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def live_states(name: str) -> dict:
+    """The states a STATE_DIGEST_CASES fixture records, regenerated by its
+    reference binary and checked against the recorded digests; returned in
+    the layout of ``load`` (mesh lists, prim and scalars per dumped step)."""
+    binary, env, at = STATE_DIGEST_CASES[name]
+    rec = load(name)
+    work = tempfile.mkdtemp(prefix="live_")
+    try:
+        snaps = _dump_states(binary, env, at, work)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    for s, want, k in zip(snaps[1:], rec["digests"], at):
+        if _digest(s["prim"]) != str(want):
+            raise RuntimeError(f"{name}: the live reference run differs from the recorded one "
+                               f"at step {k}")
+    out = {k: snaps[0][k] for k in STATIC}
+    for k in ("dh", "schedule", "initvar", "domain") + AUX:
+        if k in snaps[0]:
+            out[k] = snaps[0][k]
+    out["prim"] = np.stack([s["prim"].reshape(-1, 7) for s in snaps[1:]])
+    out["scalars"] = np.stack([s["scalars"] for s in snaps[1:]])
+    out["forces"] = np.stack([s["forces"] for s in snaps[1:]])
+    out["steps"] = np.array(at)
+    return out
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(TAG_CASES) + list(FORCE_CASES)
+    names = sys.argv[1:] or (list(CASES) + list(TAG_CASES) + list(FORCE_CASES) +
+                             list(STATE_DIGEST_CASES))
     for n in names:
-        if n in TAG_CASES:
+        if n in STATE_DIGEST_CASES:
+            print(run_state_digest_case(n, *STATE_DIGEST_CASES[n]))
+        elif n in TAG_CASES:
             print(run_tag_case(n, *TAG_CASES[n]))
         elif n in FORCE_CASES:
             print(run_force_case(n, *FORCE_CASES[n]))

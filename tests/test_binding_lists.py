@@ -137,3 +137,57 @@ def test_binding_tag_boxes_are_the_ones_tagthebox_judges():
         assert np.array_equal(rows[:, col].astype(np.int32), b[k]), k
     for col, k in ((3, "tag_xc"), (4, "tag_yc"), (5, "tag_signdis")):
         assert np.array_equal(rows[:, col], b[k]), k
+
+
+def test_binding_tag_rule_takes_each_levels_requests():
+    """TagLevel hands the GPU the case's regions with the requests the
+    regrid made of that level (AMRLevel::torefine / toderefine), not the
+    rule's own: for every level and every request (refine only, coarsen
+    only, both) the plain criterion with the binding's level rule reproduces
+    the case's AMR::TagtheBox decisions box for box, although the case rule
+    it starts from requests both on every level."""
+    pkg = load_pkg()
+    ib, wl = pkg.ibgpu, pkg.workloads
+    import indicator_oracle as io
+    work = tempfile.mkdtemp(prefix="binding_tagcheck_")
+    nlev = int(CASE_ENV["IB_LEVELS"])
+    env = dict(os.environ, **CASE_ENV, IB_DUMP=os.path.join(work, "d"),
+               IB_BINDING_TAGCHECK=work)
+    # the base rule: every level asks for both (what a rule built once holds)
+    out = subprocess.run([BINARY], cwd=work, env=dict(env, IB_BINDING_TAGCHECK=""),
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d0 = pyoracle.read_dump(os.path.join(work, "d_000000.bin"))
+    dh = d0["dh"].reshape(-1, 3)[:, 0]
+    base = wl.naca_tag_rule(nlev, dh)
+    assert base["torefine"][:nlev].all() and base["toderefine"][1:nlev].all()
+    with open(os.path.join(work, "rule.bin"), "wb") as f:
+        f.write(bytes(ib.make_tag_rule(base)))
+    out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    rows = np.fromfile(os.path.join(work, "tags.bin"), np.float64).reshape(-1, 9)
+    lr = pyoracle.read_dump(os.path.join(work, "levelrule.bin"))["levelrule"].reshape(-1, 4)
+    assert len(lr) == 3 * nlev
+    req = {0: (1, 0), 1: (0, 1), 2: (1, 1)}
+    changed = 0
+    for pas, level, tor, toder in lr:
+        assert (tor, toder) == req[(pas - 2) % 3], (pas, level, tor, toder)
+        r = rows[rows[:, 8] == pas]
+        if len(r):
+            want = io.tags_from_rftag(r[:, 6], r[:, 7])
+        else:  # TagtheBox returned before its loops: every box keeps
+            r = rows[rows[:, 8] == 2 + 3 * level]
+            want = np.zeros(len(r), np.uint8)
+        assert len(r) and np.all(r[:, 0] == level)
+        rule = {k: (np.array(v) if isinstance(v, np.ndarray) else v) for k, v in base.items()}
+        rule["torefine"] = base["torefine"].copy()
+        rule["toderefine"] = base["toderefine"].copy()
+        rule["torefine"][level] = tor
+        rule["toderefine"][level] = toder
+        got = io.tag_plain(rule, r[:, 0].astype(int), r[:, 3], r[:, 4], r[:, 5])
+        assert np.array_equal(got, want), (pas, level, int(np.sum(got != want)))
+        # the base rule alone would have decided differently wherever the
+        # request withholds refinement or coarsening
+        changed += int(np.sum(io.tag_plain(base, r[:, 0].astype(int), r[:, 3], r[:, 4],
+                                           r[:, 5]) != want))
+    assert changed > 0
