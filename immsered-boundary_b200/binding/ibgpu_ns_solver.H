@@ -142,16 +142,27 @@ struct IbgpuAdapter {
     v.push_back(bx.iy());
   }
 
+  // IBGPU_CELL_* flags of box b of level l as the mesh holds it now.
+  static uint8_t BoxFlags(Mesh &mesh, int l, int b) {
+    const int nlev = mesh.MyCurNum();
+    DataArray<Box> &boxes = mesh.ShowLevelBox(l);
+    Box &bx = boxes[b];
+    int infect = -1;
+    if (l == nlev - 1 && mesh.Infectboxnum() > b) infect = mesh.BoxInfectIndex(b);
+    const int nnorm = boxes.size();
+    return CellFlags(b < nnorm, b >= nnorm && bx.type == Blockghost, bx.solid, infect == -1,
+                     bx.pair.signdis, Body::Bodynum() > 0 && l == nlev - 1);
+  }
+
   static void Flatten(Mesh &mesh, AMR &amr, std::vector<Body> &bodies, NS_Solver &solver,
                       IbgpuLists &L) {
     L = IbgpuLists();
     const int nlev = mesh.MyCurNum();
-    const bool with_bodies = Body::Bodynum() > 0;
     // cells: Meshlevel::m_box / m_data (Meshlevel.H:688-872)
     for (int l = 0; l < nlev; ++l) {
       DataArray<Box> &boxes = mesh.ShowLevelBox(l);
       DataArray<FlowVariables> &data = mesh.LevelDataArray(l);
-      const int nreal = boxes.realsize(), nnorm = boxes.size();
+      const int nreal = boxes.realsize();
       for (int b = 0; b < nreal; ++b) {
         Box &bx = boxes[b];
         if (bx.iz() != 0) continue;
@@ -159,11 +170,7 @@ struct IbgpuAdapter {
         L.ix.push_back(bx.ix());
         L.iy.push_back(bx.iy());
         L.box.push_back(b);
-        int infect = -1;
-        if (l == nlev - 1 && mesh.Infectboxnum() > b) infect = mesh.BoxInfectIndex(b);
-        L.flags.push_back(CellFlags(b < nnorm, b >= nnorm && bx.type == Blockghost, bx.solid,
-                                    infect == -1, bx.pair.signdis,
-                                    with_bodies && l == nlev - 1));
+        L.flags.push_back(BoxFlags(mesh, l, b));
         FlowVariables &fv = data[b];
         const double r[7] = {fv.roe, fv.u, fv.v, fv.w, fv.p, fv.T, fv.e};
         L.prim.insert(L.prim.end(), r, r + 7);
@@ -206,6 +213,18 @@ struct IbgpuAdapter {
     }
     L.backpressure = B.backpressure;
     L.inlet_flow_angle = inlet_flow_angle;
+    FlattenImmersed(mesh, bodies, L);
+  }
+
+  // The immersed-boundary cells and wall patches of the bodies where they
+  // are now (replaces L's records of that kind).
+  static void FlattenImmersed(Mesh &mesh, std::vector<Body> &bodies, IbgpuLists &L) {
+    L.ib_cell.clear();
+    L.ib_cellf.clear();
+    L.patch.clear();
+    L.patchf.clear();
+    L.body_center.clear();
+    const int nlev = mesh.MyCurNum();
     // immersed-boundary cells of the finest level (IBCell, Body.cpp:1361-1496)
     const int last = nlev - 1;
     DataArray<IBCell> &mdis = mesh.ibarray();
@@ -326,6 +345,58 @@ struct IbgpuAdapter {
     return IBGPU_OK;
   }
 
+  // Body::MovingBody_Image (Bodymove.cpp:37-125) for a run whose state lives
+  // on the device: the bodies' forces and moments come from the device
+  // (ibgpu_wall_forces, the wall patches as the last upload left them: the
+  // reference's Body::ComptWallForce of the same patches), paired over the
+  // two surfaces of each profile as the reference pairs them; then the
+  // reference's own motion rule and re-immersion (wall distances of every
+  // level, removed and newly infected immersed-boundary cells, image points),
+  // and the patches' image-point stencils at the new position
+  // (Body::FindPatchHangingNode, which the reference's next ComptWallForce
+  // would run first).  The caller then hands the device the new flags and
+  // records (GpuNS_Solver::UploadImmersion).
+  static int MoveBodies(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody, double &dt00) {
+    const int nlev = amesh.MyCurNum();
+    const int last = nlev - 1;
+    std::vector<std::vector<int> > in_to_out(nlev), out_to_in(nlev);
+    gridisnew = true;
+    const int bn = (int)abody.size();
+    std::vector<double> fm(6 * (size_t)bn);
+    if (bn > 0) {
+      const int rc = ibgpu_wall_forces(ctx, fm.data());
+      if (rc) return rc;
+    }
+    for (int i = 0; i < bn; ++i)
+      for (int k = 0; k < 3; ++k) {
+        abody[i].draglift(k) = fm[6 * i + k];
+        abody[i].bodymoment(k) = fm[6 * i + 3 + k];
+      }
+    for (int i = 0; i < bn / 2; ++i)
+      for (int k = 0; k < 3; ++k) {
+        abody[2 * i].draglift(k) += abody[2 * i + 1].draglift(k);
+        abody[2 * i + 1].draglift(k) = abody[2 * i].draglift(k);
+        abody[2 * i].bodymoment(k) += abody[2 * i + 1].bodymoment(k);
+        abody[2 * i + 1].bodymoment(k) = abody[2 * i].bodymoment(k);
+      }
+    for (int i = 0; i < bn; ++i) {
+      abody[i].Motion_Rule(amesh, dt00);
+      abody[i].ModifyBoxtoPatch(amesh);
+    }
+    for (int l = 0; l < nlev; ++l) Body::RenewLevelDistance(amesh, abody, l, in_to_out[l], out_to_in[l]);
+    for (int l = 0; l < nlev; ++l) amesh.SynNormal_BlockDistance(l, in_to_out[l], out_to_in[l]);
+    Body::RemoveIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
+    Body::InfectNewIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
+    amesh.m_dis.holeplan(true);
+    amesh.m_dis.CompressArray();
+    amesh.RenewInfectIndex();
+    Body::FindImageCell(amesh, abody);
+    amesh.DataExchangeCells_Wall();
+    Body::FindImageCell_GhostIBCell(amesh, abody);
+    for (int i = 0; i < bn; ++i) abody[i].FindPatchHangingNode(amesh);
+    return IBGPU_OK;
+  }
+
   // The lists and the state into a context (ibgpu_upload_*).
   static int Upload(ibgpu_ctx *ctx, const IbgpuLists &L) {
     ibgpu_cells cells = {(int64_t)L.level.size(), L.level.data(), L.ix.data(), L.iy.data(),
@@ -339,11 +410,15 @@ struct IbgpuAdapter {
                    (int)(L.facevar.size() / 7), L.facevar.data(), L.backpressure,
                    L.inlet_flow_angle};
     if ((rc = ibgpu_upload_boundaries(ctx, &bc))) return rc;
+    if ((rc = UploadIB(ctx, L))) return rc;
+    return ibgpu_upload_state(ctx, L.prim.data());
+  }
+
+  static int UploadIB(ibgpu_ctx *ctx, const IbgpuLists &L) {
     ibgpu_ib ib = {(int64_t)L.ib_cell.size() / 18, L.ib_cell.data(), L.ib_cellf.data(),
                    (int64_t)L.patch.size() / 17, L.patch.data(), L.patchf.data(),
                    (int)(L.body_center.size() / 3), L.body_center.data()};
-    if ((rc = ibgpu_upload_ib(ctx, &ib))) return rc;
-    return ibgpu_upload_state(ctx, L.prim.data());
+    return ibgpu_upload_ib(ctx, &ib);
   }
 };
 
@@ -372,6 +447,34 @@ class GpuNS_Solver : public NS_Solver {
     if (!ctx_) return IBGPU_E_STATE;
     IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
     return IbgpuAdapter::Upload(ctx_, lists_);
+  }
+
+  // The moving-body part of Body::IBConditions_Image (Body.cpp:1352-1357)
+  // for a run stepping on the device: call before TimeMarching each step
+  // when the case moves its bodies (moveflag).  It accumulates dt00 as the
+  // reference does, moves and re-immerses the bodies on the host
+  // (IbgpuAdapter::MoveBodies) and hands the device the new cell flags and
+  // immersed-boundary records; the state stays on the device.
+  int MoveBodies(std::vector<Body> &bodies, double &dt00) {
+    if (!ctx_) return IBGPU_E_STATE;
+    dt00 += dt;
+    int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00);
+    if (rc) return rc;
+    dt00 = 0.0;
+    return UploadImmersion(bodies);
+  }
+
+  // After the bodies moved without a regrid: the flags of the same cell rows
+  // (ibgpu_update_flags) and the immersed-boundary records
+  // (ibgpu_upload_ib) from the mesh as it is now.
+  int UploadImmersion(std::vector<Body> &bodies) {
+    if (!ctx_) return IBGPU_E_STATE;
+    for (size_t i = 0; i < lists_.box.size(); ++i)
+      lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
+    int rc = ibgpu_update_flags(ctx_, lists_.flags.data());
+    if (rc) return rc;
+    IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
+    return IbgpuAdapter::UploadIB(ctx_, lists_);
   }
 
   // One step: ghost fills, CFL dt every dt_var_step steps, the stages and

@@ -92,6 +92,11 @@ struct ibgpu_ctx {
   std::vector<int> level_tile_begin, level_tile_count;  // per level
   std::vector<int64_t> level_normal_cells;
   std::vector<int32_t> h_slot_level, h_slot_ix, h_slot_iy;  // slot -> position (abort reports)
+  // the last topology upload on the host, for flag updates of the same list:
+  // each row's slot, its layout bits (PRESENT / NORMAL / ALIAS), the tile
+  // neighbour table
+  std::vector<int32_t> h_cell_slot, h_tile_nb;
+  std::vector<uint8_t> h_cell_layout;
   int32_t *d_tile_nb = nullptr, *d_tile_level = nullptr, *d_cell_slot = nullptr;
   int2 *d_tile_org = nullptr;      // (ix, iy) of each tile's first cell
   double *d_signdis = nullptr;     // per slot, after ibgpu_upload_signdis
@@ -364,6 +369,33 @@ int ibgpu_set_stream(ibgpu_ctx *ctx, void *stream) {
   return IBGPU_OK;
 }
 
+// Cell-list bits that fix the layout: a flag update may change every other
+// bit of a row, never these.
+static const uint8_t kLayoutBits = IBGPU_CELL_PRESENT | IBGPU_CELL_NORMAL | IBGPU_CELL_ALIAS;
+
+// Uniform tiles: the tile and its four side neighbours hold only leaf cells
+// that update and recover their primitives (the stage kernel then needs no
+// presence flags and no one-sided stencils).
+static std::vector<uint8_t> uniform_tiles(const std::vector<uint8_t> &slot_flags,
+                                          const std::vector<int32_t> &nb, int64_t ntiles) {
+  const uint8_t kFull = CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM;
+  std::vector<uint8_t> tile_full(ntiles, 0), uniform(ntiles, 0);
+  for (int64_t t = 0; t < ntiles; ++t) {
+    bool full = true;
+    for (int i = 0; i < kTileCells && full; ++i) full = slot_flags[t * kTileCells + i] == kFull;
+    tile_full[t] = full;
+  }
+  for (int64_t t = 0; t < ntiles; ++t) {
+    bool u = tile_full[t];
+    for (int k : {1, 3, 5, 7}) {
+      int n = nb[t * 9 + k];
+      u = u && n >= 0 && tile_full[n];
+    }
+    uniform[t] = u;
+  }
+  return uniform;
+}
+
 int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   if (!ctx || !cells || cells->n < 0 || (cells->n > 0 && (!cells->level || !cells->ix ||
                                                           !cells->iy || !cells->flags)))
@@ -520,24 +552,8 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       }
     }
   }
-  // 6. uniform tiles: the tile and its four side neighbours hold only leaf
-  //    cells that update and recover their primitives (the stage kernel then
-  //    needs no presence flags and no one-sided stencils)
-  const uint8_t kFull = CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM;
-  std::vector<uint8_t> tile_full(ntiles, 0), h_uniform(ntiles, 0);
-  for (int64_t t = 0; t < ntiles; ++t) {
-    bool full = true;
-    for (int i = 0; i < kTileCells && full; ++i) full = h_flags[t * kTileCells + i] == kFull;
-    tile_full[t] = full;
-  }
-  for (int64_t t = 0; t < ntiles; ++t) {
-    bool u = tile_full[t];
-    for (int k : {1, 3, 5, 7}) {
-      int nb = h_nb[t * 9 + k];
-      u = u && nb >= 0 && tile_full[nb];
-    }
-    h_uniform[t] = u;
-  }
+  // 6. uniform tiles (see uniform_tiles)
+  std::vector<uint8_t> h_uniform = uniform_tiles(h_flags, h_nb, ntiles);
   // 7. device arrays
   int rc;
   if ((rc = dev_alloc(&ctx->d_tile_nb, h_nb.size())) ||
@@ -578,6 +594,11 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   if (ctx->d_vsd) CK(cudaMemsetAsync(ctx->d_vsd, 0, nslots * 8 * 8, st));
   CK(cudaStreamSynchronize(st));
   ctx->tilemap = std::move(tilemap);
+  ctx->h_cell_slot = std::move(cell_slot);
+  ctx->h_tile_nb = std::move(h_nb);
+  ctx->h_cell_layout.resize(n);
+  for (int64_t c = 0; c < n; ++c)
+    ctx->h_cell_layout[c] = (cells->flags[c] & kLayoutBits) | (alias[c] ? IBGPU_CELL_ALIAS : 0);
   ctx->h_flags_present.assign(nslots, 0);
   for (int64_t s = 0; s < nslots; ++s) ctx->h_flags_present[s] = (h_flags[s] & CF_PRESENT) ? 1 : 0;
   ctx->ncells = n;
@@ -587,6 +608,33 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   return IBGPU_OK;
 }
 
+
+int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
+  if (!ctx || (!flags && ctx->ncells > 0)) return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  if (ctx->chain_open) {
+    g_last_error = "asynchronous steps pending: call ibgpu_step_result first";
+    return IBGPU_E_STATE;
+  }
+  std::vector<uint8_t> h_flags(ctx->nslots, 0);
+  for (int64_t c = 0; c < ctx->ncells; ++c) {
+    const uint8_t layout = (flags[c] & kLayoutBits) |
+                           (ctx->h_cell_layout[c] & IBGPU_CELL_ALIAS ? IBGPU_CELL_ALIAS : 0);
+    if (layout != ctx->h_cell_layout[c]) {
+      g_last_error = "a row changed its PRESENT, NORMAL or ALIAS bit: upload the topology";
+      return IBGPU_E_TOPOLOGY;
+    }
+    if (ctx->h_cell_layout[c] & IBGPU_CELL_ALIAS) continue;
+    h_flags[ctx->h_cell_slot[c]] = flags[c] & 0x3f;
+  }
+  std::vector<uint8_t> h_uniform = uniform_tiles(h_flags, ctx->h_tile_nb, ctx->ntiles);
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->d_flags, h_flags.data(), ctx->nslots, cudaMemcpyHostToDevice, st));
+  if (ctx->ntiles > 0)
+    CK(cudaMemcpyAsync(ctx->d_tile_uniform, h_uniform.data(), ctx->ntiles, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
 
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles) {
   if (!ctx) return IBGPU_E_ARG;

@@ -39,7 +39,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
-           "ibgpu_step_async", "ibgpu_step_result")
+           "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags")
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -193,6 +193,7 @@ def lib(path: str | None = None):
     L.ibgpu_set_stream.argtypes = [vp, vp]
     L.ibgpu_upload_topology.argtypes = [vp, ctypes.POINTER(Cells)]
     L.ibgpu_layout_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.ibgpu_update_flags.argtypes = [vp, vp]
     L.ibgpu_upload_interfaces.argtypes = [vp, ctypes.POINTER(CfPairs)]
     L.ibgpu_upload_boundaries.argtypes = [vp, ctypes.POINTER(Bc)]
     L.ibgpu_upload_ib.argtypes = [vp, ctypes.POINTER(Ib)]
@@ -367,6 +368,14 @@ class FlowSolver:
                       f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
         _check(lib().ibgpu_upload_topology(self._ctx, ctypes.byref(cells)), "ibgpu_upload_topology")
         self.ncells = len(lv)
+
+    def update_flags(self, flags):
+        """New IBGPU_CELL_* flags for the rows of the last topology upload
+        (a moved body: same mesh, new inside / immersed-boundary cells)."""
+        f = np.ascontiguousarray(flags, np.uint8)
+        assert len(f) == self.ncells
+        _check(lib().ibgpu_update_flags(self._ctx, f.ctypes.data_as(ctypes.c_void_p)),
+               "ibgpu_update_flags")
 
     def upload_interfaces(self, res, pro):
         """Coarse/fine pairs as (n, 11) int arrays: level, cx, cy, 4 x (fx, fy)."""

@@ -200,6 +200,18 @@ int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib);
  * in the reference's dimensional scaling. */
 int ibgpu_wall_forces(ibgpu_ctx *ctx, double *out);
 
+/* New per-cell flags for the rows of the last topology upload (same rows,
+ * same order), for a body that moved without a regrid: the moved body
+ * changes which cells lie inside it, which are immersed-boundary cells and
+ * which update (the branches IBGPU_CELL_UPDATE / PRIM / RESET / RESNORM
+ * select), while the mesh stays.  Replaces the flag part of the
+ * re-immersion in Body::MovingBody_Image (Bodymove.cpp:37-125: wall
+ * distances, removed and newly infected immersed-boundary cells); the new
+ * immersed-boundary records go through ibgpu_upload_ib.  A row whose
+ * PRESENT, NORMAL or ALIAS bit differs from the topology upload gives
+ * IBGPU_E_TOPOLOGY (that needs ibgpu_upload_topology).  The state stays. */
+int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags);
+
 /* Number of device cell slots and tiles after the last topology upload. */
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);
 

@@ -3,6 +3,18 @@
 // the reference's non-negative index origin, Mach 0.5, 2 degrees angle of
 // attack, Re 5000, uniform free-stream start, CFL 0.5).
 //
+// Built with -DORACLE_CASE_PITCH the same file is the moving-body workload: a
+// NACA0015 pitching about its quarter chord, alpha(t) = amp sin(omega t) nose
+// up with omega = 2 k U / c (amplitude IB_PITCH_AMP degrees, default 5, and
+// reduced frequency IB_PITCH_K, default 0.1), mean angle 0, Mach 0.2, Re 1e4,
+// on [0,30]^2 ([-15,15]^2 shifted), base grid IB_NX (default 256) and IB_LEVELS
+// (default 6) levels.  The motion runs through the reference's own moving-body
+// path (Body::IBConditions_Image -> MovingBody_Image -> Motion_Rule,
+// Body.cpp:1352-1357, Bodymove.cpp:37-125): Motion_Rule below sets the angle
+// and angular velocity at the end of the coming step, and the reference
+// re-immerses the body (wall distances, immersed-boundary cells, image points)
+// and gives the wall points the velocity of the rotation (Body.H:709-721).
+//
 // Test infrastructure only: this file plays the role of the reference's
 // per-case user file (Userfunction_cy_naca15.cpp) — it defines the globals
 // and hooks the reference solver expects — for this workload.  The airfoil
@@ -66,25 +78,46 @@ const int dts_time_var = 1 << 30;
 const int dts_space_var = 1 << 30;
 
 // ---- mesh ------------------------------------------------------------------
-const int max_mesh_level = case_env_int("IB_LEVELS", 4);
-const int init_level_num = case_env_int("IB_LEVELS", 4);
+#ifdef ORACLE_CASE_PITCH
+#define CASE_NX 256
+#define CASE_LEVELS 6
+#define CASE_DOMAIN 30.0
+#define CASE_MACH 0.2
+#define CASE_MU_REF (1.0 / 1.0e4)   // Re = 1e4
+#define CASE_AOA_DEG 0.0
+#define CASE_THICKNESS 0.15
+#define CASE_PROFILE "naca0015"
+#define CASE_MOVING true
+#else
+#define CASE_NX 128
+#define CASE_LEVELS 4
+#define CASE_DOMAIN 20.0
+#define CASE_MACH 0.5
+#define CASE_MU_REF (1.0 / 5000.0)  // Re = 5000
+#define CASE_AOA_DEG 2.0
+#define CASE_THICKNESS 0.12
+#define CASE_PROFILE "naca0012"
+#define CASE_MOVING false
+#endif
+const int max_mesh_level = case_env_int("IB_LEVELS", CASE_LEVELS);
+const int init_level_num = case_env_int("IB_LEVELS", CASE_LEVELS);
 const Point lowpt = Point(0, 0, 0);
-const Point highpt = Point(case_env_int("IB_NX", 128), case_env_int("IB_NX", 128), 1);
-static const double kDomainLength = 20.0;
+const Point highpt = Point(case_env_int("IB_NX", CASE_NX), case_env_int("IB_NX", CASE_NX), 1);
+static const double kDomainLength = CASE_DOMAIN;
 
 string meshfile = "none";
 Pointxyz meshscale(1.0, 1.0, 1.0);
 Pointxyz frame_rotate_vel = Pointxyz(0.0, 0.0, 0.0);
 Pointxyz frame_rotate_origin = Pointxyz(0.0, 0.0, 0.0);
 Pointxyz frame_trans_vel = Pointxyz(0.0, 0.0, 0.0);
-const bool moveflag = false;
+const bool moveflag = CASE_MOVING;
 
 // ---- reference scales (constant-initialised) ------------------------------
 double roe_ref = 1.0;
 double L_ref = 1.0;
-double mu_ref = 1.0 / 5000.0;                      // Re = 5000
+double mu_ref = CASE_MU_REF;
 double u_ref = 1.0;
-double T_ref = 1.0 / (0.5 * 0.5 * 287.4 * 1.4);   // Mach 0.5
+double T_ref = 1.0 / (CASE_MACH * CASE_MACH * 287.4 * 1.4);
 
 bool additional_output = false;
 const int init_jump = 0;
@@ -94,9 +127,14 @@ const int filebodynum = 2;
 const char soln_file_name[30] = "none";
 
 // ---- airfoil placement -----------------------------------------------------
-static const double kAoA = 2.0 / 180.0 * 3.14159265358979323846;
-static const double kLeX = 9.5, kLeY = 10.0;      // leading edge; chord 1 along +x
+static const double kPi = 3.14159265358979323846;
+static const double kAoA = CASE_AOA_DEG / 180.0 * kPi;
+// leading edge; chord 1 along +x, centred in the domain
+static const double kLeX = 0.5 * CASE_DOMAIN - 0.5, kLeY = 0.5 * CASE_DOMAIN;
 static const double kPitchX = 0.25;               // moment / body centre at quarter chord
+// prescribed pitching (moving-body build): amplitude and angular frequency
+static const double kPitchAmp = case_env_double("IB_PITCH_AMP", 5.0) / 180.0 * kPi;
+static const double kPitchOmega = 2.0 * case_env_double("IB_PITCH_K", 0.1);  // 2 k U / c
 
 // NACA 4-digit symmetric thickness, closed trailing edge
 static double naca_half_thickness(double x, double t) {
@@ -113,7 +151,7 @@ static void write_surface(const string &path, int n, double sign) {
   for (int layer = 0; layer < 2; ++layer)
     for (int i = 0; i < n; ++i) {
       double x = 0.5 * (1.0 + cos(3.14159265358979323846 * i / (n - 1)));  // 1 -> 0
-      double y = sign * naca_half_thickness(x, 0.12);
+      double y = sign * naca_half_thickness(x, CASE_THICKNESS);
       fprintf(f, "%.17g %.17g %.17g\n", x, y, layer ? 0.1 : 0.0);
     }
   for (int i = 1; i < n; ++i) fprintf(f, "%d %d %d %d\n", i, i + 1, n + i + 1, n + i);
@@ -188,7 +226,27 @@ static bool served_decisions(int ilevel, const vector<int> &plain,
 FILE *g_oracle_tag_dump = nullptr;
 int g_oracle_tag_pass = 0;
 
+#ifdef ORACLE_CASE_PITCH
+// The moving-body workload tracks the body and its wake: rectangles reaching
+// 20, 17, 12 and 9 chords downstream on the coarse levels (up, down and half
+// height per level below, cut at the last four), and on the band levels a
+// wake box 3.5 chords long and 2 high behind the trailing edge besides the
+// wall-distance band.  About 1.5 M leaf cells on the 256^2, 6-level mesh;
+// meshes of fewer levels (test sizes) keep the static airfoil's regions.
+static const double kWakeRect[4][3] = {{5.0, 20.0, 11.0}, {3.0, 17.0, 5.3}, {2.0, 12.0, 3.0},
+                                       {1.0, 9.0, 1.5}};
+#endif
+
 static bool naca_region(int k, double x, double y, double celldis) {
+#ifdef ORACLE_CASE_PITCH
+  if (max_mesh_level >= 6) {
+    if (k < max_mesh_level - 2) {
+      const double *r = kWakeRect[max(0, min(3, k - (max_mesh_level - 6)))];
+      return x - kLeX > -r[0] && x - (kLeX + 1.0) < r[1] && fabs(y - kLeY) < r[2];
+    }
+    if (x > kLeX + 0.5 && x < kLeX + 4.5 && fabs(y - kLeY) < 1.0) return true;
+  }
+#endif
   if (k < max_mesh_level - 2) {
     double s = pow(0.5, k);
     double up = 4.0 * s, down = 8.0 * s, half_h = 4.0 * s;
@@ -368,7 +426,16 @@ void AMR::TagtheBox(const int &ilevel, vector<Body> &abody) {
   MPI_Barrier(share_comm);
 }
 
-void Body::Motion_Rule(Mesh &, double &) {}
+// The body's angle and angular velocity at the time the coming step starts
+// (the step's own dt is set by its CFL evaluation after the body has moved),
+// the rotation applied by ComptNewLocation about the body centre (the quarter
+// chord).  Nose up is a clockwise rotation.
+void Body::Motion_Rule(Mesh &, double &) {
+  if (!moveflag) return;
+  rotosc_new[2] = -kPitchAmp * sin(kPitchOmega * t);
+  free_rot_vel[2] = -kPitchAmp * kPitchOmega * cos(kPitchOmega * t);
+  ComptNewLocation();
+}
 
 void SetTwodFlag() {
   level_twod_flag.resize(max_mesh_level);
@@ -387,10 +454,10 @@ void InitSpaceParams() {
 
 void Body::SetBodyParams(vector<Body> &abody, Mesh &amesh, vector<Body> &) {
   const int npts = case_env_int("IB_NPTS", 200);
-  write_surface("naca0012_upper.ugrid", npts, 1.0);
-  write_surface("naca0012_lower.ugrid", npts, -1.0);
+  write_surface(CASE_PROFILE "_upper.ugrid", npts, 1.0);
+  write_surface(CASE_PROFILE "_lower.ugrid", npts, -1.0);
   bodynum = 2;
-  const char *files[2] = {"naca0012_upper.ugrid", "naca0012_lower.ugrid"};
+  const char *files[2] = {CASE_PROFILE "_upper.ugrid", CASE_PROFILE "_lower.ugrid"};
   for (int i = 0; i < bodynum; ++i) {
     abody.push_back(Body(i));
     abody.back().FindNearBody();

@@ -64,6 +64,7 @@ using namespace std;  // the reference headers assume it (min/max/abs in macros)
 
 extern const double Ma;
 extern double p_ref, area_ref, shear_ref;
+extern double dt00;  // time since the bodies last moved (Body.cpp)
 extern FILE *g_oracle_tag_dump;  // defined by the case file (tag dump hook)
 extern int g_oracle_tag_pass;
 
@@ -569,7 +570,7 @@ int main(int argc, char **argv) {
   };
   if (dump_now(0, false)) do_dump(0);
 
-  double loop_time = 0.0;
+  double loop_time = 0.0, move_time = 0.0;
   long long cell_updates = 0;
   for (int s = 0; s < nsteps; ++s) {
     // leaf cells of the levels that march this step (subcycling schedule)
@@ -581,6 +582,14 @@ int main(int argc, char **argv) {
       amr.InterfaceExchange();
       Body::IBConditions_Image(mesh, sphere);
     }
+#ifdef ORACLE_BINDING
+    else if (moveflag) {
+      // the moving-body part of IBConditions_Image through the binding
+      const double tm0 = MPI_Wtime();
+      gpu_check(flowsolver.MoveBodies(sphere, dt00), "move bodies");
+      move_time += MPI_Wtime() - tm0;
+    }
+#endif
     flowsolver.TimeMarching(amr);
     ++ts;
     t += dt;
@@ -627,9 +636,10 @@ int main(int argc, char **argv) {
   }
   if (flog) std::fclose(flog);
   std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
-              "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g}\n",
+              "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g, "
+              "\"move_seconds\": %.9f}\n",
               nsteps - timed_from, loop_time, cell_updates,
-              loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt);
+              loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time);
   MPI_Finalize();
   return 0;
 }

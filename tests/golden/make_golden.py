@@ -34,6 +34,13 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 CONFIG1_ENV = {"IB_NX": "128", "IB_LEVELS": "4", "IB_STAGES": "4", "IB_USER_INIT": "0",
                "IB_FORCES": "1", "IB_NPTS": "200"}
 
+# the moving-body workload at a test size: the pitching NACA0015 (Mach 0.2,
+# Re 1e4, [0,30]^2) on a 64^2 base grid + 3 AMR levels, 150 points per
+# surface, regrids every 20 steps, pitching at reduced frequency 2 (omega 4)
+# so that the body moves across cells within the recorded steps
+PITCH_ENV = {"IB_NX": "64", "IB_LEVELS": "4", "IB_STAGES": "4", "IB_USER_INIT": "0",
+             "IB_FORCES": "1", "IB_NPTS": "150", "IB_REGRID_EVERY": "20", "IB_PITCH_K": "2.0"}
+
 # name -> (binary, environment, number of steps)
 CASES = {
     "vortex_vanleer_s4_n32": ("ref_vortex_vanleer", {"IB_NX": "32", "IB_STAGES": "4"}, 4),
@@ -63,6 +70,8 @@ FORCE_CASES = {
                                                    "IB_FORCES": "1", "IB_NPTS": "120"}, 400),
     # the stated 1000 steps of the plain-method airfoil workload
     "naca_forces_s1000_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, 1000),
+    # the moving body: 100 steps, four regrids
+    "pitch_forces_s100_n64_l4": ("ref_pitch_minmod", PITCH_ENV, 100),
 }
 # states of a developed flow, too large to commit (about 1 MB each): the
 # fixture records the SHA-256 of each dumped state's bytes and its scalars,
@@ -70,6 +79,8 @@ FORCE_CASES = {
 # digests: name -> (binary, environment, dumped step counts)
 STATE_DIGEST_CASES = {
     "naca_states_s600_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, (600, 601, 602, 603, 604)),
+    # the moving body: states and moved lists on both sides of the regrid at 40
+    "pitch_states_n64_l4": ("ref_pitch_minmod", PITCH_ENV, (30, 31, 32, 40, 41, 42)),
 }
 # per-case records that do not change between dumps of a static mesh
 AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
@@ -193,6 +204,36 @@ def run_state_digest_case(name: str, binary: str, env: dict, at) -> str:
         return path
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+def live_snapshots(name: str) -> list:
+    """The dumps a STATE_DIGEST_CASES fixture records, regenerated by its
+    reference binary and checked against the recorded digests: one complete
+    dump per recorded step (mesh lists, flags, immersed-boundary records and
+    state), for runs whose mesh or body moves between dumps."""
+    binary, env, at = STATE_DIGEST_CASES[name]
+    rec = load(name)
+    work = tempfile.mkdtemp(prefix="live_")
+    try:
+        snaps = _dump_states(binary, env, at, work)[1:]
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    for s, want, k in zip(snaps, rec["digests"], at):
+        if _digest(s["prim"]) != str(want):
+            raise RuntimeError(f"{name}: the live reference run differs from the recorded one "
+                               f"at step {k}")
+        s["step"] = k
+    return snaps
+
+
+def record_of(snap: dict, state_from: dict | None = None) -> dict:
+    """A single-snapshot record (the layout of ``load``) of one dump: its
+    mesh and lists, with the state and scalars of ``state_from`` if given."""
+    src = state_from if state_from is not None else snap
+    out = {k: snap[k] for k in STATIC + ("dh", "schedule", "initvar", "domain") + AUX if k in snap}
+    out["prim"] = src["prim"].reshape(1, -1, 7)
+    out["scalars"] = src["scalars"].reshape(1, -1)
+    return out
 
 
 def live_states(name: str) -> dict:

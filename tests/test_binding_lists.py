@@ -191,3 +191,26 @@ def test_binding_tag_rule_takes_each_levels_requests():
         changed += int(np.sum(io.tag_plain(base, r[:, 0].astype(int), r[:, 3], r[:, 4],
                                            r[:, 5]) != want))
     assert changed > 0
+
+
+def test_binding_build_keeps_the_reference_moving_step():
+    """The moving-body build with the binding linked in but not stepping on
+    the GPU runs the reference's own moving step: the force history equals
+    the plain reference build's bit for bit."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    outs = []
+    for b in ("ref_pitch_minmod_binding", "ref_pitch_minmod"):
+        work = tempfile.mkdtemp(prefix="pitch_")
+        log = os.path.join(work, "forces.bin")
+        env = dict(os.environ)
+        env.update(make_golden.PITCH_ENV)
+        env.update(IB_STEPS="25", IB_FORCE_LOG=log)
+        out = subprocess.run([os.path.join(ORACLE_DIR, "_ref", b)], cwd=work, env=env,
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr[-2000:]
+        outs.append(np.fromfile(log, np.float64))
+    assert len(outs[0]) == 25 * 15 and np.array_equal(outs[0], outs[1])
+    # and it is the recorded moving-body history
+    ref = make_golden.load("pitch_forces_s100_n64_l4")["history"][:25].ravel()
+    assert np.array_equal(outs[1], ref)

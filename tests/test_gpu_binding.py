@@ -38,8 +38,10 @@ def run_binding(env_case, steps, precision):
     work = tempfile.mkdtemp(prefix="binding_gpu_")
     log = os.path.join(work, "forces.bin")
     prec = {"fp64": 0, "exact": 1, "mixed": 2}[precision]
-    env = dict(os.environ, **env_case, IB_STEPS=str(steps), IB_FORCES="1", IB_FORCE_LOG=log,
-               IB_BINDING_STEP="1", IB_BINDING_PRECISION=str(prec))
+    env = dict(os.environ)
+    env.update(env_case)
+    env.update(IB_STEPS=str(steps), IB_FORCES="1", IB_FORCE_LOG=log, IB_BINDING_STEP="1",
+               IB_BINDING_PRECISION=str(prec))
     out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True,
                          timeout=600)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]

@@ -1,0 +1,154 @@
+"""The moving immersed body: a NACA0015 pitching about its quarter chord
+(Mach 0.2, Re 1e4, [0,30]^2), at a test size (64^2 base grid + 3 AMR
+levels, 150 points per surface), pitching at reduced frequency 2 so that
+the body crosses cells within the recorded steps, regrids every 20 steps.
+
+The reference moves and re-immerses the body at the start of every step
+(Body::IBConditions_Image -> MovingBody_Image, Body.cpp:1352-1357,
+Bodymove.cpp:37-125): new wall distances, cells that leave or enter the
+body, new immersed-boundary cells and image points, wall points moving with
+the rotation (Body.H:709-721).  On the device the mesh and the state stay;
+the new cell flags go through ibgpu_update_flags and the new
+immersed-boundary records through ibgpu_upload_ib.
+
+* per step, from the reference's own state with the lists the reference
+  built for the next step (on both sides of a regrid): exact build
+  <= 1e-14, FP64 <= 1e-12, mixed <= 5e-5 relative on the conserved variables;
+* the reference's own main loop stepping through the C++ binding on the
+  device (GpuNS_Solver::MoveBodies + TimeMarching) for 100 steps and four
+  regrids: the dt and force history against the reference's own run,
+  exact <= 1e-12, FP64 <= 1e-10, mixed |dCl|, |dCd| < 1e-3.
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_golden  # noqa: E402
+from conftest import ORACLE_DIR, load_pkg  # noqa: E402
+
+workloads = load_pkg().workloads
+
+pytestmark = pytest.mark.gpu
+
+STATES = "pitch_states_n64_l4"
+HISTORY = "pitch_forces_s100_n64_l4"
+BINARY = os.path.join(ORACLE_DIR, "_ref", "ref_pitch_minmod_binding")
+REL = {"exact": 1e-14, "fp64": 1e-12, "mixed": 5e-5}
+F_REF = 0.5 * 1.0 * 0.1
+
+
+def conserved(prim):
+    r, u, v, e = prim[:, 0], prim[:, 1], prim[:, 2], prim[:, 6]
+    return np.stack([r, r * u, r * v, r * e], axis=1)
+
+
+def rel_err(got, ref):
+    cg, cr = conserved(got), conserved(ref)
+    scale = np.abs(cr).max(axis=0)
+    scale[scale == 0] = 1.0
+    return (np.abs(cg - cr).max(axis=0) / scale).max()
+
+
+def prec_of(ib, name):
+    return {"exact": ib.FP64_EXACT, "fp64": ib.FP64, "mixed": ib.MIXED}[name]
+
+
+@pytest.fixture(scope="module")
+def snaps():
+    return make_golden.live_snapshots(STATES)
+
+
+def pairs(snaps):
+    """(before, after) dumps of consecutive steps on the same mesh."""
+    out = []
+    for a, b in zip(snaps, snaps[1:]):
+        if b["step"] == a["step"] + 1:
+            assert all(np.array_equal(a[k], b[k]) for k in ("level", "ix", "iy", "kind"))
+            out.append((a, b))
+    return out
+
+
+def test_the_body_moves_between_the_recorded_steps(snaps):
+    moved = 0
+    for a, b in pairs(snaps):
+        ia = set(map(tuple, a["ib"].reshape(-1, 20)[:, :2].tolist()))
+        ib_ = set(map(tuple, b["ib"].reshape(-1, 20)[:, :2].tolist()))
+        moved += len(ia ^ ib_) + int(np.sum(a["solid"] != b["solid"]))
+        assert np.abs(b["ib_f"].reshape(-1, 16)[:, 13:16]).max() > 0.05  # wall velocity
+    assert moved > 0
+    assert len(pairs(snaps)) == 4
+
+
+@pytest.mark.parametrize("precision", ["exact", "fp64", "mixed"])
+def test_step_with_the_moved_body_from_reference_states(cuda_lib, pkg, snaps, precision):
+    """The device holds step k's mesh, lists and state; the body moves (new
+    flags through ibgpu_update_flags, new records through ibgpu_upload_ib);
+    one step; the reference's state after step k + 1."""
+    ib = pkg.ibgpu
+    for a, b in pairs(snaps):
+        sol = workloads.naca_solver(make_golden.record_of(a), 0, prec_of(ib, precision))
+        moved = workloads.naca_lists(make_golden.record_of(b, state_from=a), 0)
+        sol.update_flags(moved["flags"])
+        sol.upload_ib(moved["ib"], moved["ib_f"], moved["patch"], moved["patch_f"],
+                      moved["body_center"])
+        d = sol.time_marching(int(a["step"]))
+        assert d.abort_code == 0
+        if precision == "exact":
+            assert sol.dt == b["scalars"][1]
+        err = rel_err(sol.download(), b["prim"].reshape(-1, 7))
+        assert err <= REL[precision], f"step {a['step']} -> {b['step']}: rel err {err:.3e}"
+        f = sol.wall_forces().ravel()
+        ftol = {"exact": 1e-12, "fp64": 1e-10, "mixed": 1e-4}[precision]
+        assert np.allclose(f, b["forces"], rtol=ftol, atol=1e-14), precision
+        sol.close()
+
+
+def test_flag_update_keeps_the_layout(cuda_lib, pkg, snaps):
+    """A flag update may not change which rows are leaf cells, present or
+    periodic copies: that needs a topology upload."""
+    ib = pkg.ibgpu
+    a = snaps[0]
+    sol = workloads.naca_solver(make_golden.record_of(a), 0, ib.FP64)
+    flags = workloads.naca_lists(make_golden.record_of(a), 0)["flags"].copy()
+    sol.update_flags(flags)  # unchanged: fine
+    leaf = np.flatnonzero(flags & ib.CELL_NORMAL)[0]
+    flags[leaf] &= ~ib.CELL_NORMAL
+    with pytest.raises(ib.IbgpuError) as ei:
+        sol.update_flags(flags)
+    assert ei.value.code == ib.E_TOPOLOGY
+    sol.close()
+
+
+def run_binding(precision, steps=100):
+    work = tempfile.mkdtemp(prefix="pitch_binding_")
+    log = os.path.join(work, "forces.bin")
+    env = dict(os.environ)
+    env.update(make_golden.PITCH_ENV)
+    env.update(IB_STEPS=str(steps), IB_FORCE_LOG=log, IB_BINDING_STEP="1",
+               IB_BINDING_PRECISION=str({"fp64": 0, "exact": 1, "mixed": 2}[precision]))
+    out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    return np.fromfile(log, np.float64).reshape(steps, -1), out.stdout
+
+
+@pytest.mark.skipif(not os.path.exists(BINARY), reason="binding oracle not built (make -C oracle)")
+@pytest.mark.parametrize("precision,tol", [("exact", 1e-12), ("fp64", 1e-10), ("mixed", 1e-3)])
+def test_reference_loop_moves_the_body_through_the_binding(cuda_lib, precision, tol):
+    ref = make_golden.load(HISTORY)["history"]
+    got, _ = run_binding(precision)
+    assert got.shape == ref.shape and np.array_equal(got[:, 0], ref[:, 0])
+    dt_err = np.abs(got[:, 2] - ref[:, 2]) / ref[:, 2]
+    fg = got[:, 3:].reshape(len(ref), -1, 6)[:, :, :2]
+    fr = ref[:, 3:].reshape(len(ref), -1, 6)[:, :, :2]
+    coef = np.abs(fg - fr).max() / F_REF
+    total = np.abs(fg.sum(axis=1) - fr.sum(axis=1)).max() / F_REF
+    print(f"\npitching {precision}: max rel dt {dt_err.max():.2e}, max |dC| per surface "
+          f"{coef:.2e}, airfoil {total:.2e}")
+    assert coef <= tol and total <= tol
+    assert dt_err.max() <= (tol if precision != "mixed" else 1e-4)

@@ -15,6 +15,8 @@ abort code as the regular entry point.
 Kept in a file of its own that sorts last, so a run that stops at the first
 failure has already run every other test.
 """
+import gc
+
 import numpy as np
 import pytest
 
@@ -69,12 +71,20 @@ def test_noalloc_step_matches_regular_entry_point_twice(cuda_lib, pkg, precision
     dt = P["dt0"]
     src = rows
     for ts in range(2):
-        free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
-        dt_in = dt
-        dt, diag = ib.step_periodic_noalloc(P, ts, nx, ny, src.data_ptr(), out.data_ptr(), dt,
-                                            stream)
+        # no other object may free device memory meanwhile (a collected
+        # context of an earlier test would)
+        gc.collect()
+        gc.disable()
+        try:
+            free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+            dt_in = dt
+            dt, diag = ib.step_periodic_noalloc(P, ts, nx, ny, src.data_ptr(), out.data_ptr(), dt,
+                                                stream)
+            free1 = torch.cuda.mem_get_info()[0]
+        finally:
+            gc.enable()
         if ts > 0:  # the first call on a device may load the library's module
-            assert torch.cuda.mem_get_info()[0] == free0, "the call allocated device memory"
+            assert free1 == free0, "the call allocated device memory"
             assert torch.cuda.memory_allocated() == alloc0
             assert dt == dt_in  # no CFL evaluation on this step
         assert diag.abort_code == 0 and diag.cells_marched == nx * ny
