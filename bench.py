@@ -48,6 +48,13 @@ CONFIG1_HISTORY = os.path.join(ROOT, "tests", "golden", "naca_forces_s1000_n128_
 CONFIG1_ENV = {"IB_NX": "128", "IB_LEVELS": "4", "IB_STAGES": "4", "IB_USER_INIT": "0",
                "IB_NPTS": "200"}
 F_REF = 0.5 * 1.0 * 0.1  # 0.5 rho_inf u_inf^2 * chord * slab depth (Cl, Cd scale)
+# the moving-body workload at its stated size: a NACA0015 pitching about its
+# quarter chord (5 deg, k = 0.1, mean 0), Mach 0.2, Re 1e4, 256^2 base grid on
+# [0,30]^2 + 5 AMR levels tracking the body and wake (~1.58 M leaf cells),
+# regrid every 20 steps; built and moved by the reference's own host code
+CONFIG3_ENV = {"IB_NX": "256", "IB_LEVELS": "6", "IB_STAGES": "4", "IB_USER_INIT": "0",
+               "IB_NPTS": "400", "IB_REGRID_EVERY": "20", "IB_PITCH_K": "0.1",
+               "IB_FORCES": "1"}
 
 
 def load_pkg():
@@ -615,6 +622,80 @@ def config1_section(ib, wl, stream, max_over_ranks, timed_steps: int = 400, rank
     return out
 
 
+def run_oracle_binary(binary: str, env_case: dict, extra: dict, timeout: float = 900.0):
+    """One reference-solver process (its ORACLE_RESULT line and force log)."""
+    import numpy as np
+    with tempfile.TemporaryDirectory() as wd:
+        log = os.path.join(wd, "forces.bin")
+        env = dict(os.environ)
+        env.update(env_case)
+        env.update(extra)
+        env["IB_FORCE_LOG"] = log
+        out = subprocess.run([binary], cwd=wd, env=env, capture_output=True, text=True,
+                             timeout=timeout)
+        if out.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(binary)} failed: {out.stderr[-500:]}")
+        res = next(json.loads(l.split(" ", 1)[1]) for l in out.stdout.splitlines()
+                   if l.startswith("ORACLE_RESULT"))
+        hist = np.fromfile(log, np.float64)
+    steps = int(env_case.get("IB_STEPS", extra.get("IB_STEPS", 0)))
+    return res, hist.reshape(steps, -1) if steps else hist
+
+
+def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
+    """The moving-body workload at its stated size, stepped by the
+    reference's own main loop through the C++ binding (GpuNS_Solver): every
+    step the host moves and re-immerses the body with the reference's code
+    and hands the device new flags and immersed-boundary records, the device
+    runs the step.  FP64 and mixed runs: leaf-cell updates/s of the device
+    step alone and of the whole step including the host's re-immersion, the
+    host time per step, and |dCl|, |dCd| of mixed against FP64; the
+    reference's own step (motion included) on the same mesh on one core."""
+    import numpy as np
+    binding = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod_binding")
+    if rank != 0 or not os.path.exists(binding):
+        return None
+    out = {"workload": "NACA0015 pitching about the quarter chord (5 deg, k 0.1, mean 0), Mach "
+                       "0.2, Re 1e4, 256x256 base grid on [0,30]^2 + 5 AMR levels tracking the "
+                       "body and wake, regrid every 20 steps; mesh, motion and re-immersion by "
+                       "the reference's own host code",
+           "timed_steps": steps - warm}
+    # the reference's own sample runs on one host core meanwhile (its mesh
+    # generation alone takes most of a minute)
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod")
+    pool = None
+    if os.path.exists(ref):
+        from concurrent.futures import ThreadPoolExecutor
+        pool = ThreadPoolExecutor(1)
+        ref_job = pool.submit(run_oracle_binary, ref, CONFIG3_ENV,
+                              {"IB_STEPS": "3", "IB_TIMED_FROM": "1"})
+    hist = {}
+    for name, prec in (("fp64", 0), ("mixed", 2)):
+        res, h = run_oracle_binary(binding, CONFIG3_ENV,
+                                   {"IB_STEPS": str(steps), "IB_TIMED_FROM": str(warm),
+                                    "IB_BINDING_STEP": "1", "IB_BINDING_PRECISION": str(prec)})
+        hist[name] = h
+        dev_s = res["loop_seconds"] - res["move_seconds"]
+        out[name] = {"value": res["cell_updates"] / dev_s, "unit": UNIT,
+                     "device_ms_per_step": dev_s * 1e3 / (steps - warm),
+                     "with_host_reimmersion": res["cell_updates"] / res["loop_seconds"],
+                     "host_reimmersion_ms_per_step": res["move_seconds"] * 1e3 / (steps - warm),
+                     "cell_updates_per_step": res["cell_updates"] / (steps - warm)}
+    f = {k: v[:, 3:].reshape(len(v), -1, 6)[:, :, :2].sum(axis=1) / F_REF for k, v in hist.items()}
+    d = np.abs(f["mixed"] - f["fp64"]).max(axis=0)
+    out["mixed_vs_fp64_max_dcd"], out["mixed_vs_fp64_max_dcl"] = float(d[0]), float(d[1])
+    out["device_step_note"] = ("device step = the synchronous ibgpu_step wall time (loop time "
+                               "minus the host's motion, re-immersion and record upload)")
+    if pool is not None:
+        res, _ = ref_job.result()
+        pool.shutdown()
+        out["reference"] = {"value": res["cell_updates_per_s"], "unit": UNIT, "cores": 1,
+                            "sample": "the reference's own step with its moving-body path, 2 "
+                                      "timed steps after 1, one single-rank process (run while "
+                                      "the GPU runs step)"}
+    return out
+
+
 def accuracy_section(ib, wl, stream, n: int = 2048, steps: int = 500):
     """The bandwidth workload's accuracy: the 2048^2 vortex after `steps`
     steps, L2 density error vs the exact solution for FP64 and mixed, and
@@ -769,6 +850,8 @@ def our_arm(args):
         for s in bsols:
             s.close()
         extra["config1"] = config1_section(ib, wl, stream, max_over_ranks, rank=rank)
+        if not args.no_config3:
+            extra["config3"] = config3_section(rank=rank)
         if rank == 0:
             extra["accuracy"] = accuracy_section(ib, wl, stream, n=n)
 
@@ -949,6 +1032,8 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip the moving-body section (about three minutes of host mesh work)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the batched, learned-indicator, airfoil and accuracy sections")
     ap.add_argument("--profile", choices=["stage", "batch", "mlp-grad", "mlp-tag"],

@@ -228,13 +228,14 @@ int g_oracle_tag_pass = 0;
 
 #ifdef ORACLE_CASE_PITCH
 // The moving-body workload tracks the body and its wake: rectangles reaching
-// 20, 17, 12 and 9 chords downstream on the coarse levels (up, down and half
-// height per level below, cut at the last four), and on the band levels a
+// 12, 11, 10 and 8 chords downstream on the coarse levels (up, down and half
+// height per level below, cut at the last four; every refined region keeps
+// clear of the domain boundary), and on the band levels a
 // wake box 3.5 chords long and 2 high behind the trailing edge besides the
 // wall-distance band.  About 1.5 M leaf cells on the 256^2, 6-level mesh;
 // meshes of fewer levels (test sizes) keep the static airfoil's regions.
-static const double kWakeRect[4][3] = {{5.0, 20.0, 11.0}, {3.0, 17.0, 5.3}, {2.0, 12.0, 3.0},
-                                       {1.0, 9.0, 1.5}};
+static const double kWakeRect[4][3] = {{5.0, 12.0, 11.0}, {3.0, 11.0, 6.0}, {2.0, 10.0, 3.2},
+                                       {1.0, 8.0, 1.6}};
 #endif
 
 static bool naca_region(int k, double x, double y, double celldis) {

@@ -79,8 +79,9 @@ FORCE_CASES = {
 # digests: name -> (binary, environment, dumped step counts)
 STATE_DIGEST_CASES = {
     "naca_states_s600_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, (600, 601, 602, 603, 604)),
-    # the moving body: states and moved lists on both sides of the regrid at 40
-    "pitch_states_n64_l4": ("ref_pitch_minmod", PITCH_ENV, (30, 31, 32, 40, 41, 42)),
+    # the moving body: states and moved lists around steps where cells enter
+    # or leave the body (22, 23, 50, 58), after the regrids at 20 and 40
+    "pitch_states_n64_l4": ("ref_pitch_minmod", PITCH_ENV, (21, 22, 23, 49, 50, 57, 58)),
 }
 # per-case records that do not change between dumps of a static mesh
 AUX = ("cf_res", "cf_pro", "bc", "bc_nmv", "facevar", "bc_scalars", "ib", "ib_f", "patch",
