@@ -10,10 +10,12 @@
 // of units in the last place of the correctly rounded value for the normal,
 // positive operands the flux uses (densities, sound speeds, 1 + r); they are
 // not IEEE-exact, which is why the exact build does not use them.
-// Inside the flux and the limiter a single Newton step suffices (rcp1,
-// rsqrt1: relative error of order 1e-14, far inside the FP64 build's
-// per-step tolerance, and these quantities only scale dissipation terms and
-// slopes); primitive recovery keeps the two-step versions.
+// Measured on B200 over [0.25, 16) against IEEE division and square root:
+// the approximations alone 9.9e-7 (rcp) and 9.2e-7 (rsqrt) relative, after
+// one Newton step (rcp1, rsqrt1) 9.8e-13 and 1.3e-12, after two (rcp, rsqrt)
+// 0 and 2.7e-16.  One step is used only where the result scales a
+// dissipation term or a limited slope; anything that reaches a central flux
+// or the primitive recovery takes two.
 // FP32 (mixed precision): the PTX single-precision approximations directly.
 #pragma once
 

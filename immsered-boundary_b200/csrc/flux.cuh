@@ -24,6 +24,8 @@ struct Gas {
   R gamaRg;   // gama * Rg   (the reference's left-to-right "gama*Rg*T")
   R inv_Rg;   // 1 / Rg      (fast builds)
   R inv_gm1;  // 1 / (gama - 1)
+  R gam_gm1;  // gama / (gama - 1)  (fast builds: h = gam_gm1 p/rho + |u|^2/2)
+  R two_gama; // 2 gama              (fast builds: the all-speed Mach number)
 };
 
 enum { LIM_VANLEER = 0, LIM_MINMOD = 1 };
@@ -198,61 +200,68 @@ __device__ __forceinline__ R muscl_right_fast(R q_i, R qi, R qi1) {
   return qi - R(0.5) * dqii * lv;
 }
 
-// All-speed Roe flux from reconstructed left/right states (rho, u_n, u_t, p).
-// One inverse square root per side gives both 1/rho (a^2) and sqrt(rho)
-// (rho a); the Roe weights are sqrt(rho_L,R) / (sqrt(rho_L) + sqrt(rho_R)),
-// and one inverse root of c^2 gives c and 1/c^2.
+// All-speed Roe flux from reconstructed left/right states (rho, u_n, u_t, p),
+// restated with fewer operations than the reference's term order (same
+// quantities, different rounding):
+//   * one inverse root y = (rho_L rho_R)^-1/2 gives the Roe density
+//     rho_L rho_R y, the ratio sqrt(rho_R / rho_L) = rho_R y, both inverse
+//     densities (ratio y, rho_L y^2) and the Roe weights 1 / (1 + ratio),
+//     ratio / (1 + ratio);
+//   * Cv = Rg / (gama - 1) (FlowConstants.cpp), so the total enthalpy is
+//     h = gama/(gama-1) p/rho + |u|^2/2, the energy flux (p + e rho) u_n is
+//     rho u_n h, and Rg T = p / rho: no temperature is formed;
+//   * c^2 / (gama - 1) in the energy dissipation is the bracket c^2 is made
+//     from; the halves of the all-speed eigenvalues and of the central flux
+//     go into the face area.
+// halfarea = area / 2.
 template <typename R>
-__device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R lroe, R lun, R lut,
-                                                R lp, R rroe, R run, R rut, R rp, R &f_mass,
-                                                R &f_n, R &f_t, R &f_e) {
+__device__ __forceinline__ void roe_flux_states(const Gas<R> &g, R area, R halfarea, R lroe,
+                                                R lun, R lut, R lp, R rroe, R run, R rut, R rp,
+                                                R &f_mass, R &f_n, R &f_t, R &f_e) {
   typedef FastMath<R> M;
-  const R aL = M::rsqrt1(lroe), aR = M::rsqrt1(rroe);
-  const R ilroe = aL * aL, irroe = aR * aR;
-  const R sL = lroe * aL, sR = rroe * aR;  // sqrt(rho)
-  const R lpr = lp * ilroe, rpr = rp * irroe;  // p / rho
-  const R lT = lpr * g.inv_Rg, rT = rpr * g.inv_Rg;
-  const R le = g.Cv * lT + R(0.5) * (lun * lun + lut * lut);
-  const R re = g.Cv * rT + R(0.5) * (run * run + rut * rut);
-  const R lv = lun, rv = run;
-  const R droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = rv - lv;
-  const R isum = M::rcp1(sL + sR);
-  const R wL = sL * isum, wR = sR * isum;
-  const R a_roe = sL * sR;
-  const R a_un = lun * wL + run * wR;
-  const R a_ut = lut * wL + rut * wR;
-  const R a_h = (le + lpr) * wL + (re + rpr) * wR;
-  const R csquare = g.gm1 * (a_h - R(0.5) * (a_un * a_un + a_ut * a_ut));
+  const R prod = lroe * rroe;
+  const R y = M::rsqrt(prod);
+  const R a_roe = prod * y;                // sqrt(rho_L rho_R)
+  const R ratio = rroe * y;                // sqrt(rho_R / rho_L)
+  const R ilroe = ratio * y, irroe = (lroe * y) * y;
+  const R lpr = lp * ilroe, rpr = rp * irroe;  // p / rho = Rg T
+  const R lh = fma(g.gam_gm1, lpr, R(0.5) * fma(lun, lun, lut * lut));
+  const R rh = fma(g.gam_gm1, rpr, R(0.5) * fma(run, run, rut * rut));
+  const R droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = run - lun;
+  // Roe averages w_L q_L + (1 - w_L) q_R = q_R - w_L (q_R - q_L): the
+  // weights sum to one exactly
+  const R wL = M::rcp(R(1) + ratio);
+  const R a_un = fma(-wL, dubar, run);
+  const R a_ut = fma(-wL, dut, rut);
+  const R a_h = fma(-wL, rh - lh, rh);
+  const R kin = fma(R(-0.5), fma(a_un, a_un, a_ut * a_ut), a_h);  // c^2 / (gama - 1)
+  const R csquare = g.gm1 * kin;
   const R rc = M::rsqrt1(csquare);
   const R a_c = csquare * rc;
   const R icsq = rc * rc;
   const R ubar = a_un;
-  const R namda3 = fabs(ubar);
-  const R coef12 = R(0.5) * icsq * area;
+  const R coef12 = icsq * halfarea;
   const R roe0cxdubar = a_roe * a_c * dubar;
-  const R faceareaxabsubar = area * namda3;
-  const R halffacearea = R(0.5) * area;
-  const R alpha0 = faceareaxabsubar * (droe - dp * icsq);
-  const R T_a = (lT + rT) * R(0.5);
-  const R V_a = (lv + rv) * R(0.5);
-  const R Ma_a = fabs(V_a) * M::rsqrt1(g.gamaRg * T_a);
+  const R faceareaxabsubar = area * fabs(ubar);
+  const R alpha0 = faceareaxabsubar * fma(-dp, icsq, droe);
+  // all-speed scaling: |V_a| / sqrt(gama Rg T_a) with V_a, T_a face means
+  const R Ma_a = fabs(lun + run) * M::rsqrt1(g.two_gama * (lpr + rpr));
   const R f_Ma = smin(smax(Ma_a, g.Ma), R(1));
-  const R s0 = (R(1) - f_Ma) * (R(1) - f_Ma);
-  const R n0sq = R(4) * csquare * f_Ma + s0 * ubar * ubar;
-  const R namda0 = n0sq * M::rsqrt1(n0sq);
-  const R namda1 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar + namda0));
-  const R namda2 = fabs(R(0.5) * ((R(1) + f_Ma) * ubar - namda0));
-  const R alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
-  const R alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
+  const R hm = fma(R(-0.5), f_Ma, R(0.5)) * ubar;  // (1 - f) ubar / 2
+  const R hp = fma(R(0.5), f_Ma, R(0.5)) * ubar;   // (1 + f) ubar / 2
+  const R q = fma(hm, hm, csquare * f_Ma);          // (namda0 / 2)^2
+  const R sq = q * M::rsqrt1(q);
+  const R alpha1 = coef12 * fabs(hp + sq) * (dp + roe0cxdubar);
+  const R alpha2 = coef12 * fabs(hp - sq) * (dp - roe0cxdubar);
   const R alpha3 = alpha0 + alpha1 + alpha2;
   const R alpha4 = a_c * (alpha1 - alpha2);
   const R alphat = faceareaxabsubar * (a_roe * dut);
-  const R ml = lroe * lv, mr = rroe * rv;  // mass fluxes of both states
-  f_mass = (ml + mr) * halffacearea - alpha3;
-  f_n = (ml * lun + lp + mr * run + rp) * halffacearea - (a_un * alpha3 + alpha4);
-  f_t = (ml * lut + mr * rut) * halffacearea - (a_ut * alpha3 + alphat);
-  f_e = ((lp + le * lroe) * lv + (rp + re * rroe) * rv) * halffacearea -
-        (a_h * alpha3 + ubar * alpha4 + a_ut * alphat - (csquare * g.inv_gm1) * alpha0);
+  const R ml = lroe * lun, mr = rroe * run;  // mass fluxes of both states
+  f_mass = fma(ml + mr, halfarea, -alpha3);
+  f_n = fma(fma(ml, lun, lp) + fma(mr, run, rp), halfarea, -fma(a_un, alpha3, alpha4));
+  f_t = fma(fma(ml, lut, mr * rut), halfarea, -fma(a_ut, alpha3, alphat));
+  f_e = fma(fma(ml, lh, mr * rh), halfarea,
+            -fma(a_h, alpha3, fma(ubar, alpha4, fma(a_ut, alphat, -kin * alpha0))));
 }
 
 // ---- paired flux: two faces per thread -----------------------------------
@@ -307,56 +316,49 @@ template <typename P, typename S>
 __device__ __forceinline__ void roe_flux_pair(const Gas<S> &g, P area, P lroe, P lun, P lut, P lp,
                                               P rroe, P run, P rut, P rp, P &f_mass, P &f_n,
                                               P &f_t, P &f_e) {
-  const P half = pair(S(0.5), S(0.5)), one = pair(S(1), S(1));
-  const P inv_Rg = pair(g.inv_Rg, g.inv_Rg), Cv = pair(g.Cv, g.Cv);
-  const P aL = rsqrt2(lroe), aR = rsqrt2(rroe);
-  const P ilroe = aL * aL, irroe = aR * aR;
-  const P sL = lroe * aL, sR = rroe * aR;
+  const P half = pair(S(0.5), S(0.5)), one = pair(S(1), S(1)), mhalf = pair(S(-0.5), S(-0.5));
+  const P halfarea = half * area;
+  const P prod = lroe * rroe;
+  const P y = rsqrt2(prod);
+  const P a_roe = prod * y;
+  const P ratio = rroe * y;
+  const P ilroe = ratio * y, irroe = (lroe * y) * y;
   const P lpr = lp * ilroe, rpr = rp * irroe;
-  const P lT = lpr * inv_Rg, rT = rpr * inv_Rg;
-  const P le = fma2(Cv, lT, half * fma2(lun, lun, lut * lut));
-  const P re = fma2(Cv, rT, half * fma2(run, run, rut * rut));
+  const P gg = pair(g.gam_gm1, g.gam_gm1);
+  const P lh = fma2(gg, lpr, half * fma2(lun, lun, lut * lut));
+  const P rh = fma2(gg, rpr, half * fma2(run, run, rut * rut));
   const P droe = rroe - lroe, dp = rp - lp, dut = rut - lut, dubar = run - lun;
-  const P isum = rcp2(sL + sR);
-  const P wL = sL * isum, wR = sR * isum;
-  const P a_roe = sL * sR;
-  const P a_un = fma2(lun, wL, run * wR);
-  const P a_ut = fma2(lut, wL, rut * wR);
-  const P a_h = fma2(le + lpr, wL, (re + rpr) * wR);
-  const P csquare = pair(g.gm1, g.gm1) * (a_h - half * fma2(a_un, a_un, a_ut * a_ut));
+  const P mwL = pair(S(0), S(0)) - rcp2(one + ratio);  // -w_L
+  const P a_un = fma2(mwL, dubar, run);
+  const P a_ut = fma2(mwL, dut, rut);
+  const P a_h = fma2(mwL, rh - lh, rh);
+  const P kin = fma2(mhalf, fma2(a_un, a_un, a_ut * a_ut), a_h);
+  const P csquare = pair(g.gm1, g.gm1) * kin;
   const P rc = rsqrt2(csquare);
   const P a_c = csquare * rc;
   const P icsq = rc * rc;
   const P ubar = a_un;
-  const P namda3 = abs2(ubar);
-  const P coef12 = half * icsq * area;
+  const P coef12 = icsq * halfarea;
   const P roe0cxdubar = a_roe * a_c * dubar;
-  const P faceareaxabsubar = area * namda3;
-  const P halffacearea = half * area;
+  const P faceareaxabsubar = area * abs2(ubar);
   const P alpha0 = faceareaxabsubar * (droe - dp * icsq);
-  const P T_a = (lT + rT) * half;
-  const P V_a = (lun + run) * half;
-  const P Ma_a = abs2(V_a) * rsqrt2(pair(g.gamaRg, g.gamaRg) * T_a);
+  const P Ma_a = abs2(lun + run) * rsqrt2(pair(g.two_gama, g.two_gama) * (lpr + rpr));
   const P f_Ma = clamp2(Ma_a, g.Ma, S(1));
-  const P om = one - f_Ma;
-  const P s0 = om * om;
-  const P n0sq = fma2(pair(S(4), S(4)) * csquare, f_Ma, s0 * ubar * ubar);
-  const P namda0 = n0sq * rsqrt2(n0sq);
-  const P opf = (one + f_Ma) * ubar;
-  const P namda1 = abs2(half * (opf + namda0));
-  const P namda2 = abs2(half * (opf - namda0));
-  const P alpha1 = coef12 * namda1 * (dp + roe0cxdubar);
-  const P alpha2 = coef12 * namda2 * (dp - roe0cxdubar);
+  const P hm = fma2(mhalf, f_Ma, half) * ubar;
+  const P hp = fma2(half, f_Ma, half) * ubar;
+  const P q = fma2(hm, hm, csquare * f_Ma);
+  const P sq = q * rsqrt2(q);
+  const P alpha1 = coef12 * abs2(hp + sq) * (dp + roe0cxdubar);
+  const P alpha2 = coef12 * abs2(hp - sq) * (dp - roe0cxdubar);
   const P alpha3 = alpha0 + alpha1 + alpha2;
   const P alpha4 = a_c * (alpha1 - alpha2);
   const P alphat = faceareaxabsubar * (a_roe * dut);
   const P ml = lroe * lun, mr = rroe * run;
-  f_mass = (ml + mr) * halffacearea - alpha3;
-  f_n = (fma2(ml, lun, lp) + fma2(mr, run, rp)) * halffacearea - fma2(a_un, alpha3, alpha4);
-  f_t = fma2(ml, lut, mr * rut) * halffacearea - fma2(a_ut, alpha3, alphat);
-  f_e = fma2(fma2(le, lroe, lp), lun, fma2(re, rroe, rp) * run) * halffacearea -
-        (fma2(a_h, alpha3, fma2(ubar, alpha4, a_ut * alphat)) -
-         (csquare * pair(g.inv_gm1, g.inv_gm1)) * alpha0);
+  f_mass = (ml + mr) * halfarea - alpha3;
+  f_n = (fma2(ml, lun, lp) + fma2(mr, run, rp)) * halfarea - fma2(a_un, alpha3, alpha4);
+  f_t = fma2(ml, lut, mr * rut) * halfarea - fma2(a_ut, alpha3, alphat);
+  f_e = fma2(ml, lh, mr * rh) * halfarea -
+        (fma2(a_h, alpha3, fma2(ubar, alpha4, a_ut * alphat)) - kin * alpha0);
 }
 
 }  // namespace ibgpu

@@ -438,7 +438,7 @@ template <typename R, int LIM, int NQ, int NS>
 __device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const uint8_t *sfl,
                                            const typename SRec<R>::V *sl, int rL1, int rR1, int step,
                                            int sL, int sR, bool xdir, bool uni, const Gas<R> &g,
-                                           R area) {
+                                           R area, R halfarea) {
   R ls[4], rs[4];
   Q4<R> out = {R(0), R(0), R(0), R(0)};
   if (!face_recon<R, LIM, NQ, NS>(sq, sfl, sl, rL1, rR1, step, sL, sR, uni, ls, rs)) return out;
@@ -447,7 +447,8 @@ __device__ __forceinline__ Q4<R> fast_face(const typename SRec<R>::V *sq, const 
   R fm, fn, ft, fe;
   const R lun = xdir ? ls[1] : ls[2], lut = xdir ? ls[2] : ls[1];
   const R run = xdir ? rs[1] : rs[2], rut = xdir ? rs[2] : rs[1];
-  roe_flux_states<R>(g, area, ls[0], lun, lut, ls[3], rs[0], run, rut, rs[3], fm, fn, ft, fe);
+  roe_flux_states<R>(g, area, halfarea, ls[0], lun, lut, ls[3], rs[0], run, rut, rs[3], fm, fn,
+                     ft, fe);
   out = Q4<R>{fm, xdir ? fn : ft, xdir ? ft : fn, fe};
   return out;
 }
@@ -655,7 +656,10 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   g.gamaRg = (R)cc.gamaRg;
   g.inv_Rg = (R)(1.0 / cc.Rg);
   g.inv_gm1 = (R)(1.0 / cc.gm1);
+  g.gam_gm1 = (R)(cc.gama / cc.gm1);
+  g.two_gama = (R)(2.0 * cc.gama);
   const R ax = (R)L.area_x, ay = (R)L.area_y;
+  const R hax = R(0.5) * ax, hay = R(0.5) * ay;
 
   // ---- face fluxes: west x-face and south y-face of cell (tx, ty), plus the
   //      east column (threads 0..15) and north row (threads 16..31)
@@ -685,10 +689,10 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
       else S::st(fy, ty * kTile + tx, NF, R(0), R(0), R(0), R(0));
     } else {
       o = fast_face<R, LIM, NQ, NS>(sq, sfl, slx, rR1 - 1, rR1, 1, ty * kSX + tx,
-                                    ty * kSX + tx + 1, true, uni, g, ax);
+                                    ty * kSX + tx + 1, true, uni, g, ax, hax);
       S::st(fx, ty * (kTile + 1) + tx, NF, o.x, o.y, o.z, o.w);
       o = fast_face<R, LIM, NQ, NS>(sq, sfl, sly, rR1 - kReg, rR1, kReg, ty * kTile + tx,
-                                    (ty + 1) * kTile + tx, false, uni, g, ay);
+                                    (ty + 1) * kTile + tx, false, uni, g, ay, hay);
       S::st(fy, ty * kTile + tx, NF, o.x, o.y, o.z, o.w);
     }
     const int et = tid - (NT > kTileCells ? kTileCells : 0);
@@ -702,7 +706,7 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
       const int sL = xd ? e * kSX + kTile : kTile * kTile + e;
       const int sR = xd ? e * kSX + kTile + 1 : (kTile + 1) * kTile + e;
       o = fast_face<R, LIM, NQ, NS>(sq, sfl, xd ? slx : sly, r - step, r, step, sL, sR, xd, uni,
-                                    g, xd ? ax : ay);
+                                    g, xd ? ax : ay, xd ? hax : hay);
       S::st(xd ? fx : fy, xd ? e * (kTile + 1) + kTile : kTile * kTile + e, NF, o.x, o.y, o.z, o.w);
     }
   }
