@@ -82,6 +82,7 @@ struct ibgpu_ctx {
   int chain_steps = 0;
   int64_t chain_marched = 0;
   bool download_pending = false;       // an asynchronous download may still read s0
+  int row_fields = 7;                  // state rows: 7 FlowVariables or 4 (roe u v p)
   double *d_rows_out = nullptr;        // staging of asynchronous downloads
   cudaStream_t stream = nullptr;
 
@@ -653,6 +654,34 @@ static int order_after_download(ibgpu_ctx *ctx, cudaStream_t st) {
   return IBGPU_OK;
 }
 
+// Scatter / gather of the staged state rows in the context's row format.
+static void scatter_rows(ibgpu_ctx *ctx, const double *rows, cudaStream_t st) {
+  if (ctx->row_fields == 4)
+    fast::launch_scatter4(rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->cs.Rg,
+                          ctx->cs.Cv, ctx->d_s0, ctx->nsm, st);
+  else
+    fast::launch_scatter(rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->d_s0,
+                         ctx->nsm, st);
+}
+static void gather_rows(ibgpu_ctx *ctx, double *rows, cudaStream_t st) {
+  if (ctx->row_fields == 4) fast::launch_gather4(rows, ctx->d_cell_slot, ctx->ncells, ctx->d_s0, ctx->nsm, st);
+  else fast::launch_gather(rows, ctx->d_cell_slot, ctx->ncells, ctx->d_s0, ctx->nsm, st);
+}
+
+int ibgpu_set_state_rows(ibgpu_ctx *ctx, int fields) {
+  if (!ctx || (fields != IBGPU_ROWS_FLOWVARS && fields != IBGPU_ROWS_COMPACT)) return IBGPU_E_ARG;
+  if (ctx->chain_open || ctx->download_pending || ctx->in_used) {
+    // transfers in flight use the current format's buffer layout
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(ctx->in_stream));
+    CK(cudaStreamSynchronize(ctx->copy_stream));
+    ctx->download_pending = false;
+    ctx->in_used = false;
+  }
+  ctx->row_fields = fields;
+  return IBGPU_OK;
+}
+
 int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim) {
   if (!ctx || (!prim && ctx->ncells > 0)) return IBGPU_E_ARG;
   if (!ctx->has_topology) return IBGPU_E_STATE;
@@ -660,11 +689,11 @@ int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim) {
   if (ctx->ncells > 0) {
     // the host-to-device copy may overlap a pending download (other buffer,
     // other copy direction); the scatter into the state waits for it
-    CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * 7 * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * ctx->row_fields * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
     int rc = order_after_download(ctx, st);
     if (rc) return rc;
-    fast::launch_scatter(ctx->d_rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->d_s0,
-                         ctx->nsm, st);
+    scatter_rows(ctx, ctx->d_rows, st);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(st));
@@ -677,9 +706,10 @@ int ibgpu_download_state(ibgpu_ctx *ctx, double *prim) {
   if (!ctx->has_state) return IBGPU_E_STATE;
   cudaStream_t st = ctx->stream;
   if (ctx->ncells > 0) {
-    fast::launch_gather(ctx->d_rows, ctx->d_cell_slot, ctx->ncells, ctx->d_s0, ctx->nsm, st);
+    gather_rows(ctx, ctx->d_rows, st);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(prim, ctx->d_rows, ctx->ncells * 7 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(prim, ctx->d_rows, ctx->ncells * ctx->row_fields * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));
   return IBGPU_OK;
@@ -695,12 +725,11 @@ int ibgpu_download_state_async(ibgpu_ctx *ctx, double *prim) {
   }
   CK(cudaEventRecord(ctx->ev_ready, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
-  fast::launch_gather(ctx->d_rows_out, ctx->d_cell_slot, ctx->ncells, ctx->d_s0, ctx->nsm,
-                      ctx->copy_stream);
+  gather_rows(ctx, ctx->d_rows_out, ctx->copy_stream);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev_copied, ctx->copy_stream));
   ctx->download_pending = true;
-  CK(cudaMemcpyAsync(prim, ctx->d_rows_out, ctx->ncells * 7 * sizeof(double),
+  CK(cudaMemcpyAsync(prim, ctx->d_rows_out, ctx->ncells * ctx->row_fields * sizeof(double),
                      cudaMemcpyDeviceToHost, ctx->copy_stream));
   return IBGPU_OK;
 }
@@ -1070,7 +1099,7 @@ int ibgpu_upload_state_async(ibgpu_ctx *ctx, const double *prim) {
     cudaStream_t st = ctx->stream;
     // the rows buffer is free once the previous upload's scatter has run
     if (ctx->in_used) CK(cudaStreamWaitEvent(ctx->in_stream, ctx->ev_in_free, 0));
-    CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * 7 * sizeof(double),
+    CK(cudaMemcpyAsync(ctx->d_rows, prim, ctx->ncells * ctx->row_fields * sizeof(double),
                        cudaMemcpyHostToDevice, ctx->in_stream));
     CK(cudaEventRecord(ctx->ev_in_done, ctx->in_stream));
     // the scatter follows the copy and the context's pending work, and
@@ -1078,8 +1107,7 @@ int ibgpu_upload_state_async(ibgpu_ctx *ctx, const double *prim) {
     CK(cudaStreamWaitEvent(st, ctx->ev_in_done, 0));
     int rc = order_after_download(ctx, st);
     if (rc) return rc;
-    fast::launch_scatter(ctx->d_rows, ctx->d_cell_slot, ctx->d_cell_alias, ctx->ncells, ctx->d_s0,
-                         ctx->nsm, st);
+    scatter_rows(ctx, ctx->d_rows, st);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev_in_free, st));
     ctx->in_used = true;

@@ -956,6 +956,45 @@ __global__ void gather_state_kernel(double *rows, const int32_t *cell_slot, int6
   }
 }
 
+// Compact rows (roe, u, v, p): the remaining fields as the reference derives
+// them from those four (Get_T_ideal_gas T = p / (roe Rg), Get_E e = Cv T +
+// |u|^2 / 2 with w = 0, FlowVariables.H:19-33), rounded operation by
+// operation (no contraction).
+__global__ void scatter_state4_kernel(const double *rows, const int32_t *cell_slot,
+                                      const uint8_t *cell_is_alias, int64_t n, double Rg,
+                                      double Cv, double *s0_rho, double *s0_u, double *s0_v,
+                                      double *s0_p, double *s0_e, double *s0_T) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (cell_is_alias[c]) continue;
+    int64_t s = cell_slot[c];
+    const double *r = rows + 4 * c;
+    const double roe = r[0], u = r[1], v = r[2], p = r[3];
+    const double T = __ddiv_rn(p, __dmul_rn(roe, Rg));
+    const double k = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), 0.0));
+    s0_rho[s] = roe;
+    s0_u[s] = u;
+    s0_v[s] = v;
+    s0_p[s] = p;
+    s0_T[s] = T;
+    s0_e[s] = __dadd_rn(__dmul_rn(Cv, T), k);
+  }
+}
+
+__global__ void gather_state4_kernel(double *rows, const int32_t *cell_slot, int64_t n,
+                                     const double *s0_rho, const double *s0_u,
+                                     const double *s0_v, const double *s0_p) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int64_t s = cell_slot[c];
+    double *r = rows + 4 * c;
+    r[0] = s0_rho[s];
+    r[1] = s0_u[s];
+    r[2] = s0_v[s];
+    r[3] = s0_p[s];
+  }
+}
+
 // ---- launchers (one set per arithmetic build)
 
 
@@ -1240,6 +1279,26 @@ void launch_gather(double *rows, const int32_t *cell_slot, int64_t n,
   if (blocks < 1) blocks = 1;
   gather_state_kernel<<<(unsigned)blocks, 256, 0, st>>>(rows, cell_slot, n, s0[F_RHO], s0[F_U],
                                                         s0[F_V], s0[F_P], s0[F_E], s0[F_T]);
+}
+
+void launch_scatter4(const double *rows, const int32_t *cell_slot, const uint8_t *alias, int64_t n,
+                     double Rg, double Cv, double *const s0[kStateFields], int nsm,
+                     cudaStream_t st) {
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
+  if (blocks < 1) blocks = 1;
+  scatter_state4_kernel<<<(unsigned)blocks, 256, 0, st>>>(rows, cell_slot, alias, n, Rg, Cv,
+                                                          s0[F_RHO], s0[F_U], s0[F_V], s0[F_P],
+                                                          s0[F_E], s0[F_T]);
+}
+
+void launch_gather4(double *rows, const int32_t *cell_slot, int64_t n,
+                    double *const s0[kStateFields], int nsm, cudaStream_t st) {
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
+  if (blocks < 1) blocks = 1;
+  gather_state4_kernel<<<(unsigned)blocks, 256, 0, st>>>(rows, cell_slot, n, s0[F_RHO], s0[F_U],
+                                                         s0[F_V], s0[F_P]);
 }
 
 }  // namespace IBGPU_KNS

@@ -20,6 +20,11 @@ namespace ibgpu {
                       int64_t n, double *const s0[kStateFields], int nsm, cudaStream_t st);   \
   void launch_gather(double *rows, const int32_t *cell_slot, int64_t n,                       \
                      double *const s0[kStateFields], int nsm, cudaStream_t st);               \
+  void launch_scatter4(const double *rows, const int32_t *cell_slot, const uint8_t *alias,    \
+                       int64_t n, double Rg, double Cv, double *const s0[kStateFields],       \
+                       int nsm, cudaStream_t st);                                             \
+  void launch_gather4(double *rows, const int32_t *cell_slot, int64_t n,                      \
+                      double *const s0[kStateFields], int nsm, cudaStream_t st);              \
   void launch_restrict(const PairArgs &a, const CaseConst &cc, cudaStream_t st);               \
   void launch_prolong(const PairArgs &a, const CaseConst &cc, cudaStream_t st);                \
   void launch_bc(const BcArgs &a, const CaseConst &cc, cudaStream_t st);                       \

@@ -39,7 +39,9 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
-           "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags")
+           "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
+           "ibgpu_set_state_rows")
+ROWS_FLOWVARS, ROWS_COMPACT = 7, 4
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
 TAG_REFINE, TAG_COARSEN = 1, 2
@@ -194,6 +196,7 @@ def lib(path: str | None = None):
     L.ibgpu_upload_topology.argtypes = [vp, ctypes.POINTER(Cells)]
     L.ibgpu_layout_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_update_flags.argtypes = [vp, vp]
+    L.ibgpu_set_state_rows.argtypes = [vp, ctypes.c_int]
     L.ibgpu_upload_interfaces.argtypes = [vp, ctypes.POINTER(CfPairs)]
     L.ibgpu_upload_boundaries.argtypes = [vp, ctypes.POINTER(Bc)]
     L.ibgpu_upload_ib.argtypes = [vp, ctypes.POINTER(Ib)]
@@ -482,20 +485,27 @@ class FlowSolver:
         _check(lib().ibgpu_layout_info(self._ctx, ctypes.byref(ns), ctypes.byref(nt)), "ibgpu_layout_info")
         return ns.value, nt.value
 
+    def set_state_rows(self, fields: int):
+        """Row format of the state transfers: ROWS_FLOWVARS (7 doubles per cell)
+        or ROWS_COMPACT (roe, u, v, p)."""
+        _check(lib().ibgpu_set_state_rows(self._ctx, int(fields)), "ibgpu_set_state_rows")
+        self.row_fields = int(fields)
+
     def init_flow(self, prim_rows):
-        """Upload FlowVariables rows (n, 7); also accepts a host pointer (int)."""
+        """Upload state rows (n, 7) or, in the compact format, (n, 4); also
+        accepts a host pointer (int)."""
         if isinstance(prim_rows, int):
             _check(lib().ibgpu_upload_state(self._ctx, ctypes.c_void_p(prim_rows)), "ibgpu_upload_state")
             return
         a = np.ascontiguousarray(prim_rows, np.float64)
-        assert a.shape == (self.ncells, 7)
+        assert a.shape == (self.ncells, getattr(self, "row_fields", 7))
         _check(lib().ibgpu_upload_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p)), "ibgpu_upload_state")
 
     def download(self, out=None):
         if isinstance(out, int):
             _check(lib().ibgpu_download_state(self._ctx, ctypes.c_void_p(out)), "ibgpu_download_state")
             return None
-        a = np.empty((self.ncells, 7), np.float64) if out is None else out
+        a = np.empty((self.ncells, getattr(self, "row_fields", 7)), np.float64) if out is None else out
         _check(lib().ibgpu_download_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p)), "ibgpu_download_state")
         return a
 

@@ -222,6 +222,18 @@ int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);
 int ibgpu_upload_state(ibgpu_ctx *ctx, const double *prim);
 int ibgpu_download_state(ibgpu_ctx *ctx, double *prim);
 
+/* Row format of every state transfer of the context (ibgpu_upload_state,
+ * ibgpu_download_state and their asynchronous forms) from the next call on:
+ * IBGPU_ROWS_FLOWVARS (the default) moves the 7 doubles above per cell;
+ * IBGPU_ROWS_COMPACT moves 4, (roe, u, v, p), 43 % fewer bytes for a caller
+ * that hands the state over every step.  A compact upload derives T and e as
+ * the reference derives them from those four (Get_T_ideal_gas,
+ * Get_E, FlowVariables.H:19-33); a compact download leaves them out.  Waits
+ * for transfers in flight. */
+#define IBGPU_ROWS_FLOWVARS 7
+#define IBGPU_ROWS_COMPACT 4
+int ibgpu_set_state_rows(ibgpu_ctx *ctx, int fields);
+
 /* Download without waiting: the copy runs on the context's copy stream after
  * the work enqueued so far, so it overlaps later uploads and steps (work
  * that writes the state waits for it on the device).  prim (pinned host

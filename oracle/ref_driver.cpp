@@ -587,7 +587,7 @@ int main(int argc, char **argv) {
       // the moving-body part of IBConditions_Image through the binding
       const double tm0 = MPI_Wtime();
       gpu_check(flowsolver.MoveBodies(sphere, dt00), "move bodies");
-      move_time += MPI_Wtime() - tm0;
+      if (s >= timed_from) move_time += MPI_Wtime() - tm0;
     }
 #endif
     flowsolver.TimeMarching(amr);
