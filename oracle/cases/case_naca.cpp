@@ -479,7 +479,19 @@ void Body::SetBodyParams(vector<Body> &abody, Mesh &amesh, vector<Body> &) {
 void Domain::SetBlockNum() { blocknum = Point(1, 1, 1); }
 
 // Far field: pressure inlet (x-), pressure outlet (x+), zero-gradient top
-// and bottom, periodic z (the reference case's face types).
+// and bottom, periodic z (the reference case's face types).  IB_BC=<x-,x+,y-,y+>
+// replaces the four in-plane face types (e.g. -10,-45,-51,-49) to exercise
+// the reference's other boundary conditions (BCValues.H:191-298); a slip wall
+// (-51) takes its normal from the reference cell's face on that side, as the
+// reference's own case file sets refboxface for it.
+static int case_face_type(int face, int dflt) {
+  const char *s = getenv("IB_BC");
+  if (!s || !*s) return dflt;
+  int t[4];
+  if (sscanf(s, "%d,%d,%d,%d", &t[0], &t[1], &t[2], &t[3]) != 4) MPI_Abort(MPI_COMM_WORLD, 3401);
+  return t[face];
+}
+
 void Domain::SetFaceProperty(DataArray<Box> &, DataArray<BoxCellGeom> &) {
   facenum = 6;
   faceup.resize(facenum);
@@ -489,20 +501,24 @@ void Domain::SetFaceProperty(DataArray<Box> &, DataArray<BoxCellGeom> &) {
   refboxface.resize(facenum);
   faceup[0] = Point(0, 99999, 99999);
   facedown[0] = Point(-10, -99999, -99999);
-  facetype[0] = -13;
+  facetype[0] = case_face_type(0, -13);
   facedir[0] = Point(1, 0, 0);
   faceup[1] = Point(boxnum.ix() + 10, 99999, 99999);
   facedown[1] = Point(boxnum.ix() - 1, -99999, -99999);
-  facetype[1] = -12;
+  facetype[1] = case_face_type(1, -12);
   facedir[1] = Point(-1, 0, 0);
   faceup[2] = Point(99999, 0, 99999);
   facedown[2] = Point(-99999, -10, -99999);
-  facetype[2] = -50;
+  facetype[2] = case_face_type(2, -50);
   facedir[2] = Point(0, 1, 0);
   faceup[3] = Point(99999, boxnum.iy() + 10, 99999);
   facedown[3] = Point(-99999, boxnum.iy() - 1, -99999);
-  facetype[3] = -50;
+  facetype[3] = case_face_type(3, -50);
   facedir[3] = Point(0, -1, 0);
+  // slip walls: the normal of the reference cell's face on the wall side
+  const Boxloc wall_face[4] = {Boxloc(0, 0), Boxloc(0, 1), Boxloc(1, 0), Boxloc(1, 1)};
+  for (int f = 0; f < 4; ++f)
+    if (facetype[f] == -51) refboxface[f] = wall_face[f];
   faceup[4] = Point(99999, 99999, 0);
   facedown[4] = Point(-99999, -99999, -10);
   facetype[4] = -99;

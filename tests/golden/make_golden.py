@@ -55,6 +55,17 @@ CASES = {
     # levels (~45k leaf cells), 400-point NACA0012, Mach 0.5, 2 deg, Re 5000,
     # minmod, 4 stages, CFL 0.5: the mesh, the initial state and two steps
     "naca_minmod_s4_n128_l4": ("ref_naca_minmod", CONFIG1_ENV, 2),
+    # the reference's other domain boundary conditions (BCValues.H:191-298) on
+    # the 3-level airfoil mesh: fixed values / fixed velocity / slip wall /
+    # no-slip wall, and pressure inlet / outlet / static-frame wall / slip wall
+    "naca_bc_a_s4_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
+                                                "IB_STAGES": "4", "IB_USER_INIT": "0",
+                                                "IB_FORCES": "1", "IB_NPTS": "120",
+                                                "IB_BC": "-10,-45,-51,-49"}, 4),
+    "naca_bc_b_s4_n64_l3": ("ref_naca_minmod", {"IB_NX": "64", "IB_LEVELS": "3",
+                                                "IB_STAGES": "4", "IB_USER_INIT": "0",
+                                                "IB_FORCES": "1", "IB_NPTS": "120",
+                                                "IB_BC": "-13,-12,-46,-51"}, 4),
 }
 # plain tag criterion only (TagtheBox on the initial mesh, refine and coarsen
 # requested on every level): name -> (binary, environment)
@@ -97,7 +108,8 @@ def run_case(name: str, binary: str, env: dict, steps: int) -> str:
         e.update(env)
         e["IB_STEPS"] = str(steps)
         e["IB_DUMP"] = os.path.join(work, "d")
-        e["IB_TAG_DUMP"] = os.path.join(work, "tags.bin")
+        if "IB_BC" not in env:
+            e["IB_TAG_DUMP"] = os.path.join(work, "tags.bin")
         subprocess.run([os.path.join(REF, binary)], cwd=work, env=e, check=True,
                        stdout=subprocess.DEVNULL)
         snaps = [pyoracle.read_dump(os.path.join(work, f"d_{k:06d}.bin")) for k in range(steps + 1)]
@@ -115,7 +127,8 @@ def run_case(name: str, binary: str, env: dict, steps: int) -> str:
         nf = max(len(s["forces"]) for s in snaps)
         out["forces"] = np.stack([s["forces"] if len(s["forces"]) == nf else np.full(nf, np.nan)
                                   for s in snaps])
-        tags = np.fromfile(os.path.join(work, "tags.bin"), dtype=np.float64).reshape(-1, 9)
+        tpath = os.path.join(work, "tags.bin")
+        tags = np.fromfile(tpath, dtype=np.float64).reshape(-1, 9) if os.path.exists(tpath) else []
         if len(tags):
             out["tags"] = tags
         path = os.path.join(HERE, name + ".npz")

@@ -166,7 +166,15 @@ def training_set(g, sol, dh, snapshots, every):
     return li, rule, B, labels, feats
 
 
-def test_training_beats_untrained_and_majority(cuda_lib, naca):
+def test_learned_reproduces_the_plain_criterion(cuda_lib, naca):
+    """The claim made for the learned indicator: trained on the plain
+    criterion's decisions, it reproduces them on boxes it has not seen
+    (held-out mismatch within 3 %; an untrained network and the majority
+    class are far off), and the deployment policy re-judges with the plain
+    criterion every 10th regrid.  It gains no accuracy over the plain
+    criterion, whose decisions are the labels; what it replaces is the
+    geometric rule's need for the wall distance (its inputs are the flow
+    stencil plus position features)."""
     import torch
     g, sol = naca
     _, dh = tag_rows(NAME)
@@ -185,6 +193,7 @@ def test_training_beats_untrained_and_majority(cuda_lib, naca):
     trained = np.mean(li.predict(Xte) != yte)
     print(f"\nheld-out tag mismatch: trained {trained:.4f}, untrained {untrained:.4f}, "
           f"majority class {majority:.4f}")
+    assert trained <= 0.03
     assert trained < 0.5 * majority
     assert trained < untrained
     # deployment policy: learned tags on ordinary regrids, the plain
