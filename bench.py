@@ -52,6 +52,15 @@ F_REF = 0.5 * 1.0 * 0.1  # 0.5 rho_inf u_inf^2 * chord * slab depth (Cl, Cd scal
 # quarter chord (5 deg, k = 0.1, mean 0), Mach 0.2, Re 1e4, 256^2 base grid on
 # [0,30]^2 + 5 AMR levels tracking the body and wake (~1.58 M leaf cells),
 # regrid every 20 steps; built and moved by the reference's own host code
+# the batched airfoil workload: 64 independent NACA0012 / NACA0015 cases
+# (alternating) from a seeded generator; the first CONFIG4_DEFAULT_CASES run by
+# default (the host meshes come from the reference's own mesh generation)
+CONFIG4_CASES = 64
+CONFIG4_DEFAULT_CASES = 16
+# leaf cells per base cell of the airfoil mesh by mesh level count (the base
+# grid and its AMR levels; measured on the reference's 256^2-base meshes of
+# this case family): base side = sqrt(target / f)
+CONFIG4_LEAF_FACTOR = {3: 1.81, 4: 2.71, 5: 3.95, 6: 6.22}
 CONFIG3_ENV = {"IB_NX": "256", "IB_LEVELS": "6", "IB_STAGES": "4", "IB_USER_INIT": "0",
                "IB_NPTS": "400", "IB_REGRID_EVERY": "20", "IB_PITCH_K": "0.1",
                "IB_FORCES": "1"}
@@ -706,6 +715,130 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
     return out
 
 
+def config4_cases(ncases: int = CONFIG4_CASES, seed: int = 0):
+    """The batched airfoil cases: per case, in this order from one seeded
+    generator, Mach U[0.1, 0.8], angle of attack U[-5, 10] deg, Re
+    log-uniform in [2e3, 2e4], AMR levels U{2..5} above the base grid (3..6
+    mesh levels, as the plain-method workload's "128^2 plus 3 AMR levels" is
+    4) and a target leaf count log-uniform in [5e4, 8e5] that sets the base
+    grid; profile NACA0012 and NACA0015 alternating.  Returns the reference
+    case environments."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(ncases):
+        mach = float(rng.uniform(0.1, 0.8))
+        aoa = float(rng.uniform(-5.0, 10.0))
+        re = math.exp(float(rng.uniform(math.log(2e3), math.log(2e4))))
+        levels = int(rng.integers(2, 6)) + 1  # mesh levels: the base grid and 2..5 AMR levels
+        target = math.exp(float(rng.uniform(math.log(5e4), math.log(8e5))))
+        nx = max(64, int(round(math.sqrt(target / CONFIG4_LEAF_FACTOR[levels]) / 16.0)) * 16)
+        out.append({"IB_MACH": repr(mach), "IB_AOA": repr(aoa), "IB_RE": repr(re),
+                    "IB_LEVELS": str(levels), "IB_NX": str(nx),
+                    "IB_THICK": "0.12" if i % 2 == 0 else "0.15", "IB_NPTS": "200",
+                    "IB_STAGES": "4", "IB_USER_INIT": "0", "IB_STEPS": "0"})
+    return out
+
+
+def config4_meshes(envs, workers: int):
+    """The cases' meshes and initial states from the reference's own mesh
+    generation (one process per case, `workers` at a time), as records."""
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    import pyoracle
+    binary = os.path.join(ROOT, "oracle", "_ref", "ref_naca_minmod")
+
+    def one(env_case):
+        with tempfile.TemporaryDirectory() as wd:
+            env = dict(os.environ)
+            env.update(env_case)
+            env["IB_DUMP"] = os.path.join(wd, "d")
+            subprocess.run([binary], cwd=wd, env=env, check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL, timeout=900)
+            return make_golden.record_of(pyoracle.read_dump(os.path.join(wd, "d_000000.bin")))
+
+    with ThreadPoolExecutor(max(1, workers)) as pool:
+        return list(pool.map(one, envs))
+
+
+def config4_section(ib, wl, ind, stream, ncases: int, steps: int, warm: int = 4):
+    """The batched airfoil workload: ncases of the seeded 64 (the reference's
+    own meshes, 2-5 levels, an immersed airfoil each) in one batch, mixed
+    precision and FP64, persistent graph-replayed stage launches; leaf-cell
+    updates/s over the levels that march; |dCl|, |dCd| of mixed against FP64
+    per case after the run; tagging of every leaf box by the learned
+    indicator and by the plain criterion."""
+    import numpy as np
+    import torch
+    envs = config4_cases()[:ncases]
+    t0 = time.perf_counter()
+    recs = config4_meshes(envs, host_workers(1.5e9))
+    mesh_s = time.perf_counter() - t0
+    leaves = [int((g["kind"] == 0).sum()) for g in recs]
+    per_step = sum(marched_cells(g, warm, steps) for g in recs) / steps
+    out = {"workload": f"the first {ncases} of 64 seeded NACA0012/0015 cases (seed 0): Mach "
+                       "U[0.1,0.8], AoA U[-5,10] deg, Re log-U[2e3,2e4], 2-5 AMR levels, "
+                       "leaf-count target log-U[5e4,8e5]; meshes and initial states from the "
+                       "reference's own mesh generation",
+           "cases": ncases, "leaf_cells_total": sum(leaves), "leaf_cells_min": min(leaves),
+           "leaf_cells_max": max(leaves), "cell_updates_per_step": per_step,
+           "host_mesh_generation_s": mesh_s, "timed_steps": steps}
+    forces = {}
+    for name, prec in (("mixed", ib.MIXED), ("fp64", ib.FP64)):
+        sols = []
+        for g in recs:
+            s = wl.naca_solver(g, 0, prec)
+            s.set_stream(stream.cuda_stream)
+            sols.append(s)
+        b = ib.Batch(sols)
+        b.run(0, warm)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        b.run(warm, steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        info = b.info()
+        out[name] = {"value": per_step * steps / (ms / 1e3), "unit": UNIT,
+                     "ms_per_step": ms / steps, "persistent_ctas": info["grid"]}
+        forces[name] = [s.wall_forces()[:, :2].sum(axis=0) / F_REF for s in sols]
+        if name == "mixed":
+            # tagging of every box of every case: learned (an untrained
+            # network costs what a trained one does) and plain
+            li = ind.LearnedIndicator(sols[0], seed=0)
+            rule = wl.naca_tag_rule(5, [20.0 / 128 / 2 ** k for k in range(5)])
+            nbox = sum(s.ncells for s in sols)
+            tags = torch.empty(nbox, dtype=torch.uint8).pin_memory().numpy()
+            for learned, key in ((1, "learned_tag_ms"), (0, "plain_tag_ms")):
+                dp = li.params.data_ptr() if learned else 0
+                b.tag_mesh(rule, dp, tags)
+                best = []
+                for _ in range(3):
+                    torch.cuda.synchronize()
+                    t1 = time.perf_counter()
+                    b.tag_mesh(rule, dp, tags)
+                    best.append((time.perf_counter() - t1) * 1e3)
+                out[key] = min(best)
+            out["tag_boxes"] = nbox
+            out["learned_value"] = per_step / ((ms / steps + out["learned_tag_ms"] / REGRID_EVERY)
+                                               / 1e3)
+        b.close()
+        for s in sols:
+            s.close()
+    d = np.abs(np.array(forces["mixed"]) - np.array(forces["fp64"]))
+    out["mixed_vs_fp64_max_dcd"], out["mixed_vs_fp64_max_dcl"] = float(d[:, 0].max()), float(d[:, 1].max())
+    out["gate_1e-3"] = bool(d.max() < 1e-3)
+    out["learned_note"] = ("learned_value: the mixed batch with learned tagging of every leaf box "
+                           f"once per {REGRID_EVERY} steps; the regrid itself is the reference's "
+                           "host code and not timed")
+    return out
+
+
 def accuracy_section(ib, wl, stream, n: int = 2048, steps: int = 500):
     """The bandwidth workload's accuracy: the 2048^2 vortex after `steps`
     steps, L2 density error vs the exact solution for FP64 and mixed, and
@@ -862,6 +995,9 @@ def our_arm(args):
         for s in bsols:
             s.close()
         extra["config1"] = config1_section(ib, wl, stream, max_over_ranks, rank=rank)
+        if rank == 0 and args.config4_cases > 0:
+            extra["config4"] = config4_section(ib, wl, pkg.indicator, stream, args.config4_cases,
+                                               steps=args.steps)
         if not args.no_config3:
             extra["config3"] = config3_section(rank=rank)
         if rank == 0:
@@ -1045,6 +1181,8 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config4-cases", type=int, default=CONFIG4_DEFAULT_CASES,
+                    help="batched airfoil cases of the seeded 64 to run (0 skips the section)")
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the moving-body section (about three minutes of host mesh work)")
     ap.add_argument("--headline-only", action="store_true",

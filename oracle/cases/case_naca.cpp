@@ -24,7 +24,9 @@
 // format, then read by Body::ReadShapeFile.
 //
 // Environment: IB_NX (base cells per side, default 128), IB_LEVELS (mesh
-// levels, default 4), IB_NPTS (surface points per side, default 200).
+// levels, default 4), IB_NPTS (surface points per side, default 200), and for
+// families of airfoil cases IB_MACH, IB_RE, IB_AOA (degrees) and IB_THICK
+// (thickness over chord, 0.12 for a NACA0012).
 //
 // Runtime regrids (harness options; off by default).  The shipped case calls
 // AMR::PerformAdaptive every 2 steps but requests neither refinement nor
@@ -83,7 +85,7 @@ const int dts_space_var = 1 << 30;
 #define CASE_LEVELS 6
 #define CASE_DOMAIN 30.0
 #define CASE_MACH 0.2
-#define CASE_MU_REF (1.0 / 1.0e4)   // Re = 1e4
+#define CASE_RE 1.0e4
 #define CASE_AOA_DEG 0.0
 #define CASE_THICKNESS 0.15
 #define CASE_PROFILE "naca0015"
@@ -93,7 +95,7 @@ const int dts_space_var = 1 << 30;
 #define CASE_LEVELS 4
 #define CASE_DOMAIN 20.0
 #define CASE_MACH 0.5
-#define CASE_MU_REF (1.0 / 5000.0)  // Re = 5000
+#define CASE_RE 5000.0
 #define CASE_AOA_DEG 2.0
 #define CASE_THICKNESS 0.12
 #define CASE_PROFILE "naca0012"
@@ -115,9 +117,15 @@ const bool moveflag = CASE_MOVING;
 // ---- reference scales (constant-initialised) ------------------------------
 double roe_ref = 1.0;
 double L_ref = 1.0;
-double mu_ref = CASE_MU_REF;
+// Mach number and Reynolds number of the case, IB_MACH and IB_RE overriding
+// the defaults: these two are initialised at start-up from the environment,
+// before FlowConstants.cpp derives the gas constants from them (the case
+// object is linked first, so its initialisers run first; the oracle tests
+// check the dumped constants)
+static const double kMach = case_env_double("IB_MACH", CASE_MACH);
+double mu_ref = 1.0 / case_env_double("IB_RE", CASE_RE);
 double u_ref = 1.0;
-double T_ref = 1.0 / (CASE_MACH * CASE_MACH * 287.4 * 1.4);
+double T_ref = 1.0 / (kMach * kMach * 287.4 * 1.4);
 
 bool additional_output = false;
 const int init_jump = 0;
@@ -128,7 +136,8 @@ const char soln_file_name[30] = "none";
 
 // ---- airfoil placement -----------------------------------------------------
 static const double kPi = 3.14159265358979323846;
-static const double kAoA = CASE_AOA_DEG / 180.0 * kPi;
+static const double kAoA = case_env_double("IB_AOA", CASE_AOA_DEG) / 180.0 * kPi;
+static const double kThickness = case_env_double("IB_THICK", CASE_THICKNESS);
 // leading edge; chord 1 along +x, centred in the domain
 static const double kLeX = 0.5 * CASE_DOMAIN - 0.5, kLeY = 0.5 * CASE_DOMAIN;
 static const double kPitchX = 0.25;               // moment / body centre at quarter chord
@@ -151,7 +160,7 @@ static void write_surface(const string &path, int n, double sign) {
   for (int layer = 0; layer < 2; ++layer)
     for (int i = 0; i < n; ++i) {
       double x = 0.5 * (1.0 + cos(3.14159265358979323846 * i / (n - 1)));  // 1 -> 0
-      double y = sign * naca_half_thickness(x, CASE_THICKNESS);
+      double y = sign * naca_half_thickness(x, kThickness);
       fprintf(f, "%.17g %.17g %.17g\n", x, y, layer ? 0.1 : 0.0);
     }
   for (int i = 1; i < n; ++i) fprintf(f, "%d %d %d %d\n", i, i + 1, n + i + 1, n + i);
