@@ -1171,6 +1171,13 @@ struct ibgpu_batch {
   std::vector<cudaGraphExec_t> graphs;  // per phase r (+ period with the CFL pass)
   int2 *d_cfl_work = nullptr;      // every tile of every case
   int ncfl = 0, dt_var_step = 1;
+  // cases with different CFL intervals (each dividing the schedule period):
+  // per phase r the tiles and the indices of the cases whose CFL pass runs
+  // when ts % period == r
+  bool mixed_cfl = false;
+  std::vector<int2 *> d_cfl_work_r;
+  std::vector<int *> d_cfl_cases_r;
+  std::vector<int> ncfl_r, ncfl_cases_r;
   bool folds = false;  // every case single-level without bodies: CFL folded into final stages
   int grid = 0;                    // CTAs of the persistent launch (0 = one per item)
   int device = 0;
@@ -1194,6 +1201,10 @@ struct ibgpu_batch {
     d_work.clear();
     cudaFree(d_cfl_work);
     d_cfl_work = nullptr;
+    for (auto w : d_cfl_work_r) cudaFree(w);
+    for (auto w : d_cfl_cases_r) cudaFree(w);
+    d_cfl_work_r.clear();
+    d_cfl_cases_r.clear();
     cudaFree(d_args);
     cudaFree(d_ccs);
     cudaFree(d_phase_base);
@@ -1214,7 +1225,11 @@ namespace {
 
 // cfl: 0 none, 1 the CFL pass, 2 the bound folded into the previous step
 int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
-  if (cfl == 1) {
+  if (cfl == 1 && b->mixed_cfl) {
+    fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work_r[r], b->ncfl_r[r], b->nstages,
+                           b->d_phase_base, b->ncfl_cases_r[r], 0, st, b->d_cfl_cases_r[r]);
+    CK(cudaGetLastError());
+  } else if (cfl == 1) {
     fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work, b->ncfl, b->nstages,
                            b->d_phase_base, (int)b->cases.size(), 0, st);
     CK(cudaGetLastError());
@@ -1363,10 +1378,8 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
                 (cs.viscous != 0) == (c0.viscous != 0) && cs.nstages == c0.nstages &&
                 c->device == cases[0]->device;
     for (int k = 0; same && k < cs.nstages; ++k) same = cs.tp[k] == c0.tp[k];
-    same = same && cs.dt_var_step == c0.dt_var_step;
     if (!same) {
-      g_last_error = "batched cases differ in precision, limiter, viscosity, stages, dt_var_step "
-                     "or device";
+      g_last_error = "batched cases differ in precision, limiter, viscosity, stages or device";
       return IBGPU_E_ARG;
     }
   }
@@ -1390,6 +1403,17 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
       if (b->period % c->cs.march_step[l] != 0) {
         delete b;
         g_last_error = "marching steps of the batched cases have no common period";
+        return IBGPU_E_ARG;
+      }
+  // CFL intervals: all equal, or each dividing the schedule period (then the
+  // cases whose pass runs depend only on ts % period)
+  for (auto *c : b->cases) b->mixed_cfl = b->mixed_cfl || c->cs.dt_var_step != c0.dt_var_step;
+  if (b->mixed_cfl)
+    for (auto *c : b->cases)
+      if (b->period % c->cs.dt_var_step != 0) {
+        delete b;
+        g_last_error = "batched cases with different dt_var_step need each to divide the "
+                       "schedule period";
         return IBGPU_E_ARG;
       }
   const int S = b->nstages;
@@ -1460,6 +1484,31 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
     e = cudaMemcpy(b->d_cfl_work, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_fail(e, "batch CFL work list"));
   }
+  if (b->mixed_cfl) {
+    b->d_cfl_work_r.assign(b->period, nullptr);
+    b->d_cfl_cases_r.assign(b->period, nullptr);
+    b->ncfl_r.assign(b->period, 0);
+    b->ncfl_cases_r.assign(b->period, 0);
+    for (int r = 0; r < b->period; ++r) {
+      std::vector<int2> w;
+      std::vector<int> cl;
+      for (int i = 0; i < ncases; ++i) {
+        if (r % b->cases[i]->cs.dt_var_step != 0) continue;
+        cl.push_back(i);
+        for (int t = 0; t < (int)b->cases[i]->ntiles; ++t) w.push_back(make_int2(i, t));
+      }
+      b->ncfl_r[r] = (int)w.size();
+      b->ncfl_cases_r[r] = (int)cl.size();
+      if (cl.empty()) continue;
+      if ((rc = dev_alloc(&b->d_cfl_work_r[r], w.size())) ||
+          (rc = dev_alloc(&b->d_cfl_cases_r[r], cl.size())))
+        return fail(rc);
+      e = cudaMemcpy(b->d_cfl_work_r[r], w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_cfl_cases_r[r], cl.data(), cl.size() * sizeof(int), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(cuda_fail(e, "batch CFL work list"));
+    }
+  }
   *out = b;
   return IBGPU_OK;
 }
@@ -1500,7 +1549,8 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
       if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i], true))) return rc;
       marched[i] = marched_cells(b->cases[i], ts);
     }
-    const int cfl = (ts % b->dt_var_step) != 0 ? 0 : (b->folds && step > 0 ? 2 : 1);
+    const bool cfl_now = b->mixed_cfl ? b->ncfl_cases_r[r] > 0 : (ts % b->dt_var_step) == 0;
+    const int cfl = !cfl_now ? 0 : (b->folds && step > 0 ? 2 : 1);
     fast::launch_set_phase_base(b->d_phase_base, 8 * step, b->folds && step + 1 < nsteps, st);
     if (b->timing) {
       CK(cudaEventCreate(&e0));

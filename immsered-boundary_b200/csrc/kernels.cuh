@@ -1224,13 +1224,33 @@ __global__ void step_begin_batch(const StageArgs *__restrict__ args, int ncases,
   for (int k = 0; k < 5; ++k) d->res_bits[k] = 0ull;
 }
 
+// dt of the listed batched cases only (the cases whose CFL pass ran)
+__global__ void finalize_dt_batch_list(const StageArgs *__restrict__ args,
+                                       const CaseConst *__restrict__ ccs,
+                                       const int *__restrict__ list, int n, int nstages) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = list[k];
+  DevDiag *d = args[c * nstages].diag;
+  double cdt = __longlong_as_double((long long)d->cfl_bits);
+  double cand = d->dt * ccs[c].dt_ratio;
+  d->dt = (cand < cdt) ? cand : cdt;
+}
+
 void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
-                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st) {
+                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st,
+                      const int *case_list) {
   if (nwork > 0) {
     if (grid < 1 || grid > nwork) grid = nwork;
     cfl_kernel_batch<<<grid, kTileCells, 0, st>>>(args, ccs, work, nwork, nstages, phase_base);
   }
-  finalize_dt_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, ncases, nstages);
+  if (case_list) {
+    if (ncases > 0)
+      finalize_dt_batch_list<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, case_list, ncases,
+                                                                    nstages);
+  } else {
+    finalize_dt_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, ncases, nstages);
+  }
 }
 
 void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cudaStream_t st) {

@@ -54,8 +54,11 @@ cudaError_t batch_table_write(int offset, const void *src, int bytes);
 void launch_set_phase_base(int *phase_base, int value, int fold, cudaStream_t st);
 void launch_take_folded_batch(const StageArgs *args, const CaseConst *ccs, int ncases, int nstages,
                               cudaStream_t st);
+// CFL pass over the work list's tiles, then dt of the first ncases cases, or
+// with case_list of the ncases cases it lists
 void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
-                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st);
+                      int nstages, const int *phase_base, int ncases, int grid, cudaStream_t st,
+                      const int *case_list = nullptr);
 void launch_step_begin_batch(const StageArgs *args, int ncases, int nstages, cudaStream_t st);
 }  // namespace fast
 

@@ -294,8 +294,11 @@ void ibgpu_destroy(ibgpu_ctx *ctx);
  * captured once in a CUDA graph and replayed.  On the first run an
  * autotuner times the candidate CTA counts of the persistent launch and
  * keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
- * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; the batch
- * runs on the first context's stream.  Uploads to a context (topology,
+ * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; their CFL
+ * intervals (dt_var_step) may differ when each divides the longest marching
+ * step of the batch (each case then takes its CFL pass on its own steps, as
+ * meshes of different depths do); the batch runs on the first context's
+ * stream.  Uploads to a context (topology,
  * lists) invalidate a batch that holds it: destroy and recreate it.  A batch
  * is destroyed before any context it holds.
  * ------------------------------------------------------------------------- */

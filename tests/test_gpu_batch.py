@@ -146,3 +146,27 @@ def test_batch_tag_mesh_equals_per_case_tagging(cuda_lib):
     b.close()
     for s in sols:
         s.close()
+
+
+def test_batched_cases_with_different_cfl_intervals(cuda_lib):
+    """A 3-level and a 4-level airfoil case (CFL pass every 4 and every 8
+    steps: the reference rounds dt_var_step up to the coarsest level's step)
+    in one batch for two schedule periods, against each case stepped alone:
+    each case takes its CFL pass on its own steps."""
+    g3 = make_golden.load("naca_minmod_s4_n64_l3")
+    g4 = make_golden.load("naca_minmod_s4_n128_l4")
+    dvs = [int(g["scalars"][0][15 + int(g["scalars"][0][14])]) for g in (g3, g4)]
+    assert dvs[0] != dvs[1]
+    sols = [wl.naca_solver(g, 0, ib.FP64) for g in (g3, g4)]
+    batch = ib.Batch(sols)
+    assert batch.info()["period"] == 8
+    batch.run(0, 16)
+    for s, g in zip(sols, (g3, g4)):
+        r = wl.naca_solver(g, 0, ib.FP64)
+        r.run(0, 16)
+        assert s.dt == r.dt
+        assert np.array_equal(s.download(), r.download())
+        r.close()
+    batch.close()
+    for s in sols:
+        s.close()
