@@ -221,9 +221,10 @@ __global__ void ib_compute_kernel(IbArgs a, CaseConst cc) {
   o[3] = p;
   o[4] = e;
   o[5] = T;
-  if (hT < 0.0) raise_error(a.diag, a.phase, ERR_IB_NEG_T, a.cell[i]);
+  const int phase = a.phase + (a.phase_base ? *a.phase_base : 0);
+  if (hT < 0.0) raise_error(a.diag, phase, ERR_IB_NEG_T, a.cell[i]);
   if (isnan(roe) || isnan(u) || isnan(v) || isnan(p) || isnan(T) || isnan(e))
-    raise_error(a.diag, a.phase, ERR_IB_NAN, a.cell[i]);
+    raise_error(a.diag, phase, ERR_IB_NAN, a.cell[i]);
 }
 
 // Phase 2: write them (Body.cpp:1490-1494)

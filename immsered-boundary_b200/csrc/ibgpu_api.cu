@@ -10,6 +10,8 @@
 #include <new>
 #include <string>
 #include <unordered_map>
+#include <map>
+#include <numeric>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -826,7 +828,8 @@ bool folds_cfl(const ibgpu_ctx *ctx) {
 // prolongation on their schedules, immersed-body ghosts, CFL dt, domain
 // ghosts and the viscous flux of the levels that march.
 int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer &tm,
-                     bool batched = false, bool fresh_cfl = false) {
+                     bool batched = false, bool fresh_cfl = false,
+                     const int *phase_base = nullptr) {
   const ibgpu_case &cs = ctx->cs;
   const bool exact = cs.precision == IBGPU_FP64_EXACT;
   const bool mixed = cs.precision == IBGPU_MIXED;
@@ -873,7 +876,10 @@ int enqueue_prestage(ibgpu_ctx *ctx, int ts, int step, cudaStream_t st, RunTimer
     ia.out = ctx->d_ib_out;
     ia.n = ctx->n_ib;
     for (int f = 0; f < kStateFields; ++f) ia.s0[f] = ctx->d_s0[f];
-    ia.phase = pbase + 0;
+    // the abort-order phase of this step: from the host, or (a captured
+    // batch step replayed for every step) from the batch's device counter
+    ia.phase = phase_base ? 0 : pbase + 0;
+    ia.phase_base = phase_base;
     ia.diag = ctx->d_diag;
     if (exact) exact::launch_ib(ia, ctx->cc, st);
     else fast::launch_ib(ia, ctx->cc, st);
@@ -1168,7 +1174,14 @@ struct ibgpu_batch {
   int *d_phase_base = nullptr;
   std::vector<int2 *> d_work;      // per schedule phase r = ts % period
   std::vector<int> nwork;
-  std::vector<cudaGraphExec_t> graphs;  // per phase r (+ period with the CFL pass)
+  // whole-step graphs (every case's ghost fills and viscous pass on parallel
+  // branches, then the merged CFL and stage launches), captured on first use
+  // per (ts % full_period, CFL variant)
+  std::map<int, cudaGraphExec_t> graphs;
+  bool graphs_ready = false;  // every phase's graphs captured (first run after tuning)
+  int full_period = 1;  // every schedule of every case repeats with it
+  std::vector<cudaStream_t> fork;  // branches of the captured steps
+  std::vector<cudaEvent_t> ev_fork_join;
   int2 *d_cfl_work = nullptr;      // every tile of every case
   int ncfl = 0, dt_var_step = 1;
   // cases with different CFL intervals (each dividing the schedule period):
@@ -1193,10 +1206,18 @@ struct ibgpu_batch {
   std::vector<int> tune_grid;
   std::vector<float> tune_ms;
 
-  void release() {
-    for (auto g : graphs)
-      if (g) cudaGraphExecDestroy(g);
+  void drop_graphs() {
+    for (auto &g : graphs)
+      if (g.second) cudaGraphExecDestroy(g.second);
     graphs.clear();
+    graphs_ready = false;
+  }
+  void release() {
+    drop_graphs();
+    for (auto f : fork) cudaStreamDestroy(f);
+    fork.clear();
+    for (auto e : ev_fork_join) cudaEventDestroy(e);
+    ev_fork_join.clear();
     for (auto w : d_work) cudaFree(w);
     d_work.clear();
     cudaFree(d_cfl_work);
@@ -1226,9 +1247,11 @@ namespace {
 // cfl: 0 none, 1 the CFL pass, 2 the bound folded into the previous step
 int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
   if (cfl == 1 && b->mixed_cfl) {
-    fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work_r[r], b->ncfl_r[r], b->nstages,
-                           b->d_phase_base, b->ncfl_cases_r[r], 0, st, b->d_cfl_cases_r[r]);
-    CK(cudaGetLastError());
+    if (b->ncfl_cases_r[r] > 0) {  // (phases without a CFL pass never take this graph)
+      fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work_r[r], b->ncfl_r[r], b->nstages,
+                             b->d_phase_base, b->ncfl_cases_r[r], 0, st, b->d_cfl_cases_r[r]);
+      CK(cudaGetLastError());
+    }
   } else if (cfl == 1) {
     fast::launch_cfl_batch(b->d_args, b->d_ccs, b->d_cfl_work, b->ncfl, b->nstages,
                            b->d_phase_base, (int)b->cases.size(), 0, st);
@@ -1340,22 +1363,64 @@ int write_batch_table(ibgpu_batch *b, const std::vector<StageArgs> &args,
 
 // One graph per schedule phase holding the nstages merged stage launches;
 // without a capturable stream the launches are issued directly.
-int build_graphs(ibgpu_batch *b) {
-  b->graphs.assign(3 * b->period, nullptr);
-  if (b->stream == nullptr) return IBGPU_OK;  // legacy stream: not capturable
-  for (int v = 0; v < 3 * b->period; ++v) {
-    const int r = v % b->period;
-    const int cfl = v / b->period;
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_batch_stages(b, r, cfl, b->stream);
-    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&b->graphs[v], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+// The graph of one whole batch step at schedule phase q = ts % full_period
+// with CFL variant cfl, captured on first use: the cases' ghost fills and
+// viscous passes (their abort phase read from the batch's device counter)
+// forked onto the batch's branch streams, joined, then the merged CFL and
+// stage launches.  Nothing in it depends on the step index except through
+// the device counter, so one capture serves every step of that phase.
+int batch_step_graph(ibgpu_batch *b, int q, int cfl, cudaGraphExec_t *out) {
+  const int key = q * 3 + cfl;
+  auto it = b->graphs.find(key);
+  if (it != b->graphs.end()) {
+    *out = it->second;
+    return IBGPU_OK;
   }
+  cudaStream_t st = b->stream;
+  const int nf = (int)b->fork.size();
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int rc = IBGPU_OK;
+  cudaError_t e = cudaEventRecord(b->ev_fork_join[nf], st);
+  for (int k = 0; k < nf && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(b->fork[k], b->ev_fork_join[nf], 0);
+  for (size_t i = 0; i < b->cases.size() && e == cudaSuccess && !rc; ++i) {
+    RunTimer tm{b->cases[i], b->fork[i % nf], {}, {}};
+    tm.off = true;
+    rc = enqueue_prestage(b->cases[i], q, 1, b->fork[i % nf], tm, true, false, b->d_phase_base);
+  }
+  for (int k = 0; k < nf && e == cudaSuccess && !rc; ++k) {
+    e = cudaEventRecord(b->ev_fork_join[k], b->fork[k]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_fork_join[k], 0);
+  }
+  if (e == cudaSuccess && !rc) rc = enqueue_batch_stages(b, q % b->period, cfl, st);
+  cudaError_t e2 = cudaStreamEndCapture(st, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "batch step capture");
+  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  b->graphs[key] = x;
+  *out = x;
+  return IBGPU_OK;
+}
+
+// Capture the graphs of every schedule phase up front (the first run after
+// tuning), so that later runs replay them without capturing.
+int batch_prepare_graphs(ibgpu_batch *b) {
+  if (b->graphs_ready) return IBGPU_OK;
+  for (int q = 0; q < b->full_period; ++q) {
+    const bool cfl_now = b->mixed_cfl ? b->ncfl_cases_r[q % b->period] > 0 : (q % b->dt_var_step) == 0;
+    cudaGraphExec_t gx = nullptr;
+    int rc = batch_step_graph(b, q, cfl_now ? 1 : 0, &gx);
+    if (!rc && cfl_now && b->folds) rc = batch_step_graph(b, q, 2, &gx);
+    if (rc) return rc;
+  }
+  b->graphs_ready = true;
   return IBGPU_OK;
 }
 
@@ -1405,6 +1470,21 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
         g_last_error = "marching steps of the batched cases have no common period";
         return IBGPU_E_ARG;
       }
+  // every schedule (marching, restriction, prolongation, CFL) repeats with
+  // the least common multiple of its steps
+  {
+    auto lcm = [](int a, int c) { return a / std::gcd(a, c) * c; };
+    int fp = b->period;
+    for (auto *c : b->cases) {
+      fp = lcm(fp, c->cs.dt_var_step);
+      for (int l = 0; l < c->cs.nlevels; ++l) {
+        fp = lcm(fp, c->cs.march_step[l]);
+        if (l >= 1) fp = lcm(lcm(fp, c->cs.average_step[l]), c->cs.prolong_step[l]);
+      }
+      if (fp > 4096) break;
+    }
+    b->full_period = fp;
+  }
   // CFL intervals: all equal, or each dividing the schedule period (then the
   // cases whose pass runs depend only on ts % period)
   for (auto *c : b->cases) b->mixed_cfl = b->mixed_cfl || c->cs.dt_var_step != c0.dt_var_step;
@@ -1509,6 +1589,18 @@ int ibgpu_batch_create(ibgpu_ctx *const *cases, int ncases, ibgpu_batch **out) {
       if (e != cudaSuccess) return fail(cuda_fail(e, "batch CFL work list"));
     }
   }
+  // branch streams of the captured steps: up to eight, cases round robin
+  {
+    const int nf = std::min(8, ncases);
+    b->fork.assign(nf, nullptr);
+    b->ev_fork_join.assign(nf + 1, nullptr);
+    for (int k = 0; k < nf; ++k)
+      if ((e = cudaStreamCreateWithFlags(&b->fork[k], cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_fail(e, "batch branch stream"));
+    for (auto &ev : b->ev_fork_join)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail(cuda_fail(e, "batch branch event"));
+  }
   *out = b;
   return IBGPU_OK;
 }
@@ -1527,8 +1619,14 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
     } else if ((rc = autotune(b))) {
       return rc;
     }
-    if ((rc = build_graphs(b))) return rc;
+    b->drop_graphs();  // captured with the previous CTA count
   }
+  // captured whole steps, unless something asks for per-launch timing or the
+  // batch runs on the legacy stream (not capturable); captured before this
+  // run's first work is enqueued
+  bool use_graphs = b->stream != nullptr && !b->timing && b->full_period <= 4096;
+  for (int i = 0; i < n; ++i) use_graphs = use_graphs && !b->cases[i]->timing;
+  if (use_graphs && (rc = batch_prepare_graphs(b))) return rc;
   for (int i = 0; i < n; ++i) {
     if (b->cases[i]->download_pending) {
       CK(cudaStreamWaitEvent(st, b->cases[i]->ev_copied, 0));
@@ -1538,6 +1636,7 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
   }
   std::vector<RunTimer> tms;
   for (int i = 0; i < n; ++i) tms.push_back(RunTimer{b->cases[i], st, {}, {}});
+
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sev;
   std::vector<int64_t> marched(n, 0);
@@ -1545,24 +1644,29 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
     const int ts = ts0 + step;
     const int r = ts % b->period;
     if (step > 0) fast::launch_step_begin_batch(b->d_args, n, b->nstages, st);
-    for (int i = 0; i < n; ++i) {
-      if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i], true))) return rc;
-      marched[i] = marched_cells(b->cases[i], ts);
-    }
+    for (int i = 0; i < n; ++i) marched[i] = marched_cells(b->cases[i], ts);
     const bool cfl_now = b->mixed_cfl ? b->ncfl_cases_r[r] > 0 : (ts % b->dt_var_step) == 0;
     const int cfl = !cfl_now ? 0 : (b->folds && step > 0 ? 2 : 1);
     fast::launch_set_phase_base(b->d_phase_base, 8 * step, b->folds && step + 1 < nsteps, st);
-    if (b->timing) {
-      CK(cudaEventCreate(&e0));
-      CK(cudaEventCreate(&e1));
-      CK(cudaEventRecord(e0, st));
-    }
-    const int v = r + cfl * b->period;
-    if (b->graphs[v]) CK(cudaGraphLaunch(b->graphs[v], st));
-    else if ((rc = enqueue_batch_stages(b, r, cfl, st))) return rc;
-    if (b->timing) {
-      CK(cudaEventRecord(e1, st));
-      sev.push_back({e0, e1});
+    if (use_graphs) {
+      // the whole step as one graph (the stage launches' own timing is not
+      // separable then: b->timing runs without graphs)
+      cudaGraphExec_t gx = nullptr;
+      if ((rc = batch_step_graph(b, ts % b->full_period, cfl, &gx))) return rc;
+      CK(cudaGraphLaunch(gx, st));
+    } else {
+      for (int i = 0; i < n; ++i)
+        if ((rc = enqueue_prestage(b->cases[i], ts, step, st, tms[i], true))) return rc;
+      if (b->timing) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, st));
+      }
+      if ((rc = enqueue_batch_stages(b, r, cfl, st))) return rc;
+      if (b->timing) {
+        CK(cudaEventRecord(e1, st));
+        sev.push_back({e0, e1});
+      }
     }
   }
   for (int i = 0; i < n; ++i)
@@ -1642,9 +1746,7 @@ int ibgpu_batch_tag_mesh(ibgpu_batch *b, const ibgpu_tag_rule *rule, const float
 int ibgpu_batch_set_grid(ibgpu_batch *b, int grid) {
   if (!b || grid < -1) return IBGPU_E_ARG;
   if (b->stream) CK(cudaStreamSynchronize(b->stream));  // captured graphs may be in flight
-  for (auto g : b->graphs)
-    if (g) cudaGraphExecDestroy(g);
-  b->graphs.clear();
+  b->drop_graphs();
   b->fixed_grid = grid;
   b->tuned = false;  // the next run tunes (grid -1) or takes the count, and recaptures
   return IBGPU_OK;

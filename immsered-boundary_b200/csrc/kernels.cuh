@@ -1248,7 +1248,7 @@ void launch_cfl_batch(const StageArgs *args, const CaseConst *ccs, const int2 *w
     if (ncases > 0)
       finalize_dt_batch_list<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, case_list, ncases,
                                                                     nstages);
-  } else {
+  } else if (ncases > 0) {
     finalize_dt_batch<<<(ncases + 127) / 128, 128, 0, st>>>(args, ccs, ncases, nstages);
   }
 }

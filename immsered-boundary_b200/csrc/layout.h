@@ -156,6 +156,9 @@ struct IbArgs {
   double *s0[kStateFields];
   int phase;
   DevDiag *diag;
+  // when set, the abort-order phase is *phase_base + phase (a batch replays
+  // one captured launch for every step and keeps the step's base on the device)
+  const int *phase_base;
 };
 
 struct ForceArgs {

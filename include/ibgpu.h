@@ -288,10 +288,12 @@ void ibgpu_destroy(ibgpu_ctx *ctx);
  * Batched independent cases (no counterpart in the reference, which runs one
  * case per process): several contexts, each with its own mesh, state and
  * case constants, advance together.  Every step runs each case's ghost
- * fills, CFL and viscous pass, then ONE persistent launch per stage covers
- * the marching tiles of all cases (a work list of (case, tile) pairs per
- * subcycling phase, cases interleaved); the stage launches of each phase are
- * captured once in a CUDA graph and replayed.  On the first run an
+ * fills and viscous pass, one CFL launch over the cases whose pass is due,
+ * then ONE persistent launch per stage covering the marching tiles of all
+ * cases (a work list of (case, tile) pairs per subcycling phase, cases
+ * interleaved).  The whole step is captured once per schedule phase in a
+ * CUDA graph (the cases' ghost fills on parallel branches) and replayed;
+ * the captures happen at the start of the first run.  On the first run an
  * autotuner times the candidate CTA counts of the persistent launch and
  * keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
  * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; their CFL
@@ -312,7 +314,8 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
  * per work item, > 0 = that many persistent CTAs, -1 = chosen by the
  * autotuner at the next run (the default). */
 int ibgpu_batch_set_grid(ibgpu_batch *b, int grid);
-/* Event timing of the merged stage launches (total ms, launch count). */
+/* Event timing of the merged stage launches (total ms, launch count); a
+ * batch with timing enabled runs its steps as direct launches, not graphs. */
 int ibgpu_batch_set_timing(ibgpu_batch *b, int enable);
 /* Chosen CTA count (0 = one CTA per work item), subcycling period, timing. */
 int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage_ms,
