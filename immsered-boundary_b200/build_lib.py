@@ -25,6 +25,7 @@ UNITS = {
     "kernels_exact.cu": ["-fmad=false"],
     "noalloc.cu": [],
     "indicator.cu": [],
+    "interfaces.cu": [],
 }
 
 

@@ -40,7 +40,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
            "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
-           "ibgpu_set_state_rows")
+           "ibgpu_set_state_rows", "ibgpu_build_interfaces")
 ROWS_FLOWVARS, ROWS_COMPACT = 7, 4
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
@@ -89,6 +89,13 @@ class Ib(ctypes.Structure):
                 ("cellf", ctypes.POINTER(ctypes.c_double)), ("npatches", ctypes.c_int64),
                 ("patch", ctypes.POINTER(ctypes.c_int32)), ("patchf", ctypes.POINTER(ctypes.c_double)),
                 ("nbodies", ctypes.c_int), ("body_center", ctypes.POINTER(ctypes.c_double))]
+
+
+class InterfaceLists(ctypes.Structure):
+    _fields_ = [("nres", ctypes.c_int64), ("npro", ctypes.c_int64), ("nghost", ctypes.c_int64),
+                ("cap_res", ctypes.c_int64), ("cap_pro", ctypes.c_int64),
+                ("cap_ghost", ctypes.c_int64), ("res", ctypes.c_void_p), ("pro", ctypes.c_void_p),
+                ("ghost", ctypes.c_void_p)]
 
 
 class Cells(ctypes.Structure):
@@ -197,6 +204,8 @@ def lib(path: str | None = None):
     L.ibgpu_layout_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_update_flags.argtypes = [vp, vp]
     L.ibgpu_set_state_rows.argtypes = [vp, ctypes.c_int]
+    L.ibgpu_build_interfaces.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Cells),
+                                         ctypes.POINTER(InterfaceLists)]
     L.ibgpu_upload_interfaces.argtypes = [vp, ctypes.POINTER(CfPairs)]
     L.ibgpu_upload_boundaries.argtypes = [vp, ctypes.POINTER(Bc)]
     L.ibgpu_upload_ib.argtypes = [vp, ctypes.POINTER(Ib)]
@@ -379,6 +388,31 @@ class FlowSolver:
         assert len(f) == self.ncells
         _check(lib().ibgpu_update_flags(self._ctx, f.ctypes.data_as(ctypes.c_void_p)),
                "ibgpu_update_flags")
+
+    def build_interfaces(self, nlevels: int, level, ix, iy):
+        """Coarse/fine interface lists of the mesh whose leaf cells are
+        (level, ix, iy), built on the device: (restriction rows (n, 12),
+        prolongation rows (n, 11), interface ghost cells (n, 3))."""
+        lv = np.ascontiguousarray(level, np.int32)
+        x = np.ascontiguousarray(ix, np.int32)
+        y = np.ascontiguousarray(iy, np.int32)
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        cells = Cells(len(lv), lv.ctypes.data_as(i32), x.ctypes.data_as(i32),
+                      y.ctypes.data_as(i32), None)
+        out = InterfaceLists()
+        rc = lib().ibgpu_build_interfaces(self._ctx, int(nlevels), ctypes.byref(cells),
+                                          ctypes.byref(out))
+        if rc not in (OK, E_ARG) or (rc == E_ARG and out.nres + out.npro + out.nghost == 0
+                                     and len(lv)):
+            _check(rc, "ibgpu_build_interfaces")
+        res = np.zeros((out.nres, 12), np.int32)
+        pro = np.zeros((out.npro, 11), np.int32)
+        ghost = np.zeros((out.nghost, 3), np.int32)
+        out.cap_res, out.cap_pro, out.cap_ghost = out.nres, out.npro, out.nghost
+        out.res, out.pro, out.ghost = (res.ctypes.data, pro.ctypes.data, ghost.ctypes.data)
+        _check(lib().ibgpu_build_interfaces(self._ctx, int(nlevels), ctypes.byref(cells),
+                                            ctypes.byref(out)), "ibgpu_build_interfaces")
+        return res, pro, ghost
 
     def upload_interfaces(self, res, pro):
         """Coarse/fine pairs as (n, 11) int arrays: level, cx, cy, 4 x (fx, fy)."""

@@ -212,6 +212,35 @@ int ibgpu_wall_forces(ibgpu_ctx *ctx, double *out);
  * IBGPU_E_TOPOLOGY (that needs ibgpu_upload_topology).  The state stays. */
 int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags);
 
+/* Coarse/fine interface lists of an AMR mesh from its leaf cells, built on
+ * the device: the part of the regrid's list rebuild (AMR::PerformAdaptive,
+ * AMR.cpp:6-209; TagRefineGhost, AMRGhost_refine.cpp:30-98; the pair lists
+ * f_res_ghost, f_pro_ghost and g_pro of AMRLevel.H:320-329) that follows
+ * from which cells are leaves.  With refined(l) the level-l positions whose
+ * sons are leaves or refined:
+ *   restriction pair of level l, layer 0: a refined position whose four sons
+ *     are leaves and with a leaf of level l among its 8 neighbours; layer 1:
+ *     not layer 0, four leaf sons, a leaf of level l two steps away along x
+ *     or y (rows: level, layer, cx, cy, 4 x (fx, fy));
+ *   prolongation pair of level l: a leaf of level l with a refined position
+ *     among its 8 neighbours (rows: level, cx, cy, 4 x (fx, fy));
+ *   interface ghost cells (rows: level, ix, iy): the restriction positions of
+ *     each level and the sons of the prolongation pairs of the level below;
+ * sons in the order (0,0), (0,1), (1,0), (1,1) of (x, y) offsets, rows sorted
+ * by level, then y, then x.  leaves->flags is not read.  The counts are
+ * always set; when a capacity is below its count (a first call with zero
+ * capacities asks for the counts) nothing is written and the call returns
+ * IBGPU_E_ARG.  ctx supplies the stream (no topology needed). */
+typedef struct ibgpu_interface_lists {
+  int64_t nres, npro, nghost;          /* counts, set by the call            */
+  int64_t cap_res, cap_pro, cap_ghost; /* rows the arrays below can hold     */
+  int32_t *res;   /* cap_res x 12   */
+  int32_t *pro;   /* cap_pro x 11   */
+  int32_t *ghost; /* cap_ghost x 3  */
+} ibgpu_interface_lists;
+int ibgpu_build_interfaces(ibgpu_ctx *ctx, int nlevels, const ibgpu_cells *leaves,
+                           ibgpu_interface_lists *out);
+
 /* Number of device cell slots and tiles after the last topology upload. */
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles);
 

@@ -55,7 +55,8 @@ def test_ctypes_layouts_match_c(pkg, tmp_path):
     ib = pkg.ibgpu
     mirrors = {"ibgpu_case": ib.Case, "ibgpu_cells": ib.Cells, "ibgpu_cf_pairs": ib.CfPairs,
                "ibgpu_bc": ib.Bc, "ibgpu_ib": ib.Ib, "ibgpu_diag": ib.Diag,
-               "ibgpu_tag_rule": ib.TagRule, "ibgpu_tag_cells": ib.TagCells}
+               "ibgpu_tag_rule": ib.TagRule, "ibgpu_tag_cells": ib.TagCells,
+               "ibgpu_interface_lists": ib.InterfaceLists}
     # every field of every mirrored struct
     checks = {c: (cls, [f[0] for f in cls._fields_]) for c, cls in mirrors.items()}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ibgpu.h"', "int main(void){"]
