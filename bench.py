@@ -35,8 +35,11 @@ STAGES = 4
 # algorithmic bytes per leaf cell per stage, inviscid: read U^(k-1) (32 B),
 # read U^n (32 B), write U^(k) (32 B)
 BYTES_PER_CELL_STAGE = 96
-REF_SAMPLE_N = 512   # bounded CPU sample per host core: 512 x 512 cells of the same case
-REF_BYTES_PER_WORKER = 1.2e9  # resident size of one reference process at the sample size
+# host memory of the reference's own run of the 2048^2 case (measured: 18.0 GB
+# of shared windows, ~0.25 GB private per rank); smaller grids scale with n^2
+REF_SHARED_BYTES_2048 = 18.0e9
+REF_RANK_BYTES = 0.3e9
+PORT_SAMPLE_N = 512  # the C restatement's sample (one core) when the reference build is absent
 BATCH_CASES = 64     # batched workload: independent cases, 50k..800k leaf cells each
 REGRID_EVERY = 20    # steps between regrids of the airfoil workloads (learned tagging cost)
 NACA_RECORD = os.path.join(ROOT, "tests", "golden", "naca_minmod_s4_n64_l3.npz")
@@ -299,61 +302,74 @@ def reference_binary():
     return p if os.path.exists(p) and os.access(p, os.X_OK) else None
 
 
-def host_workers(per_worker_bytes: float) -> int:
-    """Host cores this process may use, bounded by the available memory."""
+def host_cores() -> int:
+    """Host cores this process may run on."""
     try:
-        cores = len(os.sched_getaffinity(0))
+        return len(os.sched_getaffinity(0))
     except AttributeError:
-        cores = os.cpu_count() or 1
+        return os.cpu_count() or 1
+
+
+def avail_bytes() -> float:
     try:
-        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-        cores = min(cores, max(1, int(0.7 * avail // per_worker_bytes)))
+        return float(os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE"))
     except (ValueError, OSError):
-        pass
-    return max(1, cores)
+        return float("inf")
 
 
-def run_reference_binary(binary: str, env_case: dict, steps: int, warmup: int, workers: int):
-    """`workers` concurrent single-rank processes of a reference oracle binary
-    on the same case; (rate, longest timed loop s, timed cell updates)."""
-    env = dict(os.environ, IB_STEPS=str(steps), IB_TIMED_FROM=str(warmup), **env_case)
+def host_workers(per_worker_bytes: float) -> int:
+    """Concurrent host processes of `per_worker_bytes` each that fit the
+    host cores and the available memory."""
+    return max(1, min(host_cores(), int(0.7 * avail_bytes() // per_worker_bytes)))
+
+
+def run_reference_mpi(binary: str, env_case: dict, steps: int, warmup: int, ranks: int,
+                      timeout: float = 1800.0):
+    """One run of a reference oracle binary in the reference's own
+    shared-memory MPI mode: `ranks` ranks of one node (share_comm of all of
+    them, SHN = ranks; the build's MPI shim forks them and lays the
+    reference's shared windows in one arena), each marching its share of
+    every array between the reference's own barriers.  Returns (rate, timed
+    loop seconds, timed cell updates); the loop time is rank 0's between
+    barriers that span every rank."""
+    env = dict(os.environ, IB_STEPS=str(steps), IB_TIMED_FROM=str(warmup), IB_RANKS=str(ranks),
+               IB_MPI_TIMEOUT=str(int(timeout)), **env_case)
     with tempfile.TemporaryDirectory() as wd:
-        procs = []
-        for k in range(workers):
-            d = os.path.join(wd, str(k))
-            os.makedirs(d)
-            procs.append(subprocess.Popen([binary], cwd=d, env=env, stdout=subprocess.PIPE,
-                                          stderr=subprocess.DEVNULL, text=True))
-        outs = [p.communicate()[0] for p in procs]
-        if any(p.returncode != 0 for p in procs):
-            raise RuntimeError("reference run failed")
-    secs, upd = [], 0
-    for out in outs:
-        for line in out.splitlines():
-            if line.startswith("ORACLE_RESULT"):
-                r = json.loads(line.split(" ", 1)[1])
-                secs.append(r["loop_seconds"])
-                upd += r["cell_updates"]
-    if len(secs) != workers:
-        raise RuntimeError("reference run printed no result")
-    return upd / max(secs), max(secs), upd
+        out = subprocess.run([binary], cwd=wd, env=env, stdout=subprocess.PIPE,
+                             stderr=subprocess.DEVNULL, text=True, timeout=timeout + 120)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference run failed (exit {out.returncode})")
+    for line in out.stdout.splitlines():
+        if line.startswith("ORACLE_RESULT"):
+            r = json.loads(line.split(" ", 1)[1])
+            if r.get("ranks", 1) != ranks:
+                raise RuntimeError("reference run used another rank count")
+            return r["cell_updates"] / r["loop_seconds"], r["loop_seconds"], r["cell_updates"]
+    raise RuntimeError("reference run printed no result")
 
 
-def run_reference(n: int, steps: int, warmup: int = 0, workers: int = 1):
-    """The reference solver's own step (compiled from its sources with the
-    single-rank MPI shim) on the host: `workers` independent single-rank
-    processes run the same n x n case concurrently, one per host core (the
-    reference's unit of host parallelism is one rank per core; the sample
-    cases are independent, so their throughputs add).  Returns
-    (cell_updates_per_s, seconds, cell_updates, kind) with the rate =
-    all processes' timed cell updates / the longest timed loop.  Falls back
-    to the C restatement on one core (kind "port") when the reference build
-    is absent."""
+def reference_grid(n: int, ranks: int) -> int:
+    """The largest n / 2^k grid whose reference run fits the host memory."""
+    while n > 256 and (REF_SHARED_BYTES_2048 * (n / 2048) ** 2 + ranks * REF_RANK_BYTES
+                       > 0.8 * avail_bytes()):
+        n //= 2
+    return n
+
+
+def run_reference(n: int, steps: int, warmup: int = 0, ranks: int = 1):
+    """The reference solver's own step (compiled from its sources) on the
+    n x n vortex case in its shared-memory MPI mode with `ranks` ranks on the
+    host cores.  Returns (cell_updates_per_s, seconds, cell_updates, kind, n)
+    with n the grid run (smaller than asked only when the host memory is
+    short).  Falls back to the C restatement on one core (kind "port") on a
+    bounded grid when the reference build is absent."""
     binary = reference_binary()
     if binary is not None:
-        rate, sec, upd = run_reference_binary(binary, {"IB_NX": str(n), "IB_STAGES": str(STAGES)},
-                                              steps, warmup, workers)
-        return rate, sec, upd, "reference"
+        n = reference_grid(n, ranks)
+        rate, sec, upd = run_reference_mpi(binary, {"IB_NX": str(n), "IB_STAGES": str(STAGES)},
+                                           steps, warmup, ranks)
+        return rate, sec, upd, "reference", n
+    n = min(n, PORT_SAMPLE_N)
     # C restatement of the same step
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
@@ -387,30 +403,36 @@ def run_reference(n: int, steps: int, warmup: int = 0, workers: int = 1):
         rc, dt, _, _ = pyoracle.step(P, lv, ts, dt)
     sec = time.perf_counter() - t0
     upd = n * n * (steps - warmup)
-    return upd / sec, sec, upd, "port"
+    return upd / sec, sec, upd, "port", n
+
+
+def reference_sample(kind: str, ranks: int, n: int, timed: int, warm: int) -> str:
+    if kind == "port":
+        return (f"the C restatement on one core, {timed} timed steps (after {warm}) of the same "
+                f"case on a {n}x{n} grid")
+    return (f"one run of the reference's own step in its shared-memory MPI mode: {ranks} ranks "
+            f"(one per host core, SHN = {ranks}), {timed} timed steps (after {warm} warm-up) of "
+            f"the {n}x{n} case; step loop only, between barriers over every rank")
 
 
 def reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    n = REF_SAMPLE_N
-    workers = host_workers(REF_BYTES_PER_WORKER) if reference_binary() else 1
-    rate, sec, upd, kind = run_reference(n, args.warmup + args.steps, args.warmup, workers)
-    sample = (f"{workers} concurrent single-rank reference processes (one per host core), "
-              f"each {args.steps} timed steps (after {args.warmup} warm-up) of the same case on "
-              f"a {n}x{n} grid ({n * n} leaf cells per step); step loop only, rate = all "
-              f"timed cell updates / the longest loop")
+    ranks = host_cores() if reference_binary() else 1
+    rate, sec, upd, kind, n = run_reference(args.n, args.warmup + args.steps, args.warmup, ranks)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"isentropic vortex {N_DEFAULT}x{N_DEFAULT} periodic, inviscid, "
+        "config": {"workload": f"isentropic vortex {args.n}x{args.n} periodic, inviscid, "
                                "4-stage, VanLeer MUSCL, all-speed Roe, CFL 0.5",
-                   "sample_grid": f"{n}x{n}", "parallelism": "replicas"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": workers, "kind": kind,
-                         "sample": sample},
+                   "grid_run": f"{n}x{n}", "same_config": n == args.n and kind == "reference",
+                   "parallelism": f"{ranks} MPI ranks of one shared-memory node"
+                   if kind == "reference" else "one core"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": ranks, "kind": kind,
+                         "sample": reference_sample(kind, ranks, n, args.steps, args.warmup)},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -631,13 +653,12 @@ def config1_section(ib, wl, stream, max_over_ranks, timed_steps: int = 400, rank
                          "every step of the 1000-step run against the reference's own history")
     binary = os.path.join(ROOT, "oracle", "_ref", "ref_naca_minmod")
     if rank == 0 and os.path.exists(binary):
-        workers = host_workers(0.3e9)
-        rate, sec, upd = run_reference_binary(binary, CONFIG1_ENV, 3 * period, period, workers)
-        out["reference"] = {"value": rate, "unit": UNIT, "cores": workers,
-                            "sample": f"{workers} concurrent single-rank processes of the "
-                                      f"reference's own step on this case, each {2 * period} "
-                                      f"timed steps after {period}; rate = all timed cell "
-                                      f"updates / the longest loop"}
+        ranks = host_cores()
+        rate, sec, upd = run_reference_mpi(binary, CONFIG1_ENV, 5 * period, period, ranks)
+        out["reference"] = {"value": rate, "unit": UNIT, "cores": ranks,
+                            "sample": f"the reference's own step on this case in its "
+                                      f"shared-memory MPI mode, {ranks} ranks (one per host "
+                                      f"core), {4 * period} timed steps after {period}"}
     return out
 
 
@@ -669,7 +690,8 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
     runs the step.  FP64 and mixed runs: leaf-cell updates/s of the device
     step alone and of the whole step including the host's re-immersion, the
     host time per step, and |dCl|, |dCd| of mixed against FP64; the
-    reference's own step (motion included) on the same mesh on one core."""
+    reference's own step (motion included) on the same mesh in its
+    shared-memory MPI mode on the host cores, run after the GPU runs."""
     import numpy as np
     binding = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod_binding")
     if rank != 0 or not os.path.exists(binding):
@@ -679,15 +701,6 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
                        "body and wake, regrid every 20 steps; mesh, motion and re-immersion by "
                        "the reference's own host code",
            "timed_steps": steps - warm}
-    # the reference's own sample runs on one host core meanwhile (its mesh
-    # generation alone takes most of a minute)
-    ref = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod")
-    pool = None
-    if os.path.exists(ref):
-        from concurrent.futures import ThreadPoolExecutor
-        pool = ThreadPoolExecutor(1)
-        ref_job = pool.submit(run_oracle_binary, ref, CONFIG3_ENV,
-                              {"IB_STEPS": "3", "IB_TIMED_FROM": "1"})
     hist = {}
     for name, prec in (("fp64", 0), ("mixed", 2)):
         res, h = run_oracle_binary(binding, CONFIG3_ENV,
@@ -705,13 +718,14 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
     out["mixed_vs_fp64_max_dcd"], out["mixed_vs_fp64_max_dcl"] = float(d[0]), float(d[1])
     out["device_step_note"] = ("device step = the synchronous ibgpu_step wall time (loop time "
                                "minus the host's motion, re-immersion and record upload)")
-    if pool is not None:
-        res, _ = ref_job.result()
-        pool.shutdown()
-        out["reference"] = {"value": res["cell_updates_per_s"], "unit": UNIT, "cores": 1,
-                            "sample": "the reference's own step with its moving-body path, 2 "
-                                      "timed steps after 1, one single-rank process (run while "
-                                      "the GPU runs step)"}
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod")
+    if os.path.exists(ref):
+        ranks = host_cores()
+        rate, _, _ = run_reference_mpi(ref, CONFIG3_ENV, 6, 1, ranks)
+        out["reference"] = {"value": rate, "unit": UNIT, "cores": ranks,
+                            "sample": f"the reference's own step with its moving-body path in "
+                                      f"its shared-memory MPI mode, {ranks} ranks (one per host "
+                                      f"core), 5 timed steps after 1"}
     return out
 
 
@@ -1005,13 +1019,11 @@ def our_arm(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        workers = host_workers(REF_BYTES_PER_WORKER) if reference_binary() else 1
-        rate, sec, upd, kind = run_reference(REF_SAMPLE_N, 3, 1, workers)
-        cpu = {"value": rate, "unit": UNIT, "cores": workers, "kind": kind,
-               "sample": f"{workers} concurrent single-rank reference processes (one per host "
-                         f"core), each 2 timed steps (after 1 warm-up) of the same case on a "
-                         f"{REF_SAMPLE_N}x{REF_SAMPLE_N} grid; {upd} timed leaf-cell updates in "
-                         f"total, step loop only"}
+        ranks = host_cores() if reference_binary() else 1
+        rate, sec, upd, kind, rn = run_reference(n, 4, 1, ranks)
+        cpu = {"value": rate, "unit": UNIT, "cores": ranks, "kind": kind,
+               "sample": reference_sample(kind, ranks, rn, 3, 1) + f"; {upd} timed leaf-cell "
+                         "updates"}
 
     if rank == 0:
         line = {

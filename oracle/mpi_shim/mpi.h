@@ -1,14 +1,16 @@
 /*
- * Single-rank MPI stand-in used only to build the reference solver as a CPU
- * oracle (test infrastructure; never linked into the GPU library).
+ * MPI stand-in used only to build the reference solver as a CPU oracle (test
+ * infrastructure; never linked into the GPU library).
  *
  * The reference is an MPI-3 code (shared-memory windows inside a node,
- * point-to-point between nodes).  With one rank and SHN=1 every
- * communicator has size 1, shared windows are plain heap blocks, collectives
- * are copies and point-to-point messages only ever go to self.  This header
- * declares exactly the subset of MPI the reference calls (see
- * mpiparams.cpp, DataArray.H, AMRmpi.H, Nodedata.H, Mesh.cpp); the semantics
- * are those of the MPI-3.1 standard restricted to a world of one process.
+ * point-to-point between nodes).  The stand-in runs one node: one rank by
+ * default (every communicator has size 1, shared windows are plain heap
+ * blocks, collectives are copies), or IB_RANKS=N forked ranks sharing one
+ * memory arena (mpi_shim.cpp).  Point-to-point messages only ever go to self
+ * (the reference sends them between nodes).  This header declares exactly
+ * the subset of MPI the reference calls (see mpiparams.cpp, DataArray.H,
+ * AMRmpi.H, Nodedata.H, Mesh.cpp); the semantics are those of the MPI-3.1
+ * standard restricted to one shared-memory node.
  */
 #ifndef IB_ORACLE_MPI_SHIM_H
 #define IB_ORACLE_MPI_SHIM_H
@@ -61,6 +63,13 @@ typedef struct MPI_Status {
 #define MPI_UNDEFINED (-32766)
 
 #define MPI_IN_PLACE ((void *)1)
+
+/* ranks of the one node (IB_RANKS, 1 when unset); the build defines the
+ * reference's ranks-per-node constant SHN as this call */
+int ib_shim_ranks(void);
+#ifndef SHN
+#define SHN (ib_shim_ranks())
+#endif
 
 int MPI_Init(int *argc, char ***argv);
 int MPI_Finalize(void);

@@ -21,7 +21,8 @@
 // each step listed by IB_DUMP_EVERY, default every step, or only after the
 // step counts IB_DUMP_AT lists), IB_FORCES=1 (static
 // body: compute wall forces each step, Body::ComptWallForce), IB_FORCE_LOG=<file>
-// (the per-step force history).
+// (the per-step force history), IB_RANKS=N (the reference's shared-memory
+// mode with N ranks on one node; the shim in mpi_shim/ forks them).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -375,6 +376,15 @@ void dump_state(const std::string &path, Mesh &mesh, OracleSolver &solver,
 int main(int argc, char **argv) {
   MPI_Init(&argc, &argv);
   MPI_CreateNode();
+  // IB_RANKS=N runs the reference's own shared-memory mode with N ranks: the
+  // step, dumps (written by rank 0) and force logs; the harness hooks that
+  // write from inside the case file or drive the GPU binding need one rank
+  if (nprocs > 1 && (std::getenv("IB_TAG_DUMP") || std::getenv("IB_TAG_SERVER") ||
+                     std::getenv("IB_BINDING_LISTS") || std::getenv("IB_BINDING_TAGCHECK") ||
+                     env_int("IB_BINDING_STEP", 0))) {
+    if (nrank == 0) std::fprintf(stderr, "tag dumps, tag server and binding runs need one rank\n");
+    MPI_Abort(MPI_COMM_WORLD, 5);
+  }
   InitSpaceParams();
   Domain p_domain(lowpt, highpt, periodic);
   Mesh mesh(p_domain, max_mesh_level);
@@ -557,7 +567,7 @@ int main(int argc, char **argv) {
   // IB_FORCE_LOG=<file>: per step ts, t, dt and the forces/moments of every
   // body (6 doubles each) as raw doubles, the Cl/Cd history of a run
   const char *force_log = std::getenv("IB_FORCE_LOG");
-  FILE *flog = force_log ? std::fopen(force_log, "wb") : nullptr;
+  FILE *flog = (force_log && nrank == 0) ? std::fopen(force_log, "wb") : nullptr;
   std::vector<double> forces;
   auto do_dump = [&](int step) {
     if (!prefix) return;
@@ -566,7 +576,9 @@ int main(int argc, char **argv) {
 #endif
     char buf[64];
     std::snprintf(buf, sizeof buf, "_%06d.bin", step);
-    dump_state(std::string(prefix) + buf, mesh, flowsolver, forces);
+    MPI_Barrier(MPI_COMM_WORLD);  // every rank's share of the arrays written
+    if (nrank == 0) dump_state(std::string(prefix) + buf, mesh, flowsolver, forces);
+    MPI_Barrier(MPI_COMM_WORLD);
   };
   if (dump_now(0, false)) do_dump(0);
 
@@ -577,6 +589,7 @@ int main(int argc, char **argv) {
     long long marching_cells = 0;
     for (int l = 0; l < mesh.MyCurNum(); ++l)
       if (ts % marching_step[l] == marching_left_step[l]) marching_cells += mesh.ShowLevelBox(l).size();
+    MPI_Barrier(MPI_COMM_WORLD);  // the timed step spans every rank's share
     double t0 = MPI_Wtime();
     if (!gpu_step) {  // the GPU step runs both ghost fills itself
       amr.InterfaceExchange();
@@ -593,6 +606,7 @@ int main(int argc, char **argv) {
     flowsolver.TimeMarching(amr);
     ++ts;
     t += dt;
+    MPI_Barrier(MPI_COMM_WORLD);
     double t1 = MPI_Wtime();
     if (s >= timed_from) {
       loop_time += t1 - t0;
@@ -635,11 +649,13 @@ int main(int argc, char **argv) {
     if (prefix && dump_now(ts, s == nsteps - 1)) do_dump(ts);
   }
   if (flog) std::fclose(flog);
-  std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
-              "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g, "
-              "\"move_seconds\": %.9f}\n",
-              nsteps - timed_from, loop_time, cell_updates,
-              loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time);
+  if (nrank == 0)
+    std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
+                "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g, "
+                "\"move_seconds\": %.9f, \"ranks\": %d}\n",
+                nsteps - timed_from, loop_time, cell_updates,
+                loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time, nprocs);
+  std::fflush(stdout);
   MPI_Finalize();
   return 0;
 }

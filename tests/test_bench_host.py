@@ -1,6 +1,6 @@
 """Host-side parts of the benchmark (no GPU): the reference arm's JSON line,
-timed from the reference's own step (oracle/_ref) or, without it, from the
-C restatement of the same step; the clock sampler's reading of nvidia-smi;
+timed from the reference's own step (oracle/_ref, its shared-memory MPI mode)
+or, without it, from the C restatement of the same step; the clock sampler's reading of nvidia-smi;
 and the rule that re-measures a timing slowed by the hardware."""
 import io
 import json
@@ -17,7 +17,7 @@ import bench  # noqa: E402
 
 
 class Args:
-    gpus, steps, warmup = 1, 1, 3
+    gpus, steps, warmup, n = 1, 1, 3, 64
 
 
 @pytest.mark.skipif(bench.reference_binary() is None,
@@ -42,8 +42,8 @@ def test_reference_arm_prints_one_line_of_the_benchmark_format(monkeypatch):
 
 def test_port_baseline_times_the_c_restatement(monkeypatch):
     monkeypatch.setattr(bench, "reference_binary", lambda: None)
-    rate, sec, upd, kind = bench.run_reference(32, 4, 3, 1)
-    assert kind == "port" and upd == 32 * 32 and sec > 0 and rate == upd / sec
+    rate, sec, upd, kind, n = bench.run_reference(32, 4, 3, 1)
+    assert kind == "port" and n == 32 and upd == 32 * 32 and sec > 0 and rate == upd / sec
 
 
 def test_slowed_timing_is_measured_once_more():

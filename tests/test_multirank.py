@@ -50,7 +50,7 @@ def _worker(rank, ws, port, q):
     rc = 0
     if rank != 0:
         class A:
-            gpus, steps, warmup = ws, 1, 3
+            gpus, steps, warmup, n = ws, 1, 3, 64
         with redirect_stdout(out):
             rc = bench.reference_arm(A())
     q.put((rank, got, float(t.item()), rc, out.getvalue()))
