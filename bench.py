@@ -173,6 +173,7 @@ class ClockSampler:
         self._stop = None
         self._proc = None
         self.path = None
+        self.error = None
         self.t0 = self.t1 = None
 
     # ---- NVML
@@ -192,24 +193,37 @@ class ClockSampler:
             t = time.perf_counter()
             try:
                 mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
-                mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
-            except Exception:
+            except Exception as e:  # noqa: BLE001
+                self.error = f"nvmlDeviceGetClockInfo: {e}"
                 break
-            self.rows.append((t, mhz, {n for n, b in bits.items() if mask & b}))
+            try:
+                mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                reasons = {n for n, b in bits.items() if mask & b}
+            except Exception as e:  # noqa: BLE001
+                self.error = f"nvmlDeviceGetCurrentClocksEventReasons: {e}"
+                reasons = {"unknown"}
+            self.rows.append((t, mhz, reasons))
             self._stop.wait(self.interval)
 
     def start(self):
         import threading
         self.rows = []
+        self.error = None
         self._stop = threading.Event()
         try:
             nv, h = self._nvml_handle()
             self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
             self._thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
             self._thread.start()
-        except Exception:
+            # the window opens once the poller has its first sample
+            t = time.perf_counter()
+            while not self.rows and self._thread.is_alive() and time.perf_counter() - t < 0.5:
+                time.sleep(0.0002)
+        except Exception as e:  # noqa: BLE001
+            self.error = f"nvml: {e}"
             self._thread = None
             self._start_smi()
+            time.sleep(0.1)  # nvidia-smi's first sample
         self.t0 = time.perf_counter()
 
     # ---- nvidia-smi fallback
@@ -266,15 +280,27 @@ class ClockSampler:
 
     def summary(self):
         inside = [r for r in self.rows if self.t0 <= r[0] <= self.t1]
+        where = "inside the timed region"
         if not inside:
-            return None
+            # a region shorter than the poll period: the samples that bracket it
+            before = [r for r in self.rows if r[0] < self.t0][-1:]
+            after = [r for r in self.rows if r[0] > self.t1][:1]
+            inside = before + after
+            where = "nearest samples before and after the timed region"
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0,
+                    "window_ms": (self.t1 - self.t0) * 1e3, "error": self.error or "no samples",
+                    "gpu": self.bus_id}
         mx = self.max_mhz or max(r[1] for r in inside)
         loaded = [r[1] for r in inside if r[1] > 0.5 * mx] or [r[1] for r in inside]
         reasons = sorted(set().union(*(r[2] for r in inside)))
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(inside), "window_ms": (self.t1 - self.t0) * 1e3,
-                "source": "nvml" if self._thread is not None else "nvidia-smi",
-                "gpu": self.bus_id}
+        out = {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons,
+               "samples": len(inside), "window_ms": (self.t1 - self.t0) * 1e3,
+               "source": "nvml" if self._thread is not None else "nvidia-smi",
+               "sampled": where, "gpu": self.bus_id}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 # clock-event reasons that make a timing invalid (sw_power_cap is kept and noted)
