@@ -5,9 +5,12 @@
 // (tcgen05.mma, BF16 operands staged in shared memory, FP32 accumulators in
 // Tensor Memory).
 //
-// MLP shapes: X[rows x 112] -> 64 -> 64 -> 3 (padded to 16 output columns).
-// One CTA of 128 threads works on tiles of 128 rows; thread t owns row t of
-// the tile, which is Tensor Memory lane t of every M = 128 accumulator.
+// MLP shapes: X[rows x 112] -> 64 -> 64 -> 3.  Tiles of 128 rows; tile row t
+// is Tensor Memory lane t of every M = 128 accumulator.  The two hidden
+// layers (and in training every backward and weight-gradient product but
+// the 3-row last layer's) are tensor-core MMAs; the 3-row last layer runs
+// on the CUDA cores from bf16-rounded operands (3 FMAs per hidden unit, no
+// MMA round trip).  Inference kernels: one thread per row, 128 threads.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -28,11 +31,9 @@ namespace ind {
 constexpr int kIn = IBGPU_MLP_IN;         // 112 inputs
 constexpr int kHid = IBGPU_MLP_HIDDEN;    // 64
 constexpr int kOut = IBGPU_MLP_CLASSES;   // 3
-constexpr int kOutPad = 16;               // N of the last layer's MMA
 constexpr int kRows = 128;                // rows per tile = M of every MMA
 constexpr int kThreads = 128;
-constexpr int kOnesRow = kIn;             // row of X^T held at 1 (bias gradients)
-constexpr int kCatN = kHid + kOutPad;     // [dz2 | dz3] columns
+constexpr int kOnesRow = kIn;             // feature held at 1 in the training tiles (bias gradients)
 
 // parameter array offsets (floats)
 constexpr int P_W1 = 0;
@@ -44,18 +45,11 @@ constexpr int P_B3 = P_W3 + kOut * kHid;
 constexpr int P_COUNT = P_B3 + kOut;
 static_assert(P_COUNT == IBGPU_MLP_PARAMS, "parameter layout");
 
-// Tensor Memory columns (f32, one per column, lanes = tile rows)
+// Tensor Memory columns of the forward kernels (f32, lanes = tile rows)
 constexpr uint32_t T_D1 = 0;      // layer-1 pre-activation   (64)
 constexpr uint32_t T_D2 = 64;     // layer-2 pre-activation   (64)
-constexpr uint32_t T_D3 = 128;    // logits                   (16)
-constexpr uint32_t T_DH2 = 144;   // dL/dh2                   (64)
-constexpr uint32_t T_DH1 = 208;   // dL/dh1                   (64)
-constexpr uint32_t T_GCAT = 272;  // [h1|h2]^T [dz2|dz3]      (80), accumulated
-constexpr uint32_t T_GB = 352;    // X^T [dz2|dz3] (ones row)  (80), accumulated
-constexpr uint32_t T_G1 = 432;    // X^T dz1                  (64), accumulated
 constexpr uint32_t T_COLS_TRAIN = 512;
 constexpr uint32_t T_COLS_FWD = 256;
-static_assert(T_G1 + kHid <= T_COLS_TRAIN, "tensor memory budget");
 
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at the boost clock
 
@@ -63,15 +57,20 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-  return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);  // .x = lo (low half)
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ float bf16_round(float x) {
+  return __bfloat162float(__float2bfloat16_rn(x));
 }
 
 // GELU, tanh form (Hendrycks & Gimpel): 0.5 z (1 + tanh(sqrt(2/pi)(z + 0.044715 z^3)))
 constexpr float kGeluA = 0.7978845608028654f;
 constexpr float kGeluB = 0.044715f;
-// The forward passes take tanh from the SFU's tanh.approx.f32 (one
-// instruction; its error stays well below the BF16 rounding that every
-// activation goes through next), the gradient the accurate tanhf.
+// tanh comes from the SFU's tanh.approx.f32 (one instruction; its error
+// stays well below the BF16 rounding that every activation and every
+// back-propagated gradient goes through next).  The training kernel takes
+// GELU and its derivative from the same tanh in its forward pass.
 __device__ __forceinline__ float tanh_sfu(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -81,10 +80,12 @@ __device__ __forceinline__ float gelu(float z) {
   const float u = kGeluA * (z + kGeluB * z * z * z);
   return 0.5f * z * (1.0f + tanh_sfu(u));
 }
-__device__ __forceinline__ float gelu_grad(float z) {
+// GELU and its derivative d/dz [0.5 z (1 + tanh u)], u = a (z + b z^3)
+__device__ __forceinline__ void gelu_and_grad(float z, float &g, float &gp) {
   const float u = kGeluA * (z + kGeluB * z * z * z);
-  const float th = tanhf(u);
-  return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * kGeluA * (1.0f + 3.0f * kGeluB * z * z);
+  const float th = tanh_sfu(u);
+  g = 0.5f * z * (1.0f + th);
+  gp = 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * kGeluA * (1.0f + 3.0f * kGeluB * z * z);
 }
 
 __device__ __forceinline__ void st_bf16(uint8_t *base, int off, float v) {
@@ -92,42 +93,54 @@ __device__ __forceinline__ void st_bf16(uint8_t *base, int off, float v) {
 }
 
 // ---------------------------------------------------------------------------
-// shared-memory plan of the training kernel (bytes, 1024-aligned pieces)
+// Training kernel: 256 threads, two per tile row.  Warp w reads Tensor
+// Memory lane quarter w % 4 (tile rows 32 (w % 4) ..) and owns accumulator
+// columns [32 (w / 4), +32) of the 64-wide layers.  Every activation and
+// gradient tile is stored once, row-major in the K-major layout (8-column
+// slabs of 2048 bytes); the weight-gradient products read those same tiles
+// as MN-major operands of their transposes, so nothing is transposed in
+// shared memory.  Shared memory (bytes):
+constexpr int kThreadsTrain = 256;
+constexpr int kSlab = kRows * 16;  // 8 bf16 columns of a 128-row tile
 struct TrainSmem {
-  static constexpr int X = 0;                          // [128 x 112] A of layer 1
-  static constexpr int XT = X + kRows * kIn * 2;       // [128 feat x 128 rows] A of dW1, dB
-  static constexpr int H1 = XT + 128 * kRows * 2;      // [128 x 64] A of layer 2; later dz1^T
-  static constexpr int H2 = H1 + kRows * kHid * 2;     // [128 x 64] A of layer 3
-  static constexpr int HT = H2 + kRows * kHid * 2;     // [(h1|h2) 128 x 128 rows] A of dW2|dW3
-  static constexpr int DZ3 = HT + 128 * kRows * 2;     // [128 x 16] A of dh2
-  static constexpr int DZ2 = DZ3 + kRows * kOutPad * 2;  // [128 x 64] A of dh1
-  static constexpr int BCAT = DZ2 + kRows * kHid * 2;  // [80 x 128 rows] B of dW2|dW3, dB
-  static constexpr int W1 = BCAT + kCatN * kRows * 2;  // [64 x 112] B of layer 1
+  // X of two tiles (the next one is stored while the weight gradients of
+  // the current one still read it): 16 slabs, features 112 = 1 (bias rows
+  // of the weight gradients) and 113..127 = 0
+  static constexpr int X0 = 0;
+  static constexpr int X1 = X0 + 16 * kSlab;
+  static constexpr int H = X1 + 16 * kSlab;    // [h1 | h2], 16 slabs
+  static constexpr int DZ = H + 16 * kSlab;    // [dz1 | dz2 | dz3 (16 columns)], 18 slabs
+  static constexpr int W1 = DZ + 18 * kSlab;   // [64 x 112] B of layer 1
   static constexpr int W2 = W1 + kHid * kIn * 2;       // [64 x 64]  B of layer 2
   static constexpr int W2T = W2 + kHid * kHid * 2;     // [64 x 64]  B of dh1
-  static constexpr int W3 = W2T + kHid * kHid * 2;     // [16 x 64]  B of layer 3
-  static constexpr int W3T = W3 + kOutPad * kHid * 2;  // [64 x 16]  B of dh2
-  static constexpr int BIAS = W3T + kHid * kOutPad * 2;  // b1, b2, b3 (f32)
-  // unused tail: keeps every descriptor's reach inside the allocation even
-  // if a tile's stride fields were read the other way round
-  static constexpr int BYTES = BIAS + 1024 + 16384;
+  static constexpr int BIAS = W2T + kHid * kHid * 2;   // b1, b2, b3 (f32)
+  static constexpr int W3F = BIAS + 1024;              // W3 rounded to bf16, as f32 [3 x 64]
+  static constexpr int XCH = W3F + 1024;               // row exchange between column halves [128 x 4] f32
+  static constexpr int BYTES = XCH + kRows * 16;
 };
 static_assert(TrainSmem::BYTES <= 227 * 1024, "shared memory budget");
+
+// Tensor Memory columns of the training kernel (f32, lanes = tile rows)
+constexpr uint32_t TT_D1 = 0;      // z1, then gelu'(z1)                       (64)
+constexpr uint32_t TT_D2 = 64;     // z2, then dL/dh1                          (64)
+constexpr uint32_t TT_GCAT = 128;  // [h1|h2]^T [dz2|dz3], accumulated         (80)
+constexpr uint32_t TT_G1 = 208;    // [x|1]^T [dz1|dz2|dz3], accumulated      (144)
+static_assert(TT_G1 + 144 <= T_COLS_TRAIN, "tensor memory budget");
 
 struct FwdSmem {
   static constexpr int X = 0;
   static constexpr int H1 = X + kRows * kIn * 2;
-  static constexpr int H2 = H1 + kRows * kHid * 2;
-  static constexpr int W1 = H2 + kRows * kHid * 2;
+  static constexpr int W1 = H1 + kRows * kHid * 2;
   static constexpr int W2 = W1 + kHid * kIn * 2;
-  static constexpr int W3 = W2 + kHid * kHid * 2;
-  static constexpr int BIAS = W3 + kOutPad * kHid * 2;
-  static constexpr int BYTES = BIAS + 1024 + 16384;
+  static constexpr int BIAS = W2 + kHid * kHid * 2;
+  static constexpr int W3F = BIAS + 1024;  // W3 rounded to bf16, as f32 [3 x 64]
+  static constexpr int BYTES = W3F + 1024;
 };
 
-// Weights (rounded to bf16) into their B-operand tiles; biases as f32.
+// Weights (rounded to bf16) into their B-operand tiles; W3 (3 rows, used
+// on the CUDA cores) rounded to bf16 and kept as f32; biases as f32.
 __device__ void load_weights(const float *__restrict__ P, uint8_t *sW1, uint8_t *sW2,
-                             uint8_t *sW2T, uint8_t *sW3, uint8_t *sW3T, float *sB) {
+                             uint8_t *sW2T, float *sB, float *sW3f) {
   using tc::kmajor_off;
   for (int i = threadIdx.x; i < kHid * kIn; i += blockDim.x) {
     const int o = i / kIn, k = i % kIn;
@@ -139,12 +152,7 @@ __device__ void load_weights(const float *__restrict__ P, uint8_t *sW1, uint8_t 
     st_bf16(sW2, kmajor_off(kHid, o, k), w);
     if (sW2T) st_bf16(sW2T, kmajor_off(kHid, k, o), w);
   }
-  for (int i = threadIdx.x; i < kOutPad * kHid; i += blockDim.x) {
-    const int o = i / kHid, j = i % kHid;
-    const float w = (o < kOut) ? P[P_W3 + o * kHid + j] : 0.0f;
-    st_bf16(sW3, kmajor_off(kOutPad, o, j), w);
-    if (sW3T) st_bf16(sW3T, kmajor_off(kHid, j, o), w);
-  }
+  for (int i = threadIdx.x; i < kOut * kHid; i += blockDim.x) sW3f[i] = bf16_round(P[P_W3 + i]);
   for (int i = threadIdx.x; i < 2 * kHid + 4; i += blockDim.x) {
     float b = 0.0f;
     if (i < kHid) b = P[P_B1 + i];
@@ -212,29 +220,76 @@ __device__ __forceinline__ void store_row64(uint8_t *tile, int t, const float (&
   }
 }
 
-// Feature row -> X (row-major A tile) and optionally X^T (column t).
+// Feature row -> X (row-major A tile).
 __device__ __forceinline__ void load_x_row(const uint16_t *__restrict__ feat, int64_t row, bool valid,
-                                           int t, uint8_t *sX, uint8_t *sXT) {
+                                           int t, uint8_t *sX) {
   const uint4 *src = reinterpret_cast<const uint4 *>(feat + row * kIn);
 #pragma unroll 2
   for (int c = 0; c < kIn / 8; ++c) {
     uint4 w = make_uint4(0u, 0u, 0u, 0u);
     if (valid) w = __ldg(src + c);
     *reinterpret_cast<uint4 *>(sX + c * (kRows * 16) + t * 16) = w;
-    if (sXT) {
-      const uint32_t q[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        *reinterpret_cast<uint16_t *>(sXT + tc::kmajor_off(128, 8 * c + e, t)) =
-            (uint16_t)(q[e >> 1] >> (16 * (e & 1)));
-    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Gradient of the class-weighted cross entropy, accumulated over the tiles
 // this CTA processes and added to grad once at the end.
-__global__ void __launch_bounds__(kThreads, 1)
+//
+// Per tile (thread 0 issues every MMA; one commit is outstanding at a time):
+//   L1  D1 = X W1^T  -> h1 = gelu(z1) to smem, gelu'(z1) back into D1
+//   L2  D2 = h1 W2^T -> h2 = gelu(z2); the next tile's X into registers;
+//                       logits h2 W3^T, softmax, dz3 and dh2 = dz3 W3 on
+//                       the CUDA cores (W3 has 3 rows: 3 FMAs per element,
+//                       the two column halves of a row summed through
+//                       shared memory), dz2 = dh2 gelu'(z2)
+//   dh1 = dz2 W2     -> dz1 = dh1 gelu'(z1); the next tile's X to smem
+//   with dh1, unwaited: [dW2 | dW3]^T += [h1 | h2]^T [dz2 | dz3]
+//   with the next tile's L1, unwaited: [dW1 | b]^T += [x | 1]^T [dz1 | dz2 | dz3]
+// The unwaited weight-gradient MMAs overlap the next epilogue; the tile
+// buffers they read are rewritten only after a later commit covers them.
+// Products on the CUDA cores take bf16-rounded operands and accumulate in
+// f32, as the tensor core does.  (Two tiles in flight, alternating steps in
+// the same warps, measured slower: 116 us against 91 us for 262,144 rows.)
+__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t &phase, int *abort_flag) {
+  const bool ok = tc::mbar_wait_bounded(bar, phase, kWaitCycles);
+  if (ok) phase ^= 1u;
+  else atomicExch(abort_flag, 1);
+  tc_sync();
+  return *(volatile int *)abort_flag == 0;
+}
+
+// 32 f32 columns of this thread's lane (two loads, one wait)
+__device__ __forceinline__ void tmem_row32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[2][16];
+  tc::tmem_ld16(taddr, r[0]);
+  tc::tmem_ld16(taddr + 16, r[1]);
+  tc::tmem_wait_ld16(r[0]);
+  tc::tmem_tie16(r[1]);
+#pragma unroll
+  for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e >> 4][e & 15]);
+}
+__device__ __forceinline__ void tmem_store32(uint32_t taddr, const float (&v)[32]) {
+  uint32_t r[2][16];
+#pragma unroll
+  for (int e = 0; e < 32; ++e) r[e >> 4][e & 15] = __float_as_uint(v[e]);
+  tc::tmem_st16(taddr, r[0]);
+  tc::tmem_st16(taddr + 16, r[1]);
+}
+// 32 values into slabs s0..s0+3 of a row-major tile, row t
+__device__ __forceinline__ void store_row32(uint8_t *tile, int t, int s0, const float (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint4 w;
+    w.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    w.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    w.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    w.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4 *>(tile + (s0 + c) * kSlab + t * 16) = w;
+  }
+}
+
+__global__ void __launch_bounds__(kThreadsTrain, 1)
     mlp_grad_kernel(const float *__restrict__ P, const uint16_t *__restrict__ feat,
                     const uint8_t *__restrict__ label, int64_t n, float cw0, float cw1, float cw2,
                     float inv_n, float *__restrict__ grad, float *__restrict__ stats,
@@ -244,204 +299,283 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ uint32_t tbase;
   __shared__ int abort_flag;
   using S = TrainSmem;
-  using tc::kmajor_off;
-  uint8_t *sX = smem + S::X, *sXT = smem + S::XT, *sH1 = smem + S::H1, *sH2 = smem + S::H2,
-          *sHT = smem + S::HT, *sDZ3 = smem + S::DZ3, *sDZ2 = smem + S::DZ2,
-          *sBC = smem + S::BCAT, *sW1 = smem + S::W1, *sW2 = smem + S::W2, *sW2T = smem + S::W2T,
-          *sW3 = smem + S::W3, *sW3T = smem + S::W3T;
+  uint8_t *const sX[2] = {smem + S::X0, smem + S::X1};
+  uint8_t *sH = smem + S::H, *sH2 = sH + 8 * kSlab, *sDZ = smem + S::DZ, *sDZ2 = sDZ + 8 * kSlab,
+          *sDZ3 = sDZ + 16 * kSlab, *sW1 = smem + S::W1, *sW2 = smem + S::W2,
+          *sW2T = smem + S::W2T;
   float *sB = reinterpret_cast<float *>(smem + S::BIAS);
-  uint8_t *sDZ1T = sH1;  // dz1^T [64 x 128 rows] reuses the h1 tile
-  const int t = threadIdx.x;
+  const float *sW3f = reinterpret_cast<const float *>(smem + S::W3F);
+  float4 *sXch = reinterpret_cast<float4 *>(smem + S::XCH);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int t = ((warp & 3) << 5) | (tid & 31);  // tile row = Tensor Memory lane
+  const int hh = warp >> 2;                      // column half of the 64-wide layers
+  const int c0 = 32 * hh;
+  const int pair_bar = 1 + (warp & 3);  // named barrier of warps w and w + 4 (one row each)
 
-  load_weights(P, sW1, sW2, sW2T, sW3, sW3T, sB);
-  // constant parts: X^T row 112 = 1 (bias gradients), rows 113..127 = 0;
-  // [dz2|dz3] rows 67..79 = 0; dz3 columns 3..15 = 0
-  for (int f = kIn; f < 128; ++f)
-    *reinterpret_cast<uint16_t *>(sXT + kmajor_off(128, f, t)) = (f == kOnesRow) ? 0x3F80u : 0u;
-  for (int o = kHid + kOut; o < kCatN; ++o)
-    *reinterpret_cast<uint16_t *>(sBC + kmajor_off(kCatN, o, t)) = 0u;
-  *reinterpret_cast<uint4 *>(sDZ3 + 1 * (kRows * 16) + t * 16) = make_uint4(0u, 0u, 0u, 0u);
-  if (t == 0) {
+  load_weights(P, sW1, sW2, sW2T, sB, reinterpret_cast<float *>(smem + S::W3F));
+  if (tid < kRows) {
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      *reinterpret_cast<uint4 *>(sX[b] + 14 * kSlab + tid * 16) = make_uint4(0x3F80u, 0u, 0u, 0u);
+      *reinterpret_cast<uint4 *>(sX[b] + 15 * kSlab + tid * 16) = zero;
+    }
+    *reinterpret_cast<uint4 *>(sDZ3 + kSlab + tid * 16) = zero;  // dz3 columns 8..15
+  }
+  if (tid == 0) {
     tc::mbar_init(&bar, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if ((t >> 5) == 0) {
+  if (warp == 0) {
     tc::tmem_alloc(&tbase, T_COLS_TRAIN);
     tc::tmem_relinquish();
+  }
+
+  // X rows of a tile: thread tid holds row tid % 128, slab pairs
+  // (tid / 128) + 2k (one aligned 32-byte sector of the row each)
+  uint4 xr[4][2];
+  int ylab = -1, ycur = -1;  // labels of row tid (threads < 128)
+  auto load_tile = [&](int64_t tile) {
+    const int64_t row = tile * kRows + (tid & (kRows - 1));
+    const bool valid = row < n;
+    const uint4 *src = reinterpret_cast<const uint4 *>(feat + (valid ? row : 0) * kIn);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = (tid >> 7) + 2 * k;
+      if (p < kIn / 16) {
+        xr[k][0] = valid ? __ldg(src + 2 * p) : make_uint4(0u, 0u, 0u, 0u);
+        xr[k][1] = valid ? __ldg(src + 2 * p + 1) : make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    if (tid < kRows) ylab = valid ? (int)label[row] : -1;
+  };
+  auto store_tile = [&](uint8_t *dst) {
+    const int r = tid & (kRows - 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = (tid >> 7) + 2 * k;
+      if (p < kIn / 16) {
+        *reinterpret_cast<uint4 *>(dst + (2 * p) * kSlab + r * 16) = xr[k][0];
+        *reinterpret_cast<uint4 *>(dst + (2 * p + 1) * kSlab + r * 16) = xr[k][1];
+      }
+    }
+  };
+
+  const int64_t ntiles = (n + kRows - 1) / kRows;
+  int64_t tile = blockIdx.x;
+  if (tile < ntiles) {
+    load_tile(tile);
+    store_tile(sX[0]);
+    ycur = ylab;
   }
   tc::fence_async_smem();
   tc_sync();
   const uint32_t tm = tbase;
-  const uint32_t lane_off = (uint32_t)((t & ~31) << 16);  // this warp's lane quarter
-  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad),
-                 id80 = tc::idesc_bf16_f32(128, kCatN);
+  const uint32_t lane = tm + (uint32_t)((warp & 3) << 21);  // this warp's lane quarter
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id_gcat = tc::idesc_bf16_f32_mn(128, 80),
+                 id_g1 = tc::idesc_bf16_f32_mn(128, 144);
   uint32_t phase = 0;
-  bool first = true, ok = true;
+  bool ok = true, any = false;
+  int b = 0;
   float loss = 0.0f, correct = 0.0f;
   const float cw[3] = {cw0, cw1, cw2};
 
-  for (int64_t tile = blockIdx.x; ok && tile * kRows < n; tile += gridDim.x) {
-    const int64_t row = tile * kRows + t;
-    const bool valid = row < n;
-    load_x_row(feat, row, valid, t, sX, sXT);
-    const int y = valid ? (int)label[row] : -1;
-    const float wy = (y >= 0 && y < kOut) ? cw[y] * inv_n : 0.0f;
-    tc::fence_async_smem();
-    tc_sync();
-    // ---- layer 1: D1 = X W1^T
-    if (t == 0) mma_chain(tm, T_D1, sX, kRows * 16, sW1, kHid * 16, kIn / 16, id64, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+  if (tile < ntiles && tid == 0) {
+    mma_chain(tm, TT_D1, sX[0], kSlab, sW1, kHid * 16, kIn / 16, id64, false);
+    tc::mma_commit(&bar);
+  }
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int64_t next = tile + gridDim.x;
+    const bool has_next = next < ntiles;
+    // ---- layer 1 done: h1, gelu'(z1)
+    if (!(ok = wait_phase(&bar, phase, &abort_flag))) break;
     {
-      float v[64];
-      tmem_row64(tm + lane_off + T_D1, sB, v);
+      float v[32], gp[32];
+      tmem_row32(lane + TT_D1 + c0, v);
 #pragma unroll
-      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
-      store_row64(sH1, t, v);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) st_bf16(sHT, kmajor_off(128, j, t), v[j]);
+      for (int j = 0; j < 32; ++j) gelu_and_grad(v[j] + sB[c0 + j], v[j], gp[j]);
+      store_row32(sH, t, 4 * hh, v);
+      tmem_store32(lane + TT_D1 + c0, gp);
+      tc::tmem_wait_st();
     }
     tc::fence_async_smem();
     tc_sync();
-    // ---- layer 2: D2 = H1 W2^T
-    if (t == 0) mma_chain(tm, T_D2, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
-    {
-      float v[64];
-      tmem_row64(tm + lane_off + T_D2, sB + kHid, v);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
-      store_row64(sH2, t, v);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) st_bf16(sHT, kmajor_off(128, kHid + j, t), v[j]);
+    if (tid == 0) {
+      mma_chain(tm, TT_D2, sH, kSlab, sW2, kHid * 16, kHid / 16, id64, false);
+      tc::mma_commit(&bar);
     }
-    tc::fence_async_smem();
-    tc_sync();
-    // ---- layer 3: logits = H2 W3^T
-    if (t == 0) mma_chain(tm, T_D3, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    // ---- layer 2 done (and the previous tile's weight gradients): the
+    //      next tile's rows into registers; h2, logits, softmax, dz3, dz2
+    if (!(ok = wait_phase(&bar, phase, &abort_flag))) break;
+    if (has_next) load_tile(next);
     {
-      uint32_t r[16];
-      tc::tmem_ld16(tm + lane_off + T_D3, r);
-      tc::tmem_wait_ld16(r);
-      float z[3];
+      float h[32], gp[32];
+      tmem_row32(lane + TT_D2 + c0, h);
 #pragma unroll
-      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
-      const float m = fmaxf(z[0], fmaxf(z[1], z[2]));
-      float e[3], se = 0.0f;
-#pragma unroll
-      for (int o = 0; o < kOut; ++o) { e[o] = expf(z[o] - m); se += e[o]; }
-      const float inv = 1.0f / se;
-      int am = 0;
-      if (z[1] > z[am]) am = 1;
-      if (z[2] > z[am]) am = 2;
-      float dz[3] = {0.0f, 0.0f, 0.0f};
-      if (wy != 0.0f) {
-        loss += wy * (logf(se) + m - z[y]);
-#pragma unroll
-        for (int o = 0; o < kOut; ++o) dz[o] = wy * (e[o] * inv - (o == y ? 1.0f : 0.0f));
+      for (int j = 0; j < 32; ++j) {
+        gelu_and_grad(h[j] + sB[kHid + c0 + j], h[j], gp[j]);
+        h[j] = bf16_round(h[j]);  // the value the tile holds
       }
-      if (valid && y >= 0 && y < kOut && am == y) correct += 1.0f;
-      uint4 w;
-      w.x = pack_bf16(dz[0], dz[1]);
-      w.y = pack_bf16(dz[2], 0.0f);
-      w.z = 0u;
-      w.w = 0u;
-      *reinterpret_cast<uint4 *>(sDZ3 + t * 16) = w;
+      store_row32(sH2, t, 4 * hh, h);
+      // logits: this half's partial sums, the other half's through smem
+      float zp[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-      for (int o = 0; o < kOut; ++o) st_bf16(sBC, kmajor_off(kCatN, kHid + o, t), dz[o]);
+      for (int j = 0; j < 32; ++j)
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) zp[o] = fmaf(h[j], sW3f[o * kHid + c0 + j], zp[o]);
+      if (hh == 1) sXch[t] = make_float4(zp[0], zp[1], zp[2], 0.0f);
+      asm volatile("bar.sync %0, 64;" ::"r"(pair_bar) : "memory");
+      if (hh == 0) {
+        const float4 q = sXch[t];
+        const int y = ycur;
+        const float wy = (y >= 0 && y < kOut) ? cw[y] * inv_n : 0.0f;
+        const float z[3] = {zp[0] + q.x + sB[2 * kHid + 0], zp[1] + q.y + sB[2 * kHid + 1],
+                            zp[2] + q.z + sB[2 * kHid + 2]};
+        const float m = fmaxf(z[0], fmaxf(z[1], z[2]));
+        float e[3], se = 0.0f;
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) { e[o] = expf(z[o] - m); se += e[o]; }
+        const float inv = 1.0f / se;
+        int am = 0;
+        if (z[1] > z[am]) am = 1;
+        if (z[2] > z[am]) am = 2;
+        float dz[3] = {0.0f, 0.0f, 0.0f};
+        if (wy != 0.0f) {
+          loss += wy * (logf(se) + m - z[y]);
+#pragma unroll
+          for (int o = 0; o < kOut; ++o) dz[o] = bf16_round(wy * (e[o] * inv - (o == y ? 1.0f : 0.0f)));
+        }
+        if (y >= 0 && y < kOut && am == y) correct += 1.0f;
+        *reinterpret_cast<uint4 *>(sDZ3 + t * 16) =
+            make_uint4(pack_bf16(dz[0], dz[1]), pack_bf16(dz[2], 0.0f), 0u, 0u);
+        sXch[t] = make_float4(dz[0], dz[1], dz[2], 0.0f);
+      }
+      asm volatile("bar.sync %0, 64;" ::"r"(pair_bar) : "memory");
+      // dz2 = (dz3 W3) gelu'(z2) over this half's columns
+      const float4 d3 = sXch[t];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const float dh = fmaf(d3.x, sW3f[c0 + j],
+                              fmaf(d3.y, sW3f[kHid + c0 + j], d3.z * sW3f[2 * kHid + c0 + j]));
+        gp[j] *= dh;
+      }
+      store_row32(sDZ2, t, 4 * hh, gp);
     }
     tc::fence_async_smem();
     tc_sync();
-    // ---- dh2 = dz3 W3 (B = W3^T tile)
-    if (t == 0) mma_chain(tm, T_DH2, sDZ3, kRows * 16, sW3T, kHid * 16, 1, id64, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
+    if (tid == 0) {
+      mma_chain(tm, TT_D2, sDZ2, kSlab, sW2T, kHid * 16, kHid / 16, id64, false);
+      tc::mma_commit(&bar);
+      // [dW2 | dW3]^T += [h1 | h2]^T [dz2 | dz3] (K = the tile's rows)
+      for (int s = 0; s < kRows / 16; ++s)
+        tc::mma_bf16(tm + TT_GCAT, tc::smem_desc(sH + 256 * s, 128, kSlab),
+                     tc::smem_desc(sDZ2 + 256 * s, 128, kSlab), id_gcat, (any || s > 0) ? 1u : 0u);
+    }
+    // ---- dz1 = dh1 gelu'(z1); the next tile's rows into the other buffer
+    if (!(ok = wait_phase(&bar, phase, &abort_flag))) break;
     {
-      float dh[64], z[64];
-      tmem_row64(tm + lane_off + T_DH2, nullptr, dh);
-      tmem_row64(tm + lane_off + T_D2, sB + kHid, z);
+      float dh[32], gp[32];
+      tmem_row32(lane + TT_D2 + c0, dh);
+      tmem_row32(lane + TT_D1 + c0, gp);
 #pragma unroll
-      for (int j = 0; j < kHid; ++j) dh[j] *= gelu_grad(z[j]);
-      store_row64(sDZ2, t, dh);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) st_bf16(sBC, kmajor_off(kCatN, j, t), dh[j]);
+      for (int j = 0; j < 32; ++j) dh[j] *= gp[j];
+      store_row32(sDZ, t, 4 * hh, dh);
     }
+    if (has_next) store_tile(sX[b ^ 1]);
+    ycur = ylab;
     tc::fence_async_smem();
     tc_sync();
-    // ---- dh1 = dz2 W2; [dW2|dW3]^T += [h1|h2]^T [dz2|dz3]; bias rows
-    if (t == 0) {
-      mma_chain(tm, T_DH1, sDZ2, kRows * 16, sW2T, kHid * 16, kHid / 16, id64, false);
-      mma_chain(tm, T_GCAT, sHT, 128 * 16, sBC, kCatN * 16, kRows / 16, id80, !first);
-      mma_chain(tm, T_GB, sXT, 128 * 16, sBC, kCatN * 16, kRows / 16, id80, !first);
+    if (tid == 0) {
+      if (has_next) {
+        mma_chain(tm, TT_D1, sX[b ^ 1], kSlab, sW1, kHid * 16, kIn / 16, id64, false);
+        tc::mma_commit(&bar);
+      }
+      // [dW1 | db1 db2 db3]^T += [x | 1]^T [dz1 | dz2 | dz3]
+      for (int s = 0; s < kRows / 16; ++s)
+        tc::mma_bf16(tm + TT_G1, tc::smem_desc(sX[b] + 256 * s, 128, kSlab),
+                     tc::smem_desc(sDZ + 256 * s, 128, kSlab), id_g1, (any || s > 0) ? 1u : 0u);
+      if (!has_next) tc::mma_commit(&bar);
     }
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
-    {
-      float dh[64], z[64];
-      tmem_row64(tm + lane_off + T_DH1, nullptr, dh);
-      tmem_row64(tm + lane_off + T_D1, sB, z);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) st_bf16(sDZ1T, kmajor_off(kHid, j, t), dh[j] * gelu_grad(z[j]));
-    }
-    tc::fence_async_smem();
-    tc_sync();
-    // ---- dW1^T += X^T dz1 (row 112 of X^T gives db1)
-    if (t == 0) mma_chain(tm, T_G1, sXT, 128 * 16, sDZ1T, kHid * 16, kRows / 16, id64, !first);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
-    first = false;
+    any = true;
+    b ^= 1;
   }
+  if (ok && any) ok = wait_phase(&bar, phase, &abort_flag);
 
-  if (ok && !first) {
-    // lane t of the accumulators is input feature t (X^T rows) or hidden
-    // unit t (h1 for t < 64, h2 for t >= 64)
-    float g[64];
-    tmem_row64(tm + lane_off + T_G1, nullptr, g);
-    if (t < kIn) {
-      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_W1 + o * kIn + t], g[o]);
-    } else if (t == kOnesRow) {
-      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_B1 + o], g[o]);
-    }
-    float c[80];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      uint32_t r[16];
-      tc::tmem_ld16(tm + lane_off + T_GCAT + 16 * q, r);
-      tc::tmem_wait_ld16(r);
-#pragma unroll
-      for (int e = 0; e < 16; ++e) c[16 * q + e] = __uint_as_float(r[e]);
-    }
+  if (ok && any) {
+    // lanes of [h1|h2]^T [dz2|dz3]: hidden unit t of h1 (t < 64) or h2
     if (t < kHid) {
-      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_W2 + o * kHid + t], c[o]);
-    } else {
-      for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_W3 + o * kHid + (t - kHid)], c[kHid + o]);
-    }
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
+      float c[32];
+      tmem_row32(lane + TT_GCAT + c0, c);
+      for (int o = 0; o < 32; ++o) atomicAdd(&grad[P_W2 + (c0 + o) * kHid + t], c[o]);
+    } else if (hh == 0) {
       uint32_t r[16];
-      tc::tmem_ld16(tm + lane_off + T_GB + 16 * q, r);
+      tc::tmem_ld16(lane + TT_GCAT + kHid, r);
       tc::tmem_wait_ld16(r);
-#pragma unroll
-      for (int e = 0; e < 16; ++e) c[16 * q + e] = __uint_as_float(r[e]);
+      for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_W3 + o * kHid + (t - kHid)], __uint_as_float(r[o]));
     }
-    if (t == kOnesRow) {
-      for (int o = 0; o < kHid; ++o) atomicAdd(&grad[P_B2 + o], c[o]);
-      for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_B3 + o], c[kHid + o]);
+    // lanes of [x|1]^T [dz1|dz2|dz3]: input feature t, or the ones row
+    {
+      float c[32];
+      tmem_row32(lane + TT_G1 + c0, c);
+      if (t < kIn) {
+        for (int o = 0; o < 32; ++o) atomicAdd(&grad[P_W1 + (c0 + o) * kIn + t], c[o]);
+      } else if (t == kOnesRow) {
+        for (int o = 0; o < 32; ++o) atomicAdd(&grad[P_B1 + c0 + o], c[o]);
+      }
+    }
+    if ((warp & 3) == (kOnesRow >> 5)) {
+      // the ones row's dz2 and dz3 columns: db2 and db3
+      float c[32];
+      tmem_row32(lane + TT_G1 + kHid + c0, c);
+      if (t == kOnesRow)
+        for (int o = 0; o < 32; ++o) atomicAdd(&grad[P_B2 + c0 + o], c[o]);
+      if (hh == 0) {
+        uint32_t r[16];
+        tc::tmem_ld16(lane + TT_G1 + 2 * kHid, r);
+        tc::tmem_wait_ld16(r);
+        if (t == kOnesRow)
+          for (int o = 0; o < kOut; ++o) atomicAdd(&grad[P_B3 + o], __uint_as_float(r[o]));
+      }
     }
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    loss += __shfl_xor_sync(0xffffffffu, loss, off);
-    correct += __shfl_xor_sync(0xffffffffu, correct, off);
-  }
-  if ((t & 31) == 0) {
-    atomicAdd(&stats[0], loss);
-    atomicAdd(&stats[1], correct);
+  if (hh == 0) {
+    for (int off = 16; off > 0; off >>= 1) {
+      loss += __shfl_xor_sync(0xffffffffu, loss, off);
+      correct += __shfl_xor_sync(0xffffffffu, correct, off);
+    }
+    if ((tid & 31) == 0) {
+      atomicAdd(&stats[0], loss);
+      atomicAdd(&stats[1], correct);
+    }
   }
   if (!ok) {
-    if (t == 0) atomicExch(err, 1);
+    if (tid == 0) {
+      atomicExch(err, 1);
+      tc::mma_commit(&bar);
+    }
     // let the MMAs already issued finish (bounded) before freeing their memory
     tc::mbar_wait_bounded(&bar, phase, kWaitCycles);
   }
   tc_sync();
-  if ((t >> 5) == 0) tc::tmem_dealloc(tm, T_COLS_TRAIN);
+  if (warp == 0) tc::tmem_dealloc(tm, T_COLS_TRAIN);
+}
+
+// Layer 2's activations and the logits of this thread's row (one thread per
+// row): h2 = gelu(z2 + b2) rounded to bf16, z3 = h2 W3^T + b3 accumulated
+// in f32 on the CUDA cores (W3 has 3 rows: no third MMA round trip).
+__device__ __forceinline__ void logits_row(uint32_t taddr_d2, const float *sB, const float *sW3f,
+                                           float (&z)[3]) {
+  float h[64];
+  tmem_row64(taddr_d2, sB + kHid, h);
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) z[o] = sB[2 * kHid + o];
+#pragma unroll
+  for (int j = 0; j < kHid; ++j) {
+    const float g = bf16_round(gelu(h[j]));
+#pragma unroll
+    for (int o = 0; o < kOut; ++o) z[o] = fmaf(g, sW3f[o * kHid + j], z[o]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -454,11 +588,11 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ uint32_t tbase;
   __shared__ int abort_flag;
   using S = FwdSmem;
-  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sH2 = smem + S::H2, *sW1 = smem + S::W1,
-          *sW2 = smem + S::W2, *sW3 = smem + S::W3;
+  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sW1 = smem + S::W1, *sW2 = smem + S::W2;
   float *sB = reinterpret_cast<float *>(smem + S::BIAS);
+  float *sW3f = reinterpret_cast<float *>(smem + S::W3F);
   const int t = threadIdx.x;
-  load_weights(P, sW1, sW2, nullptr, sW3, nullptr, sB);
+  load_weights(P, sW1, sW2, nullptr, sB, sW3f);
   if (t == 0) {
     tc::mbar_init(&bar, 1);
     abort_flag = 0;
@@ -472,13 +606,13 @@ __global__ void __launch_bounds__(kThreads)
   tc_sync();
   const uint32_t tm = tbase;
   const uint32_t lane_off = (uint32_t)((t & ~31) << 16);
-  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad);
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid);
   uint32_t phase = 0;
   bool ok = true;
   for (int64_t tile = blockIdx.x; ok && tile * kRows < n; tile += gridDim.x) {
     const int64_t row = tile * kRows + t;
     const bool valid = row < n;
-    load_x_row(feat, row, valid, t, sX, nullptr);
+    load_x_row(feat, row, valid, t, sX);
     tc::fence_async_smem();
     tc_sync();
     if (t == 0) mma_chain(tm, T_D1, sX, kRows * 16, sW1, kHid * 16, kIn / 16, id64, false);
@@ -495,23 +629,8 @@ __global__ void __launch_bounds__(kThreads)
     if (t == 0) mma_chain(tm, T_D2, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
     if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
     {
-      float v[64];
-      tmem_row64(tm + lane_off + T_D2, sB + kHid, v);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) v[j] = gelu(v[j]);
-      store_row64(sH2, t, v);
-    }
-    tc::fence_async_smem();
-    tc_sync();
-    if (t == 0) mma_chain(tm, T_D3, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
-    {
-      uint32_t r[16];
-      tc::tmem_ld16(tm + lane_off + T_D3, r);
-      tc::tmem_wait_ld16(r);
       float z[3];
-#pragma unroll
-      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
+      logits_row(tm + lane_off + T_D2, sB, sW3f, z);
       int am = 0;
       if (z[1] > z[am]) am = 1;
       if (z[2] > z[am]) am = 2;
@@ -524,8 +643,8 @@ __global__ void __launch_bounds__(kThreads)
         }
       }
     }
-    // the next tile's layer-1 MMA overwrites D1..D3 only after every
-    // thread's loads above (tc_sync at the top of the loop)
+    // the next tile's layer-1 MMA overwrites D1 only after every thread's
+    // loads above (tc_sync at the top of the loop)
   }
   if (!ok) {
     if (t == 0) atomicExch(err, 1);
@@ -656,17 +775,19 @@ __global__ void features_kernel(FeatConst F, int64_t n, const int64_t *__restric
 // ---------------------------------------------------------------------------
 // Deployment on the mesh: every normal cell of the context, features
 // gathered straight from the state into the A tile (no feature matrix in
-// HBM), the three layers, the argmax mapped to tag bits.  Shared memory:
-// X (reused for h2), h1, weights; Tensor Memory: 128 columns (D1 0..63,
-// D2 64..127, logits reuse D1) so several CTAs share an SM.
+// HBM; each thread assembles its row's 112 values in registers and stores
+// them as 14 16-byte words), the two hidden layers on the tensor cores, the
+// logits and their argmax on the CUDA cores, mapped to tag bits.  Shared
+// memory: X, h1, weights; Tensor Memory: 128 columns (D1 0..63, D2
+// 64..127) so several CTAs share an SM.
 struct MeshSmem {
-  static constexpr int X = 0;  // also h2
+  static constexpr int X = 0;
   static constexpr int H1 = X + kRows * kIn * 2;
   static constexpr int W1 = H1 + kRows * kHid * 2;
   static constexpr int W2 = W1 + kHid * kIn * 2;
-  static constexpr int W3 = W2 + kHid * kHid * 2;
-  static constexpr int BIAS = W3 + kOutPad * kHid * 2;
-  static constexpr int BYTES = BIAS + 1024;
+  static constexpr int BIAS = W2 + kHid * kHid * 2;
+  static constexpr int W3F = BIAS + 1024;  // W3 rounded to bf16, as f32 [3 x 64]
+  static constexpr int BYTES = W3F + 1024;
 };
 constexpr uint32_t T_COLS_MESH = 128;
 
@@ -723,12 +844,11 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ float4 sn[kSH * kSW];
   __shared__ uint8_t sp[kSH * kSW];
   using S = MeshSmem;
-  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sW1 = smem + S::W1, *sW2 = smem + S::W2,
-          *sW3 = smem + S::W3;
-  uint8_t *sH2 = sX;
+  uint8_t *sX = smem + S::X, *sH1 = smem + S::H1, *sW1 = smem + S::W1, *sW2 = smem + S::W2;
   float *sB = reinterpret_cast<float *>(smem + S::BIAS);
+  float *sW3f = reinterpret_cast<float *>(smem + S::W3F);
   const int t = threadIdx.x;
-  load_weights(P, sW1, sW2, nullptr, sW3, nullptr, sB);
+  load_weights(P, sW1, sW2, nullptr, sB, sW3f);
   if (t == 0) {
     tc::mbar_init(&bar, 1);
     abort_flag = 0;
@@ -742,7 +862,7 @@ __global__ void __launch_bounds__(kThreads)
   tc_sync();
   const uint32_t tm = tbase;
   const uint32_t lane_off = (uint32_t)((t & ~31) << 16);
-  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid), id16 = tc::idesc_bf16_f32(128, kOutPad);
+  const uint32_t id64 = tc::idesc_bf16_f32(128, kHid);
   uint32_t phase = 0;
   bool ok = true;
   const int64_t nitems = m.nslots / kRows;  // half tiles
@@ -775,40 +895,50 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     {
-      // feature row of this thread's cell (zeros for other slots)
-      auto put = [&](int k, float val) {
-        *reinterpret_cast<uint16_t *>(sX + tc::kmajor_off(kRows, t, k)) = bf16_bits(val);
-      };
+      // feature row of this thread's cell (zeros for other slots), built in
+      // registers and stored as 14 16-byte words of the A tile
+      float fv[kIn];
+#pragma unroll
+      for (int k = 0; k < kIn; ++k) fv[k] = 0.0f;
       if (normal) {
         const int tile = (int)(slot >> 8), lx = (int)(slot & 15), ly = (int)((slot >> 4) & 15);
         const int rc = ((ly - 8 * half) + 2) * kSW + (lx + 2);  // centre in the staged region
         const float4 c = sn[rc];
+#pragma unroll
         for (int dy = -2; dy <= 2; ++dy) {
+#pragma unroll
           for (int dx = -2; dx <= 2; ++dx) {
             const int r = rc + dy * kSW + dx;
             const float4 q = sp[r] ? sn[r] : c;
             const int k = (dy + 2) * 5 + (dx + 2);
-            put(k, q.x);
-            put(25 + k, q.y);
-            put(50 + k, q.z);
-            put(75 + k, q.w);
+            fv[k] = q.x;
+            fv[25 + k] = q.y;
+            fv[50 + k] = q.z;
+            fv[75 + k] = q.w;
           }
         }
         const int l = m.tile_level[tile];
         const int2 org = m.tile_org[tile];
         const double xc = (org.x + lx + 0.5) * F.dx[l], yc = (org.y + ly + 0.5) * F.dy[l];
         const double sd = m.signdis ? m.signdis[slot] : 1e30;
-        put(100, (float)(fmin(fmax(sd / F.dx[l], -8.0), 8.0) * 0.125));
-        put(101, (float)(fmin(fmax(sd * F.inv_chord, -4.0), 4.0) * 0.25));
+        fv[100] = (float)(fmin(fmax(sd / F.dx[l], -8.0), 8.0) * 0.125);
+        fv[101] = (float)(fmin(fmax(sd * F.inv_chord, -4.0), 4.0) * 0.25);
         const double ry = (yc - F.yc) * F.inv_chord * 0.125;
-        put(102, (float)((xc - F.left) * F.inv_chord * 0.125));
-        put(103, (float)ry);
-        put(104, (float)fabs(ry));
+        fv[102] = (float)((xc - F.left) * F.inv_chord * 0.125);
+        fv[103] = (float)ry;
+        fv[104] = (float)fabs(ry);
         const int lc = l < 6 ? l : 6;
-        for (int e = 0; e < 7; ++e) put(105 + e, e == lc ? 1.0f : 0.0f);
-      } else {
-        for (int c = 0; c < kIn / 8; ++c)
-          *reinterpret_cast<uint4 *>(sX + c * (kRows * 16) + t * 16) = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int e = 0; e < 7; ++e) fv[105 + e] = e == lc ? 1.0f : 0.0f;
+      }
+#pragma unroll
+      for (int c = 0; c < kIn / 8; ++c) {
+        uint4 w;
+        w.x = pack_bf16(fv[8 * c + 0], fv[8 * c + 1]);
+        w.y = pack_bf16(fv[8 * c + 2], fv[8 * c + 3]);
+        w.z = pack_bf16(fv[8 * c + 4], fv[8 * c + 5]);
+        w.w = pack_bf16(fv[8 * c + 6], fv[8 * c + 7]);
+        *reinterpret_cast<uint4 *>(sX + c * (kRows * 16) + t * 16) = w;
       }
     }
     tc::fence_async_smem();
@@ -827,23 +957,8 @@ __global__ void __launch_bounds__(kThreads)
     if (t == 0) mma_chain(tm, 64, sH1, kRows * 16, sW2, kHid * 16, kHid / 16, id64, false);
     if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
     {
-      float h[64];
-      tmem_row64(tm + lane_off + 64, sB + kHid, h);
-#pragma unroll
-      for (int j = 0; j < kHid; ++j) h[j] = gelu(h[j]);
-      store_row64(sH2, t, h);  // X is free: the layer-1 MMA has completed
-    }
-    tc::fence_async_smem();
-    tc_sync();
-    if (t == 0) mma_chain(tm, 0, sH2, kRows * 16, sW3, kOutPad * 16, kHid / 16, id16, false);
-    if (!(ok = commit_and_wait(&bar, phase, &abort_flag))) break;
-    {
-      uint32_t r[16];
-      tc::tmem_ld16(tm + lane_off + 0, r);
-      tc::tmem_wait_ld16(r);
       float z[3];
-#pragma unroll
-      for (int o = 0; o < kOut; ++o) z[o] = __uint_as_float(r[o]) + sB[2 * kHid + o];
+      logits_row(tm + lane_off + 64, sB, sW3f, z);
       int am = 0;
       if (z[1] > z[am]) am = 1;
       if (z[2] > z[am]) am = 2;
@@ -851,7 +966,8 @@ __global__ void __launch_bounds__(kThreads)
                                          F.coarsen_levels)
                             : (uint8_t)0;
     }
-    tc_sync();  // every lane read before the next item's MMAs overwrite them
+    // the next item's MMAs overwrite D1 and D2 only after the tc_sync that
+    // follows its staging (every lane read above by then)
   }
   if (!ok) {
     if (t == 0) atomicExch(err, 1);
@@ -1041,7 +1157,7 @@ int launch_grad(const CtxView &V, const float *d_params, int64_t n, const uint16
                 float *d_stats) {
   const int64_t tiles = (n + kRows - 1) / kRows;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)V.nsm);
-  mlp_grad_kernel<<<grid, kThreads, TrainSmem::BYTES, V.stream>>>(
+  mlp_grad_kernel<<<grid, kThreadsTrain, TrainSmem::BYTES, V.stream>>>(
       d_params, d_feat, d_label, n, class_weight[0], class_weight[1], class_weight[2],
       (float)(1.0 / (double)n), d_grad, d_stats, V.aux_err);
   CKI(cudaGetLastError());

@@ -42,6 +42,17 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
+// The same with A and B both MN-major (bits 15 and 16): an operand tile
+// whose 16-byte runs go along M (or N) instead of K.  In the no-swizzle
+// MN-major layout a core matrix is 8 K-rows of 16 bytes (8 consecutive M/N
+// elements each) at a 16-byte stride; the descriptor's leading-dimension
+// offset is again the K-direction step between core matrices and its
+// stride-dimension offset the M/N-direction step.  A K-major [rows x cols]
+// tile in the layout above therefore reads, unchanged, as the MN-major
+// operand of its transpose (cols along M/N, rows along K).
+__host__ __device__ constexpr uint32_t idesc_bf16_f32_mn(int M, int N) {
+  return idesc_bf16_f32(M, N) | (1u << 15) | (1u << 16);
+}
 
 // Tensor Memory allocation: executed by one whole warp; the allocated base
 // address is written to *dst (shared memory).
@@ -141,6 +152,21 @@ __device__ __forceinline__ void tmem_wait_ld16(uint32_t (&r)[16]) {
                  "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
                :
                : "memory");
+}
+
+// 16 f32 columns into this thread's Tensor Memory lane (32x32b shape, the
+// same lane rule as tmem_ld16); complete after tmem_wait_st.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // No instruction: ties 16 registers loaded by tcgen05.ld before an earlier
