@@ -710,14 +710,15 @@ def run_oracle_binary(binary: str, env_case: dict, extra: dict, timeout: float =
 
 def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
     """The moving-body workload at its stated size, stepped by the
-    reference's own main loop through the C++ binding (GpuNS_Solver): every
-    step the host moves and re-immerses the body with the reference's code
-    and hands the device new flags and immersed-boundary records, the device
-    runs the step.  FP64 and mixed runs: leaf-cell updates/s of the device
-    step alone and of the whole step including the host's re-immersion, the
-    host time per step, and |dCl|, |dCd| of mixed against FP64; the
-    reference's own step (motion included) on the same mesh in its
-    shared-memory MPI mode on the host cores, run after the GPU runs."""
+    reference's own main loop through the C++ binding (GpuNS_Solver) in the
+    reference's shared-memory MPI mode on the host cores: every step all
+    ranks move and re-immerse the body with the reference's code over their
+    shares of the mesh, rank 0 hands the device the new flags and
+    immersed-boundary records and the device runs the step.  FP64 and mixed
+    runs: leaf-cell updates/s of the device step alone and of the whole step
+    including the host's re-immersion, the host time per step, and |dCl|,
+    |dCd| of mixed against FP64; the reference's own step (motion included)
+    on the same mesh and ranks, run after the GPU runs."""
     import numpy as np
     binding = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod_binding")
     if rank != 0 or not os.path.exists(binding):
@@ -728,22 +729,27 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
                        "the reference's own host code",
            "timed_steps": steps - warm}
     hist = {}
+    ranks = host_cores()
     for name, prec in (("fp64", 0), ("mixed", 2)):
         res, h = run_oracle_binary(binding, CONFIG3_ENV,
                                    {"IB_STEPS": str(steps), "IB_TIMED_FROM": str(warm),
-                                    "IB_BINDING_STEP": "1", "IB_BINDING_PRECISION": str(prec)})
+                                    "IB_BINDING_STEP": "1", "IB_BINDING_PRECISION": str(prec),
+                                    "IB_RANKS": str(ranks), "IB_MPI_TIMEOUT": "900"})
         hist[name] = h
         dev_s = res["loop_seconds"] - res["move_seconds"]
         out[name] = {"value": res["cell_updates"] / dev_s, "unit": UNIT,
                      "device_ms_per_step": dev_s * 1e3 / (steps - warm),
                      "with_host_reimmersion": res["cell_updates"] / res["loop_seconds"],
                      "host_reimmersion_ms_per_step": res["move_seconds"] * 1e3 / (steps - warm),
+                     "host_ranks": res.get("ranks", 1),
                      "cell_updates_per_step": res["cell_updates"] / (steps - warm)}
     f = {k: v[:, 3:].reshape(len(v), -1, 6)[:, :, :2].sum(axis=1) / F_REF for k, v in hist.items()}
     d = np.abs(f["mixed"] - f["fp64"]).max(axis=0)
     out["mixed_vs_fp64_max_dcd"], out["mixed_vs_fp64_max_dcl"] = float(d[0]), float(d[1])
     out["device_step_note"] = ("device step = the synchronous ibgpu_step wall time (loop time "
-                               "minus the host's motion, re-immersion and record upload)")
+                               "minus the host's motion, re-immersion and record upload); the "
+                               f"host part runs on {ranks} MPI ranks of the reference, rank 0 "
+                               "driving the device")
     ref = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod")
     if os.path.exists(ref):
         ranks = host_cores()

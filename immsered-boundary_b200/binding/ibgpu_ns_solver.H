@@ -17,6 +17,13 @@
 // (NS_Solver.H:657-702) on the device.  Upload() runs after InitFlow and
 // after every AMR::PerformAdaptive; Download() fills m_data before output,
 // host-side force evaluation or a regrid reads it.
+//
+// In the reference's shared-memory MPI mode (one node of several ranks, every
+// mesh and body array in a shared window) rank 0 of the node's share_comm
+// drives the device; every rank runs the reference's own host code (mesh
+// generation, regrids, the moving bodies' re-immersion) over its share of
+// the shared arrays, and the device rank's results (status, dt, forces) are
+// broadcast to the node.  One node: the device context holds the whole mesh.
 #pragma once
 
 #include <climits>
@@ -47,6 +54,15 @@ struct IbgpuLists {
   std::vector<int32_t> ib_cell, patch;        // 18 / 17 per row (ibgpu_ib)
   std::vector<double> ib_cellf, patchf, body_center;  // 16 / 19 / 3 per row
 };
+
+// The rank that drives the device: rank 0 of the node (share_comm,
+// mpiparams.cpp:68-105).
+inline bool ibgpu_device_rank() { return srank == 0; }
+// An ibgpu status of the device rank, known to every rank of the node.
+inline int ibgpu_share_status(int rc) {
+  MPI_Bcast(&rc, 1, MPI_INT, 0, share_comm);
+  return rc;
+}
 
 struct IbgpuAdapter {
   // Case constants (gas constants, stage coefficients, levels, schedules,
@@ -356,6 +372,8 @@ struct IbgpuAdapter {
   // (Body::FindPatchHangingNode, which the reference's next ComptWallForce
   // would run first).  The caller then hands the device the new flags and
   // records (GpuNS_Solver::UploadImmersion).
+  // Every rank of the node calls it (the re-immersion is the reference's
+  // own collective code); ctx is the device rank's context.
   static int MoveBodies(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody, double &dt00) {
     const int nlev = amesh.MyCurNum();
     const int last = nlev - 1;
@@ -364,8 +382,10 @@ struct IbgpuAdapter {
     const int bn = (int)abody.size();
     std::vector<double> fm(6 * (size_t)bn);
     if (bn > 0) {
-      const int rc = ibgpu_wall_forces(ctx, fm.data());
+      const int rc = ibgpu_share_status(ibgpu_device_rank() ? ibgpu_wall_forces(ctx, fm.data())
+                                                            : IBGPU_OK);
       if (rc) return rc;
+      MPI_Bcast(fm.data(), 6 * bn, MPI_DOUBLE, 0, share_comm);
     }
     for (int i = 0; i < bn; ++i)
       for (int k = 0; k < 3; ++k) {
@@ -435,28 +455,41 @@ class GpuNS_Solver : public NS_Solver {
   }
 
   // Device context for this case (IBGPU_FP64 / IBGPU_FP64_EXACT /
-  // IBGPU_MIXED; the limiter as the reference was compiled with).
+  // IBGPU_MIXED; the limiter as the reference was compiled with).  Every
+  // rank of the node calls it; the device rank creates the context.
   int Create(int limiter, int precision) {
-    if (ctx_) return IBGPU_E_STATE;
-    const ibgpu_case c = IbgpuAdapter::MakeCase(*this, limiter, precision);
-    return ibgpu_create(&c, &ctx_);
+    if (created_) return IBGPU_E_STATE;
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      const ibgpu_case c = IbgpuAdapter::MakeCase(*this, limiter, precision);
+      rc = ibgpu_create(&c, &ctx_);
+    }
+    rc = ibgpu_share_status(rc);
+    created_ = rc == IBGPU_OK;
+    return rc;
   }
 
-  // After InitFlow and after every AMR::PerformAdaptive.
+  // After InitFlow and after every AMR::PerformAdaptive (every rank).
   int Upload(AMR &amr, std::vector<Body> &bodies) {
-    if (!ctx_) return IBGPU_E_STATE;
-    IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
-    return IbgpuAdapter::Upload(ctx_, lists_);
+    if (!created_) return IBGPU_E_STATE;
+    MPI_Barrier(share_comm);  // every rank's share of the arrays written
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
+      rc = IbgpuAdapter::Upload(ctx_, lists_);
+    }
+    return ibgpu_share_status(rc);
   }
 
   // The moving-body part of Body::IBConditions_Image (Body.cpp:1352-1357)
   // for a run stepping on the device: call before TimeMarching each step
-  // when the case moves its bodies (moveflag).  It accumulates dt00 as the
-  // reference does, moves and re-immerses the bodies on the host
-  // (IbgpuAdapter::MoveBodies) and hands the device the new cell flags and
-  // immersed-boundary records; the state stays on the device.
+  // when the case moves its bodies (moveflag), on every rank.  It
+  // accumulates dt00 as the reference does, moves and re-immerses the
+  // bodies on the host (IbgpuAdapter::MoveBodies) and hands the device the
+  // new cell flags and immersed-boundary records; the state stays on the
+  // device.
   int MoveBodies(std::vector<Body> &bodies, double &dt00) {
-    if (!ctx_) return IBGPU_E_STATE;
+    if (!created_) return IBGPU_E_STATE;
     dt00 += dt;
     int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00);
     if (rc) return rc;
@@ -466,69 +499,98 @@ class GpuNS_Solver : public NS_Solver {
 
   // After the bodies moved without a regrid: the flags of the same cell rows
   // (ibgpu_update_flags) and the immersed-boundary records
-  // (ibgpu_upload_ib) from the mesh as it is now.
+  // (ibgpu_upload_ib) from the mesh as it is now (every rank).
   int UploadImmersion(std::vector<Body> &bodies) {
-    if (!ctx_) return IBGPU_E_STATE;
-    for (size_t i = 0; i < lists_.box.size(); ++i)
-      lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
-    int rc = ibgpu_update_flags(ctx_, lists_.flags.data());
-    if (rc) return rc;
-    IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
-    return IbgpuAdapter::UploadIB(ctx_, lists_);
+    if (!created_) return IBGPU_E_STATE;
+    MPI_Barrier(share_comm);
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      for (size_t i = 0; i < lists_.box.size(); ++i)
+        lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
+      rc = ibgpu_update_flags(ctx_, lists_.flags.data());
+      if (rc == IBGPU_OK) {
+        IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
+        rc = IbgpuAdapter::UploadIB(ctx_, lists_);
+      }
+    }
+    return ibgpu_share_status(rc);
   }
 
   // One step: ghost fills, CFL dt every dt_var_step steps, the stages and
-  // the residual, aborting with the reference's code as it would.
+  // the residual, aborting with the reference's code as it would.  Every
+  // rank calls it and leaves with the device rank's dt.
   void TimeMarching(AMR &) {
-    ibgpu_diag diag;
-    const int rc = ibgpu_step(ctx_, ts, &dt, &diag);
-    if (rc == IBGPU_E_ABORT) MPI_Abort(MPI_COMM_WORLD, diag.abort_code);
-    if (rc != IBGPU_OK) {
-      std::fprintf(stderr, "ibgpu_step: %s (%s)\n", ibgpu_errstr(rc), ibgpu_last_error());
-      MPI_Abort(MPI_COMM_WORLD, 1);
+    double r[4] = {0.0, 0.0, 0.0, 0.0};  // status, abort code, dt, CFL dt
+    if (ibgpu_device_rank()) {
+      ibgpu_diag diag;
+      std::memset(&diag, 0, sizeof diag);
+      const int rc = ibgpu_step(ctx_, ts, &dt, &diag);
+      if (rc != IBGPU_OK && rc != IBGPU_E_ABORT)
+        std::fprintf(stderr, "ibgpu_step: %s (%s)\n", ibgpu_errstr(rc), ibgpu_last_error());
+      r[0] = rc;
+      r[1] = diag.abort_code;
+      r[2] = dt;
+      r[3] = diag.cfl_dt;
     }
-    if (ts % dt_var_step == 0) CFL_dt = diag.cfl_dt;
+    MPI_Bcast(r, 4, MPI_DOUBLE, 0, share_comm);
+    const int rc = (int)r[0];
+    if (rc == IBGPU_E_ABORT) MPI_Abort(MPI_COMM_WORLD, (int)r[1]);
+    if (rc != IBGPU_OK) MPI_Abort(MPI_COMM_WORLD, 1);
+    dt = r[2];
+    if (ts % dt_var_step == 0) CFL_dt = r[3];
   }
 
-  // m_data <- the device state, for output, host-side forces or a regrid.
+  // m_data <- the device state, for output, host-side forces or a regrid
+  // (every rank; the device rank writes the shared arrays).
   int Download() {
-    if (!ctx_) return IBGPU_E_STATE;
-    std::vector<double> rows(lists_.prim.size());
-    const int rc = ibgpu_download_state(ctx_, rows.data());
-    if (rc) return rc;
-    for (size_t i = 0; i < lists_.box.size(); ++i) {
-      FlowVariables &fv = a_mesh.LevelDataArray(lists_.level[i])[lists_.box[i]];
-      const double *r = &rows[7 * i];
-      fv.roe = r[0];
-      fv.u = r[1];
-      fv.v = r[2];
-      fv.w = r[3];
-      fv.p = r[4];
-      fv.T = r[5];
-      fv.e = r[6];
+    if (!created_) return IBGPU_E_STATE;
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      std::vector<double> rows(lists_.prim.size());
+      rc = ibgpu_download_state(ctx_, rows.data());
+      for (size_t i = 0; rc == IBGPU_OK && i < lists_.box.size(); ++i) {
+        FlowVariables &fv = a_mesh.LevelDataArray(lists_.level[i])[lists_.box[i]];
+        const double *q = &rows[7 * i];
+        fv.roe = q[0];
+        fv.u = q[1];
+        fv.v = q[2];
+        fv.w = q[3];
+        fv.p = q[4];
+        fv.T = q[5];
+        fv.e = q[6];
+      }
     }
-    return IBGPU_OK;
+    rc = ibgpu_share_status(rc);
+    MPI_Barrier(share_comm);
+    return rc;
   }
 
   // A level's refine/coarsen decision for AMR::TagtheBox (after Inittag):
   // the plain criterion, or with device MLP parameters the learned
   // indicator reading the device state, which is current after a step.
+  // One rank: the decisions go into the level's tag lists of this process.
   int TagLevel(const ibgpu_tag_rule &rule, AMR &amr, int level, const float *d_params = nullptr) {
-    if (!ctx_) return IBGPU_E_STATE;
+    if (!ctx_ || sprocs != 1) return IBGPU_E_STATE;
     return IbgpuAdapter::TagLevel(ctx_, rule, a_mesh, amr, level, d_params);
   }
 
   // Force and moment of every body from the device state
   // (Body::ComptWallForce): 6 per body, force then moment.
+  // (every rank; the device rank's values)
   int WallForces(std::vector<double> &out) {
-    if (!ctx_) return IBGPU_E_STATE;
+    if (!created_) return IBGPU_E_STATE;
     out.assign(6 * (size_t)Body::Bodynum(), 0.0);
-    return out.empty() ? IBGPU_OK : ibgpu_wall_forces(ctx_, out.data());
+    if (out.empty()) return IBGPU_OK;
+    const int rc = ibgpu_share_status(ibgpu_device_rank() ? ibgpu_wall_forces(ctx_, out.data())
+                                                          : IBGPU_OK);
+    if (rc == IBGPU_OK) MPI_Bcast(out.data(), (int)out.size(), MPI_DOUBLE, 0, share_comm);
+    return rc;
   }
 
   const IbgpuLists &lists() const { return lists_; }
 
  private:
-  ibgpu_ctx *ctx_ = nullptr;
-  IbgpuLists lists_;
+  ibgpu_ctx *ctx_ = nullptr;  // the device rank's context
+  bool created_ = false;      // on every rank once Create succeeded
+  IbgpuLists lists_;          // the device rank's lists
 };

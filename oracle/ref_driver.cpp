@@ -377,12 +377,12 @@ int main(int argc, char **argv) {
   MPI_Init(&argc, &argv);
   MPI_CreateNode();
   // IB_RANKS=N runs the reference's own shared-memory mode with N ranks: the
-  // step, dumps (written by rank 0) and force logs; the harness hooks that
-  // write from inside the case file or drive the GPU binding need one rank
+  // step (the reference's, or the binding's with rank 0 driving the GPU),
+  // dumps (written by rank 0) and force logs; the harness hooks that write
+  // from inside the case file or dump the binding's lists need one rank
   if (nprocs > 1 && (std::getenv("IB_TAG_DUMP") || std::getenv("IB_TAG_SERVER") ||
-                     std::getenv("IB_BINDING_LISTS") || std::getenv("IB_BINDING_TAGCHECK") ||
-                     env_int("IB_BINDING_STEP", 0))) {
-    if (nrank == 0) std::fprintf(stderr, "tag dumps, tag server and binding runs need one rank\n");
+                     std::getenv("IB_BINDING_LISTS") || std::getenv("IB_BINDING_TAGCHECK"))) {
+    if (nrank == 0) std::fprintf(stderr, "tag dumps, tag server and binding lists need one rank\n");
     MPI_Abort(MPI_COMM_WORLD, 5);
   }
   InitSpaceParams();

@@ -18,7 +18,9 @@ immersed-boundary records through ibgpu_upload_ib.
 * the reference's own main loop stepping through the C++ binding on the
   device (GpuNS_Solver::MoveBodies + TimeMarching) for 100 steps and four
   regrids: the dt and force history against the reference's own run,
-  exact <= 1e-12, FP64 <= 1e-10, mixed |dCl|, |dCd| < 1e-3.
+  exact <= 1e-12, FP64 <= 1e-10, mixed |dCl|, |dCd| < 1e-3;
+* the same loop in the reference's shared-memory MPI mode (4 ranks, rank 0
+  on the device): the 1-rank history.
 """
 import os
 import subprocess
@@ -124,12 +126,13 @@ def test_flag_update_keeps_the_layout(cuda_lib, pkg, snaps):
     sol.close()
 
 
-def run_binding(precision, steps=100):
+def run_binding(precision, steps=100, ranks=1):
     work = tempfile.mkdtemp(prefix="pitch_binding_")
     log = os.path.join(work, "forces.bin")
     env = dict(os.environ)
     env.update(make_golden.PITCH_ENV)
-    env.update(IB_STEPS=str(steps), IB_FORCE_LOG=log, IB_BINDING_STEP="1",
+    env.update(IB_STEPS=str(steps), IB_FORCE_LOG=log, IB_BINDING_STEP="1", IB_RANKS=str(ranks),
+               IB_MPI_TIMEOUT="300",
                IB_BINDING_PRECISION=str({"fp64": 0, "exact": 1, "mixed": 2}[precision]))
     out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True,
                          timeout=600)
@@ -152,3 +155,19 @@ def test_reference_loop_moves_the_body_through_the_binding(cuda_lib, precision, 
           f"{coef:.2e}, airfoil {total:.2e}")
     assert coef <= tol and total <= tol
     assert dt_err.max() <= (tol if precision != "mixed" else 1e-4)
+
+
+@pytest.mark.skipif(not os.path.exists(BINARY), reason="binding oracle not built (make -C oracle)")
+def test_binding_in_the_references_mpi_mode(cuda_lib):
+    """The same loop with the reference's host code on 4 ranks of one
+    shared-memory node (rank 0 drives the device, every rank re-immerses
+    its share of the moving body and regrids): the 1-rank binding's dt and
+    force history, to the reference's own rank-count dependence (partial
+    sums added in rank order)."""
+    one, _ = run_binding("fp64", steps=30)
+    four, out = run_binding("fp64", steps=30, ranks=4)
+    assert '"ranks": 4' in out
+    assert one.shape == four.shape and np.array_equal(one[:, 0], four[:, 0])
+    assert np.abs(one[:, 2] - four[:, 2]).max() <= 1e-12 * np.abs(one[:, 2]).max()
+    f1, f4 = one[:, 3:], four[:, 3:]
+    assert np.abs(f1 - f4).max() <= 1e-10 * F_REF
