@@ -742,6 +742,7 @@ def config3_section(steps: int = 12, warm: int = 2, rank: int = 0):
                      "with_host_reimmersion": res["cell_updates"] / res["loop_seconds"],
                      "host_reimmersion_ms_per_step": res["move_seconds"] * 1e3 / (steps - warm),
                      "host_ranks": res.get("ranks", 1),
+                     "host_phases_s_all_steps": res.get("move_phases_seconds"),
                      "cell_updates_per_step": res["cell_updates"] / (steps - warm)}
     f = {k: v[:, 3:].reshape(len(v), -1, 6)[:, :, :2].sum(axis=1) / F_REF for k, v in hist.items()}
     d = np.abs(f["mixed"] - f["fp64"]).max(axis=0)

@@ -55,6 +55,21 @@ struct IbgpuLists {
   std::vector<double> ib_cellf, patchf, body_center;  // 16 / 19 / 3 per row
 };
 
+// Wall-clock seconds (MPI_Wtime on this rank) of the moving-body phases,
+// accumulated over GpuNS_Solver::MoveBodies calls: device forces and their
+// broadcast, motion (Motion_Rule, ModifyBoxtoPatch), wall distances
+// (RenewLevelDistance), their synchronisation to block ghosts
+// (SynNormal_BlockDistance), the immersed-boundary cells and image points
+// (RemoveIBCells .. FindPatchHangingNode), and the device upload of the new
+// flags and records (UploadImmersion).
+struct IbgpuMoveTimes {
+  double forces = 0.0, motion = 0.0, distance = 0.0, sync = 0.0, ibcells = 0.0, upload = 0.0;
+};
+inline IbgpuMoveTimes &ibgpu_move_times() {
+  static IbgpuMoveTimes t;
+  return t;
+}
+
 // The rank that drives the device: rank 0 of the node (share_comm,
 // mpiparams.cpp:68-105).
 inline bool ibgpu_device_rank() { return srank == 0; }
@@ -380,6 +395,8 @@ struct IbgpuAdapter {
     std::vector<std::vector<int> > in_to_out(nlev), out_to_in(nlev);
     gridisnew = true;
     const int bn = (int)abody.size();
+    IbgpuMoveTimes &tm = ibgpu_move_times();
+    double t0 = MPI_Wtime();
     std::vector<double> fm(6 * (size_t)bn);
     if (bn > 0) {
       const int rc = ibgpu_share_status(ibgpu_device_rank() ? ibgpu_wall_forces(ctx, fm.data())
@@ -399,12 +416,24 @@ struct IbgpuAdapter {
         abody[2 * i].bodymoment(k) += abody[2 * i + 1].bodymoment(k);
         abody[2 * i + 1].bodymoment(k) = abody[2 * i].bodymoment(k);
       }
+    double t1 = MPI_Wtime();
+    tm.forces += t1 - t0;
+    t0 = t1;
     for (int i = 0; i < bn; ++i) {
       abody[i].Motion_Rule(amesh, dt00);
       abody[i].ModifyBoxtoPatch(amesh);
     }
+    t1 = MPI_Wtime();
+    tm.motion += t1 - t0;
+    t0 = t1;
     for (int l = 0; l < nlev; ++l) Body::RenewLevelDistance(amesh, abody, l, in_to_out[l], out_to_in[l]);
+    t1 = MPI_Wtime();
+    tm.distance += t1 - t0;
+    t0 = t1;
     for (int l = 0; l < nlev; ++l) amesh.SynNormal_BlockDistance(l, in_to_out[l], out_to_in[l]);
+    t1 = MPI_Wtime();
+    tm.sync += t1 - t0;
+    t0 = t1;
     Body::RemoveIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
     Body::InfectNewIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
     amesh.m_dis.holeplan(true);
@@ -414,6 +443,7 @@ struct IbgpuAdapter {
     amesh.DataExchangeCells_Wall();
     Body::FindImageCell_GhostIBCell(amesh, abody);
     for (int i = 0; i < bn; ++i) abody[i].FindPatchHangingNode(amesh);
+    tm.ibcells += MPI_Wtime() - t0;
     return IBGPU_OK;
   }
 
@@ -478,7 +508,21 @@ class GpuNS_Solver : public NS_Solver {
       IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
       rc = IbgpuAdapter::Upload(ctx_, lists_);
     }
-    return ibgpu_share_status(rc);
+    rc = ibgpu_share_status(rc);
+    if (rc == IBGPU_OK && sprocs > 1) {
+      // every rank learns the cell rows (level, box index), to share the
+      // per-row flag pass of UploadImmersion
+      int nrows = (int)lists_.box.size();
+      MPI_Bcast(&nrows, 1, MPI_INT, 0, share_comm);
+      if (!ibgpu_device_rank()) {
+        lists_ = IbgpuLists();
+        lists_.level.resize(nrows);
+        lists_.box.resize(nrows);
+      }
+      MPI_Bcast(lists_.level.data(), nrows, MPI_INT, 0, share_comm);
+      MPI_Bcast(lists_.box.data(), nrows, MPI_INT, 0, share_comm);
+    }
+    return rc;
   }
 
   // The moving-body part of Body::IBConditions_Image (Body.cpp:1352-1357)
@@ -494,7 +538,10 @@ class GpuNS_Solver : public NS_Solver {
     int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00);
     if (rc) return rc;
     dt00 = 0.0;
-    return UploadImmersion(bodies);
+    const double t0 = MPI_Wtime();
+    rc = UploadImmersion(bodies);
+    ibgpu_move_times().upload += MPI_Wtime() - t0;
+    return rc;
   }
 
   // After the bodies moved without a regrid: the flags of the same cell rows
@@ -503,10 +550,21 @@ class GpuNS_Solver : public NS_Solver {
   int UploadImmersion(std::vector<Body> &bodies) {
     if (!created_) return IBGPU_E_STATE;
     MPI_Barrier(share_comm);
+    // the rows' flags, each rank a contiguous share, gathered on every rank
+    const int nrows = (int)lists_.box.size();
+    std::vector<int> counts(sprocs), displs(sprocs);
+    for (int r = 0; r < sprocs; ++r) {
+      displs[r] = (int)((int64_t)nrows * r / sprocs);
+      counts[r] = (int)((int64_t)nrows * (r + 1) / sprocs) - displs[r];
+    }
+    lists_.flags.resize(nrows);
+    for (int i = displs[srank]; i < displs[srank] + counts[srank]; ++i)
+      lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
+    if (sprocs > 1)
+      MPI_Allgatherv(MPI_IN_PLACE, 0, MPI_BYTE, lists_.flags.data(), counts.data(), displs.data(),
+                     MPI_BYTE, share_comm);
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
-      for (size_t i = 0; i < lists_.box.size(); ++i)
-        lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
       rc = ibgpu_update_flags(ctx_, lists_.flags.data());
       if (rc == IBGPU_OK) {
         IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);

@@ -649,12 +649,26 @@ int main(int argc, char **argv) {
     if (prefix && dump_now(ts, s == nsteps - 1)) do_dump(ts);
   }
   if (flog) std::fclose(flog);
+  std::string phases = "{}";
+#ifdef ORACLE_BINDING
+  {
+    // moving-body phases on rank 0, all steps (warm-up included)
+    const IbgpuMoveTimes &mt = ibgpu_move_times();
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "{\"forces\": %.6f, \"motion\": %.6f, \"distance\": %.6f, \"sync\": %.6f, "
+                  "\"ibcells\": %.6f, \"upload\": %.6f}",
+                  mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload);
+    phases = buf;
+  }
+#endif
   if (nrank == 0)
     std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
                 "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g, "
-                "\"move_seconds\": %.9f, \"ranks\": %d}\n",
+                "\"move_seconds\": %.9f, \"ranks\": %d, \"move_phases_seconds\": %s}\n",
                 nsteps - timed_from, loop_time, cell_updates,
-                loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time, nprocs);
+                loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time, nprocs,
+                phases.c_str());
   std::fflush(stdout);
   MPI_Finalize();
   return 0;
