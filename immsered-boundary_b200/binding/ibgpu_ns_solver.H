@@ -79,6 +79,80 @@ inline int ibgpu_share_status(int rc) {
   return rc;
 }
 
+// A byte buffer shared by the ranks of the node: a shared window on
+// share_comm, all of it held by rank 0 (collective allocation and release).
+struct IbgpuSharedBytes {
+  MPI_Win win;
+  char *base = nullptr;
+  bool live = false;
+  void alloc(size_t nbytes) {
+    release();
+    char *local = nullptr;
+    MPI_Win_allocate_shared(srank == 0 ? (MPI_Aint)nbytes : 0, 1, MPI_INFO_NULL, share_comm,
+                            &local, &win);
+    MPI_Aint sz;
+    int du;
+    MPI_Win_shared_query(win, 0, &sz, &du, &base);
+    live = true;
+  }
+  void release() {
+    if (live) MPI_Win_free(&win);
+    live = false;
+    base = nullptr;
+  }
+};
+
+// One level's exchange buffers of the device wall distances
+// (ibgpu_wall_geometry / ibgpu_wall_distance): every rank packs and unpacks
+// its share of the boxes (DataArray::GlobalOrder) and of the block pairs
+// (DataArray::ps/pe, the shares SynNormal_BlockDistance works on).
+struct IbgpuWallLevel {
+  int64_t n = 0, nblock = 0;
+  IbgpuSharedBytes mem;
+  double *center = nullptr, *dtdm = nullptr, *dist = nullptr, *sd = nullptr, *dtb = nullptr;
+  int32_t *neib = nullptr, *body = nullptr, *patch = nullptr, *block_in = nullptr,
+          *block_out = nullptr;
+  uint8_t *kind = nullptr, *solid = nullptr, *moved = nullptr, *block_moved = nullptr;
+  void layout(int64_t n_, int64_t nb_) {
+    n = n_;
+    nblock = nb_;
+    size_t off = 0;
+    auto take = [&off](size_t bytes) {
+      const size_t o = off;
+      off += (bytes + 15) & ~(size_t)15;
+      return o;
+    };
+    const size_t oc = take(24 * n), odm = take(8 * n), odi = take(8 * n), osd = take(8 * n),
+                 otb = take(8 * n), one = take(36 * n), obo = take(4 * n), opa = take(4 * n),
+                 obi = take(4 * nblock), obu = take(4 * nblock), oki = take(n), oso = take(n),
+                 omo = take(n), obm = take(nblock);
+    mem.alloc(off);
+    char *b = mem.base;
+    center = (double *)(b + oc);
+    dtdm = (double *)(b + odm);
+    dist = (double *)(b + odi);
+    sd = (double *)(b + osd);
+    dtb = (double *)(b + otb);
+    neib = (int32_t *)(b + one);
+    body = (int32_t *)(b + obo);
+    patch = (int32_t *)(b + opa);
+    block_in = (int32_t *)(b + obi);
+    block_out = (int32_t *)(b + obu);
+    kind = (uint8_t *)(b + oki);
+    solid = (uint8_t *)(b + oso);
+    moved = (uint8_t *)(b + omo);
+    block_moved = (uint8_t *)(b + obm);
+  }
+};
+
+// Boxes whose device wall distances differed from the reference's own
+// (GpuNS_Solver::SetWallDistanceCheck), summed over the node's ranks and
+// every checked move.
+inline long long &ibgpu_wall_check_mismatches() {
+  static long long n = 0;
+  return n;
+}
+
 struct IbgpuAdapter {
   // Case constants (gas constants, stage coefficients, levels, schedules,
   // domain, force scales) from the reference's globals and the solver's
@@ -376,6 +450,175 @@ struct IbgpuAdapter {
     return IBGPU_OK;
   }
 
+  // ---- device wall distances (every rank of the node calls these)
+
+  // After a regrid: every level's boxes (centres, in-plane neighbours,
+  // kinds, distances to the domain boundary) and block pairs into the
+  // levels' exchange buffers and the device.
+  static int WallGeometry(ibgpu_ctx *ctx, Mesh &mesh, std::vector<IbgpuWallLevel> &W) {
+    for (auto &L : W) L.mem.release();
+    const int nlev = mesh.MyCurNum();
+    W.clear();
+    W.resize(nlev);
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = mesh.ShowLevelBox(l);
+      DataArray<NodePair> &bp = mesh.m_level[l].blockpair;
+      IbgpuWallLevel &L = W[l];
+      L.layout(boxes.realsize(), bp.size());
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      for (int i = bs; i < be; ++i) {
+        Box &bx = boxes[i];
+        Pointxyz &c = mesh.m_level[l].m_geom[i].boxcenter;
+        for (int k = 0; k < 3; ++k) L.center[3 * i + k] = c[k];
+        L.dtdm[i] = bx.pair.distance_to_dm;
+        L.kind[i] = bx.type == Dmghost ? IBGPU_WALL_BOX_DOMAIN_GHOST
+                    : bx.type == Blockghost ? IBGPU_WALL_BOX_BLOCK_GHOST
+                                            : IBGPU_WALL_BOX_OTHER;
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) L.neib[9 * i + 3 * a + b] = bx.neib[a][b][1];
+      }
+      for (int k = bp.ps(); k < bp.pe(); ++k) {
+        L.block_in[k] = bp[k].innode;
+        L.block_out[k] = bp[k].outnode.index;
+      }
+    }
+    MPI_Barrier(share_comm);
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      std::vector<ibgpu_wall_level_geom> g(nlev);
+      for (int l = 0; l < nlev; ++l) {
+        IbgpuWallLevel &L = W[l];
+        g[l] = ibgpu_wall_level_geom{L.n, L.center, L.neib, L.kind, L.dtdm, L.nblock,
+                                     L.block_in, L.block_out};
+      }
+      rc = ibgpu_wall_geometry(ctx, nlev, g.data());
+    }
+    return ibgpu_share_status(rc);
+  }
+
+  // The wall distances of the moved bodies on the device: every level's
+  // pairs as they are, computed anew (Body::RenewLevelDistance of every
+  // level, then Mesh::SynNormal_BlockDistance's block-ghost copies).  With
+  // apply the boxes take the new pairs and solid flags and this rank's move
+  // lists get the boxes of its shares that changed sides, in the order the
+  // reference's loops would push them; without, the results stay in W.
+  static int WallDistances(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody,
+                           std::vector<IbgpuWallLevel> &W, bool apply,
+                           std::vector<std::vector<int> > &in_to_out,
+                           std::vector<std::vector<int> > &out_to_in) {
+    const int nlev = amesh.MyCurNum();
+    if ((int)W.size() != nlev) return IBGPU_E_STATE;
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = amesh.ShowLevelBox(l);
+      IbgpuWallLevel &L = W[l];
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      for (int i = bs; i < be; ++i) {
+        const BoxtoWall &w = boxes[i].pair;
+        L.body[i] = w.body;
+        L.patch[i] = w.patch;
+        L.dist[i] = w.distance;
+        L.sd[i] = w.signdis;
+        L.dtb[i] = w.distance_to_body;
+        L.solid[i] = boxes[i].solid ? 1 : 0;
+      }
+    }
+    MPI_Barrier(share_comm);
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      // the bodies' wall patches where they are now (small: the device rank alone)
+      const int nb = (int)abody.size();
+      std::vector<int32_t> start(nb + 1, 0), nbc, nbl;
+      std::vector<double> pc, nv;
+      for (int b = 0; b < nb && rc == IBGPU_OK; ++b) {
+        Body &B = abody[b];
+        if (B.bodyindex != b) rc = IBGPU_E_ARG;
+        const int np = B.patch.size();
+        start[b + 1] = start[b] + np;
+        for (int p = 0; p < np; ++p) {
+          for (int k = 0; k < 3; ++k) pc.push_back(B.patch[p].pc[k]);
+          for (int k = 0; k < 3; ++k) nv.push_back(B.patch[p].nv[k]);
+          nbc.push_back(B.patneib[p].nbnum);
+          for (int k = 0; k < IBGPU_WALL_MAX_NB; ++k)
+            nbl.push_back(k < B.patneib[p].nbnum ? B.patneib[p].nb[k] : -1);
+        }
+      }
+      if (rc == IBGPU_OK) {
+        const ibgpu_wall_bodies wb = {nb, start.data(), pc.data(), nv.data(), nbc.data(),
+                                      nbl.data(), periodic[1] ? 1 : 0, critic_ylength,
+                                      dmlength[1]};
+        std::vector<ibgpu_wall_pairs> pr(nlev);
+        for (int l = 0; l < nlev; ++l) {
+          IbgpuWallLevel &L = W[l];
+          pr[l] = ibgpu_wall_pairs{L.body, L.patch, L.dist, L.sd, L.dtb, L.solid, L.moved,
+                                   L.block_moved};
+        }
+        rc = ibgpu_wall_distance(ctx, &wb, nlev, pr.data());
+      }
+    }
+    rc = ibgpu_share_status(rc);
+    MPI_Barrier(share_comm);
+    if (rc != IBGPU_OK || !apply) return rc;
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = amesh.ShowLevelBox(l);
+      DataArray<NodePair> &bp = amesh.m_level[l].blockpair;
+      IbgpuWallLevel &L = W[l];
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      for (int i = bs; i < be; ++i) {
+        BoxtoWall &w = boxes[i].pair;
+        w.body = L.body[i];
+        w.patch = L.patch[i];
+        w.distance = L.dist[i];
+        w.signdis = L.sd[i];
+        w.distance_to_body = L.dtb[i];
+        boxes[i].solid = L.solid[i] != 0;
+        if (L.moved[i] == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(i);
+        else if (L.moved[i] == IBGPU_WALL_OUT_OF_BODY) in_to_out[l].push_back(i);
+      }
+      for (int k = bp.ps(); k < bp.pe(); ++k) {
+        if (L.block_moved[k] == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(L.block_out[k]);
+        else if (L.block_moved[k] == IBGPU_WALL_OUT_OF_BODY) in_to_out[l].push_back(L.block_out[k]);
+      }
+    }
+    MPI_Barrier(share_comm);  // every box written before the reference's next loops
+    return IBGPU_OK;
+  }
+
+  // Boxes of this rank's shares whose pair, solid flag or move-list entries
+  // differ between the device results in W and the mesh as the reference's
+  // own loops left it.
+  static long long WallMismatches(Mesh &amesh, std::vector<IbgpuWallLevel> &W,
+                                  const std::vector<std::vector<int> > &in_to_out,
+                                  const std::vector<std::vector<int> > &out_to_in) {
+    long long bad = 0;
+    for (size_t l = 0; l < W.size(); ++l) {
+      DataArray<Box> &boxes = amesh.ShowLevelBox((int)l);
+      DataArray<NodePair> &bp = amesh.m_level[l].blockpair;
+      IbgpuWallLevel &L = W[l];
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      std::vector<int> dev_in, dev_out;
+      for (int i = bs; i < be; ++i) {
+        const BoxtoWall &w = boxes[i].pair;
+        if (w.body != L.body[i] || w.patch != L.patch[i] ||
+            std::memcmp(&w.distance, &L.dist[i], 8) || std::memcmp(&w.signdis, &L.sd[i], 8) ||
+            std::memcmp(&w.distance_to_body, &L.dtb[i], 8) || boxes[i].solid != (L.solid[i] != 0))
+          ++bad;
+        if (L.moved[i] == IBGPU_WALL_INTO_BODY) dev_in.push_back(i);
+        else if (L.moved[i] == IBGPU_WALL_OUT_OF_BODY) dev_out.push_back(i);
+      }
+      for (int k = bp.ps(); k < bp.pe(); ++k) {
+        if (L.block_moved[k] == IBGPU_WALL_INTO_BODY) dev_in.push_back(L.block_out[k]);
+        else if (L.block_moved[k] == IBGPU_WALL_OUT_OF_BODY) dev_out.push_back(L.block_out[k]);
+      }
+      if (dev_in != out_to_in[l]) ++bad;
+      if (dev_out != in_to_out[l]) ++bad;
+    }
+    return bad;
+  }
+
   // Body::MovingBody_Image (Bodymove.cpp:37-125) for a run whose state lives
   // on the device: the bodies' forces and moments come from the device
   // (ibgpu_wall_forces, the wall patches as the last upload left them: the
@@ -389,7 +632,11 @@ struct IbgpuAdapter {
   // records (GpuNS_Solver::UploadImmersion).
   // Every rank of the node calls it (the re-immersion is the reference's
   // own collective code); ctx is the device rank's context.
-  static int MoveBodies(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody, double &dt00) {
+  // With W (the device wall distances, after WallGeometry) the distance
+  // and block-ghost passes run on the device; with check also the
+  // reference's own, the difference counted (ibgpu_wall_check_mismatches).
+  static int MoveBodies(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody, double &dt00,
+                        std::vector<IbgpuWallLevel> *W = nullptr, bool check = false) {
     const int nlev = amesh.MyCurNum();
     const int last = nlev - 1;
     std::vector<std::vector<int> > in_to_out(nlev), out_to_in(nlev);
@@ -426,14 +673,31 @@ struct IbgpuAdapter {
     t1 = MPI_Wtime();
     tm.motion += t1 - t0;
     t0 = t1;
-    for (int l = 0; l < nlev; ++l) Body::RenewLevelDistance(amesh, abody, l, in_to_out[l], out_to_in[l]);
-    t1 = MPI_Wtime();
-    tm.distance += t1 - t0;
-    t0 = t1;
-    for (int l = 0; l < nlev; ++l) amesh.SynNormal_BlockDistance(l, in_to_out[l], out_to_in[l]);
-    t1 = MPI_Wtime();
-    tm.sync += t1 - t0;
-    t0 = t1;
+    if (W && !check) {
+      const int rc = WallDistances(ctx, amesh, abody, *W, true, in_to_out, out_to_in);
+      if (rc) return rc;
+      t1 = MPI_Wtime();
+      tm.distance += t1 - t0;
+      t0 = t1;
+    } else {
+      if (W) {  // the device's results first, from the same pairs
+        const int rc = WallDistances(ctx, amesh, abody, *W, false, in_to_out, out_to_in);
+        if (rc) return rc;
+      }
+      for (int l = 0; l < nlev; ++l) Body::RenewLevelDistance(amesh, abody, l, in_to_out[l], out_to_in[l]);
+      t1 = MPI_Wtime();
+      tm.distance += t1 - t0;
+      t0 = t1;
+      for (int l = 0; l < nlev; ++l) amesh.SynNormal_BlockDistance(l, in_to_out[l], out_to_in[l]);
+      t1 = MPI_Wtime();
+      tm.sync += t1 - t0;
+      t0 = t1;
+      if (W) {
+        long long bad = WallMismatches(amesh, *W, in_to_out, out_to_in);
+        MPI_Allreduce(MPI_IN_PLACE, &bad, 1, MPI_LONG, MPI_SUM, share_comm);
+        ibgpu_wall_check_mismatches() += bad;
+      }
+    }
     Body::RemoveIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
     Body::InfectNewIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
     amesh.m_dis.holeplan(true);
@@ -509,6 +773,8 @@ class GpuNS_Solver : public NS_Solver {
       rc = IbgpuAdapter::Upload(ctx_, lists_);
     }
     rc = ibgpu_share_status(rc);
+    if (rc == IBGPU_OK && device_distance_ && Body::Bodynum() > 0)
+      rc = IbgpuAdapter::WallGeometry(ctx_, a_mesh, wall_);
     if (rc == IBGPU_OK && sprocs > 1) {
       // every rank learns the cell rows (level, box index), to share the
       // per-row flag pass of UploadImmersion
@@ -535,13 +801,24 @@ class GpuNS_Solver : public NS_Solver {
   int MoveBodies(std::vector<Body> &bodies, double &dt00) {
     if (!created_) return IBGPU_E_STATE;
     dt00 += dt;
-    int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00);
+    int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00,
+                                      device_distance_ ? &wall_ : nullptr, wall_check_);
     if (rc) return rc;
     dt00 = 0.0;
     const double t0 = MPI_Wtime();
     rc = UploadImmersion(bodies);
     ibgpu_move_times().upload += MPI_Wtime() - t0;
     return rc;
+  }
+
+  // Wall distances of moving bodies on the device (ibgpu_wall_distance) in
+  // place of the reference's RenewLevelDistance and SynNormal_BlockDistance
+  // (the default); with check, both, the reference's results kept and the
+  // boxes that differ counted in ibgpu_wall_check_mismatches().  Set
+  // before Upload, on every rank.
+  void SetDeviceWallDistances(bool on, bool check = false) {
+    device_distance_ = on;
+    wall_check_ = on && check;
   }
 
   // After the bodies moved without a regrid: the flags of the same cell rows
@@ -651,4 +928,6 @@ class GpuNS_Solver : public NS_Solver {
   ibgpu_ctx *ctx_ = nullptr;  // the device rank's context
   bool created_ = false;      // on every rank once Create succeeded
   IbgpuLists lists_;          // the device rank's lists
+  bool device_distance_ = true, wall_check_ = false;
+  std::vector<IbgpuWallLevel> wall_;  // exchange buffers of the device wall distances
 };

@@ -26,6 +26,7 @@ UNITS = {
     "noalloc.cu": [],
     "indicator.cu": [],
     "interfaces.cu": [],
+    "wall.cu": ["-fmad=false"],  # IEEE-exact wall distances (no contractions)
 }
 
 

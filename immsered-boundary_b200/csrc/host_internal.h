@@ -31,6 +31,9 @@ int ctx_signdis_buffer(ibgpu_ctx *ctx, double **dev, bool create);
 int ctx_tags_buffer(ibgpu_ctx *ctx, uint8_t **dev);
 // slot of box (l, ix, iy) of the uploaded topology (periodic wrap), -1 if absent
 int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy);
+// the context's wall-distance state (csrc/wall.cu), freed with the context
+void **ctx_wall_state(ibgpu_ctx *ctx);
+void wall_free(void *state);
 
 // indicator entry points shared with the batched runner (csrc/indicator.cu)
 int tag_mesh_enqueue(ibgpu_ctx *ctx, const ibgpu_tag_rule *rule, const float *d_params,

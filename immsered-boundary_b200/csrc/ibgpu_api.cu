@@ -69,6 +69,7 @@ int dev_alloc(T **p, size_t n) {
 }  // namespace
 
 struct ibgpu_ctx {
+  void *wall = nullptr;  // wall-distance state (csrc/wall.cu)
   ibgpu_case cs;
   CaseConst cc;
   int device = 0;
@@ -313,6 +314,7 @@ int ctx_tags_buffer(ibgpu_ctx *ctx, uint8_t **dev) {
 int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy) {
   return ctx ? ctx->slot_at(l, ix, iy) : -1;
 }
+void **ctx_wall_state(ibgpu_ctx *ctx) { return &ctx->wall; }
 }  // namespace ibgpu
 
 extern "C" {
@@ -2069,6 +2071,7 @@ void ibgpu_destroy(ibgpu_ctx *ctx) {
   if (ctx->in_stream) cudaStreamSynchronize(ctx->in_stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   ctx->free_layout();
+  ibgpu::wall_free(ctx->wall);
   cudaFree(ctx->d_diag);
   cudaFree(ctx->d_aux_err);
   cudaFreeHost(ctx->h_diag);

@@ -1,0 +1,473 @@
+// Wall distances of moved bodies on the device: the per-box part of the
+// reference's re-immersion (Body::RenewLevelDistance, Bodymove.cpp:127-300)
+// and the block-ghost copies of Mesh::SynNormal_BlockDistance
+// (Mesh.cpp:2303-2374), in four passes per level:
+//   walk     closest wall patch of the box's own body by the reference's
+//            walk over neighbouring patches (Body::FindClosePatchtoCell,
+//            Body.H:505-580), signed distance along that patch's normal;
+//   junction boxes whose in-plane neighbours belong to another body try that
+//            body from the neighbour's patch and take it by the reference's
+//            rule (Bodymove.cpp:158-228), reading the neighbours' walked pairs;
+//   finalise signed distance capped by the distance to the domain boundary,
+//            solid flag, and the boxes that changed sides (the reference's
+//            move lists, Bodymove.cpp:231-255);
+//   block    every block ghost takes its origin box's pair and solid flag.
+// This unit is compiled without floating-point contraction and uses the
+// correctly rounded square root, so every distance is the reference's bit
+// for bit (its host code evaluates the same expressions in the same order).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ibgpu.h"
+#include "host_internal.h"
+
+namespace ibgpu {
+namespace wall {
+
+constexpr double kCriticDis = 9.5;  // Bodymove.cpp:132
+constexpr double kFar = 999.0;      // the walk's starting distance (Bodymove.cpp:150, 199)
+
+struct BodiesDev {
+  int nbodies;
+  const int32_t *start;  // nbodies + 1
+  const double *pc, *nv;
+  const int32_t *nbc, *nb;
+  int periodic_y;
+  double critic_y, len_y;
+};
+
+struct LevelDev {
+  int64_t n, nblock;
+  const double *center, *dtdm;
+  const int32_t *neib;
+  const uint8_t *kind;
+  const int32_t *block_in, *block_out;
+  // pairs as handed in, after the walk, final
+  const int32_t *body0, *patch0;
+  const double *dist0, *sd0, *dtb0;
+  int32_t *body1, *patch1;
+  double *dist1, *sd1, *dtb1;
+  int32_t *body2, *patch2;
+  double *dist2, *sd2, *dtb2;
+  uint8_t *solid, *moved, *block_moved;
+};
+
+// PeriodicLength (mpiparams.cpp:294-310): the y offset across a periodic
+// domain
+__device__ __forceinline__ double periodic_dy(const BodiesDev &B, double dy) {
+  if (fabs(dy) > B.critic_y && B.periodic_y) {
+    if (dy > B.critic_y) dy -= B.len_y;
+    else if (dy < -B.critic_y) dy += B.len_y;
+  }
+  return dy;
+}
+
+// |centre - pc| of patch row r (Pointxyz::length, Point.H:211-214)
+__device__ __forceinline__ double patch_distance(const BodiesDev &B, int r, double cx, double cy,
+                                                 double cz) {
+  const double dx = cx - B.pc[3 * r];
+  const double dy = periodic_dy(B, cy - B.pc[3 * r + 1]);
+  const double dz = cz - B.pc[3 * r + 2];
+  return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// Body::FindClosePatchtoCell from patch p of body b with the distance still
+// at kFar: the walk to a patch no neighbour of which is closer (each step
+// strictly closer, so it ends within the body's patch count), then the
+// signed distance nv . (centre - pc).  false when the walk does not end.
+__device__ __forceinline__ bool find_close(const BodiesDev &B, int b, int p, double cx, double cy,
+                                           double cz, int &patch, double &dist, double &signdis) {
+  const int base = B.start[b], count = B.start[b + 1] - base;
+  double best = kFar;
+  int bp = p;
+  {
+    const double d = patch_distance(B, base + p, cx, cy, cz);
+    if (d < best) best = d;
+  }
+  int old = -1, ps0 = bp;
+  for (int guard = 0; old != ps0; ++guard) {
+    if (guard > count) return false;
+    old = bp;
+    const int row = base + ps0;
+    const int nn = B.nbc[row];
+    for (int k = 0; k < nn; ++k) {
+      const int q = B.nb[row * IBGPU_WALL_MAX_NB + k];
+      if (q < 0 || q >= count) return false;
+      const double d = patch_distance(B, base + q, cx, cy, cz);
+      if (d < best) {
+        best = d;
+        bp = q;
+      }
+    }
+    ps0 = bp;
+  }
+  const int r = base + bp;
+  const double dx = cx - B.pc[3 * r];
+  const double dy = periodic_dy(B, cy - B.pc[3 * r + 1]);
+  const double dz = cz - B.pc[3 * r + 2];
+  patch = bp;
+  dist = best;
+  signdis = B.nv[3 * r] * dx + B.nv[3 * r + 1] * dy + B.nv[3 * r + 2] * dz;
+  return true;
+}
+
+__device__ __forceinline__ bool valid_pair(const BodiesDev &B, int body, int patch) {
+  return body > -1 && body < B.nbodies && patch > -1 && patch < B.start[body + 1] - B.start[body];
+}
+
+__global__ void walk_kernel(LevelDev L, BodiesDev B, int *err) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  int body = L.body0[i], patch = L.patch0[i];
+  double dist = L.dist0[i], sd = L.sd0[i], dtb = L.dtb0[i];
+  if (sd < kCriticDis && L.kind[i] != IBGPU_WALL_BOX_BLOCK_GHOST) {
+    if (!valid_pair(B, body, patch) ||
+        !find_close(B, body, patch, L.center[3 * i], L.center[3 * i + 1], L.center[3 * i + 2],
+                    patch, dist, sd)) {
+      atomicExch(err, 1);
+    } else {
+      dtb = sd;
+    }
+  }
+  L.body1[i] = body;
+  L.patch1[i] = patch;
+  L.dist1[i] = dist;
+  L.sd1[i] = sd;
+  L.dtb1[i] = dtb;
+}
+
+// Boxes next to another body's boxes: that body from the neighbour's patch,
+// taken when it is on the fluid side where the own one is not, or closer
+// without a worse side (the neighbours in Point_iterator_2d order, each
+// compared with the box's pair as the earlier ones left it).
+__global__ void junction_kernel(LevelDev L, BodiesDev B, int *err) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  int body = L.body1[i], patch = L.patch1[i];
+  double dist = L.dist1[i], sd = L.sd1[i], dtb = L.dtb1[i];
+  if (sd < kCriticDis && L.kind[i] != IBGPU_WALL_BOX_BLOCK_GHOST) {
+    const int own = L.body1[i];
+    const double cx = L.center[3 * i], cy = L.center[3 * i + 1], cz = L.center[3 * i + 2];
+    for (int k = 0; k < 9; ++k) {
+      const int an = L.neib[9 * i + k];
+      if (an < 0 || L.body1[an] == own) continue;
+      const int cb = L.body1[an], cp = L.patch1[an];
+      if (body == cb) continue;
+      int np = 0;
+      double nd = 0.0, nsd = 0.0;
+      if (!valid_pair(B, cb, cp) || !find_close(B, cb, cp, cx, cy, cz, np, nd, nsd)) {
+        atomicExch(err, 1);
+        break;
+      }
+      bool change = false;
+      if (nsd > 0.0 && sd < 0.0) {
+        change = true;
+      } else if (nd < dist) {
+        if (sd * nsd > 0.0) change = true;
+        else if (nsd > 0.0) change = true;
+      }
+      if (change) {
+        body = cb;
+        patch = np;
+        dist = nd;
+        sd = nsd;
+        dtb = nsd;
+      }
+    }
+  }
+  L.body2[i] = body;
+  L.patch2[i] = patch;
+  L.dist2[i] = dist;
+  L.sd2[i] = sd;
+  L.dtb2[i] = dtb;
+}
+
+__global__ void finalize_kernel(LevelDev L) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  uint8_t mv = 0;
+  double sd = L.sd2[i];
+  const uint8_t kind = L.kind[i];
+  if (sd < kCriticDis && kind != IBGPU_WALL_BOX_BLOCK_GHOST) {
+    const double dm = L.dtdm[i];
+    sd = (dm < sd) ? dm : sd;  // std::min(signdis, distance_to_dm)
+    L.sd2[i] = sd;
+    if (sd < 0.0) {
+      if (!L.solid[i] && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_INTO_BODY;
+      L.solid[i] = 1;
+    } else {
+      if (L.solid[i] && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_OUT_OF_BODY;
+      L.solid[i] = 0;
+    }
+  }
+  L.moved[i] = mv;
+}
+
+// block ghosts: targets are distinct and never origins (checked on upload)
+__global__ void block_kernel(LevelDev L) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= L.nblock) return;
+  const int in = L.block_in[k], out = L.block_out[k];
+  L.body2[out] = L.body2[in];
+  L.patch2[out] = L.patch2[in];
+  L.dist2[out] = L.dist2[in];
+  const double sd = L.sd2[in];
+  L.sd2[out] = sd;
+  uint8_t mv = 0;
+  const bool dg = L.kind[out] == IBGPU_WALL_BOX_DOMAIN_GHOST;
+  if (sd < 0.0) {
+    if (!L.solid[out] && !dg) mv = IBGPU_WALL_INTO_BODY;
+    L.solid[out] = 1;
+  } else {
+    if (L.solid[out] && !dg) mv = IBGPU_WALL_OUT_OF_BODY;
+    L.solid[out] = 0;
+  }
+  L.block_moved[k] = mv;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+struct Buf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~Buf() { cudaFree(p); }
+  cudaError_t reserve(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b > 0 ? b : 1);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(p); }
+};
+
+struct Level {
+  int64_t n = 0, nblock = 0;
+  Buf center, dtdm, neib, kind, block_in, block_out;
+  Buf body[3], patch[3], dist[3], sd[3], dtb[3], solid, moved, block_moved;
+};
+
+struct State {
+  std::vector<Level> levels;
+  Buf start, pc, nv, nbc, nb, err;
+};
+
+}  // namespace wall
+
+void wall_free(void *state) { delete static_cast<wall::State *>(state); }
+
+}  // namespace ibgpu
+
+using namespace ibgpu;
+using namespace ibgpu::wall;
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? IBGPU_E_NOMEM : IBGPU_E_CUDA;
+}
+#define WK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+template <typename T>
+int put(Buf &b, const T *h, int64_t n, cudaStream_t st) {
+  WK(b.reserve((size_t)n * sizeof(T)));
+  if (n > 0) WK(cudaMemcpyAsync(b.p, h, (size_t)n * sizeof(T), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+template <typename T>
+int get(T *h, const Buf &b, int64_t n, cudaStream_t st) {
+  if (n > 0) WK(cudaMemcpyAsync(h, b.p, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, st));
+  return IBGPU_OK;
+}
+
+unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace
+
+extern "C" {
+
+int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom *levels) {
+  CtxView V;
+  if (!ctx || nlevels < 0 || (nlevels > 0 && !levels) || ctx_view(ctx, &V) != IBGPU_OK)
+    return IBGPU_E_ARG;
+  for (int l = 0; l < nlevels; ++l) {
+    const ibgpu_wall_level_geom &g = levels[l];
+    if (g.n < 0 || g.n > INT32_MAX || g.nblock < 0 ||
+        (g.n > 0 && (!g.center || !g.neib || !g.kind || !g.distance_to_dm)) ||
+        (g.nblock > 0 && (!g.block_in || !g.block_out)))
+      return IBGPU_E_ARG;
+    for (int64_t i = 0; i < 9 * g.n; ++i)
+      if (g.neib[i] < -1 || g.neib[i] >= g.n) {
+        set_last_error("wall geometry: neighbour index out of the level's boxes");
+        return IBGPU_E_ARG;
+      }
+    // block pairs: distinct targets, none of them an origin
+    std::vector<uint8_t> mark((size_t)g.n, 0);
+    for (int64_t k = 0; k < g.nblock; ++k) {
+      const int in = g.block_in[k], out = g.block_out[k];
+      if (in < 0 || in >= g.n || out < 0 || out >= g.n || mark[out]) {
+        set_last_error("wall geometry: block pair out of range or a ghost targeted twice");
+        return IBGPU_E_ARG;
+      }
+      mark[out] = 1;
+    }
+    for (int64_t k = 0; k < g.nblock; ++k)
+      if (mark[g.block_in[k]]) {
+        set_last_error("wall geometry: a block ghost is the origin of another pair");
+        return IBGPU_E_ARG;
+      }
+  }
+  void **slot = ctx_wall_state(ctx);
+  State *S = static_cast<State *>(*slot);
+  if (!S) *slot = S = new State();
+  S->levels.resize((size_t)nlevels);
+  cudaStream_t st = V.stream;
+  for (int l = 0; l < nlevels; ++l) {
+    const ibgpu_wall_level_geom &g = levels[l];
+    Level &L = S->levels[(size_t)l];
+    L.n = g.n;
+    L.nblock = g.nblock;
+    int rc;
+    if ((rc = put(L.center, g.center, 3 * g.n, st)) || (rc = put(L.neib, g.neib, 9 * g.n, st)) ||
+        (rc = put(L.kind, g.kind, g.n, st)) || (rc = put(L.dtdm, g.distance_to_dm, g.n, st)) ||
+        (rc = put(L.block_in, g.block_in, g.nblock, st)) ||
+        (rc = put(L.block_out, g.block_out, g.nblock, st)))
+      return rc;
+    for (int k = 0; k < 3; ++k) {
+      WK(L.body[k].reserve((size_t)g.n * 4));
+      WK(L.patch[k].reserve((size_t)g.n * 4));
+      WK(L.dist[k].reserve((size_t)g.n * 8));
+      WK(L.sd[k].reserve((size_t)g.n * 8));
+      WK(L.dtb[k].reserve((size_t)g.n * 8));
+    }
+    WK(L.solid.reserve((size_t)g.n));
+    WK(L.moved.reserve((size_t)g.n));
+    WK(L.block_moved.reserve((size_t)g.nblock));
+  }
+  WK(S->err.reserve(sizeof(int)));
+  WK(cudaStreamSynchronize(st));
+  return IBGPU_OK;
+}
+
+int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
+                        ibgpu_wall_pairs *pairs) {
+  CtxView V;
+  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !pairs) || ctx_view(ctx, &V) != IBGPU_OK)
+    return IBGPU_E_ARG;
+  State *S = static_cast<State *>(*ctx_wall_state(ctx));
+  if (!S || (int)S->levels.size() != nlevels) {
+    set_last_error("wall distances: upload the wall geometry of these levels first");
+    return IBGPU_E_STATE;
+  }
+  const int nb = bodies->nbodies;
+  if (nb < 0 || (nb > 0 && (!bodies->patch_start || !bodies->pc || !bodies->nv ||
+                            !bodies->nb_count || !bodies->nb)))
+    return IBGPU_E_ARG;
+  const int64_t np = nb > 0 ? bodies->patch_start[nb] : 0;
+  for (int b = 0; b < nb; ++b)
+    if (bodies->patch_start[b] < 0 || bodies->patch_start[b + 1] < bodies->patch_start[b])
+      return IBGPU_E_ARG;
+  for (int64_t r = 0; r < np; ++r)
+    if (bodies->nb_count[r] < 0 || bodies->nb_count[r] > IBGPU_WALL_MAX_NB) return IBGPU_E_ARG;
+  for (int l = 0; l < nlevels; ++l) {
+    const ibgpu_wall_pairs &p = pairs[l];
+    const Level &L = S->levels[(size_t)l];
+    if ((L.n > 0 && (!p.body || !p.patch || !p.distance || !p.signdis || !p.distance_to_body ||
+                     !p.solid || !p.moved)) ||
+        (L.nblock > 0 && !p.block_moved))
+      return IBGPU_E_ARG;
+  }
+  cudaStream_t st = V.stream;
+  int rc;
+  const int32_t zero_start = 0;
+  if ((rc = put(S->start, nb > 0 ? bodies->patch_start : &zero_start, nb + 1, st)) ||
+      (rc = put(S->pc, bodies->pc, 3 * np, st)) || (rc = put(S->nv, bodies->nv, 3 * np, st)) ||
+      (rc = put(S->nbc, bodies->nb_count, np, st)) ||
+      (rc = put(S->nb, bodies->nb, (int64_t)IBGPU_WALL_MAX_NB * np, st)))
+    return rc;
+  BodiesDev B;
+  B.nbodies = nb;
+  B.start = S->start.as<int32_t>();
+  B.pc = S->pc.as<double>();
+  B.nv = S->nv.as<double>();
+  B.nbc = S->nbc.as<int32_t>();
+  B.nb = S->nb.as<int32_t>();
+  B.periodic_y = bodies->periodic_y;
+  B.critic_y = bodies->critic_ylength;
+  B.len_y = bodies->dm_length_y;
+  WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
+  for (int l = 0; l < nlevels; ++l) {
+    Level &L = S->levels[(size_t)l];
+    ibgpu_wall_pairs &p = pairs[l];
+    if (L.n == 0) continue;
+    if ((rc = put(L.body[0], p.body, L.n, st)) || (rc = put(L.patch[0], p.patch, L.n, st)) ||
+        (rc = put(L.dist[0], p.distance, L.n, st)) || (rc = put(L.sd[0], p.signdis, L.n, st)) ||
+        (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) || (rc = put(L.solid, p.solid, L.n, st)))
+      return rc;
+    LevelDev D;
+    D.n = L.n;
+    D.nblock = L.nblock;
+    D.center = L.center.as<double>();
+    D.dtdm = L.dtdm.as<double>();
+    D.neib = L.neib.as<int32_t>();
+    D.kind = L.kind.as<uint8_t>();
+    D.block_in = L.block_in.as<int32_t>();
+    D.block_out = L.block_out.as<int32_t>();
+    D.body0 = L.body[0].as<int32_t>();
+    D.patch0 = L.patch[0].as<int32_t>();
+    D.dist0 = L.dist[0].as<double>();
+    D.sd0 = L.sd[0].as<double>();
+    D.dtb0 = L.dtb[0].as<double>();
+    D.body1 = L.body[1].as<int32_t>();
+    D.patch1 = L.patch[1].as<int32_t>();
+    D.dist1 = L.dist[1].as<double>();
+    D.sd1 = L.sd[1].as<double>();
+    D.dtb1 = L.dtb[1].as<double>();
+    D.body2 = L.body[2].as<int32_t>();
+    D.patch2 = L.patch[2].as<int32_t>();
+    D.dist2 = L.dist[2].as<double>();
+    D.sd2 = L.sd[2].as<double>();
+    D.dtb2 = L.dtb[2].as<double>();
+    D.solid = L.solid.as<uint8_t>();
+    D.moved = L.moved.as<uint8_t>();
+    D.block_moved = L.block_moved.as<uint8_t>();
+    int *err = S->err.as<int>();
+    walk_kernel<<<blocks(L.n), 256, 0, st>>>(D, B, err);
+    junction_kernel<<<blocks(L.n), 256, 0, st>>>(D, B, err);
+    finalize_kernel<<<blocks(L.n), 256, 0, st>>>(D);
+    if (L.nblock > 0) block_kernel<<<blocks(L.nblock), 256, 0, st>>>(D);
+    WK(cudaGetLastError());
+    if ((rc = get(p.body, L.body[2], L.n, st)) || (rc = get(p.patch, L.patch[2], L.n, st)) ||
+        (rc = get(p.distance, L.dist[2], L.n, st)) || (rc = get(p.signdis, L.sd[2], L.n, st)) ||
+        (rc = get(p.distance_to_body, L.dtb[2], L.n, st)) || (rc = get(p.solid, L.solid, L.n, st)) ||
+        (rc = get(p.moved, L.moved, L.n, st)) ||
+        (rc = get(p.block_moved, L.block_moved, L.nblock, st)))
+      return rc;
+  }
+  int herr = 0;
+  WK(cudaMemcpyAsync(&herr, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WK(cudaStreamSynchronize(st));
+  if (herr) {
+    set_last_error("wall distances: a box within 9.5 of a wall has no valid body or patch, "
+                   "or a patch walk did not end");
+    return IBGPU_E_ABORT;
+  }
+  return IBGPU_OK;
+}
+
+}  // extern "C"

@@ -40,7 +40,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
            "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
-           "ibgpu_set_state_rows", "ibgpu_build_interfaces")
+           "ibgpu_set_state_rows", "ibgpu_build_interfaces", "ibgpu_wall_geometry",
+           "ibgpu_wall_distance")
 ROWS_FLOWVARS, ROWS_COMPACT = 7, 4
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
@@ -96,6 +97,33 @@ class InterfaceLists(ctypes.Structure):
                 ("cap_res", ctypes.c_int64), ("cap_pro", ctypes.c_int64),
                 ("cap_ghost", ctypes.c_int64), ("res", ctypes.c_void_p), ("pro", ctypes.c_void_p),
                 ("ghost", ctypes.c_void_p)]
+
+
+# device wall distances of moved bodies (ibgpu_wall_*)
+WALL_BOX_OTHER, WALL_BOX_DOMAIN_GHOST, WALL_BOX_BLOCK_GHOST = 0, 1, 2
+WALL_MAX_NB = 15
+WALL_INTO_BODY, WALL_OUT_OF_BODY = 1, 2
+
+
+class WallLevelGeom(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("center", ctypes.c_void_p), ("neib", ctypes.c_void_p),
+                ("kind", ctypes.c_void_p), ("distance_to_dm", ctypes.c_void_p),
+                ("nblock", ctypes.c_int64), ("block_in", ctypes.c_void_p),
+                ("block_out", ctypes.c_void_p)]
+
+
+class WallBodies(ctypes.Structure):
+    _fields_ = [("nbodies", ctypes.c_int), ("patch_start", ctypes.c_void_p),
+                ("pc", ctypes.c_void_p), ("nv", ctypes.c_void_p), ("nb_count", ctypes.c_void_p),
+                ("nb", ctypes.c_void_p), ("periodic_y", ctypes.c_int),
+                ("critic_ylength", ctypes.c_double), ("dm_length_y", ctypes.c_double)]
+
+
+class WallPairs(ctypes.Structure):
+    _fields_ = [("body", ctypes.c_void_p), ("patch", ctypes.c_void_p),
+                ("distance", ctypes.c_void_p), ("signdis", ctypes.c_void_p),
+                ("distance_to_body", ctypes.c_void_p), ("solid", ctypes.c_void_p),
+                ("moved", ctypes.c_void_p), ("block_moved", ctypes.c_void_p)]
 
 
 class Cells(ctypes.Structure):
@@ -413,6 +441,55 @@ class FlowSolver:
         _check(lib().ibgpu_build_interfaces(self._ctx, int(nlevels), ctypes.byref(cells),
                                             ctypes.byref(out)), "ibgpu_build_interfaces")
         return res, pro, ghost
+
+    def wall_geometry(self, levels):
+        """Boxes of every level for the device wall distances: a list of
+        dicts with center (n, 3), neib (n, 9), kind (n), distance_to_dm (n),
+        block_in, block_out (ibgpu_wall_geometry)."""
+        keep, geoms = [], []
+        for g in levels:
+            c = np.ascontiguousarray(g["center"], np.float64).reshape(-1, 3)
+            nb = np.ascontiguousarray(g["neib"], np.int32).reshape(-1, 9)
+            k = np.ascontiguousarray(g["kind"], np.uint8)
+            dm = np.ascontiguousarray(g["distance_to_dm"], np.float64)
+            bi = np.ascontiguousarray(g.get("block_in", []), np.int32)
+            bo = np.ascontiguousarray(g.get("block_out", []), np.int32)
+            keep += [c, nb, k, dm, bi, bo]
+            geoms.append(WallLevelGeom(len(c), c.ctypes.data, nb.ctypes.data, k.ctypes.data,
+                                       dm.ctypes.data, len(bi), bi.ctypes.data, bo.ctypes.data))
+        arr = (WallLevelGeom * max(len(geoms), 1))(*geoms)
+        _check(lib().ibgpu_wall_geometry(self._ctx, len(geoms), arr), "ibgpu_wall_geometry")
+
+    def wall_distance(self, bodies: dict, pairs):
+        """The bodies' patches (patch_start, pc (n, 3), nv (n, 3), nb_count,
+        nb (n, 15); periodic_y, critic_ylength, dm_length_y) and every
+        level's pairs (dicts of body, patch, distance, signdis,
+        distance_to_body, solid): updated in place, with moved and
+        block_moved added (ibgpu_wall_distance)."""
+        ps = np.ascontiguousarray(bodies["patch_start"], np.int32)
+        pc = np.ascontiguousarray(bodies["pc"], np.float64)
+        nv = np.ascontiguousarray(bodies["nv"], np.float64)
+        nbc = np.ascontiguousarray(bodies["nb_count"], np.int32)
+        nbl = np.ascontiguousarray(bodies["nb"], np.int32)
+        wb = WallBodies(len(ps) - 1, ps.ctypes.data, pc.ctypes.data, nv.ctypes.data,
+                        nbc.ctypes.data, nbl.ctypes.data, int(bodies.get("periodic_y", 0)),
+                        float(bodies.get("critic_ylength", 1e300)),
+                        float(bodies.get("dm_length_y", 0.0)))
+        arrs = []
+        for p in pairs:
+            for key, dt in (("body", np.int32), ("patch", np.int32), ("distance", np.float64),
+                            ("signdis", np.float64), ("distance_to_body", np.float64),
+                            ("solid", np.uint8)):
+                p[key] = np.ascontiguousarray(p[key], dt)
+            p["moved"] = np.zeros(len(p["body"]), np.uint8)
+            p["block_moved"] = np.zeros(int(p.get("nblock", 0)), np.uint8)
+            arrs.append(WallPairs(*(p[k].ctypes.data for k in (
+                "body", "patch", "distance", "signdis", "distance_to_body", "solid", "moved",
+                "block_moved"))))
+        arr = (WallPairs * max(len(arrs), 1))(*arrs)
+        _check(lib().ibgpu_wall_distance(self._ctx, ctypes.byref(wb), len(arrs), arr),
+               "ibgpu_wall_distance")
+        return pairs
 
     def upload_interfaces(self, res, pro):
         """Coarse/fine pairs as (n, 11) int arrays: level, cx, cy, 4 x (fx, fy)."""

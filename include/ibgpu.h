@@ -195,6 +195,73 @@ int ibgpu_upload_interfaces(ibgpu_ctx *ctx, const ibgpu_cf_pairs *pairs);
 int ibgpu_upload_boundaries(ibgpu_ctx *ctx, const ibgpu_bc *bc);
 int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib);
 
+/* ---------------------------------------------------------------------------
+ * Wall distances of moved bodies, on the device: the first part of the
+ * reference's re-immersion (Body::RenewLevelDistance, Bodymove.cpp:127-300),
+ * with the block-ghost copies of Mesh::SynNormal_BlockDistance
+ * (Mesh.cpp:2303-2374).  For every box of a level closer than 9.5 to a wall
+ * (and not a block ghost): the closest wall patch of its body by the
+ * reference's walk over neighbouring patches from the box's current patch
+ * (Body::FindClosePatchtoCell, Body.H:505-580), the hand-over to another
+ * body where a neighbour box is paired with it, the signed distance capped
+ * by the distance to the domain boundary, and the solid flag with the boxes
+ * that changed sides; then every block ghost takes its origin box's pair.
+ * The same IEEE operations in the same order as the reference (no
+ * contractions, correctly rounded roots): results equal the reference's bit
+ * for bit.  The geometry is uploaded after every regrid, the pairs go in and
+ * out with every call.
+ * ------------------------------------------------------------------------- */
+#define IBGPU_WALL_BOX_OTHER 0        /* normal cells and other ghosts */
+#define IBGPU_WALL_BOX_DOMAIN_GHOST 1 /* Boxtype Dmghost */
+#define IBGPU_WALL_BOX_BLOCK_GHOST 2  /* Boxtype Blockghost */
+#define IBGPU_WALL_MAX_NB 15          /* neighbours per wall patch (PatchNeib) */
+#define IBGPU_WALL_INTO_BODY 1        /* the box joined the body (solid)      */
+#define IBGPU_WALL_OUT_OF_BODY 2      /* the box left it                       */
+
+typedef struct ibgpu_wall_level_geom {
+  int64_t n;                    /* boxes of the level, in its array order    */
+  const double *center;         /* 3 per box (Meshlevel m_geom boxcenter)    */
+  const int32_t *neib;          /* 9 per box: Box::neib[i][j][1], i-major    */
+  const uint8_t *kind;          /* IBGPU_WALL_BOX_*                          */
+  const double *distance_to_dm; /* BoxtoWall::distance_to_dm                 */
+  int64_t nblock;               /* block pairs (Meshlevel blockpair)         */
+  const int32_t *block_in;      /* origin box of pair k (innode)             */
+  const int32_t *block_out;     /* block ghost of pair k (outnode.index)     */
+} ibgpu_wall_level_geom;
+
+/* After every regrid: the boxes of every level.  IBGPU_E_ARG when a block
+ * ghost is the target of two pairs or the origin of one. */
+int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom *levels);
+
+typedef struct ibgpu_wall_bodies {
+  int nbodies;
+  const int32_t *patch_start; /* nbodies + 1: body b's patches are rows
+                                 patch_start[b] .. patch_start[b+1]-1       */
+  const double *pc;           /* 3 per patch row: centre                    */
+  const double *nv;           /* 3 per patch row: unit outward normal       */
+  const int32_t *nb_count;    /* per patch row                              */
+  const int32_t *nb;          /* IBGPU_WALL_MAX_NB per patch row: the body's
+                                 neighbouring patches (indices within the body) */
+  int periodic_y;             /* PeriodicLength (mpiparams.cpp:294-310)     */
+  double critic_ylength, dm_length_y;
+} ibgpu_wall_bodies;
+
+typedef struct ibgpu_wall_pairs {  /* one level; in and out (BoxtoWall, Box::solid) */
+  int32_t *body, *patch;
+  double *distance, *signdis, *distance_to_body;
+  uint8_t *solid;
+  uint8_t *moved;        /* out, per box: IBGPU_WALL_INTO_BODY / _OUT_OF_BODY / 0,
+                            the reference's move lists of its distance loop */
+  uint8_t *block_moved;  /* out, per block pair: the same for block_out[k] */
+} ibgpu_wall_pairs;
+
+/* The bodies where they are now and every level's pairs as the last move
+ * left them; on return the new pairs.  IBGPU_E_ABORT when a box within 9.5
+ * of a wall has no valid body or patch (the reference's assertion,
+ * Bodymove.cpp:146-147), IBGPU_E_STATE before ibgpu_wall_geometry. */
+int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
+                        ibgpu_wall_pairs *pairs);
+
 /* Wall force and moment of every body from the current state
  * (Body::ComptWallForce): out[6*b + 0..2] force, out[6*b + 3..5] moment,
  * in the reference's dimensional scaling. */

@@ -537,7 +537,12 @@ int main(int argc, char **argv) {
     std::exit(3);
   };
   if (gpu_step) {
-    // IB_BINDING_PRECISION: IBGPU_FP64 (default), IBGPU_FP64_EXACT or IBGPU_MIXED
+    // IB_BINDING_PRECISION: IBGPU_FP64 (default), IBGPU_FP64_EXACT or IBGPU_MIXED;
+    // IB_BINDING_DEVICE_DISTANCE=0: the reference's own wall-distance passes
+    // for moving bodies (default: the device's); IB_BINDING_DISTCHECK=1: both,
+    // the boxes that differ counted
+    flowsolver.SetDeviceWallDistances(env_int("IB_BINDING_DEVICE_DISTANCE", 1) != 0,
+                                      env_int("IB_BINDING_DISTCHECK", 0) != 0);
     gpu_check(flowsolver.Create(kLimiter, env_int("IB_BINDING_PRECISION", IBGPU_FP64)),
               "ibgpu_create");
     gpu_check(flowsolver.Upload(amr, sphere), "upload");
@@ -657,8 +662,9 @@ int main(int argc, char **argv) {
     char buf[256];
     std::snprintf(buf, sizeof buf,
                   "{\"forces\": %.6f, \"motion\": %.6f, \"distance\": %.6f, \"sync\": %.6f, "
-                  "\"ibcells\": %.6f, \"upload\": %.6f}",
-                  mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload);
+                  "\"ibcells\": %.6f, \"upload\": %.6f, \"distcheck_mismatches\": %lld}",
+                  mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload,
+                  ibgpu_wall_check_mismatches());
     phases = buf;
   }
 #endif

@@ -22,6 +22,7 @@ immersed-boundary records through ibgpu_upload_ib.
 * the same loop in the reference's shared-memory MPI mode (4 ranks, rank 0
   on the device): the 1-rank history.
 """
+import json
 import os
 import subprocess
 import sys
@@ -171,3 +172,25 @@ def test_binding_in_the_references_mpi_mode(cuda_lib):
     assert np.abs(one[:, 2] - four[:, 2]).max() <= 1e-12 * np.abs(one[:, 2]).max()
     f1, f4 = one[:, 3:], four[:, 3:]
     assert np.abs(f1 - f4).max() <= 1e-10 * F_REF
+
+
+@pytest.mark.skipif(not os.path.exists(BINARY), reason="binding oracle not built (make -C oracle)")
+@pytest.mark.parametrize("ranks", [1, 4])
+def test_device_wall_distances_equal_the_references_passes(cuda_lib, ranks):
+    """Every step of 25 (a regrid at 20) the device wall-distance passes
+    (ibgpu_wall_distance) from the same pairs as the reference's own
+    RenewLevelDistance and SynNormal_BlockDistance: every box's pair and
+    solid flag bit for bit and the move lists entry for entry, on each rank's
+    share."""
+    env = dict(os.environ)
+    env.update(make_golden.PITCH_ENV)
+    work = tempfile.mkdtemp(prefix="pitch_distcheck_")
+    env.update(IB_STEPS="25", IB_BINDING_STEP="1", IB_BINDING_DISTCHECK="1",
+               IB_RANKS=str(ranks), IB_MPI_TIMEOUT="300")
+    out = subprocess.run([BINARY], cwd=work, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    res = next(json.loads(l.split(" ", 1)[1]) for l in out.stdout.splitlines()
+               if l.startswith("ORACLE_RESULT"))
+    assert res["ranks"] == ranks
+    assert res["move_phases_seconds"]["distcheck_mismatches"] == 0

@@ -1,0 +1,72 @@
+"""Wall distances of moved bodies on the device (ibgpu_wall_geometry /
+ibgpu_wall_distance, csrc/wall.cu) against the CPU restatement of the
+reference's passes (oracle/wall_oracle.py: Body::RenewLevelDistance,
+Bodymove.cpp:127-300, with Mesh::SynNormal_BlockDistance's block pairs) on
+seeded synthetic bodies and boxes, bit for bit: pairs, signed distances,
+solid flags and the move lists' entries.  Against the reference itself the
+same device passes are compared at every step of a pitching run through the
+binding (tests/test_gpu_pitch.py)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                "oracle"))
+import wall_oracle as wo  # noqa: E402
+from conftest import load_pkg  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+wl = load_pkg().workloads
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint64) if a.dtype == np.float64 else a
+
+
+@pytest.mark.parametrize("seed,turn", [(0, 0.02), (3, 0.25), (5, 0.6)])
+def test_device_passes_equal_the_reference_restatement(cuda_lib, pkg, seed, turn):
+    bodies, geom, pairs = wo.synthetic_case(seed=seed, turn=turn)
+    ref = wo.wall_distance(bodies, geom, pairs)
+    P, cells, prim = wl.vortex_case(32)
+    sol = pkg.ibgpu.FlowSolver(P)
+    # two levels: the same boxes twice, the second with no block pairs
+    g2 = dict(geom, block_in=[], block_out=[])
+    sol.wall_geometry([geom, g2])
+    p1 = {k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+    p1["nblock"] = pairs["nblock"]
+    p2 = {k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+    got = sol.wall_distance(bodies, [p1, p2])
+    for k in ("body", "patch", "distance", "signdis", "distance_to_body", "solid", "moved",
+              "block_moved"):
+        assert np.array_equal(bits(got[0][k]), bits(ref[k])), k
+    ref2 = wo.wall_distance(bodies, g2, pairs)
+    for k in ("body", "patch", "distance", "signdis", "solid", "moved"):
+        assert np.array_equal(bits(got[1][k]), bits(ref2[k])), k
+    assert (got[0]["moved"] > 0).any()
+    sol.close()
+
+
+def test_invalid_pairs_and_geometry_are_reported(cuda_lib, pkg):
+    ib = pkg.ibgpu
+    bodies, geom, pairs = wo.synthetic_case(seed=1)
+    P, cells, prim = wl.vortex_case(32)
+    sol = ib.FlowSolver(P)
+    p = {k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance(bodies, [p])  # before the geometry
+    assert e.value.code == ib.E_STATE
+    bad = dict(geom, block_in=np.r_[geom["block_in"], geom["block_in"][:1]],
+               block_out=np.r_[geom["block_out"], geom["block_out"][:1]])
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_geometry([bad])  # a block ghost targeted twice
+    assert e.value.code == ib.E_ARG
+    sol.wall_geometry([geom])
+    p["body"][np.flatnonzero(p["signdis"] < 1.0)[0]] = 7  # no such body
+    p["nblock"] = pairs["nblock"]
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance(bodies, [p])
+    assert e.value.code == ib.E_ABORT
+    sol.close()
