@@ -64,6 +64,9 @@ struct IbgpuLists {
 // flags and records (UploadImmersion).
 struct IbgpuMoveTimes {
   double forces = 0.0, motion = 0.0, distance = 0.0, sync = 0.0, ibcells = 0.0, upload = 0.0;
+  // the device wall distances' parts (within distance): packing this rank's
+  // share, the device rank's call, unpacking
+  double wall_pack = 0.0, wall_device = 0.0, wall_unpack = 0.0;
 };
 inline IbgpuMoveTimes &ibgpu_move_times() {
   static IbgpuMoveTimes t;
@@ -81,11 +84,12 @@ inline int ibgpu_share_status(int rc) {
 
 // A byte buffer shared by the ranks of the node: a shared window on
 // share_comm, all of it held by rank 0 (collective allocation and release).
+// With pin the device rank pins it for its transfers (ibgpu_host_register).
 struct IbgpuSharedBytes {
   MPI_Win win;
   char *base = nullptr;
-  bool live = false;
-  void alloc(size_t nbytes) {
+  bool live = false, pinned = false;
+  void alloc(size_t nbytes, bool pin) {
     release();
     char *local = nullptr;
     MPI_Win_allocate_shared(srank == 0 ? (MPI_Aint)nbytes : 0, 1, MPI_INFO_NULL, share_comm,
@@ -94,10 +98,12 @@ struct IbgpuSharedBytes {
     int du;
     MPI_Win_shared_query(win, 0, &sz, &du, &base);
     live = true;
+    pinned = pin && srank == 0 && nbytes > 0 && ibgpu_host_register(base, nbytes) == IBGPU_OK;
   }
   void release() {
+    if (pinned) ibgpu_host_unregister(base);
     if (live) MPI_Win_free(&win);
-    live = false;
+    live = pinned = false;
     base = nullptr;
   }
 };
@@ -126,7 +132,7 @@ struct IbgpuWallLevel {
                  otb = take(8 * n), one = take(36 * n), obo = take(4 * n), opa = take(4 * n),
                  obi = take(4 * nblock), obu = take(4 * nblock), oki = take(n), oso = take(n),
                  omo = take(n), obm = take(nblock);
-    mem.alloc(off);
+    mem.alloc(off, true);
     char *b = mem.base;
     center = (double *)(b + oc);
     dtdm = (double *)(b + odm);
@@ -509,6 +515,8 @@ struct IbgpuAdapter {
                            std::vector<std::vector<int> > &out_to_in) {
     const int nlev = amesh.MyCurNum();
     if ((int)W.size() != nlev) return IBGPU_E_STATE;
+    IbgpuMoveTimes &tm = ibgpu_move_times();
+    double t0 = MPI_Wtime();
     for (int l = 0; l < nlev; ++l) {
       DataArray<Box> &boxes = amesh.ShowLevelBox(l);
       IbgpuWallLevel &L = W[l];
@@ -525,6 +533,9 @@ struct IbgpuAdapter {
       }
     }
     MPI_Barrier(share_comm);
+    double t1 = MPI_Wtime();
+    tm.wall_pack += t1 - t0;
+    t0 = t1;
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       // the bodies' wall patches where they are now (small: the device rank alone)
@@ -559,6 +570,9 @@ struct IbgpuAdapter {
     }
     rc = ibgpu_share_status(rc);
     MPI_Barrier(share_comm);
+    t1 = MPI_Wtime();
+    tm.wall_device += t1 - t0;
+    t0 = t1;
     if (rc != IBGPU_OK || !apply) return rc;
     for (int l = 0; l < nlev; ++l) {
       DataArray<Box> &boxes = amesh.ShowLevelBox(l);
@@ -583,6 +597,7 @@ struct IbgpuAdapter {
       }
     }
     MPI_Barrier(share_comm);  // every box written before the reference's next loops
+    tm.wall_unpack += MPI_Wtime() - t0;
     return IBGPU_OK;
   }
 

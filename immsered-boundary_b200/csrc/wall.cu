@@ -301,6 +301,18 @@ unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
 extern "C" {
 
+int ibgpu_host_register(void *ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return IBGPU_E_ARG;
+  WK(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return IBGPU_OK;
+}
+
+int ibgpu_host_unregister(void *ptr) {
+  if (!ptr) return IBGPU_E_ARG;
+  WK(cudaHostUnregister(ptr));
+  return IBGPU_OK;
+}
+
 int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom *levels) {
   CtxView V;
   if (!ctx || nlevels < 0 || (nlevels > 0 && !levels) || ctx_view(ctx, &V) != IBGPU_OK)

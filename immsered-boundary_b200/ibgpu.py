@@ -41,7 +41,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
            "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
            "ibgpu_set_state_rows", "ibgpu_build_interfaces", "ibgpu_wall_geometry",
-           "ibgpu_wall_distance")
+           "ibgpu_wall_distance", "ibgpu_host_register", "ibgpu_host_unregister")
 ROWS_FLOWVARS, ROWS_COMPACT = 7, 4
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16

@@ -255,6 +255,13 @@ typedef struct ibgpu_wall_pairs {  /* one level; in and out (BoxtoWall, Box::sol
   uint8_t *block_moved;  /* out, per block pair: the same for block_out[k] */
 } ibgpu_wall_pairs;
 
+/* Pin (and release) a host buffer that ibgpu calls copy from or to, e.g. the
+ * shared windows the binding exchanges wall distances through
+ * (cudaHostRegister / cudaHostUnregister on the current device): its
+ * transfers then run at the bus rate instead of through staging. */
+int ibgpu_host_register(void *ptr, size_t bytes);
+int ibgpu_host_unregister(void *ptr);
+
 /* The bodies where they are now and every level's pairs as the last move
  * left them; on return the new pairs.  IBGPU_E_ABORT when a box within 9.5
  * of a wall has no valid body or patch (the reference's assertion,

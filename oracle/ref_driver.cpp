@@ -659,12 +659,13 @@ int main(int argc, char **argv) {
   {
     // moving-body phases on rank 0, all steps (warm-up included)
     const IbgpuMoveTimes &mt = ibgpu_move_times();
-    char buf[256];
+    char buf[512];
     std::snprintf(buf, sizeof buf,
                   "{\"forces\": %.6f, \"motion\": %.6f, \"distance\": %.6f, \"sync\": %.6f, "
-                  "\"ibcells\": %.6f, \"upload\": %.6f, \"distcheck_mismatches\": %lld}",
-                  mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload,
-                  ibgpu_wall_check_mismatches());
+                  "\"ibcells\": %.6f, \"upload\": %.6f, \"wall_pack\": %.6f, "
+                  "\"wall_device\": %.6f, \"wall_unpack\": %.6f, \"distcheck_mismatches\": %lld}",
+                  mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload, mt.wall_pack,
+                  mt.wall_device, mt.wall_unpack, ibgpu_wall_check_mismatches());
     phases = buf;
   }
 #endif
