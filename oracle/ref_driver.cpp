@@ -22,7 +22,8 @@
 // step counts IB_DUMP_AT lists), IB_FORCES=1 (static
 // body: compute wall forces each step, Body::ComptWallForce), IB_FORCE_LOG=<file>
 // (the per-step force history), IB_RANKS=N (the reference's shared-memory
-// mode with N ranks on one node; the shim in mpi_shim/ forks them).
+// mode with N ranks on one node; the shim in mpi_shim/ forks them),
+// IB_PLT=<prefix> (the reference's Tecplot solution file of the final state).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -654,6 +655,15 @@ int main(int argc, char **argv) {
     if (prefix && dump_now(ts, s == nsteps - 1)) do_dump(ts);
   }
   if (flog) std::fclose(flog);
+  // IB_PLT=<prefix>: the reference's own Tecplot solution writer
+  // (Pltoutput::Output_Soln_Nobody, <prefix>-<ts>.plt) on the final state,
+  // read back from the device first when the binding steps
+  if (const char *plt = std::getenv("IB_PLT")) {
+#ifdef ORACLE_BINDING
+    if (gpu_step) gpu_check(flowsolver.Download(), "download");
+#endif
+    pltfile.Output_Soln_Nobody(plt);
+  }
   std::string phases = "{}";
 #ifdef ORACLE_BINDING
   {
