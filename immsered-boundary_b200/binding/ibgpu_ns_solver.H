@@ -27,6 +27,7 @@
 #pragma once
 
 #include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -509,15 +510,18 @@ struct IbgpuAdapter {
   // apply the boxes take the new pairs and solid flags and this rank's move
   // lists get the boxes of its shares that changed sides, in the order the
   // reference's loops would push them; without, the results stay in W.
+  // With resident the device starts from the pairs it kept from its
+  // previous call (nothing but these passes changes the pairs between
+  // regrids) and no rank packs.
   static int WallDistances(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody,
-                           std::vector<IbgpuWallLevel> &W, bool apply,
+                           std::vector<IbgpuWallLevel> &W, bool apply, bool resident,
                            std::vector<std::vector<int> > &in_to_out,
                            std::vector<std::vector<int> > &out_to_in) {
     const int nlev = amesh.MyCurNum();
     if ((int)W.size() != nlev) return IBGPU_E_STATE;
     IbgpuMoveTimes &tm = ibgpu_move_times();
     double t0 = MPI_Wtime();
-    for (int l = 0; l < nlev; ++l) {
+    for (int l = 0; l < nlev && !resident; ++l) {
       DataArray<Box> &boxes = amesh.ShowLevelBox(l);
       IbgpuWallLevel &L = W[l];
       int bs, be;
@@ -565,7 +569,7 @@ struct IbgpuAdapter {
           pr[l] = ibgpu_wall_pairs{L.body, L.patch, L.dist, L.sd, L.dtb, L.solid, L.moved,
                                    L.block_moved};
         }
-        rc = ibgpu_wall_distance(ctx, &wb, nlev, pr.data());
+        rc = ibgpu_wall_distance(ctx, &wb, nlev, pr.data(), resident ? IBGPU_WALL_RESIDENT : 0);
       }
     }
     rc = ibgpu_share_status(rc);
@@ -574,13 +578,31 @@ struct IbgpuAdapter {
     tm.wall_device += t1 - t0;
     t0 = t1;
     if (rc != IBGPU_OK || !apply) return rc;
-    for (int l = 0; l < nlev; ++l) {
-      DataArray<Box> &boxes = amesh.ShowLevelBox(l);
+    WallUnpack(amesh, W, true, &in_to_out, &out_to_in);
+    tm.wall_unpack += MPI_Wtime() - t0;
+    return IBGPU_OK;
+  }
+
+  // The device's last wall-distance results (in W) into this rank's shares
+  // of the boxes.  With near only the boxes the re-immersion reads before
+  // the next move: within kWallNearCells cells of the level from a wall,
+  // or that changed sides; the others keep their previous pairs on the host
+  // (the device keeps them all) until a call without near, which Download
+  // makes before any output or regrid reads the mesh.  With move lists this
+  // rank's entries, in the order the reference's loops push them.
+  static constexpr double kWallNearCells = 10.0;
+  static void WallUnpack(Mesh &amesh, std::vector<IbgpuWallLevel> &W, bool near,
+                         std::vector<std::vector<int> > *in_to_out,
+                         std::vector<std::vector<int> > *out_to_in) {
+    for (size_t l = 0; l < W.size(); ++l) {
+      DataArray<Box> &boxes = amesh.ShowLevelBox((int)l);
       DataArray<NodePair> &bp = amesh.m_level[l].blockpair;
       IbgpuWallLevel &L = W[l];
+      const double band = near ? kWallNearCells * dh[l][0] : HUGE_VAL;
       int bs, be;
       boxes.GlobalOrder(bs, be);
       for (int i = bs; i < be; ++i) {
+        if (!(std::fabs(L.sd[i]) < band) && L.moved[i] == 0) continue;
         BoxtoWall &w = boxes[i].pair;
         w.body = L.body[i];
         w.patch = L.patch[i];
@@ -588,17 +610,18 @@ struct IbgpuAdapter {
         w.signdis = L.sd[i];
         w.distance_to_body = L.dtb[i];
         boxes[i].solid = L.solid[i] != 0;
-        if (L.moved[i] == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(i);
-        else if (L.moved[i] == IBGPU_WALL_OUT_OF_BODY) in_to_out[l].push_back(i);
+        if (!in_to_out) continue;
+        if (L.moved[i] == IBGPU_WALL_INTO_BODY) (*out_to_in)[l].push_back(i);
+        else if (L.moved[i] == IBGPU_WALL_OUT_OF_BODY) (*in_to_out)[l].push_back(i);
       }
+      if (!in_to_out) continue;
       for (int k = bp.ps(); k < bp.pe(); ++k) {
-        if (L.block_moved[k] == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(L.block_out[k]);
-        else if (L.block_moved[k] == IBGPU_WALL_OUT_OF_BODY) in_to_out[l].push_back(L.block_out[k]);
+        if (L.block_moved[k] == IBGPU_WALL_INTO_BODY) (*out_to_in)[l].push_back(L.block_out[k]);
+        else if (L.block_moved[k] == IBGPU_WALL_OUT_OF_BODY)
+          (*in_to_out)[l].push_back(L.block_out[k]);
       }
     }
     MPI_Barrier(share_comm);  // every box written before the reference's next loops
-    tm.wall_unpack += MPI_Wtime() - t0;
-    return IBGPU_OK;
   }
 
   // Boxes of this rank's shares whose pair, solid flag or move-list entries
@@ -651,7 +674,8 @@ struct IbgpuAdapter {
   // and block-ghost passes run on the device; with check also the
   // reference's own, the difference counted (ibgpu_wall_check_mismatches).
   static int MoveBodies(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody, double &dt00,
-                        std::vector<IbgpuWallLevel> *W = nullptr, bool check = false) {
+                        std::vector<IbgpuWallLevel> *W = nullptr, bool check = false,
+                        bool *resident = nullptr) {
     const int nlev = amesh.MyCurNum();
     const int last = nlev - 1;
     std::vector<std::vector<int> > in_to_out(nlev), out_to_in(nlev);
@@ -689,14 +713,16 @@ struct IbgpuAdapter {
     tm.motion += t1 - t0;
     t0 = t1;
     if (W && !check) {
-      const int rc = WallDistances(ctx, amesh, abody, *W, true, in_to_out, out_to_in);
+      const bool res = resident && *resident;
+      const int rc = WallDistances(ctx, amesh, abody, *W, true, res, in_to_out, out_to_in);
+      if (resident) *resident = rc == IBGPU_OK;
       if (rc) return rc;
       t1 = MPI_Wtime();
       tm.distance += t1 - t0;
       t0 = t1;
     } else {
       if (W) {  // the device's results first, from the same pairs
-        const int rc = WallDistances(ctx, amesh, abody, *W, false, in_to_out, out_to_in);
+        const int rc = WallDistances(ctx, amesh, abody, *W, false, false, in_to_out, out_to_in);
         if (rc) return rc;
       }
       for (int l = 0; l < nlev; ++l) Body::RenewLevelDistance(amesh, abody, l, in_to_out[l], out_to_in[l]);
@@ -788,8 +814,10 @@ class GpuNS_Solver : public NS_Solver {
       rc = IbgpuAdapter::Upload(ctx_, lists_);
     }
     rc = ibgpu_share_status(rc);
-    if (rc == IBGPU_OK && device_distance_ && Body::Bodynum() > 0)
+    if (rc == IBGPU_OK && device_distance_ && Body::Bodynum() > 0) {
       rc = IbgpuAdapter::WallGeometry(ctx_, a_mesh, wall_);
+      wall_resident_ = false;  // the regrid's own pairs go up with the next move
+    }
     if (rc == IBGPU_OK && sprocs > 1) {
       // every rank learns the cell rows (level, box index), to share the
       // per-row flag pass of UploadImmersion
@@ -817,7 +845,8 @@ class GpuNS_Solver : public NS_Solver {
     if (!created_) return IBGPU_E_STATE;
     dt00 += dt;
     int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00,
-                                      device_distance_ ? &wall_ : nullptr, wall_check_);
+                                      device_distance_ ? &wall_ : nullptr, wall_check_,
+                                      &wall_resident_);
     if (rc) return rc;
     dt00 = 0.0;
     const double t0 = MPI_Wtime();
@@ -891,9 +920,12 @@ class GpuNS_Solver : public NS_Solver {
   }
 
   // m_data <- the device state, for output, host-side forces or a regrid
-  // (every rank; the device rank writes the shared arrays).
+  // (every rank; the device rank writes the shared arrays), and every box's
+  // wall pair from the device wall distances.
   int Download() {
     if (!created_) return IBGPU_E_STATE;
+    if (wall_resident_)  // every box's pair from the device's last wall distances
+      IbgpuAdapter::WallUnpack(a_mesh, wall_, false, nullptr, nullptr);
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       std::vector<double> rows(lists_.prim.size());
@@ -943,6 +975,8 @@ class GpuNS_Solver : public NS_Solver {
   ibgpu_ctx *ctx_ = nullptr;  // the device rank's context
   bool created_ = false;      // on every rank once Create succeeded
   IbgpuLists lists_;          // the device rank's lists
-  bool device_distance_ = true, wall_check_ = false;
+  // wall_resident_: the device holds every level's wall pairs from a move
+  // since the last geometry upload (the exchange buffers hold them too)
+  bool device_distance_ = true, wall_check_ = false, wall_resident_ = false;
   std::vector<IbgpuWallLevel> wall_;  // exchange buffers of the device wall distances
 };

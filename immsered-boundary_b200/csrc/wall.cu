@@ -237,6 +237,23 @@ __global__ void block_kernel(LevelDev L) {
 struct Buf {
   void *p = nullptr;
   size_t bytes = 0;
+  Buf() = default;
+  Buf(const Buf &) = delete;
+  Buf &operator=(const Buf &) = delete;
+  Buf(Buf &&o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  Buf &operator=(Buf &&o) noexcept {
+    if (this != &o) {
+      cudaFree(p);
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~Buf() { cudaFree(p); }
   cudaError_t reserve(size_t b) {
     if (b <= bytes) return cudaSuccess;
@@ -260,6 +277,7 @@ struct Level {
 struct State {
   std::vector<Level> levels;
   Buf start, pc, nv, nbc, nb, err;
+  bool resident = false;  // every level's last results are its next inputs
 };
 
 }  // namespace wall
@@ -373,17 +391,24 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
   }
   WK(S->err.reserve(sizeof(int)));
   WK(cudaStreamSynchronize(st));
+  S->resident = false;
   return IBGPU_OK;
 }
 
 int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
-                        ibgpu_wall_pairs *pairs) {
+                        ibgpu_wall_pairs *pairs, int flags) {
   CtxView V;
-  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !pairs) || ctx_view(ctx, &V) != IBGPU_OK)
+  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !pairs) ||
+      (flags & ~IBGPU_WALL_RESIDENT) || ctx_view(ctx, &V) != IBGPU_OK)
     return IBGPU_E_ARG;
   State *S = static_cast<State *>(*ctx_wall_state(ctx));
   if (!S || (int)S->levels.size() != nlevels) {
     set_last_error("wall distances: upload the wall geometry of these levels first");
+    return IBGPU_E_STATE;
+  }
+  const bool resident = (flags & IBGPU_WALL_RESIDENT) != 0;
+  if (resident && !S->resident) {
+    set_last_error("wall distances: no pairs on the device since the geometry upload");
     return IBGPU_E_STATE;
   }
   const int nb = bodies->nbodies;
@@ -427,9 +452,11 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
     Level &L = S->levels[(size_t)l];
     ibgpu_wall_pairs &p = pairs[l];
     if (L.n == 0) continue;
-    if ((rc = put(L.body[0], p.body, L.n, st)) || (rc = put(L.patch[0], p.patch, L.n, st)) ||
-        (rc = put(L.dist[0], p.distance, L.n, st)) || (rc = put(L.sd[0], p.signdis, L.n, st)) ||
-        (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) || (rc = put(L.solid, p.solid, L.n, st)))
+    if (!resident &&
+        ((rc = put(L.body[0], p.body, L.n, st)) || (rc = put(L.patch[0], p.patch, L.n, st)) ||
+         (rc = put(L.dist[0], p.distance, L.n, st)) || (rc = put(L.sd[0], p.signdis, L.n, st)) ||
+         (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) ||
+         (rc = put(L.solid, p.solid, L.n, st))))
       return rc;
     LevelDev D;
     D.n = L.n;
@@ -475,10 +502,20 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
   WK(cudaMemcpyAsync(&herr, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   WK(cudaStreamSynchronize(st));
   if (herr) {
+    S->resident = false;
     set_last_error("wall distances: a box within 9.5 of a wall has no valid body or patch, "
                    "or a patch walk did not end");
     return IBGPU_E_ABORT;
   }
+  // the results are the next call's inputs (the solid flags are in place)
+  for (Level &L : S->levels) {
+    std::swap(L.body[0], L.body[2]);
+    std::swap(L.patch[0], L.patch[2]);
+    std::swap(L.dist[0], L.dist[2]);
+    std::swap(L.sd[0], L.sd[2]);
+    std::swap(L.dtb[0], L.dtb[2]);
+  }
+  S->resident = true;
   return IBGPU_OK;
 }
 

@@ -103,6 +103,7 @@ class InterfaceLists(ctypes.Structure):
 WALL_BOX_OTHER, WALL_BOX_DOMAIN_GHOST, WALL_BOX_BLOCK_GHOST = 0, 1, 2
 WALL_MAX_NB = 15
 WALL_INTO_BODY, WALL_OUT_OF_BODY = 1, 2
+WALL_RESIDENT = 1
 
 
 class WallLevelGeom(ctypes.Structure):
@@ -460,12 +461,14 @@ class FlowSolver:
         arr = (WallLevelGeom * max(len(geoms), 1))(*geoms)
         _check(lib().ibgpu_wall_geometry(self._ctx, len(geoms), arr), "ibgpu_wall_geometry")
 
-    def wall_distance(self, bodies: dict, pairs):
+    def wall_distance(self, bodies: dict, pairs, resident: bool = False):
         """The bodies' patches (patch_start, pc (n, 3), nv (n, 3), nb_count,
         nb (n, 15); periodic_y, critic_ylength, dm_length_y) and every
         level's pairs (dicts of body, patch, distance, signdis,
         distance_to_body, solid): updated in place, with moved and
-        block_moved added (ibgpu_wall_distance)."""
+        block_moved added (ibgpu_wall_distance).  resident: start from the
+        pairs the device kept from the previous call (the dicts' input
+        values are not read)."""
         ps = np.ascontiguousarray(bodies["patch_start"], np.int32)
         pc = np.ascontiguousarray(bodies["pc"], np.float64)
         nv = np.ascontiguousarray(bodies["nv"], np.float64)
@@ -487,7 +490,8 @@ class FlowSolver:
                 "body", "patch", "distance", "signdis", "distance_to_body", "solid", "moved",
                 "block_moved"))))
         arr = (WallPairs * max(len(arrs), 1))(*arrs)
-        _check(lib().ibgpu_wall_distance(self._ctx, ctypes.byref(wb), len(arrs), arr),
+        _check(lib().ibgpu_wall_distance(self._ctx, ctypes.byref(wb), len(arrs), arr,
+                                         WALL_RESIDENT if resident else 0),
                "ibgpu_wall_distance")
         return pairs
 

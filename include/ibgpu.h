@@ -263,11 +263,17 @@ int ibgpu_host_register(void *ptr, size_t bytes);
 int ibgpu_host_unregister(void *ptr);
 
 /* The bodies where they are now and every level's pairs as the last move
- * left them; on return the new pairs.  IBGPU_E_ABORT when a box within 9.5
- * of a wall has no valid body or patch (the reference's assertion,
- * Bodymove.cpp:146-147), IBGPU_E_STATE before ibgpu_wall_geometry. */
+ * left them; on return the new pairs.  The device keeps the new pairs: with
+ * IBGPU_WALL_RESIDENT in flags the call starts from them (the previous
+ * call's results) and reads none of the arrays, only writes them, which
+ * saves the upload when nothing else changed the pairs since.
+ * IBGPU_E_ABORT when a box within 9.5 of a wall has no valid body or patch
+ * (the reference's assertion, Bodymove.cpp:146-147); IBGPU_E_STATE before
+ * ibgpu_wall_geometry, or with IBGPU_WALL_RESIDENT before a first call
+ * after it. */
+#define IBGPU_WALL_RESIDENT 1
 int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
-                        ibgpu_wall_pairs *pairs);
+                        ibgpu_wall_pairs *pairs, int flags);
 
 /* Wall force and moment of every body from the current state
  * (Body::ComptWallForce): out[6*b + 0..2] force, out[6*b + 3..5] moment,

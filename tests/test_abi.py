@@ -50,7 +50,7 @@ def test_null_arguments_are_rejected_without_gpu(pkg):
     assert lib.ibgpu_batch_set_grid(None, 0) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_batch_table_bytes(None) == 0
     assert lib.ibgpu_wall_geometry(None, 0, None) == pkg.ibgpu.E_ARG
-    assert lib.ibgpu_wall_distance(None, None, 0, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_wall_distance(None, None, 0, None, 0) == pkg.ibgpu.E_ARG
 
 
 def test_ctypes_layouts_match_c(pkg, tmp_path):

@@ -49,6 +49,32 @@ def test_device_passes_equal_the_reference_restatement(cuda_lib, pkg, seed, turn
     sol.close()
 
 
+def test_resident_pairs_continue_from_the_previous_call(cuda_lib, pkg):
+    """Two moves: the second starts from the pairs the device kept (its
+    input arrays hold garbage) and equals the restatement applied twice."""
+    bodies1, geom, pairs = wo.synthetic_case(seed=4, turn=0.05)
+    bodies2, _, _ = wo.synthetic_case(seed=4, turn=0.15)
+    ref1 = wo.wall_distance(bodies1, geom, pairs)
+    ref2 = wo.wall_distance(bodies2, geom, dict(ref1, nblock=pairs["nblock"]))
+    P, cells, prim = wl.vortex_case(32)
+    ib = pkg.ibgpu
+    sol = ib.FlowSolver(P)
+    sol.wall_geometry([geom])
+    p = {k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+    p["nblock"] = pairs["nblock"]
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance(bodies1, [dict(p)], resident=True)  # nothing kept yet
+    assert e.value.code == ib.E_STATE
+    sol.wall_distance(bodies1, [p])
+    for k in ("body", "patch", "distance", "signdis"):
+        p[k] = np.full_like(p[k], -7)
+    got = sol.wall_distance(bodies2, [p], resident=True)[0]
+    for k in ("body", "patch", "distance", "signdis", "distance_to_body", "solid", "moved",
+              "block_moved"):
+        assert np.array_equal(bits(got[k]), bits(ref2[k])), k
+    sol.close()
+
+
 def test_invalid_pairs_and_geometry_are_reported(cuda_lib, pkg):
     ib = pkg.ibgpu
     bodies, geom, pairs = wo.synthetic_case(seed=1)
