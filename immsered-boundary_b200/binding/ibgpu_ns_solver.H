@@ -26,6 +26,7 @@
 // broadcast to the node.  One node: the device context holds the whole mesh.
 #pragma once
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdint>
@@ -120,6 +121,10 @@ struct IbgpuWallLevel {
   int32_t *neib = nullptr, *body = nullptr, *patch = nullptr, *block_in = nullptr,
           *block_out = nullptr;
   uint8_t *kind = nullptr, *solid = nullptr, *moved = nullptr, *block_moved = nullptr;
+  // the near-wall report of a move from the pairs the device kept
+  // (ibgpu_wall_distance_near): its entries, in box order, and their number
+  ibgpu_wall_change *changes = nullptr;
+  int64_t *nchanges = nullptr;
   void layout(int64_t n_, int64_t nb_) {
     n = n_;
     nblock = nb_;
@@ -132,7 +137,8 @@ struct IbgpuWallLevel {
     const size_t oc = take(24 * n), odm = take(8 * n), odi = take(8 * n), osd = take(8 * n),
                  otb = take(8 * n), one = take(36 * n), obo = take(4 * n), opa = take(4 * n),
                  obi = take(4 * nblock), obu = take(4 * nblock), oki = take(n), oso = take(n),
-                 omo = take(n), obm = take(nblock);
+                 omo = take(n), obm = take(nblock), och = take(sizeof(ibgpu_wall_change) * n),
+                 onc = take(sizeof(int64_t));
     mem.alloc(off, true);
     char *b = mem.base;
     center = (double *)(b + oc);
@@ -149,6 +155,8 @@ struct IbgpuWallLevel {
     solid = (uint8_t *)(b + oso);
     moved = (uint8_t *)(b + omo);
     block_moved = (uint8_t *)(b + obm);
+    changes = (ibgpu_wall_change *)(b + och);
+    nchanges = (int64_t *)(b + onc);
   }
 };
 
@@ -512,7 +520,10 @@ struct IbgpuAdapter {
   // reference's loops would push them; without, the results stay in W.
   // With resident the device starts from the pairs it kept from its
   // previous call (nothing but these passes changes the pairs between
-  // regrids) and no rank packs.
+  // regrids) and no rank packs; applied, it then reports only the boxes
+  // near a wall before or after the move or on the other side now
+  // (ibgpu_wall_distance_near, kWallNearCells cells of each level), the
+  // boxes the reference's re-immersion reads before the next move.
   static int WallDistances(ibgpu_ctx *ctx, Mesh &amesh, std::vector<Body> &abody,
                            std::vector<IbgpuWallLevel> &W, bool apply, bool resident,
                            std::vector<std::vector<int> > &in_to_out,
@@ -563,13 +574,24 @@ struct IbgpuAdapter {
         const ibgpu_wall_bodies wb = {nb, start.data(), pc.data(), nv.data(), nbc.data(),
                                       nbl.data(), periodic[1] ? 1 : 0, critic_ylength,
                                       dmlength[1]};
-        std::vector<ibgpu_wall_pairs> pr(nlev);
-        for (int l = 0; l < nlev; ++l) {
-          IbgpuWallLevel &L = W[l];
-          pr[l] = ibgpu_wall_pairs{L.body, L.patch, L.dist, L.sd, L.dtb, L.solid, L.moved,
-                                   L.block_moved};
+        if (resident && apply) {
+          std::vector<ibgpu_wall_near> near(nlev);
+          for (int l = 0; l < nlev; ++l) {
+            IbgpuWallLevel &L = W[l];
+            near[l] = ibgpu_wall_near{kWallNearCells * dh[l][0], L.n, L.changes, 0,
+                                      L.block_moved};
+          }
+          rc = ibgpu_wall_distance_near(ctx, &wb, nlev, near.data());
+          for (int l = 0; l < nlev; ++l) *W[l].nchanges = near[l].count;
+        } else {
+          std::vector<ibgpu_wall_pairs> pr(nlev);
+          for (int l = 0; l < nlev; ++l) {
+            IbgpuWallLevel &L = W[l];
+            pr[l] = ibgpu_wall_pairs{L.body, L.patch, L.dist, L.sd, L.dtb, L.solid, L.moved,
+                                     L.block_moved};
+          }
+          rc = ibgpu_wall_distance(ctx, &wb, nlev, pr.data(), resident ? IBGPU_WALL_RESIDENT : 0);
         }
-        rc = ibgpu_wall_distance(ctx, &wb, nlev, pr.data(), resident ? IBGPU_WALL_RESIDENT : 0);
       }
     }
     rc = ibgpu_share_status(rc);
@@ -578,9 +600,48 @@ struct IbgpuAdapter {
     tm.wall_device += t1 - t0;
     t0 = t1;
     if (rc != IBGPU_OK || !apply) return rc;
-    WallUnpack(amesh, W, true, &in_to_out, &out_to_in);
+    if (resident) WallUnpackNear(amesh, W, in_to_out, out_to_in);
+    else WallUnpack(amesh, W, true, &in_to_out, &out_to_in);
     tm.wall_unpack += MPI_Wtime() - t0;
     return IBGPU_OK;
+  }
+
+  // The near-wall report of the last move into this rank's shares of the
+  // boxes (the report is in box order, so a share is one run of it), with
+  // this rank's move-list entries in the order the reference's loops push
+  // them; the other boxes keep their previous pairs on the host until
+  // Download fetches every pair.
+  static void WallUnpackNear(Mesh &amesh, std::vector<IbgpuWallLevel> &W,
+                             std::vector<std::vector<int> > &in_to_out,
+                             std::vector<std::vector<int> > &out_to_in) {
+    for (size_t l = 0; l < W.size(); ++l) {
+      DataArray<Box> &boxes = amesh.ShowLevelBox((int)l);
+      DataArray<NodePair> &bp = amesh.m_level[l].blockpair;
+      IbgpuWallLevel &L = W[l];
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      const ibgpu_wall_change *c = L.changes, *end = L.changes + *L.nchanges;
+      c = std::lower_bound(c, end, bs,
+                           [](const ibgpu_wall_change &a, int box) { return a.box < box; });
+      for (; c != end && c->box < be; ++c) {
+        const int i = c->box;
+        BoxtoWall &w = boxes[i].pair;
+        w.body = c->body;
+        w.patch = c->patch;
+        w.distance = c->distance;
+        w.signdis = c->signdis;
+        w.distance_to_body = c->distance_to_body;
+        boxes[i].solid = c->solid != 0;
+        if (c->moved == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(i);
+        else if (c->moved == IBGPU_WALL_OUT_OF_BODY) in_to_out[l].push_back(i);
+      }
+      for (int k = bp.ps(); k < bp.pe(); ++k) {
+        if (L.block_moved[k] == IBGPU_WALL_INTO_BODY) out_to_in[l].push_back(L.block_out[k]);
+        else if (L.block_moved[k] == IBGPU_WALL_OUT_OF_BODY)
+          in_to_out[l].push_back(L.block_out[k]);
+      }
+    }
+    MPI_Barrier(share_comm);  // every box written before the reference's next loops
   }
 
   // The device's last wall-distance results (in W) into this rank's shares
@@ -924,8 +985,20 @@ class GpuNS_Solver : public NS_Solver {
   // wall pair from the device wall distances.
   int Download() {
     if (!created_) return IBGPU_E_STATE;
-    if (wall_resident_)  // every box's pair from the device's last wall distances
+    if (wall_resident_) {  // every box's pair from the device's last wall distances
+      int rc = IBGPU_OK;
+      if (ibgpu_device_rank()) {
+        std::vector<ibgpu_wall_pairs> pr(wall_.size());
+        for (size_t l = 0; l < wall_.size(); ++l) {
+          IbgpuWallLevel &L = wall_[l];
+          pr[l] = ibgpu_wall_pairs{L.body, L.patch, L.dist, L.sd, L.dtb, L.solid, nullptr,
+                                   nullptr};
+        }
+        rc = ibgpu_wall_fetch(ctx_, (int)pr.size(), pr.data());
+      }
+      if ((rc = ibgpu_share_status(rc))) return rc;
       IbgpuAdapter::WallUnpack(a_mesh, wall_, false, nullptr, nullptr);
+    }
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       std::vector<double> rows(lists_.prim.size());

@@ -96,16 +96,16 @@ struct ibgpu_ctx {
   std::vector<int> level_tile_begin, level_tile_count;  // per level
   std::vector<int64_t> level_normal_cells;
   std::vector<int32_t> h_slot_level, h_slot_ix, h_slot_iy;  // slot -> position (abort reports)
-  // the last topology upload on the host, for flag updates of the same list:
-  // each row's slot, its layout bits (PRESENT / NORMAL / ALIAS), the tile
-  // neighbour table
-  std::vector<int32_t> h_cell_slot, h_tile_nb;
-  std::vector<uint8_t> h_cell_layout;
   int32_t *d_tile_nb = nullptr, *d_tile_level = nullptr, *d_cell_slot = nullptr;
   int2 *d_tile_org = nullptr;      // (ix, iy) of each tile's first cell
   double *d_signdis = nullptr;     // per slot, after ibgpu_upload_signdis
   uint8_t *d_tags = nullptr;       // indicator output: per slot, then per cell row
   uint8_t *d_flags = nullptr, *d_cell_alias = nullptr, *d_tile_uniform = nullptr;
+  // ibgpu_update_flags on the device: each row's layout bits (PRESENT /
+  // NORMAL / ALIAS as uploaded), the rows' new flags, per-tile scratch and
+  // the first row whose layout bits changed
+  uint8_t *d_cell_layout = nullptr, *d_row_flags = nullptr, *d_tile_full = nullptr;
+  int *d_layout_err = nullptr;
 
   // state: step state (6 fields) + two stage buffers (4 fields each)
   double *d_s0[kStateFields] = {};
@@ -139,6 +139,9 @@ struct ibgpu_ctx {
   int32_t *d_pat_body = nullptr, *d_pat_intp = nullptr, *d_body_begin = nullptr;
   double *d_pat_f = nullptr, *d_pat_out = nullptr, *d_body_center = nullptr, *d_force = nullptr;
   int n_pat = 0, nbodies = 0;
+  // element capacities of the buffers ibgpu_upload_ib refills after every
+  // move (kept between calls, grown when short), by buffer member
+  std::map<const void *, size_t> cap;
 
   // kernel timing
   bool timing = false;
@@ -166,6 +169,7 @@ struct ibgpu_ctx {
     }
     bc_waves.clear();
     n_ib = n_pat = nbodies = 0;
+    cap.clear();
   }
 
   // slot of (level, x, y) with periodic wrap, -1 if absent
@@ -190,6 +194,12 @@ struct ibgpu_ctx {
     cudaFree(d_cell_alias);
     cudaFree(d_tile_uniform);
     d_tile_uniform = nullptr;
+    for (uint8_t **p : {&d_cell_layout, &d_row_flags, &d_tile_full}) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+    cudaFree(d_layout_err);
+    d_layout_err = nullptr;
     cudaFree(d_tile_org);
     cudaFree(d_signdis);
     cudaFree(d_tags);
@@ -316,6 +326,58 @@ int64_t ctx_slot_at(const ibgpu_ctx *ctx, int l, int ix, int iy) {
 }
 void **ctx_wall_state(ibgpu_ctx *ctx) { return &ctx->wall; }
 }  // namespace ibgpu
+
+namespace {
+
+// ibgpu_update_flags on the device, over the rows' new flags in `rows`:
+// the first row whose PRESENT / NORMAL / ALIAS bits differ from the
+// topology upload (atomicMin into *err, which starts at INT_MAX) ...
+__global__ void layout_check_kernel(const uint8_t *rows, const uint8_t *layout, int64_t n,
+                                    int *err) {
+  constexpr uint8_t kBits = CF_PRESENT | CF_NORMAL | IBGPU_CELL_ALIAS;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t lay = (uint8_t)((rows[c] & kBits) | (layout[c] & IBGPU_CELL_ALIAS));
+    if (lay != layout[c]) atomicMin(err, (int)c);
+  }
+}
+
+// ... each non-alias row's flags into its slot (the slots no row maps to
+// keep the zeros of the topology upload) ...
+__global__ void flags_scatter_kernel(const uint8_t *rows, const uint8_t *layout,
+                                     const int32_t *slot, int64_t n, uint8_t *flags) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    if (!(layout[c] & IBGPU_CELL_ALIAS)) flags[slot[c]] = rows[c] & 0x3f;
+}
+
+// ... which tiles hold only recovering leaf cells (one warp per tile, eight
+// slots per lane) ...
+__global__ void tile_full_kernel(const uint8_t *flags, int64_t ntiles, uint8_t *full) {
+  constexpr uint64_t kFull8 = 0x0101010101010101ull *
+                              (uint64_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM);
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (t >= ntiles) return;  // whole warps
+  const uint64_t w = reinterpret_cast<const uint64_t *>(flags + t * kTileCells)[threadIdx.x & 31];
+  const bool all = __all_sync(0xffffffffu, w == kFull8);
+  if ((threadIdx.x & 31) == 0) full[t] = all ? 1 : 0;
+}
+
+// ... and the uniform tiles: full, with four full side neighbours (as
+// uniform_tiles on the host).
+__global__ void tile_uniform_kernel(const uint8_t *full, const int32_t *nb, int64_t ntiles,
+                                    uint8_t *uniform) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  bool u = full[t] != 0;
+  for (int k = 1; k < 9 && u; k += 2) {
+    const int n = nb[t * 9 + k];
+    u = n >= 0 && full[n] != 0;
+  }
+  uniform[t] = u ? 1 : 0;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -568,6 +630,10 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       (rc = dev_alloc(&ctx->d_tile_org, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_cell_slot, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_cell_alias, (size_t)n)) ||
+      (rc = dev_alloc(&ctx->d_cell_layout, (size_t)n)) ||
+      (rc = dev_alloc(&ctx->d_row_flags, (size_t)n)) ||
+      (rc = dev_alloc(&ctx->d_tile_full, (size_t)ntiles)) ||
+      (rc = dev_alloc(&ctx->d_layout_err, (size_t)1)) ||
       (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)))
     return rc;
   for (int f = 0; f < kStateFields; ++f)
@@ -599,11 +665,14 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   if (ctx->d_vsd) CK(cudaMemsetAsync(ctx->d_vsd, 0, nslots * 8 * 8, st));
   CK(cudaStreamSynchronize(st));
   ctx->tilemap = std::move(tilemap);
-  ctx->h_cell_slot = std::move(cell_slot);
-  ctx->h_tile_nb = std::move(h_nb);
-  ctx->h_cell_layout.resize(n);
+  // each row's layout bits, against which ibgpu_update_flags checks new flags
+  std::vector<uint8_t> layout(n);
   for (int64_t c = 0; c < n; ++c)
-    ctx->h_cell_layout[c] = (cells->flags[c] & kLayoutBits) | (alias[c] ? IBGPU_CELL_ALIAS : 0);
+    layout[c] = (cells->flags[c] & kLayoutBits) | (alias[c] ? IBGPU_CELL_ALIAS : 0);
+  if (n > 0) {
+    CK(cudaMemcpyAsync(ctx->d_cell_layout, layout.data(), n, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  }
   ctx->h_flags_present.assign(nslots, 0);
   for (int64_t s = 0; s < nslots; ++s) ctx->h_flags_present[s] = (h_flags[s] & CF_PRESENT) ? 1 : 0;
   ctx->ncells = n;
@@ -621,22 +690,35 @@ int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
     g_last_error = "asynchronous steps pending: call ibgpu_step_result first";
     return IBGPU_E_STATE;
   }
-  std::vector<uint8_t> h_flags(ctx->nslots, 0);
-  for (int64_t c = 0; c < ctx->ncells; ++c) {
-    const uint8_t layout = (flags[c] & kLayoutBits) |
-                           (ctx->h_cell_layout[c] & IBGPU_CELL_ALIAS ? IBGPU_CELL_ALIAS : 0);
-    if (layout != ctx->h_cell_layout[c]) {
-      g_last_error = "a row changed its PRESENT, NORMAL or ALIAS bit: upload the topology";
-      return IBGPU_E_TOPOLOGY;
-    }
-    if (ctx->h_cell_layout[c] & IBGPU_CELL_ALIAS) continue;
-    h_flags[ctx->h_cell_slot[c]] = flags[c] & 0x3f;
-  }
-  std::vector<uint8_t> h_uniform = uniform_tiles(h_flags, ctx->h_tile_nb, ctx->ntiles);
+  const int64_t n = ctx->ncells, nt = ctx->ntiles;
+  if (n == 0) return IBGPU_OK;
   cudaStream_t st = ctx->stream;
-  CK(cudaMemcpyAsync(ctx->d_flags, h_flags.data(), ctx->nslots, cudaMemcpyHostToDevice, st));
-  if (ctx->ntiles > 0)
-    CK(cudaMemcpyAsync(ctx->d_tile_uniform, h_uniform.data(), ctx->ntiles, cudaMemcpyHostToDevice, st));
+  const int grid = 4 * ctx->nsm;
+  // the rows' flags and the layout check first: nothing changes on the
+  // device when a row's layout bits differ
+  const int big = INT32_MAX;
+  CK(cudaMemcpyAsync(ctx->d_row_flags, flags, n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_layout_err, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+  layout_check_kernel<<<grid, 256, 0, st>>>(ctx->d_row_flags, ctx->d_cell_layout, n,
+                                            ctx->d_layout_err);
+  CK(cudaGetLastError());
+  int bad = big;
+  CK(cudaMemcpyAsync(&bad, ctx->d_layout_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (bad != big) {
+    g_last_error = "a row changed its PRESENT, NORMAL or ALIAS bit: upload the topology";
+    return IBGPU_E_TOPOLOGY;
+  }
+  flags_scatter_kernel<<<grid, 256, 0, st>>>(ctx->d_row_flags, ctx->d_cell_layout,
+                                             ctx->d_cell_slot, n, ctx->d_flags);
+  if (nt > 0) {
+    tile_full_kernel<<<(unsigned)((nt * 32 + 255) / 256), 256, 0, st>>>(ctx->d_flags, nt,
+                                                                        ctx->d_tile_full);
+    tile_uniform_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(ctx->d_tile_full,
+                                                                      ctx->d_tile_nb, nt,
+                                                                      ctx->d_tile_uniform);
+  }
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   return IBGPU_OK;
 }
@@ -1803,6 +1885,28 @@ int upload_vec(T **dst, const std::vector<T> &v, cudaStream_t st) {
   return IBGPU_OK;
 }
 
+// A context buffer of at least n elements that stays between calls (freed
+// and allocated again only when it is too short).
+template <typename T>
+int keep_alloc(ibgpu_ctx *ctx, T **dst, size_t n) {
+  size_t &c = ctx->cap[dst];
+  if (*dst && n <= c) return IBGPU_OK;
+  cudaFree(*dst);
+  *dst = nullptr;
+  c = 0;
+  const int rc = dev_alloc(dst, n);
+  if (rc) return rc;
+  c = n > 0 ? n : 1;
+  return IBGPU_OK;
+}
+template <typename T>
+int keep_upload(ibgpu_ctx *ctx, T **dst, const std::vector<T> &v, cudaStream_t st) {
+  const int rc = keep_alloc(ctx, dst, v.size());
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1984,15 +2088,6 @@ int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib) {
     return IBGPU_E_ARG;
   }
   cudaStream_t st = ctx->stream;
-  CK(cudaStreamSynchronize(st));
-  for (int32_t **p : {&ctx->d_ib_cell, &ctx->d_ib_intp, &ctx->d_pat_body, &ctx->d_pat_intp, &ctx->d_body_begin}) {
-    cudaFree(*p);
-    *p = nullptr;
-  }
-  for (double **p : {&ctx->d_ib_f, &ctx->d_ib_out, &ctx->d_pat_f, &ctx->d_pat_out, &ctx->d_body_center, &ctx->d_force}) {
-    cudaFree(*p);
-    *p = nullptr;
-  }
   std::vector<int32_t> cell, intp, pbody, pintp, begin(ib->nbodies + 1, 0);
   for (int64_t i = 0; i < ib->ncells; ++i) {
     const int32_t *c = ib->cell + 18 * i;
@@ -2022,13 +2117,27 @@ int ibgpu_upload_ib(ibgpu_ctx *ctx, const ibgpu_ib *ib) {
   std::vector<double> cf(ib->cellf, ib->cellf + 16 * (size_t)ib->ncells);
   std::vector<double> pf(ib->patchf, ib->patchf + 19 * (size_t)ib->npatches);
   std::vector<double> bc(ib->body_center, ib->body_center + 3 * (size_t)ib->nbodies);
+  // the buffers stay between moves (the copies queue behind the last step's
+  // kernels on the same stream); when one has to grow, the work that may
+  // still read it finishes first
+  const size_t nf = 6 * (size_t)std::max(ib->nbodies, 1);
+  const std::pair<const void *, size_t> need[] = {
+      {&ctx->d_ib_cell, cell.size()},       {&ctx->d_ib_intp, intp.size()},
+      {&ctx->d_ib_f, cf.size()},            {&ctx->d_ib_out, 6 * cell.size()},
+      {&ctx->d_pat_body, pbody.size()},     {&ctx->d_pat_intp, pintp.size()},
+      {&ctx->d_pat_f, pf.size()},           {&ctx->d_pat_out, 12 * pbody.size()},
+      {&ctx->d_body_center, bc.size()},     {&ctx->d_body_begin, begin.size()},
+      {&ctx->d_force, nf}};
+  bool grows = false;
+  for (const auto &q : need) grows = grows || q.second > ctx->cap[q.first];
+  if (grows) CK(cudaStreamSynchronize(st));
   int e;
-  if ((e = upload_vec(&ctx->d_ib_cell, cell, st)) || (e = upload_vec(&ctx->d_ib_intp, intp, st)) ||
-      (e = upload_vec(&ctx->d_ib_f, cf, st)) || (e = dev_alloc(&ctx->d_ib_out, 6 * cell.size())) ||
-      (e = upload_vec(&ctx->d_pat_body, pbody, st)) || (e = upload_vec(&ctx->d_pat_intp, pintp, st)) ||
-      (e = upload_vec(&ctx->d_pat_f, pf, st)) || (e = dev_alloc(&ctx->d_pat_out, 12 * pbody.size())) ||
-      (e = upload_vec(&ctx->d_body_center, bc, st)) || (e = upload_vec(&ctx->d_body_begin, begin, st)) ||
-      (e = dev_alloc(&ctx->d_force, 6 * (size_t)std::max(ib->nbodies, 1))))
+  if ((e = keep_upload(ctx, &ctx->d_ib_cell, cell, st)) || (e = keep_upload(ctx, &ctx->d_ib_intp, intp, st)) ||
+      (e = keep_upload(ctx, &ctx->d_ib_f, cf, st)) || (e = keep_alloc(ctx, &ctx->d_ib_out, 6 * cell.size())) ||
+      (e = keep_upload(ctx, &ctx->d_pat_body, pbody, st)) || (e = keep_upload(ctx, &ctx->d_pat_intp, pintp, st)) ||
+      (e = keep_upload(ctx, &ctx->d_pat_f, pf, st)) || (e = keep_alloc(ctx, &ctx->d_pat_out, 12 * pbody.size())) ||
+      (e = keep_upload(ctx, &ctx->d_body_center, bc, st)) || (e = keep_upload(ctx, &ctx->d_body_begin, begin, st)) ||
+      (e = keep_alloc(ctx, &ctx->d_force, nf)))
     return e;
   ctx->n_ib = (int)cell.size();
   ctx->n_pat = (int)pbody.size();

@@ -231,6 +231,80 @@ __global__ void block_kernel(LevelDev L) {
   L.block_moved[k] = mv;
 }
 
+// The boxes a host re-immersion reads (ibgpu_wall_distance_near): near a
+// wall before or after the move, or on the other side now; compacted in box
+// order (per-block counts, one exclusive scan, a ranked write).
+__device__ __forceinline__ bool near_box(const LevelDev &L, int64_t i, double band) {
+  return L.moved[i] != 0 || fabs(L.sd2[i]) < band || fabs(L.sd0[i]) < band;
+}
+
+constexpr int kNearBlock = 256;
+
+__global__ void near_count_kernel(LevelDev L, double band, int *block_count) {
+  const int64_t i = blockIdx.x * (int64_t)kNearBlock + threadIdx.x;
+  const int c = __syncthreads_count(i < L.n && near_box(L, i, band));
+  if (threadIdx.x == 0) block_count[blockIdx.x] = c;
+}
+
+// one block of 1024 threads: block_count[] becomes its exclusive prefix
+// sums, *total the sum
+__global__ void near_scan_kernel(int *block_count, int nb, int *total) {
+  __shared__ int wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int carry = 0;
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? block_count[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    if (i < nb) block_count[i] = carry + (warp > 0 ? wsum[warp - 1] : 0) + x - v;
+    carry += wsum[31];
+    __syncthreads();  // wsum is rewritten by the next chunk
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void near_write_kernel(LevelDev L, double band, const int *block_base,
+                                  ibgpu_wall_change *out) {
+  __shared__ int wcount[kNearBlock / 32];
+  const int64_t i = blockIdx.x * (int64_t)kNearBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool f = i < L.n && near_box(L, i, band);
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) wcount[warp] = __popc(m);
+  __syncthreads();
+  if (!f) return;
+  int pos = block_base[blockIdx.x] + __popc(m & ((1u << lane) - 1u));
+  for (int w = 0; w < warp; ++w) pos += wcount[w];
+  ibgpu_wall_change c;
+  c.box = (int32_t)i;
+  c.body = L.body2[i];
+  c.patch = L.patch2[i];
+  c.solid = L.solid[i];
+  c.moved = L.moved[i];
+  c.pad_[0] = c.pad_[1] = 0;
+  c.distance = L.dist2[i];
+  c.signdis = L.sd2[i];
+  c.distance_to_body = L.dtb2[i];
+  out[pos] = c;
+}
+
 // ---------------------------------------------------------------------------
 // host side
 
@@ -272,11 +346,12 @@ struct Level {
   int64_t n = 0, nblock = 0;
   Buf center, dtdm, neib, kind, block_in, block_out;
   Buf body[3], patch[3], dist[3], sd[3], dtb[3], solid, moved, block_moved;
+  Buf block_count, changes;  // near-wall output (ibgpu_wall_distance_near)
 };
 
 struct State {
   std::vector<Level> levels;
-  Buf start, pc, nv, nbc, nb, err;
+  Buf start, pc, nv, nbc, nb, err, totals;
   bool resident = false;  // every level's last results are its next inputs
 };
 
@@ -395,22 +470,12 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
   return IBGPU_OK;
 }
 
-int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
-                        ibgpu_wall_pairs *pairs, int flags) {
-  CtxView V;
-  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !pairs) ||
-      (flags & ~IBGPU_WALL_RESIDENT) || ctx_view(ctx, &V) != IBGPU_OK)
-    return IBGPU_E_ARG;
-  State *S = static_cast<State *>(*ctx_wall_state(ctx));
-  if (!S || (int)S->levels.size() != nlevels) {
-    set_last_error("wall distances: upload the wall geometry of these levels first");
-    return IBGPU_E_STATE;
-  }
-  const bool resident = (flags & IBGPU_WALL_RESIDENT) != 0;
-  if (resident && !S->resident) {
-    set_last_error("wall distances: no pairs on the device since the geometry upload");
-    return IBGPU_E_STATE;
-  }
+}  // extern "C"
+
+namespace {
+
+// The bodies' patch rows: checked, then on the device.
+int upload_bodies(State *S, const ibgpu_wall_bodies *bodies, cudaStream_t st, BodiesDev &B) {
   const int nb = bodies->nbodies;
   if (nb < 0 || (nb > 0 && (!bodies->patch_start || !bodies->pc || !bodies->nv ||
                             !bodies->nb_count || !bodies->nb)))
@@ -421,15 +486,6 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
       return IBGPU_E_ARG;
   for (int64_t r = 0; r < np; ++r)
     if (bodies->nb_count[r] < 0 || bodies->nb_count[r] > IBGPU_WALL_MAX_NB) return IBGPU_E_ARG;
-  for (int l = 0; l < nlevels; ++l) {
-    const ibgpu_wall_pairs &p = pairs[l];
-    const Level &L = S->levels[(size_t)l];
-    if ((L.n > 0 && (!p.body || !p.patch || !p.distance || !p.signdis || !p.distance_to_body ||
-                     !p.solid || !p.moved)) ||
-        (L.nblock > 0 && !p.block_moved))
-      return IBGPU_E_ARG;
-  }
-  cudaStream_t st = V.stream;
   int rc;
   const int32_t zero_start = 0;
   if ((rc = put(S->start, nb > 0 ? bodies->patch_start : &zero_start, nb + 1, st)) ||
@@ -437,7 +493,6 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
       (rc = put(S->nbc, bodies->nb_count, np, st)) ||
       (rc = put(S->nb, bodies->nb, (int64_t)IBGPU_WALL_MAX_NB * np, st)))
     return rc;
-  BodiesDev B;
   B.nbodies = nb;
   B.start = S->start.as<int32_t>();
   B.pc = S->pc.as<double>();
@@ -447,6 +502,109 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
   B.periodic_y = bodies->periodic_y;
   B.critic_y = bodies->critic_ylength;
   B.len_y = bodies->dm_length_y;
+  return IBGPU_OK;
+}
+
+LevelDev level_dev(Level &L) {
+  LevelDev D;
+  D.n = L.n;
+  D.nblock = L.nblock;
+  D.center = L.center.as<double>();
+  D.dtdm = L.dtdm.as<double>();
+  D.neib = L.neib.as<int32_t>();
+  D.kind = L.kind.as<uint8_t>();
+  D.block_in = L.block_in.as<int32_t>();
+  D.block_out = L.block_out.as<int32_t>();
+  D.body0 = L.body[0].as<int32_t>();
+  D.patch0 = L.patch[0].as<int32_t>();
+  D.dist0 = L.dist[0].as<double>();
+  D.sd0 = L.sd[0].as<double>();
+  D.dtb0 = L.dtb[0].as<double>();
+  D.body1 = L.body[1].as<int32_t>();
+  D.patch1 = L.patch[1].as<int32_t>();
+  D.dist1 = L.dist[1].as<double>();
+  D.sd1 = L.sd[1].as<double>();
+  D.dtb1 = L.dtb[1].as<double>();
+  D.body2 = L.body[2].as<int32_t>();
+  D.patch2 = L.patch[2].as<int32_t>();
+  D.dist2 = L.dist[2].as<double>();
+  D.sd2 = L.sd[2].as<double>();
+  D.dtb2 = L.dtb[2].as<double>();
+  D.solid = L.solid.as<uint8_t>();
+  D.moved = L.moved.as<uint8_t>();
+  D.block_moved = L.block_moved.as<uint8_t>();
+  return D;
+}
+
+// The four passes of one level (walk, junction, caps and move lists, block
+// ghosts) from its input pairs (set 0) to the new ones (set 2).
+int launch_passes(const LevelDev &D, const BodiesDev &B, int *err, cudaStream_t st) {
+  walk_kernel<<<blocks(D.n), 256, 0, st>>>(D, B, err);
+  junction_kernel<<<blocks(D.n), 256, 0, st>>>(D, B, err);
+  finalize_kernel<<<blocks(D.n), 256, 0, st>>>(D);
+  if (D.nblock > 0) block_kernel<<<blocks(D.nblock), 256, 0, st>>>(D);
+  WK(cudaGetLastError());
+  return IBGPU_OK;
+}
+
+// After the copies of a call: the walk's verdict; on success the new pairs
+// become the device's current ones (set 0).
+int settle(State *S, int herr) {
+  if (herr) {
+    S->resident = false;
+    set_last_error("wall distances: a box within 9.5 of a wall has no valid body or patch, "
+                   "or a patch walk did not end");
+    return IBGPU_E_ABORT;
+  }
+  for (Level &L : S->levels) {
+    std::swap(L.body[0], L.body[2]);
+    std::swap(L.patch[0], L.patch[2]);
+    std::swap(L.dist[0], L.dist[2]);
+    std::swap(L.sd[0], L.sd[2]);
+    std::swap(L.dtb[0], L.dtb[2]);
+  }
+  S->resident = true;
+  return IBGPU_OK;
+}
+
+State *wall_state(ibgpu_ctx *ctx, int nlevels) {
+  State *S = static_cast<State *>(*ctx_wall_state(ctx));
+  if (!S || (int)S->levels.size() != nlevels) {
+    set_last_error("wall distances: upload the wall geometry of these levels first");
+    return nullptr;
+  }
+  return S;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
+                        ibgpu_wall_pairs *pairs, int flags) {
+  CtxView V;
+  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !pairs) ||
+      (flags & ~IBGPU_WALL_RESIDENT) || ctx_view(ctx, &V) != IBGPU_OK)
+    return IBGPU_E_ARG;
+  State *S = wall_state(ctx, nlevels);
+  if (!S) return IBGPU_E_STATE;
+  const bool resident = (flags & IBGPU_WALL_RESIDENT) != 0;
+  if (resident && !S->resident) {
+    set_last_error("wall distances: no pairs on the device since the geometry upload");
+    return IBGPU_E_STATE;
+  }
+  for (int l = 0; l < nlevels; ++l) {
+    const ibgpu_wall_pairs &p = pairs[l];
+    const Level &L = S->levels[(size_t)l];
+    if ((L.n > 0 && (!p.body || !p.patch || !p.distance || !p.signdis || !p.distance_to_body ||
+                     !p.solid || !p.moved)) ||
+        (L.nblock > 0 && !p.block_moved))
+      return IBGPU_E_ARG;
+  }
+  cudaStream_t st = V.stream;
+  BodiesDev B;
+  int rc;
+  if ((rc = upload_bodies(S, bodies, st, B))) return rc;
   WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
   for (int l = 0; l < nlevels; ++l) {
     Level &L = S->levels[(size_t)l];
@@ -458,39 +616,7 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
          (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) ||
          (rc = put(L.solid, p.solid, L.n, st))))
       return rc;
-    LevelDev D;
-    D.n = L.n;
-    D.nblock = L.nblock;
-    D.center = L.center.as<double>();
-    D.dtdm = L.dtdm.as<double>();
-    D.neib = L.neib.as<int32_t>();
-    D.kind = L.kind.as<uint8_t>();
-    D.block_in = L.block_in.as<int32_t>();
-    D.block_out = L.block_out.as<int32_t>();
-    D.body0 = L.body[0].as<int32_t>();
-    D.patch0 = L.patch[0].as<int32_t>();
-    D.dist0 = L.dist[0].as<double>();
-    D.sd0 = L.sd[0].as<double>();
-    D.dtb0 = L.dtb[0].as<double>();
-    D.body1 = L.body[1].as<int32_t>();
-    D.patch1 = L.patch[1].as<int32_t>();
-    D.dist1 = L.dist[1].as<double>();
-    D.sd1 = L.sd[1].as<double>();
-    D.dtb1 = L.dtb[1].as<double>();
-    D.body2 = L.body[2].as<int32_t>();
-    D.patch2 = L.patch[2].as<int32_t>();
-    D.dist2 = L.dist[2].as<double>();
-    D.sd2 = L.sd[2].as<double>();
-    D.dtb2 = L.dtb[2].as<double>();
-    D.solid = L.solid.as<uint8_t>();
-    D.moved = L.moved.as<uint8_t>();
-    D.block_moved = L.block_moved.as<uint8_t>();
-    int *err = S->err.as<int>();
-    walk_kernel<<<blocks(L.n), 256, 0, st>>>(D, B, err);
-    junction_kernel<<<blocks(L.n), 256, 0, st>>>(D, B, err);
-    finalize_kernel<<<blocks(L.n), 256, 0, st>>>(D);
-    if (L.nblock > 0) block_kernel<<<blocks(L.nblock), 256, 0, st>>>(D);
-    WK(cudaGetLastError());
+    if ((rc = launch_passes(level_dev(L), B, S->err.as<int>(), st))) return rc;
     if ((rc = get(p.body, L.body[2], L.n, st)) || (rc = get(p.patch, L.patch[2], L.n, st)) ||
         (rc = get(p.distance, L.dist[2], L.n, st)) || (rc = get(p.signdis, L.sd[2], L.n, st)) ||
         (rc = get(p.distance_to_body, L.dtb[2], L.n, st)) || (rc = get(p.solid, L.solid, L.n, st)) ||
@@ -501,21 +627,106 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
   int herr = 0;
   WK(cudaMemcpyAsync(&herr, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   WK(cudaStreamSynchronize(st));
-  if (herr) {
-    S->resident = false;
-    set_last_error("wall distances: a box within 9.5 of a wall has no valid body or patch, "
-                   "or a patch walk did not end");
-    return IBGPU_E_ABORT;
+  return settle(S, herr);
+}
+
+int ibgpu_wall_distance_near(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
+                             ibgpu_wall_near *levels) {
+  CtxView V;
+  if (!ctx || !bodies || nlevels < 0 || (nlevels > 0 && !levels) ||
+      ctx_view(ctx, &V) != IBGPU_OK)
+    return IBGPU_E_ARG;
+  State *S = wall_state(ctx, nlevels);
+  if (!S) return IBGPU_E_STATE;
+  if (!S->resident) {
+    set_last_error("wall distances: no pairs on the device since the geometry upload");
+    return IBGPU_E_STATE;
   }
-  // the results are the next call's inputs (the solid flags are in place)
-  for (Level &L : S->levels) {
-    std::swap(L.body[0], L.body[2]);
-    std::swap(L.patch[0], L.patch[2]);
-    std::swap(L.dist[0], L.dist[2]);
-    std::swap(L.sd[0], L.sd[2]);
-    std::swap(L.dtb[0], L.dtb[2]);
+  for (int l = 0; l < nlevels; ++l) {
+    const ibgpu_wall_near &o = levels[l];
+    const Level &L = S->levels[(size_t)l];
+    if (o.capacity < 0 || (o.capacity > 0 && !o.changes) || (L.nblock > 0 && !o.block_moved) ||
+        !(o.band >= 0.0))
+      return IBGPU_E_ARG;
   }
-  S->resident = true;
+  cudaStream_t st = V.stream;
+  BodiesDev B;
+  int rc;
+  if ((rc = upload_bodies(S, bodies, st, B))) return rc;
+  WK(S->totals.reserve(sizeof(int) * (size_t)std::max(nlevels, 1)));
+  WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
+  WK(cudaMemsetAsync(S->totals.p, 0, sizeof(int) * (size_t)std::max(nlevels, 1), st));
+  int *totals = S->totals.as<int>();
+  for (int l = 0; l < nlevels; ++l) {
+    Level &L = S->levels[(size_t)l];
+    if (L.n == 0) continue;
+    const LevelDev D = level_dev(L);
+    if ((rc = launch_passes(D, B, S->err.as<int>(), st))) return rc;
+    const int nb = (int)((L.n + kNearBlock - 1) / kNearBlock);
+    WK(L.block_count.reserve(sizeof(int) * (size_t)nb));
+    WK(L.changes.reserve(sizeof(ibgpu_wall_change) * (size_t)L.n));
+    const double band = levels[l].band;
+    near_count_kernel<<<nb, kNearBlock, 0, st>>>(D, band, L.block_count.as<int>());
+    near_scan_kernel<<<1, 1024, 0, st>>>(L.block_count.as<int>(), nb, totals + l);
+    near_write_kernel<<<nb, kNearBlock, 0, st>>>(D, band, L.block_count.as<int>(),
+                                                 L.changes.as<ibgpu_wall_change>());
+    WK(cudaGetLastError());
+    if ((rc = get(levels[l].block_moved, L.block_moved, L.nblock, st))) return rc;
+  }
+  std::vector<int> count((size_t)std::max(nlevels, 1), 0);
+  int herr = 0;
+  WK(cudaMemcpyAsync(count.data(), totals, sizeof(int) * (size_t)nlevels, cudaMemcpyDeviceToHost,
+                     st));
+  WK(cudaMemcpyAsync(&herr, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WK(cudaStreamSynchronize(st));
+  if (herr) return settle(S, herr);
+  bool fits = true;
+  for (int l = 0; l < nlevels; ++l) {
+    ibgpu_wall_near &o = levels[l];
+    o.count = count[(size_t)l];
+    if (o.count > o.capacity) {
+      fits = false;
+      continue;
+    }
+    if ((rc = get(o.changes, S->levels[(size_t)l].changes, o.count, st))) return rc;
+  }
+  WK(cudaStreamSynchronize(st));
+  rc = settle(S, 0);
+  if (rc == IBGPU_OK && !fits) {
+    set_last_error("wall distances: more boxes near the walls than the output holds");
+    return IBGPU_E_ARG;
+  }
+  return rc;
+}
+
+int ibgpu_wall_fetch(ibgpu_ctx *ctx, int nlevels, ibgpu_wall_pairs *pairs) {
+  CtxView V;
+  if (!ctx || nlevels < 0 || (nlevels > 0 && !pairs) || ctx_view(ctx, &V) != IBGPU_OK)
+    return IBGPU_E_ARG;
+  State *S = wall_state(ctx, nlevels);
+  if (!S) return IBGPU_E_STATE;
+  if (!S->resident) {
+    set_last_error("wall distances: no pairs on the device since the geometry upload");
+    return IBGPU_E_STATE;
+  }
+  cudaStream_t st = V.stream;
+  for (int l = 0; l < nlevels; ++l) {
+    const Level &L = S->levels[(size_t)l];
+    ibgpu_wall_pairs &p = pairs[l];
+    if (L.n > 0 && (!p.body || !p.patch || !p.distance || !p.signdis || !p.distance_to_body ||
+                    !p.solid))
+      return IBGPU_E_ARG;
+  }
+  int rc;
+  for (int l = 0; l < nlevels; ++l) {
+    const Level &L = S->levels[(size_t)l];
+    ibgpu_wall_pairs &p = pairs[l];
+    if ((rc = get(p.body, L.body[0], L.n, st)) || (rc = get(p.patch, L.patch[0], L.n, st)) ||
+        (rc = get(p.distance, L.dist[0], L.n, st)) || (rc = get(p.signdis, L.sd[0], L.n, st)) ||
+        (rc = get(p.distance_to_body, L.dtb[0], L.n, st)) || (rc = get(p.solid, L.solid, L.n, st)))
+      return rc;
+  }
+  WK(cudaStreamSynchronize(st));
   return IBGPU_OK;
 }
 

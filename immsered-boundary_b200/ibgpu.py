@@ -41,7 +41,8 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
            "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
            "ibgpu_set_state_rows", "ibgpu_build_interfaces", "ibgpu_wall_geometry",
-           "ibgpu_wall_distance", "ibgpu_host_register", "ibgpu_host_unregister")
+           "ibgpu_wall_distance", "ibgpu_host_register", "ibgpu_host_unregister",
+           "ibgpu_wall_distance_near", "ibgpu_wall_fetch")
 ROWS_FLOWVARS, ROWS_COMPACT = 7, 4
 NOALLOC_MAX_CELLS = 65536
 TAG_MAX_LEVELS = 16
@@ -125,6 +126,25 @@ class WallPairs(ctypes.Structure):
                 ("distance", ctypes.c_void_p), ("signdis", ctypes.c_void_p),
                 ("distance_to_body", ctypes.c_void_p), ("solid", ctypes.c_void_p),
                 ("moved", ctypes.c_void_p), ("block_moved", ctypes.c_void_p)]
+
+
+class WallChange(ctypes.Structure):
+    _fields_ = [("box", ctypes.c_int32), ("body", ctypes.c_int32), ("patch", ctypes.c_int32),
+                ("solid", ctypes.c_uint8), ("moved", ctypes.c_uint8),
+                ("pad_", ctypes.c_uint8 * 2), ("distance", ctypes.c_double),
+                ("signdis", ctypes.c_double), ("distance_to_body", ctypes.c_double)]
+
+
+WALL_CHANGE_DTYPE = np.dtype([("box", np.int32), ("body", np.int32), ("patch", np.int32),
+                              ("solid", np.uint8), ("moved", np.uint8), ("pad_", np.uint8, 2),
+                              ("distance", np.float64), ("signdis", np.float64),
+                              ("distance_to_body", np.float64)])
+
+
+class WallNear(ctypes.Structure):
+    _fields_ = [("band", ctypes.c_double), ("capacity", ctypes.c_int64),
+                ("changes", ctypes.c_void_p), ("count", ctypes.c_int64),
+                ("block_moved", ctypes.c_void_p)]
 
 
 class Cells(ctypes.Structure):
@@ -461,6 +481,52 @@ class FlowSolver:
         arr = (WallLevelGeom * max(len(geoms), 1))(*geoms)
         _check(lib().ibgpu_wall_geometry(self._ctx, len(geoms), arr), "ibgpu_wall_geometry")
 
+    @staticmethod
+    def _wall_bodies(bodies: dict):
+        arrs = dict(ps=np.ascontiguousarray(bodies["patch_start"], np.int32),
+                    pc=np.ascontiguousarray(bodies["pc"], np.float64),
+                    nv=np.ascontiguousarray(bodies["nv"], np.float64),
+                    nbc=np.ascontiguousarray(bodies["nb_count"], np.int32),
+                    nbl=np.ascontiguousarray(bodies["nb"], np.int32))
+        wb = WallBodies(len(arrs["ps"]) - 1, arrs["ps"].ctypes.data, arrs["pc"].ctypes.data,
+                        arrs["nv"].ctypes.data, arrs["nbc"].ctypes.data, arrs["nbl"].ctypes.data,
+                        int(bodies.get("periodic_y", 0)),
+                        float(bodies.get("critic_ylength", 1e300)),
+                        float(bodies.get("dm_length_y", 0.0)))
+        return wb, arrs
+
+    def wall_distance_near(self, bodies: dict, bands, nboxes, nblocks):
+        """ibgpu_wall_distance_near: from the pairs the device holds, per level
+        (band, room for nboxes reported boxes, its block-pair count) a
+        structured array of the reported boxes (WALL_CHANGE_DTYPE, box order)
+        and the block pairs' moved flags."""
+        wb, keep = self._wall_bodies(bodies)
+        outs = [(np.zeros(max(int(n), 1), WALL_CHANGE_DTYPE), np.zeros(max(int(nbk), 1), np.uint8))
+                for n, nbk in zip(nboxes, nblocks)]
+        arr = (WallNear * max(len(outs), 1))(*[
+            WallNear(float(b), int(n), ch.ctypes.data, 0, bm.ctypes.data)
+            for b, n, (ch, bm) in zip(bands, nboxes, outs)])
+        _check(lib().ibgpu_wall_distance_near(self._ctx, ctypes.byref(wb), len(outs), arr),
+               "ibgpu_wall_distance_near")
+        return [(ch[:arr[l].count], bm[:int(nbk)]) for l, ((ch, bm), nbk) in
+                enumerate(zip(outs, nblocks))]
+
+    def wall_fetch(self, nboxes):
+        """ibgpu_wall_fetch: every level's pairs (dicts of body, patch,
+        distance, signdis, distance_to_body, solid) as the device holds them."""
+        out, arrs = [], []
+        for n in nboxes:
+            n = int(n)
+            p = dict(body=np.zeros(n, np.int32), patch=np.zeros(n, np.int32),
+                     distance=np.zeros(n), signdis=np.zeros(n), distance_to_body=np.zeros(n),
+                     solid=np.zeros(n, np.uint8))
+            out.append(p)
+            arrs.append(WallPairs(*(p[k].ctypes.data for k in (
+                "body", "patch", "distance", "signdis", "distance_to_body", "solid")), None, None))
+        arr = (WallPairs * max(len(arrs), 1))(*arrs)
+        _check(lib().ibgpu_wall_fetch(self._ctx, len(arrs), arr), "ibgpu_wall_fetch")
+        return out
+
     def wall_distance(self, bodies: dict, pairs, resident: bool = False):
         """The bodies' patches (patch_start, pc (n, 3), nv (n, 3), nb_count,
         nb (n, 15); periodic_y, critic_ylength, dm_length_y) and every
@@ -469,15 +535,7 @@ class FlowSolver:
         block_moved added (ibgpu_wall_distance).  resident: start from the
         pairs the device kept from the previous call (the dicts' input
         values are not read)."""
-        ps = np.ascontiguousarray(bodies["patch_start"], np.int32)
-        pc = np.ascontiguousarray(bodies["pc"], np.float64)
-        nv = np.ascontiguousarray(bodies["nv"], np.float64)
-        nbc = np.ascontiguousarray(bodies["nb_count"], np.int32)
-        nbl = np.ascontiguousarray(bodies["nb"], np.int32)
-        wb = WallBodies(len(ps) - 1, ps.ctypes.data, pc.ctypes.data, nv.ctypes.data,
-                        nbc.ctypes.data, nbl.ctypes.data, int(bodies.get("periodic_y", 0)),
-                        float(bodies.get("critic_ylength", 1e300)),
-                        float(bodies.get("dm_length_y", 0.0)))
+        wb, keep = self._wall_bodies(bodies)
         arrs = []
         for p in pairs:
             for key, dt in (("body", np.int32), ("patch", np.int32), ("distance", np.float64),

@@ -275,6 +275,41 @@ int ibgpu_host_unregister(void *ptr);
 int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
                         ibgpu_wall_pairs *pairs, int flags);
 
+/* One box of a level in the output of ibgpu_wall_distance_near. */
+typedef struct ibgpu_wall_change {
+  int32_t box;           /* index of the box in its level */
+  int32_t body, patch;
+  uint8_t solid;
+  uint8_t moved;         /* IBGPU_WALL_INTO_BODY / _OUT_OF_BODY / 0 */
+  uint8_t pad_[2];
+  double distance, signdis, distance_to_body;
+} ibgpu_wall_change;     /* 40 bytes */
+
+typedef struct ibgpu_wall_near { /* one level */
+  double band;                 /* in: a box is reported when |signdis| < band
+                                  before or after the move, or it changed sides */
+  int64_t capacity;            /* in: entries `changes` holds */
+  ibgpu_wall_change *changes;  /* out: the reported boxes, in box order */
+  int64_t count;               /* out: the number reported */
+  uint8_t *block_moved;        /* out, per block pair, as in ibgpu_wall_pairs */
+} ibgpu_wall_near;
+
+/* ibgpu_wall_distance from the pairs the device holds (as with
+ * IBGPU_WALL_RESIDENT), returning per level only the boxes near a wall
+ * before or after the move and those that changed sides (what a host
+ * re-immersion reads before the next move: a small part of the level)
+ * instead of every box.  The device keeps every new pair either way.
+ * IBGPU_E_ARG when a level reports more boxes than its capacity (count
+ * then says how many; the pairs have moved on: ibgpu_wall_fetch has them
+ * all); the other codes as ibgpu_wall_distance. */
+int ibgpu_wall_distance_near(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nlevels,
+                             ibgpu_wall_near *levels);
+
+/* Every level's pairs and solid flags as the device holds them after its
+ * last wall-distance call (the moved and block_moved arrays are not
+ * written).  IBGPU_E_STATE when there are none since the geometry upload. */
+int ibgpu_wall_fetch(ibgpu_ctx *ctx, int nlevels, ibgpu_wall_pairs *pairs);
+
 /* Wall force and moment of every body from the current state
  * (Body::ComptWallForce): out[6*b + 0..2] force, out[6*b + 3..5] moment,
  * in the reference's dimensional scaling. */

@@ -51,6 +51,8 @@ def test_null_arguments_are_rejected_without_gpu(pkg):
     assert lib.ibgpu_batch_table_bytes(None) == 0
     assert lib.ibgpu_wall_geometry(None, 0, None) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_wall_distance(None, None, 0, None, 0) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_wall_distance_near(None, None, 0, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_wall_fetch(None, 0, None) == pkg.ibgpu.E_ARG
 
 
 def test_ctypes_layouts_match_c(pkg, tmp_path):
@@ -60,7 +62,8 @@ def test_ctypes_layouts_match_c(pkg, tmp_path):
                "ibgpu_tag_rule": ib.TagRule, "ibgpu_tag_cells": ib.TagCells,
                "ibgpu_interface_lists": ib.InterfaceLists,
                "ibgpu_wall_level_geom": ib.WallLevelGeom, "ibgpu_wall_bodies": ib.WallBodies,
-               "ibgpu_wall_pairs": ib.WallPairs}
+               "ibgpu_wall_pairs": ib.WallPairs, "ibgpu_wall_change": ib.WallChange,
+               "ibgpu_wall_near": ib.WallNear}
     # every field of every mirrored struct
     checks = {c: (cls, [f[0] for f in cls._fields_]) for c, cls in mirrors.items()}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ibgpu.h"', "int main(void){"]

@@ -124,6 +124,13 @@ def test_flag_update_keeps_the_layout(cuda_lib, pkg, snaps):
     with pytest.raises(ib.IbgpuError) as ei:
         sol.update_flags(flags)
     assert ei.value.code == ib.E_TOPOLOGY
+    # the refused update changed nothing on the device: a step there equals
+    # a step of a context that never saw it
+    sol.time_marching(int(a["step"]))
+    ref = workloads.naca_solver(make_golden.record_of(a), 0, ib.FP64)
+    ref.time_marching(int(a["step"]))
+    assert np.array_equal(sol.download(), ref.download())
+    ref.close()
     sol.close()
 
 

@@ -96,3 +96,75 @@ def test_invalid_pairs_and_geometry_are_reported(cuda_lib, pkg):
         sol.wall_distance(bodies, [p])
     assert e.value.code == ib.E_ABORT
     sol.close()
+
+
+def near_reference(prev, new, band):
+    """The boxes ibgpu_wall_distance_near reports: |signdis| < band before or
+    after the move, or a changed side; in box order."""
+    keep = ((np.abs(np.asarray(prev["signdis"])) < band) | (np.abs(new["signdis"]) < band) |
+            (new["moved"] != 0))
+    return np.flatnonzero(keep)
+
+
+def test_near_output_is_the_full_output_near_the_walls(cuda_lib, pkg):
+    """From the pairs the device kept, the near-wall call reports exactly the
+    boxes near a wall before or after the move or on the other side now,
+    with the full call's pairs; the block pairs' flags in full; afterwards
+    ibgpu_wall_fetch returns every box's pair as the full call does."""
+    ib = pkg.ibgpu
+    bodies1, geom, pairs = wo.synthetic_case(seed=2, turn=0.05)
+    bodies2, _, _ = wo.synthetic_case(seed=2, turn=0.3)
+    ref1 = wo.wall_distance(bodies1, geom, pairs)
+    ref2 = wo.wall_distance(bodies2, geom, dict(ref1, nblock=pairs["nblock"]))
+    P, cells, prim = wl.vortex_case(32)
+    n, nblock = len(geom["kind"]), int(pairs["nblock"])
+    for band in (0.0, 0.4, 1e9):
+        sol = ib.FlowSolver(P)
+        sol.wall_geometry([geom, geom])
+        p = [{k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+             for _ in range(2)]
+        for q in p:
+            q["nblock"] = pairs["nblock"]
+        sol.wall_distance(bodies1, p)
+        out = sol.wall_distance_near(bodies2, [band, band], [n, n], [nblock, nblock])
+        want = near_reference(ref1, ref2, band)
+        for ch, bm in out:
+            assert np.array_equal(ch["box"], want)
+            for k in ("body", "patch", "distance", "signdis", "distance_to_body", "solid",
+                      "moved"):
+                assert np.array_equal(bits(ch[k]), bits(np.asarray(ref2[k])[want])), (band, k)
+            assert np.array_equal(bm, ref2["block_moved"])
+        got = sol.wall_fetch([n, n])
+        for g in got:
+            for k in ("body", "patch", "distance", "signdis", "distance_to_body", "solid"):
+                assert np.array_equal(bits(g[k]), bits(ref2[k])), k
+        sol.close()
+
+
+def test_near_output_needs_resident_pairs_and_room(cuda_lib, pkg):
+    ib = pkg.ibgpu
+    bodies1, geom, pairs = wo.synthetic_case(seed=6, turn=0.05)
+    bodies2, _, _ = wo.synthetic_case(seed=6, turn=0.2)
+    ref1 = wo.wall_distance(bodies1, geom, pairs)
+    ref2 = wo.wall_distance(bodies2, geom, dict(ref1, nblock=pairs["nblock"]))
+    P, cells, prim = wl.vortex_case(32)
+    n, nblock = len(geom["kind"]), int(pairs["nblock"])
+    sol = ib.FlowSolver(P)
+    sol.wall_geometry([geom])
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance_near(bodies1, [1.0], [n], [nblock])  # no pairs on the device yet
+    assert e.value.code == ib.E_STATE
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_fetch([n])
+    assert e.value.code == ib.E_STATE
+    p = {k: np.array(v, copy=True) for k, v in pairs.items() if k != "nblock"}
+    p["nblock"] = pairs["nblock"]
+    sol.wall_distance(bodies1, [p])
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance_near(bodies2, [1e9], [5], [nblock])  # room for 5 boxes only
+    assert e.value.code == ib.E_ARG
+    # the device moved on all the same: every pair is there
+    got = sol.wall_fetch([n])[0]
+    for k in ("body", "patch", "distance", "signdis", "distance_to_body", "solid"):
+        assert np.array_equal(bits(got[k]), bits(ref2[k])), k
+    sol.close()
