@@ -892,6 +892,17 @@ class GpuNS_Solver : public NS_Solver {
       MPI_Bcast(lists_.level.data(), nrows, MPI_INT, 0, share_comm);
       MPI_Bcast(lists_.box.data(), nrows, MPI_INT, 0, share_comm);
     }
+    if (rc == IBGPU_OK) {
+      // each level's box -> row map (every rank), for the flag updates of
+      // the rows near the walls after a move
+      row_of_.assign(a_mesh.MyCurNum(), std::vector<int>());
+      for (size_t i = 0; i < lists_.box.size(); ++i) {
+        std::vector<int> &m = row_of_[lists_.level[i]];
+        if ((int)m.size() <= lists_.box[i]) m.resize(lists_.box[i] + 1, -1);
+        m[lists_.box[i]] = (int)i;
+      }
+      ib_rows_.clear();
+    }
     return rc;
   }
 
@@ -905,13 +916,16 @@ class GpuNS_Solver : public NS_Solver {
   int MoveBodies(std::vector<Body> &bodies, double &dt00) {
     if (!created_) return IBGPU_E_STATE;
     dt00 += dt;
+    // a move from the pairs the device kept reports the boxes near the
+    // walls, and only their rows' flags can change
+    const bool near = device_distance_ && !wall_check_ && wall_resident_;
     int rc = IbgpuAdapter::MoveBodies(ctx_, a_mesh, bodies, dt00,
                                       device_distance_ ? &wall_ : nullptr, wall_check_,
                                       &wall_resident_);
     if (rc) return rc;
     dt00 = 0.0;
     const double t0 = MPI_Wtime();
-    rc = UploadImmersion(bodies);
+    rc = UploadImmersion(bodies, near);
     ibgpu_move_times().upload += MPI_Wtime() - t0;
     return rc;
   }
@@ -928,10 +942,15 @@ class GpuNS_Solver : public NS_Solver {
 
   // After the bodies moved without a regrid: the flags of the same cell rows
   // (ibgpu_update_flags) and the immersed-boundary records
-  // (ibgpu_upload_ib) from the mesh as it is now (every rank).
-  int UploadImmersion(std::vector<Body> &bodies) {
+  // (ibgpu_upload_ib) from the mesh as it is now (every rank).  With near
+  // (the move's wall distances came as the device's near-wall report) only
+  // the rows whose flags the move can change: the reported boxes' rows
+  // (each rank its run of every level's report) and the immersed-boundary
+  // cells' rows before and after the move (ibgpu_update_flags_rows).
+  int UploadImmersion(std::vector<Body> &bodies, bool near = false) {
     if (!created_) return IBGPU_E_STATE;
     MPI_Barrier(share_comm);
+    if (near) return UploadImmersionNear(bodies);
     // the rows' flags, each rank a contiguous share, gathered on every rank
     const int nrows = (int)lists_.box.size();
     std::vector<int> counts(sprocs), displs(sprocs);
@@ -947,7 +966,79 @@ class GpuNS_Solver : public NS_Solver {
                      MPI_BYTE, share_comm);
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
+      // the immersed-boundary cells' rows, for the next update of the rows
+      // near the walls
+      const int last = a_mesh.MyCurNum() - 1;
+      ib_rows_.clear();
+      DataArray<IBCell> &mdis = a_mesh.ibarray();
+      for (int i = 0; i < mdis.size(); ++i) {
+        const int b = mdis[i].ci;
+        if (b >= 0 && b < (int)row_of_[last].size() && row_of_[last][b] >= 0)
+          ib_rows_.push_back(row_of_[last][b]);
+      }
       rc = ibgpu_update_flags(ctx_, lists_.flags.data());
+      if (rc == IBGPU_OK) {
+        IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
+        rc = IbgpuAdapter::UploadIB(ctx_, lists_);
+      }
+    }
+    return ibgpu_share_status(rc);
+  }
+
+  int UploadImmersionNear(std::vector<Body> &bodies) {
+    const int nlev = a_mesh.MyCurNum();
+    std::vector<int> rows;
+    for (int l = 0; l < nlev && l < (int)wall_.size(); ++l) {
+      DataArray<Box> &boxes = a_mesh.ShowLevelBox(l);
+      const IbgpuWallLevel &W = wall_[l];
+      const std::vector<int> &m = row_of_[l];
+      int bs, be;
+      boxes.GlobalOrder(bs, be);
+      const ibgpu_wall_change *c = W.changes, *end = W.changes + *W.nchanges;
+      c = std::lower_bound(c, end, bs,
+                           [](const ibgpu_wall_change &a, int box) { return a.box < box; });
+      for (; c != end && c->box < be; ++c)
+        if (c->box < (int)m.size() && m[c->box] >= 0) rows.push_back(m[c->box]);
+    }
+    // this rank's rows, then every rank's, in rank order
+    int mine = (int)rows.size();
+    std::vector<int> counts(sprocs, 0), displs(sprocs, 0);
+    MPI_Allgather(&mine, 1, MPI_INT, counts.data(), 1, MPI_INT, share_comm);
+    int total = 0;
+    for (int r = 0; r < sprocs; ++r) {
+      displs[r] = total;
+      total += counts[r];
+    }
+    std::vector<uint8_t> flags(mine);
+    for (int k = 0; k < mine; ++k)
+      flags[k] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[rows[k]], lists_.box[rows[k]]);
+    std::vector<int> all_rows(total);
+    std::vector<uint8_t> all_flags(total);
+    MPI_Allgatherv(rows.data(), mine, MPI_INT, all_rows.data(), counts.data(), displs.data(),
+                   MPI_INT, share_comm);
+    MPI_Allgatherv(flags.data(), mine, MPI_BYTE, all_flags.data(), counts.data(), displs.data(),
+                   MPI_BYTE, share_comm);
+    int rc = IBGPU_OK;
+    if (ibgpu_device_rank()) {
+      std::vector<int64_t> r64(all_rows.begin(), all_rows.end());
+      // the immersed-boundary cells' rows before the move and now
+      const int last = nlev - 1;
+      std::vector<int> now_ib;
+      DataArray<IBCell> &mdis = a_mesh.ibarray();
+      for (int i = 0; i < mdis.size(); ++i) {
+        const int b = mdis[i].ci;
+        if (b >= 0 && b < (int)row_of_[last].size() && row_of_[last][b] >= 0)
+          now_ib.push_back(row_of_[last][b]);
+      }
+      for (const std::vector<int> *v : {&ib_rows_, &now_ib})
+        for (int r : *v) {
+          r64.push_back(r);
+          all_flags.push_back(IbgpuAdapter::BoxFlags(a_mesh, lists_.level[r], lists_.box[r]));
+        }
+      ib_rows_.swap(now_ib);
+      lists_.flags.resize(lists_.box.size());
+      for (size_t k = 0; k < r64.size(); ++k) lists_.flags[r64[k]] = all_flags[k];
+      rc = ibgpu_update_flags_rows(ctx_, (int64_t)r64.size(), r64.data(), all_flags.data());
       if (rc == IBGPU_OK) {
         IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
         rc = IbgpuAdapter::UploadIB(ctx_, lists_);
@@ -1052,4 +1143,6 @@ class GpuNS_Solver : public NS_Solver {
   // since the last geometry upload (the exchange buffers hold them too)
   bool device_distance_ = true, wall_check_ = false, wall_resident_ = false;
   std::vector<IbgpuWallLevel> wall_;  // exchange buffers of the device wall distances
+  std::vector<std::vector<int> > row_of_;  // per level: box -> row of lists_ (-1: none)
+  std::vector<int> ib_rows_;  // rows of the immersed-boundary cells after the last move
 };

@@ -106,6 +106,9 @@ struct ibgpu_ctx {
   // the first row whose layout bits changed
   uint8_t *d_cell_layout = nullptr, *d_row_flags = nullptr, *d_tile_full = nullptr;
   int *d_layout_err = nullptr;
+  // ibgpu_update_flags_rows: the rows and their flags (grown when short)
+  int64_t *d_row_which = nullptr;
+  uint8_t *d_row_sub = nullptr;
 
   // state: step state (6 fields) + two stage buffers (4 fields each)
   double *d_s0[kStateFields] = {};
@@ -200,6 +203,12 @@ struct ibgpu_ctx {
     }
     cudaFree(d_layout_err);
     d_layout_err = nullptr;
+    cudaFree(d_row_which);
+    cudaFree(d_row_sub);
+    d_row_which = nullptr;
+    d_row_sub = nullptr;
+    cap.erase(&d_row_which);
+    cap.erase(&d_row_sub);
     cudaFree(d_tile_org);
     cudaFree(d_signdis);
     cudaFree(d_tags);
@@ -219,6 +228,32 @@ struct ibgpu_ctx {
     has_topology = has_state = false;
   }
 };
+
+namespace {
+
+// A context buffer of at least n elements that stays between calls (freed
+// and allocated again only when it is too short).
+template <typename T>
+int keep_alloc(ibgpu_ctx *ctx, T **dst, size_t n) {
+  size_t &c = ctx->cap[dst];
+  if (*dst && n <= c) return IBGPU_OK;
+  cudaFree(*dst);
+  *dst = nullptr;
+  c = 0;
+  const int rc = dev_alloc(dst, n);
+  if (rc) return rc;
+  c = n > 0 ? n : 1;
+  return IBGPU_OK;
+}
+template <typename T>
+int keep_upload(ibgpu_ctx *ctx, T **dst, const std::vector<T> &v, cudaStream_t st) {
+  const int rc = keep_alloc(ctx, dst, v.size());
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return IBGPU_OK;
+}
+
+}  // namespace
 
 namespace ibgpu {
 void set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -332,23 +367,29 @@ namespace {
 // ibgpu_update_flags on the device, over the rows' new flags in `rows`:
 // the first row whose PRESENT / NORMAL / ALIAS bits differ from the
 // topology upload (atomicMin into *err, which starts at INT_MAX) ...
-__global__ void layout_check_kernel(const uint8_t *rows, const uint8_t *layout, int64_t n,
-                                    int *err) {
+// (with `which`, new flags rows[k] for row which[k], k < n; without, for
+// every row c < n) ...
+__global__ void layout_check_kernel(const uint8_t *rows, const int64_t *which,
+                                    const uint8_t *layout, int64_t n, int *err) {
   constexpr uint8_t kBits = CF_PRESENT | CF_NORMAL | IBGPU_CELL_ALIAS;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const uint8_t lay = (uint8_t)((rows[c] & kBits) | (layout[c] & IBGPU_CELL_ALIAS));
-    if (lay != layout[c]) atomicMin(err, (int)c);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = which ? which[k] : k;
+    const uint8_t lay = (uint8_t)((rows[k] & kBits) | (layout[c] & IBGPU_CELL_ALIAS));
+    if (lay != layout[c]) atomicMin(err, (int)k);
   }
 }
 
 // ... each non-alias row's flags into its slot (the slots no row maps to
 // keep the zeros of the topology upload) ...
-__global__ void flags_scatter_kernel(const uint8_t *rows, const uint8_t *layout,
-                                     const int32_t *slot, int64_t n, uint8_t *flags) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x)
-    if (!(layout[c] & IBGPU_CELL_ALIAS)) flags[slot[c]] = rows[c] & 0x3f;
+__global__ void flags_scatter_kernel(const uint8_t *rows, const int64_t *which,
+                                     const uint8_t *layout, const int32_t *slot, int64_t n,
+                                     uint8_t *flags) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = which ? which[k] : k;
+    if (!(layout[c] & IBGPU_CELL_ALIAS)) flags[slot[c]] = rows[k] & 0x3f;
+  }
 }
 
 // ... which tiles hold only recovering leaf cells (one warp per tile, eight
@@ -683,23 +724,38 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
 }
 
 
-int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
-  if (!ctx || (!flags && ctx->ncells > 0)) return IBGPU_E_ARG;
-  if (!ctx->has_topology) return IBGPU_E_STATE;
+}  // extern "C"
+
+// New flags of n rows (all rows in order when which is null, else rows
+// which[k]) into the device's slot flags, then the uniform tiles anew.
+static int update_flags_on_device(ibgpu_ctx *ctx, int64_t n, const int64_t *which,
+                                  const uint8_t *flags) {
   if (ctx->chain_open) {
     g_last_error = "asynchronous steps pending: call ibgpu_step_result first";
     return IBGPU_E_STATE;
   }
-  const int64_t n = ctx->ncells, nt = ctx->ntiles;
   if (n == 0) return IBGPU_OK;
   cudaStream_t st = ctx->stream;
   const int grid = 4 * ctx->nsm;
-  // the rows' flags and the layout check first: nothing changes on the
-  // device when a row's layout bits differ
+  const int64_t nt = ctx->ntiles;
+  int rc;
+  uint8_t *d_rows = ctx->d_row_flags;  // room for every row
+  int64_t *d_which = nullptr;
+  if (which) {
+    // the previous step may still read the staging buffer of an earlier call
+    if ((size_t)n > ctx->cap[&ctx->d_row_which]) CK(cudaStreamSynchronize(st));
+    if ((rc = keep_alloc(ctx, &ctx->d_row_which, (size_t)n))) return rc;
+    if ((rc = keep_alloc(ctx, &ctx->d_row_sub, (size_t)n))) return rc;
+    d_which = ctx->d_row_which;
+    d_rows = ctx->d_row_sub;
+    CK(cudaMemcpyAsync(d_which, which, n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  }
+  // the flags and the layout check first: nothing changes on the device
+  // when a row's layout bits differ
   const int big = INT32_MAX;
-  CK(cudaMemcpyAsync(ctx->d_row_flags, flags, n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_rows, flags, n, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_layout_err, &big, sizeof(int), cudaMemcpyHostToDevice, st));
-  layout_check_kernel<<<grid, 256, 0, st>>>(ctx->d_row_flags, ctx->d_cell_layout, n,
+  layout_check_kernel<<<grid, 256, 0, st>>>(d_rows, d_which, ctx->d_cell_layout, n,
                                             ctx->d_layout_err);
   CK(cudaGetLastError());
   int bad = big;
@@ -709,7 +765,7 @@ int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
     g_last_error = "a row changed its PRESENT, NORMAL or ALIAS bit: upload the topology";
     return IBGPU_E_TOPOLOGY;
   }
-  flags_scatter_kernel<<<grid, 256, 0, st>>>(ctx->d_row_flags, ctx->d_cell_layout,
+  flags_scatter_kernel<<<grid, 256, 0, st>>>(d_rows, d_which, ctx->d_cell_layout,
                                              ctx->d_cell_slot, n, ctx->d_flags);
   if (nt > 0) {
     tile_full_kernel<<<(unsigned)((nt * 32 + 255) / 256), 256, 0, st>>>(ctx->d_flags, nt,
@@ -721,6 +777,26 @@ int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   return IBGPU_OK;
+}
+
+extern "C" {
+
+int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags) {
+  if (!ctx || (!flags && ctx->ncells > 0)) return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  return update_flags_on_device(ctx, ctx->ncells, nullptr, flags);
+}
+
+int ibgpu_update_flags_rows(ibgpu_ctx *ctx, int64_t n, const int64_t *rows,
+                            const uint8_t *flags) {
+  if (!ctx || n < 0 || (n > 0 && (!rows || !flags))) return IBGPU_E_ARG;
+  if (!ctx->has_topology) return IBGPU_E_STATE;
+  for (int64_t k = 0; k < n; ++k)
+    if (rows[k] < 0 || rows[k] >= ctx->ncells) {
+      g_last_error = "flag update: a row index outside the topology's rows";
+      return IBGPU_E_ARG;
+    }
+  return update_flags_on_device(ctx, n, rows, flags);
 }
 
 int ibgpu_layout_info(const ibgpu_ctx *ctx, int64_t *nslots, int64_t *ntiles) {
@@ -1885,27 +1961,6 @@ int upload_vec(T **dst, const std::vector<T> &v, cudaStream_t st) {
   return IBGPU_OK;
 }
 
-// A context buffer of at least n elements that stays between calls (freed
-// and allocated again only when it is too short).
-template <typename T>
-int keep_alloc(ibgpu_ctx *ctx, T **dst, size_t n) {
-  size_t &c = ctx->cap[dst];
-  if (*dst && n <= c) return IBGPU_OK;
-  cudaFree(*dst);
-  *dst = nullptr;
-  c = 0;
-  const int rc = dev_alloc(dst, n);
-  if (rc) return rc;
-  c = n > 0 ? n : 1;
-  return IBGPU_OK;
-}
-template <typename T>
-int keep_upload(ibgpu_ctx *ctx, T **dst, const std::vector<T> &v, cudaStream_t st) {
-  const int rc = keep_alloc(ctx, dst, v.size());
-  if (rc) return rc;
-  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  return IBGPU_OK;
-}
 
 }  // namespace
 

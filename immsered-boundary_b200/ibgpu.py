@@ -39,7 +39,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
            "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
-           "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags",
+           "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags", "ibgpu_update_flags_rows",
            "ibgpu_set_state_rows", "ibgpu_build_interfaces", "ibgpu_wall_geometry",
            "ibgpu_wall_distance", "ibgpu_host_register", "ibgpu_host_unregister",
            "ibgpu_wall_distance_near", "ibgpu_wall_fetch")
@@ -437,6 +437,17 @@ class FlowSolver:
         assert len(f) == self.ncells
         _check(lib().ibgpu_update_flags(self._ctx, f.ctypes.data_as(ctypes.c_void_p)),
                "ibgpu_update_flags")
+
+    def update_flags_rows(self, rows, flags):
+        """New flags for some rows only (ibgpu_update_flags_rows): rows[k]
+        gets flags[k], the other rows keep theirs."""
+        r = np.ascontiguousarray(rows, np.int64)
+        f = np.ascontiguousarray(flags, np.uint8)
+        assert len(r) == len(f)
+        _check(lib().ibgpu_update_flags_rows(self._ctx, ctypes.c_int64(len(r)),
+                                             r.ctypes.data_as(ctypes.c_void_p),
+                                             f.ctypes.data_as(ctypes.c_void_p)),
+               "ibgpu_update_flags_rows")
 
     def build_interfaces(self, nlevels: int, level, ix, iy):
         """Coarse/fine interface lists of the mesh whose leaf cells are

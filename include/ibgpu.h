@@ -327,6 +327,15 @@ int ibgpu_wall_forces(ibgpu_ctx *ctx, double *out);
  * IBGPU_E_TOPOLOGY (that needs ibgpu_upload_topology).  The state stays. */
 int ibgpu_update_flags(ibgpu_ctx *ctx, const uint8_t *flags);
 
+/* The same for some of the rows: row rows[k] (an index into the rows of the
+ * last topology upload) gets flags[k], every other row keeps its flags.  A
+ * move changes the flags of the rows near the walls only, so a caller that
+ * knows them sends those (a row may appear twice with the same flags).
+ * IBGPU_E_ARG for a row index out of range; the other codes as
+ * ibgpu_update_flags, and nothing changes on the device when one fails. */
+int ibgpu_update_flags_rows(ibgpu_ctx *ctx, int64_t n, const int64_t *rows,
+                            const uint8_t *flags);
+
 /* Coarse/fine interface lists of an AMR mesh from its leaf cells, built on
  * the device: the part of the regrid's list rebuild (AMR::PerformAdaptive,
  * AMR.cpp:6-209; TagRefineGhost, AMRGhost_refine.cpp:30-98; the pair lists

@@ -53,6 +53,7 @@ def test_null_arguments_are_rejected_without_gpu(pkg):
     assert lib.ibgpu_wall_distance(None, None, 0, None, 0) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_wall_distance_near(None, None, 0, None) == pkg.ibgpu.E_ARG
     assert lib.ibgpu_wall_fetch(None, 0, None) == pkg.ibgpu.E_ARG
+    assert lib.ibgpu_update_flags_rows(None, 0, None, None) == pkg.ibgpu.E_ARG
 
 
 def test_ctypes_layouts_match_c(pkg, tmp_path):

@@ -134,6 +134,39 @@ def test_flag_update_keeps_the_layout(cuda_lib, pkg, snaps):
     sol.close()
 
 
+def test_flag_update_of_the_changed_rows_only(cuda_lib, pkg, snaps):
+    """New flags for the rows whose flags a move changed (each of them
+    sent twice) step the same bits as the full flag update; a row index out
+    of range or a changed layout bit is refused and changes nothing."""
+    ib = pkg.ibgpu
+    a, b = pairs(snaps)[0]
+    old = workloads.naca_lists(make_golden.record_of(a), 0)["flags"]
+    moved = workloads.naca_lists(make_golden.record_of(b, state_from=a), 0)
+    rows = np.flatnonzero(old != moved["flags"])
+    assert len(rows) > 0
+    out = []
+    for full in (True, False):
+        sol = workloads.naca_solver(make_golden.record_of(a), 0, ib.FP64)
+        if full:
+            sol.update_flags(moved["flags"])
+        else:
+            with pytest.raises(ib.IbgpuError) as e:
+                sol.update_flags_rows([0, sol.ncells], moved["flags"][:2])
+            assert e.value.code == ib.E_ARG
+            leaf = int(np.flatnonzero(old & ib.CELL_NORMAL)[0])
+            with pytest.raises(ib.IbgpuError) as e:
+                sol.update_flags_rows([leaf], [int(old[leaf]) & ~ib.CELL_NORMAL & 0xFF])
+            assert e.value.code == ib.E_TOPOLOGY
+            twice = np.r_[rows, rows]
+            sol.update_flags_rows(twice, moved["flags"][twice])
+        sol.upload_ib(moved["ib"], moved["ib_f"], moved["patch"], moved["patch_f"],
+                      moved["body_center"])
+        sol.time_marching(int(a["step"]))
+        out.append(sol.download())
+        sol.close()
+    assert np.array_equal(out[0], out[1])
+
+
 def run_binding(precision, steps=100, ranks=1):
     work = tempfile.mkdtemp(prefix="pitch_binding_")
     log = os.path.join(work, "forces.bin")
