@@ -121,9 +121,38 @@ __device__ __forceinline__ bool valid_pair(const BodiesDev &B, int body, int pat
   return body > -1 && body < B.nbodies && patch > -1 && patch < B.start[body + 1] - B.start[body];
 }
 
-__global__ void walk_kernel(LevelDev L, BodiesDev B, int *err) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= L.n) return;
+// The levels of one call as one index space, so each pass is one launch
+// for every level: level l's boxes at [box0[l], box0[l] + n_l), box0[l] a
+// multiple of kNearBlock (no block of the compaction straddles two
+// levels); its block pairs at [pair0[l], pair0[l + 1]).
+constexpr int kNearBlock = 256;
+constexpr int kMaxWallLevels = 16;
+struct Span {
+  int nlevels;
+  int64_t box0[kMaxWallLevels + 1], pair0[kMaxWallLevels + 1];
+  double band[kMaxWallLevels];  // near-wall report (ibgpu_wall_distance_near)
+};
+
+__device__ __forceinline__ int level_of(const int64_t *start, int nlevels, int64_t g) {
+  int l = 0;
+  while (l + 1 < nlevels && g >= start[l + 1]) ++l;
+  return l;
+}
+
+// box g of the span: its level and index there, false past the level's end
+__device__ __forceinline__ bool span_box(const Span &sp, int64_t g, int &l, int64_t &i,
+                                         const LevelDev *lv) {
+  if (g >= sp.box0[sp.nlevels]) return false;
+  l = level_of(sp.box0, sp.nlevels, g);
+  i = g - sp.box0[l];
+  return i < lv[l].n;
+}
+
+__global__ void walk_kernel(const LevelDev *lv, Span sp, BodiesDev B, int *err) {
+  int l;
+  int64_t i;
+  if (!span_box(sp, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, l, i, lv)) return;
+  const LevelDev &L = lv[l];
   int body = L.body0[i], patch = L.patch0[i];
   double dist = L.dist0[i], sd = L.sd0[i], dtb = L.dtb0[i];
   if (sd < kCriticDis && L.kind[i] != IBGPU_WALL_BOX_BLOCK_GHOST) {
@@ -146,9 +175,11 @@ __global__ void walk_kernel(LevelDev L, BodiesDev B, int *err) {
 // taken when it is on the fluid side where the own one is not, or closer
 // without a worse side (the neighbours in Point_iterator_2d order, each
 // compared with the box's pair as the earlier ones left it).
-__global__ void junction_kernel(LevelDev L, BodiesDev B, int *err) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= L.n) return;
+__global__ void junction_kernel(const LevelDev *lv, Span sp, BodiesDev B, int *err) {
+  int l;
+  int64_t i;
+  if (!span_box(sp, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, l, i, lv)) return;
+  const LevelDev &L = lv[l];
   int body = L.body1[i], patch = L.patch1[i];
   double dist = L.dist1[i], sd = L.sd1[i], dtb = L.dtb1[i];
   if (sd < kCriticDis && L.kind[i] != IBGPU_WALL_BOX_BLOCK_GHOST) {
@@ -188,9 +219,11 @@ __global__ void junction_kernel(LevelDev L, BodiesDev B, int *err) {
   L.dtb2[i] = dtb;
 }
 
-__global__ void finalize_kernel(LevelDev L) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= L.n) return;
+__global__ void finalize_kernel(const LevelDev *lv, Span sp) {
+  int l;
+  int64_t i;
+  if (!span_box(sp, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, l, i, lv)) return;
+  const LevelDev &L = lv[l];
   uint8_t mv = 0;
   double sd = L.sd2[i];
   const uint8_t kind = L.kind[i];
@@ -210,9 +243,12 @@ __global__ void finalize_kernel(LevelDev L) {
 }
 
 // block ghosts: targets are distinct and never origins (checked on upload)
-__global__ void block_kernel(LevelDev L) {
-  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= L.nblock) return;
+__global__ void block_kernel(const LevelDev *lv, Span sp) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= sp.pair0[sp.nlevels]) return;
+  const int l = level_of(sp.pair0, sp.nlevels, g);
+  const LevelDev &L = lv[l];
+  const int64_t k = g - sp.pair0[l];
   const int in = L.block_in[k], out = L.block_out[k];
   L.body2[out] = L.body2[in];
   L.patch2[out] = L.patch2[in];
@@ -232,23 +268,29 @@ __global__ void block_kernel(LevelDev L) {
 }
 
 // The boxes a host re-immersion reads (ibgpu_wall_distance_near): near a
-// wall before or after the move, or on the other side now; compacted in box
-// order (per-block counts, one exclusive scan, a ranked write).
+// wall before or after the move, or on the other side now; compacted in
+// level and box order (per-block counts, one exclusive scan, a ranked
+// write).
 __device__ __forceinline__ bool near_box(const LevelDev &L, int64_t i, double band) {
   return L.moved[i] != 0 || fabs(L.sd2[i]) < band || fabs(L.sd0[i]) < band;
 }
 
-constexpr int kNearBlock = 256;
+__device__ __forceinline__ bool near_flag(const LevelDev *lv, const Span &sp, int64_t g, int &l,
+                                          int64_t &i) {
+  return span_box(sp, g, l, i, lv) && near_box(lv[l], i, sp.band[l]);
+}
 
-__global__ void near_count_kernel(LevelDev L, double band, int *block_count) {
-  const int64_t i = blockIdx.x * (int64_t)kNearBlock + threadIdx.x;
-  const int c = __syncthreads_count(i < L.n && near_box(L, i, band));
+__global__ void near_count_kernel(const LevelDev *lv, Span sp, int *block_count) {
+  int l;
+  int64_t i;
+  const bool f = near_flag(lv, sp, blockIdx.x * (int64_t)kNearBlock + threadIdx.x, l, i);
+  const int c = __syncthreads_count(f);
   if (threadIdx.x == 0) block_count[blockIdx.x] = c;
 }
 
-// one block of 1024 threads: block_count[] becomes its exclusive prefix
-// sums, *total the sum
-__global__ void near_scan_kernel(int *block_count, int nb, int *total) {
+// one block of 1024 threads: block_count[0..nb) becomes its exclusive
+// prefix sums, block_count[nb] the sum
+__global__ void near_scan_kernel(int *block_count, int nb) {
   __shared__ int wsum[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int carry = 0;
@@ -277,21 +319,23 @@ __global__ void near_scan_kernel(int *block_count, int nb, int *total) {
     carry += wsum[31];
     __syncthreads();  // wsum is rewritten by the next chunk
   }
-  if (threadIdx.x == 0) *total = carry;
+  if (threadIdx.x == 0) block_count[nb] = carry;
 }
 
-__global__ void near_write_kernel(LevelDev L, double band, const int *block_base,
+__global__ void near_write_kernel(const LevelDev *lv, Span sp, const int *block_base,
                                   ibgpu_wall_change *out) {
   __shared__ int wcount[kNearBlock / 32];
-  const int64_t i = blockIdx.x * (int64_t)kNearBlock + threadIdx.x;
+  int l;
+  int64_t i;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool f = i < L.n && near_box(L, i, band);
+  const bool f = near_flag(lv, sp, blockIdx.x * (int64_t)kNearBlock + threadIdx.x, l, i);
   const unsigned m = __ballot_sync(0xffffffffu, f);
   if (lane == 0) wcount[warp] = __popc(m);
   __syncthreads();
   if (!f) return;
   int pos = block_base[blockIdx.x] + __popc(m & ((1u << lane) - 1u));
   for (int w = 0; w < warp; ++w) pos += wcount[w];
+  const LevelDev &L = lv[l];
   ibgpu_wall_change c;
   c.box = (int32_t)i;
   c.body = L.body2[i];
@@ -346,12 +390,13 @@ struct Level {
   int64_t n = 0, nblock = 0;
   Buf center, dtdm, neib, kind, block_in, block_out;
   Buf body[3], patch[3], dist[3], sd[3], dtb[3], solid, moved, block_moved;
-  Buf block_count, changes;  // near-wall output (ibgpu_wall_distance_near)
 };
 
 struct State {
   std::vector<Level> levels;
-  Buf start, pc, nv, nbc, nb, err, totals;
+  Buf start, pc, nv, nbc, nb, err;
+  Buf lv;                     // the levels' LevelDev records of a call
+  Buf block_count, changes;   // near-wall report (ibgpu_wall_distance_near)
   bool resident = false;  // every level's last results are its next inputs
 };
 
@@ -408,7 +453,8 @@ int ibgpu_host_unregister(void *ptr) {
 
 int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom *levels) {
   CtxView V;
-  if (!ctx || nlevels < 0 || (nlevels > 0 && !levels) || ctx_view(ctx, &V) != IBGPU_OK)
+  if (!ctx || nlevels < 0 || nlevels > kMaxWallLevels || (nlevels > 0 && !levels) ||
+      ctx_view(ctx, &V) != IBGPU_OK)
     return IBGPU_E_ARG;
   for (int l = 0; l < nlevels; ++l) {
     const ibgpu_wall_level_geom &g = levels[l];
@@ -536,13 +582,35 @@ LevelDev level_dev(Level &L) {
   return D;
 }
 
-// The four passes of one level (walk, junction, caps and move lists, block
-// ghosts) from its input pairs (set 0) to the new ones (set 2).
-int launch_passes(const LevelDev &D, const BodiesDev &B, int *err, cudaStream_t st) {
-  walk_kernel<<<blocks(D.n), 256, 0, st>>>(D, B, err);
-  junction_kernel<<<blocks(D.n), 256, 0, st>>>(D, B, err);
-  finalize_kernel<<<blocks(D.n), 256, 0, st>>>(D);
-  if (D.nblock > 0) block_kernel<<<blocks(D.nblock), 256, 0, st>>>(D);
+// Every level's LevelDev record on the device and the span of the call.
+int level_span(State *S, cudaStream_t st, Span &sp) {
+  const int nl = (int)S->levels.size();
+  std::vector<LevelDev> h((size_t)std::max(nl, 1));
+  sp.nlevels = nl;
+  sp.box0[0] = sp.pair0[0] = 0;
+  for (int l = 0; l < nl; ++l) {
+    Level &L = S->levels[(size_t)l];
+    h[(size_t)l] = level_dev(L);
+    sp.box0[l + 1] = sp.box0[l] + (L.n + kNearBlock - 1) / kNearBlock * kNearBlock;
+    sp.pair0[l + 1] = sp.pair0[l] + L.nblock;
+    sp.band[l] = 0.0;
+  }
+  return put(S->lv, h.data(), std::max(nl, 1), st);
+}
+
+// The four passes of every level (walk, junction, caps and move lists,
+// block ghosts) from the input pairs (set 0) to the new ones (set 2), one
+// launch each.
+int launch_passes(State *S, const Span &sp, const BodiesDev &B, cudaStream_t st) {
+  const LevelDev *lv = S->lv.as<LevelDev>();
+  int *err = S->err.as<int>();
+  const int64_t nbox = sp.box0[sp.nlevels], npair = sp.pair0[sp.nlevels];
+  if (nbox > 0) {
+    walk_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp, B, err);
+    junction_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp, B, err);
+    finalize_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp);
+  }
+  if (npair > 0) block_kernel<<<blocks(npair), 256, 0, st>>>(lv, sp);
   WK(cudaGetLastError());
   return IBGPU_OK;
 }
@@ -606,17 +674,19 @@ int ibgpu_wall_distance(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, int nle
   int rc;
   if ((rc = upload_bodies(S, bodies, st, B))) return rc;
   WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
+  for (int l = 0; l < nlevels && !resident; ++l) {
+    Level &L = S->levels[(size_t)l];
+    const ibgpu_wall_pairs &p = pairs[l];
+    if ((rc = put(L.body[0], p.body, L.n, st)) || (rc = put(L.patch[0], p.patch, L.n, st)) ||
+        (rc = put(L.dist[0], p.distance, L.n, st)) || (rc = put(L.sd[0], p.signdis, L.n, st)) ||
+        (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) || (rc = put(L.solid, p.solid, L.n, st)))
+      return rc;
+  }
+  Span sp;
+  if ((rc = level_span(S, st, sp)) || (rc = launch_passes(S, sp, B, st))) return rc;
   for (int l = 0; l < nlevels; ++l) {
     Level &L = S->levels[(size_t)l];
     ibgpu_wall_pairs &p = pairs[l];
-    if (L.n == 0) continue;
-    if (!resident &&
-        ((rc = put(L.body[0], p.body, L.n, st)) || (rc = put(L.patch[0], p.patch, L.n, st)) ||
-         (rc = put(L.dist[0], p.distance, L.n, st)) || (rc = put(L.sd[0], p.signdis, L.n, st)) ||
-         (rc = put(L.dtb[0], p.distance_to_body, L.n, st)) ||
-         (rc = put(L.solid, p.solid, L.n, st))))
-      return rc;
-    if ((rc = launch_passes(level_dev(L), B, S->err.as<int>(), st))) return rc;
     if ((rc = get(p.body, L.body[2], L.n, st)) || (rc = get(p.patch, L.patch[2], L.n, st)) ||
         (rc = get(p.distance, L.dist[2], L.n, st)) || (rc = get(p.signdis, L.sd[2], L.n, st)) ||
         (rc = get(p.distance_to_body, L.dtb[2], L.n, st)) || (rc = get(p.solid, L.solid, L.n, st)) ||
@@ -653,29 +723,30 @@ int ibgpu_wall_distance_near(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, in
   BodiesDev B;
   int rc;
   if ((rc = upload_bodies(S, bodies, st, B))) return rc;
-  WK(S->totals.reserve(sizeof(int) * (size_t)std::max(nlevels, 1)));
   WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
-  WK(cudaMemsetAsync(S->totals.p, 0, sizeof(int) * (size_t)std::max(nlevels, 1), st));
-  int *totals = S->totals.as<int>();
-  for (int l = 0; l < nlevels; ++l) {
-    Level &L = S->levels[(size_t)l];
-    if (L.n == 0) continue;
-    const LevelDev D = level_dev(L);
-    if ((rc = launch_passes(D, B, S->err.as<int>(), st))) return rc;
-    const int nb = (int)((L.n + kNearBlock - 1) / kNearBlock);
-    WK(L.block_count.reserve(sizeof(int) * (size_t)nb));
-    WK(L.changes.reserve(sizeof(ibgpu_wall_change) * (size_t)L.n));
-    const double band = levels[l].band;
-    near_count_kernel<<<nb, kNearBlock, 0, st>>>(D, band, L.block_count.as<int>());
-    near_scan_kernel<<<1, 1024, 0, st>>>(L.block_count.as<int>(), nb, totals + l);
-    near_write_kernel<<<nb, kNearBlock, 0, st>>>(D, band, L.block_count.as<int>(),
-                                                 L.changes.as<ibgpu_wall_change>());
-    WK(cudaGetLastError());
-    if ((rc = get(levels[l].block_moved, L.block_moved, L.nblock, st))) return rc;
-  }
-  std::vector<int> count((size_t)std::max(nlevels, 1), 0);
+  Span sp;
+  if ((rc = level_span(S, st, sp))) return rc;
+  for (int l = 0; l < nlevels; ++l) sp.band[l] = levels[l].band;
+  if ((rc = launch_passes(S, sp, B, st))) return rc;
+  const int64_t nbox = sp.box0[nlevels];
+  const int nb = (int)(nbox / kNearBlock);
+  WK(S->block_count.reserve(sizeof(int) * ((size_t)nb + 1)));
+  WK(S->changes.reserve(sizeof(ibgpu_wall_change) * (size_t)std::max<int64_t>(nbox, 1)));
+  int *base = S->block_count.as<int>();
+  if (nb > 0) near_count_kernel<<<nb, kNearBlock, 0, st>>>(S->lv.as<LevelDev>(), sp, base);
+  near_scan_kernel<<<1, 1024, 0, st>>>(base, nb);
+  if (nb > 0)
+    near_write_kernel<<<nb, kNearBlock, 0, st>>>(S->lv.as<LevelDev>(), sp, base,
+                                                 S->changes.as<ibgpu_wall_change>());
+  WK(cudaGetLastError());
+  for (int l = 0; l < nlevels; ++l)
+    if ((rc = get(levels[l].block_moved, S->levels[(size_t)l].block_moved,
+                  S->levels[(size_t)l].nblock, st)))
+      return rc;
+  // each level's first block's offset (and the total) from the scan
+  std::vector<int> hbase((size_t)nb + 1, 0);
   int herr = 0;
-  WK(cudaMemcpyAsync(count.data(), totals, sizeof(int) * (size_t)nlevels, cudaMemcpyDeviceToHost,
+  WK(cudaMemcpyAsync(hbase.data(), base, sizeof(int) * ((size_t)nb + 1), cudaMemcpyDeviceToHost,
                      st));
   WK(cudaMemcpyAsync(&herr, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   WK(cudaStreamSynchronize(st));
@@ -683,12 +754,16 @@ int ibgpu_wall_distance_near(ibgpu_ctx *ctx, const ibgpu_wall_bodies *bodies, in
   bool fits = true;
   for (int l = 0; l < nlevels; ++l) {
     ibgpu_wall_near &o = levels[l];
-    o.count = count[(size_t)l];
+    const int64_t first = hbase[(size_t)(sp.box0[l] / kNearBlock)];
+    o.count = hbase[(size_t)(sp.box0[l + 1] / kNearBlock)] - first;
     if (o.count > o.capacity) {
       fits = false;
       continue;
     }
-    if ((rc = get(o.changes, S->levels[(size_t)l].changes, o.count, st))) return rc;
+    if (o.count > 0)
+      WK(cudaMemcpyAsync(o.changes, S->changes.as<ibgpu_wall_change>() + first,
+                         sizeof(ibgpu_wall_change) * (size_t)o.count, cudaMemcpyDeviceToHost,
+                         st));
   }
   WK(cudaStreamSynchronize(st));
   rc = settle(S, 0);
