@@ -75,6 +75,17 @@ inline IbgpuMoveTimes &ibgpu_move_times() {
   return t;
 }
 
+// Seconds spent in GpuNS_Solver::Upload after regrids (this rank):
+// flattening the mesh into the device lists (device rank), the lists'
+// upload, and the wall geometry (windows, packing, the device call).
+struct IbgpuUploadTimes {
+  double flatten = 0.0, lists = 0.0, wall_geometry = 0.0;
+};
+inline IbgpuUploadTimes &ibgpu_upload_times() {
+  static IbgpuUploadTimes t;
+  return t;
+}
+
 // The rank that drives the device: rank 0 of the node (share_comm,
 // mpiparams.cpp:68-105).
 inline bool ibgpu_device_rank() { return srank == 0; }
@@ -90,9 +101,18 @@ inline int ibgpu_share_status(int rc) {
 struct IbgpuSharedBytes {
   MPI_Win win;
   char *base = nullptr;
+  size_t cap = 0;
   bool live = false, pinned = false;
+  // at least nbytes: the buffer stays when it is large enough (a regrid
+  // changes the box counts a little; a new window and its pinning cost far
+  // more than the copies), else a new one with a quarter to spare
+  void ensure(size_t nbytes, bool pin) {
+    if (live && nbytes <= cap) return;  // the same decision on every rank (collective)
+    alloc(nbytes + nbytes / 4, pin);
+  }
   void alloc(size_t nbytes, bool pin) {
     release();
+    cap = nbytes;
     char *local = nullptr;
     MPI_Win_allocate_shared(srank == 0 ? (MPI_Aint)nbytes : 0, 1, MPI_INFO_NULL, share_comm,
                             &local, &win);
@@ -107,6 +127,7 @@ struct IbgpuSharedBytes {
     if (live) MPI_Win_free(&win);
     live = pinned = false;
     base = nullptr;
+    cap = 0;
   }
 };
 
@@ -139,7 +160,7 @@ struct IbgpuWallLevel {
                  obi = take(4 * nblock), obu = take(4 * nblock), oki = take(n), oso = take(n),
                  omo = take(n), obm = take(nblock), och = take(sizeof(ibgpu_wall_change) * n),
                  onc = take(sizeof(int64_t));
-    mem.alloc(off, true);
+    mem.ensure(off, true);
     char *b = mem.base;
     center = (double *)(b + oc);
     dtdm = (double *)(b + odm);
@@ -471,9 +492,10 @@ struct IbgpuAdapter {
   // kinds, distances to the domain boundary) and block pairs into the
   // levels' exchange buffers and the device.
   static int WallGeometry(ibgpu_ctx *ctx, Mesh &mesh, std::vector<IbgpuWallLevel> &W) {
-    for (auto &L : W) L.mem.release();
     const int nlev = mesh.MyCurNum();
-    W.clear();
+    // the levels' windows stay from the last regrid where they are large
+    // enough (every rank computes the same sizes, so all keep or renew alike)
+    for (size_t l = (size_t)nlev; l < W.size(); ++l) W[l].mem.release();
     W.resize(nlev);
     for (int l = 0; l < nlev; ++l) {
       DataArray<Box> &boxes = mesh.ShowLevelBox(l);
@@ -869,16 +891,24 @@ class GpuNS_Solver : public NS_Solver {
   int Upload(AMR &amr, std::vector<Body> &bodies) {
     if (!created_) return IBGPU_E_STATE;
     MPI_Barrier(share_comm);  // every rank's share of the arrays written
+    IbgpuUploadTimes &tu = ibgpu_upload_times();
+    double t0 = MPI_Wtime();
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
+      const double t1 = MPI_Wtime();
+      tu.flatten += t1 - t0;
+      t0 = t1;
       rc = IbgpuAdapter::Upload(ctx_, lists_);
     }
     rc = ibgpu_share_status(rc);
+    tu.lists += MPI_Wtime() - t0;
+    t0 = MPI_Wtime();
     if (rc == IBGPU_OK && device_distance_ && Body::Bodynum() > 0) {
       rc = IbgpuAdapter::WallGeometry(ctx_, a_mesh, wall_);
       wall_resident_ = false;  // the regrid's own pairs go up with the next move
     }
+    tu.wall_geometry += MPI_Wtime() - t0;
     if (rc == IBGPU_OK && sprocs > 1) {
       // every rank learns the cell rows (level, box index), to share the
       // per-row flag pass of UploadImmersion

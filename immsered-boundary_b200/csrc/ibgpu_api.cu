@@ -392,8 +392,8 @@ __global__ void flags_scatter_kernel(const uint8_t *rows, const int64_t *which,
   }
 }
 
-// ... which tiles hold only recovering leaf cells (one warp per tile, eight
-// slots per lane) ...
+// ... which tiles hold only leaf cells that update and recover their
+// primitives (one warp per tile, eight slots per lane) ...
 __global__ void tile_full_kernel(const uint8_t *flags, int64_t ntiles, uint8_t *full) {
   constexpr uint64_t kFull8 = 0x0101010101010101ull *
                               (uint64_t)(CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM);
@@ -404,8 +404,9 @@ __global__ void tile_full_kernel(const uint8_t *flags, int64_t ntiles, uint8_t *
   if ((threadIdx.x & 31) == 0) full[t] = all ? 1 : 0;
 }
 
-// ... and the uniform tiles: full, with four full side neighbours (as
-// uniform_tiles on the host).
+// ... and the uniform tiles: full, with four full side neighbours (the
+// stage kernel then needs no presence flags and no one-sided stencils).
+// The topology upload makes them with the same two kernels.
 __global__ void tile_uniform_kernel(const uint8_t *full, const int32_t *nb, int64_t ntiles,
                                     uint8_t *uniform) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -416,6 +417,53 @@ __global__ void tile_uniform_kernel(const uint8_t *full, const int32_t *nb, int6
     u = n >= 0 && full[n] != 0;
   }
   uniform[t] = u ? 1 : 0;
+}
+
+// Every stencil a face of a leaf cell reads must exist (NS_Solver.H:738-756,
+// NS_Solver.cpp:410-424), checked per slot on the device over the tile
+// neighbour table (which wraps periodic directions): per face direction d
+// the face neighbour (check 0), one of the two outer MUSCL neighbours
+// (check 1), and with viscosity the four tangential neighbours (check 2).
+// The smallest (slot, d, check) that fails goes to *first as
+// slot * 16 + d * 4 + check (~0 when none fails).
+__device__ __forceinline__ bool slot_present(const uint8_t *flags, const int32_t *nb, int64_t t,
+                                             int lx, int ly, int dx, int dy) {
+  const int nx = lx + dx, ny = ly + dy;  // |dx|, |dy| <= 2: at most the next tile
+  const int ox = nx < 0 ? -1 : (nx >= kTile ? 1 : 0), oy = ny < 0 ? -1 : (ny >= kTile ? 1 : 0);
+  const int64_t tile = (ox == 0 && oy == 0) ? t : nb[t * 9 + (oy + 1) * 3 + (ox + 1)];
+  if (tile < 0) return false;
+  return (flags[tile * kTileCells + (ny - oy * kTile) * kTile + (nx - ox * kTile)] & CF_PRESENT) != 0;
+}
+
+__global__ void stencil_check_kernel(const uint8_t *flags, const int32_t *nb, int64_t nslots,
+                                     int viscous, unsigned long long *first) {
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < nslots;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    if (!(flags[s] & CF_NORMAL)) continue;
+    const int64_t t = s / kTileCells;
+    const int lx = (int)(s % kTile), ly = (int)((s / kTile) % kTile);
+    for (int d = 0; d < 4; ++d) {
+      const int dx = d == 0 ? -1 : d == 1 ? 1 : 0, dy = d == 2 ? -1 : d == 3 ? 1 : 0;
+      int bad = -1;
+      if (!slot_present(flags, nb, t, lx, ly, dx, dy)) {
+        bad = 0;
+      } else if (!slot_present(flags, nb, t, lx, ly, -dx, -dy) &&
+                 !slot_present(flags, nb, t, lx, ly, 2 * dx, 2 * dy)) {
+        bad = 1;
+      } else if (viscous) {
+        const int tx = dy != 0 ? 1 : 0, ty = dx != 0 ? 1 : 0;
+        if (!slot_present(flags, nb, t, lx, ly, tx, ty) ||
+            !slot_present(flags, nb, t, lx, ly, -tx, -ty) ||
+            !slot_present(flags, nb, t, lx, ly, dx + tx, dy + ty) ||
+            !slot_present(flags, nb, t, lx, ly, dx - tx, dy - ty))
+          bad = 2;
+      }
+      if (bad >= 0) {
+        atomicMin(first, (unsigned long long)s * 16ull + (unsigned long long)(d * 4 + bad));
+        break;
+      }
+    }
+  }
 }
 
 }  // namespace
@@ -481,29 +529,6 @@ int ibgpu_set_stream(ibgpu_ctx *ctx, void *stream) {
 // bit of a row, never these.
 static const uint8_t kLayoutBits = IBGPU_CELL_PRESENT | IBGPU_CELL_NORMAL | IBGPU_CELL_ALIAS;
 
-// Uniform tiles: the tile and its four side neighbours hold only leaf cells
-// that update and recover their primitives (the stage kernel then needs no
-// presence flags and no one-sided stencils).
-static std::vector<uint8_t> uniform_tiles(const std::vector<uint8_t> &slot_flags,
-                                          const std::vector<int32_t> &nb, int64_t ntiles) {
-  const uint8_t kFull = CF_PRESENT | CF_NORMAL | CF_UPDATE | CF_PRIM | CF_RESNORM;
-  std::vector<uint8_t> tile_full(ntiles, 0), uniform(ntiles, 0);
-  for (int64_t t = 0; t < ntiles; ++t) {
-    bool full = true;
-    for (int i = 0; i < kTileCells && full; ++i) full = slot_flags[t * kTileCells + i] == kFull;
-    tile_full[t] = full;
-  }
-  for (int64_t t = 0; t < ntiles; ++t) {
-    bool u = tile_full[t];
-    for (int k : {1, 3, 5, 7}) {
-      int n = nb[t * 9 + k];
-      u = u && n >= 0 && tile_full[n];
-    }
-    uniform[t] = u;
-  }
-  return uniform;
-}
-
 int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   if (!ctx || !cells || cells->n < 0 || (cells->n > 0 && (!cells->level || !cells->ix ||
                                                           !cells->iy || !cells->flags)))
@@ -520,11 +545,19 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   ctx->chain_steps = 0;
   ctx->free_layout();
 
-  // 1. owners vs aliases; tiles per level
+  // 1. owners vs aliases; each level's tiles in a dense index over the
+  //    bounding box of its owner cells' tiles (-1: no tile)
   std::vector<uint8_t> alias(n, 0);
-  std::vector<std::unordered_map<uint64_t, int>> tilemap(nlev);
-  std::vector<std::vector<std::pair<int, int>>> tiles(nlev);
-  std::vector<int> minx(nlev, 1 << 30), miny(nlev, 1 << 30);
+  struct Grid {
+    int x0 = 1 << 30, y0 = 1 << 30, x1 = -(1 << 30), y1 = -(1 << 30), w = 0;
+    std::vector<int> idx;
+    int at(int tx, int ty) const {
+      if (tx < x0 || ty < y0 || tx > x1 || ty > y1) return -1;
+      return idx[(size_t)(ty - y0) * w + (tx - x0)];
+    }
+    int &ref(int tx, int ty) { return idx[(size_t)(ty - y0) * w + (tx - x0)]; }
+  };
+  std::vector<Grid> grid(nlev);
   for (int64_t c = 0; c < n; ++c) {
     int l = cells->level[c];
     if (l < 0 || l >= nlev) { g_last_error = "cell level out of range"; return IBGPU_E_ARG; }
@@ -537,13 +570,27 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       alias[c] = 1;
       continue;
     }
-    int tx = floordiv(ix, kTile), ty = floordiv(iy, kTile);
-    uint64_t k = key2(tx, ty);
-    if (!tilemap[l].count(k)) {
-      tilemap[l][k] = -1;
+    Grid &g = grid[l];
+    const int tx = floordiv(ix, kTile), ty = floordiv(iy, kTile);
+    g.x0 = std::min(g.x0, tx);
+    g.y0 = std::min(g.y0, ty);
+    g.x1 = std::max(g.x1, tx);
+    g.y1 = std::max(g.y1, ty);
+  }
+  for (Grid &g : grid)
+    if (g.x1 >= g.x0) {
+      g.w = g.x1 - g.x0 + 1;
+      g.idx.assign((size_t)g.w * (g.y1 - g.y0 + 1), -1);
+    }
+  std::vector<std::vector<std::pair<int, int>>> tiles(nlev);
+  for (int64_t c = 0; c < n; ++c) {
+    if (alias[c]) continue;
+    const int l = cells->level[c];
+    const int tx = floordiv(cells->ix[c], kTile), ty = floordiv(cells->iy[c], kTile);
+    int &e = grid[l].ref(tx, ty);
+    if (e == -1) {
+      e = -2;
       tiles[l].push_back({tx, ty});
-      minx[l] = std::min(minx[l], tx);
-      miny[l] = std::min(miny[l], ty);
     }
   }
   for (int l = 0; l < nlev; ++l) {
@@ -559,16 +606,19 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   ctx->level_tile_count.assign(nlev, 0);
   std::vector<int32_t> h_tile_level;
   std::vector<std::pair<int, int>> tile_pos;
+  std::vector<std::unordered_map<uint64_t, int>> tilemap(nlev);
   for (int l = 0; l < nlev; ++l) {
     auto &tl = tiles[l];
-    int mx = minx[l], my = miny[l];
+    int mx = grid[l].x0, my = grid[l].y0;
     std::sort(tl.begin(), tl.end(), [mx, my](const std::pair<int, int> &a, const std::pair<int, int> &b) {
       return morton2((uint32_t)(a.first - mx), (uint32_t)(a.second - my)) <
              morton2((uint32_t)(b.first - mx), (uint32_t)(b.second - my));
     });
     ctx->level_tile_begin[l] = (int)h_tile_level.size();
     ctx->level_tile_count[l] = (int)tl.size();
+    tilemap[l].reserve(tl.size());
     for (auto &t : tl) {
+      grid[l].ref(t.first, t.second) = (int)h_tile_level.size();
       tilemap[l][key2(t.first, t.second)] = (int)h_tile_level.size();
       h_tile_level.push_back(l);
       tile_pos.push_back(t);
@@ -587,8 +637,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
         int tx = tile_pos[t].first + ox, ty = tile_pos[t].second + oy;
         if (cs.periodic_x) tx = ((tx % ntx) + ntx) % ntx;
         if (cs.periodic_y) ty = ((ty % nty) + nty) % nty;
-        auto it = tilemap[l].find(key2(tx, ty));
-        h_nb[t * 9 + (oy + 1) * 3 + (ox + 1)] = (it == tilemap[l].end()) ? -1 : it->second;
+        h_nb[t * 9 + (oy + 1) * 3 + (ox + 1)] = grid[l].at(tx, ty);
       }
   }
   // 4. slots of owner cells, then aliases
@@ -600,9 +649,9 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   ctx->level_normal_cells.assign(nlev, 0);
   auto slot_of = [&](int l, int ix, int iy) -> int64_t {
     int tx = floordiv(ix, kTile), ty = floordiv(iy, kTile);
-    auto it = tilemap[l].find(key2(tx, ty));
-    if (it == tilemap[l].end() || it->second < 0) return -1;
-    return (int64_t)it->second * kTileCells + (iy - ty * kTile) * kTile + (ix - tx * kTile);
+    const int t = grid[l].at(tx, ty);
+    if (t < 0) return -1;
+    return (int64_t)t * kTileCells + (iy - ty * kTile) * kTile + (ix - tx * kTile);
   };
   for (int64_t c = 0; c < n; ++c) {
     if (alias[c]) continue;
@@ -627,41 +676,8 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
     if (s < 0 || !h_flags[s]) { g_last_error = "periodic ghost without a source cell"; return IBGPU_E_TOPOLOGY; }
     cell_slot[c] = (int32_t)s;
   }
-  // 5. the stencils every face of a leaf cell reads must exist
-  //    (NS_Solver.H:738-756, NS_Solver.cpp:410-424)
-  auto present = [&](int l, int ix, int iy) -> bool {
-    int ex = cs.domain_nx << l, ey = cs.domain_ny << l;
-    if (cs.periodic_x) ix = ((ix % ex) + ex) % ex;
-    if (cs.periodic_y) iy = ((iy % ey) + ey) % ey;
-    int64_t s = slot_of(l, ix, iy);
-    return s >= 0 && (h_flags[s] & CF_PRESENT);
-  };
-  for (int64_t s = 0; s < nslots; ++s) {
-    if (!(h_flags[s] & CF_NORMAL)) continue;
-    int l = ctx->h_slot_level[s], ix = ctx->h_slot_ix[s], iy = ctx->h_slot_iy[s];
-    for (int d = 0; d < 4; ++d) {
-      int dx = d == 0 ? -1 : d == 1 ? 1 : 0, dy = d == 2 ? -1 : d == 3 ? 1 : 0;
-      if (!present(l, ix + dx, iy + dy)) {
-        g_last_error = "leaf cell with a missing face neighbour";
-        return IBGPU_E_TOPOLOGY;
-      }
-      // MUSCL: at least one outer neighbour of the face stencil
-      if (!present(l, ix - dx, iy - dy) && !present(l, ix + 2 * dx, iy + 2 * dy)) {
-        g_last_error = "face stencil with neither outer neighbour";
-        return IBGPU_E_TOPOLOGY;
-      }
-      if (cs.viscous) {
-        int tx = dy != 0 ? 1 : 0, ty = dx != 0 ? 1 : 0;
-        if (!present(l, ix + tx, iy + ty) || !present(l, ix - tx, iy - ty) ||
-            !present(l, ix + dx + tx, iy + dy + ty) || !present(l, ix + dx - tx, iy + dy - ty)) {
-          g_last_error = "viscous stencil with a missing cell";
-          return IBGPU_E_TOPOLOGY;
-        }
-      }
-    }
-  }
-  // 6. uniform tiles (see uniform_tiles)
-  std::vector<uint8_t> h_uniform = uniform_tiles(h_flags, h_nb, ntiles);
+  // 5. (the stencils of the leaf cells and 6. the uniform tiles are made on
+  //    the device below)
   // 7. device arrays
   int rc;
   if ((rc = dev_alloc(&ctx->d_tile_nb, h_nb.size())) ||
@@ -674,7 +690,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       (rc = dev_alloc(&ctx->d_cell_layout, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_row_flags, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_tile_full, (size_t)ntiles)) ||
-      (rc = dev_alloc(&ctx->d_layout_err, (size_t)1)) ||
+      (rc = dev_alloc(&ctx->d_layout_err, (size_t)2)) ||  // also the stencil check's key
       (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)))
     return rc;
   for (int f = 0; f < kStateFields; ++f)
@@ -691,9 +707,32 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   std::vector<int2> h_org(ntiles);
   for (int64_t t = 0; t < ntiles; ++t)
     h_org[t] = make_int2(tile_pos[t].first * kTile, tile_pos[t].second * kTile);
-  if (ntiles > 0) {
-    CK(cudaMemcpyAsync(ctx->d_tile_uniform, h_uniform.data(), ntiles, cudaMemcpyHostToDevice, st));
+  if (ntiles > 0)
     CK(cudaMemcpyAsync(ctx->d_tile_org, h_org.data(), ntiles * sizeof(int2), cudaMemcpyHostToDevice, st));
+  // 5. every stencil a face of a leaf cell reads exists (stencil_check_kernel)
+  if (nslots > 0) {
+    const unsigned long long none = ~0ull;
+    unsigned long long first = none;
+    unsigned long long *d_first = reinterpret_cast<unsigned long long *>(ctx->d_layout_err);
+    CK(cudaMemcpyAsync(d_first, &none, sizeof(none), cudaMemcpyHostToDevice, st));
+    stencil_check_kernel<<<4 * ctx->nsm, 256, 0, st>>>(ctx->d_flags, ctx->d_tile_nb, nslots,
+                                                       cs.viscous != 0, d_first);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&first, d_first, sizeof(first), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (first != none) {
+      const int check = (int)(first & 3);
+      g_last_error = check == 0 ? "leaf cell with a missing face neighbour"
+                     : check == 1 ? "face stencil with neither outer neighbour"
+                                  : "viscous stencil with a missing cell";
+      return IBGPU_E_TOPOLOGY;
+    }
+    // 6. uniform tiles: full tiles whose four side neighbours are full
+    tile_full_kernel<<<(unsigned)((ntiles * 32 + 255) / 256), 256, 0, st>>>(ctx->d_flags, ntiles,
+                                                                            ctx->d_tile_full);
+    tile_uniform_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(
+        ctx->d_tile_full, ctx->d_tile_nb, ntiles, ctx->d_tile_uniform);
+    CK(cudaGetLastError());
   }
   if (n > 0) {
     CK(cudaMemcpyAsync(ctx->d_cell_slot, cell_slot.data(), n * 4, cudaMemcpyHostToDevice, st));

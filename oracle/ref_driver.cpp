@@ -588,7 +588,11 @@ int main(int argc, char **argv) {
   };
   if (dump_now(0, false)) do_dump(0);
 
-  double loop_time = 0.0, move_time = 0.0;
+  // loop_time: the timed steps (motion and re-immersion, the step); the
+  // regrids between them (tagging, mesh adaptation and, through the binding,
+  // the download before and the upload after) in regrid_time
+  double loop_time = 0.0, move_time = 0.0, regrid_time = 0.0;
+  double rg_tag = 0.0, rg_download = 0.0, rg_adapt = 0.0, rg_upload = 0.0;  // regrid parts
   long long cell_updates = 0;
   for (int s = 0; s < nsteps; ++s) {
     // leaf cells of the levels that march this step (subcycling schedule)
@@ -634,9 +638,15 @@ int main(int argc, char **argv) {
       std::fwrite(head, sizeof(double), 3, flog);
       if (!forces.empty()) std::fwrite(forces.data(), sizeof(double), forces.size(), flog);
     }
+    MPI_Barrier(MPI_COMM_WORLD);
+    const double tr0 = MPI_Wtime();
+    const bool timed_regrid = s >= timed_from && s + 1 < nsteps;
     amr.ADPRule(sphere);
+    const double tr1 = MPI_Wtime();
+    double tr2 = tr1, tr3 = tr1;
 #ifdef ORACLE_BINDING
     if (adpflag && gpu_step) gpu_check(flowsolver.Download(), "download");
+    tr2 = tr3 = MPI_Wtime();
 #endif
     if (adpflag) {
       // a tag server decides from the state it sees here (case file)
@@ -647,9 +657,21 @@ int main(int argc, char **argv) {
         std::rename((path + ".part").c_str(), path.c_str());
       }
       amr.PerformAdaptive(sphere);
+      tr3 = MPI_Wtime();
 #ifdef ORACLE_BINDING
       if (gpu_step) gpu_check(flowsolver.Upload(amr, sphere), "upload");
 #endif
+    }
+    MPI_Barrier(MPI_COMM_WORLD);
+    if (timed_regrid) {
+      const double tr4 = MPI_Wtime();
+      regrid_time += tr4 - tr0;
+      if (adpflag) {
+        rg_tag += tr1 - tr0;
+        rg_download += tr2 - tr1;
+        rg_adapt += tr3 - tr2;
+        rg_upload += tr4 - tr3;
+      }
     }
     adpflag = false;
     if (prefix && dump_now(ts, s == nsteps - 1)) do_dump(ts);
@@ -664,7 +686,25 @@ int main(int argc, char **argv) {
 #endif
     pltfile.Output_Soln_Nobody(plt);
   }
-  std::string phases = "{}";
+  std::string phases = "{}", rphases;
+  {
+    // the timed regrids' parts on rank 0: tagging (ADPRule), reading the
+    // device state back, the reference's PerformAdaptive, the upload
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "{\"tag\": %.6f, \"download\": %.6f, \"adapt\": %.6f, \"upload\": %.6f",
+                  rg_tag, rg_download, rg_adapt, rg_upload);
+    rphases = buf;
+#ifdef ORACLE_BINDING
+    const IbgpuUploadTimes &ut = ibgpu_upload_times();
+    std::snprintf(buf, sizeof buf,
+                  ", \"upload_flatten_all\": %.6f, \"upload_lists_all\": %.6f, "
+                  "\"upload_wall_geometry_all\": %.6f",
+                  ut.flatten, ut.lists, ut.wall_geometry);
+    rphases += buf;
+#endif
+    rphases += "}";
+  }
 #ifdef ORACLE_BINDING
   {
     // moving-body phases on rank 0, all steps (warm-up included)
@@ -682,10 +722,11 @@ int main(int argc, char **argv) {
   if (nrank == 0)
     std::printf("ORACLE_RESULT {\"steps\": %d, \"loop_seconds\": %.9f, \"cell_updates\": %lld, "
                 "\"cell_updates_per_s\": %.6e, \"t\": %.17g, \"dt\": %.17g, "
-                "\"move_seconds\": %.9f, \"ranks\": %d, \"move_phases_seconds\": %s}\n",
+                "\"move_seconds\": %.9f, \"regrid_seconds\": %.9f, \"ranks\": %d, "
+                "\"move_phases_seconds\": %s, \"regrid_phases_seconds\": %s}\n",
                 nsteps - timed_from, loop_time, cell_updates,
-                loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time, nprocs,
-                phases.c_str());
+                loop_time > 0 ? (double)cell_updates / loop_time : 0.0, t, dt, move_time,
+                regrid_time, nprocs, phases.c_str(), rphases.c_str());
   std::fflush(stdout);
   MPI_Finalize();
   return 0;

@@ -311,6 +311,22 @@ def test_topology_errors(cuda_lib, pkg):
     with pytest.raises(ib.IbgpuError) as ei:
         sol.upload_topology(**cells)
     assert ei.value.code == ib.E_TOPOLOGY
+    assert "missing face neighbour" in str(ei.value)
+    # a west face whose outer MUSCL neighbours are both missing: a column of
+    # leaves with one ghost column to the west and nothing to the east
+    leaf = ib.CELL_PRESENT | ib.CELL_NORMAL | ib.CELL_UPDATE | ib.CELL_PRIM | ib.CELL_RESNORM
+    lv, xs, ys, fl = [], [], [], []
+    for iy in range(32):
+        for ix, f in ((-1, ib.CELL_PRESENT), (0, leaf)):
+            lv.append(0)
+            xs.append(ix)
+            ys.append(iy)
+            fl.append(f)
+    sol = ib.FlowSolver(P2)
+    with pytest.raises(ib.IbgpuError) as ei:
+        sol.upload_topology(np.array(lv), np.array(xs), np.array(ys), np.array(fl))
+    assert ei.value.code == ib.E_TOPOLOGY
+    assert "neither outer neighbour" in str(ei.value)
     # step before any state
     sol = ib.FlowSolver(P)
     sol.upload_topology(**cells)
