@@ -1015,6 +1015,13 @@ def our_arm(args):
     with near_gpu_cores(torch.cuda.current_device()) as e2e_cores:
         host_in = torch.from_numpy(np.ascontiguousarray(prim[:, [0, 1, 2, 4]])).pin_memory()
         host_out = torch.empty_like(host_in).pin_memory()
+        # warm-up of the pipelined path (untimed), as for the device-timed line
+        for s in range(2):
+            sol.upload_async(host_in.data_ptr())
+            sol.step_async(s)
+            sol.download_async(host_out.data_ptr())
+        sol.step_result()
+        sol.synchronize()
         barrier()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)

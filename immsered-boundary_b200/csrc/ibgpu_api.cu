@@ -691,7 +691,10 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
       (rc = dev_alloc(&ctx->d_row_flags, (size_t)n)) ||
       (rc = dev_alloc(&ctx->d_tile_full, (size_t)ntiles)) ||
       (rc = dev_alloc(&ctx->d_layout_err, (size_t)2)) ||  // also the stencil check's key
-      (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)))
+      (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)) ||
+      // staging of asynchronous downloads, here so that the first one in a
+      // pipelined loop does not allocate (and wait for the device)
+      (rc = dev_alloc(&ctx->d_rows_out, (size_t)n * 7)))
     return rc;
   for (int f = 0; f < kStateFields; ++f)
     if ((rc = dev_alloc(&ctx->d_s0[f], (size_t)nslots))) return rc;
@@ -920,10 +923,6 @@ int ibgpu_download_state_async(ibgpu_ctx *ctx, double *prim) {
   if (!ctx || (!prim && ctx->ncells > 0)) return IBGPU_E_ARG;
   if (!ctx->has_state) return IBGPU_E_STATE;
   if (ctx->ncells == 0) return IBGPU_OK;
-  if (!ctx->d_rows_out) {
-    int rc = dev_alloc(&ctx->d_rows_out, (size_t)ctx->ncells * 7);
-    if (rc) return rc;
-  }
   CK(cudaEventRecord(ctx->ev_ready, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
   gather_rows(ctx, ctx->d_rows_out, ctx->copy_stream);
