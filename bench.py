@@ -513,7 +513,8 @@ def batched_section(args, ib, wl, stream, barrier, max_over_ranks, ws, rank):
            "cases": BATCH_CASES, "leaf_cells_total": total, "leaf_cells_min": min(sizes),
            "leaf_cells_max": max(sizes), "dtype": "f32 flux/limiter, f64 accumulation",
            "scaling": "strong", "sharding": "cases, largest first, no collective",
-           "persistent_ctas": info["grid"], "autotune_ms": info["tuning"],
+           "persistent_ctas": info["grid"], "block_threads": info["threads"],
+           "autotune_ms": info["tuning"],
            "stage_ms_per_launch": info["stage_ms"] / max(info["stage_launches"], 1),
            "workload": "periodic vortex cases, side 16k with n^2 log-uniform in [5e4, 8e5], "
                        "Mach U[0.1,0.8], direction U[-5,10] deg (seed 0), single level"}
@@ -861,7 +862,8 @@ def config4_section(ib, wl, ind, stream, ncases: int, steps: int, warm: int = 4)
         ms = ev0.elapsed_time(ev1)
         info = b.info()
         out[name] = {"value": per_step * steps / (ms / 1e3), "unit": UNIT,
-                     "ms_per_step": ms / steps, "persistent_ctas": info["grid"]}
+                     "ms_per_step": ms / steps, "persistent_ctas": info["grid"],
+                     "block_threads": info["threads"]}
         forces[name] = [s.wall_forces()[:, :2].sum(axis=0) / F_REF for s in sols]
         if name == "mixed":
             # tagging of every box of every case: learned (an untrained

@@ -1398,10 +1398,12 @@ struct ibgpu_batch {
   int *h_err = nullptr;  // pinned: the cases' time-out flags (batch tagging)
   std::vector<cudaEvent_t> ev_tag;  // batch tagging: per case, + the fork
   int fixed_grid = -1;  // >= 0: CTA count set by the caller (no autotuning)
+  int threads = 0;        // threads per CTA of the merged stage launch (256 / 288)
+  int fixed_threads = 0;  // set by the caller (0: autotuned)
   bool timing = false;
   double stage_ms = 0.0;
   int64_t stage_launches = 0;
-  std::vector<int> tune_grid;
+  std::vector<int> tune_grid, tune_threads;
   std::vector<float> tune_ms;
 
   void drop_graphs() {
@@ -1461,7 +1463,7 @@ int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
   for (int k = 0; k < b->nstages; ++k) {
     fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], k, b->nstages,
                              b->d_phase_base, b->limiter, b->visc, k == b->nstages - 1, b->mixed,
-                             b->grid, b->table, st);
+                             b->grid, b->threads, b->table, st);
     CK(cudaGetLastError());
   }
   return IBGPU_OK;
@@ -1471,48 +1473,76 @@ int enqueue_batch_stages(ibgpu_batch *b, int r, int cfl, cudaStream_t st) {
 // candidate CTA count (one CTA per item, or 1..6 resident CTAs per SM) and
 // keep the fastest.  Runs before the run's diag is initialised; it writes
 // only the first stage buffer, which stage 0 of every step rewrites.
+// Threads per CTA of the merged stage launch by default: 288 for FP64 (a
+// ninth warp owns the tile's edge faces), 256 for the mixed build.
+int default_threads(const ibgpu_batch *b) { return b->mixed ? kTileCells : kTileCells + 32; }
+
+// The merged stage launch's shape from timed candidates on the busiest
+// phase's work list: the CTA count (one CTA per work item, or 1..4 (FP64) /
+// 1..6 (mixed) persistent CTAs per SM) and the block (256 or 288 threads),
+// each unless the caller fixed it.
 int autotune(ibgpu_batch *b) {
   int r = 0;
   for (int i = 1; i < b->period; ++i)
     if (b->nwork[i] > b->nwork[r]) r = i;
+  b->tune_grid.clear();
+  b->tune_threads.clear();
+  b->tune_ms.clear();
   if (b->nwork[r] == 0) {
+    b->grid = std::max(b->fixed_grid, 0);
+    b->threads = b->fixed_threads ? b->fixed_threads : default_threads(b);
     b->tuned = true;
     return IBGPU_OK;
   }
-  std::vector<int> cand = {0};
-  for (int m = 1; m <= (b->mixed ? 6 : 4); ++m)
-    if (m * b->nsm < b->nwork[r]) cand.push_back(m * b->nsm);
+  std::vector<int> grids, blocks;
+  if (b->fixed_grid >= 0) {
+    grids.push_back(b->fixed_grid);
+  } else {
+    grids.push_back(0);
+    for (int m = 1; m <= (b->mixed ? 6 : 4); ++m)
+      if (m * b->nsm < b->nwork[r]) grids.push_back(m * b->nsm);
+  }
+  if (b->fixed_threads) blocks.push_back(b->fixed_threads);
+  else blocks = {default_threads(b), b->mixed ? kTileCells + 32 : kTileCells};
+  if (grids.size() * blocks.size() == 1) {
+    b->grid = grids[0];
+    b->threads = blocks[0];
+    b->tuned = true;
+    return IBGPU_OK;
+  }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   float best = 1e30f;
-  int best_grid = 0;
-  b->tune_grid.clear();
-  b->tune_ms.clear();
-  for (int g : cand) {
-    float tbest = 1e30f;
-    for (int rep = 0; rep < 3; ++rep) {
-      CK(cudaEventRecord(e0, b->stream));
-      fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], 0, b->nstages,
-                               b->d_phase_base, b->limiter, b->visc, b->nstages == 1, b->mixed, g,
-                               b->table, b->stream);
-      CK(cudaGetLastError());
-      CK(cudaEventRecord(e1, b->stream));
-      CK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (rep > 0 && ms < tbest) tbest = ms;  // the first launch warms up
+  int best_grid = grids[0], best_threads = blocks[0];
+  for (int nt : blocks)
+    for (int g : grids) {
+      float tbest = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(e0, b->stream));
+        fast::launch_stage_batch(b->d_args, b->d_ccs, b->d_work[r], b->nwork[r], 0, b->nstages,
+                                 b->d_phase_base, b->limiter, b->visc, b->nstages == 1, b->mixed,
+                                 g, nt, b->table, b->stream);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(e1, b->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0 && ms < tbest) tbest = ms;  // the first launch warms up
+      }
+      b->tune_grid.push_back(g);
+      b->tune_threads.push_back(nt);
+      b->tune_ms.push_back(tbest);
+      if (tbest < best) {
+        best = tbest;
+        best_grid = g;
+        best_threads = nt;
+      }
     }
-    b->tune_grid.push_back(g);
-    b->tune_ms.push_back(tbest);
-    if (tbest < best) {
-      best = tbest;
-      best_grid = g;
-    }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->grid = best_grid;
+  b->threads = best_threads;
   b->tuned = true;
   return IBGPU_OK;
 }
@@ -1809,15 +1839,8 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
   cudaStream_t st = b->stream;
   int rc;
   if (!b->tuned) {
-    if (b->fixed_grid >= 0) {
-      b->grid = b->fixed_grid;
-      b->tune_grid.clear();
-      b->tune_ms.clear();
-      b->tuned = true;
-    } else if ((rc = autotune(b))) {
-      return rc;
-    }
-    b->drop_graphs();  // captured with the previous CTA count
+    if ((rc = autotune(b))) return rc;
+    b->drop_graphs();  // captured with the previous launch shape
   }
   // captured whole steps, unless something asks for per-launch timing or the
   // batch runs on the legacy stream (not capturable); captured before this
@@ -1950,6 +1973,16 @@ int ibgpu_batch_set_grid(ibgpu_batch *b, int grid) {
   return IBGPU_OK;
 }
 
+int ibgpu_batch_set_block(ibgpu_batch *b, int threads) {
+  if (!b || (threads != 0 && threads != kTileCells && threads != kTileCells + 32))
+    return IBGPU_E_ARG;
+  if (b->stream) CK(cudaStreamSynchronize(b->stream));  // captured graphs may be in flight
+  b->drop_graphs();
+  b->fixed_threads = threads;
+  b->tuned = false;
+  return IBGPU_OK;
+}
+
 int ibgpu_batch_set_timing(ibgpu_batch *b, int enable) {
   if (!b) return IBGPU_E_ARG;
   b->timing = enable != 0;
@@ -1958,21 +1991,23 @@ int ibgpu_batch_set_timing(ibgpu_batch *b, int enable) {
   return IBGPU_OK;
 }
 
-int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage_ms,
-                     int64_t *stage_launches) {
+int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *threads, int *period,
+                     double *stage_ms, int64_t *stage_launches) {
   if (!b) return IBGPU_E_ARG;
   if (grid) *grid = b->grid;
+  if (threads) *threads = b->threads;
   if (period) *period = b->period;
   if (stage_ms) *stage_ms = b->stage_ms;
   if (stage_launches) *stage_launches = b->stage_launches;
   return IBGPU_OK;
 }
 
-int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms) {
+int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, int *threads, float *ms) {
   if (!b || max < 0) return IBGPU_E_ARG;
   const int n = std::min<int>(max, (int)b->tune_grid.size());
   for (int i = 0; i < n; ++i) {
     if (grids) grids[i] = b->tune_grid[i];
+    if (threads) threads[i] = b->tune_threads[i];
     if (ms) ms[i] = b->tune_ms[i];
   }
   return (int)b->tune_grid.size();

@@ -62,6 +62,13 @@ struct StageThreads {
   static constexpr int value = sizeof(R) == 8 ? 288 : kTileCells;
 };
 
+// Resident CTAs per SM the register budget is fixed for, by arithmetic and
+// block shape (the batched stage tunes between 256 and 288 threads).
+template <typename R, int NT>
+constexpr int stage_min_blocks() {
+  return sizeof(R) == 8 ? 4 : (NT > kTileCells ? 5 : 6);
+}
+
 // Residual max-norm of a block of up to 9 warps into the step's diag: warp and
 // block maxima, then one atomicMax per component and block whose result
 // nobody reads, so it retires as a fire-and-forget reduction (reading the
@@ -480,7 +487,10 @@ __device__ __forceinline__ void fast_slope(const typename SRec<R>::V *sq, const 
 // Faces whose outer stencil cell is missing use the reference's one-sided
 // reconstruction (NS_Solver.H:743-750).  The residual, update and primitive
 // recovery run in FP64 in every mode.
-template <typename R, int LIM, bool VISC, bool FINAL, typename TI>
+// NT: threads of the CTA, 256 (edge faces on the first two warps) or 288
+// (a ninth warp owns them); the same arithmetic either way.
+template <typename R, int LIM, bool VISC, bool FINAL, typename TI,
+          int NT = StageThreads<R>::value>
 __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageVar &v,
                                                 const CaseConst &cc,
                                                 const int tile, const int phase,
@@ -496,7 +506,7 @@ __device__ __forceinline__ void stage_tile_fast(const StageArgs &a, const StageV
   __shared__ V fx[S::kPlanes * NF];   // x-face (i, j) at j*17 + i
   __shared__ V fy[S::kPlanes * NF];   // y-face (i, j) at j*16 + i
 
-  constexpr int NT = StageThreads<R>::value;
+  static_assert(NT == kTileCells || NT == kTileCells + 32, "256 or 288 threads");
   const int tid = threadIdx.x;
   const int tx = tid & (kTile - 1), ty = (NT > kTileCells) ? ((tid >> 4) & (kTile - 1)) : (tid >> 4);
   // a cell of the tile (the ninth warp owns none)
@@ -838,8 +848,8 @@ __constant__ __align__(16) unsigned char c_batch_table[kBatchTableBytes];
 // step.  LOOP: persistent CTAs striding over the list; otherwise one CTA per
 // item (no loop state, which keeps the tile body's register spills at the
 // single-case kernel's level).
-template <typename R, int LIM, bool VISC, bool FINAL, bool LOOP, bool TABLE, typename TI>
-__global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6)
+template <typename R, int LIM, bool VISC, bool FINAL, bool LOOP, bool TABLE, typename TI, int NT>
+__global__ void __launch_bounds__(NT, stage_min_blocks<R, NT>())
     stage_kernel_batch(const StageArgs *__restrict__ args, const CaseConst *__restrict__ ccs,
                        const int2 *__restrict__ work, int nwork, int stage, int nstages,
                        const int *__restrict__ phase_base, int table) {
@@ -855,13 +865,13 @@ __global__ void __launch_bounds__(StageThreads<R>::value, sizeof(R) == 8 ? 4 : 6
       const StageVar &v = reinterpret_cast<const StageVar *>(c_batch_table + h.y)[stage];
       const CaseConst &cc = *reinterpret_cast<const CaseConst *>(c_batch_table + h.z);
       const int fold = (FINAL && fold_step && v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL, TI>(a, v, cc, it.y, pb + 2 + stage, fold, 0);
+      stage_tile_fast<R, LIM, VISC, FINAL, TI, NT>(a, v, cc, it.y, pb + 2 + stage, fold, 0);
     } else
 #endif
     {
       const StageArgs &a = args[it.x * nstages + stage];
       const int fold = (FINAL && fold_step && a.v.cfl_next) ? 1 + pb + 8 + 1 : 0;
-      stage_tile_fast<R, LIM, VISC, FINAL, TI>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold, 0);
+      stage_tile_fast<R, LIM, VISC, FINAL, TI, NT>(a, a.v, ccs[it.x], it.y, pb + 2 + stage, fold, 0);
     }
     if (!LOOP) break;
     __syncthreads();  // shared-memory reuse by the next work item
@@ -1056,22 +1066,32 @@ void launch_stage(const StageArgs &a, const CaseConst &cc, int ntiles, int limit
 }
 
 #ifdef IBGPU_FAST_BUILD
+template <typename R, int LIM, bool LOOP, bool TABLE, typename TI, int NT>
+static void launch_batch_n(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
+                           int stage, int nstages, const int *phase_base, bool visc,
+                           bool final_stage, int grid, int table, cudaStream_t st) {
+  dim3 g(grid), block(NT);
+  if (visc) {
+    if (final_stage)
+      stage_kernel_batch<R, LIM, true, true, LOOP, TABLE, TI, NT><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+    else
+      stage_kernel_batch<R, LIM, true, false, LOOP, TABLE, TI, NT><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+  } else {
+    if (final_stage)
+      stage_kernel_batch<R, LIM, false, true, LOOP, TABLE, TI, NT><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+    else
+      stage_kernel_batch<R, LIM, false, false, LOOP, TABLE, TI, NT><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
+  }
+}
+
 template <typename R, int LIM, bool LOOP, bool TABLE, typename TI>
 static void launch_batch_l(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
-                           bool final_stage, int grid, int table, cudaStream_t st) {
-  dim3 g(grid), block(StageThreads<R>::value);
-  if (visc) {
-    if (final_stage)
-      stage_kernel_batch<R, LIM, true, true, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
-    else
-      stage_kernel_batch<R, LIM, true, false, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
-  } else {
-    if (final_stage)
-      stage_kernel_batch<R, LIM, false, true, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
-    else
-      stage_kernel_batch<R, LIM, false, false, LOOP, TABLE, TI><<<g, block, 0, st>>>(args, ccs, work, nwork, stage, nstages, phase_base, table);
-  }
+                           bool final_stage, int grid, int threads, int table, cudaStream_t st) {
+  if (threads == kTileCells + 32)
+    launch_batch_n<R, LIM, LOOP, TABLE, TI, kTileCells + 32>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+  else
+    launch_batch_n<R, LIM, LOOP, TABLE, TI, kTileCells>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
 }
 
 // stage input element type: the FP64 step state for the first stage, the
@@ -1079,14 +1099,14 @@ static void launch_batch_l(const StageArgs *args, const CaseConst *ccs, const in
 template <typename R, int LIM, bool LOOP, bool TABLE>
 static void launch_batch_i(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
-                           bool final_stage, int grid, int table, cudaStream_t st) {
+                           bool final_stage, int grid, int threads, int table, cudaStream_t st) {
   if constexpr (sizeof(R) == 4) {
     if (stage > 0) {
-      launch_batch_l<R, LIM, LOOP, TABLE, float>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+      launch_batch_l<R, LIM, LOOP, TABLE, float>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
       return;
     }
   }
-  launch_batch_l<R, LIM, LOOP, TABLE, double>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+  launch_batch_l<R, LIM, LOOP, TABLE, double>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
 }
 
 // grid == nwork: one CTA per work item; fewer: persistent CTAs.  table >= 0:
@@ -1094,30 +1114,33 @@ static void launch_batch_i(const StageArgs *args, const CaseConst *ccs, const in
 template <typename R, int LIM>
 static void launch_batch_t(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                            int stage, int nstages, const int *phase_base, bool visc,
-                           bool final_stage, int grid, int table, cudaStream_t st) {
+                           bool final_stage, int grid, int threads, int table, cudaStream_t st) {
   const bool loop = grid < nwork;
   if (!loop) grid = nwork;
   if (table >= 0) {
-    if (loop) launch_batch_i<R, LIM, true, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
-    else launch_batch_i<R, LIM, false, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    if (loop) launch_batch_i<R, LIM, true, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
+    else launch_batch_i<R, LIM, false, true>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
   } else {
-    if (loop) launch_batch_i<R, LIM, true, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
-    else launch_batch_i<R, LIM, false, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, -1, st);
+    if (loop) launch_batch_i<R, LIM, true, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, -1, st);
+    else launch_batch_i<R, LIM, false, false>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, -1, st);
   }
 }
 
 void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                         int stage, int nstages, const int *phase_base, int limiter, bool visc,
-                        bool final_stage, bool mixed, int grid, int table, cudaStream_t st) {
+                        bool final_stage, bool mixed, int grid, int threads, int table,
+                        cudaStream_t st) {
   if (nwork <= 0) return;
   if (grid < 1 || grid > nwork) grid = nwork;
   if (table >= kBatchTableBytes) table = -1;
+  if (threads != kTileCells && threads != kTileCells + 32)
+    threads = mixed ? StageThreads<float>::value : StageThreads<double>::value;
   if (mixed) {
-    if (limiter == LIM_MINMOD) launch_batch_t<float, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
-    else launch_batch_t<float, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    if (limiter == LIM_MINMOD) launch_batch_t<float, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
+    else launch_batch_t<float, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
   } else {
-    if (limiter == LIM_MINMOD) launch_batch_t<double, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
-    else launch_batch_t<double, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, table, st);
+    if (limiter == LIM_MINMOD) launch_batch_t<double, LIM_MINMOD>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
+    else launch_batch_t<double, LIM_VANLEER>(args, ccs, work, nwork, stage, nstages, phase_base, visc, final_stage, grid, threads, table, st);
   }
 }
 

@@ -39,12 +39,14 @@ IBGPU_DECLARE_LAUNCHERS(exact)
 
 // batched stage over several cases (fast builds only): work = (case, tile)
 // pairs, args[case * nstages + stage], ccs[case]; grid 0 = one CTA per item;
-// table >= 0: byte offset of the batch's header in the constant-memory table
-// (the arguments are read from there instead)
+// threads 256 or 288 per CTA (others: the precision's default); table >= 0:
+// byte offset of the batch's header in the constant-memory table (the
+// arguments are read from there instead)
 namespace fast {
 void launch_stage_batch(const StageArgs *args, const CaseConst *ccs, const int2 *work, int nwork,
                         int stage, int nstages, const int *phase_base, int limiter, bool visc,
-                        bool final_stage, bool mixed, int grid, int table, cudaStream_t st);
+                        bool final_stage, bool mixed, int grid, int threads, int table,
+                        cudaStream_t st);
 // constant-memory table of batched stage arguments: reserve a byte range on
 // a device (16-byte aligned offset, -1 when it does not fit), release it,
 // write bytes at an offset (current device; blocking)

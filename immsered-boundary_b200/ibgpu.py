@@ -38,7 +38,7 @@ EXPORTS = ("ibgpu_create", "ibgpu_set_stream", "ibgpu_upload_topology", "ibgpu_l
            "ibgpu_batch_run", "ibgpu_batch_set_timing", "ibgpu_batch_info", "ibgpu_batch_tuning",
            "ibgpu_batch_destroy", "ibgpu_upload_signdis", "ibgpu_tag_mesh",
            "ibgpu_download_state_async", "ibgpu_synchronize", "ibgpu_batch_tag_mesh",
-           "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_upload_state_async",
+           "ibgpu_batch_table_bytes", "ibgpu_batch_set_grid", "ibgpu_batch_set_block", "ibgpu_upload_state_async",
            "ibgpu_step_async", "ibgpu_step_result", "ibgpu_update_flags", "ibgpu_update_flags_rows",
            "ibgpu_set_state_rows", "ibgpu_build_interfaces", "ibgpu_wall_geometry",
            "ibgpu_wall_distance", "ibgpu_host_register", "ibgpu_host_unregister",
@@ -283,9 +283,11 @@ def lib(path: str | None = None):
                                   ctypes.POINTER(Diag)]
     L.ibgpu_batch_set_timing.argtypes = [vp, ctypes.c_int]
     L.ibgpu_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int64)]
     L.ibgpu_batch_tuning.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
-                                     ctypes.POINTER(ctypes.c_float)]
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
+    L.ibgpu_batch_set_block.argtypes = [vp, ctypes.c_int]
     L.ibgpu_batch_table_bytes.argtypes = [vp]
     L.ibgpu_batch_set_grid.argtypes = [vp, ctypes.c_int]
     L.ibgpu_upload_state_async.argtypes = [vp, vp]
@@ -846,16 +848,22 @@ class Batch:
         persistent CTAs, -1 autotuned at the next run (default)."""
         _check(lib().ibgpu_batch_set_grid(self._b, int(grid)), "ibgpu_batch_set_grid")
 
+    def set_block(self, threads: int):
+        """Threads per CTA of the merged stage launches: 256 or 288, 0
+        autotuned at the next run (default); the same results either way."""
+        _check(lib().ibgpu_batch_set_block(self._b, int(threads)), "ibgpu_batch_set_block")
+
     def info(self) -> dict:
-        g, p = ctypes.c_int(), ctypes.c_int()
+        g, nt, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         ms, nl = ctypes.c_double(), ctypes.c_int64()
-        _check(lib().ibgpu_batch_info(self._b, ctypes.byref(g), ctypes.byref(p), ctypes.byref(ms),
-                                      ctypes.byref(nl)), "ibgpu_batch_info")
-        grids = (ctypes.c_int * 16)()
-        tms = (ctypes.c_float * 16)()
-        k = lib().ibgpu_batch_tuning(self._b, 16, grids, tms)
-        return dict(grid=g.value, period=p.value, stage_ms=ms.value, stage_launches=nl.value,
-                    tuning=[(grids[i], tms[i]) for i in range(max(0, min(k, 16)))],
+        _check(lib().ibgpu_batch_info(self._b, ctypes.byref(g), ctypes.byref(nt), ctypes.byref(p),
+                                      ctypes.byref(ms), ctypes.byref(nl)), "ibgpu_batch_info")
+        grids, blocks = (ctypes.c_int * 32)(), (ctypes.c_int * 32)()
+        tms = (ctypes.c_float * 32)()
+        k = lib().ibgpu_batch_tuning(self._b, 32, grids, blocks, tms)
+        return dict(grid=g.value, threads=nt.value, period=p.value, stage_ms=ms.value,
+                    stage_launches=nl.value,
+                    tuning=[(grids[i], blocks[i], tms[i]) for i in range(max(0, min(k, 32)))],
                     table_bytes=lib().ibgpu_batch_table_bytes(self._b))
 
     def close(self):

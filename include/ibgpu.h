@@ -447,8 +447,9 @@ void ibgpu_destroy(ibgpu_ctx *ctx);
  * interleaved).  The whole step is captured once per schedule phase in a
  * CUDA graph (the cases' ghost fills on parallel branches) and replayed;
  * the captures happen at the start of the first run.  On the first run an
- * autotuner times the candidate CTA counts of the persistent launch and
- * keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
+ * autotuner times the candidate shapes of the merged stage launch (CTA
+ * count: one CTA per work item or 1-4 / 1-6 persistent CTAs per SM; block:
+ * 256 or 288 threads) and keeps the fastest.  The cases must agree on precision (IBGPU_FP64 or
  * IBGPU_MIXED), limiter, viscosity, stage count and coefficients; their CFL
  * intervals (dt_var_step) may differ when each divides the longest marching
  * step of the batch (each case then takes its CFL pass on its own steps, as
@@ -467,15 +468,21 @@ int ibgpu_batch_run(ibgpu_batch *b, int ts0, int nsteps, double *dt, ibgpu_diag 
  * per work item, > 0 = that many persistent CTAs, -1 = chosen by the
  * autotuner at the next run (the default). */
 int ibgpu_batch_set_grid(ibgpu_batch *b, int grid);
+/* Threads per CTA of the merged stage launches from the next run on: 256
+ * (the tile's edge faces on its first two warps) or 288 (a ninth warp owns
+ * them), 0 = chosen by the autotuner at the next run (the default; it times
+ * both with every CTA count it tries).  The same results either way. */
+int ibgpu_batch_set_block(ibgpu_batch *b, int threads);
 /* Event timing of the merged stage launches (total ms, launch count); a
  * batch with timing enabled runs its steps as direct launches, not graphs. */
 int ibgpu_batch_set_timing(ibgpu_batch *b, int enable);
-/* Chosen CTA count (0 = one CTA per work item), subcycling period, timing. */
-int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *period, double *stage_ms,
-                     int64_t *stage_launches);
-/* Autotuner record: up to max (CTA count, ms) pairs; returns the number of
- * candidates timed. */
-int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, float *ms);
+/* Chosen CTA count (0 = one CTA per work item) and threads per CTA,
+ * subcycling period, timing. */
+int ibgpu_batch_info(const ibgpu_batch *b, int *grid, int *threads, int *period,
+                     double *stage_ms, int64_t *stage_launches);
+/* Autotuner record: up to max (CTA count, threads per CTA, ms) candidates;
+ * returns the number of candidates timed. */
+int ibgpu_batch_tuning(const ibgpu_batch *b, int max, int *grids, int *threads, float *ms);
 /* Bytes of the device's constant-memory argument table this batch holds
  * (its stage kernels read their arguments from there); 0 when the batch did
  * not fit and its stage kernels read the arguments from global memory.  The

@@ -62,7 +62,9 @@ def test_batch_fixed_cta_counts_equal_single_runs(cuda_lib, grid):
     b.set_grid(grid)
     b.run(0, 3)
     info = b.info()
-    assert info["grid"] == grid and info["tuning"] == []
+    # the block shape is still tuned, at the caller's CTA count
+    assert info["grid"] == grid and {t[0] for t in info["tuning"]} == {grid}
+    assert {t[1] for t in info["tuning"]} == {256, 288}
     for s, t in zip(single, batched):
         assert t.dt == s.dt
         assert np.array_equal(t.download(), s.download())
@@ -70,6 +72,36 @@ def test_batch_fixed_cta_counts_equal_single_runs(cuda_lib, grid):
         b.set_grid(-2)
     b.close()
     for s in single + batched:
+        s.close()
+
+
+@pytest.mark.parametrize("precision", [ib.FP64, ib.MIXED])
+@pytest.mark.parametrize("threads", [256, 288])
+def test_batch_block_shapes_equal_single_runs(cuda_lib, precision, threads):
+    """Both block shapes of the merged stage launch (the tile's edge faces
+    on the first two warps, or on a ninth warp), fixed by the caller, with
+    one CTA per item and with persistent CTAs: the cases' bits alone."""
+    cases = [wl.vortex_case(n, precision=precision, mach=m) for n, m in [(64, 0.4), (48, 0.7)]]
+    single = [make_solver(c) for c in cases]
+    for s in single:
+        s.run(0, 4)
+    for grid in (0, 5):
+        batched = [make_solver(c) for c in cases]
+        b = ib.Batch(batched)
+        b.set_block(threads)
+        b.set_grid(grid)
+        b.run(0, 4)
+        info = b.info()
+        assert info["threads"] == threads and info["grid"] == grid and info["tuning"] == []
+        for s, t in zip(single, batched):
+            assert t.dt == s.dt
+            assert np.array_equal(t.download(), s.download())
+        with pytest.raises(ib.IbgpuError):
+            b.set_block(128)
+        b.close()
+        for t in batched:
+            t.close()
+    for s in single:
         s.close()
 
 
