@@ -42,9 +42,18 @@ extern double p_ref, area_ref, shear_ref;
 
 // The reference's mesh, pair lists, boundary ghosts and immersed-boundary
 // records as the C ABI's canonical lists (positions, never array indices).
+// The cell rows of the device lists: one row per box of the z = 0 plane of
+// every level, normal cells and 2-D ghosts, in level order and each level's
+// array order (the cell list of ibgpu_upload_topology and the state rows).
+struct IbgpuRows {
+  int64_t n = 0;
+  int32_t *level = nullptr, *ix = nullptr, *iy = nullptr, *box = nullptr;
+  uint8_t *flags = nullptr;  // IBGPU_CELL_*
+  double *prim = nullptr;    // 7 per row: roe, u, v, w, p, T, e
+};
+
 struct IbgpuLists {
-  // one row per box of the z = 0 plane of every level, normal cells and 2-D
-  // ghosts, in level order and each level's array order
+  // the cell rows (IbgpuRows) as vectors, for a single-process flattening
   std::vector<int32_t> level, ix, iy;
   std::vector<uint8_t> flags;  // IBGPU_CELL_*
   std::vector<double> prim;    // 7 per row: roe, u, v, w, p, T, e
@@ -295,11 +304,48 @@ struct IbgpuAdapter {
                      bx.pair.signdis, Body::Bodynum() > 0 && l == nlev - 1);
   }
 
+  // Every list of the device from the mesh (one process).
   static void Flatten(Mesh &mesh, AMR &amr, std::vector<Body> &bodies, NS_Solver &solver,
                       IbgpuLists &L) {
     L = IbgpuLists();
+    FlattenRows(mesh, L);
+    FlattenLists(mesh, amr, bodies, solver, L);
+  }
+
+  static IbgpuRows RowsOf(IbgpuLists &L) {
+    IbgpuRows R;
+    R.n = (int64_t)L.level.size();
+    R.level = L.level.data();
+    R.ix = L.ix.data();
+    R.iy = L.iy.data();
+    R.box = L.box.data();
+    R.flags = L.flags.data();
+    R.prim = L.prim.data();
+    return R;
+  }
+
+  // One cell row (IbgpuRows) of box b of level l.
+  static void FillRow(Mesh &mesh, int l, int b, const IbgpuRows &R, int64_t i) {
+    Box &bx = mesh.ShowLevelBox(l)[b];
+    R.level[i] = l;
+    R.ix[i] = bx.ix();
+    R.iy[i] = bx.iy();
+    R.box[i] = b;
+    R.flags[i] = BoxFlags(mesh, l, b);
+    FlowVariables &fv = mesh.LevelDataArray(l)[b];
+    double *q = R.prim + 7 * i;
+    q[0] = fv.roe;
+    q[1] = fv.u;
+    q[2] = fv.v;
+    q[3] = fv.w;
+    q[4] = fv.p;
+    q[5] = fv.T;
+    q[6] = fv.e;
+  }
+
+  // The cell rows: Meshlevel::m_box / m_data (Meshlevel.H:688-872).
+  static void FlattenRows(Mesh &mesh, IbgpuLists &L) {
     const int nlev = mesh.MyCurNum();
-    // cells: Meshlevel::m_box / m_data (Meshlevel.H:688-872)
     for (int l = 0; l < nlev; ++l) {
       DataArray<Box> &boxes = mesh.ShowLevelBox(l);
       DataArray<FlowVariables> &data = mesh.LevelDataArray(l);
@@ -317,6 +363,12 @@ struct IbgpuAdapter {
         L.prim.insert(L.prim.end(), r, r + 7);
       }
     }
+  }
+
+  // The pair, domain-ghost and immersed-boundary lists.
+  static void FlattenLists(Mesh &mesh, AMR &amr, std::vector<Body> &bodies, NS_Solver &solver,
+                           IbgpuLists &L) {
+    const int nlev = mesh.MyCurNum();
     // coarse/fine pairs: AMRLevel::f_res_ghost, f_pro_ghost, g_pro
     // (AMRLevel.H:320-329), the four z = 0 sons in Point_iterator_2d order
     for (int l = 0; l + 1 < nlev; ++l) {
@@ -836,9 +888,8 @@ struct IbgpuAdapter {
   }
 
   // The lists and the state into a context (ibgpu_upload_*).
-  static int Upload(ibgpu_ctx *ctx, const IbgpuLists &L) {
-    ibgpu_cells cells = {(int64_t)L.level.size(), L.level.data(), L.ix.data(), L.iy.data(),
-                         L.flags.data()};
+  static int Upload(ibgpu_ctx *ctx, const IbgpuLists &L, const IbgpuRows &R) {
+    ibgpu_cells cells = {R.n, R.level, R.ix, R.iy, R.flags};
     int rc = ibgpu_upload_topology(ctx, &cells);
     if (rc) return rc;
     ibgpu_cf_pairs cf = {(int64_t)L.res.size() / 11, L.res.data(), (int64_t)L.pro.size() / 11,
@@ -849,7 +900,7 @@ struct IbgpuAdapter {
                    L.inlet_flow_angle};
     if ((rc = ibgpu_upload_boundaries(ctx, &bc))) return rc;
     if ((rc = UploadIB(ctx, L))) return rc;
-    return ibgpu_upload_state(ctx, L.prim.data());
+    return ibgpu_upload_state(ctx, R.prim);
   }
 
   static int UploadIB(ibgpu_ctx *ctx, const IbgpuLists &L) {
@@ -893,13 +944,15 @@ class GpuNS_Solver : public NS_Solver {
     MPI_Barrier(share_comm);  // every rank's share of the arrays written
     IbgpuUploadTimes &tu = ibgpu_upload_times();
     double t0 = MPI_Wtime();
+    FlattenRowsShared();
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
-      IbgpuAdapter::Flatten(a_mesh, amr, bodies, *this, lists_);
+      lists_ = IbgpuLists();
+      IbgpuAdapter::FlattenLists(a_mesh, amr, bodies, *this, lists_);
       const double t1 = MPI_Wtime();
       tu.flatten += t1 - t0;
       t0 = t1;
-      rc = IbgpuAdapter::Upload(ctx_, lists_);
+      rc = IbgpuAdapter::Upload(ctx_, lists_, rows_);
     }
     rc = ibgpu_share_status(rc);
     tu.lists += MPI_Wtime() - t0;
@@ -909,31 +962,63 @@ class GpuNS_Solver : public NS_Solver {
       wall_resident_ = false;  // the regrid's own pairs go up with the next move
     }
     tu.wall_geometry += MPI_Wtime() - t0;
-    if (rc == IBGPU_OK && sprocs > 1) {
-      // every rank learns the cell rows (level, box index), to share the
-      // per-row flag pass of UploadImmersion
-      int nrows = (int)lists_.box.size();
-      MPI_Bcast(&nrows, 1, MPI_INT, 0, share_comm);
-      if (!ibgpu_device_rank()) {
-        lists_ = IbgpuLists();
-        lists_.level.resize(nrows);
-        lists_.box.resize(nrows);
-      }
-      MPI_Bcast(lists_.level.data(), nrows, MPI_INT, 0, share_comm);
-      MPI_Bcast(lists_.box.data(), nrows, MPI_INT, 0, share_comm);
-    }
     if (rc == IBGPU_OK) {
-      // each level's box -> row map (every rank), for the flag updates of
-      // the rows near the walls after a move
+      // each level's box -> row map (every rank, from the shared rows), for
+      // the flag updates of the rows near the walls after a move
       row_of_.assign(a_mesh.MyCurNum(), std::vector<int>());
-      for (size_t i = 0; i < lists_.box.size(); ++i) {
-        std::vector<int> &m = row_of_[lists_.level[i]];
-        if ((int)m.size() <= lists_.box[i]) m.resize(lists_.box[i] + 1, -1);
-        m[lists_.box[i]] = (int)i;
-      }
+      for (int l = 0; l < a_mesh.MyCurNum(); ++l)
+        row_of_[l].assign(a_mesh.ShowLevelBox(l).realsize(), -1);
+      for (int64_t i = 0; i < rows_.n; ++i) row_of_[rows_.level[i]][rows_.box[i]] = (int)i;
       ib_rows_.clear();
     }
     return rc;
+  }
+
+  // The cell rows (IbgpuRows) in a window shared by the node, every rank
+  // filling the rows of its share of each level's boxes (collective; the
+  // window stays across regrids while it is large enough, pinned on the
+  // device rank for the state's transfers).
+  void FlattenRowsShared() {
+    const int nlev = a_mesh.MyCurNum();
+    // this rank's boxes of each level and its rows among them
+    std::vector<int> mine(nlev, 0), lo(nlev), hi(nlev);
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = a_mesh.ShowLevelBox(l);
+      const int64_t nreal = boxes.realsize();
+      lo[l] = (int)(nreal * srank / sprocs);
+      hi[l] = (int)(nreal * (srank + 1) / sprocs);
+      for (int b = lo[l]; b < hi[l]; ++b) mine[l] += boxes[b].iz() == 0;
+    }
+    std::vector<int> all((size_t)nlev * sprocs);
+    MPI_Allgather(mine.data(), nlev, MPI_INT, all.data(), nlev, MPI_INT, share_comm);
+    // rows in level order, then rank order (each rank's share is a run of
+    // its level's boxes), so in each level's array order: this rank's first
+    // row of level l follows the rows of the levels before and of the ranks
+    // before it
+    std::vector<int64_t> off(nlev);
+    int64_t n = 0;
+    for (int l = 0; l < nlev; ++l)
+      for (int r = 0; r < sprocs; ++r) {
+        if (r == srank) off[l] = n;
+        n += all[(size_t)r * nlev + l];
+      }
+    const size_t bytes = (size_t)n * (4 * sizeof(int32_t) + 1 + 7 * sizeof(double)) + 64;
+    rows_mem_.ensure(bytes, true);
+    char *base = rows_mem_.base;
+    rows_.n = n;
+    rows_.prim = (double *)base;  // 8-byte aligned first
+    rows_.level = (int32_t *)(base + (size_t)n * 7 * sizeof(double));
+    rows_.ix = rows_.level + n;
+    rows_.iy = rows_.ix + n;
+    rows_.box = rows_.iy + n;
+    rows_.flags = (uint8_t *)(rows_.box + n);
+    for (int l = 0; l < nlev; ++l) {
+      DataArray<Box> &boxes = a_mesh.ShowLevelBox(l);
+      int64_t i = off[l];
+      for (int b = lo[l]; b < hi[l]; ++b)
+        if (boxes[b].iz() == 0) IbgpuAdapter::FillRow(a_mesh, l, b, rows_, i++);
+    }
+    MPI_Barrier(share_comm);  // every rank's rows written
   }
 
   // The moving-body part of Body::IBConditions_Image (Body.cpp:1352-1357)
@@ -981,19 +1066,11 @@ class GpuNS_Solver : public NS_Solver {
     if (!created_) return IBGPU_E_STATE;
     MPI_Barrier(share_comm);
     if (near) return UploadImmersionNear(bodies);
-    // the rows' flags, each rank a contiguous share, gathered on every rank
-    const int nrows = (int)lists_.box.size();
-    std::vector<int> counts(sprocs), displs(sprocs);
-    for (int r = 0; r < sprocs; ++r) {
-      displs[r] = (int)((int64_t)nrows * r / sprocs);
-      counts[r] = (int)((int64_t)nrows * (r + 1) / sprocs) - displs[r];
-    }
-    lists_.flags.resize(nrows);
-    for (int i = displs[srank]; i < displs[srank] + counts[srank]; ++i)
-      lists_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[i], lists_.box[i]);
-    if (sprocs > 1)
-      MPI_Allgatherv(MPI_IN_PLACE, 0, MPI_BYTE, lists_.flags.data(), counts.data(), displs.data(),
-                     MPI_BYTE, share_comm);
+    // the rows' flags into the shared rows, each rank a contiguous share
+    const int64_t nrows = rows_.n;
+    for (int64_t i = nrows * srank / sprocs; i < nrows * (srank + 1) / sprocs; ++i)
+      rows_.flags[i] = IbgpuAdapter::BoxFlags(a_mesh, rows_.level[i], rows_.box[i]);
+    MPI_Barrier(share_comm);
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       // the immersed-boundary cells' rows, for the next update of the rows
@@ -1006,7 +1083,7 @@ class GpuNS_Solver : public NS_Solver {
         if (b >= 0 && b < (int)row_of_[last].size() && row_of_[last][b] >= 0)
           ib_rows_.push_back(row_of_[last][b]);
       }
-      rc = ibgpu_update_flags(ctx_, lists_.flags.data());
+      rc = ibgpu_update_flags(ctx_, rows_.flags);
       if (rc == IBGPU_OK) {
         IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
         rc = IbgpuAdapter::UploadIB(ctx_, lists_);
@@ -1041,7 +1118,7 @@ class GpuNS_Solver : public NS_Solver {
     }
     std::vector<uint8_t> flags(mine);
     for (int k = 0; k < mine; ++k)
-      flags[k] = IbgpuAdapter::BoxFlags(a_mesh, lists_.level[rows[k]], lists_.box[rows[k]]);
+      flags[k] = IbgpuAdapter::BoxFlags(a_mesh, rows_.level[rows[k]], rows_.box[rows[k]]);
     std::vector<int> all_rows(total);
     std::vector<uint8_t> all_flags(total);
     MPI_Allgatherv(rows.data(), mine, MPI_INT, all_rows.data(), counts.data(), displs.data(),
@@ -1063,11 +1140,10 @@ class GpuNS_Solver : public NS_Solver {
       for (const std::vector<int> *v : {&ib_rows_, &now_ib})
         for (int r : *v) {
           r64.push_back(r);
-          all_flags.push_back(IbgpuAdapter::BoxFlags(a_mesh, lists_.level[r], lists_.box[r]));
+          all_flags.push_back(IbgpuAdapter::BoxFlags(a_mesh, rows_.level[r], rows_.box[r]));
         }
       ib_rows_.swap(now_ib);
-      lists_.flags.resize(lists_.box.size());
-      for (size_t k = 0; k < r64.size(); ++k) lists_.flags[r64[k]] = all_flags[k];
+      for (size_t k = 0; k < r64.size(); ++k) rows_.flags[r64[k]] = all_flags[k];
       rc = ibgpu_update_flags_rows(ctx_, (int64_t)r64.size(), r64.data(), all_flags.data());
       if (rc == IBGPU_OK) {
         IbgpuAdapter::FlattenImmersed(a_mesh, bodies, lists_);
@@ -1120,25 +1196,25 @@ class GpuNS_Solver : public NS_Solver {
       if ((rc = ibgpu_share_status(rc))) return rc;
       IbgpuAdapter::WallUnpack(a_mesh, wall_, false, nullptr, nullptr);
     }
+    // the state into the shared rows (pinned), then every rank writes its
+    // share of them into the mesh
     int rc = IBGPU_OK;
-    if (ibgpu_device_rank()) {
-      std::vector<double> rows(lists_.prim.size());
-      rc = ibgpu_download_state(ctx_, rows.data());
-      for (size_t i = 0; rc == IBGPU_OK && i < lists_.box.size(); ++i) {
-        FlowVariables &fv = a_mesh.LevelDataArray(lists_.level[i])[lists_.box[i]];
-        const double *q = &rows[7 * i];
-        fv.roe = q[0];
-        fv.u = q[1];
-        fv.v = q[2];
-        fv.w = q[3];
-        fv.p = q[4];
-        fv.T = q[5];
-        fv.e = q[6];
-      }
+    if (ibgpu_device_rank()) rc = ibgpu_download_state(ctx_, rows_.prim);
+    if ((rc = ibgpu_share_status(rc))) return rc;
+    const int64_t nrows = rows_.n;
+    for (int64_t i = nrows * srank / sprocs; i < nrows * (srank + 1) / sprocs; ++i) {
+      FlowVariables &fv = a_mesh.LevelDataArray(rows_.level[i])[rows_.box[i]];
+      const double *q = rows_.prim + 7 * i;
+      fv.roe = q[0];
+      fv.u = q[1];
+      fv.v = q[2];
+      fv.w = q[3];
+      fv.p = q[4];
+      fv.T = q[5];
+      fv.e = q[6];
     }
-    rc = ibgpu_share_status(rc);
     MPI_Barrier(share_comm);
-    return rc;
+    return IBGPU_OK;
   }
 
   // A level's refine/coarsen decision for AMR::TagtheBox (after Inittag):
@@ -1163,12 +1239,13 @@ class GpuNS_Solver : public NS_Solver {
     return rc;
   }
 
-  const IbgpuLists &lists() const { return lists_; }
 
  private:
   ibgpu_ctx *ctx_ = nullptr;  // the device rank's context
   bool created_ = false;      // on every rank once Create succeeded
-  IbgpuLists lists_;          // the device rank's lists
+  IbgpuLists lists_;          // the device rank's pair, ghost and immersed-boundary lists
+  IbgpuSharedBytes rows_mem_;  // the cell rows, shared by the node's ranks
+  IbgpuRows rows_;            // ... laid out in rows_mem_
   // wall_resident_: the device holds every level's wall pairs from a move
   // since the last geometry upload (the exchange buffers hold them too)
   bool device_distance_ = true, wall_check_ = false, wall_resident_ = false;
