@@ -78,6 +78,11 @@ struct IbgpuMoveTimes {
   // the device wall distances' parts (within distance): packing this rank's
   // share, the device rank's call, unpacking
   double wall_pack = 0.0, wall_device = 0.0, wall_unpack = 0.0;
+  // the immersed-boundary part's pieces (within ibcells): removed and newly
+  // infected cells, the IB array's compaction and index, the image cells,
+  // the wall cells' exchange, the ghost IB cells, the patches' hanging nodes
+  double ib_infect = 0.0, ib_compact = 0.0, ib_image = 0.0, ib_exchange = 0.0, ib_ghost = 0.0,
+         ib_patch = 0.0;
 };
 inline IbgpuMoveTimes &ibgpu_move_times() {
   static IbgpuMoveTimes t;
@@ -874,15 +879,27 @@ struct IbgpuAdapter {
         ibgpu_wall_check_mismatches() += bad;
       }
     }
+    double ti = MPI_Wtime();
+    auto lap = [&ti](double &acc) {
+      const double t = MPI_Wtime();
+      acc += t - ti;
+      ti = t;
+    };
     Body::RemoveIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
     Body::InfectNewIBCells(amesh, abody, in_to_out[last], out_to_in[last]);
+    lap(tm.ib_infect);
     amesh.m_dis.holeplan(true);
     amesh.m_dis.CompressArray();
     amesh.RenewInfectIndex();
+    lap(tm.ib_compact);
     Body::FindImageCell(amesh, abody);
+    lap(tm.ib_image);
     amesh.DataExchangeCells_Wall();
+    lap(tm.ib_exchange);
     Body::FindImageCell_GhostIBCell(amesh, abody);
+    lap(tm.ib_ghost);
     for (int i = 0; i < bn; ++i) abody[i].FindPatchHangingNode(amesh);
+    lap(tm.ib_patch);
     tm.ibcells += MPI_Wtime() - t0;
     return IBGPU_OK;
   }

@@ -709,13 +709,16 @@ int main(int argc, char **argv) {
   {
     // moving-body phases on rank 0, all steps (warm-up included)
     const IbgpuMoveTimes &mt = ibgpu_move_times();
-    char buf[512];
+    char buf[768];
     std::snprintf(buf, sizeof buf,
                   "{\"forces\": %.6f, \"motion\": %.6f, \"distance\": %.6f, \"sync\": %.6f, "
                   "\"ibcells\": %.6f, \"upload\": %.6f, \"wall_pack\": %.6f, "
-                  "\"wall_device\": %.6f, \"wall_unpack\": %.6f, \"distcheck_mismatches\": %lld}",
+                  "\"wall_device\": %.6f, \"wall_unpack\": %.6f, \"ib_infect\": %.6f, "
+                  "\"ib_compact\": %.6f, \"ib_image\": %.6f, \"ib_exchange\": %.6f, "
+                  "\"ib_ghost\": %.6f, \"ib_patch\": %.6f, \"distcheck_mismatches\": %lld}",
                   mt.forces, mt.motion, mt.distance, mt.sync, mt.ibcells, mt.upload, mt.wall_pack,
-                  mt.wall_device, mt.wall_unpack, ibgpu_wall_check_mismatches());
+                  mt.wall_device, mt.wall_unpack, mt.ib_infect, mt.ib_compact, mt.ib_image,
+                  mt.ib_exchange, mt.ib_ghost, mt.ib_patch, ibgpu_wall_check_mismatches());
     phases = buf;
   }
 #endif
