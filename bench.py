@@ -764,11 +764,23 @@ def config3_section(steps: int = 22, warm: int = 2, rank: int = 0):
     ref = os.path.join(ROOT, "oracle", "_ref", "ref_pitch_minmod")
     if os.path.exists(ref):
         ranks = host_cores()
-        rate, _, _ = run_reference_mpi(ref, CONFIG3_ENV, 6, 1, ranks)
-        out["reference"] = {"value": rate, "unit": UNIT, "cores": ranks,
+        # the same window as the GPU runs: 20 timed steps from step 2, the
+        # regrid at step 20 between them
+        res, _ = run_oracle_binary(ref, CONFIG3_ENV,
+                                   {"IB_STEPS": str(steps), "IB_TIMED_FROM": str(warm),
+                                    "IB_RANKS": str(ranks), "IB_MPI_TIMEOUT": "900"},
+                                   timeout=1800.0)
+        if res.get("ranks", 1) != ranks:
+            raise RuntimeError("reference run used another rank count")
+        out["reference"] = {"value": res["cell_updates"] / res["loop_seconds"], "unit": UNIT,
+                            "cores": ranks,
+                            "regrid_ms": res.get("regrid_seconds", 0.0) * 1e3,
+                            "with_regrids": res["cell_updates"] / (
+                                res["loop_seconds"] + res.get("regrid_seconds", 0.0)),
                             "sample": f"the reference's own step with its moving-body path in "
                                       f"its shared-memory MPI mode, {ranks} ranks (one per host "
-                                      f"core), 5 timed steps after 1"}
+                                      f"core), {steps - warm} timed steps after {warm} (the "
+                                      f"regrid at step 20 timed apart, as for the GPU runs)"}
     return out
 
 
