@@ -1,7 +1,7 @@
 // Wall distances of moved bodies on the device: the per-box part of the
 // reference's re-immersion (Body::RenewLevelDistance, Bodymove.cpp:127-300)
 // and the block-ghost copies of Mesh::SynNormal_BlockDistance
-// (Mesh.cpp:2303-2374), in four passes per level:
+// (Mesh.cpp:2303-2374), in three passes over every level at once:
 //   walk     closest wall patch of the box's own body by the reference's
 //            walk over neighbouring patches (Body::FindClosePatchtoCell,
 //            Body.H:505-580), signed distance along that patch's normal;
@@ -10,8 +10,10 @@
 //            rule (Bodymove.cpp:158-228), reading the neighbours' walked pairs;
 //   finalise signed distance capped by the distance to the domain boundary,
 //            solid flag, and the boxes that changed sides (the reference's
-//            move lists, Bodymove.cpp:231-255);
-//   block    every block ghost takes its origin box's pair and solid flag.
+//            move lists, Bodymove.cpp:231-255); then each box's block ghosts
+//            take its final pair and their solid flags;
+// and, for ibgpu_wall_distance_near, the compaction of the boxes near the
+// walls.
 // This unit is compiled without floating-point contraction and uses the
 // correctly rounded square root, so every distance is the reference's bit
 // for bit (its host code evaluates the same expressions in the same order).
@@ -48,6 +50,9 @@ struct LevelDev {
   const int32_t *neib;
   const uint8_t *kind;
   const int32_t *block_in, *block_out;
+  // the block pairs of each origin box: pair indices blk_pair[blk_first[i]
+  // .. blk_first[i + 1]) (origins' pairs in pair order)
+  const int32_t *blk_first, *blk_pair;
   // pairs as handed in, after the walk, final
   const int32_t *body0, *patch0;
   const double *dist0, *sd0, *dtb0;
@@ -124,12 +129,12 @@ __device__ __forceinline__ bool valid_pair(const BodiesDev &B, int body, int pat
 // The levels of one call as one index space, so each pass is one launch
 // for every level: level l's boxes at [box0[l], box0[l] + n_l), box0[l] a
 // multiple of kNearBlock (no block of the compaction straddles two
-// levels); its block pairs at [pair0[l], pair0[l + 1]).
+// levels).
 constexpr int kNearBlock = 256;
 constexpr int kMaxWallLevels = 16;
 struct Span {
   int nlevels;
-  int64_t box0[kMaxWallLevels + 1], pair0[kMaxWallLevels + 1];
+  int64_t box0[kMaxWallLevels + 1];
   double band[kMaxWallLevels];  // near-wall report (ibgpu_wall_distance_near)
 };
 
@@ -219,52 +224,58 @@ __global__ void junction_kernel(const LevelDev *lv, Span sp, BodiesDev B, int *e
   L.dtb2[i] = dtb;
 }
 
+// Caps, solid flags and move lists; then the box's block ghosts take its
+// final pair (Mesh::SynNormal_BlockDistance: targets are distinct and never
+// origins, checked on upload, so no ghost is written twice and none is an
+// input here).
 __global__ void finalize_kernel(const LevelDev *lv, Span sp) {
   int l;
   int64_t i;
   if (!span_box(sp, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, l, i, lv)) return;
   const LevelDev &L = lv[l];
   uint8_t mv = 0;
-  double sd = L.sd2[i];
   const uint8_t kind = L.kind[i];
-  if (sd < kCriticDis && kind != IBGPU_WALL_BOX_BLOCK_GHOST) {
+  if (kind == IBGPU_WALL_BOX_BLOCK_GHOST) {
+    L.moved[i] = 0;  // its pair comes from its origin
+    return;
+  }
+  double sd = L.sd2[i];
+  uint8_t solid = L.solid[i];
+  if (sd < kCriticDis) {
     const double dm = L.dtdm[i];
     sd = (dm < sd) ? dm : sd;  // std::min(signdis, distance_to_dm)
     L.sd2[i] = sd;
     if (sd < 0.0) {
-      if (!L.solid[i] && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_INTO_BODY;
-      L.solid[i] = 1;
+      if (!solid && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_INTO_BODY;
+      solid = 1;
     } else {
-      if (L.solid[i] && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_OUT_OF_BODY;
-      L.solid[i] = 0;
+      if (solid && kind != IBGPU_WALL_BOX_DOMAIN_GHOST) mv = IBGPU_WALL_OUT_OF_BODY;
+      solid = 0;
     }
+    L.solid[i] = solid;
   }
   L.moved[i] = mv;
-}
-
-// block ghosts: targets are distinct and never origins (checked on upload)
-__global__ void block_kernel(const LevelDev *lv, Span sp) {
-  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= sp.pair0[sp.nlevels]) return;
-  const int l = level_of(sp.pair0, sp.nlevels, g);
-  const LevelDev &L = lv[l];
-  const int64_t k = g - sp.pair0[l];
-  const int in = L.block_in[k], out = L.block_out[k];
-  L.body2[out] = L.body2[in];
-  L.patch2[out] = L.patch2[in];
-  L.dist2[out] = L.dist2[in];
-  const double sd = L.sd2[in];
-  L.sd2[out] = sd;
-  uint8_t mv = 0;
-  const bool dg = L.kind[out] == IBGPU_WALL_BOX_DOMAIN_GHOST;
-  if (sd < 0.0) {
-    if (!L.solid[out] && !dg) mv = IBGPU_WALL_INTO_BODY;
-    L.solid[out] = 1;
-  } else {
-    if (L.solid[out] && !dg) mv = IBGPU_WALL_OUT_OF_BODY;
-    L.solid[out] = 0;
+  const int k0 = L.blk_first[i], k1 = L.blk_first[i + 1];
+  if (k0 == k1) return;
+  const int body = L.body2[i], patch = L.patch2[i];
+  const double dist = L.dist2[i];
+  for (int q = k0; q < k1; ++q) {
+    const int k = L.blk_pair[q], out = L.block_out[k];
+    L.body2[out] = body;
+    L.patch2[out] = patch;
+    L.dist2[out] = dist;
+    L.sd2[out] = sd;
+    uint8_t gm = 0;
+    const bool dg = L.kind[out] == IBGPU_WALL_BOX_DOMAIN_GHOST;
+    if (sd < 0.0) {
+      if (!L.solid[out] && !dg) gm = IBGPU_WALL_INTO_BODY;
+      L.solid[out] = 1;
+    } else {
+      if (L.solid[out] && !dg) gm = IBGPU_WALL_OUT_OF_BODY;
+      L.solid[out] = 0;
+    }
+    L.block_moved[k] = gm;
   }
-  L.block_moved[k] = mv;
 }
 
 // The boxes a host re-immersion reads (ibgpu_wall_distance_near): near a
@@ -388,7 +399,7 @@ struct Buf {
 
 struct Level {
   int64_t n = 0, nblock = 0;
-  Buf center, dtdm, neib, kind, block_in, block_out;
+  Buf center, dtdm, neib, kind, block_in, block_out, blk_first, blk_pair;
   Buf body[3], patch[3], dist[3], sd[3], dtb[3], solid, moved, block_moved;
 };
 
@@ -499,6 +510,17 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
         (rc = put(L.block_in, g.block_in, g.nblock, st)) ||
         (rc = put(L.block_out, g.block_out, g.nblock, st)))
       return rc;
+    // each origin's block pairs (a counting sort of the pairs by origin)
+    std::vector<int32_t> first((size_t)g.n + 1, 0), order((size_t)std::max<int64_t>(g.nblock, 1));
+    for (int64_t k = 0; k < g.nblock; ++k) ++first[(size_t)g.block_in[k] + 1];
+    for (int64_t i = 0; i < g.n; ++i) first[(size_t)i + 1] += first[(size_t)i];
+    {
+      std::vector<int32_t> fill(first.begin(), first.end() - 1);
+      for (int64_t k = 0; k < g.nblock; ++k) order[(size_t)fill[(size_t)g.block_in[k]]++] = (int32_t)k;
+    }
+    if ((rc = put(L.blk_first, first.data(), g.n + 1, st)) ||
+        (rc = put(L.blk_pair, order.data(), std::max<int64_t>(g.nblock, 1), st)))
+      return rc;
     for (int k = 0; k < 3; ++k) {
       WK(L.body[k].reserve((size_t)g.n * 4));
       WK(L.patch[k].reserve((size_t)g.n * 4));
@@ -561,6 +583,8 @@ LevelDev level_dev(Level &L) {
   D.kind = L.kind.as<uint8_t>();
   D.block_in = L.block_in.as<int32_t>();
   D.block_out = L.block_out.as<int32_t>();
+  D.blk_first = L.blk_first.as<int32_t>();
+  D.blk_pair = L.blk_pair.as<int32_t>();
   D.body0 = L.body[0].as<int32_t>();
   D.patch0 = L.patch[0].as<int32_t>();
   D.dist0 = L.dist[0].as<double>();
@@ -587,30 +611,28 @@ int level_span(State *S, cudaStream_t st, Span &sp) {
   const int nl = (int)S->levels.size();
   std::vector<LevelDev> h((size_t)std::max(nl, 1));
   sp.nlevels = nl;
-  sp.box0[0] = sp.pair0[0] = 0;
+  sp.box0[0] = 0;
   for (int l = 0; l < nl; ++l) {
     Level &L = S->levels[(size_t)l];
     h[(size_t)l] = level_dev(L);
     sp.box0[l + 1] = sp.box0[l] + (L.n + kNearBlock - 1) / kNearBlock * kNearBlock;
-    sp.pair0[l + 1] = sp.pair0[l] + L.nblock;
     sp.band[l] = 0.0;
   }
   return put(S->lv, h.data(), std::max(nl, 1), st);
 }
 
-// The four passes of every level (walk, junction, caps and move lists,
-// block ghosts) from the input pairs (set 0) to the new ones (set 2), one
-// launch each.
+// The passes of every level (walk, junction, then caps, move lists and the
+// block ghosts' copies) from the input pairs (set 0) to the new ones (set
+// 2), one launch each.
 int launch_passes(State *S, const Span &sp, const BodiesDev &B, cudaStream_t st) {
   const LevelDev *lv = S->lv.as<LevelDev>();
   int *err = S->err.as<int>();
-  const int64_t nbox = sp.box0[sp.nlevels], npair = sp.pair0[sp.nlevels];
+  const int64_t nbox = sp.box0[sp.nlevels];
   if (nbox > 0) {
     walk_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp, B, err);
     junction_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp, B, err);
     finalize_kernel<<<blocks(nbox), 256, 0, st>>>(lv, sp);
   }
-  if (npair > 0) block_kernel<<<blocks(npair), 256, 0, st>>>(lv, sp);
   WK(cudaGetLastError());
   return IBGPU_OK;
 }
