@@ -164,15 +164,28 @@ struct ibgpu_ctx {
                         &d_pat_body, &d_pat_intp, &d_body_begin}) {
       cudaFree(*p);
       *p = nullptr;
+      cap.erase(p);
     }
     for (double **p : {&d_bc_nmv, &d_facevar, &d_ib_f, &d_ib_out, &d_pat_f, &d_pat_out,
                        &d_body_center, &d_force}) {
       cudaFree(*p);
       *p = nullptr;
+      cap.erase(p);
     }
     bc_waves.clear();
     n_ib = n_pat = nbodies = 0;
-    cap.clear();
+  }
+
+  // Before a new topology: the lists that belong to the old one go, and the
+  // per-slot buffers made on demand (sized by the old slot count); the
+  // layout's own buffers stay for the new one to reuse when large enough.
+  void reset_layout() {
+    free_aux();
+    cudaFree(d_signdis);
+    cudaFree(d_tags);
+    d_signdis = nullptr;
+    d_tags = nullptr;
+    has_topology = has_state = false;
   }
 
   // slot of (level, x, y) with periodic wrap, -1 if absent
@@ -226,6 +239,7 @@ struct ibgpu_ctx {
     d_flags = d_cell_alias = nullptr;
     d_vsd = d_rows = nullptr;
     has_topology = has_state = false;
+    cap.clear();
   }
 };
 
@@ -543,7 +557,7 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   ctx->in_used = false;
   ctx->chain_open = false;  // a new mesh ends any chain of asynchronous steps
   ctx->chain_steps = 0;
-  ctx->free_layout();
+  ctx->reset_layout();
 
   // 1. owners vs aliases; each level's tiles in a dense index over the
   //    bounding box of its owner cells' tiles (-1: no tile)
@@ -678,31 +692,32 @@ int ibgpu_upload_topology(ibgpu_ctx *ctx, const ibgpu_cells *cells) {
   }
   // 5. (the stencils of the leaf cells and 6. the uniform tiles are made on
   //    the device below)
-  // 7. device arrays
+  // 7. device arrays (a regrid's new layout reuses the old one's buffers
+  //    where they are large enough)
   int rc;
-  if ((rc = dev_alloc(&ctx->d_tile_nb, h_nb.size())) ||
-      (rc = dev_alloc(&ctx->d_tile_level, (size_t)ntiles)) ||
-      (rc = dev_alloc(&ctx->d_flags, (size_t)nslots)) ||
-      (rc = dev_alloc(&ctx->d_tile_uniform, (size_t)ntiles)) ||
-      (rc = dev_alloc(&ctx->d_tile_org, (size_t)ntiles)) ||
-      (rc = dev_alloc(&ctx->d_cell_slot, (size_t)n)) ||
-      (rc = dev_alloc(&ctx->d_cell_alias, (size_t)n)) ||
-      (rc = dev_alloc(&ctx->d_cell_layout, (size_t)n)) ||
-      (rc = dev_alloc(&ctx->d_row_flags, (size_t)n)) ||
-      (rc = dev_alloc(&ctx->d_tile_full, (size_t)ntiles)) ||
-      (rc = dev_alloc(&ctx->d_layout_err, (size_t)2)) ||  // also the stencil check's key
-      (rc = dev_alloc(&ctx->d_rows, (size_t)n * 7)) ||
+  if ((rc = keep_alloc(ctx, &ctx->d_tile_nb, h_nb.size())) ||
+      (rc = keep_alloc(ctx, &ctx->d_tile_level, (size_t)ntiles)) ||
+      (rc = keep_alloc(ctx, &ctx->d_flags, (size_t)nslots)) ||
+      (rc = keep_alloc(ctx, &ctx->d_tile_uniform, (size_t)ntiles)) ||
+      (rc = keep_alloc(ctx, &ctx->d_tile_org, (size_t)ntiles)) ||
+      (rc = keep_alloc(ctx, &ctx->d_cell_slot, (size_t)n)) ||
+      (rc = keep_alloc(ctx, &ctx->d_cell_alias, (size_t)n)) ||
+      (rc = keep_alloc(ctx, &ctx->d_cell_layout, (size_t)n)) ||
+      (rc = keep_alloc(ctx, &ctx->d_row_flags, (size_t)n)) ||
+      (rc = keep_alloc(ctx, &ctx->d_tile_full, (size_t)ntiles)) ||
+      (rc = keep_alloc(ctx, &ctx->d_layout_err, (size_t)2)) ||  // also the stencil check's key
+      (rc = keep_alloc(ctx, &ctx->d_rows, (size_t)n * 7)) ||
       // staging of asynchronous downloads, here so that the first one in a
       // pipelined loop does not allocate (and wait for the device)
-      (rc = dev_alloc(&ctx->d_rows_out, (size_t)n * 7)))
+      (rc = keep_alloc(ctx, &ctx->d_rows_out, (size_t)n * 7)))
     return rc;
   for (int f = 0; f < kStateFields; ++f)
-    if ((rc = dev_alloc(&ctx->d_s0[f], (size_t)nslots))) return rc;
+    if ((rc = keep_alloc(ctx, &ctx->d_s0[f], (size_t)nslots))) return rc;
   const size_t buf_elem = cs.precision == IBGPU_MIXED ? sizeof(float) : sizeof(double);
   for (int b = 0; b < 2; ++b)
     for (int f = 0; f < 4; ++f)
-      if ((rc = dev_alloc((unsigned char **)&ctx->d_buf[b][f], (size_t)nslots * buf_elem))) return rc;
-  if (cs.viscous && (rc = dev_alloc(&ctx->d_vsd, (size_t)nslots * 8))) return rc;
+      if ((rc = keep_alloc(ctx, (unsigned char **)&ctx->d_buf[b][f], (size_t)nslots * buf_elem))) return rc;
+  if (cs.viscous && (rc = keep_alloc(ctx, &ctx->d_vsd, (size_t)nslots * 8))) return rc;
   cudaStream_t st = ctx->stream;
   CK(cudaMemcpyAsync(ctx->d_tile_nb, h_nb.data(), h_nb.size() * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_tile_level, h_tile_level.data(), ntiles * 4, cudaMemcpyHostToDevice, st));
