@@ -150,3 +150,26 @@ def test_cl_cd_history_1000_steps(cuda_lib, pkg, precision):
           f"{worst_body:.2e} over {len(hist)} steps")
     assert worst.max() <= COEF_TOL[precision] and worst_body <= COEF_TOL[precision]
     sol.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_case_batch_equals_run(cuda_lib, pkg, precision):
+    """The graph-replayed batch entry point with this one case gives the bits
+    of ibgpu_run over three coarse-level periods (24 steps: every level's
+    schedule, the CFL passes and the folded CFL bound)."""
+    ib = pkg.ibgpu
+    g = make_golden.load(NAME)
+    period = int(g["schedule"].reshape(-1, 6)[:, 0].max())
+    steps = 3 * period
+    ref = workloads.naca_solver(g, 0, precision_of(ib, precision))
+    ref.run(0, steps)
+    sol = workloads.naca_solver(g, 0, precision_of(ib, precision))
+    b = ib.Batch([sol])
+    d = b.run(0, steps)
+    assert d[0].abort_code == 0
+    assert sol.dt == ref.dt
+    assert np.array_equal(sol.download(), ref.download())
+    assert np.array_equal(sol.wall_forces(), ref.wall_forces())
+    b.close()
+    sol.close()
+    ref.close()
