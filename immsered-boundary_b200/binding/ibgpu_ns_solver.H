@@ -93,7 +93,10 @@ inline IbgpuMoveTimes &ibgpu_move_times() {
 // flattening the mesh into the device lists (device rank), the lists'
 // upload, and the wall geometry (windows, packing, the device call).
 struct IbgpuUploadTimes {
-  double flatten = 0.0, lists = 0.0, wall_geometry = 0.0;
+  // wall_geometry = wall_pack (every rank's share, then the node barrier) +
+  // wall_device (ibgpu_wall_geometry on the device rank, status shared)
+  double flatten = 0.0, lists = 0.0, wall_geometry = 0.0, wall_pack = 0.0, wall_device = 0.0,
+         rows_map = 0.0;
 };
 inline IbgpuUploadTimes &ibgpu_upload_times() {
   static IbgpuUploadTimes t;
@@ -549,6 +552,7 @@ struct IbgpuAdapter {
   // kinds, distances to the domain boundary) and block pairs into the
   // levels' exchange buffers and the device.
   static int WallGeometry(ibgpu_ctx *ctx, Mesh &mesh, std::vector<IbgpuWallLevel> &W) {
+    const double t0 = MPI_Wtime();
     const int nlev = mesh.MyCurNum();
     // the levels' windows stay from the last regrid where they are large
     // enough (every rank computes the same sizes, so all keep or renew alike)
@@ -578,6 +582,9 @@ struct IbgpuAdapter {
       }
     }
     MPI_Barrier(share_comm);
+    IbgpuUploadTimes &tu = ibgpu_upload_times();
+    const double t1 = MPI_Wtime();
+    tu.wall_pack += t1 - t0;
     int rc = IBGPU_OK;
     if (ibgpu_device_rank()) {
       std::vector<ibgpu_wall_level_geom> g(nlev);
@@ -588,7 +595,9 @@ struct IbgpuAdapter {
       }
       rc = ibgpu_wall_geometry(ctx, nlev, g.data());
     }
-    return ibgpu_share_status(rc);
+    rc = ibgpu_share_status(rc);
+    tu.wall_device += MPI_Wtime() - t1;
+    return rc;
   }
 
   // The wall distances of the moved bodies on the device: every level's
@@ -979,6 +988,7 @@ class GpuNS_Solver : public NS_Solver {
       wall_resident_ = false;  // the regrid's own pairs go up with the next move
     }
     tu.wall_geometry += MPI_Wtime() - t0;
+    t0 = MPI_Wtime();
     if (rc == IBGPU_OK) {
       // each level's box -> row map (every rank, from the shared rows), for
       // the flag updates of the rows near the walls after a move
@@ -988,6 +998,7 @@ class GpuNS_Solver : public NS_Solver {
       for (int64_t i = 0; i < rows_.n; ++i) row_of_[rows_.level[i]][rows_.box[i]] = (int)i;
       ib_rows_.clear();
     }
+    tu.rows_map += MPI_Wtime() - t0;
     return rc;
   }
 

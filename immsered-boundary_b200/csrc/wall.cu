@@ -384,13 +384,17 @@ struct Buf {
     return *this;
   }
   ~Buf() { cudaFree(p); }
+  // at least b bytes; a buffer that grows takes a quarter to spare, since
+  // a regrid changes the box counts a little and a free + allocation
+  // costs far more than the spare bytes
   cudaError_t reserve(size_t b) {
     if (b <= bytes) return cudaSuccess;
     cudaFree(p);
     p = nullptr;
     bytes = 0;
-    cudaError_t e = cudaMalloc(&p, b > 0 ? b : 1);
-    if (e == cudaSuccess) bytes = b;
+    const size_t want = b + b / 4;
+    cudaError_t e = cudaMalloc(&p, want > 0 ? want : 1);
+    if (e == cudaSuccess) bytes = want;
     return e;
   }
   template <typename T>
@@ -446,6 +450,18 @@ int get(T *h, const Buf &b, int64_t n, cudaStream_t st) {
 
 unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
+// Every neighbour index of a level's geometry is a box of the level or -1;
+// *bad becomes 1 when one is not (grid-stride over at most four blocks per
+// SM of a B200).
+constexpr int64_t kCheckBlocks = 4 * 148;
+__global__ void neib_check_kernel(const int32_t *neib, int64_t m, int64_t n, int *bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = neib[i];
+    if (v < -1 || v >= n) *bad = 1;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -473,11 +489,7 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
         (g.n > 0 && (!g.center || !g.neib || !g.kind || !g.distance_to_dm)) ||
         (g.nblock > 0 && (!g.block_in || !g.block_out)))
       return IBGPU_E_ARG;
-    for (int64_t i = 0; i < 9 * g.n; ++i)
-      if (g.neib[i] < -1 || g.neib[i] >= g.n) {
-        set_last_error("wall geometry: neighbour index out of the level's boxes");
-        return IBGPU_E_ARG;
-      }
+    // (the neighbour indices are checked on the device below)
     // block pairs: distinct targets, none of them an origin
     std::vector<uint8_t> mark((size_t)g.n, 0);
     for (int64_t k = 0; k < g.nblock; ++k) {
@@ -499,6 +511,8 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
   if (!S) *slot = S = new State();
   S->levels.resize((size_t)nlevels);
   cudaStream_t st = V.stream;
+  WK(S->err.reserve(sizeof(int)));
+  WK(cudaMemsetAsync(S->err.p, 0, sizeof(int), st));
   for (int l = 0; l < nlevels; ++l) {
     const ibgpu_wall_level_geom &g = levels[l];
     Level &L = S->levels[(size_t)l];
@@ -508,8 +522,13 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
     if ((rc = put(L.center, g.center, 3 * g.n, st)) || (rc = put(L.neib, g.neib, 9 * g.n, st)) ||
         (rc = put(L.kind, g.kind, g.n, st)) || (rc = put(L.dtdm, g.distance_to_dm, g.n, st)) ||
         (rc = put(L.block_in, g.block_in, g.nblock, st)) ||
-        (rc = put(L.block_out, g.block_out, g.nblock, st)))
+        (rc = put(L.block_out, g.block_out, g.nblock, st))) {
+      S->levels.clear();
       return rc;
+    }
+    if (g.n > 0)
+      neib_check_kernel<<<std::min<int64_t>(blocks(9 * g.n), kCheckBlocks), 256, 0, st>>>(
+          L.neib.as<int32_t>(), 9 * g.n, g.n, S->err.as<int>());
     // each origin's block pairs (a counting sort of the pairs by origin)
     std::vector<int32_t> first((size_t)g.n + 1, 0), order((size_t)std::max<int64_t>(g.nblock, 1));
     for (int64_t k = 0; k < g.nblock; ++k) ++first[(size_t)g.block_in[k] + 1];
@@ -532,9 +551,15 @@ int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom
     WK(L.moved.reserve((size_t)g.n));
     WK(L.block_moved.reserve((size_t)g.nblock));
   }
-  WK(S->err.reserve(sizeof(int)));
+  int bad = 0;
+  WK(cudaMemcpyAsync(&bad, S->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   WK(cudaStreamSynchronize(st));
   S->resident = false;
+  if (bad) {
+    S->levels.clear();  // no geometry: the distance calls refuse until the next upload
+    set_last_error("wall geometry: neighbour index out of the level's boxes");
+    return IBGPU_E_ARG;
+  }
   return IBGPU_OK;
 }
 

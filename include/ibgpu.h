@@ -230,7 +230,10 @@ typedef struct ibgpu_wall_level_geom {
 } ibgpu_wall_level_geom;
 
 /* After every regrid: the boxes of every level.  IBGPU_E_ARG when a block
- * ghost is the target of two pairs or the origin of one. */
+ * ghost is the target of two pairs or the origin of one (the geometry held
+ * before stays), or when a neighbour index lies outside its level's boxes
+ * (checked on the device after the copies: the context then holds no wall
+ * geometry until the next call). */
 int ibgpu_wall_geometry(ibgpu_ctx *ctx, int nlevels, const ibgpu_wall_level_geom *levels);
 
 typedef struct ibgpu_wall_bodies {

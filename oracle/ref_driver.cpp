@@ -593,6 +593,9 @@ int main(int argc, char **argv) {
   // the download before and the upload after) in regrid_time
   double loop_time = 0.0, move_time = 0.0, regrid_time = 0.0;
   double rg_tag = 0.0, rg_download = 0.0, rg_adapt = 0.0, rg_upload = 0.0;  // regrid parts
+#ifdef ORACLE_BINDING
+  IbgpuUploadTimes rg_up;  // the upload's parts over the timed regrids
+#endif
   long long cell_updates = 0;
   for (int s = 0; s < nsteps; ++s) {
     // leaf cells of the levels that march this step (subcycling schedule)
@@ -659,7 +662,17 @@ int main(int argc, char **argv) {
       amr.PerformAdaptive(sphere);
       tr3 = MPI_Wtime();
 #ifdef ORACLE_BINDING
+      const IbgpuUploadTimes u0 = ibgpu_upload_times();
       if (gpu_step) gpu_check(flowsolver.Upload(amr, sphere), "upload");
+      if (timed_regrid) {
+        const IbgpuUploadTimes &u1 = ibgpu_upload_times();
+        rg_up.flatten += u1.flatten - u0.flatten;
+        rg_up.lists += u1.lists - u0.lists;
+        rg_up.wall_geometry += u1.wall_geometry - u0.wall_geometry;
+        rg_up.wall_pack += u1.wall_pack - u0.wall_pack;
+        rg_up.wall_device += u1.wall_device - u0.wall_device;
+        rg_up.rows_map += u1.rows_map - u0.rows_map;
+      }
 #endif
     }
     MPI_Barrier(MPI_COMM_WORLD);
@@ -696,11 +709,14 @@ int main(int argc, char **argv) {
                   rg_tag, rg_download, rg_adapt, rg_upload);
     rphases = buf;
 #ifdef ORACLE_BINDING
-    const IbgpuUploadTimes &ut = ibgpu_upload_times();
+    // the upload's parts over the timed regrids (rank 0): the cell rows and
+    // lists flattened, the library's uploads, the wall geometry (packing
+    // with the node barrier, then the device call), the box -> row maps
     std::snprintf(buf, sizeof buf,
-                  ", \"upload_flatten_all\": %.6f, \"upload_lists_all\": %.6f, "
-                  "\"upload_wall_geometry_all\": %.6f",
-                  ut.flatten, ut.lists, ut.wall_geometry);
+                  ", \"upload_flatten\": %.6f, \"upload_lists\": %.6f, "
+                  "\"upload_wall_pack\": %.6f, \"upload_wall_device\": %.6f, "
+                  "\"upload_rows_map\": %.6f",
+                  rg_up.flatten, rg_up.lists, rg_up.wall_pack, rg_up.wall_device, rg_up.rows_map);
     rphases += buf;
 #endif
     rphases += "}";

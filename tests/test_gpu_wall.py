@@ -89,6 +89,14 @@ def test_invalid_pairs_and_geometry_are_reported(cuda_lib, pkg):
     with pytest.raises(ib.IbgpuError) as e:
         sol.wall_geometry([bad])  # a block ghost targeted twice
     assert e.value.code == ib.E_ARG
+    neib = np.array(geom["neib"], copy=True)
+    neib.reshape(-1)[-1] = len(geom["kind"])  # one past the level's boxes
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_geometry([dict(geom, neib=neib)])
+    assert e.value.code == ib.E_ARG
+    with pytest.raises(ib.IbgpuError) as e:
+        sol.wall_distance(bodies, [p])  # the bad geometry was dropped
+    assert e.value.code == ib.E_STATE
     sol.wall_geometry([geom])
     p["body"][np.flatnonzero(p["signdis"] < 1.0)[0]] = 7  # no such body
     p["nblock"] = pairs["nblock"]
